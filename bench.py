@@ -1,0 +1,382 @@
+"""Benchmark: batched slab-graph updates on R-MAT scale 22 (the large config).
+
+Workload (`rmat22_mixed_1M`): R-MAT scale 22 (4,194,304 vertices, 67,108,864
+distinct directed edges, a/b/c/d = .57/.19/.19/.05, seeded), uint32 weights
+uniform in [1, 1000], weighted slab graph with exact degree hints and load
+factor 0.7.  One step applies one mixed batch of 1,000,000 edges: a delete
+sub-batch of 500,000 present edges, then an insert sub-batch of 500,000
+absent edges (uniformly sampled, seeded, generated on the host).
+
+Reported:
+  value      edge updates/s over the K timed steps (inputs resident in HBM)
+  e2e        the same through the C ABI with pinned host batches: the H2D
+             copies of each step's batch and the D2H read of the applied counts
+             are inside the timed region
+  roofline   algorithmic bytes of the update kernels / their event-timed
+             duration vs the measured HBM copy bandwidth
+  incremental / decremental BFS and SSSP ms per batch after each sub-batch
+  cpu_baseline  the CPU oracle (multithreaded port) applying mixed batches
+                on the same graph
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SEED = 0x4D45524B + 1  # large config
+METRIC = "edge updates/s"
+HALF = 500_000
+SCALE = 22
+EDGES = 67_108_864
+W_LO, W_HI = 1, 1000
+# algorithmic bytes per applied edge (record + one 128-B slab probe + entry write)
+INS_BYTES = 12 + 128 + 8
+DEL_BYTES = 8 + 128 + 4
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per update launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "k_update_rmat22.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_step:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def make_workload(n_batches: int):
+    import meerkat_b200 as mk
+    t0 = time.time()
+    s, d, w = mk.gen_rmat(SCALE, EDGES, seed=SEED, w_lo=W_LO, w_hi=W_HI)
+    log(f"[bench] R-MAT s{SCALE}: {len(s)} edges in {time.time() - t0:.1f}s")
+    t0 = time.time()
+    es = mk.EdgeSet(1 << SCALE, s, d)
+    batches = []
+    rng = np.random.default_rng(SEED)
+    for b in range(n_batches):
+        ds, dd = es.sample_present(HALF, seed=SEED * 1000 + 2 * b)
+        is_, id_ = es.sample_absent(HALF, seed=SEED * 1000 + 2 * b + 1)
+        iw = rng.integers(W_LO, W_HI + 1, HALF).astype(np.uint32)
+        batches.append((ds, dd, is_, id_, iw))
+    log(f"[bench] {n_batches} mixed batches in {time.time() - t0:.1f}s")
+    return (s, d, w), batches
+
+
+def cpu_baseline(graph, batches, max_batches=3):
+    """The oracle (C, OpenMP, one thread per host core) applying mixed batches."""
+    from oracle import OracleGraph
+    s, d, w = graph
+    T = os.cpu_count() or 1
+    O = OracleGraph(1 << SCALE, threads=T)
+    t0 = time.time()
+    O.insert(s, d, w)
+    log(f"[bench] oracle load {time.time() - t0:.1f}s on {T} threads")
+    times = []
+    applied = 0
+    for (ds, dd, is_, id_, iw) in batches[:max_batches]:
+        t0 = time.perf_counter()
+        n1, _ = O.delete(ds, dd)
+        n2, _ = O.insert(is_, id_, iw)
+        times.append(time.perf_counter() - t0)
+        applied += n1 + n2
+    total = sum(times)
+    return {"value": applied / total, "unit": METRIC, "cores": T, "kind": "port",
+            "sample": f"{len(times)} mixed batches of {2 * HALF} edges on the full R-MAT s22 "
+                      f"graph (hash-set adjacency, one shard per thread)",
+            "seconds": total}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl" if os.environ.get("MK_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path does not exist (the reference is
+    GPU-only and does not build here), so the oracle port stands in, timed on
+    the host cores on the same config and metric."""
+    if rank != 0:
+        return 0
+    graph, batches = make_workload(args.steps + args.warmup)
+    cb = cpu_baseline(graph, batches, max_batches=min(len(batches), max(args.steps, 1)))
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC,
+            "n_gpus": args.gpus, "steps": min(len(batches), args.steps), "warmup": 0,
+            "ms_per_step": 1000.0 * cb["seconds"] / max(1, min(len(batches), args.steps)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": config_block(args.gpus),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_block(n):
+    return {"workload": "rmat22_mixed_1M", "graph": "R-MAT scale 22, 67108864 directed edges, "
+            "a/b/c/d .57/.19/.19/.05, weights U[1,1000]", "batch": "500000 deletes of present "
+            "edges then 500000 inserts of absent edges", "load_factor": 0.7,
+            "degree_hints": "exact", "l2": "inputs larger than L2 (slab pool ~2.5 GB, random "
+            "bucket probes)", "parallelism": f"replicas x{n}" if n > 1 else "single GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--algo-batches", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    import meerkat_b200 as mk
+    from meerkat_b200.build import build
+    if rank == 0:
+        build()
+    barrier(world)
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    W, K, A = args.warmup, args.steps, args.algo_batches
+    graph, batches = make_workload(W + 2 * K + A)
+    s, d, w = graph
+    V = 1 << SCALE
+
+    def todev(a):
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).to(dev)
+
+    hints = np.bincount(s, minlength=V).astype(np.uint32)
+    G = mk.DynamicGraph(V, load_factor=0.7, degree_hints=hints, weighted=True, device=local)
+    G.reserve_batch(HALF)
+    t0 = time.time()
+    G.InsertEdges(todev(s), todev(d), vals=todev(w))
+    assert G.sync() == 0
+    info = G.info()
+    log(f"[bench] graph built in {time.time() - t0:.1f}s: {info}")
+
+    dbatches = [tuple(todev(x) for x in b) for b in batches[:W + K]]
+    stream = torch.cuda.current_stream(dev)
+
+    def step(b, ev=None):
+        ds, dd, is_, id_, iw = b
+        if ev is not None:
+            ev[0].record(stream)
+        G.DeleteEdges(ds, dd)
+        if ev is not None:
+            ev[1].record(stream)
+        G.InsertEdges(is_, id_, vals=iw)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for i in range(W):
+        step(dbatches[i])
+    torch.cuda.synchronize(dev)
+    assert G.sync() == 0
+    barrier(world)
+    clocks = Clocks(local)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    start.record(stream)
+    for i in range(K):
+        step(dbatches[W + i], evs[i])
+    stop.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier(world)
+    ms = start.elapsed_time(stop)
+    ms_max = max_over_ranks(ms, world, dev)
+    assert G.sync() == 0
+    del_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    ins_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    upd_per_step = 2 * HALF
+    value = world * K * upd_per_step / (ms_max / 1000.0)
+
+    # ---- e2e through the C ABI with pinned host batches ----
+    pinned = []
+    for b in batches[W + K:W + 2 * K]:
+        pinned.append(tuple(torch.from_numpy(np.ascontiguousarray(x, dtype=np.uint32).view(np.int32))
+                            .pin_memory() for x in b))
+    bufs = [torch.empty(HALF, dtype=torch.int32, device=dev) for _ in range(5)]
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    applied_e2e = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for b in pinned:
+        for dst_t, src_t in zip(bufs, b):
+            dst_t.copy_(src_t, non_blocking=True)
+        G.DeleteEdges(bufs[0], bufs[1])
+        applied_e2e += G.last_applied()  # 8-byte D2H read of the applied count
+        G.InsertEdges(bufs[2], bufs[3], vals=bufs[4])
+        applied_e2e += G.last_applied()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, dev)
+    assert G.sync() == 0
+    e2e_value = world * K * upd_per_step / (e2e_ms / 1000.0)
+    assert applied_e2e == K * upd_per_step, applied_e2e
+    h2d = HALF * 4 * 5
+    d2h = 16
+
+    # ---- incremental / decremental BFS and SSSP on the same graph ----
+    algo = {}
+    if A > 0:
+        src_v = int(np.argmax(hints))
+        bfs, sssp = mk.BFS(G, src_v, V), mk.SSSP(G, src_v, V)
+        algo["bfs_static_ms"] = bfs.Static()
+        algo["sssp_static_ms"] = sssp.Static()
+        rec = {k: [] for k in ("bfs_dec_ms", "sssp_dec_ms", "bfs_inc_ms", "sssp_inc_ms")}
+        for b in batches[W + 2 * K:W + 2 * K + A]:
+            ds, dd, is_, id_, iw = (todev(x) for x in b)
+            G.DeleteEdges(ds, dd)
+            rec["bfs_dec_ms"].append(bfs.Decremental(ds, dd))
+            rec["sssp_dec_ms"].append(sssp.Decremental(ds, dd))
+            G.InsertEdges(is_, id_, vals=iw)
+            rec["bfs_inc_ms"].append(bfs.Incremental(is_, id_))
+            rec["sssp_inc_ms"].append(sssp.Incremental(is_, id_, wgt=iw))
+        assert G.sync() == 0
+        for k, v in rec.items():
+            algo[k + "_p50"] = statistics.median(v)
+        algo["source"] = src_v
+
+    peak, peak_kind = measured_peak()
+    upd_bytes = HALF * DEL_BYTES + HALF * INS_BYTES
+    upd_ms = statistics.mean(a + b for a, b in zip(del_ms, ins_ms))
+    achieved = upd_bytes / (upd_ms / 1000.0) / 1e9
+    traffic = profile_traffic()
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_baseline(graph, batches[W:W + K], max_batches=3)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": config_block(world),
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": 3 * K,
+            "roofline": {"bound": "hbm", "kernel": "k_delete + k_insert (one mixed batch)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "algorithmic_bytes_per_step": upd_bytes,
+                         "traffic": traffic},
+            "delete_ms_mean": statistics.mean(del_ms), "insert_ms_mean": statistics.mean(ins_ms),
+            "clocks": clk,
+            "queries": algo,
+            "graph": {"slabs_used": info["slabs_used"], "buckets": info["num_buckets"],
+                      "device_bytes": info["device_bytes"]},
+        }
+        if cb is not None:
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

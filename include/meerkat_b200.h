@@ -1,0 +1,281 @@
+/*
+ * meerkat_b200.h -- C ABI of the B200-native dynamic-graph engine.
+ *
+ * Every entry point takes plain pointers and sizes.  Pointers named d_* are
+ * device pointers, h_* are host pointers.  `stream` is a cudaStream_t passed
+ * as void* (NULL = legacy default stream) so this header needs no CUDA
+ * include.  Calls are stream-ordered and asynchronous unless they take a
+ * `float *ms_out`: when ms_out is non-NULL the call synchronises and writes
+ * the elapsed device time of its kernels in milliseconds (the reference's
+ * algorithm calls return that float).
+ *
+ * Each declaration cites the reference interface it replaces
+ * (path:line inside meerkat-pkd/Meerkat).
+ */
+#ifndef MEERKAT_B200_H_
+#define MEERKAT_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Slab word sentinels.  Vertex ids must be < MK_TOMBSTONE_KEY. */
+#define MK_EMPTY_KEY 0xFFFFFFFFu
+#define MK_TOMBSTONE_KEY 0xFFFFFFFEu
+#define MK_EMPTY_SLAB 0xFFFFFFFFu
+/* Unreachable distance (reference: INF, include/Algorithms/definitions.cuh:4). */
+#define MK_INF 0xFFFFFFFFu
+/* Packed distance/parent word: dist << 32 | parent
+ * (reference: PACK/DISTANCE/PARENT, include/Algorithms/definitions.cuh:14-17). */
+#define MK_INFINF 0xFFFFFFFFFFFFFFFFull
+
+typedef enum mk_status {
+  MK_OK = 0,
+  MK_ERR_INVALID = 1, /* bad argument or out-of-range vertex id in a batch  */
+  MK_ERR_OOM = 2,     /* slab pool or device memory exhausted              */
+  MK_ERR_TIMEOUT = 3, /* a bounded device-side wait gave up                */
+  MK_ERR_CUDA = 4,    /* a CUDA runtime call failed                        */
+  MK_ERR_STATE = 5    /* call made in the wrong state (e.g. before Static) */
+} mk_status;
+
+/* Sticky device error bits reported by mk_graph_sync / mk_*_sync. */
+#define MK_DEVERR_INVALID_ID 0x1u
+#define MK_DEVERR_OOM 0x2u
+#define MK_DEVERR_TIMEOUT 0x4u
+#define MK_DEVERR_OVERFLOW 0x8u
+
+/* Message of the last failing call on this host thread. */
+const char *mk_last_error_string(void);
+/* Library version string. */
+const char *mk_version(void);
+
+/* ------------------------------------------------------------------------
+ * Dynamic graph: per-vertex slab hash tables of 128-byte slabs.
+ * Replaces DynamicGraph<EdgePolicy, IsWeighted>
+ * (include/Graph/SlabGraph.cuh:343-506 weighted, :508-752 unweighted).
+ * ---------------------------------------------------------------------- */
+typedef struct mk_graph mk_graph;
+
+typedef struct mk_graph_desc {
+  uint32_t num_vertices;  /* N (reference ctor arg, SlabGraph.cuh:382)        */
+  uint32_t weighted;      /* 1 = (key, value) slabs: WeightedEdgePolicyMapT    */
+  uint32_t reverse;       /* 1 = edges keyed by destination: Rev*EdgePolicyT   */
+  uint32_t flags;         /* reserved, must be 0                               */
+  double load_factor;     /* LoadFactor (SlabGraph.cuh:403-407), e.g. 0.7      */
+  const uint32_t *h_degree_hints; /* VertexDegreeHints[N] or NULL (= all 1)    */
+  int32_t device;         /* DeviceIdx                                         */
+  uint32_t pad0;
+  uint64_t pool_slabs;    /* overflow slab capacity; 0 = automatic             */
+} mk_graph_desc;
+
+typedef struct mk_graph_info {
+  uint32_t num_vertices;
+  uint32_t weighted;
+  uint32_t reverse;
+  uint32_t keys_per_slab;  /* 31 (set) or 15 (map)                      */
+  uint64_t num_buckets;    /* head slabs                                */
+  uint64_t pool_capacity;  /* head + overflow slabs                     */
+  uint64_t slabs_used;     /* head + allocated overflow slabs           */
+  uint64_t num_edges;      /* live edges = sum of degrees               */
+  uint64_t device_bytes;   /* bytes of device memory held by the graph  */
+} mk_graph_info;
+
+/* DynamicGraph(N, Allocator&, LoadFactor, DegreeHints*, DeviceIdx)
+ * (SlabGraph.cuh:382-466, :633-717). */
+mk_status mk_graph_create(const mk_graph_desc *desc, mk_graph **out);
+/* ~DynamicGraph (SlabGraph.cuh:470-480). */
+mk_status mk_graph_destroy(mk_graph *g);
+
+/* InsertEdges(src*, dst*, n, vals*) (SlabGraph.cuh:486-488, impl
+ * SlabGraphImpl.cuh:6-34).  Self-loops are skipped (InsertEdgeKernel.cuh:25).
+ * Set semantics: an edge that is already live is left unchanged; of several
+ * copies of one edge inside a batch the lowest batch index wins.  d_w may be
+ * NULL (weight 0) and is ignored for unweighted graphs. */
+mk_status mk_graph_insert_edges(mk_graph *g, const uint32_t *d_src,
+                                const uint32_t *d_dst, const uint32_t *d_w,
+                                uint32_t n, void *stream);
+/* DeleteEdges(src*, dst*, n) (SlabGraph.cuh:490-491, SlabGraphImpl.cuh:36-62).
+ * A live edge becomes a tombstone; absent edges and self-loops are no-ops. */
+mk_status mk_graph_delete_edges(mk_graph *g, const uint32_t *d_src,
+                                const uint32_t *d_dst, uint32_t n,
+                                void *stream);
+/* Batched SearchEdge (include/Graph/warp/SearchEdge.cuh:8-63, :118-142):
+ * d_found[i] = 1 if (src[i], dst[i]) is live; d_w[i] = its value (may be NULL). */
+mk_status mk_graph_search_edges(mk_graph *g, const uint32_t *d_src,
+                                const uint32_t *d_dst, uint32_t n,
+                                uint8_t *d_found, uint32_t *d_w, void *stream);
+/* Waits for the graph's work on `stream`, returns MK_OK or the first error and
+ * writes the sticky device error bits (MK_DEVERR_*) to *h_deverr if given. */
+mk_status mk_graph_sync(mk_graph *g, void *stream, uint32_t *h_deverr);
+/* Number of batch edges the last insert/delete actually applied (synchronises). */
+mk_status mk_graph_last_applied(mk_graph *g, uint64_t *h_count);
+/* Device pointer to the per-edge applied flags (uint8, one per batch entry)
+ * of the last insert/delete; valid until the next update call. */
+mk_status mk_graph_last_applied_flags(mk_graph *g, const uint8_t **d_flags,
+                                      uint32_t *n);
+/* Vertex degrees: GetVertexDegrees (SlabGraph.cuh:303-305). */
+mk_status mk_graph_degrees(mk_graph *g, uint32_t *d_out, void *stream);
+/* GetVertexBucketsOffsets / GetBucketsPerVertex (SlabGraph.cuh:483-484):
+ * host copies, N entries each (either pointer may be NULL). */
+mk_status mk_graph_bucket_layout(mk_graph *g, uint32_t *h_offsets,
+                                 uint32_t *h_buckets_per_vertex);
+mk_status mk_graph_get_info(mk_graph *g, mk_graph_info *out);
+/* Compacts live edges into CSR (row_ptr has N+1 entries; rows in slab order).
+ * Mirrors CollectEdges (include/Algorithms/impl/TCImpl.cuh:110-147) and the
+ * test kernels CollectEdges (test/GraphTest.cu:285-346).  d_col and d_w need
+ * room for num_edges entries; d_w may be NULL. */
+mk_status mk_graph_export_csr(mk_graph *g, uint64_t *d_row_ptr,
+                              uint32_t *d_col, uint32_t *d_w, void *stream);
+/* Per-vertex tombstone count (test/GraphTest.cu:58-95 CountTombstones). */
+mk_status mk_graph_count_tombstones(mk_graph *g, uint32_t *d_out,
+                                    void *stream);
+/* Pre-sizes the per-batch scratch for batches of up to n edges so later
+ * updates of that size allocate nothing. */
+mk_status mk_graph_reserve_batch(mk_graph *g, uint32_t n);
+
+/* ------------------------------------------------------------------------
+ * BFS and SSSP (replace BFS<AllocPolicy>, include/Algorithms/BFS.cuh:13-69,
+ * and SSSP<AllocPolicy>, include/Algorithms/SSSP.cuh:11-69).  A BFS may run
+ * on a weighted graph (weights ignored).  SSSP needs a weighted graph.
+ * Call protocol as in the reference drivers (src/BFS.cu:111-121): update the
+ * graph first, then call Incremental/Decremental with the same batch.
+ * ---------------------------------------------------------------------- */
+typedef struct mk_traversal mk_traversal;
+
+/* BFS(G, SourceVertex, VertexN) (BFS.cuh:34-53); sets dist[src] = 0. */
+mk_status mk_bfs_create(mk_graph *g, uint32_t source, mk_traversal **out);
+/* SSSP(G, SourceVertex, VertexN) (SSSP.cuh:33-52). */
+mk_status mk_sssp_create(mk_graph *g, uint32_t source, mk_traversal **out);
+/* float Static(EdgesN) (BFSImpl.cuh:590-662, SSSPImpl.cuh:607-690). */
+mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out);
+/* float Incremental(src*, dst*, n) (BFSImpl.cuh:664-753, SSSPImpl.cuh:692-785).
+ * d_w is accepted for the SSSP signature and ignored: the stored weight of
+ * each edge is used. */
+mk_status mk_traversal_incremental(mk_traversal *t, const uint32_t *d_src,
+                                   const uint32_t *d_dst, const uint32_t *d_w,
+                                   uint32_t n, void *stream, float *ms_out);
+/* float Decremental(src*, dst*, n) (BFSImpl.cuh:755-846, SSSPImpl.cuh:787-876). */
+mk_status mk_traversal_decremental(mk_traversal *t, const uint32_t *d_src,
+                                   const uint32_t *d_dst, const uint32_t *d_w,
+                                   uint32_t n, void *stream, float *ms_out);
+/* Distances() (BFS.cuh:55-60): N distances, MK_INF = unreachable (host). */
+mk_status mk_traversal_distances(mk_traversal *t, uint32_t *h_out);
+/* Device pointer to the packed dist<<32|parent array (N entries). */
+mk_status mk_traversal_packed(mk_traversal *t, const uint64_t **d_packed);
+/* Host copy of the packed array (N entries). */
+mk_status mk_traversal_packed_host(mk_traversal *t, uint64_t *h_out);
+/* Work counters of the last call: levels run and vertices pushed. */
+mk_status mk_traversal_stats(mk_traversal *t, uint32_t *h_levels,
+                             uint64_t *h_pushed);
+mk_status mk_traversal_destroy(mk_traversal *t);
+
+/* ------------------------------------------------------------------------
+ * PageRank (replaces PageRank<AllocPolicy>, include/Algorithms/PageRank.cuh:9-67).
+ * g must be a reverse graph (in-edges), as RevUnweightedEdgePolicyT in the
+ * reference.  h_out_degree (N entries) may be NULL: out-degrees are then
+ * counted from the graph.
+ * ---------------------------------------------------------------------- */
+typedef struct mk_pagerank mk_pagerank;
+
+/* PageRank(G, DampingFactor, ErrorMargin, VertexN, OutDeg*, MaxIter)
+ * (PageRank.cuh:32-46). */
+mk_status mk_pagerank_create(mk_graph *g_rev, float damping, float tol,
+                             uint32_t max_iter, const uint32_t *h_out_degree,
+                             mk_pagerank **out);
+/* float Static() (PageRankImpl.cuh:218-220). */
+mk_status mk_pagerank_static(mk_pagerank *p, void *stream, float *ms_out);
+/* float Incremental/Decremental(src*, dst*, n) (PageRankImpl.cuh:222-251):
+ * out-degrees follow the edges the last graph update applied, then the
+ * ranks are re-solved warm-started from the previous ranks. */
+mk_status mk_pagerank_incremental(mk_pagerank *p, const uint32_t *d_src,
+                                  const uint32_t *d_dst, uint32_t n,
+                                  void *stream, float *ms_out);
+mk_status mk_pagerank_decremental(mk_pagerank *p, const uint32_t *d_src,
+                                  const uint32_t *d_dst, uint32_t n,
+                                  void *stream, float *ms_out);
+/* Values() (PageRank.cuh:48-53), host. */
+mk_status mk_pagerank_values(mk_pagerank *p, float *h_out);
+mk_status mk_pagerank_values_device(mk_pagerank *p, const float **d_values);
+/* Iterations run and the final L1 change of the last solve. */
+mk_status mk_pagerank_stats(mk_pagerank *p, uint32_t *h_iters,
+                            float *h_delta);
+mk_status mk_pagerank_destroy(mk_pagerank *p);
+
+/* ------------------------------------------------------------------------
+ * Triangle counting on a symmetric graph (replaces TC<AllocPolicy>,
+ * include/Algorithms/TC.cuh:9-40).
+ * ---------------------------------------------------------------------- */
+typedef struct mk_tc mk_tc;
+mk_status mk_tc_create(mk_graph *g, mk_tc **out);
+/* float Static(EdgesN) (TCImpl.cuh:288-380). */
+mk_status mk_tc_static(mk_tc *t, void *stream, float *ms_out);
+/* float Incremental/Decremental(src*, dst*, n, Alloc)
+ * (TCImpl.cuh:431-565).  The batch is read as undirected pairs. */
+mk_status mk_tc_incremental(mk_tc *t, const uint32_t *d_src,
+                            const uint32_t *d_dst, uint32_t n, void *stream,
+                            float *ms_out);
+mk_status mk_tc_decremental(mk_tc *t, const uint32_t *d_src,
+                            const uint32_t *d_dst, uint32_t n, void *stream,
+                            float *ms_out);
+/* GetCount() (TC.cuh:31). */
+mk_status mk_tc_count(mk_tc *t, uint64_t *h_count);
+mk_status mk_tc_destroy(mk_tc *t);
+
+/* ------------------------------------------------------------------------
+ * Weakly connected components by lock-free union-find with min-id labels.
+ * The reference ships only the device primitives
+ * (include/Util/UnionFind.cuh:24-254) and no entry point; these are new.
+ * ---------------------------------------------------------------------- */
+typedef struct mk_wcc mk_wcc;
+mk_status mk_wcc_create(mk_graph *g, mk_wcc **out);
+mk_status mk_wcc_static(mk_wcc *w, void *stream, float *ms_out);
+mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src,
+                             const uint32_t *d_dst, uint32_t n, void *stream,
+                             float *ms_out);
+mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src,
+                             const uint32_t *d_dst, uint32_t n, void *stream,
+                             float *ms_out);
+/* N labels: the minimum vertex id of each vertex's component (host). */
+mk_status mk_wcc_labels(mk_wcc *w, uint32_t *h_out);
+mk_status mk_wcc_labels_device(mk_wcc *w, const uint32_t **d_labels);
+mk_status mk_wcc_destroy(mk_wcc *w);
+
+/* ------------------------------------------------------------------------
+ * Synthetic inputs (host only; no GPU needed).  Seeded and deterministic.
+ * ---------------------------------------------------------------------- */
+/* R-MAT: exactly num_edges distinct directed edges without self-loops over
+ * 2^scale vertices, probabilities a, b, c (d = 1-a-b-c).  h_w (may be NULL)
+ * gets weights uniform in [w_lo, w_hi]. */
+mk_status mk_gen_rmat(uint32_t scale, uint64_t num_edges, double a, double b,
+                      double c, uint64_t seed, uint32_t w_lo, uint32_t w_hi,
+                      uint32_t *h_src, uint32_t *h_dst, uint32_t *h_w);
+/* side x side 4-neighbour grid, both directions, plus `shortcuts` random
+ * directed long-range edges.  Returns the edge count in *h_num_edges; pass
+ * NULL arrays first to query the count. */
+mk_status mk_gen_grid(uint32_t side, uint64_t shortcuts, uint64_t seed,
+                      uint32_t w_lo, uint32_t w_hi, uint32_t *h_src,
+                      uint32_t *h_dst, uint32_t *h_w, uint64_t *h_num_edges);
+
+/* Host edge-set tracker used to draw valid update batches: absent-edge
+ * inserts and present-edge deletes, sampled uniformly. */
+typedef struct mk_edgeset mk_edgeset;
+mk_status mk_edgeset_create(uint32_t num_vertices, const uint32_t *h_src,
+                            const uint32_t *h_dst, uint64_t n,
+                            mk_edgeset **out);
+mk_status mk_edgeset_destroy(mk_edgeset *s);
+uint64_t mk_edgeset_size(const mk_edgeset *s);
+/* Draws n distinct absent edges (u != v), adds them to the set. */
+mk_status mk_edgeset_sample_absent(mk_edgeset *s, uint64_t n, uint64_t seed,
+                                   uint32_t *h_src, uint32_t *h_dst);
+/* Draws n distinct present edges uniformly, removes them from the set. */
+mk_status mk_edgeset_sample_present(mk_edgeset *s, uint64_t n, uint64_t seed,
+                                    uint32_t *h_src, uint32_t *h_dst);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MEERKAT_B200_H_ */

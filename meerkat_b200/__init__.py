@@ -1,0 +1,446 @@
+"""meerkat_b200: B200-native dynamic-graph engine (slab-hash graph, batched
+updates, incremental/decremental BFS, SSSP, PageRank, triangle counting and
+connected components) behind a C ABI.
+
+This module is the Python mirror of the reference's C++ classes
+(DynamicGraph, BFS, SSSP, PageRank, TC; meerkat-pkd/Meerkat
+include/Graph/SlabGraph.cuh and include/Algorithms/*.cuh) over that ABI.
+Batch arrays are CUDA tensors (int32 or uint32 storage) or raw device
+pointers.  There is no CPU fallback: every call runs the sm_100a kernels of
+libmeerkat_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, check, lib)
+
+__all__ = ["DynamicGraph", "BFS", "SSSP", "PageRank", "TC", "WCC", "EdgeSet", "gen_rmat",
+           "gen_grid", "MeerkatError", "MK_INF", "lib", "version"]
+
+
+def version() -> str:
+    return lib().mk_version().decode()
+
+
+def _ptr(x) -> Optional[int]:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return x.data_ptr()
+
+
+def _count(x, n):
+    if n is not None:
+        return int(n)
+    return int(x.numel()) if hasattr(x, "numel") else int(len(x))
+
+
+def _stream(s) -> Optional[int]:
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    return s.cuda_stream
+
+
+class _Timed:
+    """Reference algorithm calls return elapsed milliseconds (float)."""
+
+    def _call(self, fn, *args, timed=True):
+        ms = C.c_float(0.0)
+        check(fn(*args, C.byref(ms) if timed else None), fn.__name__)
+        return ms.value if timed else None
+
+
+class DynamicGraph:
+    """DynamicGraph<EdgePolicy, IsWeighted>(N, Allocator&, LoadFactor, hints, dev)
+    (include/Graph/SlabGraph.cuh:382-466).  `weighted` selects the map slabs of
+    WeightedEdgePolicyMapT, `reverse` the Rev* policies (edges keyed by
+    destination)."""
+
+    def __init__(self, num_vertices: int, load_factor: float = 0.7, degree_hints=None,
+                 weighted: bool = False, reverse: bool = False, device: int = 0,
+                 pool_slabs: int = 0):
+        L = lib()
+        self.num_vertices = int(num_vertices)
+        self.weighted = bool(weighted)
+        self.reverse = bool(reverse)
+        self._hints = None
+        d = GraphDesc()
+        d.num_vertices = self.num_vertices
+        d.weighted = int(weighted)
+        d.reverse = int(reverse)
+        d.flags = 0
+        d.load_factor = float(load_factor)
+        if degree_hints is not None:
+            self._hints = np.ascontiguousarray(np.asarray(degree_hints, dtype=np.uint32))
+            d.h_degree_hints = self._hints.ctypes.data_as(C.POINTER(C.c_uint32))
+        d.device = int(device)
+        d.pool_slabs = int(pool_slabs)
+        h = C.c_void_p()
+        check(L.mk_graph_create(C.byref(d), C.byref(h)), "mk_graph_create")
+        self._h = h
+        self.device = int(device)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def InsertEdges(self, src, dst, n=None, vals=None, stream=None):
+        """InsertEdges(src*, dst*, n, vals*) (SlabGraph.cuh:486-488)."""
+        check(lib().mk_graph_insert_edges(self._h, _ptr(src), _ptr(dst), _ptr(vals),
+                                          _count(src, n), _stream(stream)),
+              "mk_graph_insert_edges")
+
+    def DeleteEdges(self, src, dst, n=None, stream=None):
+        """DeleteEdges(src*, dst*, n) (SlabGraph.cuh:490-491)."""
+        check(lib().mk_graph_delete_edges(self._h, _ptr(src), _ptr(dst), _count(src, n),
+                                          _stream(stream)), "mk_graph_delete_edges")
+
+    def SearchEdges(self, src, dst, found, weights=None, n=None, stream=None):
+        check(lib().mk_graph_search_edges(self._h, _ptr(src), _ptr(dst), _count(src, n),
+                                          _ptr(found), _ptr(weights), _stream(stream)),
+              "mk_graph_search_edges")
+
+    def reserve_batch(self, n: int) -> None:
+        check(lib().mk_graph_reserve_batch(self._h, int(n)), "mk_graph_reserve_batch")
+
+    def sync(self, stream=None) -> int:
+        err = C.c_uint32(0)
+        check(lib().mk_graph_sync(self._h, _stream(stream), C.byref(err)), "mk_graph_sync")
+        return err.value
+
+    def last_applied(self) -> int:
+        c = C.c_uint64(0)
+        check(lib().mk_graph_last_applied(self._h, C.byref(c)), "mk_graph_last_applied")
+        return c.value
+
+    def degrees_into(self, out, stream=None):
+        check(lib().mk_graph_degrees(self._h, _ptr(out), _stream(stream)), "mk_graph_degrees")
+
+    def GetVertexBucketsOffsets(self) -> np.ndarray:
+        out = np.zeros(self.num_vertices, dtype=np.uint32)
+        check(lib().mk_graph_bucket_layout(self._h, out.ctypes.data, None), "bucket_layout")
+        return out
+
+    def GetBucketsPerVertex(self) -> np.ndarray:
+        out = np.zeros(self.num_vertices, dtype=np.uint32)
+        check(lib().mk_graph_bucket_layout(self._h, None, out.ctypes.data), "bucket_layout")
+        return out
+
+    def info(self) -> dict:
+        i = GraphInfo()
+        check(lib().mk_graph_get_info(self._h, C.byref(i)), "mk_graph_get_info")
+        return {f: getattr(i, f) for f, _ in GraphInfo._fields_}
+
+    # --- host-side views used by the tests (need torch for device buffers) ---
+    def degrees(self) -> np.ndarray:
+        import torch
+        out = torch.empty(self.num_vertices, dtype=torch.int32, device=f"cuda:{self.device}")
+        self.degrees_into(out)
+        torch.cuda.synchronize(self.device)
+        return out.cpu().numpy().view(np.uint32)
+
+    def tombstones(self) -> np.ndarray:
+        import torch
+        out = torch.empty(self.num_vertices, dtype=torch.int32, device=f"cuda:{self.device}")
+        check(lib().mk_graph_count_tombstones(self._h, out.data_ptr(), None), "tombstones")
+        torch.cuda.synchronize(self.device)
+        return out.cpu().numpy().view(np.uint32)
+
+    def export_csr(self, sort_rows: bool = True):
+        """Live edges as CSR (row_ptr u64[N+1], col u32[E], w u32[E] or None)."""
+        import torch
+        dev = f"cuda:{self.device}"
+        E = self.info()["num_edges"]
+        rp = torch.empty(self.num_vertices + 1, dtype=torch.int64, device=dev)
+        col = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+        w = torch.empty(max(E, 1), dtype=torch.int32, device=dev) if self.weighted else None
+        check(lib().mk_graph_export_csr(self._h, rp.data_ptr(), col.data_ptr(), _ptr(w), None),
+              "mk_graph_export_csr")
+        torch.cuda.synchronize(self.device)
+        rp_h = rp.cpu().numpy().view(np.uint64)
+        col_h = col.cpu().numpy().view(np.uint32)[:E]
+        w_h = w.cpu().numpy().view(np.uint32)[:E] if w is not None else None
+        if sort_rows:
+            rows = np.repeat(np.arange(self.num_vertices, dtype=np.uint64), np.diff(rp_h))
+            order = np.lexsort((col_h, rows))
+            col_h = col_h[order]
+            if w_h is not None:
+                w_h = w_h[order]
+        return rp_h, col_h, w_h
+
+
+class _Traversal(_Timed):
+    _create = None
+
+    def __init__(self, G: DynamicGraph, source: int, num_vertices: Optional[int] = None):
+        if num_vertices is not None and int(num_vertices) != G.num_vertices:
+            raise ValueError("VertexN must equal the graph's vertex count")
+        self.G = G
+        self.source = int(source)
+        h = C.c_void_p()
+        check(getattr(lib(), self._create)(G.handle, self.source, C.byref(h)), self._create)
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_traversal_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Static(self, edges_n=None, stream=None, timed=True):
+        return self._call(lib().mk_traversal_static, self._h, _stream(stream), timed=timed)
+
+    def Incremental(self, src, dst, n=None, wgt=None, stream=None, timed=True):
+        return self._call(lib().mk_traversal_incremental, self._h, _ptr(src), _ptr(dst),
+                          _ptr(wgt), _count(src, n), _stream(stream), timed=timed)
+
+    def Decremental(self, src, dst, n=None, wgt=None, stream=None, timed=True):
+        return self._call(lib().mk_traversal_decremental, self._h, _ptr(src), _ptr(dst),
+                          _ptr(wgt), _count(src, n), _stream(stream), timed=timed)
+
+    def Distances(self) -> np.ndarray:
+        out = np.zeros(self.G.num_vertices, dtype=np.uint32)
+        check(lib().mk_traversal_distances(self._h, out.ctypes.data), "mk_traversal_distances")
+        return out
+
+    def packed_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib().mk_traversal_packed(self._h, C.byref(p)), "mk_traversal_packed")
+        return p.value
+
+    def packed(self) -> np.ndarray:
+        """Host copy of the packed dist<<32|parent array."""
+        out = np.zeros(self.G.num_vertices, dtype=np.uint64)
+        check(lib().mk_traversal_packed_host(self._h, out.ctypes.data), "mk_traversal_packed_host")
+        return out
+
+    def stats(self):
+        lv = C.c_uint32(0)
+        pushed = C.c_uint64(0)
+        check(lib().mk_traversal_stats(self._h, C.byref(lv), C.byref(pushed)), "stats")
+        return lv.value, pushed.value
+
+
+class BFS(_Traversal):
+    """BFS<AllocPolicy>(G, SourceVertex, VertexN) (include/Algorithms/BFS.cuh:13-69)."""
+    _create = "mk_bfs_create"
+
+
+class SSSP(_Traversal):
+    """SSSP<AllocPolicy>(G, SourceVertex, VertexN) (include/Algorithms/SSSP.cuh:11-69)."""
+    _create = "mk_sssp_create"
+
+
+class PageRank(_Timed):
+    """PageRank<AllocPolicy>(G, d, tol, N, OutDeg*, MaxIter)
+    (include/Algorithms/PageRank.cuh:9-67); G must be a reverse graph."""
+
+    def __init__(self, G: DynamicGraph, damping: float, tol: float, num_vertices=None,
+                 out_degree=None, max_iter: int = 100):
+        if not G.reverse:
+            raise ValueError("PageRank pulls over in-edges: build the graph with reverse=True")
+        self.G = G
+        self._od = None
+        if out_degree is not None:
+            self._od = np.ascontiguousarray(np.asarray(out_degree, dtype=np.uint32))
+        h = C.c_void_p()
+        check(lib().mk_pagerank_create(G.handle, float(damping), float(tol), int(max_iter),
+                                       _ptr(self._od), C.byref(h)), "mk_pagerank_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_pagerank_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Static(self, stream=None, timed=True):
+        return self._call(lib().mk_pagerank_static, self._h, _stream(stream), timed=timed)
+
+    def Incremental(self, src, dst, n=None, stream=None, timed=True):
+        return self._call(lib().mk_pagerank_incremental, self._h, _ptr(src), _ptr(dst),
+                          _count(src, n), _stream(stream), timed=timed)
+
+    def Decremental(self, src, dst, n=None, stream=None, timed=True):
+        return self._call(lib().mk_pagerank_decremental, self._h, _ptr(src), _ptr(dst),
+                          _count(src, n), _stream(stream), timed=timed)
+
+    def Values(self) -> np.ndarray:
+        out = np.zeros(self.G.num_vertices, dtype=np.float32)
+        check(lib().mk_pagerank_values(self._h, out.ctypes.data), "mk_pagerank_values")
+        return out
+
+    def stats(self):
+        it = C.c_uint32(0)
+        dl = C.c_float(0)
+        check(lib().mk_pagerank_stats(self._h, C.byref(it), C.byref(dl)), "mk_pagerank_stats")
+        return it.value, dl.value
+
+
+class TC(_Timed):
+    """TC<AllocPolicy>(G, N) (include/Algorithms/TC.cuh:9-40); G symmetric."""
+
+    def __init__(self, G: DynamicGraph, num_vertices=None):
+        self.G = G
+        h = C.c_void_p()
+        check(lib().mk_tc_create(G.handle, C.byref(h)), "mk_tc_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_tc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Static(self, edges_n=None, stream=None, timed=True):
+        return self._call(lib().mk_tc_static, self._h, _stream(stream), timed=timed)
+
+    def Incremental(self, src, dst, n=None, alloc=None, stream=None, timed=True):
+        return self._call(lib().mk_tc_incremental, self._h, _ptr(src), _ptr(dst), _count(src, n),
+                          _stream(stream), timed=timed)
+
+    def Decremental(self, src, dst, n=None, alloc=None, stream=None, timed=True):
+        return self._call(lib().mk_tc_decremental, self._h, _ptr(src), _ptr(dst), _count(src, n),
+                          _stream(stream), timed=timed)
+
+    def GetCount(self) -> int:
+        c = C.c_uint64(0)
+        check(lib().mk_tc_count(self._h, C.byref(c)), "mk_tc_count")
+        return c.value
+
+
+class WCC(_Timed):
+    """Connected components (new entry points over include/Util/UnionFind.cuh)."""
+
+    def __init__(self, G: DynamicGraph):
+        self.G = G
+        h = C.c_void_p()
+        check(lib().mk_wcc_create(G.handle, C.byref(h)), "mk_wcc_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_wcc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Static(self, stream=None, timed=True):
+        return self._call(lib().mk_wcc_static, self._h, _stream(stream), timed=timed)
+
+    def Incremental(self, src, dst, n=None, stream=None, timed=True):
+        return self._call(lib().mk_wcc_incremental, self._h, _ptr(src), _ptr(dst), _count(src, n),
+                          _stream(stream), timed=timed)
+
+    def Decremental(self, src, dst, n=None, stream=None, timed=True):
+        return self._call(lib().mk_wcc_decremental, self._h, _ptr(src), _ptr(dst), _count(src, n),
+                          _stream(stream), timed=timed)
+
+    def Labels(self) -> np.ndarray:
+        out = np.zeros(self.G.num_vertices, dtype=np.uint32)
+        check(lib().mk_wcc_labels(self._h, out.ctypes.data), "mk_wcc_labels")
+        return out
+
+
+# ---------------------------------------------------------------------------
+# synthetic inputs (host only)
+# ---------------------------------------------------------------------------
+def gen_rmat(scale: int, num_edges: int, a=0.57, b=0.19, c=0.19, seed=0, w_lo=1, w_hi=64,
+             weights=True):
+    src = np.empty(num_edges, dtype=np.uint32)
+    dst = np.empty(num_edges, dtype=np.uint32)
+    w = np.empty(num_edges, dtype=np.uint32) if weights else None
+    check(lib().mk_gen_rmat(scale, num_edges, a, b, c, seed, w_lo, w_hi, src.ctypes.data,
+                            dst.ctypes.data, _ptr(w)), "mk_gen_rmat")
+    return src, dst, w
+
+
+def gen_grid(side: int, shortcuts: int, seed=0, w_lo=1, w_hi=1000, weights=True):
+    n = C.c_uint64(0)
+    check(lib().mk_gen_grid(side, shortcuts, seed, w_lo, w_hi, None, None, None, C.byref(n)),
+          "mk_gen_grid")
+    src = np.empty(n.value, dtype=np.uint32)
+    dst = np.empty(n.value, dtype=np.uint32)
+    w = np.empty(n.value, dtype=np.uint32) if weights else None
+    check(lib().mk_gen_grid(side, shortcuts, seed, w_lo, w_hi, src.ctypes.data, dst.ctypes.data,
+                            _ptr(w), C.byref(n)), "mk_gen_grid")
+    return src, dst, w
+
+
+class EdgeSet:
+    """Host edge set for drawing valid batches (absent inserts / present deletes)."""
+
+    def __init__(self, num_vertices: int, src: np.ndarray, dst: np.ndarray):
+        h = C.c_void_p()
+        src = np.ascontiguousarray(src, dtype=np.uint32)
+        dst = np.ascontiguousarray(dst, dtype=np.uint32)
+        check(lib().mk_edgeset_create(num_vertices, src.ctypes.data, dst.ctypes.data, len(src),
+                                      C.byref(h)), "mk_edgeset_create")
+        self._h = h
+
+    def __len__(self):
+        return int(lib().mk_edgeset_size(self._h))
+
+    def sample_absent(self, n: int, seed: int):
+        s = np.empty(n, dtype=np.uint32)
+        d = np.empty(n, dtype=np.uint32)
+        check(lib().mk_edgeset_sample_absent(self._h, n, seed, s.ctypes.data, d.ctypes.data),
+              "sample_absent")
+        return s, d
+
+    def sample_present(self, n: int, seed: int):
+        s = np.empty(n, dtype=np.uint32)
+        d = np.empty(n, dtype=np.uint32)
+        check(lib().mk_edgeset_sample_present(self._h, n, seed, s.ctypes.data, d.ctypes.data),
+              "sample_present")
+        return s, d
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_edgeset_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,881 @@
+// Slab-hash dynamic graph: construction, batched insert / delete / search,
+// CSR export and structural counters.
+//
+// Reference behaviour followed:
+//   bucket count per vertex  max(1, ceil(hint / (slots * LoadFactor)))
+//                            (include/Graph/SlabGraph.cuh:403-407; the
+//                            reference divides by 32 for both slab kinds, this
+//                            build divides by the slots a slab really holds:
+//                            31 keys, or 15 pairs for weighted graphs)
+//   head slabs               one contiguous 128-B slab per bucket, 0xFF filled
+//                            (SlabGraph.cuh:417-423)
+//   insert                   skip self loops (InsertEdgeKernel.cuh:21-26),
+//                            key already present -> unchanged, otherwise take
+//                            the first EMPTY key word of the bucket's slab chain,
+//                            growing the chain with a pool slab when it is full
+//                            (the slab-hash insertKey semantics used at
+//                            include/Graph/warp/InsertEdge.cuh:86-88)
+//   delete                   live key -> TOMBSTONE, degree - 1
+//                            (include/Graph/warp/DeleteEdge.cuh:7-39)
+//   search                   (include/Graph/warp/SearchEdge.cuh:8-63)
+//
+// B200 design: one 8-lane group per batch edge reads a whole 128-B slab with
+// one 16-B load per lane (L2-coherent ld.global.cg), decides with two redux.sync
+// reductions, and commits with one CAS.  No sort, no locks: a key can only be
+// placed in the first EMPTY word of the chain, which makes concurrent inserts
+// of the same key collide on one word, so duplicates are impossible.  For
+// weighted graphs a batch-local hash table first elects the lowest batch index
+// of every repeated (u, v), so the stored weight is deterministic.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "mk_internal.h"
+#include "mk_slab.cuh"
+
+namespace mk {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+mk_status fail(mk_status st, const std::string &msg) {
+  g_last_error = msg;
+  return st;
+}
+
+mk_status cuda_fail(cudaError_t e, const char *what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? MK_ERR_OOM : MK_ERR_CUDA;
+}
+
+int device_sm_count(int device) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+  return n > 0 ? n : 1;
+}
+
+int persistent_blocks(const void *kernel, int block, size_t smem, int device) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
+  if (per_sm < 1) per_sm = 1;
+  return per_sm * device_sm_count(device);
+}
+
+mk_status Timer::start(cudaStream_t st, bool enable) {
+  on = enable;
+  s = st;
+  if (!on) return MK_OK;
+  if (!a) MK_CUDA(cudaEventCreate(&a));
+  if (!b) MK_CUDA(cudaEventCreate(&b));
+  MK_CUDA(cudaEventRecord(a, s));
+  return MK_OK;
+}
+
+mk_status Timer::stop(float *ms_out) {
+  if (!on) return MK_OK;
+  MK_CUDA(cudaEventRecord(b, s));
+  MK_CUDA(cudaEventSynchronize(b));
+  float ms = 0.f;
+  MK_CUDA(cudaEventElapsedTime(&ms, a, b));
+  if (ms_out) *ms_out = ms;
+  return MK_OK;
+}
+
+Timer::~Timer() {
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan u32 -> u64 (three passes: tile sums, scan of sums, tiles).
+// ---------------------------------------------------------------------------
+constexpr int kScanBlock = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v,
+                                                              unsigned long long *sm,
+                                                              unsigned long long *total) {
+  // sm has blockDim.x/32 + 1 entries
+  uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) sm[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t nw = blockDim.x >> 5;
+    unsigned long long s = lane < nw ? sm[lane] : 0ull;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+      if (lane >= (uint32_t)o) s += y;
+    }
+    if (lane < nw) sm[lane] = s;  // inclusive warp totals
+  }
+  __syncthreads();
+  unsigned long long warp_off = warp ? sm[warp - 1] : 0ull;
+  if (total) *total = sm[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return warp_off + x - v;
+}
+
+__global__ void k_scan_tiles(const uint32_t *__restrict__ in, uint32_t n,
+                             unsigned long long *__restrict__ tile_sums) {
+  __shared__ unsigned long long sm[kScanBlock / 32 + 1];
+  uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+  unsigned long long s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    uint64_t idx = base + (uint64_t)i * kScanBlock + threadIdx.x;
+    if (idx < n) s += in[idx];
+  }
+  unsigned long long tot;
+  block_excl_scan(s, sm, &tot);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void k_scan_sums(unsigned long long *sums, uint32_t m) {
+  __shared__ unsigned long long sm[kScanBlock / 32 + 1];
+  unsigned long long carry = 0;
+  for (uint32_t base = 0; base < m; base += kScanBlock) {
+    uint32_t idx = base + threadIdx.x;
+    unsigned long long v = idx < m ? sums[idx] : 0ull;
+    unsigned long long tot;
+    unsigned long long ex = block_excl_scan(v, sm, &tot);
+    if (idx < m) sums[idx] = carry + ex;
+    carry += tot;
+    __syncthreads();
+  }
+}
+
+__global__ void k_scan_apply(const uint32_t *__restrict__ in, uint32_t n,
+                             const unsigned long long *__restrict__ tile_off,
+                             unsigned long long *__restrict__ out) {
+  __shared__ unsigned long long sm[kScanBlock / 32 + 1];
+  uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  unsigned long long s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    uint64_t idx = base + i;
+    v[i] = idx < n ? in[idx] : 0u;
+    s += v[i];
+  }
+  unsigned long long tot;
+  unsigned long long ex = block_excl_scan(s, sm, &tot) + tile_off[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    uint64_t idx = base + i;
+    if (idx < n) out[idx] = ex;
+    ex += v[i];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) out[n] = ex;
+}
+
+mk_status scan_u32_to_u64(const uint32_t *d_in, unsigned long long *d_out,
+                          uint32_t n, DevBuf<unsigned long long> &tmp,
+                          cudaStream_t s) {
+  uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+  if (tiles == 0) {
+    MK_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), s));
+    return MK_OK;
+  }
+  MK_CHECK(tmp.reserve(tiles));
+  k_scan_tiles<<<tiles, kScanBlock, 0, s>>>(d_in, n, tmp.ptr);
+  k_scan_sums<<<1, kScanBlock, 0, s>>>(tmp.ptr, tiles);
+  k_scan_apply<<<tiles, kScanBlock, 0, s>>>(d_in, n, tmp.ptr, d_out);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Update kernels
+// ---------------------------------------------------------------------------
+constexpr uint32_t kProbeLimit = 1u << 24;  // slab steps per edge before giving up
+constexpr int kUpdBlock = 256;
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdull;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ull;
+  x ^= x >> 33;
+  return x;
+}
+
+// Batch-local election of the first occurrence of each (u, v).
+__global__ void k_dedupe_elect(GraphView g, const uint32_t *__restrict__ src,
+                               const uint32_t *__restrict__ dst, uint32_t n,
+                               unsigned long long *keys, uint32_t *idx,
+                               uint32_t mask) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  uint32_t u = src[e], v = dst[e];
+  if (u == v || u >= g.V || v >= g.V) return;
+  unsigned long long key = ((unsigned long long)u << 32) | v;
+  uint32_t h = (uint32_t)mix64(key) & mask;
+  for (uint32_t it = 0; it <= mask; ++it) {
+    unsigned long long k = __ldcg(keys + h);
+    if (k == ~0ull) {
+      unsigned long long old = atomicCAS(keys + h, ~0ull, key);
+      if (old == ~0ull || old == key) {
+        atomicMin(idx + h, e);
+        return;
+      }
+    } else if (k == key) {
+      atomicMin(idx + h, e);
+      return;
+    }
+    h = (h + 1) & mask;
+  }
+}
+
+__device__ __forceinline__ bool dedupe_is_first(const unsigned long long *keys,
+                                                const uint32_t *idx, uint32_t mask,
+                                                uint32_t u, uint32_t v, uint32_t e) {
+  unsigned long long key = ((unsigned long long)u << 32) | v;
+  uint32_t h = (uint32_t)mix64(key) & mask;
+  for (uint32_t it = 0; it <= mask; ++it) {
+    unsigned long long k = keys[h];
+    if (k == key) return idx[h] == e;
+    if (k == ~0ull) return false;
+    h = (h + 1) & mask;
+  }
+  return false;
+}
+
+template <bool kWeighted, bool kDedupe>
+__global__ void __launch_bounds__(kUpdBlock)
+    k_insert(GraphView g, const uint32_t *__restrict__ src,
+             const uint32_t *__restrict__ dst, const uint32_t *__restrict__ w,
+             uint32_t n, const unsigned long long *__restrict__ dd_keys,
+             const uint32_t *__restrict__ dd_idx, uint32_t dd_mask,
+             uint8_t *__restrict__ applied, unsigned long long *count) {
+  __shared__ uint32_t blk_count;
+  if (threadIdx.x == 0) blk_count = 0;
+  __syncthreads();
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  uint32_t mine = 0;
+  for (uint32_t e = group; e < n; e += ngroups) {
+    uint32_t u = src[e], v = dst[e];
+    uint32_t wt = (kWeighted && w) ? w[e] : 0u;
+    if (g.reverse) {
+      uint32_t t = u;
+      u = v;
+      v = t;
+    }
+    uint8_t app = 0;
+    bool ok = (u != v);
+    if (u >= g.V || v >= g.V) {
+      ok = false;
+      if (L.gl == 0) atomicOr(g.err, kErrInvalidId);
+    }
+    if (kDedupe && ok) ok = dedupe_is_first(dd_keys, dd_idx, dd_mask, u, v, e);
+    if (ok) {
+      const uint32_t b0 = g.boff[u];
+      const uint32_t nb = g.boff[u + 1] - b0;
+      uint32_t s = b0 + bucket_of(v, nb);
+      uint32_t it = 0;
+      for (; it < kProbeLimit; ++it) {
+        uint4 q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
+        bool found;
+        uint32_t fslot, eslot, next;
+        probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
+        if (found) break;
+        if (eslot != 255) {
+          uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(eslot);
+          uint32_t old = 0;
+          if (L.gl == 0) {
+            old = atomicCAS(wp, kEmptyKey, v);
+            if (kWeighted && old == kEmptyKey) wp[1] = wt;
+          }
+          old = __shfl_sync(L.gmask, old, L.gbase);
+          if (old == kEmptyKey) {
+            app = 1;
+            break;
+          }
+          if (old == v) break;
+          continue;  // lost the word to another key: re-read this slab
+        }
+        if (next != kNoSlab) {
+          s = next;
+          continue;
+        }
+        // chain is full: take a pool slab holding the key, then link it.
+        uint32_t res = 0;  // 0 = pool exhausted, 1 = linked, 2 = lost the link race
+        uint32_t other = kNoSlab;
+        if (L.gl == 0) {
+          uint32_t ns = atomicAdd(g.pool_top, 1u);
+          if (ns >= g.pool_cap) {
+            atomicOr(g.err, kErrOom);
+            res = 0;
+          } else {
+            uint32_t *np = reinterpret_cast<uint32_t *>(g.slabs + 8ull * ns);
+            np[0] = v;
+            if (kWeighted) np[1] = wt;
+            __threadfence();
+            uint32_t *nextp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + 31;
+            uint32_t prev = atomicCAS(nextp, kNoSlab, ns);
+            if (prev == kNoSlab) {
+              res = 1;
+            } else {
+              res = 2;
+              other = prev;
+              np[0] = kEmptyKey;  // slab stays unreachable
+            }
+          }
+        }
+        res = __shfl_sync(L.gmask, res, L.gbase);
+        other = __shfl_sync(L.gmask, other, L.gbase);
+        if (res == 0) break;
+        if (res == 1) {
+          app = 1;
+          break;
+        }
+        s = other;
+      }
+      if (it >= kProbeLimit && L.gl == 0) atomicOr(g.err, kErrTimeout);
+    }
+    if (L.gl == 0) {
+      applied[e] = app;
+      if (app) {
+        atomicAdd(g.deg + u, 1u);
+        ++mine;
+      }
+    }
+  }
+  if (mine) atomicAdd(&blk_count, mine);
+  __syncthreads();
+  if (threadIdx.x == 0 && blk_count) atomicAdd(count, (unsigned long long)blk_count);
+}
+
+template <bool kWeighted>
+__global__ void __launch_bounds__(kUpdBlock)
+    k_delete(GraphView g, const uint32_t *__restrict__ src,
+             const uint32_t *__restrict__ dst, uint32_t n,
+             uint8_t *__restrict__ applied, unsigned long long *count) {
+  __shared__ uint32_t blk_count;
+  if (threadIdx.x == 0) blk_count = 0;
+  __syncthreads();
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  uint32_t mine = 0;
+  for (uint32_t e = group; e < n; e += ngroups) {
+    uint32_t u = src[e], v = dst[e];
+    if (g.reverse) {
+      uint32_t t = u;
+      u = v;
+      v = t;
+    }
+    uint8_t app = 0;
+    bool ok = (u != v);
+    if (u >= g.V || v >= g.V) {
+      ok = false;
+      if (L.gl == 0) atomicOr(g.err, kErrInvalidId);
+    }
+    if (ok) {
+      const uint32_t b0 = g.boff[u];
+      const uint32_t nb = g.boff[u + 1] - b0;
+      uint32_t s = b0 + bucket_of(v, nb);
+      uint32_t it = 0;
+      for (; it < kProbeLimit && s != kNoSlab; ++it) {
+        uint4 q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
+        bool found;
+        uint32_t fslot, eslot, next;
+        probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
+        if (found) {
+          uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(fslot);
+          uint32_t old = 0;
+          if (L.gl == 0) old = atomicCAS(wp, v, kTombKey);
+          old = __shfl_sync(L.gmask, old, L.gbase);
+          app = (old == v);
+          break;
+        }
+        s = next;
+      }
+      if (it >= kProbeLimit && L.gl == 0) atomicOr(g.err, kErrTimeout);
+    }
+    if (L.gl == 0) {
+      applied[e] = app;
+      if (app) {
+        atomicSub(g.deg + u, 1u);
+        ++mine;
+      }
+    }
+  }
+  if (mine) atomicAdd(&blk_count, mine);
+  __syncthreads();
+  if (threadIdx.x == 0 && blk_count) atomicAdd(count, (unsigned long long)blk_count);
+}
+
+template <bool kWeighted>
+__global__ void __launch_bounds__(kUpdBlock)
+    k_search(GraphView g, const uint32_t *__restrict__ src,
+             const uint32_t *__restrict__ dst, uint32_t n,
+             uint8_t *__restrict__ found_out, uint32_t *__restrict__ w_out) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t e = group; e < n; e += ngroups) {
+    uint32_t u = src[e], v = dst[e];
+    if (g.reverse) {
+      uint32_t t = u;
+      u = v;
+      v = t;
+    }
+    bool hit = false;
+    uint32_t val = 0;
+    if (u < g.V && v < g.V && u != v) {
+      const uint32_t b0 = g.boff[u];
+      const uint32_t nb = g.boff[u + 1] - b0;
+      uint32_t s = b0 + bucket_of(v, nb);
+      for (uint32_t it = 0; it < kProbeLimit && s != kNoSlab; ++it) {
+        uint4 q = ld_slab_ro(g.slabs + 8ull * s + L.gl);
+        bool f;
+        uint32_t fslot, eslot, next;
+        probe_slab<kWeighted>(q, v, L, f, fslot, eslot, next);
+        if (f) {
+          hit = true;
+          if (kWeighted) {
+            // value word 2*fslot+1 lives in lane fslot/2, component y or w
+            uint32_t owner = fslot >> 1;
+            uint32_t cand = (fslot & 1) ? q.w : q.y;
+            val = __shfl_sync(L.gmask, cand, L.gbase + owner);
+          }
+          break;
+        }
+        s = next;
+      }
+    }
+    if (L.gl == 0) {
+      if (found_out) found_out[e] = hit ? 1 : 0;
+      if (w_out) w_out[e] = val;
+    }
+  }
+}
+
+// Per-vertex walk helpers ----------------------------------------------------
+
+// Number of live keys and tombstones held by one lane's 16-byte quarter.
+template <bool kWeighted>
+__device__ __forceinline__ void lane_counts(const uint4 &q, uint32_t gl,
+                                            uint32_t &live, uint32_t &tomb) {
+  live = 0;
+  tomb = 0;
+  auto acc = [&](uint32_t k) {
+    live += (k < kTombKey);
+    tomb += (k == kTombKey);
+  };
+  if (!kWeighted) {
+    acc(q.x);
+    acc(q.y);
+    acc(q.z);
+    if (gl != 7) acc(q.w);
+  } else {
+    acc(q.x);
+    if (gl != 7) acc(q.z);
+  }
+}
+
+template <bool kWeighted>
+__global__ void k_count_tombstones(GraphView g, uint32_t *__restrict__ out) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t u = group; u < g.V; u += ngroups) {
+    uint32_t tomb_total = 0;
+    for (uint32_t b = g.boff[u]; b < g.boff[u + 1]; ++b) {
+      uint32_t s = b;
+      while (s != kNoSlab) {
+        uint4 q = ld_slab_ro(g.slabs + 8ull * s + L.gl);
+        uint32_t live, tomb;
+        lane_counts<kWeighted>(q, L.gl, live, tomb);
+        tomb_total += __reduce_add_sync(L.gmask, tomb);
+        s = __shfl_sync(L.gmask, q.w, L.gbase + 7);
+      }
+    }
+    if (L.gl == 0) out[u] = tomb_total;
+  }
+}
+
+template <bool kWeighted>
+__global__ void k_export_csr(GraphView g, const unsigned long long *__restrict__ row_ptr,
+                             uint32_t *__restrict__ col, uint32_t *__restrict__ wout) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t u = group; u < g.V; u += ngroups) {
+    unsigned long long pos = row_ptr[u];
+    const unsigned long long end = row_ptr[u + 1];
+    for (uint32_t b = g.boff[u]; b < g.boff[u + 1]; ++b) {
+      uint32_t s = b;
+      while (s != kNoSlab) {
+        uint4 q = ld_slab_ro(g.slabs + 8ull * s + L.gl);
+        uint32_t live, tomb;
+        lane_counts<kWeighted>(q, L.gl, live, tomb);
+        // exclusive prefix over the 8 lanes
+        uint32_t incl = live;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+          uint32_t y = __shfl_up_sync(L.gmask, incl, o, 8);
+          if (L.gl >= (uint32_t)o) incl += y;
+        }
+        uint32_t total = __shfl_sync(L.gmask, incl, L.gbase + 7);
+        unsigned long long p = pos + (incl - live);
+        auto put = [&](uint32_t k, uint32_t val) {
+          if (k < kTombKey) {
+            if (p < end) {
+              col[p] = k;
+              if (wout) wout[p] = val;
+            }
+            ++p;
+          }
+        };
+        if (!kWeighted) {
+          put(q.x, 0);
+          put(q.y, 0);
+          put(q.z, 0);
+          if (L.gl != 7) put(q.w, 0);
+        } else {
+          put(q.x, q.y);
+          if (L.gl != 7) put(q.z, q.w);
+        }
+        pos += total;
+        s = __shfl_sync(L.gmask, q.w, L.gbase + 7);
+      }
+    }
+  }
+}
+
+static int update_grid(uint32_t n, int device) {
+  // 8 lanes per edge; enough resident groups to cover HBM latency.
+  uint64_t groups_needed = (uint64_t)n;
+  uint64_t blocks = (groups_needed * 8 + kUpdBlock - 1) / kUpdBlock;
+  uint64_t cap = (uint64_t)device_sm_count(device) * 8;  // 8 x 256 threads per SM
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+}  // namespace mk
+
+using namespace mk;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char *mk_last_error_string(void) { return g_last_error.c_str(); }
+const char *mk_version(void) { return "meerkat_b200 0.1 sm_100a"; }
+
+mk_status mk_graph_create(const mk_graph_desc *desc, mk_graph **out) {
+  if (!desc || !out) return fail(MK_ERR_INVALID, "mk_graph_create: null argument");
+  *out = nullptr;
+  if (desc->num_vertices == 0 || desc->num_vertices >= kTombKey)
+    return fail(MK_ERR_INVALID, "mk_graph_create: num_vertices out of range");
+  if (!(desc->load_factor > 0.0) || !std::isfinite(desc->load_factor))
+    return fail(MK_ERR_INVALID, "mk_graph_create: load_factor must be > 0");
+  if (desc->flags != 0) return fail(MK_ERR_INVALID, "mk_graph_create: flags must be 0");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(MK_ERR_CUDA, "mk_graph_create: no CUDA device");
+  if (desc->device < 0 || desc->device >= ndev)
+    return fail(MK_ERR_INVALID, "mk_graph_create: bad device index");
+  DeviceGuard dg(desc->device);
+
+  mk_graph *g = new mk_graph();
+  g->device = desc->device;
+  g->V = desc->num_vertices;
+  g->weighted = desc->weighted ? 1u : 0u;
+  g->reverse = desc->reverse ? 1u : 0u;
+  g->keys_per_slab = g->weighted ? 15u : 31u;
+  g->load_factor = desc->load_factor;
+
+  const uint32_t V = g->V;
+  g->h_boff.resize((size_t)V + 1);
+  uint64_t total = 0, hint_sum = 0;
+  const double per_bucket = (double)g->keys_per_slab * desc->load_factor;
+  for (uint32_t i = 0; i < V; ++i) {
+    uint32_t hint = desc->h_degree_hints ? desc->h_degree_hints[i] : 1u;
+    hint_sum += hint;
+    double x = std::ceil((double)hint / per_bucket);
+    uint64_t nb = x < 1.0 ? 1 : (uint64_t)x;
+    g->h_boff[i] = (uint32_t)total;
+    total += nb;
+    if (total >= 0xF0000000ull) {
+      delete g;
+      return fail(MK_ERR_INVALID, "mk_graph_create: too many buckets");
+    }
+  }
+  g->h_boff[V] = (uint32_t)total;
+  g->num_buckets = total;
+  uint64_t overflow = desc->pool_slabs;
+  if (overflow == 0) {
+    overflow = std::max<uint64_t>(65536, 2 * total + hint_sum / g->keys_per_slab);
+  }
+  g->pool_cap = total + overflow;
+  if (g->pool_cap >= 0xFFFFFFF0ull) g->pool_cap = 0xFFFFFFF0ull;
+
+  auto cleanup = [&](mk_status st, const char *what, cudaError_t e) {
+    mk_graph_destroy(g);
+    return cuda_fail(e, what), st;
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&g->slabs, g->pool_cap * 128ull)) != cudaSuccess)
+    return cleanup(MK_ERR_OOM, "cudaMalloc(slab pool)", e);
+  if ((e = cudaMalloc(&g->boff, ((size_t)V + 1) * 4)) != cudaSuccess)
+    return cleanup(MK_ERR_OOM, "cudaMalloc(bucket offsets)", e);
+  if ((e = cudaMalloc(&g->deg, (size_t)V * 4)) != cudaSuccess)
+    return cleanup(MK_ERR_OOM, "cudaMalloc(degrees)", e);
+  if ((e = cudaMalloc(&g->pool_top, 4 * sizeof(uint32_t))) != cudaSuccess)
+    return cleanup(MK_ERR_OOM, "cudaMalloc(pool counter)", e);
+  if ((e = cudaMalloc(&g->counters, 4 * sizeof(unsigned long long))) != cudaSuccess)
+    return cleanup(MK_ERR_OOM, "cudaMalloc(counters)", e);
+  g->device_bytes = g->pool_cap * 128ull + ((size_t)V + 1) * 4 + (size_t)V * 4 + 16 + 32;
+  if ((e = cudaMemset(g->slabs, 0xFF, g->pool_cap * 128ull)) != cudaSuccess)
+    return cleanup(MK_ERR_CUDA, "cudaMemset(slabs)", e);
+  if ((e = cudaMemcpy(g->boff, g->h_boff.data(), ((size_t)V + 1) * 4,
+                      cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cleanup(MK_ERR_CUDA, "cudaMemcpy(bucket offsets)", e);
+  if ((e = cudaMemset(g->deg, 0, (size_t)V * 4)) != cudaSuccess)
+    return cleanup(MK_ERR_CUDA, "cudaMemset(degrees)", e);
+  uint32_t init[4] = {(uint32_t)total, 0u, 0u, 0u};
+  if ((e = cudaMemcpy(g->pool_top, init, sizeof(init), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cleanup(MK_ERR_CUDA, "cudaMemcpy(pool counter)", e);
+  if ((e = cudaMemset(g->counters, 0, 4 * sizeof(unsigned long long))) != cudaSuccess)
+    return cleanup(MK_ERR_CUDA, "cudaMemset(counters)", e);
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess)
+    return cleanup(MK_ERR_CUDA, "cudaDeviceSynchronize(create)", e);
+  *out = g;
+  return MK_OK;
+}
+
+mk_status mk_graph_destroy(mk_graph *g) {
+  if (!g) return MK_OK;
+  DeviceGuard dg(g->device);
+  if (g->slabs) cudaFree(g->slabs);
+  if (g->boff) cudaFree(g->boff);
+  if (g->deg) cudaFree(g->deg);
+  if (g->pool_top) cudaFree(g->pool_top);
+  if (g->counters) cudaFree(g->counters);
+  g->applied.release();
+  g->dd_keys.release();
+  g->dd_idx.release();
+  g->scan_tmp.release();
+  delete g;
+  return MK_OK;
+}
+
+mk_status mk_graph_reserve_batch(mk_graph *g, uint32_t n) {
+  if (!g) return fail(MK_ERR_INVALID, "mk_graph_reserve_batch: null graph");
+  DeviceGuard dg(g->device);
+  MK_CHECK(g->applied.reserve(std::max<uint32_t>(n, 1), &g->device_bytes));
+  if (g->weighted) {
+    uint32_t cap = 1024;
+    while (cap < 2ull * n) cap <<= 1;
+    MK_CHECK(g->dd_keys.reserve(cap, &g->device_bytes));
+    MK_CHECK(g->dd_idx.reserve(cap, &g->device_bytes));
+  }
+  return MK_OK;
+}
+
+static mk_status begin_update(mk_graph *g, const uint32_t *d_src,
+                              const uint32_t *d_dst, uint32_t n, int op,
+                              cudaStream_t s) {
+  MK_CHECK(g->applied.reserve(std::max<uint32_t>(n, 1), &g->device_bytes));
+  MK_CUDA(cudaMemsetAsync(g->counters, 0, sizeof(unsigned long long), s));
+  g->last_n = n;
+  g->last_src = d_src;
+  g->last_dst = d_dst;
+  g->last_op = op;
+  return MK_OK;
+}
+
+mk_status mk_graph_insert_edges(mk_graph *g, const uint32_t *d_src,
+                                const uint32_t *d_dst, const uint32_t *d_w,
+                                uint32_t n, void *stream) {
+  if (!g) return fail(MK_ERR_INVALID, "mk_graph_insert_edges: null graph");
+  if (n && (!d_src || !d_dst)) return fail(MK_ERR_INVALID, "mk_graph_insert_edges: null batch");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(begin_update(g, d_src, d_dst, n, 1, s));
+  if (n == 0) return MK_OK;
+  GraphView v = g->view();
+  int blocks = update_grid(n, g->device);
+  if (g->weighted) {
+    uint32_t cap = 1024;
+    while (cap < 2ull * n) cap <<= 1;
+    MK_CHECK(g->dd_keys.reserve(cap, &g->device_bytes));
+    MK_CHECK(g->dd_idx.reserve(cap, &g->device_bytes));
+    MK_CUDA(cudaMemsetAsync(g->dd_keys.ptr, 0xFF, (size_t)cap * 8, s));
+    MK_CUDA(cudaMemsetAsync(g->dd_idx.ptr, 0xFF, (size_t)cap * 4, s));
+    const uint32_t *ks = g->reverse ? d_dst : d_src;
+    const uint32_t *kd = g->reverse ? d_src : d_dst;
+    k_dedupe_elect<<<(n + 255) / 256, 256, 0, s>>>(v, ks, kd, n, g->dd_keys.ptr,
+                                                   g->dd_idx.ptr, cap - 1);
+    k_insert<true, true><<<blocks, kUpdBlock, 0, s>>>(
+        v, d_src, d_dst, d_w, n, g->dd_keys.ptr, g->dd_idx.ptr, cap - 1,
+        g->applied.ptr, g->counters);
+  } else {
+    k_insert<false, false><<<blocks, kUpdBlock, 0, s>>>(
+        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr,
+        g->counters);
+  }
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+mk_status mk_graph_delete_edges(mk_graph *g, const uint32_t *d_src,
+                                const uint32_t *d_dst, uint32_t n,
+                                void *stream) {
+  if (!g) return fail(MK_ERR_INVALID, "mk_graph_delete_edges: null graph");
+  if (n && (!d_src || !d_dst)) return fail(MK_ERR_INVALID, "mk_graph_delete_edges: null batch");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(begin_update(g, d_src, d_dst, n, 2, s));
+  if (n == 0) return MK_OK;
+  GraphView v = g->view();
+  int blocks = update_grid(n, g->device);
+  if (g->weighted)
+    k_delete<true><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, g->applied.ptr, g->counters);
+  else
+    k_delete<false><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, g->applied.ptr, g->counters);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+mk_status mk_graph_search_edges(mk_graph *g, const uint32_t *d_src,
+                                const uint32_t *d_dst, uint32_t n,
+                                uint8_t *d_found, uint32_t *d_w, void *stream) {
+  if (!g) return fail(MK_ERR_INVALID, "mk_graph_search_edges: null graph");
+  if (n == 0) return MK_OK;
+  if (!d_src || !d_dst) return fail(MK_ERR_INVALID, "mk_graph_search_edges: null batch");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  GraphView v = g->view();
+  int blocks = update_grid(n, g->device);
+  if (g->weighted)
+    k_search<true><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, d_found, d_w);
+  else
+    k_search<false><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, d_found, d_w);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+mk_status mk_graph_sync(mk_graph *g, void *stream, uint32_t *h_deverr) {
+  if (!g) return fail(MK_ERR_INVALID, "mk_graph_sync: null graph");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  uint32_t err = 0;
+  MK_CUDA(cudaMemcpyAsync(&err, g->err_word(), 4, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  if (h_deverr) *h_deverr = err;
+  if (err & kErrTimeout) return fail(MK_ERR_TIMEOUT, "device wait or probe limit exceeded");
+  if (err & kErrOom) return fail(MK_ERR_OOM, "slab pool exhausted");
+  if (err & kErrInvalidId) return fail(MK_ERR_INVALID, "batch holds a vertex id >= num_vertices");
+  return MK_OK;
+}
+
+mk_status mk_graph_last_applied(mk_graph *g, uint64_t *h_count) {
+  if (!g || !h_count) return fail(MK_ERR_INVALID, "mk_graph_last_applied: null argument");
+  DeviceGuard dg(g->device);
+  unsigned long long c = 0;
+  MK_CUDA(cudaMemcpy(&c, g->counters, 8, cudaMemcpyDeviceToHost));
+  *h_count = c;
+  return MK_OK;
+}
+
+mk_status mk_graph_last_applied_flags(mk_graph *g, const uint8_t **d_flags,
+                                      uint32_t *n) {
+  if (!g) return fail(MK_ERR_INVALID, "mk_graph_last_applied_flags: null graph");
+  if (d_flags) *d_flags = g->applied.ptr;
+  if (n) *n = g->last_n;
+  return MK_OK;
+}
+
+mk_status mk_graph_degrees(mk_graph *g, uint32_t *d_out, void *stream) {
+  if (!g || !d_out) return fail(MK_ERR_INVALID, "mk_graph_degrees: null argument");
+  DeviceGuard dg(g->device);
+  MK_CUDA(cudaMemcpyAsync(d_out, g->deg, (size_t)g->V * 4, cudaMemcpyDeviceToDevice,
+                          as_stream(stream)));
+  return MK_OK;
+}
+
+mk_status mk_graph_bucket_layout(mk_graph *g, uint32_t *h_offsets,
+                                 uint32_t *h_buckets_per_vertex) {
+  if (!g) return fail(MK_ERR_INVALID, "mk_graph_bucket_layout: null graph");
+  for (uint32_t i = 0; i < g->V; ++i) {
+    if (h_offsets) h_offsets[i] = g->h_boff[i];
+    if (h_buckets_per_vertex) h_buckets_per_vertex[i] = g->h_boff[i + 1] - g->h_boff[i];
+  }
+  return MK_OK;
+}
+
+mk_status mk_graph_get_info(mk_graph *g, mk_graph_info *out) {
+  if (!g || !out) return fail(MK_ERR_INVALID, "mk_graph_get_info: null argument");
+  DeviceGuard dg(g->device);
+  uint32_t top = 0;
+  MK_CUDA(cudaMemcpy(&top, g->pool_top, 4, cudaMemcpyDeviceToHost));
+  // live edges: sum of degrees
+  std::vector<uint32_t> deg(g->V);
+  MK_CUDA(cudaMemcpy(deg.data(), g->deg, (size_t)g->V * 4, cudaMemcpyDeviceToHost));
+  uint64_t e = 0;
+  for (uint32_t d : deg) e += d;
+  out->num_vertices = g->V;
+  out->weighted = g->weighted;
+  out->reverse = g->reverse;
+  out->keys_per_slab = g->keys_per_slab;
+  out->num_buckets = g->num_buckets;
+  out->pool_capacity = g->pool_cap;
+  out->slabs_used = std::min<uint64_t>(top, g->pool_cap);
+  out->num_edges = e;
+  out->device_bytes = g->device_bytes;
+  return MK_OK;
+}
+
+mk_status mk_graph_export_csr(mk_graph *g, uint64_t *d_row_ptr, uint32_t *d_col,
+                              uint32_t *d_w, void *stream) {
+  if (!g || !d_row_ptr || !d_col) return fail(MK_ERR_INVALID, "mk_graph_export_csr: null argument");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  unsigned long long *rp = reinterpret_cast<unsigned long long *>(d_row_ptr);
+  MK_CHECK(scan_u32_to_u64(g->deg, rp, g->V, g->scan_tmp, s));
+  GraphView v = g->view();
+  int blocks = std::min<uint64_t>((uint64_t)g->V * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  if (g->weighted)
+    k_export_csr<true><<<blocks, 256, 0, s>>>(v, rp, d_col, d_w);
+  else
+    k_export_csr<false><<<blocks, 256, 0, s>>>(v, rp, d_col, nullptr);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+mk_status mk_graph_count_tombstones(mk_graph *g, uint32_t *d_out, void *stream) {
+  if (!g || !d_out) return fail(MK_ERR_INVALID, "mk_graph_count_tombstones: null argument");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  GraphView v = g->view();
+  int blocks = std::min<uint64_t>((uint64_t)g->V * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  if (g->weighted)
+    k_count_tombstones<true><<<blocks, 256, 0, s>>>(v, d_out);
+  else
+    k_count_tombstones<false><<<blocks, 256, 0, s>>>(v, d_out);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// Host-side internals shared by the C ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/meerkat_b200.h"
+#include "mk_common.cuh"
+
+namespace mk {
+
+void set_error(const std::string &msg);
+mk_status fail(mk_status st, const std::string &msg);
+mk_status cuda_fail(cudaError_t e, const char *what);
+
+#define MK_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return ::mk::cuda_fail(e_, #call); \
+  } while (0)
+
+#define MK_CHECK(call)                      \
+  do {                                      \
+    mk_status s_ = (call);                  \
+    if (s_ != MK_OK) return s_;             \
+  } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Device buffer that grows on demand (never shrinks).
+template <class T>
+struct DevBuf {
+  T *ptr = nullptr;
+  size_t cap = 0;  // elements
+  mk_status reserve(size_t n, size_t *bytes_acc = nullptr) {
+    if (n <= cap) return MK_OK;
+    size_t want = cap ? cap : 1024;
+    while (want < n) want *= 2;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&ptr, want * sizeof(T));
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      return cuda_fail(e, "cudaMalloc(scratch)");
+    }
+    if (bytes_acc) *bytes_acc += (want - cap) * sizeof(T);
+    cap = want;
+    return MK_OK;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+};
+
+int device_sm_count(int device);
+
+// Scoped device switch.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Event pair used by the ms_out timing of the algorithm calls.
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s = nullptr;
+  bool on = false;
+  mk_status start(cudaStream_t st, bool enable);
+  mk_status stop(float *ms_out);
+  ~Timer();
+};
+
+// Exclusive scan of n u32 counts into u64 offsets (out has n+1 entries).
+mk_status scan_u32_to_u64(const uint32_t *d_in, unsigned long long *d_out,
+                          uint32_t n, DevBuf<unsigned long long> &tmp,
+                          cudaStream_t s);
+
+// Number of co-resident blocks for a persistent cooperative launch.
+int persistent_blocks(const void *kernel, int block, size_t smem, int device);
+
+}  // namespace mk
+
+struct mk_graph {
+  int device = 0;
+  uint32_t V = 0;
+  uint32_t weighted = 0;
+  uint32_t reverse = 0;
+  uint32_t keys_per_slab = 31;
+  double load_factor = 0.7;
+  uint64_t num_buckets = 0;
+  uint64_t pool_cap = 0;
+  uint4 *slabs = nullptr;
+  uint32_t *boff = nullptr;
+  uint32_t *deg = nullptr;
+  uint32_t *pool_top = nullptr;   // [0] bump pointer; [1] error word
+  std::vector<uint32_t> h_boff;
+  unsigned long long *counters = nullptr;  // [0] applied count of last update
+  // per-batch scratch
+  mk::DevBuf<uint8_t> applied;     // per-edge applied flags of the last update
+  mk::DevBuf<unsigned long long> dd_keys;  // weighted-insert dedupe table
+  mk::DevBuf<uint32_t> dd_idx;
+  mk::DevBuf<unsigned long long> scan_tmp;
+  uint32_t last_n = 0;
+  const uint32_t *last_src = nullptr;
+  const uint32_t *last_dst = nullptr;
+  int last_op = 0;  // 1 insert, 2 delete
+  size_t device_bytes = 0;
+
+  mk::GraphView view() const {
+    mk::GraphView v;
+    v.slabs = slabs;
+    v.boff = boff;
+    v.deg = deg;
+    v.pool_top = pool_top;
+    v.err = pool_top + 1;
+    v.V = V;
+    v.pool_cap = static_cast<uint32_t>(pool_cap);
+    v.weighted = weighted;
+    v.reverse = reverse;
+    return v;
+  }
+  uint32_t *err_word() const { return pool_top + 1; }
+};

@@ -1,0 +1,561 @@
+// Triangle counting on a symmetric slab graph.
+//
+// Reference (include/Algorithms/impl/TCImpl.cuh): Static collects all edges,
+// orients each from its lower-degree endpoint and counts, per edge (u, v),
+// the w in N(u) with (w, v) present, dividing the total by 6 (:149-214,
+// :288-380).  Incremental/Decremental combine three batch-local counts
+// (:431-565); that combination is broken as written (the batch graph is
+// built with zero vertices before the mapping is known, and the decremental
+// path divides by a zero load factor), so this build keeps the contract --
+// the count of triangles of the current graph after each call -- and
+// re-derives the update rule:
+//
+//   every changed undirected edge e = {a, b} (an edge the last update applied)
+//   counts the triangles {a, b, w} of the new graph (insert) or of the old
+//   graph (delete) whose other changed edges all order after e; each changed
+//   triangle is therefore counted exactly once, at its smallest changed edge.
+//
+// B200 design.  Static: degree-ordered orientation (rank = (deg, id)),
+// oriented CSR built from the slabs (count, scan, fill), then the forward
+// algorithm: a warp stages N+(u) in a shared-memory hash set and streams
+// N+(v) for every v in N+(u) with coalesced 128-byte reads; vertices with a
+// large N+(u) use a block and a global-memory set.  Dynamic: one 8-lane group
+// per changed edge walks the slabs of the lower-degree endpoint and probes the
+// other endpoint's slab hash per candidate (one lane per candidate).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "mk_internal.h"
+#include "mk_slab.cuh"
+
+namespace mk {
+
+__device__ __forceinline__ bool rank_less(uint32_t du, uint32_t u, uint32_t dv, uint32_t v) {
+  return du < dv || (du == dv && u < v);
+}
+
+template <bool kW>
+__global__ void k_orient_count(GraphView g, uint32_t *__restrict__ ocnt) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t u = group; u < g.V; u += ngroups) {
+    const uint32_t du = g.deg[u];
+    uint32_t c = 0;
+    if (du) {
+      walk_vertex(g, L, u, [&](const uint4 &q) {
+        uint32_t k[4], w[4];
+        lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+        for (int i = 0; i < keys_per_lane<kW>(); ++i)
+          if (k[i] < kTombKey && k[i] != u && rank_less(du, u, g.deg[k[i]], k[i])) ++c;
+      });
+    }
+    c = __reduce_add_sync(L.gmask, c);
+    if (L.gl == 0) ocnt[u] = c;
+  }
+}
+
+template <bool kW>
+__global__ void k_orient_fill(GraphView g, const unsigned long long *__restrict__ orow,
+                              uint32_t *__restrict__ ocol) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t u = group; u < g.V; u += ngroups) {
+    const uint32_t du = g.deg[u];
+    unsigned long long pos = orow[u];
+    const unsigned long long end = orow[u + 1];
+    if (pos == end) continue;
+    walk_vertex(g, L, u, [&](const uint4 &q) {
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+      uint32_t keep[4];
+      uint32_t cnt = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        keep[i] = (i < keys_per_lane<kW>()) && k[i] < kTombKey && k[i] != u &&
+                  rank_less(du, u, g.deg[k[i]], k[i]);
+        cnt += keep[i];
+      }
+      uint32_t incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        uint32_t y = __shfl_up_sync(L.gmask, incl, o, 8);
+        if (L.gl >= (uint32_t)o) incl += y;
+      }
+      uint32_t total = __shfl_sync(L.gmask, incl, L.gbase + 7);
+      unsigned long long p = pos + (incl - cnt);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (keep[i]) {
+          if (p < end) ocol[p] = k[i];
+          ++p;
+        }
+      pos += total;
+    });
+  }
+}
+
+constexpr int kTcWarps = 4;           // warps per block in the small kernel (32 KB of sets)
+constexpr int kTcSetCap = 2048;       // per-warp shared hash capacity (entries)
+constexpr uint32_t kTcSmallMax = 1024;  // N+(u) handled by one warp
+
+__device__ __forceinline__ void set_insert(uint32_t *set, uint32_t cap_mask, uint32_t key) {
+  uint32_t h = mix32(key) & cap_mask;
+  while (true) {
+    uint32_t old = atomicCAS(set + h, kEmptyKey, key);
+    if (old == kEmptyKey || old == key) return;
+    h = (h + 1) & cap_mask;
+  }
+}
+
+__device__ __forceinline__ bool set_contains(const uint32_t *set, uint32_t cap_mask, uint32_t key) {
+  uint32_t h = mix32(key) & cap_mask;
+  while (true) {
+    uint32_t k = set[h];
+    if (k == key) return true;
+    if (k == kEmptyKey) return false;
+    h = (h + 1) & cap_mask;
+  }
+}
+
+// Same probe for a set in global memory, read through L2 (the set is
+// rebuilt for every vertex, so L1 may hold stale lines).
+__device__ __forceinline__ bool set_contains_cg(const uint32_t *set, uint32_t cap_mask, uint32_t key) {
+  uint32_t h = mix32(key) & cap_mask;
+  while (true) {
+    uint32_t k = __ldcg(set + h);
+    if (k == key) return true;
+    if (k == kEmptyKey) return false;
+    h = (h + 1) & cap_mask;
+  }
+}
+
+__global__ void __launch_bounds__(kTcWarps * 32)
+    k_tc_small(uint32_t V, const unsigned long long *__restrict__ orow,
+               const uint32_t *__restrict__ ocol, unsigned long long *count,
+               uint32_t *big_list, uint32_t *big_n) {
+  __shared__ uint32_t sets[kTcWarps][kTcSetCap];
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t *set = sets[wib];
+  unsigned long long c = 0;
+  for (uint32_t u = warp; u < V; u += nwarps) {
+    const unsigned long long r0 = orow[u], r1 = orow[u + 1];
+    const uint32_t du = (uint32_t)(r1 - r0);
+    if (du < 2) continue;  // a triangle needs two oriented edges out of u
+    if (du > kTcSmallMax) {
+      if (lane == 0) big_list[atomicAdd(big_n, 1u)] = u;
+      continue;
+    }
+    uint32_t cap = 64;
+    while (cap < 2 * du) cap <<= 1;
+    for (uint32_t i = lane; i < cap; i += 32) set[i] = kEmptyKey;
+    __syncwarp();
+    for (uint32_t i = lane; i < du; i += 32) set_insert(set, cap - 1, ocol[r0 + i]);
+    __syncwarp();
+    for (uint32_t i = 0; i < du; ++i) {
+      const uint32_t v = ocol[r0 + i];
+      const unsigned long long s0 = orow[v], s1 = orow[v + 1];
+      for (unsigned long long j = s0 + lane; j < s1; j += 32)
+        c += set_contains(set, cap - 1, ocol[j]);
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+  if (lane == 0 && c) atomicAdd(count, c);
+}
+
+__global__ void k_tc_big(const unsigned long long *__restrict__ orow,
+                         const uint32_t *__restrict__ ocol, const uint32_t *__restrict__ big_list,
+                         const uint32_t *__restrict__ big_n, uint32_t *scratch, uint32_t cap,
+                         unsigned long long *count) {
+  __shared__ unsigned long long red[32];
+  uint32_t *set = scratch + (size_t)blockIdx.x * cap;
+  unsigned long long c = 0;
+  const uint32_t nbig = *big_n;
+  for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+    const uint32_t u = big_list[bi];
+    const unsigned long long r0 = orow[u], r1 = orow[u + 1];
+    const uint32_t du = (uint32_t)(r1 - r0);
+    uint32_t cp = 64;
+    while (cp < 2 * du && cp < cap) cp <<= 1;
+    for (uint32_t i = threadIdx.x; i < cp; i += blockDim.x) set[i] = kEmptyKey;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < du; i += blockDim.x) set_insert(set, cp - 1, ocol[r0 + i]);
+    __syncthreads();
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (uint32_t i = warp; i < du; i += nw) {
+      const uint32_t v = ocol[r0 + i];
+      const unsigned long long s0 = orow[v], s1 = orow[v + 1];
+      for (unsigned long long j = s0 + lane; j < s1; j += 32) c += set_contains_cg(set, cp - 1, ocol[j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (uint32_t i = 0; i < (blockDim.x >> 5); ++i) t += red[i];
+    if (t) atomicAdd(count, t);
+  }
+}
+
+// ---- dynamic counting ------------------------------------------------------
+
+__device__ __forceinline__ unsigned long long pair_key(uint32_t a, uint32_t b) {
+  return a < b ? ((unsigned long long)a << 32) | b : ((unsigned long long)b << 32) | a;
+}
+
+__device__ __forceinline__ unsigned long long hmix64(unsigned long long x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdull;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ull;
+  x ^= x >> 33;
+  return x;
+}
+
+// Elects one batch entry per changed undirected pair (lowest index).
+__global__ void k_pairs_elect(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                              const uint8_t *__restrict__ applied, uint32_t n,
+                              unsigned long long *keys, uint32_t *idx, uint32_t mask) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || !applied[e]) return;
+  uint32_t a = src[e], b = dst[e];
+  if (a == b) return;
+  unsigned long long key = pair_key(a, b);
+  uint32_t h = (uint32_t)hmix64(key) & mask;
+  for (uint32_t it = 0; it <= mask; ++it) {
+    unsigned long long k = __ldcg(keys + h);
+    if (k == key) {
+      atomicMin(idx + h, e);
+      return;
+    }
+    if (k == ~0ull) {
+      unsigned long long old = atomicCAS(keys + h, ~0ull, key);
+      if (old == ~0ull || old == key) {
+        atomicMin(idx + h, e);
+        return;
+      }
+    }
+    h = (h + 1) & mask;
+  }
+}
+
+__device__ __forceinline__ uint32_t pairs_find(const unsigned long long *keys, const uint32_t *idx,
+                                               uint32_t mask, unsigned long long key) {
+  uint32_t h = (uint32_t)hmix64(key) & mask;
+  for (uint32_t it = 0; it <= mask; ++it) {
+    unsigned long long k = keys[h];
+    if (k == key) return idx[h];
+    if (k == ~0ull) return kEmptyKey;
+    h = (h + 1) & mask;
+  }
+  return kEmptyKey;
+}
+
+// Batch adjacency (both directions) of the elected pairs, for deletions.
+__global__ void k_pairs_degree(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                               const uint8_t *__restrict__ applied, uint32_t n,
+                               const unsigned long long *keys, const uint32_t *idx, uint32_t mask,
+                               uint32_t *bcnt) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || !applied[e]) return;
+  uint32_t a = src[e], b = dst[e];
+  if (a == b || pairs_find(keys, idx, mask, pair_key(a, b)) != e) return;
+  atomicAdd(bcnt + a, 1u);
+  atomicAdd(bcnt + b, 1u);
+}
+
+__global__ void k_pairs_fill(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                             const uint8_t *__restrict__ applied, uint32_t n,
+                             const unsigned long long *keys, const uint32_t *idx, uint32_t mask,
+                             const unsigned long long *brow, uint32_t *bfill, uint32_t *bcol) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || !applied[e]) return;
+  uint32_t a = src[e], b = dst[e];
+  if (a == b || pairs_find(keys, idx, mask, pair_key(a, b)) != e) return;
+  bcol[brow[a] + atomicAdd(bfill + a, 1u)] = b;
+  bcol[brow[b] + atomicAdd(bfill + b, 1u)] = a;
+}
+
+// Lane-level membership test of (u, v) in the slab graph.
+template <bool kW>
+__device__ __forceinline__ bool lane_find(const GraphView &g, uint32_t u, uint32_t v) {
+  const uint32_t b0 = g.boff[u];
+  const uint32_t nb = g.boff[u + 1] - b0;
+  uint32_t s = b0 + bucket_of(v, nb);
+  for (uint32_t it = 0; it < (1u << 24) && s != kNoSlab; ++it) {
+    const uint4 *p = g.slabs + 8ull * s;
+    uint4 last;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      uint4 q = __ldg(p + j);
+      if (!kW) {
+        if (q.x == v || q.y == v || q.z == v || (j != 7 && q.w == v)) return true;
+      } else {
+        if (q.x == v || (j != 7 && q.z == v)) return true;
+      }
+      last = q;
+    }
+    s = last.w;
+  }
+  return false;
+}
+
+template <bool kW>
+__global__ void k_tc_delta(GraphView g, const uint32_t *__restrict__ src,
+                           const uint32_t *__restrict__ dst, const uint8_t *__restrict__ applied,
+                           uint32_t n, const unsigned long long *keys, const uint32_t *idx,
+                           uint32_t mask, const unsigned long long *__restrict__ brow,
+                           const uint32_t *__restrict__ bcol, bool deletion,
+                           unsigned long long *acc) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  unsigned long long c = 0;
+  for (uint32_t e = group; e < n; e += ngroups) {
+    if (!applied[e]) continue;
+    uint32_t a = src[e], b = dst[e];
+    if (a == b) continue;
+    const unsigned long long ke = pair_key(a, b);
+    if (pairs_find(keys, idx, mask, ke) != e) continue;
+    // iterate the lower-degree endpoint
+    uint32_t x = a, y = b;
+    uint32_t dx = g.deg[a] + (deletion ? (uint32_t)(brow[a + 1] - brow[a]) : 0u);
+    uint32_t dy = g.deg[b] + (deletion ? (uint32_t)(brow[b + 1] - brow[b]) : 0u);
+    if (dy < dx) {
+      x = b;
+      y = a;
+    }
+    auto consider = [&](uint32_t w) {
+      if (w == x || w == y || w >= kTombKey) return;
+      unsigned long long k1 = pair_key(x, w);
+      if (pairs_find(keys, idx, mask, k1) != kEmptyKey && k1 < ke) return;
+      unsigned long long k2 = pair_key(y, w);
+      bool in_b2 = pairs_find(keys, idx, mask, k2) != kEmptyKey;
+      if (in_b2 && k2 < ke) return;
+      bool present = lane_find<kW>(g, y, w) || (deletion && in_b2);
+      if (present) ++c;
+    };
+    walk_vertex(g, L, x, [&](const uint4 &q) {
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+      for (int i = 0; i < keys_per_lane<kW>(); ++i) consider(k[i]);
+    });
+    if (deletion) {
+      for (unsigned long long j = brow[x] + L.gl; j < brow[x + 1]; j += 8) consider(bcol[j]);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(acc, c);
+}
+
+__global__ void k_tc_apply(unsigned long long *count, const unsigned long long *acc, int sign) {
+  if (sign > 0)
+    *count += *acc;
+  else
+    *count -= *acc;
+}
+
+}  // namespace mk
+
+using namespace mk;
+
+struct mk_tc {
+  mk_graph *g = nullptr;
+  unsigned long long *dcount = nullptr;  // [0] count, [1] scratch accumulator
+  uint32_t *small = nullptr;             // [0] big_n
+  DevBuf<uint32_t> ocnt, ocol, big_list, big_scratch, bcnt, bfill, bcol, pidx;
+  DevBuf<unsigned long long> orow, tmp, brow, pkeys;
+  Timer timer;
+};
+
+static int groups_grid(uint64_t items, int device) {
+  uint64_t b = items * 8 / 256 + 1;
+  uint64_t cap = (uint64_t)device_sm_count(device) * 8;
+  return (int)std::min(b, cap);
+}
+
+static mk_status tc_static(mk_tc *t, cudaStream_t s) {
+  mk_graph *g = t->g;
+  const uint32_t V = g->V;
+  size_t acc = 0;
+  MK_CHECK(t->ocnt.reserve(V, &acc));
+  MK_CHECK(t->orow.reserve((size_t)V + 1, &acc));
+  GraphView gv = g->view();
+  int blocks = groups_grid(V, g->device);
+  if (g->weighted)
+    k_orient_count<true><<<blocks, 256, 0, s>>>(gv, t->ocnt.ptr);
+  else
+    k_orient_count<false><<<blocks, 256, 0, s>>>(gv, t->ocnt.ptr);
+  MK_CHECK(scan_u32_to_u64(t->ocnt.ptr, t->orow.ptr, V, t->tmp, s));
+  unsigned long long total = 0;
+  MK_CUDA(cudaMemcpyAsync(&total, t->orow.ptr + V, 8, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  MK_CHECK(t->ocol.reserve(std::max<unsigned long long>(total, 1), &acc));
+  if (g->weighted)
+    k_orient_fill<true><<<blocks, 256, 0, s>>>(gv, t->orow.ptr, t->ocol.ptr);
+  else
+    k_orient_fill<false><<<blocks, 256, 0, s>>>(gv, t->orow.ptr, t->ocol.ptr);
+  MK_CHECK(t->big_list.reserve(V, &acc));
+  MK_CUDA(cudaMemsetAsync(t->dcount, 0, 8, s));
+  MK_CUDA(cudaMemsetAsync(t->small, 0, 4, s));
+  int sblocks = std::min<uint64_t>((uint64_t)V / kTcWarps + 1, (uint64_t)device_sm_count(g->device) * 4);
+  k_tc_small<<<sblocks, kTcWarps * 32, 0, s>>>(V, t->orow.ptr, t->ocol.ptr, t->dcount,
+                                              t->big_list.ptr, t->small);
+  // big vertices: one block each, global-memory set
+  uint32_t nbig = 0;
+  MK_CUDA(cudaMemcpyAsync(&nbig, t->small, 4, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  if (nbig) {
+    // capacity: next power of two >= 2 * max oriented degree (<= 2^26)
+    std::vector<uint32_t> cnt(V);
+    MK_CUDA(cudaMemcpy(cnt.data(), t->ocnt.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost));
+    uint32_t mx = *std::max_element(cnt.begin(), cnt.end());
+    uint32_t cap = 64;
+    while (cap < 2ull * mx) cap <<= 1;
+    int bb = std::min<uint32_t>(nbig, (uint32_t)device_sm_count(g->device) * 2);
+    MK_CHECK(t->big_scratch.reserve((size_t)bb * cap, &acc));
+    k_tc_big<<<bb, 512, 0, s>>>(t->orow.ptr, t->ocol.ptr, t->big_list.ptr, t->small,
+                                t->big_scratch.ptr, cap, t->dcount);
+  }
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+static mk_status tc_dynamic(mk_tc *t, const uint32_t *d_src, const uint32_t *d_dst,
+                            uint32_t n, bool deletion, void *stream, float *ms_out) {
+  mk_graph *g = t->g;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(t->timer.start(s, ms_out != nullptr));
+  const bool matches = n == g->last_n && d_src == g->last_src && d_dst == g->last_dst &&
+                       g->last_op == (deletion ? 2 : 1);
+  if (!matches) {
+    // the batch is not the one the graph just applied: recount from scratch
+    MK_CHECK(tc_static(t, s));
+    return t->timer.stop(ms_out);
+  }
+  if (n == 0) return t->timer.stop(ms_out);
+  size_t acc = 0;
+  uint32_t cap = 1024;
+  while (cap < 2ull * n) cap <<= 1;
+  MK_CHECK(t->pkeys.reserve(cap, &acc));
+  MK_CHECK(t->pidx.reserve(cap, &acc));
+  MK_CUDA(cudaMemsetAsync(t->pkeys.ptr, 0xFF, (size_t)cap * 8, s));
+  MK_CUDA(cudaMemsetAsync(t->pidx.ptr, 0xFF, (size_t)cap * 4, s));
+  const uint8_t *applied = g->applied.ptr;
+  k_pairs_elect<<<(n + 255) / 256, 256, 0, s>>>(d_src, d_dst, applied, n, t->pkeys.ptr,
+                                                t->pidx.ptr, cap - 1);
+  const uint32_t V = g->V;
+  if (deletion) {
+    MK_CHECK(t->bcnt.reserve(V, &acc));
+    MK_CHECK(t->bfill.reserve(V, &acc));
+    MK_CHECK(t->brow.reserve((size_t)V + 1, &acc));
+    MK_CHECK(t->bcol.reserve(2ull * n + 1, &acc));
+    MK_CUDA(cudaMemsetAsync(t->bcnt.ptr, 0, (size_t)V * 4, s));
+    MK_CUDA(cudaMemsetAsync(t->bfill.ptr, 0, (size_t)V * 4, s));
+    k_pairs_degree<<<(n + 255) / 256, 256, 0, s>>>(d_src, d_dst, applied, n, t->pkeys.ptr,
+                                                   t->pidx.ptr, cap - 1, t->bcnt.ptr);
+    MK_CHECK(scan_u32_to_u64(t->bcnt.ptr, t->brow.ptr, V, t->tmp, s));
+    k_pairs_fill<<<(n + 255) / 256, 256, 0, s>>>(d_src, d_dst, applied, n, t->pkeys.ptr,
+                                                 t->pidx.ptr, cap - 1, t->brow.ptr,
+                                                 t->bfill.ptr, t->bcol.ptr);
+  }
+  MK_CUDA(cudaMemsetAsync(t->dcount + 1, 0, 8, s));
+  int blocks = groups_grid(n, g->device);
+  if (g->weighted)
+    k_tc_delta<true><<<blocks, 256, 0, s>>>(g->view(), d_src, d_dst, applied, n, t->pkeys.ptr,
+                                            t->pidx.ptr, cap - 1, t->brow.ptr, t->bcol.ptr,
+                                            deletion, t->dcount + 1);
+  else
+    k_tc_delta<false><<<blocks, 256, 0, s>>>(g->view(), d_src, d_dst, applied, n, t->pkeys.ptr,
+                                             t->pidx.ptr, cap - 1, t->brow.ptr, t->bcol.ptr,
+                                             deletion, t->dcount + 1);
+  k_tc_apply<<<1, 1, 0, s>>>(t->dcount, t->dcount + 1, deletion ? -1 : 1);
+  MK_CUDA(cudaGetLastError());
+  return t->timer.stop(ms_out);
+}
+
+extern "C" {
+
+mk_status mk_tc_create(mk_graph *g, mk_tc **out) {
+  if (!g || !out) return fail(MK_ERR_INVALID, "mk_tc_create: null argument");
+  DeviceGuard dg(g->device);
+  mk_tc *t = new mk_tc();
+  t->g = g;
+  cudaError_t e = cudaMalloc(&t->dcount, 16);
+  if (e == cudaSuccess) e = cudaMalloc(&t->small, 16);
+  if (e == cudaSuccess) e = cudaMemset(t->dcount, 0, 16);
+  if (e != cudaSuccess) {
+    mk_tc_destroy(t);
+    return cuda_fail(e, "mk_tc_create");
+  }
+  *out = t;
+  return MK_OK;
+}
+
+mk_status mk_tc_static(mk_tc *t, void *stream, float *ms_out) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_tc_static: null handle");
+  DeviceGuard dg(t->g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(t->timer.start(s, ms_out != nullptr));
+  MK_CHECK(tc_static(t, s));
+  return t->timer.stop(ms_out);
+}
+
+mk_status mk_tc_incremental(mk_tc *t, const uint32_t *d_src, const uint32_t *d_dst,
+                            uint32_t n, void *stream, float *ms_out) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_tc_incremental: null handle");
+  return tc_dynamic(t, d_src, d_dst, n, false, stream, ms_out);
+}
+
+mk_status mk_tc_decremental(mk_tc *t, const uint32_t *d_src, const uint32_t *d_dst,
+                            uint32_t n, void *stream, float *ms_out) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_tc_decremental: null handle");
+  return tc_dynamic(t, d_src, d_dst, n, true, stream, ms_out);
+}
+
+mk_status mk_tc_count(mk_tc *t, uint64_t *h_count) {
+  if (!t || !h_count) return fail(MK_ERR_INVALID, "mk_tc_count: null argument");
+  DeviceGuard dg(t->g->device);
+  MK_CUDA(cudaDeviceSynchronize());
+  unsigned long long c = 0;
+  MK_CUDA(cudaMemcpy(&c, t->dcount, 8, cudaMemcpyDeviceToHost));
+  *h_count = c;
+  return MK_OK;
+}
+
+mk_status mk_tc_destroy(mk_tc *t) {
+  if (!t) return MK_OK;
+  DeviceGuard dg(t->g->device);
+  cudaFree(t->dcount);
+  cudaFree(t->small);
+  t->ocnt.release();
+  t->ocol.release();
+  t->big_list.release();
+  t->big_scratch.release();
+  t->bcnt.release();
+  t->bfill.release();
+  t->bcol.release();
+  t->pidx.release();
+  t->orow.release();
+  t->tmp.release();
+  t->brow.release();
+  t->pkeys.release();
+  delete t;
+  return MK_OK;
+}
+
+}  // extern "C"

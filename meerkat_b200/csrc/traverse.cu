@@ -1,0 +1,495 @@
+// BFS and SSSP: static, incremental and decremental, one persistent
+// cooperative launch per call.
+//
+// Reference semantics followed (include/Algorithms/impl/BFSImpl.cuh,
+// include/Algorithms/impl/SSSPImpl.cuh):
+//   * distances are packed dist<<32 | parent in a u64 and relaxed with
+//     atomicMin (definitions.cuh:14-17, BFSImpl.cuh:307-314); the source holds
+//     PACK(0, src) (BFS.cuh:47-52); unreachable = INFINF;
+//   * incremental: after the inserts are in the graph, every batch edge (s, d)
+//     with finite dist[s] seeds d, then frontier relaxation runs to a fixed
+//     point (BFSImpl.cuh:296-381, SSSPImpl.cuh:280-364);
+//   * decremental: a deleted edge (s, d) with PARENT(dist[d]) == s
+//     invalidates d and its whole shortest-path subtree; invalidated vertices
+//     are re-seeded from valid in-neighbours and relaxed again
+//     (BFSImpl.cuh:3-42, :384-496).
+//
+// B200 design differences:
+//   * vertex frontiers (not edge frontiers), deduplicated per level with a
+//     stamp word per vertex, staged in a shared-memory queue per block;
+//   * the subtree is invalidated level by level along tree edges
+//     (O(sum of subtree out-degrees)) instead of walking every vertex's parent
+//     chain (O(V * depth), BFSImpl.cuh:17-42);
+//   * re-seeding streams every valid vertex's slabs once (the reference's own
+//     strategy, BFSImpl.cuh:419-440), skipping vertices of degree 0;
+//   * the stored edge weight is probed for every seeding batch edge, so a
+//     batch entry that did not change the graph cannot seed a wrong distance;
+//   * one 8-lane group per frontier vertex reads 128-byte slabs with 16-byte
+//     loads; grid-wide barriers are bounded (MK_ERR_TIMEOUT, never a hang).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "mk_internal.h"
+#include "mk_slab.cuh"
+
+namespace mk {
+
+enum TravMode : uint32_t { kStatic = 0, kIncremental = 1, kDecremental = 2 };
+
+// ctl words (u32)
+enum Ctl : int {
+  kBar0 = 0,      // barrier arrival
+  kBar1 = 1,      // barrier generation
+  kErr = 2,       // sticky error bits
+  kSz0 = 4,       // frontier sizes kSz0 + (level % 3)
+  kInvCount = 8,  // invalidated vertices so far (append cursor of inv_list)
+  kLevels = 9,    // relaxation levels run by the last call
+  kDSz0 = 10,     // invalidation frontier sizes kDSz0 + (level % 3)
+  kRound = 15,    // stamp base, persists across calls
+  kCtlWords = 16
+};
+
+struct TravArgs {
+  GraphView g;
+  unsigned long long *dist;
+  uint32_t *stamp;
+  uint32_t *inval;  // bitmap, one bit per vertex
+  uint32_t *fr0;
+  uint32_t *fr1;
+  uint32_t *inv_list;
+  uint32_t *ctl;
+  unsigned long long *pushed;
+  const uint32_t *bsrc;
+  const uint32_t *bdst;
+  uint32_t bn;
+  uint32_t source;
+  uint32_t mode;
+  unsigned long long limit_ns;
+};
+
+constexpr int kTravBlock = 256;
+constexpr int kQueueCap = 2048;
+
+struct BlockQueue {
+  uint32_t *q;
+  uint32_t *qn;
+};
+
+__device__ __forceinline__ void queue_push(const BlockQueue &Q, uint32_t v,
+                                           uint32_t *gfr, uint32_t *gsz) {
+  uint32_t pos = atomicAdd(Q.qn, 1u);
+  if (pos < kQueueCap) {
+    Q.q[pos] = v;
+  } else {
+    uint32_t gp = atomicAdd(gsz, 1u);
+    gfr[gp] = v;
+  }
+}
+
+// Flushes the block queue into the global frontier; all threads call it.
+__device__ __forceinline__ void queue_flush(const BlockQueue &Q, uint32_t *gfr,
+                                            uint32_t *gsz,
+                                            unsigned long long *pushed,
+                                            uint32_t *base_s) {
+  __syncthreads();
+  uint32_t cnt = min(*Q.qn, (uint32_t)kQueueCap);
+  if (threadIdx.x == 0) {
+    *base_s = cnt ? atomicAdd(gsz, cnt) : 0u;
+    uint32_t total = *Q.qn;
+    if (total) atomicAdd(pushed, (unsigned long long)total);
+  }
+  __syncthreads();
+  uint32_t base = *base_s;
+  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) gfr[base + i] = Q.q[i];
+  __syncthreads();
+  if (threadIdx.x == 0) *Q.qn = 0;
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool inval_test(const uint32_t *bits, uint32_t v) {
+  return (__ldcg(bits + (v >> 5)) >> (v & 31)) & 1u;
+}
+// Sets v's bit; true if this call set it.
+__device__ __forceinline__ bool inval_set(uint32_t *bits, uint32_t v) {
+  uint32_t m = 1u << (v & 31);
+  return (atomicOr(bits + (v >> 5), m) & m) == 0;
+}
+
+__device__ __forceinline__ unsigned long long ld_dist(const unsigned long long *p) {
+  return __ldcg(p);
+}
+
+// Relaxes v with candidate distance nd via parent u; pushes v on improvement.
+__device__ __forceinline__ void relax(const TravArgs &a, const BlockQueue &Q,
+                                      uint32_t v, unsigned long long nd,
+                                      uint32_t u, uint32_t stamp_next,
+                                      uint32_t *gfr, uint32_t *gsz) {
+  if (nd >= kInf) return;
+  unsigned long long cur = ld_dist(a.dist + v);
+  if (nd >= pack_hi(cur)) return;
+  unsigned long long cand = pack((uint32_t)nd, u);
+  unsigned long long old = atomicMin(a.dist + v, cand);
+  if (pack_hi(old) > nd) {
+    if (atomicExch(a.stamp + v, stamp_next) != stamp_next) queue_push(Q, v, gfr, gsz);
+  }
+}
+
+// Expands vertex u: relax every live out-neighbour.
+template <bool kW, bool kUseW>
+__device__ __forceinline__ void expand(const TravArgs &a, const Lanes &L,
+                                       const BlockQueue &Q, uint32_t u,
+                                       uint32_t du, uint32_t stamp_next,
+                                       uint32_t *gfr, uint32_t *gsz,
+                                       bool only_invalid) {
+  walk_vertex(a.g, L, u, [&](const uint4 &q) {
+    uint32_t k[4], w[4];
+    lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+    for (int i = 0; i < keys_per_lane<kW>(); ++i) {
+      uint32_t v = k[i];
+      if (v < kTombKey && v != u) {
+        if (only_invalid && !inval_test(a.inval, v)) continue;
+        unsigned long long nd = (unsigned long long)du + (kUseW ? w[i] : 1u);
+        relax(a, Q, v, nd, u, stamp_next, gfr, gsz);
+      }
+    }
+  });
+}
+
+template <bool kW, bool kUseW>
+__global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
+  __shared__ uint32_t q_s[kQueueCap];
+  __shared__ uint32_t qn_s;
+  __shared__ uint32_t base_s;
+  if (threadIdx.x == 0) qn_s = 0;
+  __syncthreads();
+  BlockQueue Q{q_s, &qn_s};
+  const Lanes L = lanes();
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  const uint32_t group = tid >> 3;
+  const uint32_t ngroups = nthreads >> 3;
+  uint32_t *ctl = a.ctl;
+  uint32_t *err = ctl + kErr;
+  uint32_t *fr[2] = {a.fr0, a.fr1};
+  uint32_t round = ld_acquire_u32(ctl + kRound);
+
+  // ---- seeding (level -1 pushes into fr[0] / sz[0]) ----
+  if (a.mode == kStatic) {
+    if (tid == 0) {
+      a.dist[a.source] = pack(0, a.source);
+      a.stamp[a.source] = round + 1;
+      a.fr0[0] = a.source;
+      ctl[kSz0] = 1;
+      atomicAdd(a.pushed, 1ull);
+    }
+  } else if (a.mode == kIncremental) {
+    for (uint32_t e = group; e < a.bn; e += ngroups) {
+      uint32_t s = a.bsrc[e], d = a.bdst[e];
+      if (s == d || s >= a.g.V || d >= a.g.V) continue;
+      // one lane loads, the group decides together
+      unsigned long long ps = 0, pd = 0;
+      if (L.gl == 0) {
+        ps = ld_dist(a.dist + s);
+        pd = ld_dist(a.dist + d);
+      }
+      ps = __shfl_sync(L.gmask, ps, L.gbase);
+      pd = __shfl_sync(L.gmask, pd, L.gbase);
+      if (ps == kInfInf) continue;
+      uint32_t ds = pack_hi(ps);
+      if (ds >= pack_hi(pd)) continue;
+      uint32_t wv = 1;
+      bool present = find_edge<kW>(a.g, L, s, d, &wv);
+      if (!present) continue;
+      if (L.gl == 0) {
+        unsigned long long nd = (unsigned long long)ds + (kUseW ? wv : 1u);
+        relax(a, Q, d, nd, s, round + 1, a.fr0, ctl + kSz0);
+      }
+    }
+  } else {  // kDecremental
+    // D1: children of deleted tree edges.  Every invalidated vertex goes to
+    // inv_list (for the final flag reset) and to the invalidation frontier.
+    auto invalidate = [&](uint32_t v, uint32_t *gfr, uint32_t *gsz) {
+      a.dist[v] = kInfInf;
+      a.inv_list[atomicAdd(ctl + kInvCount, 1u)] = v;
+      gfr[atomicAdd(gsz, 1u)] = v;
+    };
+    for (uint32_t e = tid; e < a.bn; e += nthreads) {
+      uint32_t s = a.bsrc[e], d = a.bdst[e];
+      if (s == d || s >= a.g.V || d >= a.g.V || d == a.source) continue;
+      unsigned long long pd = ld_dist(a.dist + d);
+      if (pd != kInfInf && pack_lo(pd) == s && inval_set(a.inval, d))
+        invalidate(d, a.fr0, ctl + kDSz0);
+    }
+    if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+    // D2: invalidate whole subtrees along tree edges, level by level.  Sizes
+    // rotate over three counters so no block reads a counter that another
+    // block is already filling for the next level.
+    for (uint32_t dl = 0;; ++dl) {
+      const uint32_t n = ld_acquire_u32(ctl + kDSz0 + (dl % 3));
+      if (n == 0) break;
+      if (tid == 0) ctl[kDSz0 + ((dl + 2) % 3)] = 0;
+      const uint32_t *cur = fr[dl & 1];
+      uint32_t *nxt = fr[(dl + 1) & 1];
+      uint32_t *nsz = ctl + kDSz0 + ((dl + 1) % 3);
+      for (uint32_t i = group; i < n; i += ngroups) {
+        const uint32_t x = cur[i];
+        walk_vertex(a.g, L, x, [&](const uint4 &q) {
+          uint32_t k[4], w[4];
+          lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+          for (int j = 0; j < keys_per_lane<kW>(); ++j) {
+            uint32_t y = k[j];
+            if (y < kTombKey && y != x && y != a.source && !inval_test(a.inval, y)) {
+              unsigned long long py = ld_dist(a.dist + y);
+              if (py != kInfInf && pack_lo(py) == x && inval_set(a.inval, y)) invalidate(y, nxt, nsz);
+            }
+          }
+        });
+      }
+      if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+    }
+    const uint32_t hi = ld_acquire_u32(ctl + kInvCount);
+    // D3: re-seed invalidated vertices from valid in-neighbours (full sweep)
+    if (hi > 0) {
+      for (uint32_t u = group; u < a.g.V; u += ngroups) {
+        if (a.g.deg[u] == 0 || inval_test(a.inval, u)) continue;
+        unsigned long long pu = 0;
+        if (L.gl == 0) pu = ld_dist(a.dist + u);
+        pu = __shfl_sync(L.gmask, pu, L.gbase);
+        if (pu == kInfInf) continue;
+        expand<kW, kUseW>(a, L, Q, u, pack_hi(pu), round + 1, a.fr0, ctl + kSz0, true);
+      }
+    }
+  }
+  queue_flush(Q, a.fr0, ctl + kSz0, a.pushed, &base_s);
+  if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+
+  // ---- relaxation levels ----
+  uint32_t lv = 0;
+  for (;; ++lv) {
+    uint32_t n = ld_acquire_u32(ctl + kSz0 + (lv % 3));
+    if (n == 0) break;
+    if (tid == 0) ctl[kSz0 + ((lv + 2) % 3)] = 0;
+    uint32_t *cur = fr[lv & 1];
+    uint32_t *nxt = fr[(lv + 1) & 1];
+    uint32_t *nsz = ctl + kSz0 + ((lv + 1) % 3);
+    const uint32_t stamp_next = round + 2 + lv;
+    for (uint32_t i = group; i < n; i += ngroups) {
+      uint32_t u = cur[i];
+      unsigned long long pu = 0;
+      if (L.gl == 0) pu = ld_dist(a.dist + u);
+      pu = __shfl_sync(L.gmask, pu, L.gbase);
+      if (pu == kInfInf) continue;
+      expand<kW, kUseW>(a, L, Q, u, pack_hi(pu), stamp_next, nxt, nsz, false);
+    }
+    queue_flush(Q, nxt, nsz, a.pushed, &base_s);
+    if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+  }
+
+  // ---- epilogue: clear invalidation flags, publish counters ----
+  if (a.mode == kDecremental) {
+    uint32_t ninv = ld_acquire_u32(ctl + kInvCount);
+    for (uint32_t i = tid; i < ninv; i += nthreads) a.inval[a.inv_list[i] >> 5] = 0u;
+  }
+  if (tid == 0) {
+    ctl[kLevels] = lv;
+    ctl[kRound] = round + 3 + lv;
+  }
+}
+
+}  // namespace mk
+
+using namespace mk;
+
+struct mk_traversal {
+  mk_graph *g = nullptr;
+  uint32_t source = 0;
+  bool sssp = false;
+  bool has_static = false;
+  int nblocks = 0;
+  unsigned long long *dist = nullptr;
+  uint32_t *stamp = nullptr;
+  uint32_t *inval = nullptr;
+  uint32_t *fr0 = nullptr, *fr1 = nullptr, *inv_list = nullptr;
+  uint32_t *ctl = nullptr;
+  unsigned long long *pushed = nullptr;
+  Timer timer;
+};
+
+static mk_status trav_create(mk_graph *g, uint32_t source, bool sssp, mk_traversal **out) {
+  if (!g || !out) return fail(MK_ERR_INVALID, "traversal create: null argument");
+  *out = nullptr;
+  if (source >= g->V) return fail(MK_ERR_INVALID, "traversal create: source out of range");
+  if (g->reverse) return fail(MK_ERR_INVALID, "traversal create: graph must store out-edges");
+  if (sssp && !g->weighted) return fail(MK_ERR_INVALID, "SSSP needs a weighted graph");
+  DeviceGuard dg(g->device);
+  mk_traversal *t = new mk_traversal();
+  t->g = g;
+  t->source = source;
+  t->sssp = sssp;
+  const size_t V = g->V;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](void **p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  A((void **)&t->dist, V * 8);
+  A((void **)&t->stamp, V * 4);
+  A((void **)&t->inval, (V + 31) / 32 * 4);
+  A((void **)&t->fr0, V * 4 + 16);
+  A((void **)&t->fr1, V * 4 + 16);
+  A((void **)&t->inv_list, V * 4 + 16);
+  A((void **)&t->ctl, kCtlWords * 4);
+  A((void **)&t->pushed, 8);
+  if (e == cudaSuccess) e = cudaMemset(t->dist, 0xFF, V * 8);
+  if (e == cudaSuccess) e = cudaMemset(t->stamp, 0, V * 4);
+  if (e == cudaSuccess) e = cudaMemset(t->inval, 0, (V + 31) / 32 * 4);
+  if (e == cudaSuccess) e = cudaMemset(t->ctl, 0, kCtlWords * 4);
+  if (e == cudaSuccess) {
+    // dist[src] = PACK(0, src) as the reference constructor does (BFS.cuh:49-52)
+    unsigned long long s0 = pack(0, source);
+    e = cudaMemcpy(t->dist + source, &s0, 8, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) {
+    uint32_t one = 1;
+    e = cudaMemcpy(t->ctl + kRound, &one, 4, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    mk_traversal_destroy(t);
+    return cuda_fail(e, "traversal create");
+  }
+  *out = t;
+  return MK_OK;
+}
+
+static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
+                             const uint32_t *bd, uint32_t n, void *stream,
+                             float *ms_out) {
+  mk_graph *g = t->g;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  if (n && (!bs || !bd)) return fail(MK_ERR_INVALID, "traversal: null batch");
+  MK_CHECK(t->timer.start(s, ms_out != nullptr));
+  if (mode == kStatic) MK_CUDA(cudaMemsetAsync(t->dist, 0xFF, (size_t)g->V * 8, s));
+  // clear everything but the persistent round counter
+  MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
+  MK_CUDA(cudaMemsetAsync(t->pushed, 0, 8, s));
+  TravArgs a;
+  a.g = g->view();
+  a.dist = t->dist;
+  a.stamp = t->stamp;
+  a.inval = t->inval;
+  a.fr0 = t->fr0;
+  a.fr1 = t->fr1;
+  a.inv_list = t->inv_list;
+  a.ctl = t->ctl;
+  a.pushed = t->pushed;
+  a.bsrc = bs;
+  a.bdst = bd;
+  a.bn = n;
+  a.source = t->source;
+  a.mode = mode;
+  a.limit_ns = 4000000000ull;
+  const void *fn;
+  if (g->weighted)
+    fn = t->sssp ? (const void *)k_traverse<true, true> : (const void *)k_traverse<true, false>;
+  else
+    fn = (const void *)k_traverse<false, false>;
+  if (t->nblocks == 0) t->nblocks = persistent_blocks(fn, kTravBlock, 0, g->device);
+  void *args[] = {&a};
+  MK_CUDA(cudaLaunchCooperativeKernel(fn, dim3(t->nblocks), dim3(kTravBlock), args, 0, s));
+  MK_CHECK(t->timer.stop(ms_out));
+  if (mode == kStatic) t->has_static = true;
+  return MK_OK;
+}
+
+extern "C" {
+
+mk_status mk_bfs_create(mk_graph *g, uint32_t source, mk_traversal **out) {
+  return trav_create(g, source, false, out);
+}
+
+mk_status mk_sssp_create(mk_graph *g, uint32_t source, mk_traversal **out) {
+  return trav_create(g, source, true, out);
+}
+
+mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_traversal_static: null handle");
+  return trav_launch(t, kStatic, nullptr, nullptr, 0, stream, ms_out);
+}
+
+mk_status mk_traversal_incremental(mk_traversal *t, const uint32_t *d_src,
+                                   const uint32_t *d_dst, const uint32_t *d_w,
+                                   uint32_t n, void *stream, float *ms_out) {
+  (void)d_w;
+  if (!t) return fail(MK_ERR_INVALID, "mk_traversal_incremental: null handle");
+  return trav_launch(t, kIncremental, d_src, d_dst, n, stream, ms_out);
+}
+
+mk_status mk_traversal_decremental(mk_traversal *t, const uint32_t *d_src,
+                                   const uint32_t *d_dst, const uint32_t *d_w,
+                                   uint32_t n, void *stream, float *ms_out) {
+  (void)d_w;
+  if (!t) return fail(MK_ERR_INVALID, "mk_traversal_decremental: null handle");
+  return trav_launch(t, kDecremental, d_src, d_dst, n, stream, ms_out);
+}
+
+mk_status mk_traversal_distances(mk_traversal *t, uint32_t *h_out) {
+  if (!t || !h_out) return fail(MK_ERR_INVALID, "mk_traversal_distances: null argument");
+  DeviceGuard dg(t->g->device);
+  const size_t V = t->g->V;
+  std::vector<unsigned long long> tmp(V);
+  MK_CUDA(cudaDeviceSynchronize());
+  uint32_t err = 0;
+  MK_CUDA(cudaMemcpy(&err, t->ctl + kErr, 4, cudaMemcpyDeviceToHost));
+  MK_CUDA(cudaMemcpy(tmp.data(), t->dist, V * 8, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < V; ++i) h_out[i] = pack_hi(tmp[i]);
+  if (err & kErrTimeout) return fail(MK_ERR_TIMEOUT, "traversal: grid barrier timed out");
+  return MK_OK;
+}
+
+mk_status mk_traversal_packed(mk_traversal *t, const uint64_t **d_packed) {
+  if (!t || !d_packed) return fail(MK_ERR_INVALID, "mk_traversal_packed: null argument");
+  *d_packed = reinterpret_cast<const uint64_t *>(t->dist);
+  return MK_OK;
+}
+
+mk_status mk_traversal_packed_host(mk_traversal *t, uint64_t *h_out) {
+  if (!t || !h_out) return fail(MK_ERR_INVALID, "mk_traversal_packed_host: null argument");
+  DeviceGuard dg(t->g->device);
+  MK_CUDA(cudaDeviceSynchronize());
+  MK_CUDA(cudaMemcpy(h_out, t->dist, (size_t)t->g->V * 8, cudaMemcpyDeviceToHost));
+  return MK_OK;
+}
+
+mk_status mk_traversal_stats(mk_traversal *t, uint32_t *h_levels, uint64_t *h_pushed) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_traversal_stats: null handle");
+  DeviceGuard dg(t->g->device);
+  MK_CUDA(cudaDeviceSynchronize());
+  uint32_t ctl[kCtlWords];
+  unsigned long long p = 0;
+  MK_CUDA(cudaMemcpy(ctl, t->ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+  MK_CUDA(cudaMemcpy(&p, t->pushed, 8, cudaMemcpyDeviceToHost));
+  if (h_levels) *h_levels = ctl[kLevels];
+  if (h_pushed) *h_pushed = p;
+  if (ctl[kErr] & kErrTimeout) return fail(MK_ERR_TIMEOUT, "traversal: grid barrier timed out");
+  return MK_OK;
+}
+
+mk_status mk_traversal_destroy(mk_traversal *t) {
+  if (!t) return MK_OK;
+  DeviceGuard dg(t->g->device);
+  cudaFree(t->dist);
+  cudaFree(t->stamp);
+  cudaFree(t->inval);
+  cudaFree(t->fr0);
+  cudaFree(t->fr1);
+  cudaFree(t->inv_list);
+  cudaFree(t->ctl);
+  cudaFree(t->pushed);
+  delete t;
+  return MK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,258 @@
+// Weakly connected components by lock-free union-find.
+//
+// The reference ships the device primitives only
+// (include/Util/UnionFind.cuh:24-254): find with path splitting/halving, and
+// union that hooks the larger root under the smaller one with a CAS
+// (UnionAsync, :194-215), so every root is the minimum vertex id of its tree.
+// This build adds the entry points:
+//   static       every vertex is its own parent, every live edge is a union,
+//                then every vertex is compressed to its root;
+//   incremental  union of the edges the last insert applied, then compress;
+//   decremental  union-find cannot split, so every component that lost an
+//                edge is reset and rebuilt from its vertices' out-edges (an
+//                edge into an affected vertex comes from the same old
+//                component, so those out-edges are all its edges).
+// Labels are the minimum vertex id of each weakly connected component.
+//
+// Every retry loop is bounded; on expiry the kernel sets MK_DEVERR_TIMEOUT.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "mk_internal.h"
+#include "mk_slab.cuh"
+
+namespace mk {
+
+constexpr uint32_t kUfLimit = 1u << 26;
+
+// find with path halving; parent words are read through L2 because other
+// SMs hook and halve concurrently.
+__device__ __forceinline__ uint32_t uf_find(uint32_t *p, uint32_t x) {
+  for (uint32_t it = 0; it < kUfLimit; ++it) {
+    uint32_t px = __ldcg(p + x);
+    if (px == x) return x;
+    uint32_t gx = __ldcg(p + px);
+    if (px != gx) p[x] = gx;  // x is not a root: only halving writes it
+    x = gx;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b, uint32_t *err) {
+  for (uint32_t it = 0; it < kUfLimit; ++it) {
+    uint32_t ra = uf_find(p, a), rb = uf_find(p, b);
+    if (ra == rb) return;
+    uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+    if (atomicCAS(p + hi, hi, lo) == hi) return;
+  }
+  atomicOr(err, kErrTimeout);
+}
+
+__global__ void k_uf_init(uint32_t *p, uint32_t V) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) p[i] = i;
+}
+
+// Union every out-edge of the vertices selected by `sel` (all if null).
+template <bool kW>
+__global__ void k_uf_edges(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t u = group; u < g.V; u += ngroups) {
+    if (g.deg[u] == 0) continue;
+    if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
+    walk_vertex(g, L, u, [&](const uint4 &q) {
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+      for (int i = 0; i < keys_per_lane<kW>(); ++i)
+        if (k[i] < kTombKey && k[i] != u) uf_union(p, u, k[i], err);
+    });
+  }
+}
+
+__global__ void k_uf_batch(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                           const uint8_t *__restrict__ applied, uint32_t n, uint32_t V,
+                           uint32_t *p, uint32_t *err) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || !applied[e]) return;
+  uint32_t a = src[e], b = dst[e];
+  if (a != b && a < V && b < V) uf_union(p, a, b, err);
+}
+
+__global__ void k_uf_compress(uint32_t *p, uint32_t V, const uint32_t *sel_bits) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+    if (sel_bits && !((sel_bits[i >> 5] >> (i & 31)) & 1u)) continue;
+    p[i] = uf_find(p, i);
+  }
+}
+
+// Marks the label (root) of every endpoint of an applied deletion.
+__global__ void k_uf_mark(const uint32_t *__restrict__ src, const uint8_t *__restrict__ applied,
+                          uint32_t n, uint32_t V, const uint32_t *p, uint32_t *aff_labels) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || !applied[e]) return;
+  uint32_t a = src[e];
+  if (a >= V) return;
+  uint32_t r = p[a];
+  atomicOr(aff_labels + (r >> 5), 1u << (r & 31));
+}
+
+// Resets the vertices of affected components and records them.
+__global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, uint32_t *aff_vertices) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+    uint32_t r = p[i];
+    if ((aff_labels[r >> 5] >> (r & 31)) & 1u) {
+      p[i] = i;
+      atomicOr(aff_vertices + (i >> 5), 1u << (i & 31));
+    }
+  }
+}
+
+}  // namespace mk
+
+using namespace mk;
+
+struct mk_wcc {
+  mk_graph *g = nullptr;
+  uint32_t *parent = nullptr;
+  uint32_t *aff_labels = nullptr;
+  uint32_t *aff_vertices = nullptr;
+  uint32_t *err = nullptr;
+  Timer timer;
+};
+
+static int flat_grid(uint64_t n, int device) {
+  return (int)std::min<uint64_t>(n / 256 + 1, (uint64_t)device_sm_count(device) * 8);
+}
+
+static mk_status wcc_edges(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
+  mk_graph *g = w->g;
+  int blocks = (int)std::min<uint64_t>((uint64_t)g->V * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  if (g->weighted)
+    k_uf_edges<true><<<blocks, 256, 0, s>>>(g->view(), w->parent, sel, w->err);
+  else
+    k_uf_edges<false><<<blocks, 256, 0, s>>>(g->view(), w->parent, sel, w->err);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+static mk_status wcc_static(mk_wcc *w, cudaStream_t s) {
+  mk_graph *g = w->g;
+  k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V);
+  MK_CHECK(wcc_edges(w, nullptr, s));
+  k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, nullptr);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+static bool batch_matches(const mk_graph *g, const uint32_t *d_src, const uint32_t *d_dst,
+                          uint32_t n, int op) {
+  return n == g->last_n && d_src == g->last_src && d_dst == g->last_dst && g->last_op == op;
+}
+
+extern "C" {
+
+mk_status mk_wcc_create(mk_graph *g, mk_wcc **out) {
+  if (!g || !out) return fail(MK_ERR_INVALID, "mk_wcc_create: null argument");
+  DeviceGuard dg(g->device);
+  mk_wcc *w = new mk_wcc();
+  w->g = g;
+  const size_t V = g->V, words = (V + 31) / 32;
+  cudaError_t e = cudaMalloc(&w->parent, V * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&w->aff_labels, words * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&w->aff_vertices, words * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&w->err, 4);
+  if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4);
+  if (e != cudaSuccess) {
+    mk_wcc_destroy(w);
+    return cuda_fail(e, "mk_wcc_create");
+  }
+  k_uf_init<<<flat_grid(V, g->device), 256>>>(w->parent, (uint32_t)V);
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    mk_wcc_destroy(w);
+    return cuda_fail(e, "mk_wcc_create");
+  }
+  *out = w;
+  return MK_OK;
+}
+
+mk_status mk_wcc_static(mk_wcc *w, void *stream, float *ms_out) {
+  if (!w) return fail(MK_ERR_INVALID, "mk_wcc_static: null handle");
+  DeviceGuard dg(w->g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(w->timer.start(s, ms_out != nullptr));
+  MK_CHECK(wcc_static(w, s));
+  return w->timer.stop(ms_out);
+}
+
+mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d_dst,
+                             uint32_t n, void *stream, float *ms_out) {
+  if (!w) return fail(MK_ERR_INVALID, "mk_wcc_incremental: null handle");
+  mk_graph *g = w->g;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(w->timer.start(s, ms_out != nullptr));
+  if (!batch_matches(g, d_src, d_dst, n, 1)) {
+    MK_CHECK(wcc_static(w, s));
+  } else if (n) {
+    k_uf_batch<<<(n + 255) / 256, 256, 0, s>>>(d_src, d_dst, g->applied.ptr, n, g->V, w->parent, w->err);
+    k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, nullptr);
+    MK_CUDA(cudaGetLastError());
+  }
+  return w->timer.stop(ms_out);
+}
+
+mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d_dst,
+                             uint32_t n, void *stream, float *ms_out) {
+  if (!w) return fail(MK_ERR_INVALID, "mk_wcc_decremental: null handle");
+  mk_graph *g = w->g;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(w->timer.start(s, ms_out != nullptr));
+  if (!batch_matches(g, d_src, d_dst, n, 2)) {
+    MK_CHECK(wcc_static(w, s));
+  } else if (n) {
+    const size_t words = ((size_t)g->V + 31) / 32;
+    MK_CUDA(cudaMemsetAsync(w->aff_labels, 0, words * 4, s));
+    MK_CUDA(cudaMemsetAsync(w->aff_vertices, 0, words * 4, s));
+    k_uf_mark<<<(n + 255) / 256, 256, 0, s>>>(d_src, g->applied.ptr, n, g->V, w->parent, w->aff_labels);
+    k_uf_reset<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, w->aff_labels, w->aff_vertices);
+    MK_CHECK(wcc_edges(w, w->aff_vertices, s));
+    k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, w->aff_vertices);
+    MK_CUDA(cudaGetLastError());
+  }
+  return w->timer.stop(ms_out);
+}
+
+mk_status mk_wcc_labels(mk_wcc *w, uint32_t *h_out) {
+  if (!w || !h_out) return fail(MK_ERR_INVALID, "mk_wcc_labels: null argument");
+  DeviceGuard dg(w->g->device);
+  MK_CUDA(cudaDeviceSynchronize());
+  uint32_t err = 0;
+  MK_CUDA(cudaMemcpy(&err, w->err, 4, cudaMemcpyDeviceToHost));
+  MK_CUDA(cudaMemcpy(h_out, w->parent, (size_t)w->g->V * 4, cudaMemcpyDeviceToHost));
+  if (err & kErrTimeout) return fail(MK_ERR_TIMEOUT, "wcc: union-find retry limit exceeded");
+  return MK_OK;
+}
+
+mk_status mk_wcc_labels_device(mk_wcc *w, const uint32_t **d_labels) {
+  if (!w || !d_labels) return fail(MK_ERR_INVALID, "mk_wcc_labels_device: null argument");
+  *d_labels = w->parent;
+  return MK_OK;
+}
+
+mk_status mk_wcc_destroy(mk_wcc *w) {
+  if (!w) return MK_OK;
+  DeviceGuard dg(w->g->device);
+  cudaFree(w->parent);
+  cudaFree(w->aff_labels);
+  cudaFree(w->aff_vertices);
+  cudaFree(w->err);
+  delete w;
+  return MK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,7 @@
+"""CPU oracle of the dynamic-graph semantics (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+package, as the checker.  See mk_oracle.c for the restated semantics and the
+reference lines they follow.
+"""
+from .oracle import OracleGraph, build_oracle  # noqa: F401

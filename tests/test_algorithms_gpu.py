@@ -1,0 +1,269 @@
+"""GPU parity of BFS, SSSP, PageRank, TC and WCC (static, incremental,
+decremental) against the golden vectors and the oracle.
+
+Integer results are bit-exact; BFS/SSSP parents must be valid shortest-path
+parents; PageRank must be within L1 <= 1e-6 of the FP64 oracle."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import meerkat_b200 as mk
+from helpers import degree_hints, make_pair, symmetrise, to_dev
+from oracle import OracleGraph
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden" / "rmat10.npz"
+PR_L1_TOL = 1e-6  # north-star tolerance for FP32 PageRank vs the FP64 oracle
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return dict(np.load(GOLD))
+
+
+def test_golden_fixture_through_the_abi(gold):
+    V = 1024
+    s, d, w = gold["src"], gold["dst"], gold["w"]
+    G = mk.DynamicGraph(V, degree_hints=degree_hints(s, V), weighted=True)
+    Gr = mk.DynamicGraph(V, degree_hints=degree_hints(d, V), reverse=True)
+    ss, sd = symmetrise(s, d)
+    Gs = mk.DynamicGraph(V, degree_hints=degree_hints(ss, V))
+    ts, td, tw = to_dev(s), to_dev(d), to_dev(w)
+    G.InsertEdges(ts, td, vals=tw)
+    Gr.InsertEdges(ts, td)
+    Gs.InsertEdges(to_dev(ss), to_dev(sd))
+    for g in (G, Gr, Gs):
+        assert g.sync() == 0
+    bfs, sssp = mk.BFS(G, 0, V), mk.SSSP(G, 0, V)
+    pr = mk.PageRank(Gr, 0.85, 1e-6, V, max_iter=500)
+    tc, wcc = mk.TC(Gs, V), mk.WCC(G)
+    bfs.Static(len(s))
+    sssp.Static(len(s))
+    pr.Static()
+    tc.Static(len(ss))
+    wcc.Static()
+
+    def check(prefix):
+        np.testing.assert_array_equal(bfs.Distances(), gold[prefix + "bfs"])
+        np.testing.assert_array_equal(sssp.Distances(), gold[prefix + "sssp"])
+        np.testing.assert_array_equal(wcc.Labels(), gold[prefix + "wcc"])
+        assert np.abs(pr.Values().astype(np.float64) - gold[prefix + "pr"]).sum() <= PR_L1_TOL
+        assert tc.GetCount() == int(gold[prefix + "tc"])
+
+    check("base_")
+    # insert batch: graph first, then the algorithms with the same batch
+    i_s, i_d, i_w = to_dev(gold["ins_src"]), to_dev(gold["ins_dst"]), to_dev(gold["ins_w"])
+    G.InsertEdges(i_s, i_d, vals=i_w)
+    Gr.InsertEdges(i_s, i_d)
+    sym_s = to_dev(np.concatenate([gold["ins_src"], gold["ins_dst"]]))
+    sym_d = to_dev(np.concatenate([gold["ins_dst"], gold["ins_src"]]))
+    Gs.InsertEdges(sym_s, sym_d)
+    bfs.Incremental(i_s, i_d)
+    sssp.Incremental(i_s, i_d, wgt=i_w)
+    wcc.Incremental(i_s, i_d)
+    pr.Incremental(i_s, i_d)
+    tc.Incremental(sym_s, sym_d)
+    check("ins_")
+    # delete batch
+    d_s, d_d = to_dev(gold["del_src"]), to_dev(gold["del_dst"])
+    G.DeleteEdges(d_s, d_d)
+    Gr.DeleteEdges(d_s, d_d)
+    sym_s = to_dev(np.concatenate([gold["del_src"], gold["del_dst"]]))
+    sym_d = to_dev(np.concatenate([gold["del_dst"], gold["del_src"]]))
+    Gs.DeleteEdges(sym_s, sym_d)
+    bfs.Decremental(d_s, d_d)
+    sssp.Decremental(d_s, d_d)
+    wcc.Decremental(d_s, d_d)
+    pr.Decremental(d_s, d_d)
+    tc.Decremental(sym_s, sym_d)
+    check("del_")
+
+
+def _traversal_rounds(V, s, d, w, rounds, batch, seed, hints="exact"):
+    G, O = make_pair(V, s, d, w, weighted=True, hints=hints)
+    es = mk.EdgeSet(V, s, d)
+    src = int(np.argmax(np.bincount(s, minlength=V)))
+    bfs, sssp = mk.BFS(G, src, V), mk.SSSP(G, src, V)
+    bfs.Static()
+    sssp.Static()
+    rng = np.random.default_rng(seed)
+
+    def check():
+        np.testing.assert_array_equal(bfs.Distances(), O.bfs(src))
+        np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
+        assert O.check_parents(src, bfs.packed(), weighted=False) == 0
+        assert O.check_parents(src, sssp.packed(), weighted=True) == 0
+
+    check()
+    for r in range(rounds):
+        ds, dd = es.sample_present(batch, seed=seed * 100 + 2 * r)
+        # also delete some current shortest-path tree edges (subtree invalidation)
+        packed = sssp.packed()
+        par = (packed & 0xFFFFFFFF).astype(np.uint32)
+        tree_v = np.nonzero((packed != np.uint64(2**64 - 1)) & (par != np.arange(V)))[0]
+        pick = rng.choice(tree_v, size=min(batch // 2, len(tree_v)), replace=False)
+        ts, td = par[pick], pick.astype(np.uint32)
+        ds = np.concatenate([ds, ts]).astype(np.uint32)
+        dd = np.concatenate([dd, td]).astype(np.uint32)
+        tds, tdd = to_dev(ds), to_dev(dd)
+        G.DeleteEdges(tds, tdd)
+        assert G.sync() == 0
+        O.delete(ds, dd)
+        bfs.Decremental(tds, tdd)
+        sssp.Decremental(tds, tdd)
+        check()
+        ins_s, ins_d = es.sample_absent(batch, seed=seed * 100 + 2 * r + 1)
+        ins_w = rng.integers(1, 65, batch).astype(np.uint32)
+        tis, tid, tiw = to_dev(ins_s), to_dev(ins_d), to_dev(ins_w)
+        G.InsertEdges(tis, tid, vals=tiw)
+        assert G.sync() == 0
+        O.insert(ins_s, ins_d, ins_w)
+        bfs.Incremental(tis, tid)
+        sssp.Incremental(tis, tid, wgt=tiw)
+        check()
+
+
+def test_traversals_rmat_rounds():
+    V = 1 << 13
+    s, d, w = mk.gen_rmat(13, 80000, seed=21, w_lo=1, w_hi=64)
+    _traversal_rounds(V, s, d, w, rounds=3, batch=2000, seed=5)
+
+
+def test_traversals_rmat_hints_one():
+    V = 1 << 12
+    s, d, w = mk.gen_rmat(12, 40000, seed=22, w_lo=1, w_hi=1000)
+    _traversal_rounds(V, s, d, w, rounds=2, batch=1000, seed=6, hints="ones")
+
+
+def test_traversals_grid_high_diameter():
+    side = 64
+    s, d, w = mk.gen_grid(side, 80, seed=7, w_lo=1, w_hi=1000)
+    _traversal_rounds(side * side, s, d, w, rounds=3, batch=600, seed=7)
+
+
+def test_incremental_with_stale_batch_entries():
+    """Batch entries that did not change the graph (already present with a
+    different weight, self loops) must not seed distances."""
+    V = 6
+    G, O = make_pair(V, np.array([0, 1, 2], np.uint32), np.array([1, 2, 3], np.uint32),
+                     np.array([10, 10, 10], np.uint32), weighted=True)
+    sssp = mk.SSSP(G, 0, V)
+    sssp.Static()
+    bs = np.array([0, 0, 4, 3], np.uint32)
+    bd = np.array([2, 1, 4, 5], np.uint32)
+    bw = np.array([3, 1, 1, 1], np.uint32)  # (0,1) already live with weight 10
+    tbs, tbd, tbw = to_dev(bs), to_dev(bd), to_dev(bw)
+    G.InsertEdges(tbs, tbd, vals=tbw)
+    assert G.sync() == 0
+    O.insert(bs, bd, bw)
+    sssp.Incremental(tbs, tbd, wgt=tbw)
+    np.testing.assert_array_equal(sssp.Distances(), O.sssp(0))
+
+
+def test_pagerank_static_and_dynamic():
+    V = 1 << 13
+    s, d, _ = mk.gen_rmat(13, 80000, seed=31)
+    G, O = make_pair(V, s, d, reverse=True)
+    Of = OracleGraph(V)
+    Of.insert(s, d)
+    pr = mk.PageRank(G, 0.85, 1e-6, V, out_degree=np.bincount(s, minlength=V), max_iter=1000)
+    pr.Static()
+    ref, _ = Of.pagerank(0.85, 1e-14)
+    assert np.abs(pr.Values().astype(np.float64) - ref).sum() <= PR_L1_TOL
+    es = mk.EdgeSet(V, s, d)
+    for r in range(2):
+        ds, dd = es.sample_present(3000, seed=40 + r)
+        tds, tdd = to_dev(ds), to_dev(dd)
+        G.DeleteEdges(tds, tdd)
+        Of.delete(ds, dd)
+        pr.Decremental(tds, tdd)
+        ref, _ = Of.pagerank(0.85, 1e-14)
+        assert np.abs(pr.Values().astype(np.float64) - ref).sum() <= PR_L1_TOL
+        is_, id_ = es.sample_absent(3000, seed=50 + r)
+        tis, tid = to_dev(is_), to_dev(id_)
+        G.InsertEdges(tis, tid)
+        Of.insert(is_, id_)
+        pr.Incremental(tis, tid)
+        ref, _ = Of.pagerank(0.85, 1e-14)
+        assert np.abs(pr.Values().astype(np.float64) - ref).sum() <= PR_L1_TOL
+    # out-degrees counted from the graph when none are given
+    pr2 = mk.PageRank(G, 0.85, 1e-6, V, max_iter=1000)
+    pr2.Static()
+    assert np.abs(pr2.Values().astype(np.float64) - ref).sum() <= PR_L1_TOL
+
+
+def _sym_batch(s, d):
+    return (np.concatenate([s, d]).astype(np.uint32), np.concatenate([d, s]).astype(np.uint32))
+
+
+@pytest.mark.parametrize("scale,edges", [(11, 30000), (13, 120000)])
+def test_triangles_static_and_dynamic(scale, edges):
+    V = 1 << scale
+    s, d, _ = mk.gen_rmat(scale, edges, seed=61)
+    ss, sd = symmetrise(s, d)
+    G, O = make_pair(V, ss, sd)
+    tc = mk.TC(G, V)
+    tc.Static()
+    assert tc.GetCount() == O.triangles()
+    es = mk.EdgeSet(V, ss, sd)
+    rng = np.random.default_rng(62)
+    for r in range(3):
+        # delete undirected edges (both directions)
+        ds, dd = es.sample_present(1500, seed=70 + r)
+        keep = ds < dd
+        us, ud = ds[keep], dd[keep]
+        bs, bd = _sym_batch(us, ud)
+        tbs, tbd = to_dev(bs), to_dev(bd)
+        G.DeleteEdges(tbs, tbd)
+        O.delete(bs, bd)
+        tc.Decremental(tbs, tbd)
+        assert tc.GetCount() == O.triangles()
+        # insert undirected edges, some closing triangles around hubs
+        hs = rng.integers(0, 64, 800).astype(np.uint32)
+        hd = rng.integers(0, V, 800).astype(np.uint32)
+        bs, bd = _sym_batch(hs, hd)
+        tbs, tbd = to_dev(bs), to_dev(bd)
+        G.InsertEdges(tbs, tbd)
+        O.insert(bs, bd)
+        tc.Incremental(tbs, tbd)
+        assert tc.GetCount() == O.triangles()
+
+
+def test_wcc_static_and_dynamic():
+    V = 1 << 12
+    s, d, _ = mk.gen_rmat(12, 6000, seed=81)  # sparse: many components
+    G, O = make_pair(V, s, d)
+    wcc = mk.WCC(G)
+    wcc.Static()
+    np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+    es = mk.EdgeSet(V, s, d)
+    for r in range(3):
+        ds, dd = es.sample_present(1500, seed=90 + r)
+        tds, tdd = to_dev(ds), to_dev(dd)
+        G.DeleteEdges(tds, tdd)
+        O.delete(ds, dd)
+        wcc.Decremental(tds, tdd)
+        np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+        is_, id_ = es.sample_absent(800, seed=95 + r)
+        tis, tid = to_dev(is_), to_dev(id_)
+        G.InsertEdges(tis, tid)
+        O.insert(is_, id_)
+        wcc.Incremental(tis, tid)
+        np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+
+
+def test_algorithms_with_a_foreign_batch_fall_back_to_recompute():
+    """Dynamic calls whose batch is not the graph's last update recompute."""
+    V = 1 << 10
+    s, d, _ = mk.gen_rmat(10, 6000, seed=3)
+    G, O = make_pair(V, s, d)
+    wcc = mk.WCC(G)
+    wcc.Static()
+    es = mk.EdgeSet(V, s, d)
+    ds, dd = es.sample_present(500, seed=4)
+    G.DeleteEdges(to_dev(ds), to_dev(dd))
+    O.delete(ds, dd)
+    wcc.Decremental(to_dev(ds), to_dev(dd))  # fresh tensors: different pointers
+    np.testing.assert_array_equal(wcc.Labels(), O.wcc())
