@@ -26,9 +26,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -39,9 +37,9 @@ sys.path.insert(0, str(ROOT))
 
 SEED = 0x4D45524B + 1  # large config
 METRIC = "edge updates/s"
-HALF = 500_000
+HALF = 500_000          # sub-batch size (delete, then insert)
 SCALE = 22
-EDGES = 67_108_864
+EDGES = 67_108_864      # 16 * 2^22
 W_LO, W_HI = 1, 1000
 # algorithmic bytes per applied edge (record + one 128-B slab probe + entry write)
 INS_BYTES = 12 + 128 + 8
@@ -77,44 +75,61 @@ def profile_traffic():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled through NVML by a polling thread
+    for the whole timed region (reads only; no GPU setting is changed)."""
+
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, gpu_index: int):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        import threading
+        self.samples = []
+        self.stop_flag = threading.Event()
+        self.t = None
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as N
+            N.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[gpu_index]) if vis and vis.split(",")[0].isdigit() else gpu_index
+            self.N, self.h = N, N.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM)
+        except Exception as ex:  # no NVML: report nothing rather than guess
+            log(f"[bench] NVML unavailable: {ex}")
+            self.N = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def _sample(self):
+        N = self.N
+        sm = N.nvmlDeviceGetClockInfo(self.h, N.NVML_CLOCK_SM)
+        try:
+            r = N.nvmlDeviceGetCurrentClocksEventReasons(self.h)
         except Exception:
-            self.p = None
+            r = N.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+        self.samples.append((time.perf_counter(), sm, r))
+
+    def _run(self):
+        while not self.stop_flag.is_set():
+            try:
+                self._sample()
+            except Exception:
+                break
 
     def stop(self):
-        if self.p is None:
+        if self.N is None:
             return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        self.f.flush()
-        rows = []
-        for line in Path(self.f.name).read_text().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        os.unlink(self.f.name)
-        if not rows:
+        self.stop_flag.set()
+        self.t.join(timeout=5)
+        if not self.samples:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
-                          and "Not" not in r[5 + i]})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+        names = [k for k, attr in self.REASONS.items()
+                 if any(r & getattr(self.N, attr, 0) for _, _, r in self.samples)]
+        sm = [x for _, x, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(names), "samples": len(sm), "source": "nvml"}
 
 
 def make_workload(n_batches: int):
@@ -154,8 +169,8 @@ def cpu_baseline(graph, batches, max_batches=3):
         applied += n1 + n2
     total = sum(times)
     return {"value": applied / total, "unit": METRIC, "cores": T, "kind": "port",
-            "sample": f"{len(times)} mixed batches of {2 * HALF} edges on the full R-MAT s22 "
-                      f"graph (hash-set adjacency, one shard per thread)",
+            "sample": f"{len(times)} mixed batches of {2 * HALF} edges on the full R-MAT "
+                      f"s{SCALE} graph (hash-set adjacency, one shard per thread)",
             "seconds": total}
 
 
@@ -208,9 +223,10 @@ def run_reference(args, rank, world):
 
 
 def config_block(n):
-    return {"workload": "rmat22_mixed_1M", "graph": "R-MAT scale 22, 67108864 directed edges, "
-            "a/b/c/d .57/.19/.19/.05, weights U[1,1000]", "batch": "500000 deletes of present "
-            "edges then 500000 inserts of absent edges", "load_factor": 0.7,
+    name = "rmat22_mixed_1M" if (SCALE, HALF) == (22, 500_000) else f"rmat{SCALE}_mixed_{2 * HALF}"
+    return {"workload": name, "graph": f"R-MAT scale {SCALE}, {EDGES} directed edges, "
+            "a/b/c/d .57/.19/.19/.05, weights U[1,1000]", "batch": f"{HALF} deletes of present "
+            f"edges then {HALF} inserts of absent edges", "load_factor": 0.7,
             "degree_hints": "exact", "l2": "inputs larger than L2 (slab pool ~2.5 GB, random "
             "bucket probes)", "parallelism": f"replicas x{n}" if n > 1 else "single GPU"}
 
@@ -218,12 +234,17 @@ def config_block(n):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--algo-batches", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=int, default=22,
+                    help="R-MAT scale (22 = the benchmark config; smaller only for profiling)")
+    ap.add_argument("--batch", type=int, default=500_000, help="edges per sub-batch")
     args = ap.parse_args()
+    global SCALE, EDGES, HALF
+    SCALE, EDGES, HALF = args.scale, 16 << args.scale, args.batch
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         return run_reference(args, rank, world)

@@ -181,7 +181,8 @@ class DynamicGraph:
         col_h = col.cpu().numpy().view(np.uint32)[:E]
         w_h = w.cpu().numpy().view(np.uint32)[:E] if w is not None else None
         if sort_rows:
-            rows = np.repeat(np.arange(self.num_vertices, dtype=np.uint64), np.diff(rp_h))
+            rows = np.repeat(np.arange(self.num_vertices, dtype=np.int64),
+                             np.diff(rp_h).astype(np.int64))
             order = np.lexsort((col_h, rows))
             col_h = col_h[order]
             if w_h is not None:

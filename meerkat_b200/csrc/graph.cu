@@ -254,169 +254,228 @@ __device__ __forceinline__ bool dedupe_is_first(const unsigned long long *keys,
   return false;
 }
 
-template <bool kWeighted, bool kDedupe>
-__global__ void __launch_bounds__(kUpdBlock)
-    k_insert(GraphView g, const uint32_t *__restrict__ src,
-             const uint32_t *__restrict__ dst, const uint32_t *__restrict__ w,
-             uint32_t n, const unsigned long long *__restrict__ dd_keys,
-             const uint32_t *__restrict__ dd_idx, uint32_t dd_mask,
-             uint8_t *__restrict__ applied, unsigned long long *count) {
-  __shared__ uint32_t blk_count;
-  if (threadIdx.x == 0) blk_count = 0;
-  __syncthreads();
-  const Lanes L = lanes();
-  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  uint32_t mine = 0;
-  for (uint32_t e = group; e < n; e += ngroups) {
-    uint32_t u = src[e], v = dst[e];
-    uint32_t wt = (kWeighted && w) ? w[e] : 0u;
-    if (g.reverse) {
-      uint32_t t = u;
-      u = v;
-      v = t;
-    }
-    uint8_t app = 0;
-    bool ok = (u != v);
-    if (u >= g.V || v >= g.V) {
-      ok = false;
-      if (L.gl == 0) atomicOr(g.err, kErrInvalidId);
-    }
-    if (kDedupe && ok) ok = dedupe_is_first(dd_keys, dd_idx, dd_mask, u, v, e);
-    if (ok) {
-      const uint32_t b0 = g.boff[u];
-      const uint32_t nb = g.boff[u + 1] - b0;
-      uint32_t s = b0 + bucket_of(v, nb);
-      uint32_t it = 0;
-      for (; it < kProbeLimit; ++it) {
-        uint4 q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
-        bool found;
-        uint32_t fslot, eslot, next;
-        probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
-        if (found) break;
-        if (eslot != 255) {
-          uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(eslot);
-          uint32_t old = 0;
-          if (L.gl == 0) {
-            old = atomicCAS(wp, kEmptyKey, v);
-            if (kWeighted && old == kEmptyKey) wp[1] = wt;
-          }
-          old = __shfl_sync(L.gmask, old, L.gbase);
-          if (old == kEmptyKey) {
-            app = 1;
-            break;
-          }
-          if (old == v) break;
-          continue;  // lost the word to another key: re-read this slab
-        }
-        if (next != kNoSlab) {
-          s = next;
-          continue;
-        }
-        // chain is full: take a pool slab holding the key, then link it.
-        uint32_t res = 0;  // 0 = pool exhausted, 1 = linked, 2 = lost the link race
-        uint32_t other = kNoSlab;
-        if (L.gl == 0) {
-          uint32_t ns = atomicAdd(g.pool_top, 1u);
-          if (ns >= g.pool_cap) {
-            atomicOr(g.err, kErrOom);
-            res = 0;
-          } else {
-            uint32_t *np = reinterpret_cast<uint32_t *>(g.slabs + 8ull * ns);
-            np[0] = v;
-            if (kWeighted) np[1] = wt;
-            __threadfence();
-            uint32_t *nextp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + 31;
-            uint32_t prev = atomicCAS(nextp, kNoSlab, ns);
-            if (prev == kNoSlab) {
-              res = 1;
-            } else {
-              res = 2;
-              other = prev;
-              np[0] = kEmptyKey;  // slab stays unreachable
-            }
-          }
-        }
-        res = __shfl_sync(L.gmask, res, L.gbase);
-        other = __shfl_sync(L.gmask, other, L.gbase);
-        if (res == 0) break;
-        if (res == 1) {
-          app = 1;
-          break;
-        }
-        s = other;
+// Inserts key v into the chain starting at slab s whose first slab is
+// already loaded in q (possibly stale).  Returns 1 when this group stored the
+// key.  Group-cooperative; every lane of the group calls it.
+template <bool kWeighted>
+__device__ __forceinline__ uint32_t insert_chain(const GraphView &g, const Lanes &L, uint32_t s,
+                                                 uint4 q, uint32_t v, uint32_t wt) {
+  for (uint32_t it = 0; it < kProbeLimit; ++it) {
+    if (it) q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
+    bool found;
+    uint32_t fslot, eslot, next;
+    probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
+    if (found) return 0;
+    if (eslot != 255) {
+      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(eslot);
+      uint32_t old = 0;
+      if (L.gl == 0) {
+        old = atomicCAS(wp, kEmptyKey, v);
+        if (kWeighted && old == kEmptyKey) wp[1] = wt;
       }
-      if (it >= kProbeLimit && L.gl == 0) atomicOr(g.err, kErrTimeout);
+      old = __shfl_sync(L.gmask, old, L.gbase);
+      if (old == kEmptyKey) return 1;
+      if (old == v) return 0;
+      continue;  // lost the word to another key: re-read this slab
     }
+    if (next == kLinkBusy) {  // another group is extending this chain
+      __nanosleep(64);
+      continue;
+    }
+    if (next != kNoSlab) {
+      s = next;
+      continue;
+    }
+    // Chain is full: claim its next word, take a pool slab holding the key,
+    // then publish the link.  Racing groups see kLinkBusy and wait, so no slab
+    // is ever allocated and dropped.
+    uint32_t res = 0;  // 0 = retry, 1 = inserted, 2 = pool exhausted
     if (L.gl == 0) {
-      applied[e] = app;
-      if (app) {
-        atomicAdd(g.deg + u, 1u);
-        ++mine;
+      uint32_t *nextp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + 31;
+      uint32_t prev = atomicCAS(nextp, kNoSlab, kLinkBusy);
+      if (prev == kNoSlab) {
+        uint32_t ns = atomicAdd(g.pool_top, 1u);
+        if (ns >= g.pool_cap) {
+          atomicOr(g.err, kErrOom);
+          atomicExch(nextp, kNoSlab);
+          res = 2;
+        } else {
+          uint32_t *np = reinterpret_cast<uint32_t *>(g.slabs + 8ull * ns);
+          np[0] = v;
+          if (kWeighted) np[1] = wt;
+          __threadfence();
+          atomicExch(nextp, ns);
+          res = 1;
+        }
       }
     }
+    res = __shfl_sync(L.gmask, res, L.gbase);
+    if (res == 2) return 0;
+    if (res == 1) return 1;
   }
-  if (mine) atomicAdd(&blk_count, mine);
-  __syncthreads();
-  if (threadIdx.x == 0 && blk_count) atomicAdd(count, (unsigned long long)blk_count);
+  if (L.gl == 0) atomicOr(g.err, kErrTimeout);
+  return 0;
 }
 
+// Tombstones key v in the chain starting at s (first slab preloaded in q).
 template <bool kWeighted>
-__global__ void __launch_bounds__(kUpdBlock)
-    k_delete(GraphView g, const uint32_t *__restrict__ src,
-             const uint32_t *__restrict__ dst, uint32_t n,
-             uint8_t *__restrict__ applied, unsigned long long *count) {
+__device__ __forceinline__ uint32_t delete_chain(const GraphView &g, const Lanes &L, uint32_t s,
+                                                 uint4 q, uint32_t v) {
+  for (uint32_t it = 0; it < kProbeLimit; ++it) {
+    if (it) q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
+    bool found;
+    uint32_t fslot, eslot, next;
+    probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
+    if (found) {
+      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(fslot);
+      uint32_t old = 0;
+      if (L.gl == 0) old = atomicCAS(wp, v, kTombKey);
+      old = __shfl_sync(L.gmask, old, L.gbase);
+      return old == v ? 1u : 0u;
+    }
+    if (next == kNoSlab) return 0;
+    s = next;
+  }
+  if (L.gl == 0) atomicOr(g.err, kErrTimeout);
+  return 0;
+}
+
+// Update kernels.  A warp takes 32 batch edges:
+//   1. every lane resolves its edge to the bucket's head slab;
+//   2. the warp issues all 32 head-slab loads (8 rounds x 4 groups, 16 B per
+//      lane) before using any of them;
+//   3. each group analyses its 8 slabs (redux.sync) and hands every decision
+//      to the lane that owns the edge;
+//   4. the owning lanes issue their CASes together (one warp instruction,
+//      32 independent atomics in flight);
+//   5. the rare edges whose CAS lost a race, whose chain continues or needs a
+//      new slab fall back to the group-cooperative chain walk.
+// A prefetched slab that went stale only costs the slow path: inside one
+// insert call key words only ever move EMPTY -> key, and inside one delete
+// call only key -> TOMBSTONE.
+constexpr int kRounds = 8;
+constexpr uint32_t kActNoop = 0x100;  // key already present (insert) / absent (delete)
+constexpr uint32_t kActSlow = 0x200;  // needs the chain walk
+constexpr uint32_t kActSkip = 0x300;  // lane has no edge
+
+template <bool kWeighted, bool kDedupe, bool kInsert>
+__global__ void __launch_bounds__(kUpdBlock, 4)
+    k_update(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+             const uint32_t *__restrict__ w, uint32_t n,
+             const unsigned long long *__restrict__ dd_keys, const uint32_t *__restrict__ dd_idx,
+             uint32_t dd_mask, uint8_t *__restrict__ applied, unsigned long long *count) {
   __shared__ uint32_t blk_count;
   if (threadIdx.x == 0) blk_count = 0;
   __syncthreads();
   const Lanes L = lanes();
-  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t mine = 0;
-  for (uint32_t e = group; e < n; e += ngroups) {
-    uint32_t u = src[e], v = dst[e];
-    if (g.reverse) {
-      uint32_t t = u;
-      u = v;
-      v = t;
+  for (uint64_t base = (uint64_t)warp * 32; base < n; base += (uint64_t)nwarps * 32) {
+    // 1. resolve the lane's edge
+    const uint64_t e = base + L.lane;
+    uint32_t u = 0, v = 0, wt = 0, head = kNoSlab;
+    if (e < n) {
+      u = src[e];
+      v = dst[e];
+      if (kWeighted && kInsert && w) wt = w[e];
+      if (g.reverse) {
+        uint32_t t = u;
+        u = v;
+        v = t;
+      }
+      bool ok = (u != v);
+      if (u >= g.V || v >= g.V) {
+        ok = false;
+        atomicOr(g.err, kErrInvalidId);
+      }
+      if (kDedupe && ok) ok = dedupe_is_first(dd_keys, dd_idx, dd_mask, u, v, (uint32_t)e);
+      if (ok) {
+        const uint32_t b0 = g.boff[u];
+        head = b0 + bucket_of(v, g.boff[u + 1] - b0);
+      } else {
+        applied[e] = 0;
+      }
     }
-    uint8_t app = 0;
-    bool ok = (u != v);
-    if (u >= g.V || v >= g.V) {
-      ok = false;
-      if (L.gl == 0) atomicOr(g.err, kErrInvalidId);
+    // 2. all head slabs in flight
+    uint4 q[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      const uint32_t hs = __shfl_sync(0xFFFFFFFFu, head, 4 * r + L.grp);
+      if (hs != kNoSlab) q[r] = ld_slab_cg(g.slabs + 8ull * hs + L.gl);
     }
-    if (ok) {
-      const uint32_t b0 = g.boff[u];
-      const uint32_t nb = g.boff[u + 1] - b0;
-      uint32_t s = b0 + bucket_of(v, nb);
-      uint32_t it = 0;
-      for (; it < kProbeLimit && s != kNoSlab; ++it) {
-        uint4 q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
+    // 3. per-round decisions, delivered to the owning lanes
+    uint32_t my_act = kActSkip;
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      const uint32_t sl = 4 * r + L.grp;
+      const uint32_t hs = __shfl_sync(0xFFFFFFFFu, head, sl);
+      const uint32_t vv = __shfl_sync(0xFFFFFFFFu, v, sl);
+      uint32_t act = kActSkip;
+      if (hs != kNoSlab) {
         bool found;
         uint32_t fslot, eslot, next;
-        probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
-        if (found) {
-          uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(fslot);
-          uint32_t old = 0;
-          if (L.gl == 0) old = atomicCAS(wp, v, kTombKey);
-          old = __shfl_sync(L.gmask, old, L.gbase);
-          app = (old == v);
-          break;
-        }
-        s = next;
+        probe_slab<kWeighted>(q[r], vv, L, found, fslot, eslot, next);
+        if (kInsert)
+          act = found ? kActNoop : (eslot != 255 ? eslot : kActSlow);
+        else
+          act = found ? fslot : (next == kNoSlab ? kActNoop : kActSlow);
       }
-      if (it >= kProbeLimit && L.gl == 0) atomicOr(g.err, kErrTimeout);
+      // lane (4r + g) takes the decision of group g for round r
+      const uint32_t t = __shfl_sync(0xFFFFFFFFu, act, (L.lane & 3u) * 8u);
+      if ((L.lane >> 2) == (uint32_t)r) my_act = t;
     }
-    if (L.gl == 0) {
-      applied[e] = app;
+    // 4. one CAS per owning lane, all issued together
+    uint32_t app = 0;
+    bool slow = (my_act == kActSlow);
+    if (my_act < 255) {
+      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * head) + slot_word<kWeighted>(my_act);
+      if (kInsert) {
+        const uint32_t old = atomicCAS(wp, kEmptyKey, v);
+        if (old == kEmptyKey) {
+          app = 1;
+          if (kWeighted) wp[1] = wt;
+        } else if (old != v) {
+          slow = true;  // lost the word to another key
+        }
+      } else {
+        app = (atomicCAS(wp, v, kTombKey) == v) ? 1u : 0u;
+      }
+    }
+    // 5. slow path, round by round, group-cooperative
+    const uint32_t slow_mask = __ballot_sync(0xFFFFFFFFu, slow);
+    if (slow_mask) {
+#pragma unroll 1
+      for (int r = 0; r < kRounds; ++r) {
+        const uint32_t sl = 4 * r + L.grp;
+        const uint32_t hs = __shfl_sync(0xFFFFFFFFu, head, sl);
+        const uint32_t vv = __shfl_sync(0xFFFFFFFFu, v, sl);
+        const uint32_t ww = __shfl_sync(0xFFFFFFFFu, wt, sl);
+        uint32_t res = 0;
+        if ((slow_mask >> sl) & 1u) {
+          const uint4 q0 = ld_slab_cg(g.slabs + 8ull * hs + L.gl);
+          res = kInsert ? insert_chain<kWeighted>(g, L, hs, q0, vv, ww)
+                        : delete_chain<kWeighted>(g, L, hs, q0, vv);
+        }
+        __syncwarp();
+        const uint32_t t = __shfl_sync(0xFFFFFFFFu, res, (L.lane & 3u) * 8u);
+        if ((L.lane >> 2) == (uint32_t)r && slow) app = t;
+      }
+    }
+    // owning lane publishes the outcome
+    if (head != kNoSlab) {
+      applied[e] = (uint8_t)app;
       if (app) {
-        atomicSub(g.deg + u, 1u);
+        if (kInsert)
+          atomicAdd(g.deg + u, 1u);
+        else
+          atomicSub(g.deg + u, 1u);
         ++mine;
       }
     }
   }
-  if (mine) atomicAdd(&blk_count, mine);
+  mine = __reduce_add_sync(0xFFFFFFFFu, mine);
+  if (L.lane == 0 && mine) atomicAdd(&blk_count, mine);
   __syncthreads();
   if (threadIdx.x == 0 && blk_count) atomicAdd(count, (unsigned long long)blk_count);
 }
@@ -490,81 +549,106 @@ __device__ __forceinline__ void lane_counts(const uint4 &q, uint32_t gl,
   }
 }
 
+// Live keys per bucket (group per bucket: balanced under degree skew).
+template <bool kWeighted>
+__global__ void k_bucket_live(GraphView g, uint32_t *__restrict__ bcnt) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    uint32_t c = 0;
+    walk_bucket(g, L, b, [&](const uint4 &q) {
+      uint32_t live, tomb;
+      lane_counts<kWeighted>(q, L.gl, live, tomb);
+      c += live;
+    });
+    c = __reduce_add_sync(L.gmask, c);
+    if (L.gl == 0) bcnt[b] = c;
+  }
+}
+
 template <bool kWeighted>
 __global__ void k_count_tombstones(GraphView g, uint32_t *__restrict__ out) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t u = group; u < g.V; u += ngroups) {
-    uint32_t tomb_total = 0;
-    for (uint32_t b = g.boff[u]; b < g.boff[u + 1]; ++b) {
-      uint32_t s = b;
-      while (s != kNoSlab) {
-        uint4 q = ld_slab_ro(g.slabs + 8ull * s + L.gl);
-        uint32_t live, tomb;
-        lane_counts<kWeighted>(q, L.gl, live, tomb);
-        tomb_total += __reduce_add_sync(L.gmask, tomb);
-        s = __shfl_sync(L.gmask, q.w, L.gbase + 7);
-      }
-    }
-    if (L.gl == 0) out[u] = tomb_total;
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    uint32_t t = 0;
+    walk_bucket(g, L, b, [&](const uint4 &q) {
+      uint32_t live, tomb;
+      lane_counts<kWeighted>(q, L.gl, live, tomb);
+      t += tomb;
+    });
+    t = __reduce_add_sync(L.gmask, t);
+    if (L.gl == 0 && t) atomicAdd(out + g.bowner[b], t);
   }
 }
 
+// row_ptr[u] = bucket position of u's first bucket.
+__global__ void k_rows_from_buckets(const uint32_t *__restrict__ boff, uint32_t V, uint32_t nb,
+                                    const unsigned long long *__restrict__ bpos,
+                                    unsigned long long *__restrict__ row_ptr) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= V; u += gridDim.x * blockDim.x)
+    row_ptr[u] = bpos[u < V ? boff[u] : nb];
+}
+
+// Writes the live keys of every bucket at its scanned position.
 template <bool kWeighted>
-__global__ void k_export_csr(GraphView g, const unsigned long long *__restrict__ row_ptr,
-                             uint32_t *__restrict__ col, uint32_t *__restrict__ wout) {
+__global__ void k_bucket_fill(GraphView g, const unsigned long long *__restrict__ bpos,
+                              uint32_t *__restrict__ col, uint32_t *__restrict__ wout) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t u = group; u < g.V; u += ngroups) {
-    unsigned long long pos = row_ptr[u];
-    const unsigned long long end = row_ptr[u + 1];
-    for (uint32_t b = g.boff[u]; b < g.boff[u + 1]; ++b) {
-      uint32_t s = b;
-      while (s != kNoSlab) {
-        uint4 q = ld_slab_ro(g.slabs + 8ull * s + L.gl);
-        uint32_t live, tomb;
-        lane_counts<kWeighted>(q, L.gl, live, tomb);
-        // exclusive prefix over the 8 lanes
-        uint32_t incl = live;
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    unsigned long long pos = bpos[b];
+    const unsigned long long end = bpos[b + 1];
+    walk_bucket(g, L, b, [&](const uint4 &q) {
+      uint32_t live, tomb;
+      lane_counts<kWeighted>(q, L.gl, live, tomb);
+      uint32_t incl = live;
 #pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
-          uint32_t y = __shfl_up_sync(L.gmask, incl, o, 8);
-          if (L.gl >= (uint32_t)o) incl += y;
-        }
-        uint32_t total = __shfl_sync(L.gmask, incl, L.gbase + 7);
-        unsigned long long p = pos + (incl - live);
-        auto put = [&](uint32_t k, uint32_t val) {
-          if (k < kTombKey) {
-            if (p < end) {
-              col[p] = k;
-              if (wout) wout[p] = val;
-            }
-            ++p;
-          }
-        };
-        if (!kWeighted) {
-          put(q.x, 0);
-          put(q.y, 0);
-          put(q.z, 0);
-          if (L.gl != 7) put(q.w, 0);
-        } else {
-          put(q.x, q.y);
-          if (L.gl != 7) put(q.z, q.w);
-        }
-        pos += total;
-        s = __shfl_sync(L.gmask, q.w, L.gbase + 7);
+      for (int o = 1; o < 8; o <<= 1) {
+        uint32_t y = __shfl_up_sync(L.gmask, incl, o, 8);
+        if (L.gl >= (uint32_t)o) incl += y;
       }
-    }
+      uint32_t total = __shfl_sync(L.gmask, incl, L.gbase + 7);
+      unsigned long long p = pos + (incl - live);
+      auto put = [&](uint32_t k, uint32_t val) {
+        if (k < kTombKey) {
+          if (p < end) {
+            col[p] = k;
+            if (wout) wout[p] = val;
+          }
+          ++p;
+        }
+      };
+      if (!kWeighted) {
+        put(q.x, 0);
+        put(q.y, 0);
+        put(q.z, 0);
+        if (L.gl != 7) put(q.w, 0);
+      } else {
+        put(q.x, q.y);
+        if (L.gl != 7) put(q.z, q.w);
+      }
+      pos += total;
+    });
   }
 }
 
 static int update_grid(uint32_t n, int device) {
-  // 8 lanes per edge; enough resident groups to cover HBM latency.
-  uint64_t groups_needed = (uint64_t)n;
-  uint64_t blocks = (groups_needed * 8 + kUpdBlock - 1) / kUpdBlock;
-  uint64_t cap = (uint64_t)device_sm_count(device) * 8;  // 8 x 256 threads per SM
+  // one warp per 32 edges, capped at the resident block count
+  uint64_t blocks = ((uint64_t)n + kUpdBlock - 1) / kUpdBlock;
+  uint64_t cap = (uint64_t)device_sm_count(device) * 8;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+static int group_grid(uint32_t n, int device) {
+  // 8 lanes per item
+  uint64_t blocks = ((uint64_t)n * 8 + kUpdBlock - 1) / kUpdBlock;
+  uint64_t cap = (uint64_t)device_sm_count(device) * 8;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   return (int)blocks;
@@ -641,11 +725,13 @@ mk_status mk_graph_create(const mk_graph_desc *desc, mk_graph **out) {
     return cleanup(MK_ERR_OOM, "cudaMalloc(bucket offsets)", e);
   if ((e = cudaMalloc(&g->deg, (size_t)V * 4)) != cudaSuccess)
     return cleanup(MK_ERR_OOM, "cudaMalloc(degrees)", e);
+  if ((e = cudaMalloc(&g->bowner, total * 4)) != cudaSuccess)
+    return cleanup(MK_ERR_OOM, "cudaMalloc(bucket owners)", e);
   if ((e = cudaMalloc(&g->pool_top, 4 * sizeof(uint32_t))) != cudaSuccess)
     return cleanup(MK_ERR_OOM, "cudaMalloc(pool counter)", e);
   if ((e = cudaMalloc(&g->counters, 4 * sizeof(unsigned long long))) != cudaSuccess)
     return cleanup(MK_ERR_OOM, "cudaMalloc(counters)", e);
-  g->device_bytes = g->pool_cap * 128ull + ((size_t)V + 1) * 4 + (size_t)V * 4 + 16 + 32;
+  g->device_bytes = g->pool_cap * 128ull + ((size_t)V + 1) * 4 + (size_t)V * 4 + total * 4 + 48;
   if ((e = cudaMemset(g->slabs, 0xFF, g->pool_cap * 128ull)) != cudaSuccess)
     return cleanup(MK_ERR_CUDA, "cudaMemset(slabs)", e);
   if ((e = cudaMemcpy(g->boff, g->h_boff.data(), ((size_t)V + 1) * 4,
@@ -653,6 +739,13 @@ mk_status mk_graph_create(const mk_graph_desc *desc, mk_graph **out) {
     return cleanup(MK_ERR_CUDA, "cudaMemcpy(bucket offsets)", e);
   if ((e = cudaMemset(g->deg, 0, (size_t)V * 4)) != cudaSuccess)
     return cleanup(MK_ERR_CUDA, "cudaMemset(degrees)", e);
+  {
+    std::vector<uint32_t> owner(total);
+    for (uint32_t i = 0; i < V; ++i)
+      for (uint32_t b = g->h_boff[i]; b < g->h_boff[i + 1]; ++b) owner[b] = i;
+    if ((e = cudaMemcpy(g->bowner, owner.data(), total * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cleanup(MK_ERR_CUDA, "cudaMemcpy(bucket owners)", e);
+  }
   uint32_t init[4] = {(uint32_t)total, 0u, 0u, 0u};
   if ((e = cudaMemcpy(g->pool_top, init, sizeof(init), cudaMemcpyHostToDevice)) != cudaSuccess)
     return cleanup(MK_ERR_CUDA, "cudaMemcpy(pool counter)", e);
@@ -670,12 +763,15 @@ mk_status mk_graph_destroy(mk_graph *g) {
   if (g->slabs) cudaFree(g->slabs);
   if (g->boff) cudaFree(g->boff);
   if (g->deg) cudaFree(g->deg);
+  if (g->bowner) cudaFree(g->bowner);
   if (g->pool_top) cudaFree(g->pool_top);
   if (g->counters) cudaFree(g->counters);
   g->applied.release();
   g->dd_keys.release();
   g->dd_idx.release();
   g->scan_tmp.release();
+  g->bucket_cnt.release();
+  g->bucket_pos.release();
   delete g;
   return MK_OK;
 }
@@ -727,11 +823,11 @@ mk_status mk_graph_insert_edges(mk_graph *g, const uint32_t *d_src,
     const uint32_t *kd = g->reverse ? d_src : d_dst;
     k_dedupe_elect<<<(n + 255) / 256, 256, 0, s>>>(v, ks, kd, n, g->dd_keys.ptr,
                                                    g->dd_idx.ptr, cap - 1);
-    k_insert<true, true><<<blocks, kUpdBlock, 0, s>>>(
+    k_update<true, true, true><<<blocks, kUpdBlock, 0, s>>>(
         v, d_src, d_dst, d_w, n, g->dd_keys.ptr, g->dd_idx.ptr, cap - 1,
         g->applied.ptr, g->counters);
   } else {
-    k_insert<false, false><<<blocks, kUpdBlock, 0, s>>>(
+    k_update<false, false, true><<<blocks, kUpdBlock, 0, s>>>(
         v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr,
         g->counters);
   }
@@ -751,9 +847,11 @@ mk_status mk_graph_delete_edges(mk_graph *g, const uint32_t *d_src,
   GraphView v = g->view();
   int blocks = update_grid(n, g->device);
   if (g->weighted)
-    k_delete<true><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, g->applied.ptr, g->counters);
+    k_update<true, false, false><<<blocks, kUpdBlock, 0, s>>>(
+        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
   else
-    k_delete<false><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, g->applied.ptr, g->counters);
+    k_update<false, false, false><<<blocks, kUpdBlock, 0, s>>>(
+        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
   MK_CUDA(cudaGetLastError());
   return MK_OK;
 }
@@ -767,7 +865,7 @@ mk_status mk_graph_search_edges(mk_graph *g, const uint32_t *d_src,
   DeviceGuard dg(g->device);
   cudaStream_t s = as_stream(stream);
   GraphView v = g->view();
-  int blocks = update_grid(n, g->device);
+  int blocks = group_grid(n, g->device);
   if (g->weighted)
     k_search<true><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, d_found, d_w);
   else
@@ -852,14 +950,22 @@ mk_status mk_graph_export_csr(mk_graph *g, uint64_t *d_row_ptr, uint32_t *d_col,
   if (!g || !d_row_ptr || !d_col) return fail(MK_ERR_INVALID, "mk_graph_export_csr: null argument");
   DeviceGuard dg(g->device);
   cudaStream_t s = as_stream(stream);
-  unsigned long long *rp = reinterpret_cast<unsigned long long *>(d_row_ptr);
-  MK_CHECK(scan_u32_to_u64(g->deg, rp, g->V, g->scan_tmp, s));
+  const uint32_t nb = (uint32_t)g->num_buckets;
+  MK_CHECK(g->bucket_cnt.reserve(nb, &g->device_bytes));
+  MK_CHECK(g->bucket_pos.reserve((size_t)nb + 1, &g->device_bytes));
   GraphView v = g->view();
-  int blocks = std::min<uint64_t>((uint64_t)g->V * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  int blocks = group_grid(nb, g->device);
   if (g->weighted)
-    k_export_csr<true><<<blocks, 256, 0, s>>>(v, rp, d_col, d_w);
+    k_bucket_live<true><<<blocks, 256, 0, s>>>(v, g->bucket_cnt.ptr);
   else
-    k_export_csr<false><<<blocks, 256, 0, s>>>(v, rp, d_col, nullptr);
+    k_bucket_live<false><<<blocks, 256, 0, s>>>(v, g->bucket_cnt.ptr);
+  MK_CHECK(scan_u32_to_u64(g->bucket_cnt.ptr, g->bucket_pos.ptr, nb, g->scan_tmp, s));
+  unsigned long long *rp = reinterpret_cast<unsigned long long *>(d_row_ptr);
+  k_rows_from_buckets<<<(g->V + 256) / 256, 256, 0, s>>>(g->boff, g->V, nb, g->bucket_pos.ptr, rp);
+  if (g->weighted)
+    k_bucket_fill<true><<<blocks, 256, 0, s>>>(v, g->bucket_pos.ptr, d_col, d_w);
+  else
+    k_bucket_fill<false><<<blocks, 256, 0, s>>>(v, g->bucket_pos.ptr, d_col, nullptr);
   MK_CUDA(cudaGetLastError());
   return MK_OK;
 }
@@ -868,8 +974,9 @@ mk_status mk_graph_count_tombstones(mk_graph *g, uint32_t *d_out, void *stream) 
   if (!g || !d_out) return fail(MK_ERR_INVALID, "mk_graph_count_tombstones: null argument");
   DeviceGuard dg(g->device);
   cudaStream_t s = as_stream(stream);
+  MK_CUDA(cudaMemsetAsync(d_out, 0, (size_t)g->V * 4, s));
   GraphView v = g->view();
-  int blocks = std::min<uint64_t>((uint64_t)g->V * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  int blocks = group_grid((uint32_t)g->num_buckets, g->device);
   if (g->weighted)
     k_count_tombstones<true><<<blocks, 256, 0, s>>>(v, d_out);
   else

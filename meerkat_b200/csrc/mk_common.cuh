@@ -27,6 +27,9 @@ namespace mk {
 constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
 constexpr uint32_t kTombKey = 0xFFFFFFFEu;
 constexpr uint32_t kNoSlab = 0xFFFFFFFFu;
+// Next-slab word while one insert group is linking a new slab (transient,
+// only ever seen inside the insert kernel).
+constexpr uint32_t kLinkBusy = 0xFFFFFFFEu;
 constexpr uint32_t kInf = 0xFFFFFFFFu;
 constexpr unsigned long long kInfInf = 0xFFFFFFFFFFFFFFFFull;
 
@@ -41,6 +44,8 @@ constexpr int kGroup = 8;  // lanes per slab probe (8 x 16 B = 128 B)
 struct GraphView {
   uint4 *slabs;           // slab s = slabs[8*s .. 8*s+7]
   const uint32_t *boff;   // bucket offsets, V+1 entries; head slab id = bucket
+  const uint32_t *bowner; // owning vertex of each bucket (nbuckets entries)
+  uint32_t nbuckets;
   uint32_t *deg;          // live out-degree (in-degree for reverse graphs)
   uint32_t *pool_top;     // next free overflow slab id (bump pointer)
   uint32_t *err;          // sticky MK_DEVERR_* bits

@@ -105,6 +105,7 @@ struct mk_graph {
   uint64_t pool_cap = 0;
   uint4 *slabs = nullptr;
   uint32_t *boff = nullptr;
+  uint32_t *bowner = nullptr;     // owning vertex of every bucket
   uint32_t *deg = nullptr;
   uint32_t *pool_top = nullptr;   // [0] bump pointer; [1] error word
   std::vector<uint32_t> h_boff;
@@ -114,6 +115,8 @@ struct mk_graph {
   mk::DevBuf<unsigned long long> dd_keys;  // weighted-insert dedupe table
   mk::DevBuf<uint32_t> dd_idx;
   mk::DevBuf<unsigned long long> scan_tmp;
+  mk::DevBuf<uint32_t> bucket_cnt;             // export / orientation scratch
+  mk::DevBuf<unsigned long long> bucket_pos;
   uint32_t last_n = 0;
   const uint32_t *last_src = nullptr;
   const uint32_t *last_dst = nullptr;
@@ -124,6 +127,8 @@ struct mk_graph {
     mk::GraphView v;
     v.slabs = slabs;
     v.boff = boff;
+    v.bowner = bowner;
+    v.nbuckets = static_cast<uint32_t>(num_buckets);
     v.deg = deg;
     v.pool_top = pool_top;
     v.err = pool_top + 1;

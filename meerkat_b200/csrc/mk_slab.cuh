@@ -122,4 +122,42 @@ __device__ __forceinline__ void walk_vertex(const GraphView &g, const Lanes &L,
   }
 }
 
+// Visits the slab chain of one bucket (head slab id = bucket index).
+template <class F>
+__device__ __forceinline__ void walk_bucket(const GraphView &g, const Lanes &L, uint32_t b,
+                                            F &&f) {
+  uint32_t s = b;
+  while (s != kNoSlab) {
+    uint4 q = ld_slab_ro(g.slabs + 8ull * s + L.gl);
+    f(q);
+    s = __shfl_sync(L.gmask, q.w, L.gbase + 7);
+  }
+}
+
+// Visits buckets [b0, b1) with the head slabs of up to 4 buckets loaded
+// together (independent loads in flight), then follows overflow chains.
+template <class F>
+__device__ __forceinline__ void walk_buckets(const GraphView &g, const Lanes &L, uint32_t b0,
+                                             uint32_t b1, F &&f) {
+  for (uint32_t b = b0; b < b1; b += 4) {
+    uint4 q[4];
+    const uint32_t n = min(4u, b1 - b);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if ((uint32_t)j < n) q[j] = ld_slab_ro(g.slabs + 8ull * (b + j) + L.gl);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if ((uint32_t)j < n) {
+        f(q[j]);
+        uint32_t s = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
+        while (s != kNoSlab) {
+          uint4 r = ld_slab_ro(g.slabs + 8ull * s + L.gl);
+          f(r);
+          s = __shfl_sync(L.gmask, r.w, L.gbase + 7);
+        }
+      }
+    }
+  }
+}
+
 }  // namespace mk

@@ -10,10 +10,12 @@
 //                 (PageRankImpl.cuh:222-251).
 //
 // B200 design: the whole solve is one cooperative launch.  Each iteration
-// is one pull pass (8-lane group per vertex, 16-byte slab loads, 4-byte
-// gathers of c[] which stays L2 resident) that also writes the next
-// contributions and accumulates |delta| and the dangling mass; one bounded
-// grid barrier separates iterations.  All sums are Kahan-compensated FP32 in
+// is one pull pass over fixed work items (chunks of up to 32 buckets of one
+// vertex, 8-lane group per item, 16-byte slab loads, 4-byte gathers of c[]
+// which stays L2 resident) that also writes the next contributions and
+// accumulates |delta| and the dangling mass.  A vertex with one item is
+// finished in that pass; hubs with several items combine the item partials
+// in a second, fixed-order pass.  Bounded grid barriers separate the passes.  All sums are Kahan-compensated FP32 in
 // a fixed order (per-lane, 8-lane butterfly, per-block tree, per-grid fixed
 // order), so a solve is deterministic for a given slab layout.
 //
@@ -58,6 +60,12 @@ enum PrCtl : int { kPBar0 = 0, kPBar1 = 1, kPErr = 2, kPIters = 3, kPCur = 4, kP
 
 struct PrArgs {
   GraphView g;       // reverse graph
+  const uint32_t *item_b0;   // first bucket of each work item (items of a vertex are contiguous)
+  const uint32_t *item_off;  // V+1: items of vertex u are [item_off[u], item_off[u+1])
+  const uint32_t *multi;     // vertices with more than one item
+  uint32_t nitems;
+  uint32_t nmulti;
+  float *ipart;      // per-item Kahan partials (s, c) = 2 * nitems
   float *pr0, *pr1;
   float *c0, *c1;
   const uint32_t *outdeg;
@@ -132,6 +140,25 @@ __device__ __forceinline__ float grid_total(const float *p) {
   return r;
 }
 
+constexpr uint32_t kPrChunk = 32;  // buckets per work item
+
+// Kahan sum of contributions over buckets [b0, b1) (group-cooperative).
+template <bool kW>
+__device__ __forceinline__ Kahan pull_range(const GraphView &g, const Lanes &L, uint32_t b0,
+                                            uint32_t b1, const float *__restrict__ c) {
+  Kahan acc;
+  walk_buckets(g, L, b0, b1, [&](const uint4 &q) {
+    uint32_t k[4], w[4];
+    lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+    for (int i = 0; i < keys_per_lane<kW>(); ++i)
+      if (k[i] < kTombKey) acc.add(__ldcg(c + k[i]));  // c is rewritten every iteration
+  });
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) acc.merge(shfl_xor_kahan(acc, L.gmask, o));
+  return acc;
+}
+
 template <bool kW>
 __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
   const Lanes L = lanes();
@@ -171,24 +198,45 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
     float *pnew = pr[cur ^ 1];
     float *cnew = cb[cur ^ 1];
     Kahan kd, kdang;
-    for (uint32_t u = group; u < V; u += ngroups) {
-      Kahan acc;
-      walk_vertex(a.g, L, u, [&](const uint4 &q) {
-        uint32_t k[4], w[4];
-        lane_keys<kW>(q, L.gl, k, w);
-#pragma unroll
-        for (int i = 0; i < keys_per_lane<kW>(); ++i)
-          if (k[i] < kTombKey) acc.add(__ldg(c + k[i]));
-      });
-#pragma unroll
-      for (int o = 4; o > 0; o >>= 1) acc.merge(shfl_xor_kahan(acc, L.gmask, o));
+    auto finalize = [&](uint32_t u, float sum) {  // lane 0 of a group
+      float nv = base + d * sum;
+      pnew[u] = nv;
+      kd.add(fabsf(nv - __ldcg(pold + u)));
+      uint32_t od = a.outdeg[u];
+      cnew[u] = od ? nv / (float)od : 0.0f;
+      if (!od) kdang.add(nv);
+    };
+    // pass A: every work item; a vertex with a single item is finished here
+    for (uint32_t i = group; i < a.nitems; i += ngroups) {
+      const uint32_t b0 = a.item_b0[i];
+      const uint32_t u = a.g.bowner[b0];
+      const uint32_t b1 = min(a.g.boff[u + 1], b0 + kPrChunk);
+      Kahan acc = pull_range<kW>(a.g, L, b0, b1, c);
       if (L.gl == 0) {
-        float nv = base + d * acc.value();
-        pnew[u] = nv;
-        kd.add(fabsf(nv - pold[u]));
-        uint32_t od = a.outdeg[u];
-        cnew[u] = od ? nv / (float)od : 0.0f;
-        if (!od) kdang.add(nv);
+        if (a.item_off[u + 1] - a.item_off[u] == 1) {
+          finalize(u, acc.value());
+        } else {
+          a.ipart[2 * i] = acc.s;
+          a.ipart[2 * i + 1] = acc.c;
+        }
+      }
+    }
+    if (a.nmulti) {
+      if (!grid_barrier(a.ctl + kPBar0, a.ctl + kPErr, a.limit_ns)) return;
+      // pass B: vertices with several items combine their partials in order
+      for (uint32_t m = group; m < a.nmulti; m += ngroups) {
+        const uint32_t u = a.multi[m];
+        const uint32_t i0 = a.item_off[u], i1 = a.item_off[u + 1];
+        Kahan acc;
+        for (uint32_t i = i0 + L.gl; i < i1; i += 8) {
+          Kahan t;
+          t.s = __ldcg(a.ipart + 2 * i);
+          t.c = __ldcg(a.ipart + 2 * i + 1);
+          acc.merge(t);
+        }
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) acc.merge(shfl_xor_kahan(acc, L.gmask, o));
+        if (L.gl == 0) finalize(u, acc.value());
       }
     }
     block_reduce2(kdang, kd, part(wp, 0), part(wp, 1));
@@ -212,14 +260,15 @@ __global__ void k_outdeg_adjust(const uint32_t *__restrict__ src, const uint8_t 
   if (e < n && applied[e]) atomicAdd(outdeg + src[e], (uint32_t)sign);
 }
 
-// out-degree from scratch: count every key of the reverse graph
+// out-degree from scratch: count every key of the reverse graph (one group
+// per bucket, balanced whatever the degree skew)
 template <bool kW>
 __global__ void k_outdeg_count(GraphView g, uint32_t *outdeg) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t u = group; u < g.V; u += ngroups) {
-    walk_vertex(g, L, u, [&](const uint4 &q) {
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    walk_bucket(g, L, b, [&](const uint4 &q) {
       uint32_t k[4], w[4];
       lane_keys<kW>(q, L.gl, k, w);
 #pragma unroll
@@ -245,6 +294,9 @@ struct mk_pagerank {
   uint32_t *outdeg = nullptr;
   float *part = nullptr;
   float *delta = nullptr;
+  uint32_t *item_b0 = nullptr, *item_off = nullptr, *multi = nullptr;
+  float *ipart = nullptr;
+  uint32_t nitems = 0, nmulti = 0;
   uint32_t *ctl = nullptr;
   uint32_t cur = 0;  // host mirror of the buffer with the latest ranks
   int nblocks = 0;
@@ -254,7 +306,7 @@ struct mk_pagerank {
 static mk_status pr_recount_outdeg(mk_pagerank *p, cudaStream_t s) {
   mk_graph *g = p->g;
   MK_CUDA(cudaMemsetAsync(p->outdeg, 0, (size_t)g->V * 4, s));
-  int blocks = std::min<uint64_t>((uint64_t)g->V * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  int blocks = std::min<uint64_t>(g->num_buckets * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
   if (g->weighted)
     k_outdeg_count<true><<<blocks, 256, 0, s>>>(g->view(), p->outdeg);
   else
@@ -274,6 +326,12 @@ static mk_status pr_solve(mk_pagerank *p, cudaStream_t s) {
   MK_CUDA(cudaMemsetAsync(p->ctl, 0, kPCtlWords * 4, s));
   PrArgs a;
   a.g = g->view();
+  a.item_b0 = p->item_b0;
+  a.item_off = p->item_off;
+  a.multi = p->multi;
+  a.nitems = p->nitems;
+  a.nmulti = p->nmulti;
+  a.ipart = p->ipart;
   a.pr0 = p->pr0;
   a.pr1 = p->pr1;
   a.c0 = p->c0;
@@ -324,6 +382,24 @@ mk_status mk_pagerank_create(mk_graph *g_rev, float damping, float tol,
   A((void **)&p->outdeg, V * 4);
   A((void **)&p->delta, 4);
   A((void **)&p->ctl, kPCtlWords * 4);
+  // fixed work items: chunks of kPrChunk buckets, contiguous per vertex
+  std::vector<uint32_t> ib0, ioff(V + 1), mul;
+  for (uint32_t u = 0; u < V; ++u) {
+    ioff[u] = (uint32_t)ib0.size();
+    const uint32_t lo = g_rev->h_boff[u], hi = g_rev->h_boff[u + 1];
+    for (uint32_t b = lo; b < hi; b += kPrChunk) ib0.push_back(b);
+    if (hi - lo > kPrChunk) mul.push_back(u);
+  }
+  ioff[V] = (uint32_t)ib0.size();
+  p->nitems = (uint32_t)ib0.size();
+  p->nmulti = (uint32_t)mul.size();
+  A((void **)&p->item_b0, ib0.size() * 4);
+  A((void **)&p->item_off, ioff.size() * 4);
+  A((void **)&p->multi, std::max<size_t>(mul.size(), 1) * 4);
+  A((void **)&p->ipart, ib0.size() * 8);
+  if (e == cudaSuccess) e = cudaMemcpy(p->item_b0, ib0.data(), ib0.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(p->item_off, ioff.data(), ioff.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !mul.empty()) e = cudaMemcpy(p->multi, mul.data(), mul.size() * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     mk_pagerank_destroy(p);
     return cuda_fail(e, "mk_pagerank_create");
@@ -436,6 +512,10 @@ mk_status mk_pagerank_destroy(mk_pagerank *p) {
   cudaFree(p->part);
   cudaFree(p->delta);
   cudaFree(p->ctl);
+  cudaFree(p->item_b0);
+  cudaFree(p->item_off);
+  cudaFree(p->multi);
+  cudaFree(p->ipart);
   delete p;
   return MK_OK;
 }

@@ -36,16 +36,19 @@ __device__ __forceinline__ bool rank_less(uint32_t du, uint32_t u, uint32_t dv, 
   return du < dv || (du == dv && u < v);
 }
 
+// Oriented CSR from the slabs, one 8-lane group per bucket (balanced under
+// degree skew): per-bucket counts, a scan over buckets, then the fill.
 template <bool kW>
-__global__ void k_orient_count(GraphView g, uint32_t *__restrict__ ocnt) {
+__global__ void k_orient_count(GraphView g, uint32_t *__restrict__ bcnt) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t u = group; u < g.V; u += ngroups) {
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    const uint32_t u = g.bowner[b];
     const uint32_t du = g.deg[u];
     uint32_t c = 0;
     if (du) {
-      walk_vertex(g, L, u, [&](const uint4 &q) {
+      walk_bucket(g, L, b, [&](const uint4 &q) {
         uint32_t k[4], w[4];
         lane_keys<kW>(q, L.gl, k, w);
 #pragma unroll
@@ -54,22 +57,30 @@ __global__ void k_orient_count(GraphView g, uint32_t *__restrict__ ocnt) {
       });
     }
     c = __reduce_add_sync(L.gmask, c);
-    if (L.gl == 0) ocnt[u] = c;
+    if (L.gl == 0) bcnt[b] = c;
   }
 }
 
+__global__ void k_tc_rows(const uint32_t *__restrict__ boff, uint32_t V, uint32_t nb,
+                          const unsigned long long *__restrict__ bpos,
+                          unsigned long long *__restrict__ row_ptr) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= V; u += gridDim.x * blockDim.x)
+    row_ptr[u] = bpos[u < V ? boff[u] : nb];
+}
+
 template <bool kW>
-__global__ void k_orient_fill(GraphView g, const unsigned long long *__restrict__ orow,
+__global__ void k_orient_fill(GraphView g, const unsigned long long *__restrict__ bpos,
                               uint32_t *__restrict__ ocol) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t u = group; u < g.V; u += ngroups) {
-    const uint32_t du = g.deg[u];
-    unsigned long long pos = orow[u];
-    const unsigned long long end = orow[u + 1];
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    unsigned long long pos = bpos[b];
+    const unsigned long long end = bpos[b + 1];
     if (pos == end) continue;
-    walk_vertex(g, L, u, [&](const uint4 &q) {
+    const uint32_t u = g.bowner[b];
+    const uint32_t du = g.deg[u];
+    walk_bucket(g, L, b, [&](const uint4 &q) {
       uint32_t k[4], w[4];
       lane_keys<kW>(q, L.gl, k, w);
       uint32_t keep[4];
@@ -377,7 +388,7 @@ struct mk_tc {
   unsigned long long *dcount = nullptr;  // [0] count, [1] scratch accumulator
   uint32_t *small = nullptr;             // [0] big_n
   DevBuf<uint32_t> ocnt, ocol, big_list, big_scratch, bcnt, bfill, bcol, pidx;
-  DevBuf<unsigned long long> orow, tmp, brow, pkeys;
+  DevBuf<unsigned long long> orow, tmp, brow, pkeys, bpos;
   Timer timer;
 };
 
@@ -390,24 +401,27 @@ static int groups_grid(uint64_t items, int device) {
 static mk_status tc_static(mk_tc *t, cudaStream_t s) {
   mk_graph *g = t->g;
   const uint32_t V = g->V;
+  const uint32_t nb = (uint32_t)g->num_buckets;
   size_t acc = 0;
-  MK_CHECK(t->ocnt.reserve(V, &acc));
+  MK_CHECK(t->ocnt.reserve(nb, &acc));
+  MK_CHECK(t->bpos.reserve((size_t)nb + 1, &acc));
   MK_CHECK(t->orow.reserve((size_t)V + 1, &acc));
   GraphView gv = g->view();
-  int blocks = groups_grid(V, g->device);
+  int blocks = groups_grid(nb, g->device);
   if (g->weighted)
     k_orient_count<true><<<blocks, 256, 0, s>>>(gv, t->ocnt.ptr);
   else
     k_orient_count<false><<<blocks, 256, 0, s>>>(gv, t->ocnt.ptr);
-  MK_CHECK(scan_u32_to_u64(t->ocnt.ptr, t->orow.ptr, V, t->tmp, s));
+  MK_CHECK(scan_u32_to_u64(t->ocnt.ptr, t->bpos.ptr, nb, t->tmp, s));
+  k_tc_rows<<<(V + 256) / 256, 256, 0, s>>>(g->boff, V, nb, t->bpos.ptr, t->orow.ptr);
   unsigned long long total = 0;
-  MK_CUDA(cudaMemcpyAsync(&total, t->orow.ptr + V, 8, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaMemcpyAsync(&total, t->bpos.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
   MK_CUDA(cudaStreamSynchronize(s));
   MK_CHECK(t->ocol.reserve(std::max<unsigned long long>(total, 1), &acc));
   if (g->weighted)
-    k_orient_fill<true><<<blocks, 256, 0, s>>>(gv, t->orow.ptr, t->ocol.ptr);
+    k_orient_fill<true><<<blocks, 256, 0, s>>>(gv, t->bpos.ptr, t->ocol.ptr);
   else
-    k_orient_fill<false><<<blocks, 256, 0, s>>>(gv, t->orow.ptr, t->ocol.ptr);
+    k_orient_fill<false><<<blocks, 256, 0, s>>>(gv, t->bpos.ptr, t->ocol.ptr);
   MK_CHECK(t->big_list.reserve(V, &acc));
   MK_CUDA(cudaMemsetAsync(t->dcount, 0, 8, s));
   MK_CUDA(cudaMemsetAsync(t->small, 0, 4, s));
@@ -419,10 +433,11 @@ static mk_status tc_static(mk_tc *t, cudaStream_t s) {
   MK_CUDA(cudaMemcpyAsync(&nbig, t->small, 4, cudaMemcpyDeviceToHost, s));
   MK_CUDA(cudaStreamSynchronize(s));
   if (nbig) {
-    // capacity: next power of two >= 2 * max oriented degree (<= 2^26)
-    std::vector<uint32_t> cnt(V);
-    MK_CUDA(cudaMemcpy(cnt.data(), t->ocnt.ptr, (size_t)V * 4, cudaMemcpyDeviceToHost));
-    uint32_t mx = *std::max_element(cnt.begin(), cnt.end());
+    // capacity: next power of two >= 2 * max oriented degree
+    std::vector<unsigned long long> rows((size_t)V + 1);
+    MK_CUDA(cudaMemcpy(rows.data(), t->orow.ptr, rows.size() * 8, cudaMemcpyDeviceToHost));
+    uint32_t mx = 0;
+    for (uint32_t u = 0; u < V; ++u) mx = std::max<uint32_t>(mx, (uint32_t)(rows[u + 1] - rows[u]));
     uint32_t cap = 64;
     while (cap < 2ull * mx) cap <<= 1;
     int bb = std::min<uint32_t>(nbig, (uint32_t)device_sm_count(g->device) * 2);
@@ -554,6 +569,7 @@ mk_status mk_tc_destroy(mk_tc *t) {
   t->tmp.release();
   t->brow.release();
   t->pkeys.release();
+  t->bpos.release();
   delete t;
   return MK_OK;
 }

@@ -24,8 +24,12 @@
 //     strategy, BFSImpl.cuh:419-440), skipping vertices of degree 0;
 //   * the stored edge weight is probed for every seeding batch edge, so a
 //     batch entry that did not change the graph cannot seed a wrong distance;
-//   * one 8-lane group per frontier vertex reads 128-byte slabs with 16-byte
-//     loads; grid-wide barriers are bounded (MK_ERR_TIMEOUT, never a hang).
+//   * frontier entries are work items (vertex, chunk of kChunk buckets), so a
+//     hub's buckets spread over many 8-lane groups instead of one; a group
+//     reads 128-byte slabs with 16-byte loads, up to 4 head slabs at once;
+//   * the re-seed sweep runs over buckets (bucket -> owner map), not vertices,
+//     so it is balanced whatever the degree skew;
+//   * grid-wide barriers are bounded (MK_ERR_TIMEOUT, never a hang).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,8 +59,8 @@ struct TravArgs {
   unsigned long long *dist;
   uint32_t *stamp;
   uint32_t *inval;  // bitmap, one bit per vertex
-  uint32_t *fr0;
-  uint32_t *fr1;
+  unsigned long long *fr0;  // work items (chunk << 32 | vertex)
+  unsigned long long *fr1;
   uint32_t *inv_list;
   uint32_t *ctl;
   unsigned long long *pushed;
@@ -70,27 +74,41 @@ struct TravArgs {
 
 constexpr int kTravBlock = 256;
 constexpr int kQueueCap = 2048;
+constexpr uint32_t kChunk = 4;  // buckets per frontier work item
+
+__host__ __device__ __forceinline__ unsigned long long item(uint32_t v, uint32_t chunk) {
+  return ((unsigned long long)chunk << 32) | v;
+}
 
 struct BlockQueue {
-  uint32_t *q;
+  unsigned long long *q;
   uint32_t *qn;
 };
 
-__device__ __forceinline__ void queue_push(const BlockQueue &Q, uint32_t v,
-                                           uint32_t *gfr, uint32_t *gsz) {
-  uint32_t pos = atomicAdd(Q.qn, 1u);
-  if (pos < kQueueCap) {
-    Q.q[pos] = v;
+// Pushes vertex v as ceil(buckets / kChunk) work items.
+__device__ __forceinline__ void push_vertex(const TravArgs &a, const BlockQueue &Q, uint32_t v,
+                                            unsigned long long *gfr, uint32_t *gsz) {
+  const uint32_t nb = a.g.boff[v + 1] - a.g.boff[v];
+  const uint32_t k = (nb + kChunk - 1) / kChunk;
+  if (k <= 1) {
+    uint32_t pos = atomicAdd(Q.qn, 1u);
+    if (pos < kQueueCap) {
+      Q.q[pos] = item(v, 0);
+    } else {
+      gfr[atomicAdd(gsz, 1u)] = item(v, 0);
+    }
   } else {
-    uint32_t gp = atomicAdd(gsz, 1u);
-    gfr[gp] = v;
+    uint32_t base = atomicAdd(gsz, k);
+    for (uint32_t j = 0; j < k; ++j) gfr[base + j] = item(v, j);
   }
 }
 
+// Frontier buffers, sizes and dist words are rewritten by other SMs inside
+// this launch, so every read of them goes through L2 (__ldcg / acquire).
+
 // Flushes the block queue into the global frontier; all threads call it.
-__device__ __forceinline__ void queue_flush(const BlockQueue &Q, uint32_t *gfr,
-                                            uint32_t *gsz,
-                                            unsigned long long *pushed,
+__device__ __forceinline__ void queue_flush(const BlockQueue &Q, unsigned long long *gfr,
+                                            uint32_t *gsz, unsigned long long *pushed,
                                             uint32_t *base_s) {
   __syncthreads();
   uint32_t cnt = min(*Q.qn, (uint32_t)kQueueCap);
@@ -121,45 +139,52 @@ __device__ __forceinline__ unsigned long long ld_dist(const unsigned long long *
 }
 
 // Relaxes v with candidate distance nd via parent u; pushes v on improvement.
-__device__ __forceinline__ void relax(const TravArgs &a, const BlockQueue &Q,
-                                      uint32_t v, unsigned long long nd,
-                                      uint32_t u, uint32_t stamp_next,
-                                      uint32_t *gfr, uint32_t *gsz) {
+__device__ __forceinline__ void relax(const TravArgs &a, const BlockQueue &Q, uint32_t v,
+                                      unsigned long long nd, uint32_t u, uint32_t stamp_next,
+                                      unsigned long long *gfr, uint32_t *gsz) {
   if (nd >= kInf) return;
   unsigned long long cur = ld_dist(a.dist + v);
   if (nd >= pack_hi(cur)) return;
   unsigned long long cand = pack((uint32_t)nd, u);
   unsigned long long old = atomicMin(a.dist + v, cand);
   if (pack_hi(old) > nd) {
-    if (atomicExch(a.stamp + v, stamp_next) != stamp_next) queue_push(Q, v, gfr, gsz);
+    if (atomicExch(a.stamp + v, stamp_next) != stamp_next) push_vertex(a, Q, v, gfr, gsz);
   }
 }
 
-// Expands vertex u: relax every live out-neighbour.
+// Relaxes the live out-neighbours held by one slab quarter.
 template <bool kW, bool kUseW>
-__device__ __forceinline__ void expand(const TravArgs &a, const Lanes &L,
-                                       const BlockQueue &Q, uint32_t u,
-                                       uint32_t du, uint32_t stamp_next,
-                                       uint32_t *gfr, uint32_t *gsz,
-                                       bool only_invalid) {
-  walk_vertex(a.g, L, u, [&](const uint4 &q) {
-    uint32_t k[4], w[4];
-    lane_keys<kW>(q, L.gl, k, w);
+__device__ __forceinline__ void relax_slab(const TravArgs &a, const Lanes &L,
+                                           const BlockQueue &Q, const uint4 &q, uint32_t u,
+                                           uint32_t du, uint32_t stamp_next,
+                                           unsigned long long *gfr, uint32_t *gsz,
+                                           bool only_invalid) {
+  uint32_t k[4], w[4];
+  lane_keys<kW>(q, L.gl, k, w);
 #pragma unroll
-    for (int i = 0; i < keys_per_lane<kW>(); ++i) {
-      uint32_t v = k[i];
-      if (v < kTombKey && v != u) {
-        if (only_invalid && !inval_test(a.inval, v)) continue;
-        unsigned long long nd = (unsigned long long)du + (kUseW ? w[i] : 1u);
-        relax(a, Q, v, nd, u, stamp_next, gfr, gsz);
-      }
+  for (int i = 0; i < keys_per_lane<kW>(); ++i) {
+    uint32_t v = k[i];
+    if (v < kTombKey && v != u) {
+      if (only_invalid && !inval_test(a.inval, v)) continue;
+      unsigned long long nd = (unsigned long long)du + (kUseW ? w[i] : 1u);
+      relax(a, Q, v, nd, u, stamp_next, gfr, gsz);
     }
-  });
+  }
+}
+
+// Bucket range of a work item.
+__device__ __forceinline__ void item_range(const GraphView &g, unsigned long long it,
+                                           uint32_t &v, uint32_t &b0, uint32_t &b1) {
+  v = (uint32_t)it;
+  const uint32_t c = (uint32_t)(it >> 32);
+  const uint32_t lo = g.boff[v], hi = g.boff[v + 1];
+  b0 = lo + c * kChunk;
+  b1 = min(hi, b0 + kChunk);
 }
 
 template <bool kW, bool kUseW>
 __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
-  __shared__ uint32_t q_s[kQueueCap];
+  __shared__ unsigned long long q_s[kQueueCap];
   __shared__ uint32_t qn_s;
   __shared__ uint32_t base_s;
   if (threadIdx.x == 0) qn_s = 0;
@@ -172,17 +197,22 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   const uint32_t ngroups = nthreads >> 3;
   uint32_t *ctl = a.ctl;
   uint32_t *err = ctl + kErr;
-  uint32_t *fr[2] = {a.fr0, a.fr1};
-  uint32_t round = ld_acquire_u32(ctl + kRound);
+  unsigned long long *fr[2] = {a.fr0, a.fr1};
+  const uint32_t round = ld_acquire_u32(ctl + kRound);
 
   // ---- seeding (level -1 pushes into fr[0] / sz[0]) ----
   if (a.mode == kStatic) {
     if (tid == 0) {
       a.dist[a.source] = pack(0, a.source);
       a.stamp[a.source] = round + 1;
-      a.fr0[0] = a.source;
-      ctl[kSz0] = 1;
       atomicAdd(a.pushed, 1ull);
+    }
+    if (tid < 32) {
+      // the source's items (a hub source has many)
+      const uint32_t nb = a.g.boff[a.source + 1] - a.g.boff[a.source];
+      const uint32_t k = max(1u, (nb + kChunk - 1) / kChunk);
+      for (uint32_t j = tid; j < k; j += 32) a.fr0[j] = item(a.source, j);
+      if (tid == 0) ctl[kSz0] = k;
     }
   } else if (a.mode == kIncremental) {
     for (uint32_t e = group; e < a.bn; e += ngroups) {
@@ -210,10 +240,13 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   } else {  // kDecremental
     // D1: children of deleted tree edges.  Every invalidated vertex goes to
     // inv_list (for the final flag reset) and to the invalidation frontier.
-    auto invalidate = [&](uint32_t v, uint32_t *gfr, uint32_t *gsz) {
+    auto invalidate = [&](uint32_t v, unsigned long long *gfr, uint32_t *gsz) {
       a.dist[v] = kInfInf;
       a.inv_list[atomicAdd(ctl + kInvCount, 1u)] = v;
-      gfr[atomicAdd(gsz, 1u)] = v;
+      const uint32_t nb = a.g.boff[v + 1] - a.g.boff[v];
+      const uint32_t k = max(1u, (nb + kChunk - 1) / kChunk);
+      const uint32_t base = atomicAdd(gsz, k);
+      for (uint32_t j = 0; j < k; ++j) gfr[base + j] = item(v, j);
     };
     for (uint32_t e = tid; e < a.bn; e += nthreads) {
       uint32_t s = a.bsrc[e], d = a.bdst[e];
@@ -230,12 +263,13 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       const uint32_t n = ld_acquire_u32(ctl + kDSz0 + (dl % 3));
       if (n == 0) break;
       if (tid == 0) ctl[kDSz0 + ((dl + 2) % 3)] = 0;
-      const uint32_t *cur = fr[dl & 1];
-      uint32_t *nxt = fr[(dl + 1) & 1];
+      const unsigned long long *cur = fr[dl & 1];
+      unsigned long long *nxt = fr[(dl + 1) & 1];
       uint32_t *nsz = ctl + kDSz0 + ((dl + 1) % 3);
       for (uint32_t i = group; i < n; i += ngroups) {
-        const uint32_t x = cur[i];
-        walk_vertex(a.g, L, x, [&](const uint4 &q) {
+        uint32_t x, b0, b1;
+        item_range(a.g, __ldcg(cur + i), x, b0, b1);
+        walk_buckets(a.g, L, b0, b1, [&](const uint4 &q) {
           uint32_t k[4], w[4];
           lane_keys<kW>(q, L.gl, k, w);
 #pragma unroll
@@ -251,15 +285,19 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
     }
     const uint32_t hi = ld_acquire_u32(ctl + kInvCount);
-    // D3: re-seed invalidated vertices from valid in-neighbours (full sweep)
+    // D3: re-seed invalidated vertices from valid in-neighbours: one sweep
+    // over all buckets (balanced by construction)
     if (hi > 0) {
-      for (uint32_t u = group; u < a.g.V; u += ngroups) {
+      for (uint32_t b = group; b < a.g.nbuckets; b += ngroups) {
+        const uint32_t u = a.g.bowner[b];
         if (a.g.deg[u] == 0 || inval_test(a.inval, u)) continue;
         unsigned long long pu = 0;
         if (L.gl == 0) pu = ld_dist(a.dist + u);
         pu = __shfl_sync(L.gmask, pu, L.gbase);
         if (pu == kInfInf) continue;
-        expand<kW, kUseW>(a, L, Q, u, pack_hi(pu), round + 1, a.fr0, ctl + kSz0, true);
+        walk_bucket(a.g, L, b, [&](const uint4 &q) {
+          relax_slab<kW, kUseW>(a, L, Q, q, u, pack_hi(pu), round + 1, a.fr0, ctl + kSz0, true);
+        });
       }
     }
   }
@@ -269,20 +307,24 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   // ---- relaxation levels ----
   uint32_t lv = 0;
   for (;; ++lv) {
-    uint32_t n = ld_acquire_u32(ctl + kSz0 + (lv % 3));
+    const uint32_t n = ld_acquire_u32(ctl + kSz0 + (lv % 3));
     if (n == 0) break;
     if (tid == 0) ctl[kSz0 + ((lv + 2) % 3)] = 0;
-    uint32_t *cur = fr[lv & 1];
-    uint32_t *nxt = fr[(lv + 1) & 1];
+    const unsigned long long *cur = fr[lv & 1];
+    unsigned long long *nxt = fr[(lv + 1) & 1];
     uint32_t *nsz = ctl + kSz0 + ((lv + 1) % 3);
     const uint32_t stamp_next = round + 2 + lv;
     for (uint32_t i = group; i < n; i += ngroups) {
-      uint32_t u = cur[i];
+      uint32_t u, b0, b1;
+      item_range(a.g, __ldcg(cur + i), u, b0, b1);
       unsigned long long pu = 0;
       if (L.gl == 0) pu = ld_dist(a.dist + u);
       pu = __shfl_sync(L.gmask, pu, L.gbase);
       if (pu == kInfInf) continue;
-      expand<kW, kUseW>(a, L, Q, u, pack_hi(pu), stamp_next, nxt, nsz, false);
+      const uint32_t du = pack_hi(pu);
+      walk_buckets(a.g, L, b0, b1, [&](const uint4 &q) {
+        relax_slab<kW, kUseW>(a, L, Q, q, u, du, stamp_next, nxt, nsz, false);
+      });
     }
     queue_flush(Q, nxt, nsz, a.pushed, &base_s);
     if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
@@ -291,7 +333,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   // ---- epilogue: clear invalidation flags, publish counters ----
   if (a.mode == kDecremental) {
     uint32_t ninv = ld_acquire_u32(ctl + kInvCount);
-    for (uint32_t i = tid; i < ninv; i += nthreads) a.inval[a.inv_list[i] >> 5] = 0u;
+    for (uint32_t i = tid; i < ninv; i += nthreads) a.inval[__ldcg(a.inv_list + i) >> 5] = 0u;
   }
   if (tid == 0) {
     ctl[kLevels] = lv;
@@ -312,7 +354,8 @@ struct mk_traversal {
   unsigned long long *dist = nullptr;
   uint32_t *stamp = nullptr;
   uint32_t *inval = nullptr;
-  uint32_t *fr0 = nullptr, *fr1 = nullptr, *inv_list = nullptr;
+  unsigned long long *fr0 = nullptr, *fr1 = nullptr;
+  uint32_t *inv_list = nullptr;
   uint32_t *ctl = nullptr;
   unsigned long long *pushed = nullptr;
   Timer timer;
@@ -337,8 +380,10 @@ static mk_status trav_create(mk_graph *g, uint32_t source, bool sssp, mk_travers
   A((void **)&t->dist, V * 8);
   A((void **)&t->stamp, V * 4);
   A((void **)&t->inval, (V + 31) / 32 * 4);
-  A((void **)&t->fr0, V * 4 + 16);
-  A((void **)&t->fr1, V * 4 + 16);
+  // a level holds every vertex at most once, as ceil(buckets / kChunk) items
+  const size_t items = V + g->num_buckets / kChunk + 64;
+  A((void **)&t->fr0, items * 8);
+  A((void **)&t->fr1, items * 8);
   A((void **)&t->inv_list, V * 4 + 16);
   A((void **)&t->ctl, kCtlWords * 4);
   A((void **)&t->pushed, 8);

@@ -53,16 +53,18 @@ __global__ void k_uf_init(uint32_t *p, uint32_t V) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) p[i] = i;
 }
 
-// Union every out-edge of the vertices selected by `sel` (all if null).
+// Union every out-edge of the vertices selected by `sel` (all if null); one
+// group per bucket so hubs do not serialise the pass.
 template <bool kW>
 __global__ void k_uf_edges(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t u = group; u < g.V; u += ngroups) {
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    const uint32_t u = g.bowner[b];
     if (g.deg[u] == 0) continue;
     if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
-    walk_vertex(g, L, u, [&](const uint4 &q) {
+    walk_bucket(g, L, b, [&](const uint4 &q) {
       uint32_t k[4], w[4];
       lane_keys<kW>(q, L.gl, k, w);
 #pragma unroll
@@ -129,7 +131,7 @@ static int flat_grid(uint64_t n, int device) {
 
 static mk_status wcc_edges(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
   mk_graph *g = w->g;
-  int blocks = (int)std::min<uint64_t>((uint64_t)g->V * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  int blocks = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
   if (g->weighted)
     k_uf_edges<true><<<blocks, 256, 0, s>>>(g->view(), w->parent, sel, w->err);
   else

@@ -70,8 +70,16 @@ def test_golden_fixture_through_the_abi(gold):
     d_s, d_d = to_dev(gold["del_src"]), to_dev(gold["del_dst"])
     G.DeleteEdges(d_s, d_d)
     Gr.DeleteEdges(d_s, d_d)
-    sym_s = to_dev(np.concatenate([gold["del_src"], gold["del_dst"]]))
-    sym_d = to_dev(np.concatenate([gold["del_dst"], gold["del_src"]]))
+    # an undirected edge leaves the symmetric graph only if neither direction
+    # survives in the directed graph
+    alive = set(zip(np.concatenate([s, gold["ins_src"]]).tolist(),
+                    np.concatenate([d, gold["ins_dst"]]).tolist()))
+    alive -= set(zip(gold["del_src"].tolist(), gold["del_dst"].tolist()))
+    gone = np.array([(a, b) not in alive and (b, a) not in alive
+                     for a, b in zip(gold["del_src"].tolist(), gold["del_dst"].tolist())])
+    us, ud = gold["del_src"][gone], gold["del_dst"][gone]
+    sym_s = to_dev(np.concatenate([us, ud]))
+    sym_d = to_dev(np.concatenate([ud, us]))
     Gs.DeleteEdges(sym_s, sym_d)
     bfs.Decremental(d_s, d_d)
     sssp.Decremental(d_s, d_d)
