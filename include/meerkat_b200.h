@@ -136,6 +136,19 @@ mk_status mk_graph_count_tombstones(mk_graph *g, uint32_t *d_out,
  * updates of that size allocate nothing. */
 mk_status mk_graph_reserve_batch(mk_graph *g, uint32_t n);
 
+/* Kernel choices of the update path (no counterpart in the reference, which
+ * has a single insert/delete kernel).  The autotuner in
+ * meerkat_b200/autotune.py measures the variants on live batches. */
+typedef struct mk_tuning {
+  uint32_t update_kernel;        /* 0 = warp-staged (TMA bulk copies into shared
+                                    memory), 1 = one lane per edge             */
+  uint32_t update_blocks_per_sm; /* resident blocks per SM, 0 = automatic     */
+  uint32_t reserved0;
+  uint32_t reserved1;
+} mk_tuning;
+mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t);
+mk_status mk_graph_get_tuning(mk_graph *g, mk_tuning *t);
+
 /* ------------------------------------------------------------------------
  * BFS and SSSP (replace BFS<AllocPolicy>, include/Algorithms/BFS.cuh:13-69,
  * and SSSP<AllocPolicy>, include/Algorithms/SSSP.cuh:11-69).  A BFS may run

@@ -16,7 +16,7 @@ from typing import Optional
 
 import numpy as np
 
-from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, check, lib)
+from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
 __all__ = ["DynamicGraph", "BFS", "SSSP", "PageRank", "TC", "WCC", "EdgeSet", "gen_rmat",
            "gen_grid", "MeerkatError", "MK_INF", "lib", "version"]
@@ -119,6 +119,15 @@ class DynamicGraph:
         check(lib().mk_graph_search_edges(self._h, _ptr(src), _ptr(dst), _count(src, n),
                                           _ptr(found), _ptr(weights), _stream(stream)),
               "mk_graph_search_edges")
+
+    def set_tuning(self, update_kernel: int = 1, update_blocks_per_sm: int = 0) -> None:
+        t = Tuning(int(update_kernel), int(update_blocks_per_sm), 0, 0)
+        check(lib().mk_graph_set_tuning(self._h, C.byref(t)), "mk_graph_set_tuning")
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        check(lib().mk_graph_get_tuning(self._h, C.byref(t)), "mk_graph_get_tuning")
+        return {"update_kernel": t.update_kernel, "update_blocks_per_sm": t.update_blocks_per_sm}
 
     def reserve_batch(self, n: int) -> None:
         check(lib().mk_graph_reserve_batch(self._h, int(n)), "mk_graph_reserve_batch")

@@ -32,6 +32,11 @@ class GraphInfo(C.Structure):
                 ("num_edges", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("update_kernel", C.c_uint32), ("update_blocks_per_sm", C.c_uint32),
+                ("reserved0", C.c_uint32), ("reserved1", C.c_uint32)]
+
+
 # (name, restype, argtypes); every function returns mk_status unless noted
 _S = C.c_int
 SIGNATURES = [
@@ -51,6 +56,8 @@ SIGNATURES = [
     ("mk_graph_export_csr", _S, [vp, vp, vp, vp, vp]),
     ("mk_graph_count_tombstones", _S, [vp, vp, vp]),
     ("mk_graph_reserve_batch", _S, [vp, C.c_uint32]),
+    ("mk_graph_set_tuning", _S, [vp, C.POINTER(Tuning)]),
+    ("mk_graph_get_tuning", _S, [vp, C.POINTER(Tuning)]),
     ("mk_bfs_create", _S, [vp, C.c_uint32, C.POINTER(vp)]),
     ("mk_sssp_create", _S, [vp, C.c_uint32, C.POINTER(vp)]),
     ("mk_traversal_static", _S, [vp, vp, f32p]),

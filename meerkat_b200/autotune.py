@@ -1,0 +1,85 @@
+"""Autotuner for the update path.
+
+Measures every update-kernel variant (mk_tuning.update_kernel and
+update_blocks_per_sm) on live update batches of the caller's graph and keeps
+the fastest.  Each trial applies a real mixed batch (deletes of present
+edges, then inserts of absent edges), so tuning consumes batches exactly like
+the timed run and leaves the graph in a valid state.  Results can be cached
+in a JSON file keyed by GPU name and graph shape.
+
+There is no counterpart in the reference (it has one insert and one delete
+kernel with fixed 128-thread blocks, include/Graph/SlabGraphImpl.cuh:6-62).
+"""
+from __future__ import annotations
+
+import json
+import os
+from pathlib import Path
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+# (update_kernel, update_blocks_per_sm): warp-staged TMA kernel, lane-per-edge
+# kernel at three residency caps
+VARIANTS: Tuple[Tuple[int, int], ...] = ((0, 0), (1, 4), (1, 6), (1, 8))
+
+
+def _key(G, device_name: str) -> str:
+    info = G.info()
+    return (f"{device_name}|V={info['num_vertices']}|E~{info['num_edges'] >> 20}M|"
+            f"w={info['weighted']}|r={info['reverse']}")
+
+
+def cache_path() -> Path:
+    return Path(os.environ.get("MK_TUNING_CACHE",
+                               Path.home() / ".cache" / "meerkat_b200" / "tuning.json"))
+
+
+def load_cached(G, device_name: str) -> Optional[dict]:
+    p = cache_path()
+    if not p.exists():
+        return None
+    try:
+        return json.loads(p.read_text()).get(_key(G, device_name))
+    except (OSError, ValueError):
+        return None
+
+
+def store_cached(G, device_name: str, best: dict) -> None:
+    p = cache_path()
+    try:
+        p.parent.mkdir(parents=True, exist_ok=True)
+        data = json.loads(p.read_text()) if p.exists() else {}
+        data[_key(G, device_name)] = best
+        p.write_text(json.dumps(data, indent=1, sort_keys=True))
+    except (OSError, ValueError):
+        pass
+
+
+def tune_updates(G, batches: Iterable[Sequence], variants: Sequence[Tuple[int, int]] = VARIANTS,
+                 stream=None) -> dict:
+    """Times one mixed batch per variant (batches: (del_src, del_dst, ins_src,
+    ins_dst, ins_w) device tensors, valid in sequence) and selects the fastest.
+    Returns {"best": {...}, "trials": [...]}."""
+    import torch
+    it = iter(batches)
+    trials: List[dict] = []
+    s = stream if stream is not None else torch.cuda.current_stream()
+    for kern, bps in variants:
+        b = next(it)
+        G.set_tuning(update_kernel=kern, update_blocks_per_sm=bps)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(s)
+        G.DeleteEdges(b[0], b[1], stream=s)
+        e1.record(s)
+        G.InsertEdges(b[2], b[3], vals=b[4], stream=s)
+        e2.record(s)
+        e2.synchronize()
+        if G.sync() != 0:
+            raise RuntimeError("device error during tuning")
+        trials.append({"update_kernel": kern, "update_blocks_per_sm": bps,
+                       "delete_ms": e0.elapsed_time(e1), "insert_ms": e1.elapsed_time(e2)})
+    best = min(trials, key=lambda t: t["delete_ms"] + t["insert_ms"])
+    G.set_tuning(update_kernel=best["update_kernel"],
+                 update_blocks_per_sm=best["update_blocks_per_sm"])
+    return {"best": {"update_kernel": best["update_kernel"],
+                     "update_blocks_per_sm": best["update_blocks_per_sm"]},
+            "trials": trials}

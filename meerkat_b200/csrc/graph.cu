@@ -32,6 +32,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 
@@ -340,117 +341,166 @@ __device__ __forceinline__ uint32_t delete_chain(const GraphView &g, const Lanes
   return 0;
 }
 
-// Update kernels.  A warp takes 32 batch edges:
+// Update kernels.  A warp takes 32 batch edges at a time:
 //   1. every lane resolves its edge to the bucket's head slab;
-//   2. the warp issues all 32 head-slab loads (8 rounds x 4 groups, 16 B per
-//      lane) before using any of them;
-//   3. each group analyses its 8 slabs (redux.sync) and hands every decision
-//      to the lane that owns the edge;
-//   4. the owning lanes issue their CASes together (one warp instruction,
-//      32 independent atomics in flight);
-//   5. the rare edges whose CAS lost a race, whose chain continues or needs a
-//      new slab fall back to the group-cooperative chain walk.
-// A prefetched slab that went stale only costs the slow path: inside one
-// insert call key words only ever move EMPTY -> key, and inside one delete
-// call only key -> TOMBSTONE.
+//   2. every lane issues one 128-byte TMA bulk copy of that slab into the
+//      warp's shared-memory stage (completion on the stage's mbarrier), and
+//      the warp moves on to resolve its next 32 edges into the other stage
+//      while the copies are in flight (double buffering);
+//   3. each 8-lane group analyses 8 staged slabs (redux.sync) and hands every
+//      decision to the lane that owns the edge;
+//   4. the owning lanes issue their CASes together (one warp instruction);
+//   5. edges whose CAS lost a race, whose chain continues or that need a new
+//      slab take the group-cooperative chain walk.
+// A staged slab that went stale only costs the slow path: inside one insert
+// call key words only move EMPTY -> key, inside one delete call only
+// key -> TOMBSTONE.
 constexpr int kRounds = 8;
+constexpr int kUpdWarps = 4;  // warps per block
 constexpr uint32_t kActNoop = 0x100;  // key already present (insert) / absent (delete)
 constexpr uint32_t kActSlow = 0x200;  // needs the chain walk
 constexpr uint32_t kActSkip = 0x300;  // lane has no edge
+constexpr size_t kUpdSmem = (size_t)kUpdWarps * 2 * 32 * 128;  // 2 stages x 32 slabs per warp
+
+struct UpdEdge {
+  uint32_t u, v, wt, head;
+};
 
 template <bool kWeighted, bool kDedupe, bool kInsert>
-__global__ void __launch_bounds__(kUpdBlock, 4)
+__device__ __forceinline__ UpdEdge upd_resolve(const GraphView &g, const uint32_t *__restrict__ src,
+                                               const uint32_t *__restrict__ dst,
+                                               const uint32_t *__restrict__ w, uint32_t n, uint64_t e,
+                                               const unsigned long long *__restrict__ dd_keys,
+                                               const uint32_t *__restrict__ dd_idx, uint32_t dd_mask,
+                                               uint8_t *__restrict__ applied) {
+  UpdEdge E{0u, 0u, 0u, kNoSlab};
+  if (e < n) {
+    uint32_t u = src[e], v = dst[e];
+    if (kWeighted && kInsert && w) E.wt = w[e];
+    if (g.reverse) {
+      uint32_t t = u;
+      u = v;
+      v = t;
+    }
+    E.u = u;
+    E.v = v;
+    bool ok = (u != v);
+    if (u >= g.V || v >= g.V) {
+      ok = false;
+      atomicOr(g.err, kErrInvalidId);
+    }
+    if (ok) {
+      const uint32_t b0 = g.boff[u];
+      const uint32_t b1 = g.boff[u + 1];
+      if (kDedupe) ok = dedupe_is_first(dd_keys, dd_idx, dd_mask, u, v, (uint32_t)e);
+      if (ok) E.head = b0 + bucket_of(v, b1 - b0);
+    }
+    if (!ok) applied[e] = 0;
+  }
+  return E;
+}
+
+template <bool kWeighted, bool kDedupe, bool kInsert>
+__global__ void __launch_bounds__(kUpdWarps * 32)
     k_update(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
              const uint32_t *__restrict__ w, uint32_t n,
              const unsigned long long *__restrict__ dd_keys, const uint32_t *__restrict__ dd_idx,
              uint32_t dd_mask, uint8_t *__restrict__ applied, unsigned long long *count) {
-  __shared__ uint32_t blk_count;
-  if (threadIdx.x == 0) blk_count = 0;
-  __syncthreads();
+  extern __shared__ __align__(128) uint4 stage_smem[];
+  __shared__ __align__(8) uint64_t bars[kUpdWarps][2];
   const Lanes L = lanes();
+  const uint32_t wib = threadIdx.x >> 5;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  uint4 *wst = stage_smem + (size_t)wib * 2 * 32 * 8;  // [stage][slab][quarter]
+  if (L.lane == 0) {
+    mbar_init(&bars[wib][0], 1);
+    mbar_init(&bars[wib][1], 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  uint32_t parity[2] = {0u, 0u};
   uint32_t mine = 0;
-  for (uint64_t base = (uint64_t)warp * 32; base < n; base += (uint64_t)nwarps * 32) {
-    // 1. resolve the lane's edge
-    const uint64_t e = base + L.lane;
-    uint32_t u = 0, v = 0, wt = 0, head = kNoSlab;
-    if (e < n) {
-      u = src[e];
-      v = dst[e];
-      if (kWeighted && kInsert && w) wt = w[e];
-      if (g.reverse) {
-        uint32_t t = u;
-        u = v;
-        v = t;
-      }
-      bool ok = (u != v);
-      if (u >= g.V || v >= g.V) {
-        ok = false;
-        atomicOr(g.err, kErrInvalidId);
-      }
-      if (kDedupe && ok) ok = dedupe_is_first(dd_keys, dd_idx, dd_mask, u, v, (uint32_t)e);
-      if (ok) {
-        const uint32_t b0 = g.boff[u];
-        head = b0 + bucket_of(v, g.boff[u + 1] - b0);
-      } else {
-        applied[e] = 0;
-      }
+
+  // stage the head slabs of edge record E into stage st
+  auto issue = [&](const UpdEdge &E, uint32_t st) {
+    const uint32_t valid = __ballot_sync(0xFFFFFFFFu, E.head != kNoSlab);
+    fence_proxy_async_smem();  // this warp's earlier reads of the buffer come first
+    __syncwarp();
+    if (L.lane == 0) mbar_arrive_expect_tx(&bars[wib][st], 128u * __popc(valid));
+    __syncwarp();
+    if (E.head != kNoSlab)
+      bulk_load(wst + ((size_t)st * 32 + L.lane) * 8, g.slabs + 8ull * E.head, 128u, &bars[wib][st]);
+  };
+
+  uint64_t base = (uint64_t)warp * 32;
+  if (base >= n) return;
+  UpdEdge cur = upd_resolve<kWeighted, kDedupe, kInsert>(g, src, dst, w, n, base + L.lane, dd_keys,
+                                                         dd_idx, dd_mask, applied);
+  uint32_t st = 0;
+  issue(cur, st);
+  for (;;) {
+    const uint64_t nbase = base + (uint64_t)nwarps * 32;
+    const bool has_next = nbase < n;
+    UpdEdge nxt{0u, 0u, 0u, kNoSlab};
+    if (has_next) {
+      nxt = upd_resolve<kWeighted, kDedupe, kInsert>(g, src, dst, w, n, nbase + L.lane, dd_keys,
+                                                     dd_idx, dd_mask, applied);
+      issue(nxt, st ^ 1u);
     }
-    // 2. all head slabs in flight
-    uint4 q[kRounds];
-#pragma unroll
-    for (int r = 0; r < kRounds; ++r) {
-      const uint32_t hs = __shfl_sync(0xFFFFFFFFu, head, 4 * r + L.grp);
-      if (hs != kNoSlab) q[r] = ld_slab_cg(g.slabs + 8ull * hs + L.gl);
-    }
-    // 3. per-round decisions, delivered to the owning lanes
+    const bool ready = mbar_wait(&bars[wib][st], parity[st], g.err);
+    parity[st] ^= 1u;
+    // decisions per round, delivered to the owning lanes
     uint32_t my_act = kActSkip;
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
       const uint32_t sl = 4 * r + L.grp;
-      const uint32_t hs = __shfl_sync(0xFFFFFFFFu, head, sl);
-      const uint32_t vv = __shfl_sync(0xFFFFFFFFu, v, sl);
+      const uint32_t hs = __shfl_sync(0xFFFFFFFFu, cur.head, sl);
+      const uint32_t vv = __shfl_sync(0xFFFFFFFFu, cur.v, sl);
       uint32_t act = kActSkip;
       if (hs != kNoSlab) {
-        bool found;
-        uint32_t fslot, eslot, next;
-        probe_slab<kWeighted>(q[r], vv, L, found, fslot, eslot, next);
-        if (kInsert)
-          act = found ? kActNoop : (eslot != 255 ? eslot : kActSlow);
-        else
-          act = found ? fslot : (next == kNoSlab ? kActNoop : kActSlow);
+        if (ready) {
+          const uint4 q = wst[((size_t)st * 32 + sl) * 8 + L.gl];
+          bool found;
+          uint32_t fslot, eslot, next;
+          probe_slab<kWeighted>(q, vv, L, found, fslot, eslot, next);
+          if (kInsert)
+            act = found ? kActNoop : (eslot != 255 ? eslot : kActSlow);
+          else
+            act = found ? fslot : (next == kNoSlab ? kActNoop : kActSlow);
+        } else {
+          act = kActSlow;
+        }
       }
-      // lane (4r + g) takes the decision of group g for round r
       const uint32_t t = __shfl_sync(0xFFFFFFFFu, act, (L.lane & 3u) * 8u);
       if ((L.lane >> 2) == (uint32_t)r) my_act = t;
     }
-    // 4. one CAS per owning lane, all issued together
+    // one CAS per owning lane, all issued together
     uint32_t app = 0;
     bool slow = (my_act == kActSlow);
     if (my_act < 255) {
-      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * head) + slot_word<kWeighted>(my_act);
+      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * cur.head) + slot_word<kWeighted>(my_act);
       if (kInsert) {
-        const uint32_t old = atomicCAS(wp, kEmptyKey, v);
+        const uint32_t old = atomicCAS(wp, kEmptyKey, cur.v);
         if (old == kEmptyKey) {
           app = 1;
-          if (kWeighted) wp[1] = wt;
-        } else if (old != v) {
+          if (kWeighted) wp[1] = cur.wt;
+        } else if (old != cur.v) {
           slow = true;  // lost the word to another key
         }
       } else {
-        app = (atomicCAS(wp, v, kTombKey) == v) ? 1u : 0u;
+        app = (atomicCAS(wp, cur.v, kTombKey) == cur.v) ? 1u : 0u;
       }
     }
-    // 5. slow path, round by round, group-cooperative
+    // slow path, round by round, group-cooperative (reads global memory)
     const uint32_t slow_mask = __ballot_sync(0xFFFFFFFFu, slow);
     if (slow_mask) {
 #pragma unroll 1
       for (int r = 0; r < kRounds; ++r) {
         const uint32_t sl = 4 * r + L.grp;
-        const uint32_t hs = __shfl_sync(0xFFFFFFFFu, head, sl);
-        const uint32_t vv = __shfl_sync(0xFFFFFFFFu, v, sl);
-        const uint32_t ww = __shfl_sync(0xFFFFFFFFu, wt, sl);
+        const uint32_t hs = __shfl_sync(0xFFFFFFFFu, cur.head, sl);
+        const uint32_t vv = __shfl_sync(0xFFFFFFFFu, cur.v, sl);
+        const uint32_t ww = __shfl_sync(0xFFFFFFFFu, cur.wt, sl);
         uint32_t res = 0;
         if ((slow_mask >> sl) & 1u) {
           const uint4 q0 = ld_slab_cg(g.slabs + 8ull * hs + L.gl);
@@ -463,21 +513,153 @@ __global__ void __launch_bounds__(kUpdBlock, 4)
       }
     }
     // owning lane publishes the outcome
-    if (head != kNoSlab) {
-      applied[e] = (uint8_t)app;
+    if (cur.head != kNoSlab) {
+      applied[base + L.lane] = (uint8_t)app;
       if (app) {
         if (kInsert)
-          atomicAdd(g.deg + u, 1u);
+          atomicAdd(g.deg + cur.u, 1u);
         else
-          atomicSub(g.deg + u, 1u);
+          atomicSub(g.deg + cur.u, 1u);
         ++mine;
       }
     }
+    if (!has_next) break;
+    __syncwarp();
+    cur = nxt;
+    base = nbase;
+    st ^= 1u;
   }
   mine = __reduce_add_sync(0xFFFFFFFFu, mine);
-  if (L.lane == 0 && mine) atomicAdd(&blk_count, mine);
-  __syncthreads();
-  if (threadIdx.x == 0 && blk_count) atomicAdd(count, (unsigned long long)blk_count);
+  if (L.lane == 0 && mine) atomicAdd(count, (unsigned long long)mine);
+}
+
+// ---------------------------------------------------------------------------
+// Thread-per-edge variant: a lane loads its edge's whole head slab with 8
+// independent 16-byte loads, decides alone (no cross-lane synchronisation),
+// and commits with one CAS.  Chains and lost races are walked by the same
+// lane.  Selected by the tuner when it beats the warp-staged kernel.
+// ---------------------------------------------------------------------------
+struct LaneProbe {
+  uint32_t found_word;  // word index of the key, 32 if absent
+  uint32_t empty_word;  // first EMPTY key word, 32 if none
+  uint32_t next;        // next-slab id
+};
+
+template <bool kWeighted>
+__device__ __forceinline__ LaneProbe lane_probe(const uint4 (&q)[8], uint32_t key) {
+  LaneProbe r{32u, 32u, q[7].w};
+#pragma unroll
+  for (int j = 7; j >= 0; --j) {
+    const uint32_t wv[4] = {q[j].x, q[j].y, q[j].z, q[j].w};
+#pragma unroll
+    for (int c = 3; c >= 0; --c) {
+      const uint32_t word = 4 * j + c;
+      const bool is_key = kWeighted ? ((word & 1u) == 0 && word < 30) : (word < 31);
+      if (!is_key) continue;
+      if (wv[c] == key) r.found_word = word;
+      if (wv[c] == kEmptyKey) r.empty_word = word;
+    }
+  }
+  return r;
+}
+
+__device__ __forceinline__ void lane_load_slab(const GraphView &g, uint32_t s, uint4 (&q)[8]) {
+  const uint4 *p = g.slabs + 8ull * s;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) q[j] = __ldcg(p + j);
+}
+
+// Single-lane insert into the chain at s (first slab already in q).
+template <bool kWeighted>
+__device__ uint32_t lane_insert_chain(const GraphView &g, uint32_t s, uint4 (&q)[8], uint32_t v,
+                                      uint32_t wt) {
+  for (uint32_t it = 0; it < kProbeLimit; ++it) {
+    if (it) lane_load_slab(g, s, q);
+    const LaneProbe p = lane_probe<kWeighted>(q, v);
+    if (p.found_word < 32) return 0;
+    if (p.empty_word < 32) {
+      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + p.empty_word;
+      const uint32_t old = atomicCAS(wp, kEmptyKey, v);
+      if (old == kEmptyKey) {
+        if (kWeighted) wp[1] = wt;
+        return 1;
+      }
+      if (old == v) return 0;
+      continue;
+    }
+    if (p.next == kLinkBusy) {
+      __nanosleep(64);
+      continue;
+    }
+    if (p.next != kNoSlab) {
+      s = p.next;
+      continue;
+    }
+    uint32_t *nextp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + 31;
+    if (atomicCAS(nextp, kNoSlab, kLinkBusy) == kNoSlab) {
+      const uint32_t ns = atomicAdd(g.pool_top, 1u);
+      if (ns >= g.pool_cap) {
+        atomicOr(g.err, kErrOom);
+        atomicExch(nextp, kNoSlab);
+        return 0;
+      }
+      uint32_t *np = reinterpret_cast<uint32_t *>(g.slabs + 8ull * ns);
+      np[0] = v;
+      if (kWeighted) np[1] = wt;
+      __threadfence();
+      atomicExch(nextp, ns);
+      return 1;
+    }
+  }
+  atomicOr(g.err, kErrTimeout);
+  return 0;
+}
+
+template <bool kWeighted>
+__device__ uint32_t lane_delete_chain(const GraphView &g, uint32_t s, uint4 (&q)[8], uint32_t v) {
+  for (uint32_t it = 0; it < kProbeLimit; ++it) {
+    if (it) lane_load_slab(g, s, q);
+    const LaneProbe p = lane_probe<kWeighted>(q, v);
+    if (p.found_word < 32) {
+      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + p.found_word;
+      return atomicCAS(wp, v, kTombKey) == v ? 1u : 0u;
+    }
+    if (p.next == kNoSlab) return 0;
+    s = p.next;
+  }
+  atomicOr(g.err, kErrTimeout);
+  return 0;
+}
+
+template <bool kWeighted, bool kDedupe, bool kInsert>
+__global__ void __launch_bounds__(256)
+    k_update_lane(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                  const uint32_t *__restrict__ w, uint32_t n,
+                  const unsigned long long *__restrict__ dd_keys,
+                  const uint32_t *__restrict__ dd_idx, uint32_t dd_mask,
+                  uint8_t *__restrict__ applied, unsigned long long *count) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nthreads = gridDim.x * blockDim.x;
+  uint32_t mine = 0;
+  for (uint64_t e = tid; e < n; e += nthreads) {
+    const UpdEdge E = upd_resolve<kWeighted, kDedupe, kInsert>(g, src, dst, w, n, e, dd_keys, dd_idx,
+                                                               dd_mask, applied);
+    if (E.head == kNoSlab) continue;
+    uint4 q[8];
+    lane_load_slab(g, E.head, q);
+    const uint32_t app = kInsert ? lane_insert_chain<kWeighted>(g, E.head, q, E.v, E.wt)
+                                 : lane_delete_chain<kWeighted>(g, E.head, q, E.v);
+    applied[e] = (uint8_t)app;
+    if (app) {
+      if (kInsert)
+        atomicAdd(g.deg + E.u, 1u);
+      else
+        atomicSub(g.deg + E.u, 1u);
+      ++mine;
+    }
+  }
+  mine = __reduce_add_sync(0xFFFFFFFFu, mine);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(count, (unsigned long long)mine);
 }
 
 template <bool kWeighted>
@@ -637,12 +819,35 @@ __global__ void k_bucket_fill(GraphView g, const unsigned long long *__restrict_
 }
 
 static int update_grid(uint32_t n, int device) {
-  // one warp per 32 edges, capped at the resident block count
-  uint64_t blocks = ((uint64_t)n + kUpdBlock - 1) / kUpdBlock;
-  uint64_t cap = (uint64_t)device_sm_count(device) * 8;
+  // one warp per 32 edges, at most the resident blocks (each warp loops)
+  uint64_t blocks = ((uint64_t)n + kUpdWarps * 32 - 1) / (kUpdWarps * 32);
+  uint64_t cap = (uint64_t)device_sm_count(device) * 6;  // 6 x 32 KB stages per SM
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   return (int)blocks;
+}
+
+static int lane_grid(uint32_t n, const mk_graph *g) {
+  // one lane per edge; 256-thread blocks, capped at the resident count
+  uint64_t blocks = ((uint64_t)n + 255) / 256;
+  uint32_t per_sm = g->tuning.update_blocks_per_sm ? g->tuning.update_blocks_per_sm : 6;
+  uint64_t cap = (uint64_t)device_sm_count(g->device) * per_sm;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
+// Opts a kernel into kUpdSmem of dynamic shared memory, once per device.
+template <class K>
+static mk_status set_update_smem(K kernel) {
+  static std::atomic<uint64_t> done{0};  // bit per device ordinal
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done.load(std::memory_order_acquire) & bit) return MK_OK;
+  MK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdSmem));
+  done.fetch_or(bit, std::memory_order_acq_rel);
+  return MK_OK;
 }
 
 static int group_grid(uint32_t n, int device) {
@@ -823,13 +1028,23 @@ mk_status mk_graph_insert_edges(mk_graph *g, const uint32_t *d_src,
     const uint32_t *kd = g->reverse ? d_src : d_dst;
     k_dedupe_elect<<<(n + 255) / 256, 256, 0, s>>>(v, ks, kd, n, g->dd_keys.ptr,
                                                    g->dd_idx.ptr, cap - 1);
-    k_update<true, true, true><<<blocks, kUpdBlock, 0, s>>>(
-        v, d_src, d_dst, d_w, n, g->dd_keys.ptr, g->dd_idx.ptr, cap - 1,
-        g->applied.ptr, g->counters);
+    if (g->tuning.update_kernel == 1) {
+      k_update_lane<true, true, true><<<lane_grid(n, g), 256, 0, s>>>(
+          v, d_src, d_dst, d_w, n, g->dd_keys.ptr, g->dd_idx.ptr, cap - 1, g->applied.ptr,
+          g->counters);
+    } else {
+      MK_CHECK(set_update_smem(k_update<true, true, true>));
+      k_update<true, true, true><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
+          v, d_src, d_dst, d_w, n, g->dd_keys.ptr, g->dd_idx.ptr, cap - 1, g->applied.ptr,
+          g->counters);
+    }
+  } else if (g->tuning.update_kernel == 1) {
+    k_update_lane<false, false, true><<<lane_grid(n, g), 256, 0, s>>>(
+        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
   } else {
-    k_update<false, false, true><<<blocks, kUpdBlock, 0, s>>>(
-        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr,
-        g->counters);
+    MK_CHECK(set_update_smem(k_update<false, false, true>));
+    k_update<false, false, true><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
+        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
   }
   MK_CUDA(cudaGetLastError());
   return MK_OK;
@@ -846,12 +1061,22 @@ mk_status mk_graph_delete_edges(mk_graph *g, const uint32_t *d_src,
   if (n == 0) return MK_OK;
   GraphView v = g->view();
   int blocks = update_grid(n, g->device);
-  if (g->weighted)
-    k_update<true, false, false><<<blocks, kUpdBlock, 0, s>>>(
+  if (g->tuning.update_kernel == 1) {
+    if (g->weighted)
+      k_update_lane<true, false, false><<<lane_grid(n, g), 256, 0, s>>>(
+          v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+    else
+      k_update_lane<false, false, false><<<lane_grid(n, g), 256, 0, s>>>(
+          v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+  } else if (g->weighted) {
+    MK_CHECK(set_update_smem(k_update<true, false, false>));
+    k_update<true, false, false><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
         v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
-  else
-    k_update<false, false, false><<<blocks, kUpdBlock, 0, s>>>(
+  } else {
+    MK_CHECK(set_update_smem(k_update<false, false, false>));
+    k_update<false, false, false><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
         v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+  }
   MK_CUDA(cudaGetLastError());
   return MK_OK;
 }
@@ -871,6 +1096,20 @@ mk_status mk_graph_search_edges(mk_graph *g, const uint32_t *d_src,
   else
     k_search<false><<<blocks, kUpdBlock, 0, s>>>(v, d_src, d_dst, n, d_found, d_w);
   MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
+mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t) {
+  if (!g || !t) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: null argument");
+  if (t->update_kernel > 1) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_kernel must be 0 or 1");
+  if (t->update_blocks_per_sm > 32) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_blocks_per_sm > 32");
+  g->tuning = *t;
+  return MK_OK;
+}
+
+mk_status mk_graph_get_tuning(mk_graph *g, mk_tuning *t) {
+  if (!g || !t) return fail(MK_ERR_INVALID, "mk_graph_get_tuning: null argument");
+  *t = g->tuning;
   return MK_OK;
 }
 

@@ -60,17 +60,19 @@ struct DevBuf {
 
 int device_sm_count(int device);
 
-// Scoped device switch.
+// Scoped device switch (one cudaGetDevice when the device is already current).
 struct DeviceGuard {
   int prev = -1;
+  bool switched = false;
   explicit DeviceGuard(int dev) {
     cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
+    if (prev != dev) {
+      cudaSetDevice(dev);
+      switched = true;
+    }
   }
   ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    if (switched && prev >= 0) cudaSetDevice(prev);
   }
 };
 
@@ -122,6 +124,7 @@ struct mk_graph {
   const uint32_t *last_dst = nullptr;
   int last_op = 0;  // 1 insert, 2 delete
   size_t device_bytes = 0;
+  mk_tuning tuning = {1u, 0u, 0u, 0u};
 
   mk::GraphView view() const {
     mk::GraphView v;

@@ -101,7 +101,7 @@ __device__ __forceinline__ void lane_keys(const uint4 &q, uint32_t gl,
 }
 
 template <bool kWeighted>
-constexpr int keys_per_lane() {
+__host__ __device__ constexpr int keys_per_lane() {
   return kWeighted ? 2 : 4;
 }
 

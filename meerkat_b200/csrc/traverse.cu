@@ -172,6 +172,69 @@ __device__ __forceinline__ void relax_slab(const TravArgs &a, const Lanes &L,
   }
 }
 
+// Relaxes the keys of up to 4 slab quarters at once: every dist word is
+// loaded before any is used, so a lane keeps up to 16 loads in flight.
+template <bool kW, bool kUseW>
+__device__ __forceinline__ void relax_slabs4(const TravArgs &a, const Lanes &L,
+                                             const BlockQueue &Q, const uint4 (&q)[4], uint32_t nq,
+                                             uint32_t u, uint32_t du, uint32_t stamp_next,
+                                             unsigned long long *gfr, uint32_t *gsz) {
+  constexpr int KP = keys_per_lane<kW>();
+  uint32_t k[4][4], w[4][4];
+  unsigned long long cur[4][KP];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    lane_keys<kW>(q[j], L.gl, k[j], w[j]);
+#pragma unroll
+    for (int i = 0; i < KP; ++i) {
+      const uint32_t v = k[j][i];
+      const bool live = (uint32_t)j < nq && v < kTombKey && v != u;
+      if (!live) k[j][i] = kEmptyKey;
+      cur[j][i] = live ? ld_dist(a.dist + v) : 0ull;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+#pragma unroll
+    for (int i = 0; i < KP; ++i) {
+      const uint32_t v = k[j][i];
+      if (v == kEmptyKey) continue;
+      const unsigned long long nd = (unsigned long long)du + (kUseW ? w[j][i] : 1u);
+      if (nd >= kInf || nd >= pack_hi(cur[j][i])) continue;
+      const unsigned long long old = atomicMin(a.dist + v, pack((uint32_t)nd, u));
+      if (pack_hi(old) > nd && atomicExch(a.stamp + v, stamp_next) != stamp_next)
+        push_vertex(a, Q, v, gfr, gsz);
+    }
+  }
+}
+
+// Expands buckets [b0, b1) of vertex u: head slabs 4 at a time (batched
+// relaxation), overflow chains slab by slab.
+template <bool kW, bool kUseW>
+__device__ __forceinline__ void expand_range(const TravArgs &a, const Lanes &L,
+                                             const BlockQueue &Q, uint32_t u, uint32_t du,
+                                             uint32_t b0, uint32_t b1, uint32_t stamp_next,
+                                             unsigned long long *gfr, uint32_t *gsz) {
+  for (uint32_t b = b0; b < b1; b += 4) {
+    const uint32_t nq = min(4u, b1 - b);
+    uint4 q[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      q[j] = ((uint32_t)j < nq) ? ld_slab_ro(a.g.slabs + 8ull * (b + j) + L.gl)
+                                : make_uint4(kEmptyKey, kEmptyKey, kEmptyKey, kNoSlab);
+    relax_slabs4<kW, kUseW>(a, L, Q, q, nq, u, du, stamp_next, gfr, gsz);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      uint32_t s = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
+      while (s != kNoSlab) {
+        const uint4 r = ld_slab_ro(a.g.slabs + 8ull * s + L.gl);
+        relax_slab<kW, kUseW>(a, L, Q, r, u, du, stamp_next, gfr, gsz, false);
+        s = __shfl_sync(L.gmask, r.w, L.gbase + 7);
+      }
+    }
+  }
+}
+
 // Bucket range of a work item.
 __device__ __forceinline__ void item_range(const GraphView &g, unsigned long long it,
                                            uint32_t &v, uint32_t &b0, uint32_t &b1) {
@@ -321,10 +384,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       if (L.gl == 0) pu = ld_dist(a.dist + u);
       pu = __shfl_sync(L.gmask, pu, L.gbase);
       if (pu == kInfInf) continue;
-      const uint32_t du = pack_hi(pu);
-      walk_buckets(a.g, L, b0, b1, [&](const uint4 &q) {
-        relax_slab<kW, kUseW>(a, L, Q, q, u, du, stamp_next, nxt, nsz, false);
-      });
+      expand_range<kW, kUseW>(a, L, Q, u, pack_hi(pu), b0, b1, stamp_next, nxt, nsz);
     }
     queue_flush(Q, nxt, nsz, a.pushed, &base_s);
     if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;

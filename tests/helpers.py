@@ -19,7 +19,7 @@ def degree_hints(src, V):
 
 
 def make_pair(V, src, dst, w=None, weighted=False, reverse=False, hints="exact",
-              load_factor=0.7, pool_slabs=0):
+              load_factor=0.7, pool_slabs=0, variant=None):
     """Builds the GPU graph and the oracle graph from the same edge list."""
     if hints == "exact":
         h = degree_hints(dst if reverse else src, V)
@@ -29,6 +29,8 @@ def make_pair(V, src, dst, w=None, weighted=False, reverse=False, hints="exact",
         h = hints
     G = mk.DynamicGraph(V, load_factor=load_factor, degree_hints=h, weighted=weighted,
                         reverse=reverse, pool_slabs=pool_slabs)
+    if variant is not None:
+        G.set_tuning(update_kernel=variant)
     O = OracleGraph(V)
     if len(src):
         s, d = to_dev(src), to_dev(dst)

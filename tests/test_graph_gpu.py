@@ -20,11 +20,15 @@ def rmat12():
     return mk.gen_rmat(12, 60000, seed=11, w_lo=1, w_hi=64)
 
 
+VARIANTS = [0, 1]  # update kernels: warp-staged TMA, lane per edge
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("weighted", [False, True])
 @pytest.mark.parametrize("hints", ["exact", "ones"])
-def test_degree_and_element(rmat12, weighted, hints):
+def test_degree_and_element(rmat12, weighted, hints, variant):
     s, d, w = rmat12
-    G, O = make_pair(V12, s, d, w, weighted=weighted, hints=hints)
+    G, O = make_pair(V12, s, d, w, weighted=weighted, hints=hints, variant=variant)
     assert G.last_applied() == len(s)
     assert_same_graph(G, O, weighted)
     info = G.info()
@@ -32,10 +36,11 @@ def test_degree_and_element(rmat12, weighted, hints):
     assert info["keys_per_slab"] == (15 if weighted else 31)
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("weighted", [False, True])
-def test_partial_delete(rmat12, weighted):
+def test_partial_delete(rmat12, weighted, variant):
     s, d, w = rmat12
-    G, O = make_pair(V12, s, d, w, weighted=weighted)
+    G, O = make_pair(V12, s, d, w, weighted=weighted, variant=variant)
     rng = np.random.default_rng(45)
     sel = rng.random(len(s)) < 0.45
     ds, dd = to_dev(s[sel]), to_dev(d[sel])
@@ -46,9 +51,10 @@ def test_partial_delete(rmat12, weighted):
     assert_same_graph(G, O, weighted)
 
 
-def test_full_delete_leaves_tombstones(rmat12):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_full_delete_leaves_tombstones(rmat12, variant):
     s, d, _ = rmat12
-    G, O = make_pair(V12, s, d)
+    G, O = make_pair(V12, s, d, variant=variant)
     deg0 = G.degrees().copy()
     G.DeleteEdges(to_dev(s), to_dev(d))
     assert G.sync() == 0
@@ -56,9 +62,11 @@ def test_full_delete_leaves_tombstones(rmat12):
     np.testing.assert_array_equal(G.tombstones(), deg0)
 
 
-def test_batch_semantics_weighted():
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_batch_semantics_weighted(variant):
     V = 16
-    G, O = make_pair(V, np.array([], np.uint32), np.array([], np.uint32), weighted=True)
+    G, O = make_pair(V, np.array([], np.uint32), np.array([], np.uint32), weighted=True,
+                     variant=variant)
     src = np.array([1, 2, 2, 3, 1, 4, 4, 4], np.uint32)
     dst = np.array([1, 3, 3, 4, 2, 5, 5, 6], np.uint32)
     w = np.array([5, 7, 8, 9, 2, 11, 12, 13], np.uint32)
@@ -125,12 +133,14 @@ def test_out_of_range_ids_report_invalid():
     assert_same_graph(G, O)
 
 
-def test_pool_exhaustion_reports_oom_and_stays_consistent():
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_pool_exhaustion_reports_oom_and_stays_consistent(variant):
     V = 64
     rng = np.random.default_rng(5)
     s = rng.integers(0, V, 4000).astype(np.uint32)
     d = rng.integers(0, V, 4000).astype(np.uint32)
     G = mk.DynamicGraph(V, degree_hints=None, pool_slabs=16)
+    G.set_tuning(update_kernel=variant)
     G.InsertEdges(to_dev(s), to_dev(d))
     with pytest.raises(mk.MeerkatError) as e:
         G.sync()
@@ -145,11 +155,12 @@ def test_pool_exhaustion_reports_oom_and_stays_consistent():
         assert u not in row
 
 
-def test_small_config_insert_delete():
-    """BASELINE small config: R-MAT s16, 1,048,576 edges, +10k absent, -10k present."""
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_small_config_insert_delete(variant):
+    """Small config: R-MAT s16, 1,048,576 edges, +10k absent, -10k present."""
     V = 1 << 16
     s, d, w = mk.gen_rmat(16, 1 << 20, seed=0x4D45524B, w_lo=1, w_hi=64)
-    G, O = make_pair(V, s, d, w, weighted=True, hints="ones")
+    G, O = make_pair(V, s, d, w, weighted=True, hints="ones", variant=variant)
     es = mk.EdgeSet(V, s, d)
     ins_s, ins_d = es.sample_absent(10000, seed=1)
     ins_w = (np.arange(10000, dtype=np.uint32) % 64) + 1
@@ -161,3 +172,11 @@ def test_small_config_insert_delete():
     assert G.sync() == 0 and G.last_applied() == 10000
     O.delete(del_s, del_d)
     assert_same_graph(G, O, weighted=True)
+
+
+def test_tuning_round_trip_and_validation():
+    G, _ = make_pair(64, np.array([1], np.uint32), np.array([2], np.uint32))
+    G.set_tuning(update_kernel=0, update_blocks_per_sm=3)
+    assert G.get_tuning() == {"update_kernel": 0, "update_blocks_per_sm": 3}
+    with pytest.raises(mk.MeerkatError):
+        G.set_tuning(update_kernel=7)
