@@ -263,6 +263,8 @@ def main():
     ap.add_argument("--scale", type=int, default=22,
                     help="R-MAT scale (22 = the benchmark config; smaller only for profiling)")
     ap.add_argument("--batch", type=int, default=500_000, help="edges per sub-batch")
+    ap.add_argument("--update-kernel", default="auto", choices=["auto", "0", "1"],
+                    help="auto = autotune on the first batches; 0/1 pins a variant")
     args = ap.parse_args()
     global SCALE, EDGES, HALF
     SCALE, EDGES, HALF = args.scale, 16 << args.scale, args.batch
@@ -300,7 +302,9 @@ def main():
 
     stream = torch.cuda.current_stream(dev)
     # autotune the update kernel on the first T batches (they are real updates)
-    tuning = tune_updates(G, [tuple(todev(x) for x in b) for b in batches[:T]], stream=stream)
+    variants = VARIANTS if args.update_kernel == "auto" else [(int(args.update_kernel), 0)] * T
+    tuning = tune_updates(G, [tuple(todev(x) for x in b) for b in batches[:T]], variants=variants,
+                          stream=stream)
     log(f"[bench] tuning: {tuning}")
     batches = batches[T:]
     dbatches = [tuple(todev(x) for x in b) for b in batches[:W + K]]

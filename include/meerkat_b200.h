@@ -91,9 +91,11 @@ mk_status mk_graph_destroy(mk_graph *g);
 
 /* InsertEdges(src*, dst*, n, vals*) (SlabGraph.cuh:486-488, impl
  * SlabGraphImpl.cuh:6-34).  Self-loops are skipped (InsertEdgeKernel.cuh:25).
- * Set semantics: an edge that is already live is left unchanged; of several
- * copies of one edge inside a batch the lowest batch index wins.  d_w may be
- * NULL (weight 0) and is ignored for unweighted graphs. */
+ * Set semantics: a live edge is never duplicated; on weighted graphs its
+ * stored weight becomes the minimum of the live weight and every inserted copy
+ * (upsert-min), which is independent of the order of concurrent inserts.  An
+ * entry counts as applied only when it adds a new edge.  d_w may be NULL
+ * (weight 0) and is ignored for unweighted graphs. */
 mk_status mk_graph_insert_edges(mk_graph *g, const uint32_t *d_src,
                                 const uint32_t *d_dst, const uint32_t *d_w,
                                 uint32_t n, void *stream);

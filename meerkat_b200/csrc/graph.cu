@@ -19,13 +19,16 @@
 //                            (include/Graph/warp/DeleteEdge.cuh:7-39)
 //   search                   (include/Graph/warp/SearchEdge.cuh:8-63)
 //
-// B200 design: one 8-lane group per batch edge reads a whole 128-B slab with
-// one 16-B load per lane (L2-coherent ld.global.cg), decides with two redux.sync
-// reductions, and commits with one CAS.  No sort, no locks: a key can only be
-// placed in the first EMPTY word of the chain, which makes concurrent inserts
-// of the same key collide on one word, so duplicates are impossible.  For
-// weighted graphs a batch-local hash table first elects the lowest batch index
-// of every repeated (u, v), so the stored weight is deterministic.
+// B200 design: a warp takes 32 batch edges; every lane resolves its edge to
+// the bucket's head slab and issues a 128-B TMA bulk copy of it (L2
+// evict_last) into the warp's shared-memory stage, double-buffered so the next
+// 32 edges' copies are in flight while these are decided.  Each lane then
+// decides alone from its staged slab and commits with one CAS.  No sort, no
+// locks: a key can only be placed in the first EMPTY word of the chain, which
+// makes concurrent inserts of the same key collide on one word, so duplicates
+// are impossible.  On weighted graphs the stored weight of an edge is the
+// minimum over its live value and every inserted copy (atomicMin on the value
+// word), so the result does not depend on the order of concurrent inserts.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -214,132 +217,6 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
   return x;
 }
 
-// Batch-local election of the first occurrence of each (u, v).
-__global__ void k_dedupe_elect(GraphView g, const uint32_t *__restrict__ src,
-                               const uint32_t *__restrict__ dst, uint32_t n,
-                               unsigned long long *keys, uint32_t *idx,
-                               uint32_t mask) {
-  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n) return;
-  uint32_t u = src[e], v = dst[e];
-  if (u == v || u >= g.V || v >= g.V) return;
-  unsigned long long key = ((unsigned long long)u << 32) | v;
-  uint32_t h = (uint32_t)mix64(key) & mask;
-  for (uint32_t it = 0; it <= mask; ++it) {
-    unsigned long long k = __ldcg(keys + h);
-    if (k == ~0ull) {
-      unsigned long long old = atomicCAS(keys + h, ~0ull, key);
-      if (old == ~0ull || old == key) {
-        atomicMin(idx + h, e);
-        return;
-      }
-    } else if (k == key) {
-      atomicMin(idx + h, e);
-      return;
-    }
-    h = (h + 1) & mask;
-  }
-}
-
-__device__ __forceinline__ bool dedupe_is_first(const unsigned long long *keys,
-                                                const uint32_t *idx, uint32_t mask,
-                                                uint32_t u, uint32_t v, uint32_t e) {
-  unsigned long long key = ((unsigned long long)u << 32) | v;
-  uint32_t h = (uint32_t)mix64(key) & mask;
-  for (uint32_t it = 0; it <= mask; ++it) {
-    unsigned long long k = keys[h];
-    if (k == key) return idx[h] == e;
-    if (k == ~0ull) return false;
-    h = (h + 1) & mask;
-  }
-  return false;
-}
-
-// Inserts key v into the chain starting at slab s whose first slab is
-// already loaded in q (possibly stale).  Returns 1 when this group stored the
-// key.  Group-cooperative; every lane of the group calls it.
-template <bool kWeighted>
-__device__ __forceinline__ uint32_t insert_chain(const GraphView &g, const Lanes &L, uint32_t s,
-                                                 uint4 q, uint32_t v, uint32_t wt) {
-  for (uint32_t it = 0; it < kProbeLimit; ++it) {
-    if (it) q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
-    bool found;
-    uint32_t fslot, eslot, next;
-    probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
-    if (found) return 0;
-    if (eslot != 255) {
-      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(eslot);
-      uint32_t old = 0;
-      if (L.gl == 0) {
-        old = atomicCAS(wp, kEmptyKey, v);
-        if (kWeighted && old == kEmptyKey) wp[1] = wt;
-      }
-      old = __shfl_sync(L.gmask, old, L.gbase);
-      if (old == kEmptyKey) return 1;
-      if (old == v) return 0;
-      continue;  // lost the word to another key: re-read this slab
-    }
-    if (next == kLinkBusy) {  // another group is extending this chain
-      __nanosleep(64);
-      continue;
-    }
-    if (next != kNoSlab) {
-      s = next;
-      continue;
-    }
-    // Chain is full: claim its next word, take a pool slab holding the key,
-    // then publish the link.  Racing groups see kLinkBusy and wait, so no slab
-    // is ever allocated and dropped.
-    uint32_t res = 0;  // 0 = retry, 1 = inserted, 2 = pool exhausted
-    if (L.gl == 0) {
-      uint32_t *nextp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + 31;
-      uint32_t prev = atomicCAS(nextp, kNoSlab, kLinkBusy);
-      if (prev == kNoSlab) {
-        uint32_t ns = atomicAdd(g.pool_top, 1u);
-        if (ns >= g.pool_cap) {
-          atomicOr(g.err, kErrOom);
-          atomicExch(nextp, kNoSlab);
-          res = 2;
-        } else {
-          uint32_t *np = reinterpret_cast<uint32_t *>(g.slabs + 8ull * ns);
-          np[0] = v;
-          if (kWeighted) np[1] = wt;
-          __threadfence();
-          atomicExch(nextp, ns);
-          res = 1;
-        }
-      }
-    }
-    res = __shfl_sync(L.gmask, res, L.gbase);
-    if (res == 2) return 0;
-    if (res == 1) return 1;
-  }
-  if (L.gl == 0) atomicOr(g.err, kErrTimeout);
-  return 0;
-}
-
-// Tombstones key v in the chain starting at s (first slab preloaded in q).
-template <bool kWeighted>
-__device__ __forceinline__ uint32_t delete_chain(const GraphView &g, const Lanes &L, uint32_t s,
-                                                 uint4 q, uint32_t v) {
-  for (uint32_t it = 0; it < kProbeLimit; ++it) {
-    if (it) q = ld_slab_cg(g.slabs + 8ull * s + L.gl);
-    bool found;
-    uint32_t fslot, eslot, next;
-    probe_slab<kWeighted>(q, v, L, found, fslot, eslot, next);
-    if (found) {
-      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + slot_word<kWeighted>(fslot);
-      uint32_t old = 0;
-      if (L.gl == 0) old = atomicCAS(wp, v, kTombKey);
-      old = __shfl_sync(L.gmask, old, L.gbase);
-      return old == v ? 1u : 0u;
-    }
-    if (next == kNoSlab) return 0;
-    s = next;
-  }
-  if (L.gl == 0) atomicOr(g.err, kErrTimeout);
-  return 0;
-}
 
 // Update kernels.  A warp takes 32 batch edges at a time:
 //   1. every lane resolves its edge to the bucket's head slab;
@@ -347,31 +224,24 @@ __device__ __forceinline__ uint32_t delete_chain(const GraphView &g, const Lanes
 //      warp's shared-memory stage (completion on the stage's mbarrier), and
 //      the warp moves on to resolve its next 32 edges into the other stage
 //      while the copies are in flight (double buffering);
-//   3. each 8-lane group analyses 8 staged slabs (redux.sync) and hands every
-//      decision to the lane that owns the edge;
-//   4. the owning lanes issue their CASes together (one warp instruction);
-//   5. edges whose CAS lost a race, whose chain continues or that need a new
-//      slab take the group-cooperative chain walk.
-// A staged slab that went stale only costs the slow path: inside one insert
-// call key words only move EMPTY -> key, inside one delete call only
-// key -> TOMBSTONE.
-constexpr int kRounds = 8;
+//   3. each lane decides from its staged slab (144-B stride: conflict-free
+//      reads) and commits with one CAS;
+//   4. a lane whose CAS lost a race, whose chain continues or that needs a
+//      new slab walks the chain itself from global memory.
+// A staged slab that went stale only costs step 4: inside one insert call key
+// words only move EMPTY -> key, inside one delete call only key -> TOMBSTONE.
 constexpr int kUpdWarps = 4;  // warps per block
-constexpr uint32_t kActNoop = 0x100;  // key already present (insert) / absent (delete)
-constexpr uint32_t kActSlow = 0x200;  // needs the chain walk
-constexpr uint32_t kActSkip = 0x300;  // lane has no edge
-constexpr size_t kUpdSmem = (size_t)kUpdWarps * 2 * 32 * 128;  // 2 stages x 32 slabs per warp
+constexpr size_t kStageStride = 9;  // uint4 per staged slab: 128 B + 16 B pad
+constexpr size_t kUpdSmem = (size_t)kUpdWarps * 2 * 32 * kStageStride * 16;  // 2 stages x 32 slabs per warp
 
 struct UpdEdge {
   uint32_t u, v, wt, head;
 };
 
-template <bool kWeighted, bool kDedupe, bool kInsert>
+template <bool kWeighted, bool kInsert>
 __device__ __forceinline__ UpdEdge upd_resolve(const GraphView &g, const uint32_t *__restrict__ src,
                                                const uint32_t *__restrict__ dst,
                                                const uint32_t *__restrict__ w, uint32_t n, uint64_t e,
-                                               const unsigned long long *__restrict__ dd_keys,
-                                               const uint32_t *__restrict__ dd_idx, uint32_t dd_mask,
                                                uint8_t *__restrict__ applied) {
   UpdEdge E{0u, 0u, 0u, kNoSlab};
   if (e < n) {
@@ -392,145 +262,11 @@ __device__ __forceinline__ UpdEdge upd_resolve(const GraphView &g, const uint32_
     if (ok) {
       const uint32_t b0 = g.boff[u];
       const uint32_t b1 = g.boff[u + 1];
-      if (kDedupe) ok = dedupe_is_first(dd_keys, dd_idx, dd_mask, u, v, (uint32_t)e);
       if (ok) E.head = b0 + bucket_of(v, b1 - b0);
     }
     if (!ok) applied[e] = 0;
   }
   return E;
-}
-
-template <bool kWeighted, bool kDedupe, bool kInsert>
-__global__ void __launch_bounds__(kUpdWarps * 32)
-    k_update(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
-             const uint32_t *__restrict__ w, uint32_t n,
-             const unsigned long long *__restrict__ dd_keys, const uint32_t *__restrict__ dd_idx,
-             uint32_t dd_mask, uint8_t *__restrict__ applied, unsigned long long *count) {
-  extern __shared__ __align__(128) uint4 stage_smem[];
-  __shared__ __align__(8) uint64_t bars[kUpdWarps][2];
-  const Lanes L = lanes();
-  const uint32_t wib = threadIdx.x >> 5;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  uint4 *wst = stage_smem + (size_t)wib * 2 * 32 * 8;  // [stage][slab][quarter]
-  if (L.lane == 0) {
-    mbar_init(&bars[wib][0], 1);
-    mbar_init(&bars[wib][1], 1);
-    mbar_init_fence();
-  }
-  __syncwarp();
-  uint32_t parity[2] = {0u, 0u};
-  uint32_t mine = 0;
-
-  // stage the head slabs of edge record E into stage st
-  auto issue = [&](const UpdEdge &E, uint32_t st) {
-    const uint32_t valid = __ballot_sync(0xFFFFFFFFu, E.head != kNoSlab);
-    fence_proxy_async_smem();  // this warp's earlier reads of the buffer come first
-    __syncwarp();
-    if (L.lane == 0) mbar_arrive_expect_tx(&bars[wib][st], 128u * __popc(valid));
-    __syncwarp();
-    if (E.head != kNoSlab)
-      bulk_load(wst + ((size_t)st * 32 + L.lane) * 8, g.slabs + 8ull * E.head, 128u, &bars[wib][st]);
-  };
-
-  uint64_t base = (uint64_t)warp * 32;
-  if (base >= n) return;
-  UpdEdge cur = upd_resolve<kWeighted, kDedupe, kInsert>(g, src, dst, w, n, base + L.lane, dd_keys,
-                                                         dd_idx, dd_mask, applied);
-  uint32_t st = 0;
-  issue(cur, st);
-  for (;;) {
-    const uint64_t nbase = base + (uint64_t)nwarps * 32;
-    const bool has_next = nbase < n;
-    UpdEdge nxt{0u, 0u, 0u, kNoSlab};
-    if (has_next) {
-      nxt = upd_resolve<kWeighted, kDedupe, kInsert>(g, src, dst, w, n, nbase + L.lane, dd_keys,
-                                                     dd_idx, dd_mask, applied);
-      issue(nxt, st ^ 1u);
-    }
-    const bool ready = mbar_wait(&bars[wib][st], parity[st], g.err);
-    parity[st] ^= 1u;
-    // decisions per round, delivered to the owning lanes
-    uint32_t my_act = kActSkip;
-#pragma unroll
-    for (int r = 0; r < kRounds; ++r) {
-      const uint32_t sl = 4 * r + L.grp;
-      const uint32_t hs = __shfl_sync(0xFFFFFFFFu, cur.head, sl);
-      const uint32_t vv = __shfl_sync(0xFFFFFFFFu, cur.v, sl);
-      uint32_t act = kActSkip;
-      if (hs != kNoSlab) {
-        if (ready) {
-          const uint4 q = wst[((size_t)st * 32 + sl) * 8 + L.gl];
-          bool found;
-          uint32_t fslot, eslot, next;
-          probe_slab<kWeighted>(q, vv, L, found, fslot, eslot, next);
-          if (kInsert)
-            act = found ? kActNoop : (eslot != 255 ? eslot : kActSlow);
-          else
-            act = found ? fslot : (next == kNoSlab ? kActNoop : kActSlow);
-        } else {
-          act = kActSlow;
-        }
-      }
-      const uint32_t t = __shfl_sync(0xFFFFFFFFu, act, (L.lane & 3u) * 8u);
-      if ((L.lane >> 2) == (uint32_t)r) my_act = t;
-    }
-    // one CAS per owning lane, all issued together
-    uint32_t app = 0;
-    bool slow = (my_act == kActSlow);
-    if (my_act < 255) {
-      uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * cur.head) + slot_word<kWeighted>(my_act);
-      if (kInsert) {
-        const uint32_t old = atomicCAS(wp, kEmptyKey, cur.v);
-        if (old == kEmptyKey) {
-          app = 1;
-          if (kWeighted) wp[1] = cur.wt;
-        } else if (old != cur.v) {
-          slow = true;  // lost the word to another key
-        }
-      } else {
-        app = (atomicCAS(wp, cur.v, kTombKey) == cur.v) ? 1u : 0u;
-      }
-    }
-    // slow path, round by round, group-cooperative (reads global memory)
-    const uint32_t slow_mask = __ballot_sync(0xFFFFFFFFu, slow);
-    if (slow_mask) {
-#pragma unroll 1
-      for (int r = 0; r < kRounds; ++r) {
-        const uint32_t sl = 4 * r + L.grp;
-        const uint32_t hs = __shfl_sync(0xFFFFFFFFu, cur.head, sl);
-        const uint32_t vv = __shfl_sync(0xFFFFFFFFu, cur.v, sl);
-        const uint32_t ww = __shfl_sync(0xFFFFFFFFu, cur.wt, sl);
-        uint32_t res = 0;
-        if ((slow_mask >> sl) & 1u) {
-          const uint4 q0 = ld_slab_cg(g.slabs + 8ull * hs + L.gl);
-          res = kInsert ? insert_chain<kWeighted>(g, L, hs, q0, vv, ww)
-                        : delete_chain<kWeighted>(g, L, hs, q0, vv);
-        }
-        __syncwarp();
-        const uint32_t t = __shfl_sync(0xFFFFFFFFu, res, (L.lane & 3u) * 8u);
-        if ((L.lane >> 2) == (uint32_t)r && slow) app = t;
-      }
-    }
-    // owning lane publishes the outcome
-    if (cur.head != kNoSlab) {
-      applied[base + L.lane] = (uint8_t)app;
-      if (app) {
-        if (kInsert)
-          atomicAdd(g.deg + cur.u, 1u);
-        else
-          atomicSub(g.deg + cur.u, 1u);
-        ++mine;
-      }
-    }
-    if (!has_next) break;
-    __syncwarp();
-    cur = nxt;
-    base = nbase;
-    st ^= 1u;
-  }
-  mine = __reduce_add_sync(0xFFFFFFFFu, mine);
-  if (L.lane == 0 && mine) atomicAdd(count, (unsigned long long)mine);
 }
 
 // ---------------------------------------------------------------------------
@@ -576,15 +312,20 @@ __device__ uint32_t lane_insert_chain(const GraphView &g, uint32_t s, uint4 (&q)
   for (uint32_t it = 0; it < kProbeLimit; ++it) {
     if (it) lane_load_slab(g, s, q);
     const LaneProbe p = lane_probe<kWeighted>(q, v);
-    if (p.found_word < 32) return 0;
+    if (p.found_word < 32) {
+      // live edge: weighted graphs keep the smaller weight (upsert-min)
+      if (kWeighted) atomicMin(reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + p.found_word + 1, wt);
+      return 0;
+    }
     if (p.empty_word < 32) {
       uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + p.empty_word;
       const uint32_t old = atomicCAS(wp, kEmptyKey, v);
-      if (old == kEmptyKey) {
-        if (kWeighted) wp[1] = wt;
-        return 1;
+      if (old == kEmptyKey || old == v) {
+        // the value word of a never-used slot is EMPTY (0xFFFFFFFF), so
+        // atomicMin leaves the minimum over every concurrent copy
+        if (kWeighted) atomicMin(wp + 1, wt);
+        return old == kEmptyKey ? 1u : 0u;
       }
-      if (old == v) return 0;
       continue;
     }
     if (p.next == kLinkBusy) {
@@ -631,19 +372,97 @@ __device__ uint32_t lane_delete_chain(const GraphView &g, uint32_t s, uint4 (&q)
   return 0;
 }
 
-template <bool kWeighted, bool kDedupe, bool kInsert>
+template <bool kWeighted, bool kInsert>
+__global__ void __launch_bounds__(kUpdWarps * 32)
+    k_update(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+             const uint32_t *__restrict__ w, uint32_t n, uint8_t *__restrict__ applied,
+             unsigned long long *count) {
+  extern __shared__ __align__(128) uint4 stage_smem[];
+  __shared__ __align__(8) uint64_t bars[kUpdWarps][2];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t wib = threadIdx.x >> 5;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  // [stage][lane] slabs of kStageStride uint4 (144 B: conflict-free lane reads)
+  uint4 *wst = stage_smem + (size_t)wib * 2 * 32 * kStageStride;
+  if (lane == 0) {
+    mbar_init(&bars[wib][0], 1);
+    mbar_init(&bars[wib][1], 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  const unsigned long long pol = l2_policy_evict_last();
+  uint32_t parity[2] = {0u, 0u};
+  uint32_t mine = 0;
+
+  // stage the head slab of this lane's edge into stage st
+  auto issue = [&](const UpdEdge &E, uint32_t st) {
+    const uint32_t valid = __ballot_sync(0xFFFFFFFFu, E.head != kNoSlab);
+    fence_proxy_async_smem();  // this warp's earlier reads of the buffer come first
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(&bars[wib][st], 128u * __popc(valid));
+    __syncwarp();
+    if (E.head != kNoSlab)
+      bulk_load_hint(wst + ((size_t)st * 32 + lane) * kStageStride, g.slabs + 8ull * E.head, 128u,
+                     &bars[wib][st], pol);
+  };
+
+  uint64_t base = (uint64_t)warp * 32;
+  if (base >= n) return;
+  UpdEdge cur = upd_resolve<kWeighted, kInsert>(g, src, dst, w, n, base + lane, applied);
+  uint32_t st = 0;
+  issue(cur, st);
+  for (;;) {
+    const uint64_t nbase = base + (uint64_t)nwarps * 32;
+    const bool has_next = nbase < n;
+    UpdEdge nxt{0u, 0u, 0u, kNoSlab};
+    if (has_next) {
+      nxt = upd_resolve<kWeighted, kInsert>(g, src, dst, w, n, nbase + lane, applied);
+      issue(nxt, st ^ 1u);
+    }
+    const bool ready = mbar_wait(&bars[wib][st], parity[st], g.err);
+    parity[st] ^= 1u;
+    if (cur.head != kNoSlab) {
+      // the lane decides alone from its staged slab, then commits
+      uint4 q[8];
+      const uint4 *sp = wst + ((size_t)st * 32 + lane) * kStageStride;
+      if (ready) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) q[j] = sp[j];
+      } else {
+        lane_load_slab(g, cur.head, q);
+      }
+      const uint32_t app = kInsert ? lane_insert_chain<kWeighted>(g, cur.head, q, cur.v, cur.wt)
+                                   : lane_delete_chain<kWeighted>(g, cur.head, q, cur.v);
+      applied[base + lane] = (uint8_t)app;
+      if (app) {
+        if (kInsert)
+          atomicAdd(g.deg + cur.u, 1u);
+        else
+          atomicSub(g.deg + cur.u, 1u);
+        ++mine;
+      }
+    }
+    if (!has_next) break;
+    __syncwarp();
+    cur = nxt;
+    base = nbase;
+    st ^= 1u;
+  }
+  mine = __reduce_add_sync(0xFFFFFFFFu, mine);
+  if (lane == 0 && mine) atomicAdd(count, (unsigned long long)mine);
+}
+
+template <bool kWeighted, bool kInsert>
 __global__ void __launch_bounds__(256)
     k_update_lane(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
-                  const uint32_t *__restrict__ w, uint32_t n,
-                  const unsigned long long *__restrict__ dd_keys,
-                  const uint32_t *__restrict__ dd_idx, uint32_t dd_mask,
-                  uint8_t *__restrict__ applied, unsigned long long *count) {
+                  const uint32_t *__restrict__ w, uint32_t n, uint8_t *__restrict__ applied,
+                  unsigned long long *count) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
   uint32_t mine = 0;
   for (uint64_t e = tid; e < n; e += nthreads) {
-    const UpdEdge E = upd_resolve<kWeighted, kDedupe, kInsert>(g, src, dst, w, n, e, dd_keys, dd_idx,
-                                                               dd_mask, applied);
+    const UpdEdge E = upd_resolve<kWeighted, kInsert>(g, src, dst, w, n, e, applied);
     if (E.head == kNoSlab) continue;
     uint4 q[8];
     lane_load_slab(g, E.head, q);
@@ -972,8 +791,6 @@ mk_status mk_graph_destroy(mk_graph *g) {
   if (g->pool_top) cudaFree(g->pool_top);
   if (g->counters) cudaFree(g->counters);
   g->applied.release();
-  g->dd_keys.release();
-  g->dd_idx.release();
   g->scan_tmp.release();
   g->bucket_cnt.release();
   g->bucket_pos.release();
@@ -985,12 +802,6 @@ mk_status mk_graph_reserve_batch(mk_graph *g, uint32_t n) {
   if (!g) return fail(MK_ERR_INVALID, "mk_graph_reserve_batch: null graph");
   DeviceGuard dg(g->device);
   MK_CHECK(g->applied.reserve(std::max<uint32_t>(n, 1), &g->device_bytes));
-  if (g->weighted) {
-    uint32_t cap = 1024;
-    while (cap < 2ull * n) cap <<= 1;
-    MK_CHECK(g->dd_keys.reserve(cap, &g->device_bytes));
-    MK_CHECK(g->dd_idx.reserve(cap, &g->device_bytes));
-  }
   return MK_OK;
 }
 
@@ -1017,34 +828,21 @@ mk_status mk_graph_insert_edges(mk_graph *g, const uint32_t *d_src,
   if (n == 0) return MK_OK;
   GraphView v = g->view();
   int blocks = update_grid(n, g->device);
-  if (g->weighted) {
-    uint32_t cap = 1024;
-    while (cap < 2ull * n) cap <<= 1;
-    MK_CHECK(g->dd_keys.reserve(cap, &g->device_bytes));
-    MK_CHECK(g->dd_idx.reserve(cap, &g->device_bytes));
-    MK_CUDA(cudaMemsetAsync(g->dd_keys.ptr, 0xFF, (size_t)cap * 8, s));
-    MK_CUDA(cudaMemsetAsync(g->dd_idx.ptr, 0xFF, (size_t)cap * 4, s));
-    const uint32_t *ks = g->reverse ? d_dst : d_src;
-    const uint32_t *kd = g->reverse ? d_src : d_dst;
-    k_dedupe_elect<<<(n + 255) / 256, 256, 0, s>>>(v, ks, kd, n, g->dd_keys.ptr,
-                                                   g->dd_idx.ptr, cap - 1);
-    if (g->tuning.update_kernel == 1) {
-      k_update_lane<true, true, true><<<lane_grid(n, g), 256, 0, s>>>(
-          v, d_src, d_dst, d_w, n, g->dd_keys.ptr, g->dd_idx.ptr, cap - 1, g->applied.ptr,
-          g->counters);
-    } else {
-      MK_CHECK(set_update_smem(k_update<true, true, true>));
-      k_update<true, true, true><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
-          v, d_src, d_dst, d_w, n, g->dd_keys.ptr, g->dd_idx.ptr, cap - 1, g->applied.ptr,
-          g->counters);
-    }
-  } else if (g->tuning.update_kernel == 1) {
-    k_update_lane<false, false, true><<<lane_grid(n, g), 256, 0, s>>>(
-        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+  if (g->tuning.update_kernel == 1) {
+    if (g->weighted)
+      k_update_lane<true, true><<<lane_grid(n, g), 256, 0, s>>>(v, d_src, d_dst, d_w, n,
+                                                                g->applied.ptr, g->counters);
+    else
+      k_update_lane<false, true><<<lane_grid(n, g), 256, 0, s>>>(v, d_src, d_dst, nullptr, n,
+                                                                 g->applied.ptr, g->counters);
+  } else if (g->weighted) {
+    MK_CHECK(set_update_smem(k_update<true, true>));
+    k_update<true, true><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(v, d_src, d_dst, d_w, n,
+                                                                  g->applied.ptr, g->counters);
   } else {
-    MK_CHECK(set_update_smem(k_update<false, false, true>));
-    k_update<false, false, true><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
-        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+    MK_CHECK(set_update_smem(k_update<false, true>));
+    k_update<false, true><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(v, d_src, d_dst, nullptr, n,
+                                                                   g->applied.ptr, g->counters);
   }
   MK_CUDA(cudaGetLastError());
   return MK_OK;
@@ -1063,19 +861,19 @@ mk_status mk_graph_delete_edges(mk_graph *g, const uint32_t *d_src,
   int blocks = update_grid(n, g->device);
   if (g->tuning.update_kernel == 1) {
     if (g->weighted)
-      k_update_lane<true, false, false><<<lane_grid(n, g), 256, 0, s>>>(
-          v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+      k_update_lane<true, false><<<lane_grid(n, g), 256, 0, s>>>(v, d_src, d_dst, nullptr, n,
+                                                                 g->applied.ptr, g->counters);
     else
-      k_update_lane<false, false, false><<<lane_grid(n, g), 256, 0, s>>>(
-          v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+      k_update_lane<false, false><<<lane_grid(n, g), 256, 0, s>>>(v, d_src, d_dst, nullptr, n,
+                                                                  g->applied.ptr, g->counters);
   } else if (g->weighted) {
-    MK_CHECK(set_update_smem(k_update<true, false, false>));
-    k_update<true, false, false><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
-        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+    MK_CHECK(set_update_smem(k_update<true, false>));
+    k_update<true, false><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(v, d_src, d_dst, nullptr, n,
+                                                                   g->applied.ptr, g->counters);
   } else {
-    MK_CHECK(set_update_smem(k_update<false, false, false>));
-    k_update<false, false, false><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(
-        v, d_src, d_dst, nullptr, n, nullptr, nullptr, 0, g->applied.ptr, g->counters);
+    MK_CHECK(set_update_smem(k_update<false, false>));
+    k_update<false, false><<<blocks, kUpdWarps * 32, kUpdSmem, s>>>(v, d_src, d_dst, nullptr, n,
+                                                                    g->applied.ptr, g->counters);
   }
   MK_CUDA(cudaGetLastError());
   return MK_OK;

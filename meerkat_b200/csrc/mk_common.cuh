@@ -202,6 +202,22 @@ __device__ __forceinline__ void bulk_load(void *dst_smem, const void *src_gmem, 
       "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
+// L2 policy that keeps lines resident (used for slabs that are about to be
+// updated with an atomic right after the bulk copy).
+__device__ __forceinline__ unsigned long long l2_policy_evict_last() {
+  unsigned long long pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// Bulk copy global -> shared with an L2 cache policy (no multicast).
+__device__ __forceinline__ void bulk_load_hint(void *dst_smem, const void *src_gmem, uint32_t bytes,
+                                               uint64_t *bar, unsigned long long policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+      "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst_smem)),
+      "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
 // Orders this thread's earlier generic-proxy shared accesses before later
 // async-proxy (TMA) writes to the same buffer.
 __device__ __forceinline__ void fence_proxy_async_smem() {

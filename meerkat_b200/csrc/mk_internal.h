@@ -114,8 +114,6 @@ struct mk_graph {
   unsigned long long *counters = nullptr;  // [0] applied count of last update
   // per-batch scratch
   mk::DevBuf<uint8_t> applied;     // per-edge applied flags of the last update
-  mk::DevBuf<unsigned long long> dd_keys;  // weighted-insert dedupe table
-  mk::DevBuf<uint32_t> dd_idx;
   mk::DevBuf<unsigned long long> scan_tmp;
   mk::DevBuf<uint32_t> bucket_cnt;             // export / orientation scratch
   mk::DevBuf<unsigned long long> bucket_pos;

@@ -17,9 +17,11 @@
  *
  * Semantics restated (reference file:line):
  *   insert  skip self loops (include/Graph/device/InsertEdgeKernel.cuh:21-26);
- *           an edge already present is left unchanged (set semantics of the
- *           slab-hash insertKey, include/Graph/warp/InsertEdge.cuh:86-98);
- *           the first copy of a repeated edge in one batch wins.
+ *           an edge already present is not duplicated (set semantics of the
+ *           slab-hash insertKey, include/Graph/warp/InsertEdge.cuh:86-98); on
+ *           weighted graphs the stored weight becomes the minimum of the live
+ *           weight and every inserted copy (upsert-min; the reference's
+ *           weighted insertPair duplicates keys, which is unpinned).
  *   delete  a present edge is removed, absent ones ignored
  *           (include/Graph/warp/DeleteEdge.cuh:7-39).
  *   BFS     hop levels from the source (BFSImpl.cuh:498-588), MK_INF for
@@ -163,7 +165,10 @@ static int og_insert_one(og *g, omap *m, uint32_t u, uint32_t v, uint32_t w) {
   uint64_t k = ((uint64_t)u << 32) | v;
   if ((m->size + 1) * 2 > m->cap) omap_grow(m);
   uint64_t p = omap_slot(m, k);
-  if (m->keys[p] == k) return 0;
+  if (m->keys[p] == k) { /* live edge: keep the smaller weight (upsert-min) */
+    if (w < m->wt[p]) m->wt[p] = w;
+    return 0;
+  }
   m->keys[p] = k;
   m->wt[p] = w;
   m->pos[p] = g->adj[u].n;

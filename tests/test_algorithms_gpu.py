@@ -152,16 +152,17 @@ def test_traversals_grid_high_diameter():
 
 
 def test_incremental_with_stale_batch_entries():
-    """Batch entries that did not change the graph (already present with a
-    different weight, self loops) must not seed distances."""
+    """Incremental SSSP seeds from the stored edges, not from the batch: an
+    entry for a live edge with a larger weight changes nothing, one with a
+    smaller weight lowers the edge (upsert-min), self loops are ignored."""
     V = 6
     G, O = make_pair(V, np.array([0, 1, 2], np.uint32), np.array([1, 2, 3], np.uint32),
                      np.array([10, 10, 10], np.uint32), weighted=True)
     sssp = mk.SSSP(G, 0, V)
     sssp.Static()
-    bs = np.array([0, 0, 4, 3], np.uint32)
-    bd = np.array([2, 1, 4, 5], np.uint32)
-    bw = np.array([3, 1, 1, 1], np.uint32)  # (0,1) already live with weight 10
+    bs = np.array([0, 0, 4, 3, 1], np.uint32)
+    bd = np.array([2, 1, 4, 5, 2], np.uint32)
+    bw = np.array([3, 1, 1, 1, 50], np.uint32)  # (0,1) live with weight 10, (1,2) too
     tbs, tbd, tbw = to_dev(bs), to_dev(bd), to_dev(bw)
     G.InsertEdges(tbs, tbd, vals=tbw)
     assert G.sync() == 0

@@ -76,9 +76,14 @@ def test_batch_semantics_weighted(variant):
     n, ap = O.insert(src, dst, w)
     assert G.last_applied() == n == 5
     assert_same_graph(G, O, weighted=True)
-    # re-insert of live edges with new weights: no-op
+    # re-insert of live edges with larger weights: nothing changes
     G.InsertEdges(to_dev([2, 4]), to_dev([3, 5]), vals=to_dev([100, 100]))
     assert G.sync() == 0 and G.last_applied() == 0
+    assert_same_graph(G, O, weighted=True)
+    # with smaller weights (several copies in one batch): the minimum is kept
+    G.InsertEdges(to_dev([4, 2, 4, 4]), to_dev([5, 3, 5, 6]), vals=to_dev([9, 3, 4, 20]))
+    assert G.sync() == 0 and G.last_applied() == 0
+    O.insert([4, 2, 4, 4], [5, 3, 5, 6], [9, 3, 4, 20])
     assert_same_graph(G, O, weighted=True)
     # delete absent, self loop, duplicate
     dsrc = np.array([2, 2, 7, 1], np.uint32)

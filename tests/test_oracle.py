@@ -41,17 +41,23 @@ def test_oracle_matches_golden(gold, threads):
 
 def test_insert_semantics_known_answers():
     g = OracleGraph(8)
-    # self loop skipped, duplicate in batch: first copy wins, out-of-range skipped
+    # self loop skipped, duplicate in batch: one edge with the smaller weight,
+    # out-of-range skipped
     n, ap = g.insert([1, 2, 2, 3, 9, 1], [1, 3, 3, 4, 0, 2], [5, 7, 8, 9, 1, 2])
     assert n == 3
     assert ap.tolist() == [0, 1, 0, 1, 0, 1]
     rp, col, w = g.csr(weights=True)
     assert col.tolist() == [2, 3, 4] and w.tolist() == [2, 7, 9]
-    # re-insert of a live edge is a no-op and keeps the old weight
+    # re-insert of a live edge adds nothing; a larger weight changes nothing
     n, ap = g.insert([2], [3], [100])
     assert n == 0 and ap.tolist() == [0]
     _, _, w = g.csr(weights=True)
     assert w.tolist() == [2, 7, 9]
+    # ... and a smaller one lowers it (upsert-min)
+    n, ap = g.insert([3, 3], [4, 4], [6, 5])
+    assert n == 0 and ap.tolist() == [0, 0]
+    _, _, w = g.csr(weights=True)
+    assert w.tolist() == [2, 7, 5]
     assert g.degrees().tolist() == [0, 1, 1, 1, 0, 0, 0, 0]
 
 
