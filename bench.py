@@ -438,7 +438,7 @@ def main():
             "config": config_block(world),
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": 3 * K,
+            "gpu_launches": 2 * K,  # one delete and one insert kernel per step
             "roofline": {"bound": "hbm", "kernel": "k_update delete + insert (one mixed batch, graph replay)",
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak,

@@ -145,8 +145,9 @@ typedef struct mk_tuning {
   uint32_t update_kernel;        /* 0 = warp-staged (TMA bulk copies into shared
                                     memory), 1 = one lane per edge             */
   uint32_t update_blocks_per_sm; /* resident blocks per SM, 0 = automatic     */
-  uint32_t reserved0;
-  uint32_t reserved1;
+  uint32_t frontier_chunk;       /* buckets per BFS/SSSP frontier work item,
+                                    1..1024, 0 = 4                            */
+  uint32_t reserved;
 } mk_tuning;
 mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t);
 mk_status mk_graph_get_tuning(mk_graph *g, mk_tuning *t);
@@ -164,6 +165,15 @@ typedef struct mk_traversal mk_traversal;
 mk_status mk_bfs_create(mk_graph *g, uint32_t source, mk_traversal **out);
 /* SSSP(G, SourceVertex, VertexN) (SSSP.cuh:33-52). */
 mk_status mk_sssp_create(mk_graph *g, uint32_t source, mk_traversal **out);
+/* One traversal from several distinct sources at once (no counterpart in the
+ * reference): every vertex gets its distance from the nearest source.  On a
+ * graph set (below) with one source per member graph this runs one query per
+ * member in a single launch.  h_sources is host memory; repeated or
+ * out-of-range sources are rejected. */
+mk_status mk_bfs_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n,
+                              mk_traversal **out);
+mk_status mk_sssp_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n,
+                               mk_traversal **out);
 /* float Static(EdgesN) (BFSImpl.cuh:590-662, SSSPImpl.cuh:607-690). */
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out);
 /* float Incremental(src*, dst*, n) (BFSImpl.cuh:664-753, SSSPImpl.cuh:692-785).
@@ -247,6 +257,12 @@ mk_status mk_tc_destroy(mk_tc *t);
 typedef struct mk_wcc mk_wcc;
 mk_status mk_wcc_create(mk_graph *g, mk_wcc **out);
 mk_status mk_wcc_static(mk_wcc *w, void *stream, float *ms_out);
+/* Recomputes the labels of the selected vertices only (bit v of d_sel_bits,
+ * a device bitmap of ceil(V/32) words); the other labels stay as they are.
+ * The selection must be closed under edges: whole components, or whole
+ * member graphs of a graph set.  No counterpart in the reference. */
+mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stream,
+                               float *ms_out);
 mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src,
                              const uint32_t *d_dst, uint32_t n, void *stream,
                              float *ms_out);
@@ -257,6 +273,54 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src,
 mk_status mk_wcc_labels(mk_wcc *w, uint32_t *h_out);
 mk_status mk_wcc_labels_device(mk_wcc *w, const uint32_t **d_labels);
 mk_status mk_wcc_destroy(mk_wcc *w);
+
+/* ------------------------------------------------------------------------
+ * Graph sets: many small dynamic graphs stored and updated as one (no
+ * counterpart in the reference, whose drivers hold one graph per process).
+ * Member m owns the global vertex ids [offsets[m], offsets[m+1]); members
+ * share no edge, so one batch, one multi-source traversal (one source per
+ * member) or one subset WCC pass serves them all, and each member's result
+ * equals that of a DynamicGraph holding the member alone.
+ * ---------------------------------------------------------------------- */
+typedef struct mk_graphset mk_graphset;
+/* h_num_vertices[num_graphs] member sizes (each >= 1, sum < 2^32 - 2);
+ * h_degree_hints NULL or an array of num_graphs host pointers, each NULL or
+ * the member's per-vertex hints.  Bucket sizing follows mk_graph_create. */
+mk_status mk_graphset_create(uint32_t num_graphs, const uint32_t *h_num_vertices,
+                             const uint32_t *const *h_degree_hints, double load_factor,
+                             uint32_t weighted, int32_t device, uint64_t pool_slabs,
+                             mk_graphset **out);
+mk_status mk_graphset_destroy(mk_graphset *s);
+/* The union graph, owned by the set: use it with every mk_graph_*, BFS,
+ * SSSP, PageRank, TC and WCC entry point; never destroy it directly. */
+mk_status mk_graphset_union(mk_graphset *s, mk_graph **g);
+/* Copies the num_graphs + 1 vertex offsets to host memory. */
+mk_status mk_graphset_offsets(mk_graphset *s, uint32_t *h_offsets);
+/* Vertex bitmap (ceil(V/32) device words) of the members whose byte in
+ * d_graph_flags[num_graphs] is non-zero; feeds mk_wcc_static_subset. */
+mk_status mk_graphset_select_bits(mk_graphset *s, const uint8_t *d_graph_flags,
+                                  uint32_t *d_bits, void *stream);
+/* R-MAT edges per member on the device: member m gets the edges
+ * [d_edge_offsets[m], d_edge_offsets[m+1]) (u64 device array of
+ * num_graphs + 1 ascending entries), drawn with probabilities a, b, c over
+ * the member's own vertex range; no self-loops (members of one vertex get
+ * self-loops, which updates skip); duplicates possible.  d_w may be NULL. */
+mk_status mk_gen_rmat_set(mk_graphset *s, const uint64_t *d_edge_offsets, double a,
+                          double b, double c, uint64_t seed, uint32_t w_lo,
+                          uint32_t w_hi, uint32_t *d_src, uint32_t *d_dst,
+                          uint32_t *d_w, void *stream);
+/* Random update batches per member on the device: deletes of live edges
+ * drawn from a CSR export of the union graph (d_row_ptr, d_col as written
+ * by mk_graph_export_csr) and inserts of uniform pairs of distinct vertices
+ * inside each member, counts per member given by the u64 offset arrays
+ * d_del_offsets / d_ins_offsets (num_graphs + 1 entries).  d_ins_w may be
+ * NULL. */
+mk_status mk_gen_set_batches(mk_graphset *s, const uint64_t *d_row_ptr,
+                             const uint32_t *d_col, const uint64_t *d_del_offsets,
+                             const uint64_t *d_ins_offsets, uint64_t seed,
+                             uint32_t w_lo, uint32_t w_hi, uint32_t *d_del_src,
+                             uint32_t *d_del_dst, uint32_t *d_ins_src,
+                             uint32_t *d_ins_dst, uint32_t *d_ins_w, void *stream);
 
 /* ------------------------------------------------------------------------
  * Synthetic inputs (host only; no GPU needed).  Seeded and deterministic.

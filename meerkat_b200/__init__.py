@@ -18,8 +18,8 @@ import numpy as np
 
 from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
-__all__ = ["DynamicGraph", "BFS", "SSSP", "PageRank", "TC", "WCC", "EdgeSet", "gen_rmat",
-           "gen_grid", "MeerkatError", "MK_INF", "lib", "version"]
+__all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "TC", "WCC", "EdgeSet",
+           "gen_rmat", "gen_grid", "MeerkatError", "MK_INF", "lib", "version"]
 
 
 def version() -> str:
@@ -93,7 +93,23 @@ class DynamicGraph:
     def handle(self):
         return self._h
 
+    @classmethod
+    def _borrow(cls, handle, num_vertices: int, weighted: bool, device: int, owner):
+        """View of a graph owned by another object (a GraphSet's union graph)."""
+        g = cls.__new__(cls)
+        g.num_vertices = int(num_vertices)
+        g.weighted = bool(weighted)
+        g.reverse = False
+        g._hints = None
+        g._h = handle
+        g.device = int(device)
+        g._owner = owner
+        return g
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             lib().mk_graph_destroy(self._h)
             self._h = None
@@ -120,14 +136,23 @@ class DynamicGraph:
                                           _ptr(found), _ptr(weights), _stream(stream)),
               "mk_graph_search_edges")
 
-    def set_tuning(self, update_kernel: int = 1, update_blocks_per_sm: int = 0) -> None:
-        t = Tuning(int(update_kernel), int(update_blocks_per_sm), 0, 0)
+    def set_tuning(self, update_kernel: Optional[int] = None,
+                   update_blocks_per_sm: Optional[int] = None,
+                   frontier_chunk: Optional[int] = None) -> None:
+        """Sets the given kernel knobs; the others keep their values."""
+        cur = self.get_tuning()
+        for k, v in (("update_kernel", update_kernel), ("update_blocks_per_sm", update_blocks_per_sm),
+                     ("frontier_chunk", frontier_chunk)):
+            if v is not None:
+                cur[k] = int(v)
+        t = Tuning(cur["update_kernel"], cur["update_blocks_per_sm"], cur["frontier_chunk"], 0)
         check(lib().mk_graph_set_tuning(self._h, C.byref(t)), "mk_graph_set_tuning")
 
     def get_tuning(self) -> dict:
         t = Tuning()
         check(lib().mk_graph_get_tuning(self._h, C.byref(t)), "mk_graph_get_tuning")
-        return {"update_kernel": t.update_kernel, "update_blocks_per_sm": t.update_blocks_per_sm}
+        return {"update_kernel": t.update_kernel, "update_blocks_per_sm": t.update_blocks_per_sm,
+                "frontier_chunk": t.frontier_chunk}
 
     def reserve_batch(self, n: int) -> None:
         check(lib().mk_graph_reserve_batch(self._h, int(n)), "mk_graph_reserve_batch")
@@ -202,13 +227,22 @@ class DynamicGraph:
 class _Traversal(_Timed):
     _create = None
 
-    def __init__(self, G: DynamicGraph, source: int, num_vertices: Optional[int] = None):
+    def __init__(self, G: DynamicGraph, source, num_vertices: Optional[int] = None):
+        """`source` is one vertex, or a sequence of distinct vertices for one
+        multi-source traversal (e.g. one source per member of a GraphSet)."""
         if num_vertices is not None and int(num_vertices) != G.num_vertices:
             raise ValueError("VertexN must equal the graph's vertex count")
         self.G = G
-        self.source = int(source)
         h = C.c_void_p()
-        check(getattr(lib(), self._create)(G.handle, self.source, C.byref(h)), self._create)
+        if np.ndim(source) == 0:
+            self.source = int(source)
+            check(getattr(lib(), self._create)(G.handle, self.source, C.byref(h)), self._create)
+        else:
+            self.sources = np.ascontiguousarray(np.asarray(source, dtype=np.uint32))
+            self.source = self.sources
+            name = self._create + "_multi"
+            check(getattr(lib(), name)(G.handle, self.sources.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                       len(self.sources), C.byref(h)), name)
         self._h = h
 
     def close(self):
@@ -377,6 +411,12 @@ class WCC(_Timed):
     def Static(self, stream=None, timed=True):
         return self._call(lib().mk_wcc_static, self._h, _stream(stream), timed=timed)
 
+    def StaticSubset(self, sel_bits, stream=None, timed=True):
+        """Recomputes the labels of the vertices whose bit is set in the device
+        bitmap `sel_bits` (ceil(V/32) words, closed under edges)."""
+        return self._call(lib().mk_wcc_static_subset, self._h, _ptr(sel_bits), _stream(stream),
+                          timed=timed)
+
     def Incremental(self, src, dst, n=None, stream=None, timed=True):
         return self._call(lib().mk_wcc_incremental, self._h, _ptr(src), _ptr(dst), _count(src, n),
                           _stream(stream), timed=timed)
@@ -389,6 +429,125 @@ class WCC(_Timed):
         out = np.zeros(self.G.num_vertices, dtype=np.uint32)
         check(lib().mk_wcc_labels(self._h, out.ctypes.data), "mk_wcc_labels")
         return out
+
+
+class GraphSet:
+    """Many small dynamic graphs stored, updated and queried as one union
+    graph (member m owns vertex ids offsets[m] .. offsets[m+1]-1).  `graph` is
+    a DynamicGraph view of the union graph for every update and algorithm
+    call; the set owns it."""
+
+    def __init__(self, num_vertices, degree_hints=None, load_factor: float = 0.7,
+                 weighted: bool = False, device: int = 0, pool_slabs: int = 0):
+        nv = np.ascontiguousarray(np.asarray(num_vertices, dtype=np.uint32))
+        G = len(nv)
+        self.num_graphs = G
+        self.device = int(device)
+        self.weighted = bool(weighted)
+        self._hint_arrays = None
+        hp = None
+        if degree_hints is not None:
+            self._hint_arrays = [None if h is None else
+                                 np.ascontiguousarray(np.asarray(h, dtype=np.uint32))
+                                 for h in degree_hints]
+            if len(self._hint_arrays) != G:
+                raise ValueError("one degree-hint array (or None) per member graph")
+            for h, n in zip(self._hint_arrays, nv):
+                if h is not None and len(h) != n:
+                    raise ValueError("degree hints must have one entry per member vertex")
+            hp = (C.POINTER(C.c_uint32) * G)(*[
+                C.cast(None, C.POINTER(C.c_uint32)) if h is None
+                else h.ctypes.data_as(C.POINTER(C.c_uint32)) for h in self._hint_arrays])
+        h = C.c_void_p()
+        check(lib().mk_graphset_create(G, nv.ctypes.data_as(C.POINTER(C.c_uint32)), hp,
+                                       float(load_factor), int(weighted), int(device),
+                                       int(pool_slabs), C.byref(h)), "mk_graphset_create")
+        self._h = h
+        self.offsets = np.zeros(G + 1, dtype=np.uint32)
+        check(lib().mk_graphset_offsets(h, self.offsets.ctypes.data_as(C.POINTER(C.c_uint32))),
+              "mk_graphset_offsets")
+        gh = C.c_void_p()
+        check(lib().mk_graphset_union(h, C.byref(gh)), "mk_graphset_union")
+        self.graph = DynamicGraph._borrow(gh, int(self.offsets[-1]), weighted, device, self)
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.offsets[-1])
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.graph._h = None
+            lib().mk_graphset_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _dev(self):
+        return f"cuda:{self.device}"
+
+    def select_bits(self, graph_flags, stream=None):
+        """Device vertex bitmap of the members whose flag is non-zero."""
+        import torch
+        flags = graph_flags
+        if not hasattr(flags, "data_ptr"):
+            flags = torch.from_numpy(np.ascontiguousarray(np.asarray(graph_flags, dtype=np.uint8)))
+        flags = flags.to(self._dev(), dtype=torch.uint8)
+        bits = torch.empty((self.num_vertices + 31) // 32, dtype=torch.int32, device=self._dev())
+        check(lib().mk_graphset_select_bits(self._h, flags.data_ptr(), bits.data_ptr(),
+                                            _stream(stream)), "mk_graphset_select_bits")
+        return bits
+
+    def gen_rmat(self, edges_per_graph, a=0.57, b=0.19, c=0.19, seed=0, w_lo=1, w_hi=64,
+                 weights=True, stream=None):
+        """Device R-MAT edges, edges_per_graph[m] inside member m (int32 tensors
+        holding uint32 ids)."""
+        import torch
+        cnt = np.asarray(edges_per_graph, dtype=np.uint64)
+        off = np.zeros(self.num_graphs + 1, dtype=np.uint64)
+        np.cumsum(cnt, out=off[1:])
+        E = int(off[-1])
+        d_off = torch.from_numpy(off.view(np.int64)).to(self._dev())
+        src = torch.empty(max(E, 1), dtype=torch.int32, device=self._dev())
+        dst = torch.empty(max(E, 1), dtype=torch.int32, device=self._dev())
+        w = torch.empty(max(E, 1), dtype=torch.int32, device=self._dev()) if weights else None
+        check(lib().mk_gen_rmat_set(self._h, d_off.data_ptr(), a, b, c, seed, w_lo, w_hi,
+                                    src.data_ptr(), dst.data_ptr(), _ptr(w), _stream(stream)),
+              "mk_gen_rmat_set")
+        return src[:E], dst[:E], (w[:E] if w is not None else None)
+
+    def gen_batches(self, deletes_per_graph, inserts_per_graph, seed=0, w_lo=1, w_hi=64,
+                    weights=True, stream=None):
+        """Device update batches: deletes of live edges and inserts of random
+        pairs, per member.  Returns (del_src, del_dst, ins_src, ins_dst, ins_w)."""
+        import torch
+        dev = self._dev()
+        E = self.graph.info()["num_edges"]
+        rp = torch.empty(self.num_vertices + 1, dtype=torch.int64, device=dev)
+        col = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+        check(lib().mk_graph_export_csr(self.graph.handle, rp.data_ptr(), col.data_ptr(), None,
+                                        _stream(stream)), "mk_graph_export_csr")
+        offs = []
+        for cnt in (deletes_per_graph, inserts_per_graph):
+            o = np.zeros(self.num_graphs + 1, dtype=np.uint64)
+            np.cumsum(np.asarray(cnt, dtype=np.uint64), out=o[1:])
+            offs.append(o)
+        nd, ni = int(offs[0][-1]), int(offs[1][-1])
+        d_do = torch.from_numpy(offs[0].view(np.int64)).to(dev)
+        d_io = torch.from_numpy(offs[1].view(np.int64)).to(dev)
+        ds = torch.empty(max(nd, 1), dtype=torch.int32, device=dev)
+        dd = torch.empty(max(nd, 1), dtype=torch.int32, device=dev)
+        is_ = torch.empty(max(ni, 1), dtype=torch.int32, device=dev)
+        id_ = torch.empty(max(ni, 1), dtype=torch.int32, device=dev)
+        iw = torch.empty(max(ni, 1), dtype=torch.int32, device=dev) if weights else None
+        check(lib().mk_gen_set_batches(self._h, rp.data_ptr(), col.data_ptr(), d_do.data_ptr(),
+                                       d_io.data_ptr(), seed, w_lo, w_hi, ds.data_ptr(),
+                                       dd.data_ptr(), is_.data_ptr(), id_.data_ptr(), _ptr(iw),
+                                       _stream(stream)), "mk_gen_set_batches")
+        return ds[:nd], dd[:nd], is_[:ni], id_[:ni], (iw[:ni] if iw is not None else None)
 
 
 # ---------------------------------------------------------------------------

@@ -34,7 +34,7 @@ class GraphInfo(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("update_kernel", C.c_uint32), ("update_blocks_per_sm", C.c_uint32),
-                ("reserved0", C.c_uint32), ("reserved1", C.c_uint32)]
+                ("frontier_chunk", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 # (name, restype, argtypes); every function returns mk_status unless noted
@@ -60,6 +60,8 @@ SIGNATURES = [
     ("mk_graph_get_tuning", _S, [vp, C.POINTER(Tuning)]),
     ("mk_bfs_create", _S, [vp, C.c_uint32, C.POINTER(vp)]),
     ("mk_sssp_create", _S, [vp, C.c_uint32, C.POINTER(vp)]),
+    ("mk_bfs_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
+    ("mk_sssp_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
     ("mk_traversal_static", _S, [vp, vp, f32p]),
     ("mk_traversal_incremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_traversal_decremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),
@@ -84,11 +86,22 @@ SIGNATURES = [
     ("mk_tc_destroy", _S, [vp]),
     ("mk_wcc_create", _S, [vp, C.POINTER(vp)]),
     ("mk_wcc_static", _S, [vp, vp, f32p]),
+    ("mk_wcc_static_subset", _S, [vp, vp, vp, f32p]),
     ("mk_wcc_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_decremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_labels", _S, [vp, vp]),
     ("mk_wcc_labels_device", _S, [vp, C.POINTER(vp)]),
     ("mk_wcc_destroy", _S, [vp]),
+    ("mk_graphset_create", _S, [C.c_uint32, u32p, C.POINTER(u32p), C.c_double, C.c_uint32,
+                                C.c_int32, C.c_uint64, C.POINTER(vp)]),
+    ("mk_graphset_destroy", _S, [vp]),
+    ("mk_graphset_union", _S, [vp, C.POINTER(vp)]),
+    ("mk_graphset_offsets", _S, [vp, u32p]),
+    ("mk_graphset_select_bits", _S, [vp, vp, vp, vp]),
+    ("mk_gen_rmat_set", _S, [vp, vp, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint32,
+                             C.c_uint32, vp, vp, vp, vp]),
+    ("mk_gen_set_batches", _S, [vp, vp, vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp,
+                                vp, vp, vp]),
     ("mk_gen_rmat", _S, [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                          C.c_uint32, C.c_uint32, vp, vp, vp]),
     ("mk_gen_grid", _S, [C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp,

@@ -901,6 +901,7 @@ mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t) {
   if (!g || !t) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: null argument");
   if (t->update_kernel > 1) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_kernel must be 0 or 1");
   if (t->update_blocks_per_sm > 32) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_blocks_per_sm > 32");
+  if (t->frontier_chunk > 1024) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: frontier_chunk > 1024");
   g->tuning = *t;
   return MK_OK;
 }

@@ -24,7 +24,7 @@
 //     strategy, BFSImpl.cuh:419-440), skipping vertices of degree 0;
 //   * the stored edge weight is probed for every seeding batch edge, so a
 //     batch entry that did not change the graph cannot seed a wrong distance;
-//   * frontier entries are work items (vertex, chunk of kChunk buckets), so a
+//   * frontier entries are work items (vertex, chunk of `chunk` buckets), so a
 //     hub's buckets spread over many 8-lane groups instead of one; a group
 //     reads 128-byte slabs with 16-byte loads, up to 4 head slabs at once;
 //   * the re-seed sweep runs over buckets (bucket -> owner map), not vertices,
@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "mk_internal.h"
 #include "mk_slab.cuh"
@@ -67,14 +68,16 @@ struct TravArgs {
   const uint32_t *bsrc;
   const uint32_t *bdst;
   uint32_t bn;
-  uint32_t source;
+  const uint32_t *sources;  // distinct source vertices (one per query)
+  uint32_t nsources;
+  uint32_t chunk;           // buckets per frontier work item
   uint32_t mode;
   unsigned long long limit_ns;
 };
 
 constexpr int kTravBlock = 256;
 constexpr int kQueueCap = 2048;
-constexpr uint32_t kChunk = 4;  // buckets per frontier work item
+constexpr uint32_t kDefaultChunk = 4;  // buckets per frontier work item
 
 __host__ __device__ __forceinline__ unsigned long long item(uint32_t v, uint32_t chunk) {
   return ((unsigned long long)chunk << 32) | v;
@@ -85,11 +88,11 @@ struct BlockQueue {
   uint32_t *qn;
 };
 
-// Pushes vertex v as ceil(buckets / kChunk) work items.
+// Pushes vertex v as ceil(buckets / chunk) work items.
 __device__ __forceinline__ void push_vertex(const TravArgs &a, const BlockQueue &Q, uint32_t v,
                                             unsigned long long *gfr, uint32_t *gsz) {
   const uint32_t nb = a.g.boff[v + 1] - a.g.boff[v];
-  const uint32_t k = (nb + kChunk - 1) / kChunk;
+  const uint32_t k = (nb + a.chunk - 1) / a.chunk;
   if (k <= 1) {
     uint32_t pos = atomicAdd(Q.qn, 1u);
     if (pos < kQueueCap) {
@@ -236,13 +239,19 @@ __device__ __forceinline__ void expand_range(const TravArgs &a, const Lanes &L,
 }
 
 // Bucket range of a work item.
-__device__ __forceinline__ void item_range(const GraphView &g, unsigned long long it,
+__device__ __forceinline__ void item_range(const GraphView &g, unsigned long long it, uint32_t chunk,
                                            uint32_t &v, uint32_t &b0, uint32_t &b1) {
   v = (uint32_t)it;
   const uint32_t c = (uint32_t)(it >> 32);
   const uint32_t lo = g.boff[v], hi = g.boff[v + 1];
-  b0 = lo + c * kChunk;
-  b1 = min(hi, b0 + kChunk);
+  b0 = lo + c * chunk;
+  b1 = min(hi, b0 + chunk);
+}
+
+// A source holds PACK(0, itself) (BFS.cuh:47-52) and is the only vertex whose
+// parent is itself, so sources are never invalidated.
+__device__ __forceinline__ bool is_source(unsigned long long p, uint32_t v) {
+  return p == pack(0, v);
 }
 
 template <bool kW, bool kUseW>
@@ -265,17 +274,16 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
 
   // ---- seeding (level -1 pushes into fr[0] / sz[0]) ----
   if (a.mode == kStatic) {
-    if (tid == 0) {
-      a.dist[a.source] = pack(0, a.source);
-      a.stamp[a.source] = round + 1;
+    // every source seeds its own work items (a hub source has many)
+    for (uint32_t i = tid; i < a.nsources; i += nthreads) {
+      const uint32_t src = a.sources[i];
+      a.dist[src] = pack(0, src);
+      a.stamp[src] = round + 1;
+      const uint32_t nb = a.g.boff[src + 1] - a.g.boff[src];
+      const uint32_t k = max(1u, (nb + a.chunk - 1) / a.chunk);
+      const uint32_t base = atomicAdd(ctl + kSz0, k);
+      for (uint32_t j = 0; j < k; ++j) a.fr0[base + j] = item(src, j);
       atomicAdd(a.pushed, 1ull);
-    }
-    if (tid < 32) {
-      // the source's items (a hub source has many)
-      const uint32_t nb = a.g.boff[a.source + 1] - a.g.boff[a.source];
-      const uint32_t k = max(1u, (nb + kChunk - 1) / kChunk);
-      for (uint32_t j = tid; j < k; j += 32) a.fr0[j] = item(a.source, j);
-      if (tid == 0) ctl[kSz0] = k;
     }
   } else if (a.mode == kIncremental) {
     for (uint32_t e = group; e < a.bn; e += ngroups) {
@@ -307,15 +315,15 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       a.dist[v] = kInfInf;
       a.inv_list[atomicAdd(ctl + kInvCount, 1u)] = v;
       const uint32_t nb = a.g.boff[v + 1] - a.g.boff[v];
-      const uint32_t k = max(1u, (nb + kChunk - 1) / kChunk);
+      const uint32_t k = max(1u, (nb + a.chunk - 1) / a.chunk);
       const uint32_t base = atomicAdd(gsz, k);
       for (uint32_t j = 0; j < k; ++j) gfr[base + j] = item(v, j);
     };
     for (uint32_t e = tid; e < a.bn; e += nthreads) {
       uint32_t s = a.bsrc[e], d = a.bdst[e];
-      if (s == d || s >= a.g.V || d >= a.g.V || d == a.source) continue;
+      if (s == d || s >= a.g.V || d >= a.g.V) continue;
       unsigned long long pd = ld_dist(a.dist + d);
-      if (pd != kInfInf && pack_lo(pd) == s && inval_set(a.inval, d))
+      if (pd != kInfInf && !is_source(pd, d) && pack_lo(pd) == s && inval_set(a.inval, d))
         invalidate(d, a.fr0, ctl + kDSz0);
     }
     if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
@@ -331,16 +339,17 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       uint32_t *nsz = ctl + kDSz0 + ((dl + 1) % 3);
       for (uint32_t i = group; i < n; i += ngroups) {
         uint32_t x, b0, b1;
-        item_range(a.g, __ldcg(cur + i), x, b0, b1);
+        item_range(a.g, __ldcg(cur + i), a.chunk, x, b0, b1);
         walk_buckets(a.g, L, b0, b1, [&](const uint4 &q) {
           uint32_t k[4], w[4];
           lane_keys<kW>(q, L.gl, k, w);
 #pragma unroll
           for (int j = 0; j < keys_per_lane<kW>(); ++j) {
             uint32_t y = k[j];
-            if (y < kTombKey && y != x && y != a.source && !inval_test(a.inval, y)) {
+            if (y < kTombKey && y != x && !inval_test(a.inval, y)) {
               unsigned long long py = ld_dist(a.dist + y);
-              if (py != kInfInf && pack_lo(py) == x && inval_set(a.inval, y)) invalidate(y, nxt, nsz);
+              if (py != kInfInf && !is_source(py, y) && pack_lo(py) == x && inval_set(a.inval, y))
+                invalidate(y, nxt, nsz);
             }
           }
         });
@@ -379,7 +388,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
     const uint32_t stamp_next = round + 2 + lv;
     for (uint32_t i = group; i < n; i += ngroups) {
       uint32_t u, b0, b1;
-      item_range(a.g, __ldcg(cur + i), u, b0, b1);
+      item_range(a.g, __ldcg(cur + i), a.chunk, u, b0, b1);
       unsigned long long pu = 0;
       if (L.gl == 0) pu = ld_dist(a.dist + u);
       pu = __shfl_sync(L.gmask, pu, L.gbase);
@@ -407,7 +416,8 @@ using namespace mk;
 
 struct mk_traversal {
   mk_graph *g = nullptr;
-  uint32_t source = 0;
+  uint32_t nsources = 0;
+  uint32_t *sources = nullptr;  // device copy
   bool sssp = false;
   bool has_static = false;
   int nblocks = 0;
@@ -421,16 +431,29 @@ struct mk_traversal {
   Timer timer;
 };
 
-static mk_status trav_create(mk_graph *g, uint32_t source, bool sssp, mk_traversal **out) {
-  if (!g || !out) return fail(MK_ERR_INVALID, "traversal create: null argument");
+__global__ void k_set_sources(unsigned long long *dist, const uint32_t *sources, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dist[sources[i]] = pack(0, sources[i]);
+}
+
+static mk_status trav_create(mk_graph *g, const uint32_t *h_sources, uint32_t nsrc, bool sssp,
+                             mk_traversal **out) {
+  if (!g || !out || !h_sources) return fail(MK_ERR_INVALID, "traversal create: null argument");
   *out = nullptr;
-  if (source >= g->V) return fail(MK_ERR_INVALID, "traversal create: source out of range");
+  if (nsrc == 0) return fail(MK_ERR_INVALID, "traversal create: no source");
   if (g->reverse) return fail(MK_ERR_INVALID, "traversal create: graph must store out-edges");
   if (sssp && !g->weighted) return fail(MK_ERR_INVALID, "SSSP needs a weighted graph");
+  {
+    std::vector<uint32_t> sorted(h_sources, h_sources + nsrc);
+    std::sort(sorted.begin(), sorted.end());
+    if (sorted.back() >= g->V) return fail(MK_ERR_INVALID, "traversal create: source out of range");
+    if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+      return fail(MK_ERR_INVALID, "traversal create: repeated source");
+  }
   DeviceGuard dg(g->device);
   mk_traversal *t = new mk_traversal();
   t->g = g;
-  t->source = source;
+  t->nsources = nsrc;
   t->sssp = sssp;
   const size_t V = g->V;
   cudaError_t e = cudaSuccess;
@@ -440,26 +463,31 @@ static mk_status trav_create(mk_graph *g, uint32_t source, bool sssp, mk_travers
   A((void **)&t->dist, V * 8);
   A((void **)&t->stamp, V * 4);
   A((void **)&t->inval, (V + 31) / 32 * 4);
-  // a level holds every vertex at most once, as ceil(buckets / kChunk) items
-  const size_t items = V + g->num_buckets / kChunk + 64;
+  // a level holds every vertex at most once, as at most one item per bucket
+  // (any chunk size >= 1)
+  const size_t items = g->num_buckets + 64;
   A((void **)&t->fr0, items * 8);
   A((void **)&t->fr1, items * 8);
   A((void **)&t->inv_list, V * 4 + 16);
   A((void **)&t->ctl, kCtlWords * 4);
   A((void **)&t->pushed, 8);
+  A((void **)&t->sources, (size_t)nsrc * 4);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->sources, h_sources, (size_t)nsrc * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(t->dist, 0xFF, V * 8);
   if (e == cudaSuccess) e = cudaMemset(t->stamp, 0, V * 4);
   if (e == cudaSuccess) e = cudaMemset(t->inval, 0, (V + 31) / 32 * 4);
   if (e == cudaSuccess) e = cudaMemset(t->ctl, 0, kCtlWords * 4);
   if (e == cudaSuccess) {
     // dist[src] = PACK(0, src) as the reference constructor does (BFS.cuh:49-52)
-    unsigned long long s0 = pack(0, source);
-    e = cudaMemcpy(t->dist + source, &s0, 8, cudaMemcpyHostToDevice);
+    k_set_sources<<<(nsrc + 255) / 256, 256>>>(t->dist, t->sources, nsrc);
+    e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
     uint32_t one = 1;
     e = cudaMemcpy(t->ctl + kRound, &one, 4, cudaMemcpyHostToDevice);
   }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     mk_traversal_destroy(t);
     return cuda_fail(e, "traversal create");
@@ -493,7 +521,9 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   a.bsrc = bs;
   a.bdst = bd;
   a.bn = n;
-  a.source = t->source;
+  a.sources = t->sources;
+  a.nsources = t->nsources;
+  a.chunk = g->tuning.frontier_chunk ? g->tuning.frontier_chunk : kDefaultChunk;
   a.mode = mode;
   a.limit_ns = 4000000000ull;
   const void *fn;
@@ -512,11 +542,21 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
 extern "C" {
 
 mk_status mk_bfs_create(mk_graph *g, uint32_t source, mk_traversal **out) {
-  return trav_create(g, source, false, out);
+  return trav_create(g, &source, 1, false, out);
 }
 
 mk_status mk_sssp_create(mk_graph *g, uint32_t source, mk_traversal **out) {
-  return trav_create(g, source, true, out);
+  return trav_create(g, &source, 1, true, out);
+}
+
+mk_status mk_bfs_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n,
+                              mk_traversal **out) {
+  return trav_create(g, h_sources, n, false, out);
+}
+
+mk_status mk_sssp_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n,
+                               mk_traversal **out) {
+  return trav_create(g, h_sources, n, true, out);
 }
 
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out) {
@@ -593,6 +633,7 @@ mk_status mk_traversal_destroy(mk_traversal *t) {
   cudaFree(t->inv_list);
   cudaFree(t->ctl);
   cudaFree(t->pushed);
+  cudaFree(t->sources);
   delete t;
   return MK_OK;
 }

@@ -49,8 +49,11 @@ __device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b, ui
   atomicOr(err, kErrTimeout);
 }
 
-__global__ void k_uf_init(uint32_t *p, uint32_t V) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) p[i] = i;
+__global__ void k_uf_init(uint32_t *p, uint32_t V, const uint32_t *sel_bits = nullptr) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+    if (sel_bits && !((sel_bits[i >> 5] >> (i & 31)) & 1u)) continue;
+    p[i] = i;
+  }
 }
 
 // Union every out-edge of the vertices selected by `sel` (all if null); one
@@ -187,6 +190,20 @@ mk_status mk_wcc_static(mk_wcc *w, void *stream, float *ms_out) {
   cudaStream_t s = as_stream(stream);
   MK_CHECK(w->timer.start(s, ms_out != nullptr));
   MK_CHECK(wcc_static(w, s));
+  return w->timer.stop(ms_out);
+}
+
+mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stream,
+                               float *ms_out) {
+  if (!w || !d_sel_bits) return fail(MK_ERR_INVALID, "mk_wcc_static_subset: null argument");
+  mk_graph *g = w->g;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(w->timer.start(s, ms_out != nullptr));
+  k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, d_sel_bits);
+  MK_CHECK(wcc_edges(w, d_sel_bits, s));
+  k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, d_sel_bits);
+  MK_CUDA(cudaGetLastError());
   return w->timer.stop(ms_out);
 }
 

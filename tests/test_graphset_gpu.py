@@ -1,0 +1,197 @@
+"""Graph sets: many small graphs in one union graph.  Every member's result
+must equal the oracle's result for that member alone."""
+import numpy as np
+import pytest
+
+import meerkat_b200 as mk
+from oracle import OracleGraph
+
+from helpers import degree_hints, to_dev
+
+pytestmark = pytest.mark.gpu
+
+INFINF = np.uint64(2**64 - 1)
+
+
+def members(n=12, seed=40):
+    """n seeded R-MAT graphs of scale 7..10 (local ids)."""
+    out = []
+    for m in range(n):
+        scale = 7 + m % 4
+        V = 1 << scale
+        s, d, w = mk.gen_rmat(scale, V * (2 + m % 3), seed=seed + m, w_lo=1, w_hi=64)
+        out.append((V, s, d, w))
+    return out
+
+
+def build_set(mem, chunk=None):
+    nv = [V for V, *_ in mem]
+    hints = [degree_hints(s, V) for V, s, _, _ in mem]
+    S = mk.GraphSet(nv, degree_hints=hints, weighted=True)
+    if chunk is not None:
+        S.graph.set_tuning(frontier_chunk=chunk)
+    off = S.offsets.astype(np.int64)
+    s = np.concatenate([s + off[m] for m, (_, s, _, _) in enumerate(mem)]).astype(np.uint32)
+    d = np.concatenate([d + off[m] for m, (_, _, d, _) in enumerate(mem)]).astype(np.uint32)
+    w = np.concatenate([w for *_, w in mem]).astype(np.uint32)
+    S.graph.InsertEdges(to_dev(s), to_dev(d), vals=to_dev(w))
+    assert S.graph.sync() == 0
+    oracles = []
+    for V, ms, md, mw in mem:
+        O = OracleGraph(V)
+        O.insert(ms, md, mw)
+        oracles.append(O)
+    return S, oracles
+
+
+def local_packed(packed, lo, hi):
+    """Member slice of a packed dist<<32|parent array with local parent ids."""
+    p = packed[lo:hi].copy()
+    live = p != INFINF
+    p[live] = (p[live] & np.uint64(0xFFFFFFFF00000000)) | ((p[live] & np.uint64(0xFFFFFFFF)) - np.uint64(lo))
+    return p
+
+
+@pytest.mark.parametrize("chunk", [None, 1, 64])
+def test_multi_source_traversals_and_subset_wcc_match_members(chunk):
+    mem = members()
+    S, oracles = build_set(mem, chunk)
+    off = S.offsets.astype(np.int64)
+    G = S.graph
+    # one source (the member's hub) for every even member; odd members stay unreached
+    src_local = {m: int(np.argmax(np.bincount(s, minlength=V)))
+                 for m, (V, s, _, _) in enumerate(mem) if m % 2 == 0}
+    sources = [off[m] + v for m, v in src_local.items()]
+    bfs, sssp = mk.BFS(G, sources), mk.SSSP(G, sources)
+    wcc = mk.WCC(G)
+    bfs.Static()
+    sssp.Static()
+    wcc.Static()
+
+    def check(labels_expected=None):
+        bd, sd = bfs.Distances(), sssp.Distances()
+        bp, sp = bfs.packed(), sssp.packed()
+        lab = wcc.Labels()
+        for m, O in enumerate(oracles):
+            lo, hi = off[m], off[m + 1]
+            if m in src_local:
+                v = src_local[m]
+                np.testing.assert_array_equal(bd[lo:hi], O.bfs(v))
+                np.testing.assert_array_equal(sd[lo:hi], O.sssp(v))
+                assert O.check_parents(v, local_packed(bp, lo, hi), weighted=False) == 0
+                assert O.check_parents(v, local_packed(sp, lo, hi), weighted=True) == 0
+            else:
+                assert (bd[lo:hi] == mk.MK_INF).all() and (sd[lo:hi] == mk.MK_INF).all()
+            if labels_expected is None:
+                np.testing.assert_array_equal(lab[lo:hi].astype(np.int64) - lo, O.wcc())
+            else:
+                np.testing.assert_array_equal(lab[lo:hi], labels_expected[lo:hi])
+
+    check()
+    labels_before = wcc.Labels()
+    # one mixed batch over all members: deletes (incl. tree edges) then inserts
+    rng = np.random.default_rng(9)
+    packed = sssp.packed()
+    del_s, del_d, ins_s, ins_d, ins_w = [], [], [], [], []
+    for m, (V, s, d, _) in enumerate(mem):
+        es = mk.EdgeSet(V, s, d)
+        ds, dd = es.sample_present(len(s) // 8, seed=100 + m)
+        if m in src_local:
+            lp = local_packed(packed, off[m], off[m + 1])
+            par = (lp & np.uint64(0xFFFFFFFF)).astype(np.int64)
+            tree = np.nonzero((lp != INFINF) & (par != np.arange(V)))[0]
+            pick = rng.choice(tree, size=min(8, len(tree)), replace=False)
+            ds = np.concatenate([ds, par[pick]]).astype(np.uint32)
+            dd = np.concatenate([dd, pick]).astype(np.uint32)
+        is_, id_ = es.sample_absent(len(s) // 10, seed=200 + m)
+        iw = rng.integers(1, 65, len(is_)).astype(np.uint32)
+        oracles[m].delete(ds, dd)
+        oracles[m].insert(is_, id_, iw)
+        del_s.append(ds + off[m]), del_d.append(dd + off[m])
+        ins_s.append(is_ + off[m]), ins_d.append(id_ + off[m]), ins_w.append(iw)
+    cat = lambda xs: to_dev(np.concatenate(xs).astype(np.uint32))
+    tds, tdd = cat(del_s), cat(del_d)
+    G.DeleteEdges(tds, tdd)
+    assert G.sync() == 0
+    bfs.Decremental(tds, tdd)
+    sssp.Decremental(tds, tdd)
+    tis, tid, tiw = cat(ins_s), cat(ins_d), cat(ins_w)
+    G.InsertEdges(tis, tid, vals=tiw)
+    assert G.sync() == 0
+    bfs.Incremental(tis, tid)
+    sssp.Incremental(tis, tid, wgt=tiw)
+    # recompute components of the odd members only: even members keep their
+    # (now stale) labels
+    flags = np.array([m % 2 for m in range(len(mem))], np.uint8)
+    wcc.StaticSubset(S.select_bits(flags))
+    expect = labels_before.copy()
+    for m, O in enumerate(oracles):
+        if m % 2:
+            expect[off[m]:off[m + 1]] = O.wcc() + off[m]
+    check(expect)
+
+
+def test_select_bits_layout():
+    S = mk.GraphSet([5, 40, 1, 30])
+    bits = S.select_bits(np.array([1, 0, 1, 1], np.uint8)).cpu().numpy().view(np.uint32)
+    V = S.num_vertices
+    got = np.array([(bits[v >> 5] >> (v & 31)) & 1 for v in range(V)])
+    owner = np.searchsorted(S.offsets, np.arange(V), side="right") - 1
+    np.testing.assert_array_equal(got, np.array([1, 0, 1, 1])[owner])
+    assert (bits[-1] >> (V & 31)) == 0  # padding bits stay clear
+
+
+def test_device_generators_stay_inside_members():
+    import torch
+    nv = [300, 1024, 77, 5000, 2048, 1]
+    S = mk.GraphSet(nv, weighted=True)
+    off = S.offsets.astype(np.int64)
+    epg = [2000, 8000, 300, 40000, 0, 5]
+    src, dst, w = S.gen_rmat(epg, seed=3, w_lo=2, w_hi=9)
+    s = src.cpu().numpy().view(np.uint32).astype(np.int64)
+    d = dst.cpu().numpy().view(np.uint32).astype(np.int64)
+    ww = w.cpu().numpy().view(np.uint32)
+    assert len(s) == sum(epg)
+    owner = np.repeat(np.arange(len(nv)), epg)
+    assert ((s >= off[owner]) & (s < off[owner + 1])).all()
+    assert ((d >= off[owner]) & (d < off[owner + 1])).all()
+    single = owner == 5
+    assert (s[~single] != d[~single]).all() and (s[single] == d[single]).all()
+    assert ww.min() >= 2 and ww.max() <= 9
+    # same seed, same edges
+    src2, dst2, _ = S.gen_rmat(epg, seed=3, w_lo=2, w_hi=9)
+    assert torch.equal(src, src2) and torch.equal(dst, dst2)
+    # R-MAT skew inside member 3: its low ids are the heavy ones
+    deg = np.bincount(s[owner == 3] - off[3], minlength=nv[3])
+    assert deg[:64].sum() > deg[-64:].sum()
+    S.graph.InsertEdges(src, dst, vals=w)
+    assert S.graph.sync() == 0
+    dpg = [100, 200, 50, 500, 10, 3]  # member 4 has no edge, member 5 only loops
+    ipg = [30, 60, 10, 100, 10, 2]
+    ds, dd, is_, id_, iw = S.gen_batches(dpg, ipg, seed=5, w_lo=2, w_hi=9)
+    dsh = ds.cpu().numpy().view(np.uint32).astype(np.int64)
+    ddh = dd.cpu().numpy().view(np.uint32).astype(np.int64)
+    own_d = np.repeat(np.arange(len(nv)), dpg)
+    live = (own_d != 4) & (own_d != 5)
+    found = torch.zeros(len(dsh), dtype=torch.uint8, device="cuda:0")
+    S.graph.SearchEdges(ds, dd, found)
+    torch.cuda.synchronize()
+    assert found.cpu().numpy()[live].all()
+    assert ((dsh >= off[own_d]) & (dsh < off[own_d + 1])).all()
+    assert (dsh[~live] == ddh[~live]).all()  # no live edge: a self-loop no-op
+    ish = is_.cpu().numpy().view(np.uint32).astype(np.int64)
+    idh = id_.cpu().numpy().view(np.uint32).astype(np.int64)
+    own_i = np.repeat(np.arange(len(nv)), ipg)
+    assert ((ish >= off[own_i]) & (ish < off[own_i + 1])).all()
+    assert ((idh >= off[own_i]) & (idh < off[own_i + 1])).all()
+    assert (ish[own_i != 5] != idh[own_i != 5]).all()
+    iwh = iw.cpu().numpy().view(np.uint32)
+    assert iwh.min() >= 2 and iwh.max() <= 9
+
+
+def test_multi_source_rejects_bad_sources():
+    S = mk.GraphSet([10, 10], weighted=True)
+    with pytest.raises(mk.MeerkatError):
+        mk.BFS(S.graph, [1, 1])
+    with pytest.raises(mk.MeerkatError):
+        mk.SSSP(S.graph, [3, 20])
