@@ -131,6 +131,21 @@ mk_status mk_graph_get_info(mk_graph *g, mk_graph_info *out);
  * room for num_edges entries; d_w may be NULL. */
 mk_status mk_graph_export_csr(mk_graph *g, uint64_t *d_row_ptr,
                               uint32_t *d_col, uint32_t *d_w, void *stream);
+/* Same output as mk_graph_export_csr, for callers that must not allocate
+ * device memory after start-up (no counterpart in the reference).  The
+ * plain export grows its scratch with cudaMalloc, which synchronises the
+ * whole device and fails once a pool has taken the free memory; this one
+ * calls no allocator: its scratch is one fixed array of about 3 MiB inside
+ * the library, shared by every call on a device.
+ *   - Limit: graphs of at most 262,144 buckets (num_buckets of
+ *     mk_graph_get_info); larger graphs get MK_ERR_INVALID.
+ *   - The first call on each device looks the array up and may load the
+ *     library's device code; make that first call before any stream capture.
+ *   - Calls that overlap in time on one device (different streams, or
+ *     host threads) race on the shared scratch: order them on one stream. */
+mk_status mk_graph_export_csr_noalloc(mk_graph *g, uint64_t *d_row_ptr,
+                                      uint32_t *d_col, uint32_t *d_w,
+                                      void *stream);
 /* Per-vertex tombstone count (test/GraphTest.cu:58-95 CountTombstones). */
 mk_status mk_graph_count_tombstones(mk_graph *g, uint32_t *d_out,
                                     void *stream);

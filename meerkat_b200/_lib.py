@@ -54,6 +54,7 @@ SIGNATURES = [
     ("mk_graph_bucket_layout", _S, [vp, vp, vp]),
     ("mk_graph_get_info", _S, [vp, C.POINTER(GraphInfo)]),
     ("mk_graph_export_csr", _S, [vp, vp, vp, vp, vp]),
+    ("mk_graph_export_csr_noalloc", _S, [vp, vp, vp, vp, vp]),
     ("mk_graph_count_tombstones", _S, [vp, vp, vp]),
     ("mk_graph_reserve_batch", _S, [vp, C.c_uint32]),
     ("mk_graph_set_tuning", _S, [vp, C.POINTER(Tuning)]),

@@ -1008,6 +1008,93 @@ mk_status mk_graph_export_csr(mk_graph *g, uint64_t *d_row_ptr, uint32_t *d_col,
   return MK_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// CSR export that allocates nothing.  mk_graph_export_csr keeps its per-bucket
+// counts and positions in buffers it grows on demand with cudaMalloc, which
+// synchronises the whole device and can fail once the memory is spoken for.
+// Callers that must not allocate after start-up -- a serving process that
+// handed all free memory to its own pool, or a loop whose concurrent streams
+// must not be stalled by an implicit device synchronisation -- use this
+// variant instead: its scratch is a fixed file-scope device array, sized for
+// graphs of up to kNoAllocMaxBuckets buckets.
+// ---------------------------------------------------------------------------
+namespace mk {
+
+constexpr uint32_t kNoAllocMaxBuckets = 1u << 18;  // 262,144 buckets
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr uint32_t kNaMaxTiles = (kNoAllocMaxBuckets + kScanTile - 1) / kScanTile;
+constexpr size_t kNaCntOff = 0;  // uint32 live count per bucket
+constexpr size_t kNaPosOff = align256(kNaCntOff + (size_t)kNoAllocMaxBuckets * 4);  // uint64[nb + 1]
+constexpr size_t kNaTileOff = align256(kNaPosOff + ((size_t)kNoAllocMaxBuckets + 1) * 8);  // uint64 per scan tile
+constexpr size_t kNaBytes = align256(kNaTileOff + (size_t)kNaMaxTiles * 8);  // about 3 MiB
+
+// Shared by every call on a device.  Nothing in it has to start at zero:
+// each word a call reads was written earlier in the same call.
+static __device__ __align__(256) unsigned char g_export_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+static std::mutex g_na_mu;
+static unsigned char *g_na_ptr[kNaMaxDevices] = {};
+
+// Device address of the scratch array, looked up once per device (the
+// calling thread has that device current).
+static mk_status export_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= kNaMaxDevices)
+    return fail(MK_ERR_INVALID, "mk_graph_export_csr_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (!g_na_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_export_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "mk_graph_export_csr_noalloc: cudaGetSymbolAddress");
+    g_na_ptr[device] = static_cast<unsigned char *>(p);
+  }
+  *out = g_na_ptr[device];
+  return MK_OK;
+}
+
+}  // namespace mk
+
+extern "C" {
+
+mk_status mk_graph_export_csr_noalloc(mk_graph *g, uint64_t *d_row_ptr, uint32_t *d_col,
+                                      uint32_t *d_w, void *stream) {
+  if (!g || !d_row_ptr || !d_col)
+    return fail(MK_ERR_INVALID, "mk_graph_export_csr_noalloc: null argument");
+  if (g->num_buckets > kNoAllocMaxBuckets)
+    return fail(MK_ERR_INVALID,
+                "mk_graph_export_csr_noalloc: the graph has " + std::to_string(g->num_buckets) +
+                    " buckets, more than the " + std::to_string(kNoAllocMaxBuckets) +
+                    " its fixed scratch holds; use mk_graph_export_csr");
+  DeviceGuard dg(g->device);
+  unsigned char *base = nullptr;
+  MK_CHECK(export_scratch(g->device, &base));
+  uint32_t *cnt = reinterpret_cast<uint32_t *>(base + kNaCntOff);
+  unsigned long long *pos = reinterpret_cast<unsigned long long *>(base + kNaPosOff);
+  unsigned long long *tiles = reinterpret_cast<unsigned long long *>(base + kNaTileOff);
+  cudaStream_t s = as_stream(stream);
+  const uint32_t nb = (uint32_t)g->num_buckets;  // >= 1: every vertex owns a bucket
+  const uint32_t nt = (nb + kScanTile - 1) / kScanTile;
+  GraphView v = g->view();
+  const int blocks = group_grid(nb, g->device);
+  if (g->weighted)
+    k_bucket_live<true><<<blocks, 256, 0, s>>>(v, cnt);
+  else
+    k_bucket_live<false><<<blocks, 256, 0, s>>>(v, cnt);
+  k_scan_tiles<<<nt, kScanBlock, 0, s>>>(cnt, nb, tiles);
+  k_scan_sums<<<1, kScanBlock, 0, s>>>(tiles, nt);
+  k_scan_apply<<<nt, kScanBlock, 0, s>>>(cnt, nb, tiles, pos);
+  unsigned long long *rp = reinterpret_cast<unsigned long long *>(d_row_ptr);
+  k_rows_from_buckets<<<(g->V + 256) / 256, 256, 0, s>>>(g->boff, g->V, nb, pos, rp);
+  if (g->weighted)
+    k_bucket_fill<true><<<blocks, 256, 0, s>>>(v, pos, d_col, d_w);
+  else
+    k_bucket_fill<false><<<blocks, 256, 0, s>>>(v, pos, d_col, nullptr);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
 mk_status mk_graph_count_tombstones(mk_graph *g, uint32_t *d_out, void *stream) {
   if (!g || !d_out) return fail(MK_ERR_INVALID, "mk_graph_count_tombstones: null argument");
   DeviceGuard dg(g->device);
