@@ -311,26 +311,34 @@ mk_status mk_graphset_destroy(mk_graphset *s);
 mk_status mk_graphset_union(mk_graphset *s, mk_graph **g);
 /* Copies the num_graphs + 1 vertex offsets to host memory. */
 mk_status mk_graphset_offsets(mk_graphset *s, uint32_t *h_offsets);
+/* Device copy of the same offsets, owned by the set. */
+mk_status mk_graphset_offsets_device(mk_graphset *s, const uint32_t **d_offsets);
 /* Vertex bitmap (ceil(V/32) device words) of the members whose byte in
  * d_graph_flags[num_graphs] is non-zero; feeds mk_wcc_static_subset. */
 mk_status mk_graphset_select_bits(mk_graphset *s, const uint8_t *d_graph_flags,
                                   uint32_t *d_bits, void *stream);
-/* R-MAT edges per member on the device: member m gets the edges
- * [d_edge_offsets[m], d_edge_offsets[m+1]) (u64 device array of
- * num_graphs + 1 ascending entries), drawn with probabilities a, b, c over
- * the member's own vertex range; no self-loops (members of one vertex get
- * self-loops, which updates skip); duplicates possible.  d_w may be NULL. */
-mk_status mk_gen_rmat_set(mk_graphset *s, const uint64_t *d_edge_offsets, double a,
-                          double b, double c, uint64_t seed, uint32_t w_lo,
-                          uint32_t w_hi, uint32_t *d_src, uint32_t *d_dst,
-                          uint32_t *d_w, void *stream);
+/* R-MAT edges per member on the current device.  Member m owns the vertex
+ * ids [d_vertex_offsets[m], d_vertex_offsets[m+1]) (u32 device array of
+ * num_graphs + 1 ascending entries, as a set's offsets) and gets the edges
+ * [d_edge_offsets[m], d_edge_offsets[m+1]) (u64 device array), drawn with
+ * probabilities a, b, c over its own vertex range; no self-loops (members of
+ * one vertex get self-loops, which updates skip); duplicates possible.
+ * Edge i depends only on (seed, i).  d_w may be NULL.  Needs no graph, so
+ * degree hints can be computed before the set is created. */
+mk_status mk_gen_rmat_set(const uint32_t *d_vertex_offsets, uint32_t num_graphs,
+                          const uint64_t *d_edge_offsets, double a, double b,
+                          double c, uint64_t seed, uint32_t w_lo, uint32_t w_hi,
+                          uint32_t *d_src, uint32_t *d_dst, uint32_t *d_w,
+                          void *stream);
 /* Random update batches per member on the device: deletes of live edges
  * drawn from a CSR export of the union graph (d_row_ptr, d_col as written
  * by mk_graph_export_csr) and inserts of uniform pairs of distinct vertices
  * inside each member, counts per member given by the u64 offset arrays
- * d_del_offsets / d_ins_offsets (num_graphs + 1 entries).  d_ins_w may be
- * NULL. */
-mk_status mk_gen_set_batches(mk_graphset *s, const uint64_t *d_row_ptr,
+ * d_del_offsets / d_ins_offsets (num_graphs + 1 entries); vertex offsets
+ * as for mk_gen_rmat_set.  A member without live edges gets self-loop
+ * deletes (no-ops).  d_ins_w may be NULL. */
+mk_status mk_gen_set_batches(const uint32_t *d_vertex_offsets, uint32_t num_graphs,
+                             const uint64_t *d_row_ptr,
                              const uint32_t *d_col, const uint64_t *d_del_offsets,
                              const uint64_t *d_ins_offsets, uint64_t seed,
                              uint32_t w_lo, uint32_t w_hi, uint32_t *d_del_src,

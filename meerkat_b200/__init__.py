@@ -19,7 +19,7 @@ import numpy as np
 from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
 __all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "TC", "WCC", "EdgeSet",
-           "gen_rmat", "gen_grid", "MeerkatError", "MK_INF", "lib", "version"]
+           "gen_rmat", "gen_grid", "gen_rmat_members", "MeerkatError", "MK_INF", "lib", "version"]
 
 
 def version() -> str:
@@ -501,23 +501,18 @@ class GraphSet:
                                             _stream(stream)), "mk_graphset_select_bits")
         return bits
 
+    def offsets_device(self) -> int:
+        p = C.c_void_p()
+        check(lib().mk_graphset_offsets_device(self._h, C.byref(p)), "mk_graphset_offsets_device")
+        return p.value
+
     def gen_rmat(self, edges_per_graph, a=0.57, b=0.19, c=0.19, seed=0, w_lo=1, w_hi=64,
                  weights=True, stream=None):
         """Device R-MAT edges, edges_per_graph[m] inside member m (int32 tensors
         holding uint32 ids)."""
-        import torch
-        cnt = np.asarray(edges_per_graph, dtype=np.uint64)
-        off = np.zeros(self.num_graphs + 1, dtype=np.uint64)
-        np.cumsum(cnt, out=off[1:])
-        E = int(off[-1])
-        d_off = torch.from_numpy(off.view(np.int64)).to(self._dev())
-        src = torch.empty(max(E, 1), dtype=torch.int32, device=self._dev())
-        dst = torch.empty(max(E, 1), dtype=torch.int32, device=self._dev())
-        w = torch.empty(max(E, 1), dtype=torch.int32, device=self._dev()) if weights else None
-        check(lib().mk_gen_rmat_set(self._h, d_off.data_ptr(), a, b, c, seed, w_lo, w_hi,
-                                    src.data_ptr(), dst.data_ptr(), _ptr(w), _stream(stream)),
-              "mk_gen_rmat_set")
-        return src[:E], dst[:E], (w[:E] if w is not None else None)
+        return gen_rmat_members(self.offsets, edges_per_graph, a, b, c, seed, w_lo, w_hi, weights,
+                                device=self.device, stream=stream,
+                                d_vertex_offsets=self.offsets_device())
 
     def gen_batches(self, deletes_per_graph, inserts_per_graph, seed=0, w_lo=1, w_hi=64,
                     weights=True, stream=None):
@@ -543,11 +538,44 @@ class GraphSet:
         is_ = torch.empty(max(ni, 1), dtype=torch.int32, device=dev)
         id_ = torch.empty(max(ni, 1), dtype=torch.int32, device=dev)
         iw = torch.empty(max(ni, 1), dtype=torch.int32, device=dev) if weights else None
-        check(lib().mk_gen_set_batches(self._h, rp.data_ptr(), col.data_ptr(), d_do.data_ptr(),
+        check(lib().mk_gen_set_batches(self.offsets_device(), self.num_graphs, rp.data_ptr(),
+                                       col.data_ptr(), d_do.data_ptr(),
                                        d_io.data_ptr(), seed, w_lo, w_hi, ds.data_ptr(),
                                        dd.data_ptr(), is_.data_ptr(), id_.data_ptr(), _ptr(iw),
                                        _stream(stream)), "mk_gen_set_batches")
         return ds[:nd], dd[:nd], is_[:ni], id_[:ni], (iw[:ni] if iw is not None else None)
+
+
+def gen_rmat_members(vertex_offsets, edges_per_graph, a=0.57, b=0.19, c=0.19, seed=0, w_lo=1,
+                     w_hi=64, weights=True, device: int = 0, stream=None, d_vertex_offsets=None):
+    """Device R-MAT edges for the members of a (future) graph set: member m
+    owns vertex ids vertex_offsets[m] .. vertex_offsets[m+1]-1 and gets
+    edges_per_graph[m] edges.  Returns int32 tensors holding uint32 ids."""
+    import torch
+    dev = f"cuda:{device}"
+    voff = np.ascontiguousarray(np.asarray(vertex_offsets, dtype=np.uint32))
+    G = len(voff) - 1
+    keep = None
+    if d_vertex_offsets is None:
+        keep = torch.from_numpy(voff.view(np.int32)).to(dev)
+        d_vertex_offsets = keep.data_ptr()
+    cnt = np.asarray(edges_per_graph, dtype=np.uint64)
+    if len(cnt) != G:
+        raise ValueError("one edge count per member")
+    off = np.zeros(G + 1, dtype=np.uint64)
+    np.cumsum(cnt, out=off[1:])
+    E = int(off[-1])
+    d_off = torch.from_numpy(off.view(np.int64)).to(dev)
+    src = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+    dst = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+    w = torch.empty(max(E, 1), dtype=torch.int32, device=dev) if weights else None
+    check(lib().mk_gen_rmat_set(d_vertex_offsets, G, d_off.data_ptr(), a, b, c, seed, w_lo, w_hi,
+                                src.data_ptr(), dst.data_ptr(), _ptr(w), _stream(stream)),
+          "mk_gen_rmat_set")
+    if keep is not None:  # the kernel reads the offsets: keep them until it is done
+        torch.cuda.synchronize(dev)
+        del keep
+    return src[:E], dst[:E], (w[:E] if w is not None else None)
 
 
 # ---------------------------------------------------------------------------

@@ -99,10 +99,11 @@ SIGNATURES = [
     ("mk_graphset_union", _S, [vp, C.POINTER(vp)]),
     ("mk_graphset_offsets", _S, [vp, u32p]),
     ("mk_graphset_select_bits", _S, [vp, vp, vp, vp]),
-    ("mk_gen_rmat_set", _S, [vp, vp, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_uint32,
-                             C.c_uint32, vp, vp, vp, vp]),
-    ("mk_gen_set_batches", _S, [vp, vp, vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp,
-                                vp, vp, vp]),
+    ("mk_graphset_offsets_device", _S, [vp, C.POINTER(vp)]),
+    ("mk_gen_rmat_set", _S, [vp, C.c_uint32, vp, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                             C.c_uint32, C.c_uint32, vp, vp, vp, vp]),
+    ("mk_gen_set_batches", _S, [vp, C.c_uint32, vp, vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32,
+                                vp, vp, vp, vp, vp, vp]),
     ("mk_gen_rmat", _S, [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_double, C.c_uint64,
                          C.c_uint32, C.c_uint32, vp, vp, vp]),
     ("mk_gen_grid", _S, [C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp,

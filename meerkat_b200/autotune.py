@@ -83,3 +83,21 @@ def tune_updates(G, batches: Iterable[Sequence], variants: Sequence[Tuple[int, i
     return {"best": {"update_kernel": best["update_kernel"],
                      "update_blocks_per_sm": best["update_blocks_per_sm"]},
             "trials": trials}
+
+
+# buckets per BFS/SSSP frontier work item
+CHUNKS: Tuple[int, ...] = (1, 2, 4, 8, 16, 32)
+
+
+def tune_frontier_chunk(G, traversal, chunks: Sequence[int] = CHUNKS, repeats: int = 2) -> dict:
+    """Times traversal.Static() (idempotent: it recomputes from the sources)
+    once per frontier chunk size, keeps the fastest on G.  Returns
+    {"best": chunk, "trials": [{"frontier_chunk": c, "static_ms": t}, ...]}."""
+    trials: List[dict] = []
+    for c in chunks:
+        G.set_tuning(frontier_chunk=c)
+        t = min(traversal.Static() for _ in range(max(1, repeats)))
+        trials.append({"frontier_chunk": int(c), "static_ms": t})
+    best = min(trials, key=lambda t: t["static_ms"])
+    G.set_tuning(frontier_chunk=best["frontier_chunk"])
+    return {"best": best["frontier_chunk"], "trials": trials}

@@ -271,51 +271,64 @@ mk_status mk_graphset_select_bits(mk_graphset *s, const uint8_t *d_graph_flags, 
   return MK_OK;
 }
 
-mk_status mk_gen_rmat_set(mk_graphset *s, const uint64_t *d_edge_offsets, double a, double b,
-                          double c, uint64_t seed, uint32_t w_lo, uint32_t w_hi, uint32_t *d_src,
+mk_status mk_graphset_offsets_device(mk_graphset *s, const uint32_t **d_offsets) {
+  if (!s || !d_offsets) return fail(MK_ERR_INVALID, "mk_graphset_offsets_device: null argument");
+  *d_offsets = s->d_off;
+  return MK_OK;
+}
+
+mk_status mk_gen_rmat_set(const uint32_t *d_vertex_offsets, uint32_t num_graphs,
+                          const uint64_t *d_edge_offsets, double a, double b, double c,
+                          uint64_t seed, uint32_t w_lo, uint32_t w_hi, uint32_t *d_src,
                           uint32_t *d_dst, uint32_t *d_w, void *stream) {
-  if (!s || !d_edge_offsets || !d_src || !d_dst)
+  if (!d_vertex_offsets || !d_edge_offsets || !d_src || !d_dst)
     return fail(MK_ERR_INVALID, "mk_gen_rmat_set: null argument");
+  if (num_graphs == 0) return fail(MK_ERR_INVALID, "mk_gen_rmat_set: no member graph");
   if (!(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0))
     return fail(MK_ERR_INVALID, "mk_gen_rmat_set: a, b, c must be probabilities with a+b+c <= 1");
   if (w_lo > w_hi) return fail(MK_ERR_INVALID, "mk_gen_rmat_set: w_lo > w_hi");
-  DeviceGuard dg(s->g->device);
+  int device = 0;
+  MK_CUDA(cudaGetDevice(&device));
   cudaStream_t st = as_stream(stream);
   const unsigned long long *eoff = reinterpret_cast<const unsigned long long *>(d_edge_offsets);
   unsigned long long total = 0;
-  MK_CHECK(read_total(eoff, s->ngraphs, st, &total));
+  MK_CHECK(read_total(eoff, num_graphs, st, &total));
   if (total == 0) return MK_OK;
-  k_gen_rmat_set<<<gen_grid(total, s->g->device), 256, 0, st>>>(
-      s->d_off, s->ngraphs, eoff, total, a, a + b, a + b + c, seed, w_lo, w_hi, d_src, d_dst, d_w);
+  k_gen_rmat_set<<<gen_grid(total, device), 256, 0, st>>>(
+      d_vertex_offsets, num_graphs, eoff, total, a, a + b, a + b + c, seed, w_lo, w_hi, d_src,
+      d_dst, d_w);
   MK_CUDA(cudaGetLastError());
   return MK_OK;
 }
 
-mk_status mk_gen_set_batches(mk_graphset *s, const uint64_t *d_row_ptr, const uint32_t *d_col,
+mk_status mk_gen_set_batches(const uint32_t *d_vertex_offsets, uint32_t num_graphs,
+                             const uint64_t *d_row_ptr, const uint32_t *d_col,
                              const uint64_t *d_del_offsets, const uint64_t *d_ins_offsets,
                              uint64_t seed, uint32_t w_lo, uint32_t w_hi, uint32_t *d_del_src,
                              uint32_t *d_del_dst, uint32_t *d_ins_src, uint32_t *d_ins_dst,
                              uint32_t *d_ins_w, void *stream) {
-  if (!s || !d_row_ptr || !d_col || !d_del_offsets || !d_ins_offsets)
+  if (!d_vertex_offsets || !d_row_ptr || !d_col || !d_del_offsets || !d_ins_offsets)
     return fail(MK_ERR_INVALID, "mk_gen_set_batches: null argument");
+  if (num_graphs == 0) return fail(MK_ERR_INVALID, "mk_gen_set_batches: no member graph");
   if (w_lo > w_hi) return fail(MK_ERR_INVALID, "mk_gen_set_batches: w_lo > w_hi");
-  DeviceGuard dg(s->g->device);
+  int device = 0;
+  MK_CUDA(cudaGetDevice(&device));
   cudaStream_t st = as_stream(stream);
   const auto *doff = reinterpret_cast<const unsigned long long *>(d_del_offsets);
   const auto *ioff = reinterpret_cast<const unsigned long long *>(d_ins_offsets);
   const auto *rp = reinterpret_cast<const unsigned long long *>(d_row_ptr);
   unsigned long long nd = 0, ni = 0;
-  MK_CHECK(read_total(doff, s->ngraphs, st, &nd));
-  MK_CHECK(read_total(ioff, s->ngraphs, st, &ni));
+  MK_CHECK(read_total(doff, num_graphs, st, &nd));
+  MK_CHECK(read_total(ioff, num_graphs, st, &ni));
   if (nd) {
     if (!d_del_src || !d_del_dst) return fail(MK_ERR_INVALID, "mk_gen_set_batches: null delete output");
-    k_gen_set_deletes<<<gen_grid(nd, s->g->device), 256, 0, st>>>(s->d_off, s->ngraphs, rp, d_col,
-                                                                    doff, nd, seed, d_del_src, d_del_dst);
+    k_gen_set_deletes<<<gen_grid(nd, device), 256, 0, st>>>(d_vertex_offsets, num_graphs, rp, d_col,
+                                                              doff, nd, seed, d_del_src, d_del_dst);
   }
   if (ni) {
     if (!d_ins_src || !d_ins_dst) return fail(MK_ERR_INVALID, "mk_gen_set_batches: null insert output");
-    k_gen_set_inserts<<<gen_grid(ni, s->g->device), 256, 0, st>>>(
-        s->d_off, s->ngraphs, ioff, ni, seed, w_lo, w_hi, d_ins_src, d_ins_dst, d_ins_w);
+    k_gen_set_inserts<<<gen_grid(ni, device), 256, 0, st>>>(
+        d_vertex_offsets, num_graphs, ioff, ni, seed, w_lo, w_hi, d_ins_src, d_ins_dst, d_ins_w);
   }
   MK_CUDA(cudaGetLastError());
   return MK_OK;
