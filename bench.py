@@ -17,8 +17,14 @@ Reported:
   incremental / decremental BFS and SSSP ms per batch after each sub-batch
   cpu_baseline  the CPU oracle (multithreaded port) applying mixed batches
                 on the same graph
+  batched    4,096 small graphs (V log-uniform in [1024, 65536]) advanced by
+             the batched runner (one graph set, one coalesced launch sequence
+             per step, CUDA-graph replay) against the per-graph launch
+             sequence on the same members and batches, with every member's
+             answer checked equal in both arms
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --workload batched [--graphs G]   # the batched comparison alone
 """
 from __future__ import annotations
 
@@ -252,29 +258,27 @@ def config_block(n):
             "bucket probes)", "parallelism": f"replicas x{n}" if n > 1 else "single GPU"}
 
 
-def run_batched(args, rank, world, local):
+def batched_compare(num_graphs, K, W, rank, world, local):
     """Many small graphs: the batched runner (one GraphSet, one coalesced launch
     sequence per step, CUDA-graph replay) against the plain per-graph launch
     sequence (one DynamicGraph and one BFS/WCC object per member) on the same
     seeded members and batches.  A step = one mixed update batch per member
     (U[1%,10%] of its edges, half deletes of live edges, half inserts of
-    random pairs; steps alternate a batch and its inverse) plus one query per
-    member (BFS from a seeded source or the member's components).  Every
-    member's final BFS levels / component labels must be equal in both arms."""
+    random pairs; steps alternate a batch and its inverse, so from the second
+    step on the graphs cycle through two states) plus one query per member
+    (BFS from a seeded source or the member's components).  The plain arm is
+    timed twice: issued from the host, and captured into a CUDA graph.  Every
+    member's final BFS levels / component labels must be equal in both arms.
+    Returns the summary dict (rank 0 reports it)."""
     import torch
 
     import meerkat_b200 as mk
     from meerkat_b200 import batched as B
     from meerkat_b200.autotune import VARIANTS, tune_frontier_chunk, tune_updates
-    from meerkat_b200.build import build
-    if rank == 0:
-        build()
-    barrier(world)
-    torch.cuda.set_device(local)
     dev = torch.device(f"cuda:{local}")
     stream = torch.cuda.current_stream(dev)
-    K, W = args.steps, max(args.warmup, len(VARIANTS))
-    spec = B.make_spec(args.graphs, seed=B.DEFAULT_SEED + rank)
+    K = max(2, K + (K % 2))  # even: both arms end in the same state of the cycle
+    spec = B.make_spec(num_graphs, seed=B.DEFAULT_SEED + rank)
     Gn = spec.num_graphs
     voff = B._offsets(spec.num_vertices)
     eoff = B._offsets(spec.num_edges)
@@ -307,10 +311,8 @@ def run_batched(args, rank, world, local):
     deg = gs.graph.degrees()
     bfs_members = np.flatnonzero(spec.query == B.QUERY_BFS)
     srcs = B.pick_sources(deg, voff, bfs_members, seed=spec.seed + 1)
-    t0 = time.time()
     br = B.BatchedRunner(gs, spec.query, srcs)
     pr = B.PlainRunner(plain, spec.query, srcs)
-    log(f"[batched] runners ready in {time.time() - t0:.1f}s")
 
     # one batch and its inverse, global ids for the set, local ids per member
     fwd = gs.gen_batches(spec.deletes, spec.inserts, seed=spec.seed + 2, w_lo=1, w_hi=64)
@@ -334,69 +336,78 @@ def run_batched(args, rank, world, local):
 
     fwd_local = local_slices(fwd, spec.deletes, spec.inserts)
     rev_local = local_slices(rev, spec.inserts, spec.deletes)
-    upd_per_step = [int(spec.deletes.sum() + spec.inserts.sum())] * 2
-    gs.graph.reserve_batch(max(int(spec.deletes.sum()), int(spec.inserts.sum())))
+    upd = int(spec.deletes.sum() + spec.inserts.sum())
+    both = [fwd, rev]
+    both_local = [fwd_local, rev_local]
 
-    # warm-up: the first steps tune the update kernel on the set (real steps)
-    tuning = tune_updates(gs.graph, [fwd if i % 2 == 0 else rev for i in range(len(VARIANTS))],
-                          stream=stream)
-    for i in range(len(VARIANTS)):
-        br.query()
-    for i in range(len(VARIANTS), W):
-        br.step(fwd if i % 2 == 0 else rev)
+    # warm-up: one cold step, then 2 rounds of the update tuner (real steps),
+    # then the frontier-chunk tuner (static BFS is idempotent)
+    nt = 2 * len(VARIANTS)
+    Wb = max(W, 1 + nt)
+    br.step(both[0])
+    tuning = tune_updates(gs.graph, [both[i % 2] for i in range(1, 1 + nt)], stream=stream,
+                          rounds=2)
+    for i in range(1 + nt, Wb):
+        br.step(both[i % 2])
+    br.query()
     chunk = tune_frontier_chunk(gs.graph, br.bfs) if br.bfs is not None else None
-    for i in range(W):
-        pr.step(fwd_local if i % 2 == 0 else rev_local)
+    for i in range(Wb):
+        pr.step(both_local[i % 2])
     torch.cuda.synchronize(dev)
     assert gs.graph.sync() == 0 and all(g.sync() == 0 for g in plain)
 
-    # ---- batched arm: K steps captured into one CUDA graph, replayed once ----
-    cap_stream = torch.cuda.Stream(dev)
-    cap_stream.wait_stream(stream)
-    captured = True
-    try:
-        cgraph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(cgraph, stream=cap_stream):
-            for i in range(W, W + K):
-                br.step(fwd if i % 2 == 0 else rev, stream=cap_stream)
-    except Exception as ex:  # capture refused: time the same launches directly
-        log(f"[batched] CUDA-graph capture failed ({ex}); timing direct launches")
-        captured = False
-        cgraph = None
-    torch.cuda.synchronize(dev)
-    barrier(world)
-    clocks = Clocks(local)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(cap_stream):
-        e0.record(cap_stream)
-        if captured:
-            cgraph.replay()
-        else:
-            for i in range(W, W + K):
-                br.step(fwd if i % 2 == 0 else rev, stream=cap_stream)
-        e1.record(cap_stream)
-    e1.synchronize()
-    batched_ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / K
-    assert gs.graph.sync() == 0
-    # ---- plain arm: the per-graph launch sequence, issued from the host ----
-    torch.cuda.synchronize(dev)
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    p0.record(stream)
-    for i in range(W, W + K):
-        pr.step(fwd_local if i % 2 == 0 else rev_local)
-    p1.record(stream)
-    p1.synchronize()
-    clk = clocks.stop()
-    plain_ms = max_over_ranks(p0.elapsed_time(p1), world, dev) / K
-    assert all(g.sync() == 0 for g in plain)
-    del cgraph
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_ = torch.cuda.current_stream(dev)
+        e0.record(s_)
+        fn()
+        e1.record(s_)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1), world, dev)
 
-    # ---- every member's answer is the same in both arms ----
+    def capture(fn):
+        cs = torch.cuda.Stream(dev)
+        cs.wait_stream(stream)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=cs):
+            fn(cs)
+        torch.cuda.synchronize(dev)
+        return g, cs
+
+    clocks = Clocks(local)
+    # batched arm: K steps captured into one CUDA graph, replayed once
+    bg, bs = capture(lambda cs: [br.step(both[i % 2], stream=cs) for i in range(Wb, Wb + K)])
+    barrier(world)
+    with torch.cuda.stream(bs):
+        batched_ms = timed(bg.replay) / K
+    assert gs.graph.sync() == 0
+    del bg
+    # plain arm, issued from the host: K steps
+    barrier(world)
+    plain_ms = timed(lambda: [pr.step(both_local[i % 2]) for i in range(Wb, Wb + K)]) / K
+    assert all(g.sync() == 0 for g in plain)
+    # plain arm captured: the next two steps of the alternation per graph,
+    # replayed K / 2 times, so the plain graphs end on the same state of the
+    # two-state cycle as the batched set
+    t0 = time.time()
+    pg, ps = capture(lambda cs: [pr.step(both_local[(Wb + K + i) % 2], stream=cs)
+                                 for i in range(2)])
+    cap_s = time.time() - t0
+    barrier(world)
+
+    def replays():
+        for _ in range(K // 2):
+            pg.replay()
+    with torch.cuda.stream(ps):
+        plain_graph_ms = timed(replays) / K
+    clk = clocks.stop()
+    assert all(g.sync() == 0 for g in plain)
+    del pg
+
+    # every member's answer is the same in both arms
     mism = {"bfs": 0, "wcc": 0}
-    if br.bfs is not None:
-        d_union = br.bfs.Distances()
-    if br.wcc is not None:
-        l_union = br.wcc.Labels().astype(np.int64)
+    d_union = br.bfs.Distances() if br.bfs is not None else None
+    l_union = br.wcc.Labels().astype(np.int64) if br.wcc is not None else None
     for m in range(Gn):
         lo, hi = int(voff[m]), int(voff[m + 1])
         a = pr.algos[m]
@@ -405,33 +416,59 @@ def run_batched(args, rank, world, local):
         else:
             mism["wcc"] += int(not np.array_equal(a.Labels().astype(np.int64), l_union[lo:hi] - lo))
     assert mism == {"bfs": 0, "wcc": 0}, mism
+    out = {
+        "speedup_vs_plain": plain_ms / batched_ms,
+        "speedup_vs_plain_cuda_graph": plain_graph_ms / batched_ms,
+        "batched_ms_per_step": batched_ms, "plain_ms_per_step": plain_ms,
+        "plain_cuda_graph_ms_per_step": plain_graph_ms, "plain_capture_s": cap_s,
+        "steps": K, "warmup": Wb,
+        "workload": f"batched_{Gn}_graphs",
+        "graphs": f"{Gn} R-MAT members, V log-uniform [1024, 65536], average degree power law "
+                  "(exponent 2) on [4, 32], weights U[1,64]",
+        "step": "per member: mixed batch of U[1%,10%] of its edges (half deletes of live edges, "
+                "half inserts), then one BFS or WCC query (coin flip); a batch and its inverse "
+                "alternate",
+        "vertices": V, "edges": E, "updates_per_step": upd,
+        "batched_updates_per_s": upd / (batched_ms / 1000.0),
+        "gpu_launches_per_step": br.launches_per_step(),
+        "plain_launches_per_step": pr.launches_per_step(),
+        "queries": {"bfs_members": int(len(br.bfs_members)), "wcc_members": int(len(br.wcc_members))},
+        "tuning": {"updates": tuning["best"], "frontier_chunk": chunk["best"] if chunk else None},
+        "tuning_trials": {"updates": tuning["trials"], "frontier_chunk": chunk["trials"] if chunk else None},
+        "equality": {"members_checked": Gn, "bfs_mismatches": mism["bfs"],
+                     "wcc_mismatches": mism["wcc"]},
+        "clocks": clk,
+        "graph": {"buckets": info["num_buckets"], "slabs_used": info["slabs_used"],
+                  "device_bytes": info["device_bytes"]},
+    }
+    # release the per-graph objects before the set
+    del pr, br
+    for g in plain:
+        g.close()
+    gs.close()
+    torch.cuda.synchronize(dev)
+    return out
 
-    upd = upd_per_step[0]
+
+def run_batched(args, rank, world, local):
+    import torch
+    from meerkat_b200.build import build
+    if rank == 0:
+        build()
+    barrier(world)
+    torch.cuda.set_device(local)
+    r = batched_compare(args.graphs, args.steps, args.warmup, rank, world, local)
     if rank == 0:
         line = {
             "metric": "batched step speedup (per-graph launches / batched runner)",
-            "value": plain_ms / batched_ms, "unit": "x", "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": batched_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"batched_{Gn}_graphs",
-                       "graphs": f"{Gn} R-MAT members, V log-uniform [1024, 65536], average "
-                                 "degree power law (exponent 2) on [4, 32], weights U[1,64]",
-                       "step": "per member: mixed batch of U[1%,10%] of its edges (half "
-                               "deletes, half inserts), then one BFS or WCC query (coin flip)",
-                       "vertices": V, "edges": E, "updates_per_step": upd,
+            "value": r["speedup_vs_plain"], "unit": "x", "n_gpus": world, "steps": r["steps"],
+            "warmup": r["warmup"], "ms_per_step": r["batched_ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": r["workload"], "graphs": r["graphs"], "step": r["step"],
                        "l2": "inputs larger than L2 (union slab pool and per-graph pools)"},
-            "batched_ms_per_step": batched_ms, "plain_ms_per_step": plain_ms,
-            "batched_updates_per_s": upd / (batched_ms / 1000.0),
-            "batched_cuda_graph": captured,
-            "gpu_launches": K * br.launches_per_step(),
-            "plain_launches_per_step": pr.launches_per_step(),
-            "queries": {"bfs_members": int(len(br.bfs_members)),
-                        "wcc_members": int(len(br.wcc_members))},
-            "tuning": {"updates": tuning, "frontier_chunk": chunk},
-            "equality": {"members_checked": Gn, **mism},
-            "clocks": clk,
-            "graph": {"buckets": info["num_buckets"], "slabs_used": info["slabs_used"],
-                      "device_bytes": info["device_bytes"]},
+            "gpu_launches": r["steps"] * r["gpu_launches_per_step"], "clocks": r["clocks"],
+            "batched": r,
         }
         print(json.dumps(line), flush=True)
     barrier(world)
@@ -458,6 +495,10 @@ def main():
                     help="updates = the headline mixed-batch benchmark; batched = many small "
                          "graphs, batched runner against per-graph launches")
     ap.add_argument("--graphs", type=int, default=4096, help="member graphs (batched workload)")
+    ap.add_argument("--batched-graphs", type=int, default=4096,
+                    help="updates workload: also run the batched many-graph comparison on this "
+                         "many graphs and attach it to the line (0 = skip)")
+    ap.add_argument("--batched-steps", type=int, default=6)
     args = ap.parse_args()
     if args.workload == "batched":
         rank, world, local = dist_setup(args.gpus)
@@ -605,6 +646,7 @@ def main():
 
     # ---- incremental / decremental BFS and SSSP on the same graph ----
     algo = {}
+    bfs = sssp = None
     if A > 0:
         src_v = int(np.argmax(hints))
         bfs, sssp = mk.BFS(G, src_v, V), mk.SSSP(G, src_v, V)
@@ -632,6 +674,17 @@ def main():
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(graph, batches[W:W + K], max_batches=3)
+    batched = None
+    if args.batched_graphs > 0:
+        del bfs, sssp
+        G.close()
+        torch.cuda.synchronize(dev)
+        r = batched_compare(args.batched_graphs, args.batched_steps, W, rank, world, local)
+        batched = {k: r[k] for k in (
+            "workload", "speedup_vs_plain", "speedup_vs_plain_cuda_graph", "batched_ms_per_step",
+            "plain_ms_per_step", "plain_cuda_graph_ms_per_step", "batched_updates_per_s",
+            "updates_per_step", "vertices", "edges", "gpu_launches_per_step",
+            "plain_launches_per_step", "queries", "tuning", "equality", "clocks", "steps")}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
@@ -658,6 +711,8 @@ def main():
         }
         if cb is not None:
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     barrier(world)
     if world > 1:

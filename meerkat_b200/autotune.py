@@ -55,33 +55,43 @@ def store_cached(G, device_name: str, best: dict) -> None:
 
 
 def tune_updates(G, batches: Iterable[Sequence], variants: Sequence[Tuple[int, int]] = VARIANTS,
-                 stream=None) -> dict:
-    """Times one mixed batch per variant (batches: (del_src, del_dst, ins_src,
-    ins_dst, ins_w) device tensors, valid in sequence) and selects the fastest.
-    Returns {"best": {...}, "trials": [...]}."""
+                 stream=None, rounds: int = 1) -> dict:
+    """Times one mixed batch per variant and round (batches: (del_src, del_dst,
+    ins_src, ins_dst, ins_w) device tensors, valid in sequence; rounds x
+    len(variants) of them are consumed) and selects the variant with the
+    smallest mean step time.  Round r visits the variants rotated by r, so with
+    an even variant count and batches of two alternating kinds every variant
+    meets both kinds.  Returns {"best": {...}, "trials": [...]}."""
     import torch
     it = iter(batches)
     trials: List[dict] = []
     s = stream if stream is not None else torch.cuda.current_stream()
-    for kern, bps in variants:
-        b = next(it)
-        G.set_tuning(update_kernel=kern, update_blocks_per_sm=bps)
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        e0.record(s)
-        G.DeleteEdges(b[0], b[1], stream=s)
-        e1.record(s)
-        G.InsertEdges(b[2], b[3], vals=b[4], stream=s)
-        e2.record(s)
-        e2.synchronize()
-        if G.sync() != 0:
-            raise RuntimeError("device error during tuning")
-        trials.append({"update_kernel": kern, "update_blocks_per_sm": bps,
-                       "delete_ms": e0.elapsed_time(e1), "insert_ms": e1.elapsed_time(e2)})
-    best = min(trials, key=lambda t: t["delete_ms"] + t["insert_ms"])
-    G.set_tuning(update_kernel=best["update_kernel"],
-                 update_blocks_per_sm=best["update_blocks_per_sm"])
-    return {"best": {"update_kernel": best["update_kernel"],
-                     "update_blocks_per_sm": best["update_blocks_per_sm"]},
+    n = len(variants)
+    for r in range(max(1, rounds)):
+        for j in range(n):
+            kern, bps = variants[(j + r) % n]
+            b = next(it)
+            G.set_tuning(update_kernel=kern, update_blocks_per_sm=bps)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(s)
+            G.DeleteEdges(b[0], b[1], stream=s)
+            e1.record(s)
+            G.InsertEdges(b[2], b[3], vals=b[4], stream=s)
+            e2.record(s)
+            e2.synchronize()
+            if G.sync() != 0:
+                raise RuntimeError("device error during tuning")
+            trials.append({"update_kernel": kern, "update_blocks_per_sm": bps,
+                           "delete_ms": e0.elapsed_time(e1), "insert_ms": e1.elapsed_time(e2)})
+
+    def mean_ms(v):
+        ts = [t["delete_ms"] + t["insert_ms"] for t in trials
+              if (t["update_kernel"], t["update_blocks_per_sm"]) == v]
+        return sum(ts) / len(ts)
+
+    best = min(variants, key=mean_ms)
+    G.set_tuning(update_kernel=best[0], update_blocks_per_sm=best[1])
+    return {"best": {"update_kernel": best[0], "update_blocks_per_sm": best[1]},
             "trials": trials}
 
 

@@ -39,6 +39,18 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t *p, uint32_t x) {
   return x;
 }
 
+// Root of x without writing: the compress pass uses it, because there a
+// halving store from one thread (p[x] = grandparent) could land after
+// another thread's final p[x] = root and leave x below a non-root.
+__device__ __forceinline__ uint32_t uf_root(const uint32_t *p, uint32_t x) {
+  for (uint32_t it = 0; it < kUfLimit; ++it) {
+    const uint32_t px = __ldcg(p + x);
+    if (px == x) return x;
+    x = px;
+  }
+  return x;
+}
+
 __device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b, uint32_t *err) {
   for (uint32_t it = 0; it < kUfLimit; ++it) {
     uint32_t ra = uf_find(p, a), rb = uf_find(p, b);
@@ -89,7 +101,7 @@ __global__ void k_uf_batch(const uint32_t *__restrict__ src, const uint32_t *__r
 __global__ void k_uf_compress(uint32_t *p, uint32_t V, const uint32_t *sel_bits) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
     if (sel_bits && !((sel_bits[i >> 5] >> (i & 31)) & 1u)) continue;
-    p[i] = uf_find(p, i);
+    p[i] = uf_root(p, i);
   }
 }
 

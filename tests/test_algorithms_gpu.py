@@ -276,3 +276,25 @@ def test_algorithms_with_a_foreign_batch_fall_back_to_recompute():
     O.delete(ds, dd)
     wcc.Decremental(to_dev(ds), to_dev(dd))  # fresh tensors: different pointers
     np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+
+
+def test_wcc_labels_are_roots_on_deep_trees():
+    """Long random paths give deep union-find trees; every label must be the
+    component minimum on every run (the compress pass walks to the root
+    without path-halving stores, which could otherwise overwrite a finished
+    label with a non-root ancestor)."""
+    V = 1 << 20
+    rng = np.random.default_rng(17)
+    perm = rng.permutation(V).astype(np.uint32)
+    # 16 paths of V/16 vertices each, vertex ids shuffled
+    paths = perm.reshape(16, -1)
+    s = paths[:, :-1].ravel()
+    d = paths[:, 1:].ravel()
+    G, _ = make_pair(V, s, d, hints="ones")
+    want = np.empty(V, np.uint32)
+    for row in paths:
+        want[row] = row.min()
+    wcc = mk.WCC(G)
+    for _ in range(8):
+        wcc.Static()
+        np.testing.assert_array_equal(wcc.Labels(), want)
