@@ -131,6 +131,18 @@ mk_status mk_graph_get_info(mk_graph *g, mk_graph_info *out);
  * room for num_edges entries; d_w may be NULL. */
 mk_status mk_graph_export_csr(mk_graph *g, uint64_t *d_row_ptr,
                               uint32_t *d_col, uint32_t *d_w, void *stream);
+/* Live edges of the vertices [v_begin, v_end) (sum of their degrees);
+ * synchronises the stream.  No counterpart in the reference. */
+mk_status mk_graph_count_edges_range(mk_graph *g, uint32_t v_begin, uint32_t v_end,
+                                     void *stream, uint64_t *h_count);
+/* CSR of the rows [v_begin, v_end) only: d_row_ptr gets v_end - v_begin + 1
+ * offsets starting at 0, d_col / d_w (may be NULL) the edges of those rows
+ * (room for mk_graph_count_edges_range of the range).  Column ids stay
+ * global.  Exports one member of a graph set without touching the others;
+ * no counterpart in the reference. */
+mk_status mk_graph_export_csr_range(mk_graph *g, uint32_t v_begin, uint32_t v_end,
+                                    uint64_t *d_row_ptr, uint32_t *d_col,
+                                    uint32_t *d_w, void *stream);
 /* Same output as mk_graph_export_csr, for callers that must not allocate
  * device memory after start-up (no counterpart in the reference).  The
  * plain export grows its scratch with cudaMalloc, which synchronises the
@@ -189,6 +201,11 @@ mk_status mk_bfs_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n
                               mk_traversal **out);
 mk_status mk_sssp_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n,
                                mk_traversal **out);
+/* Replaces the source set (h_sources: n distinct vertices, host memory) of a
+ * BFS or SSSP; the next call must be mk_traversal_static.  Lets a server run
+ * one multi-source query per round with one resident traversal.  No
+ * counterpart in the reference. */
+mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, uint32_t n);
 /* float Static(EdgesN) (BFSImpl.cuh:590-662, SSSPImpl.cuh:607-690). */
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out);
 /* float Incremental(src*, dst*, n) (BFSImpl.cuh:664-753, SSSPImpl.cuh:692-785).
@@ -227,6 +244,10 @@ mk_status mk_pagerank_create(mk_graph *g_rev, float damping, float tol,
                              mk_pagerank **out);
 /* float Static() (PageRankImpl.cuh:218-220). */
 mk_status mk_pagerank_static(mk_pagerank *p, void *stream, float *ms_out);
+/* Static after out-degrees are recounted from the graph: for a graph that
+ * was updated without passing the batches to Incremental/Decremental (a
+ * server's cached view).  No counterpart in the reference. */
+mk_status mk_pagerank_static_recount(mk_pagerank *p, void *stream, float *ms_out);
 /* float Incremental/Decremental(src*, dst*, n) (PageRankImpl.cuh:222-251):
  * out-degrees follow the edges the last graph update applied, then the
  * ranks are re-solved warm-started from the previous ranks. */

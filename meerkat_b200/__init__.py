@@ -200,6 +200,29 @@ class DynamicGraph:
         torch.cuda.synchronize(self.device)
         return out.cpu().numpy().view(np.uint32)
 
+    def count_edges(self, v_begin: int = 0, v_end: Optional[int] = None, stream=None) -> int:
+        """Live edges of the vertices [v_begin, v_end)."""
+        c = C.c_uint64(0)
+        v_end = self.num_vertices if v_end is None else int(v_end)
+        check(lib().mk_graph_count_edges_range(self._h, int(v_begin), v_end, _stream(stream),
+                                               C.byref(c)), "mk_graph_count_edges_range")
+        return c.value
+
+    def export_csr_range_device(self, v_begin: int, v_end: int, weights: bool = False,
+                                stream=None):
+        """Device CSR of the rows [v_begin, v_end): (row_ptr int64[n+1] from 0,
+        col int32[E] with global ids, w int32[E] or None)."""
+        import torch
+        dev = f"cuda:{self.device}"
+        E = self.count_edges(v_begin, v_end, stream=stream)
+        rp = torch.empty(int(v_end) - int(v_begin) + 1, dtype=torch.int64, device=dev)
+        col = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+        w = torch.empty(max(E, 1), dtype=torch.int32, device=dev) if (weights and self.weighted) else None
+        check(lib().mk_graph_export_csr_range(self._h, int(v_begin), int(v_end), rp.data_ptr(),
+                                              col.data_ptr(), _ptr(w), _stream(stream)),
+              "mk_graph_export_csr_range")
+        return rp, col[:E], (w[:E] if w is not None else None)
+
     def export_csr(self, sort_rows: bool = True):
         """Live edges as CSR (row_ptr u64[N+1], col u32[E], w u32[E] or None)."""
         import torch
@@ -255,6 +278,13 @@ class _Traversal(_Timed):
             self.close()
         except Exception:
             pass
+
+    def set_sources(self, sources) -> None:
+        """Replaces the source set (distinct vertices); call Static next."""
+        self.sources = np.ascontiguousarray(np.atleast_1d(np.asarray(sources, dtype=np.uint32)))
+        self.source = self.sources
+        check(lib().mk_traversal_set_sources(self._h, self.sources.ctypes.data_as(
+            C.POINTER(C.c_uint32)), len(self.sources)), "mk_traversal_set_sources")
 
     def Static(self, edges_n=None, stream=None, timed=True):
         return self._call(lib().mk_traversal_static, self._h, _stream(stream), timed=timed)
@@ -330,6 +360,10 @@ class PageRank(_Timed):
 
     def Static(self, stream=None, timed=True):
         return self._call(lib().mk_pagerank_static, self._h, _stream(stream), timed=timed)
+
+    def StaticRecount(self, stream=None, timed=True):
+        """Static after recounting out-degrees (graph updated behind its back)."""
+        return self._call(lib().mk_pagerank_static_recount, self._h, _stream(stream), timed=timed)
 
     def Incremental(self, src, dst, n=None, stream=None, timed=True):
         return self._call(lib().mk_pagerank_incremental, self._h, _ptr(src), _ptr(dst),

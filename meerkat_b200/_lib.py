@@ -55,6 +55,8 @@ SIGNATURES = [
     ("mk_graph_get_info", _S, [vp, C.POINTER(GraphInfo)]),
     ("mk_graph_export_csr", _S, [vp, vp, vp, vp, vp]),
     ("mk_graph_export_csr_noalloc", _S, [vp, vp, vp, vp, vp]),
+    ("mk_graph_count_edges_range", _S, [vp, C.c_uint32, C.c_uint32, vp, u64p]),
+    ("mk_graph_export_csr_range", _S, [vp, C.c_uint32, C.c_uint32, vp, vp, vp, vp]),
     ("mk_graph_count_tombstones", _S, [vp, vp, vp]),
     ("mk_graph_reserve_batch", _S, [vp, C.c_uint32]),
     ("mk_graph_set_tuning", _S, [vp, C.POINTER(Tuning)]),
@@ -63,6 +65,7 @@ SIGNATURES = [
     ("mk_sssp_create", _S, [vp, C.c_uint32, C.POINTER(vp)]),
     ("mk_bfs_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
     ("mk_sssp_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
+    ("mk_traversal_set_sources", _S, [vp, u32p, C.c_uint32]),
     ("mk_traversal_static", _S, [vp, vp, f32p]),
     ("mk_traversal_incremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_traversal_decremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),
@@ -73,6 +76,7 @@ SIGNATURES = [
     ("mk_traversal_destroy", _S, [vp]),
     ("mk_pagerank_create", _S, [vp, C.c_float, C.c_float, C.c_uint32, vp, C.POINTER(vp)]),
     ("mk_pagerank_static", _S, [vp, vp, f32p]),
+    ("mk_pagerank_static_recount", _S, [vp, vp, f32p]),
     ("mk_pagerank_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_pagerank_decremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_pagerank_values", _S, [vp, vp]),

@@ -637,6 +637,91 @@ __global__ void k_bucket_fill(GraphView g, const unsigned long long *__restrict_
   }
 }
 
+// Sum of deg[vb .. ve) into *out (zeroed by the caller).
+__global__ void k_sum_degrees(const uint32_t *__restrict__ deg, uint32_t vb, uint32_t ve,
+                              unsigned long long *out) {
+  unsigned long long acc = 0;
+  for (uint32_t u = vb + blockIdx.x * blockDim.x + threadIdx.x; u < ve; u += gridDim.x * blockDim.x)
+    acc += deg[u];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc) atomicAdd(out, acc);
+}
+
+// Range export: live keys per bucket of the buckets [b0, b0 + nbr), written
+// at bcnt[b - b0].
+template <bool kWeighted>
+__global__ void k_bucket_live_range(GraphView g, uint32_t b0, uint32_t nbr,
+                                    uint32_t *__restrict__ bcnt) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t i = group; i < nbr; i += ngroups) {
+    uint32_t c = 0;
+    walk_bucket(g, L, b0 + i, [&](const uint4 &q) {
+      uint32_t live, tomb;
+      lane_counts<kWeighted>(q, L.gl, live, tomb);
+      c += live;
+    });
+    c = __reduce_add_sync(L.gmask, c);
+    if (L.gl == 0) bcnt[i] = c;
+  }
+}
+
+// row_ptr[u - vb] = position of u's first bucket, relative to the range.
+__global__ void k_rows_from_buckets_range(const uint32_t *__restrict__ boff, uint32_t vb,
+                                          uint32_t nv, uint32_t b0, uint32_t nbr,
+                                          const unsigned long long *__restrict__ bpos,
+                                          unsigned long long *__restrict__ row_ptr) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u <= nv; u += gridDim.x * blockDim.x)
+    row_ptr[u] = bpos[u < nv ? boff[vb + u] - b0 : nbr];
+}
+
+// Writes the live keys of the buckets [b0, b0 + nbr) at their positions.
+template <bool kWeighted>
+__global__ void k_bucket_fill_range(GraphView g, uint32_t b0, uint32_t nbr,
+                                    const unsigned long long *__restrict__ bpos,
+                                    uint32_t *__restrict__ col, uint32_t *__restrict__ wout) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t i = group; i < nbr; i += ngroups) {
+    unsigned long long pos = bpos[i];
+    const unsigned long long end = bpos[i + 1];
+    walk_bucket(g, L, b0 + i, [&](const uint4 &q) {
+      uint32_t live, tomb;
+      lane_counts<kWeighted>(q, L.gl, live, tomb);
+      uint32_t incl = live;
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        uint32_t y = __shfl_up_sync(L.gmask, incl, o, 8);
+        if (L.gl >= (uint32_t)o) incl += y;
+      }
+      uint32_t total = __shfl_sync(L.gmask, incl, L.gbase + 7);
+      unsigned long long p = pos + (incl - live);
+      auto put = [&](uint32_t k, uint32_t val) {
+        if (k < kTombKey) {
+          if (p < end) {
+            col[p] = k;
+            if (wout) wout[p] = val;
+          }
+          ++p;
+        }
+      };
+      if (!kWeighted) {
+        put(q.x, 0);
+        put(q.y, 0);
+        put(q.z, 0);
+        if (L.gl != 7) put(q.w, 0);
+      } else {
+        put(q.x, q.y);
+        if (L.gl != 7) put(q.z, q.w);
+      }
+      pos += total;
+    });
+  }
+}
+
 static int update_grid(uint32_t n, int device) {
   // one warp per 32 edges, at most the resident blocks (each warp loops)
   uint64_t blocks = ((uint64_t)n + kUpdWarps * 32 - 1) / (kUpdWarps * 32);
@@ -967,10 +1052,8 @@ mk_status mk_graph_get_info(mk_graph *g, mk_graph_info *out) {
   uint32_t top = 0;
   MK_CUDA(cudaMemcpy(&top, g->pool_top, 4, cudaMemcpyDeviceToHost));
   // live edges: sum of degrees
-  std::vector<uint32_t> deg(g->V);
-  MK_CUDA(cudaMemcpy(deg.data(), g->deg, (size_t)g->V * 4, cudaMemcpyDeviceToHost));
   uint64_t e = 0;
-  for (uint32_t d : deg) e += d;
+  MK_CHECK(mk_graph_count_edges_range(g, 0, g->V, nullptr, &e));
   out->num_vertices = g->V;
   out->weighted = g->weighted;
   out->reverse = g->reverse;
@@ -980,6 +1063,60 @@ mk_status mk_graph_get_info(mk_graph *g, mk_graph_info *out) {
   out->slabs_used = std::min<uint64_t>(top, g->pool_cap);
   out->num_edges = e;
   out->device_bytes = g->device_bytes;
+  return MK_OK;
+}
+
+mk_status mk_graph_count_edges_range(mk_graph *g, uint32_t v_begin, uint32_t v_end, void *stream,
+                                     uint64_t *h_count) {
+  if (!g || !h_count) return fail(MK_ERR_INVALID, "mk_graph_count_edges_range: null argument");
+  if (v_begin > v_end || v_end > g->V)
+    return fail(MK_ERR_INVALID, "mk_graph_count_edges_range: bad vertex range");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  unsigned long long *acc = g->counters + 1;
+  MK_CUDA(cudaMemsetAsync(acc, 0, 8, s));
+  if (v_end > v_begin) {
+    const uint32_t n = v_end - v_begin;
+    const int blocks = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)device_sm_count(g->device) * 8);
+    k_sum_degrees<<<blocks, 256, 0, s>>>(g->deg, v_begin, v_end, acc);
+    MK_CUDA(cudaGetLastError());
+  }
+  unsigned long long c = 0;
+  MK_CUDA(cudaMemcpyAsync(&c, acc, 8, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  *h_count = c;
+  return MK_OK;
+}
+
+mk_status mk_graph_export_csr_range(mk_graph *g, uint32_t v_begin, uint32_t v_end,
+                                    uint64_t *d_row_ptr, uint32_t *d_col, uint32_t *d_w,
+                                    void *stream) {
+  if (!g || !d_row_ptr || !d_col)
+    return fail(MK_ERR_INVALID, "mk_graph_export_csr_range: null argument");
+  if (v_begin >= v_end || v_end > g->V)
+    return fail(MK_ERR_INVALID, "mk_graph_export_csr_range: bad vertex range");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  const uint32_t b0 = g->h_boff[v_begin];
+  const uint32_t nbr = g->h_boff[v_end] - b0;
+  MK_CHECK(g->bucket_cnt.reserve(nbr, &g->device_bytes));
+  MK_CHECK(g->bucket_pos.reserve((size_t)nbr + 1, &g->device_bytes));
+  GraphView v = g->view();
+  const int blocks = group_grid(nbr, g->device);
+  if (g->weighted)
+    k_bucket_live_range<true><<<blocks, 256, 0, s>>>(v, b0, nbr, g->bucket_cnt.ptr);
+  else
+    k_bucket_live_range<false><<<blocks, 256, 0, s>>>(v, b0, nbr, g->bucket_cnt.ptr);
+  MK_CHECK(scan_u32_to_u64(g->bucket_cnt.ptr, g->bucket_pos.ptr, nbr, g->scan_tmp, s));
+  const uint32_t nv = v_end - v_begin;
+  unsigned long long *rp = reinterpret_cast<unsigned long long *>(d_row_ptr);
+  k_rows_from_buckets_range<<<(nv + 256) / 256, 256, 0, s>>>(g->boff, v_begin, nv, b0, nbr,
+                                                             g->bucket_pos.ptr, rp);
+  if (g->weighted)
+    k_bucket_fill_range<true><<<blocks, 256, 0, s>>>(v, b0, nbr, g->bucket_pos.ptr, d_col, d_w);
+  else
+    k_bucket_fill_range<false><<<blocks, 256, 0, s>>>(v, b0, nbr, g->bucket_pos.ptr, d_col, nullptr);
+  MK_CUDA(cudaGetLastError());
   return MK_OK;
 }
 

@@ -438,6 +438,18 @@ mk_status mk_pagerank_static(mk_pagerank *p, void *stream, float *ms_out) {
   return p->timer.stop(ms_out);
 }
 
+mk_status mk_pagerank_static_recount(mk_pagerank *p, void *stream, float *ms_out) {
+  if (!p) return fail(MK_ERR_INVALID, "mk_pagerank_static_recount: null handle");
+  DeviceGuard dg(p->g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(p->timer.start(s, ms_out != nullptr));
+  MK_CHECK(pr_recount_outdeg(p, s));
+  p->cur = 0;
+  k_fill<<<256, 256, 0, s>>>(p->pr0, p->g->V, 1.0f / (float)p->g->V);
+  MK_CHECK(pr_solve(p, s));
+  return p->timer.stop(ms_out);
+}
+
 static mk_status pr_dynamic(mk_pagerank *p, const uint32_t *d_src, const uint32_t *d_dst,
                             uint32_t n, bool inc, void *stream, float *ms_out) {
   if (!p) return fail(MK_ERR_INVALID, "pagerank dynamic: null handle");

@@ -417,6 +417,7 @@ using namespace mk;
 struct mk_traversal {
   mk_graph *g = nullptr;
   uint32_t nsources = 0;
+  uint32_t src_cap = 0;
   uint32_t *sources = nullptr;  // device copy
   bool sssp = false;
   bool has_static = false;
@@ -436,6 +437,16 @@ __global__ void k_set_sources(unsigned long long *dist, const uint32_t *sources,
     dist[sources[i]] = pack(0, sources[i]);
 }
 
+static mk_status check_sources(const mk_graph *g, const uint32_t *h_sources, uint32_t n,
+                               const char *what) {
+  std::vector<uint32_t> sorted(h_sources, h_sources + n);
+  std::sort(sorted.begin(), sorted.end());
+  if (sorted.back() >= g->V) return fail(MK_ERR_INVALID, std::string(what) + ": source out of range");
+  if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+    return fail(MK_ERR_INVALID, std::string(what) + ": repeated source");
+  return MK_OK;
+}
+
 static mk_status trav_create(mk_graph *g, const uint32_t *h_sources, uint32_t nsrc, bool sssp,
                              mk_traversal **out) {
   if (!g || !out || !h_sources) return fail(MK_ERR_INVALID, "traversal create: null argument");
@@ -443,17 +454,12 @@ static mk_status trav_create(mk_graph *g, const uint32_t *h_sources, uint32_t ns
   if (nsrc == 0) return fail(MK_ERR_INVALID, "traversal create: no source");
   if (g->reverse) return fail(MK_ERR_INVALID, "traversal create: graph must store out-edges");
   if (sssp && !g->weighted) return fail(MK_ERR_INVALID, "SSSP needs a weighted graph");
-  {
-    std::vector<uint32_t> sorted(h_sources, h_sources + nsrc);
-    std::sort(sorted.begin(), sorted.end());
-    if (sorted.back() >= g->V) return fail(MK_ERR_INVALID, "traversal create: source out of range");
-    if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
-      return fail(MK_ERR_INVALID, "traversal create: repeated source");
-  }
+  MK_CHECK(check_sources(g, h_sources, nsrc, "traversal create"));
   DeviceGuard dg(g->device);
   mk_traversal *t = new mk_traversal();
   t->g = g;
   t->nsources = nsrc;
+  t->src_cap = nsrc;
   t->sssp = sssp;
   const size_t V = g->V;
   cudaError_t e = cudaSuccess;
@@ -557,6 +563,26 @@ mk_status mk_bfs_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n
 mk_status mk_sssp_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t n,
                                mk_traversal **out) {
   return trav_create(g, h_sources, n, true, out);
+}
+
+mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, uint32_t n) {
+  if (!t || !h_sources) return fail(MK_ERR_INVALID, "mk_traversal_set_sources: null argument");
+  if (n == 0) return fail(MK_ERR_INVALID, "mk_traversal_set_sources: no source");
+  MK_CHECK(check_sources(t->g, h_sources, n, "mk_traversal_set_sources"));
+  DeviceGuard dg(t->g->device);
+  if (n > t->src_cap) {
+    uint32_t *p = nullptr;
+    MK_CUDA(cudaMalloc(&p, (size_t)n * 4));
+    cudaFree(t->sources);
+    t->sources = p;
+    t->src_cap = n;
+  }
+  // ordered after every earlier launch of this traversal on any stream
+  MK_CUDA(cudaDeviceSynchronize());
+  MK_CUDA(cudaMemcpy(t->sources, h_sources, (size_t)n * 4, cudaMemcpyHostToDevice));
+  t->nsources = n;
+  t->has_static = false;
+  return MK_OK;
 }
 
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out) {

@@ -1,0 +1,119 @@
+"""Serving loop: every query answer is the same when the request is served
+in a coalesced round with other graphs' requests and when it is served alone,
+and equals the oracle's answer on its graph after the updates that arrived
+before it."""
+import copy
+
+import numpy as np
+import pytest
+
+import meerkat_b200 as mk
+from meerkat_b200 import serving as S
+from oracle import OracleGraph
+
+PR_L1_TOL = 1e-6
+
+
+def make_server(seed):
+    nv, ne = S.make_graph_sizes(6, 8, 11, 8, seed)
+    gs, edges = S.build_set(nv, ne, seed)
+    wl = S.Workload(nv, ne, seed)
+    return gs, edges, wl
+
+
+def oracle_answers(nv, edges_h, voff, reqs, pool):
+    """Replays every graph's requests in arrival order on the oracle."""
+    src, dst, w = edges_h
+    Os = []
+    for g in range(len(nv)):
+        Os.append(OracleGraph(int(nv[g])))
+    # initial edges of each member (R-MAT, duplicates collapse in the oracle)
+    owner = np.searchsorted(voff, src, side="right") - 1
+    for g in range(len(nv)):
+        m = owner == g
+        Os[g].insert((src[m] - voff[g]).astype(np.uint32), (dst[m] - voff[g]).astype(np.uint32),
+                     w[m])
+    ps, pd, pw = pool
+    out = {}
+    for r in sorted(reqs, key=lambda r: r.arrival):
+        O, base = Os[r.graph], int(voff[r.graph])
+        if r.kind == S.INSERT:
+            O.insert((ps[r.lo:r.hi] - base).astype(np.uint32), (pd[r.lo:r.hi] - base).astype(np.uint32),
+                     pw[r.lo:r.hi])
+        elif r.kind == S.DELETE:
+            O.delete((ps[r.lo:r.hi] - base).astype(np.uint32), (pd[r.lo:r.hi] - base).astype(np.uint32))
+        elif r.kind == S.BFS_Q:
+            out[r.rid] = O.bfs(r.source)
+        elif r.kind == S.SSSP_Q:
+            out[r.rid] = O.sssp(r.source)
+        elif r.kind == S.WCC_Q:
+            out[r.rid] = O.wcc()
+        elif r.kind == S.TC_Q:
+            out[r.rid] = O.triangles()
+        elif r.kind == S.PAGERANK_Q:
+            out[r.rid] = O.pagerank(0.85, 1e-14)[0]
+    return out
+
+
+def h(t):
+    return t.cpu().numpy().view(np.uint32).astype(np.int64)
+
+
+@pytest.mark.gpu
+def test_alone_and_coalesced_answers_match_each_other_and_the_oracle():
+    seed = 21
+    gsA, edgesA, wlA = make_server(seed)
+    gsB, edgesB, wlB = make_server(seed)
+    # the same seeded log on both sets; every request arrives at once, so the
+    # coalesced server packs up to one request per graph into each round
+    reqsA = S.make_requests(wlA, edgesA, 90, rate=1e7, seed=seed + 1, upd_lo=10, upd_hi=3000)
+    reqsB = S.make_requests(wlB, edgesB, 90, rate=1e7, seed=seed + 1, upd_lo=10, upd_hi=3000)
+    import torch
+    assert torch.equal(wlA.pool_src, wlB.pool_src) and torch.equal(wlA.pool_dst, wlB.pool_dst)
+    kinds = {r.kind for r in reqsA}
+    assert kinds == set(range(7)), kinds
+    voff = gsA.offsets.astype(np.int64)
+    oracle = oracle_answers(wlA.num_vertices, tuple(h(x) for x in edgesA), voff, reqsA,
+                            (h(wlA.pool_src), h(wlA.pool_dst), h(wlA.pool_w)))
+    A = S.GraphServer(gsA, budget_bytes=1 << 36, record=True)
+    B = S.GraphServer(gsB, budget_bytes=1 << 36, record=True)
+    ra = A.run(reqsA, wlA, mode="coalesced")
+    rb = B.run(reqsB, wlB, mode="alone")
+    assert rb["rounds"] == len(reqsB) and ra["rounds"] < len(reqsA)
+    for x, y in zip(reqsA, reqsB):
+        assert x.rid == y.rid and x.kind == y.kind
+        if x.kind in (S.INSERT, S.DELETE):
+            continue
+        want = oracle[x.rid]
+        if x.kind == S.PAGERANK_Q:
+            assert np.abs(x.result.astype(np.float64) - want).sum() <= PR_L1_TOL
+            assert np.abs(y.result.astype(np.float64) - want).sum() <= PR_L1_TOL
+            assert np.abs(x.result.astype(np.float64) - y.result).sum() <= PR_L1_TOL
+        elif x.kind == S.TC_Q:
+            assert x.result == y.result == want
+        else:
+            np.testing.assert_array_equal(x.result, want)
+            np.testing.assert_array_equal(y.result, want)
+    A.close()
+    B.close()
+
+
+@pytest.mark.gpu
+def test_views_are_evicted_under_a_small_budget():
+    seed = 5
+    gs, edges, wl = make_server(seed)
+    reqs = S.make_requests(wl, edges, 40, rate=1e7, seed=7,
+                           mix=(0.1, 0.1, 0, 0, 0.4, 0.4, 0), upd_lo=10, upd_hi=500)
+    srv = S.GraphServer(gs, budget_bytes=1 << 40, record=True)
+    srv.budget = srv.resident + (4 << 20)  # room for about one view
+    r = srv.run(reqs, wl, mode="coalesced")
+    assert r["view_builds"] >= 2 and r["view_evictions"] >= 1
+    assert srv.resident + srv.view_bytes() <= srv.budget
+    srv.close()
+
+
+def test_request_log_is_seeded():
+    nv, ne = S.make_graph_sizes(8, 10, 14, 16, 3)
+    nv2, ne2 = S.make_graph_sizes(8, 10, 14, 16, 3)
+    assert (nv == nv2).all() and (ne == 16 * nv).all()
+    assert nv.min() >= 1 << 10 and nv.max() <= 1 << 14
