@@ -450,6 +450,85 @@ def batched_compare(num_graphs, K, W, rank, world, local):
     return out
 
 
+def run_serving(args, rank, world, local):
+    """Open-loop serving: G resident R-MAT graphs (scales uniform in the given
+    range, edge factor 16, weights U[1,1000]) in one graph set under a device
+    memory budget; Poisson arrivals at each offered rate; mix 50% updates
+    (log-uniform 1K-1M edges, half inserts, half deletes), 30% BFS/SSSP, 10%
+    PageRank, 10% TC/WCC.  Each rate is served twice with the same request
+    log: coalesced (continuous batching, one request per graph per round) and
+    alone (one request per round: the plain per-request launch sequence)."""
+    import torch
+
+    from meerkat_b200 import serving as S
+    from meerkat_b200.build import build
+    if rank == 0:
+        build()
+    barrier(world)
+    torch.cuda.set_device(local)
+    seed = SEED + 7 + rank
+    lo_s, hi_s = (int(x) for x in args.serving_scales.split(","))
+    rates = [float(x) for x in args.serving_rates.split(",")]
+    N = args.serving_requests
+    t0 = time.time()
+    nv, ne = S.make_graph_sizes(args.serving_graphs, lo_s, hi_s, 16, seed)
+    gs, edges = S.build_set(nv, ne, seed, device=local)
+    log(f"[serving] {len(nv)} graphs, {int(nv.sum())} vertices, {int(ne.sum())} edges loaded "
+        f"in {time.time() - t0:.1f}s: {gs.graph.info()}")
+    wl = S.Workload(nv, ne, seed)
+    warm = S.make_requests(wl, edges, 64, rate=1e6, seed=seed + 1, device=local)
+    blocks = []
+    for j, rate in enumerate(rates):
+        reqs = S.make_requests(wl, edges, N, rate=rate, seed=seed + 100 + j, device=local)
+        blocks.append((rate, reqs))
+    del edges
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    srv = S.GraphServer(gs, budget_bytes=int(args.serving_budget_gb * 1e9), device=local)
+    srv.run(warm, wl, mode="coalesced")
+    clocks = Clocks(local)
+    table = []
+    for rate, reqs in blocks:
+        row = {"offered_rps": rate}
+        for mode in ("coalesced", "alone"):
+            rs = [S.Request(r.rid, r.graph, r.kind, r.arrival, r.source, r.lo, r.hi) for r in reqs]
+            t1 = time.time()
+            out = srv.run(rs, wl, mode=mode)
+            log(f"[serving] {rate:.0f} rps {mode}: p50 {out['p50_ms']:.2f} ms p99 "
+                f"{out['p99_ms']:.2f} ms, {out['throughput_rps']:.1f} rps, {out['rounds']} rounds, "
+                f"{time.time() - t1:.1f}s")
+            row[mode] = out
+        table.append(row)
+    clk = clocks.stop()
+    top = table[-1]
+    if rank == 0:
+        line = {
+            "metric": "serving throughput at the highest offered rate (coalesced)",
+            "value": top["coalesced"]["throughput_rps"], "unit": "requests/s", "n_gpus": world,
+            "steps": len(rates), "warmup": len(warm), "ms_per_step": top["coalesced"]["p50_ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": f"serving_{len(nv)}_graphs",
+                       "graphs": f"{len(nv)} R-MAT graphs, scales U{{{lo_s}..{hi_s}}}, edge factor "
+                                 "16, weights U[1,1000]",
+                       "vertices": int(nv.sum()), "edges": int(ne.sum()),
+                       "mix": "25% insert, 25% delete (1K-1M edges, log-uniform), 15% BFS, "
+                              "15% SSSP, 10% PageRank, 5% TC, 5% WCC; graph uniform",
+                       "arrivals": "open-loop Poisson", "requests_per_rate": N,
+                       "budget_gb": args.serving_budget_gb},
+            "p50_ms": top["coalesced"]["p50_ms"], "p99_ms": top["coalesced"]["p99_ms"],
+            "rates": table, "clocks": clk,
+            "resident_bytes": srv.resident, "view_bytes": srv.view_bytes(),
+        }
+        print(json.dumps(line), flush=True)
+    srv.close()
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def run_batched(args, rank, world, local):
     import torch
     from meerkat_b200.build import build
@@ -491,7 +570,7 @@ def main():
     ap.add_argument("--batch", type=int, default=500_000, help="edges per sub-batch")
     ap.add_argument("--update-kernel", default="auto", choices=["auto", "0", "1"],
                     help="auto = autotune on the first batches; 0/1 pins a variant")
-    ap.add_argument("--workload", default="updates", choices=["updates", "batched"],
+    ap.add_argument("--workload", default="updates", choices=["updates", "batched", "serving"],
                     help="updates = the headline mixed-batch benchmark; batched = many small "
                          "graphs, batched runner against per-graph launches")
     ap.add_argument("--graphs", type=int, default=4096, help="member graphs (batched workload)")
@@ -499,7 +578,21 @@ def main():
                     help="updates workload: also run the batched many-graph comparison on this "
                          "many graphs and attach it to the line (0 = skip)")
     ap.add_argument("--batched-steps", type=int, default=6)
+    ap.add_argument("--serving-graphs", type=int, default=64)
+    ap.add_argument("--serving-scales", default="18,23", help="R-MAT scale range lo,hi")
+    ap.add_argument("--serving-rates", default="25,50,100,200,400", help="offered req/s")
+    ap.add_argument("--serving-requests", type=int, default=300, help="requests per rate")
+    ap.add_argument("--serving-budget-gb", type=float, default=120.0)
     args = ap.parse_args()
+    if args.workload == "serving":
+        rank, world, local = dist_setup(args.gpus)
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "workload": "serving",
+                                  "unavailable": "the reference has no serving loop and no "
+                                  "CPU path; the oracle port is timed by the updates workload"}))
+            return 0
+        return run_serving(args, rank, world, local)
     if args.workload == "batched":
         rank, world, local = dist_setup(args.gpus)
         if args.impl == "reference":

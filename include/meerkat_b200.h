@@ -299,6 +299,13 @@ mk_status mk_wcc_static(mk_wcc *w, void *stream, float *ms_out);
  * member graphs of a graph set.  No counterpart in the reference. */
 mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stream,
                                float *ms_out);
+/* Recomputes the labels of the vertex ranges [r[2i], r[2i+1]) only
+ * (h_vertex_ranges: 2 * nranges host words), touching nothing else: the
+ * work is proportional to the ranges, not to the graph.  Each range must be
+ * closed under edges (a member of a graph set).  No counterpart in the
+ * reference. */
+mk_status mk_wcc_static_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges,
+                               uint32_t nranges, void *stream, float *ms_out);
 mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src,
                              const uint32_t *d_dst, uint32_t n, void *stream,
                              float *ms_out);

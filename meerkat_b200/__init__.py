@@ -445,6 +445,14 @@ class WCC(_Timed):
     def Static(self, stream=None, timed=True):
         return self._call(lib().mk_wcc_static, self._h, _stream(stream), timed=timed)
 
+    def StaticRanges(self, ranges, stream=None, timed=True):
+        """Recomputes the labels of the vertex ranges [(begin, end), ...] only
+        (each closed under edges, e.g. members of a GraphSet)."""
+        r = np.ascontiguousarray(np.asarray(ranges, dtype=np.uint32).reshape(-1))
+        return self._call(lib().mk_wcc_static_ranges, self._h,
+                          r.ctypes.data_as(C.POINTER(C.c_uint32)), len(r) // 2, _stream(stream),
+                          timed=timed)
+
     def StaticSubset(self, sel_bits, stream=None, timed=True):
         """Recomputes the labels of the vertices whose bit is set in the device
         bitmap `sel_bits` (ceil(V/32) words, closed under edges)."""

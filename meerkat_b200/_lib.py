@@ -92,6 +92,7 @@ SIGNATURES = [
     ("mk_wcc_create", _S, [vp, C.POINTER(vp)]),
     ("mk_wcc_static", _S, [vp, vp, f32p]),
     ("mk_wcc_static_subset", _S, [vp, vp, vp, f32p]),
+    ("mk_wcc_static_ranges", _S, [vp, u32p, C.c_uint32, vp, f32p]),
     ("mk_wcc_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_decremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_labels", _S, [vp, vp]),

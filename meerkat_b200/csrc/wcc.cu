@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "mk_internal.h"
 #include "mk_slab.cuh"
@@ -127,6 +128,61 @@ __global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, 
   }
 }
 
+// ---- vertex-range variants: only the listed ranges are touched ----
+// Ranges are given as prefix sums: range r covers the global indices
+// [pre[r], pre[r+1]) of a concatenation, starting at base[r].
+__device__ __forceinline__ uint32_t range_at(const uint32_t *pre, uint32_t nr, uint32_t i,
+                                             const uint32_t *base) {
+  uint32_t lo = 0, hi = nr;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (pre[mid] <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return base[lo] + (i - pre[lo]);
+}
+
+__global__ void k_uf_init_ranges(uint32_t *p, const uint32_t *vpre, const uint32_t *vbase,
+                                 uint32_t nr) {
+  const uint32_t total = vpre[nr];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const uint32_t v = range_at(vpre, nr, i, vbase);
+    p[v] = v;
+  }
+}
+
+template <bool kW>
+__global__ void k_uf_edges_ranges(GraphView g, uint32_t *p, const uint32_t *bpre,
+                                  const uint32_t *bbase, uint32_t nr, uint32_t *err) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  const uint32_t total = bpre[nr];
+  for (uint32_t i = group; i < total; i += ngroups) {
+    const uint32_t b = range_at(bpre, nr, i, bbase);
+    const uint32_t u = g.bowner[b];
+    if (g.deg[u] == 0) continue;
+    walk_bucket(g, L, b, [&](const uint4 &q) {
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+      for (int j = 0; j < keys_per_lane<kW>(); ++j)
+        if (k[j] < kTombKey && k[j] != u) uf_union(p, u, k[j], err);
+    });
+  }
+}
+
+__global__ void k_uf_compress_ranges(uint32_t *p, const uint32_t *vpre, const uint32_t *vbase,
+                                     uint32_t nr) {
+  const uint32_t total = vpre[nr];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const uint32_t v = range_at(vpre, nr, i, vbase);
+    p[v] = uf_root(p, v);
+  }
+}
+
 }  // namespace mk
 
 using namespace mk;
@@ -137,6 +193,7 @@ struct mk_wcc {
   uint32_t *aff_labels = nullptr;
   uint32_t *aff_vertices = nullptr;
   uint32_t *err = nullptr;
+  DevBuf<uint32_t> ranges;  // vpre, vbase, bpre, bbase of the last range call
   Timer timer;
 };
 
@@ -219,6 +276,49 @@ mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stre
   return w->timer.stop(ms_out);
 }
 
+mk_status mk_wcc_static_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges, uint32_t nranges,
+                               void *stream, float *ms_out) {
+  if (!w || (nranges && !h_vertex_ranges))
+    return fail(MK_ERR_INVALID, "mk_wcc_static_ranges: null argument");
+  mk_graph *g = w->g;
+  std::vector<uint32_t> host(4 * ((size_t)nranges + 1));
+  uint32_t *vpre = host.data(), *vbase = vpre + nranges + 1;
+  uint32_t *bpre = vbase + nranges + 1, *bbase = bpre + nranges + 1;
+  uint64_t vt = 0, bt = 0;
+  for (uint32_t r = 0; r < nranges; ++r) {
+    const uint32_t b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
+    if (b >= e || e > g->V) return fail(MK_ERR_INVALID, "mk_wcc_static_ranges: bad vertex range");
+    vpre[r] = (uint32_t)vt;
+    vbase[r] = b;
+    bpre[r] = (uint32_t)bt;
+    bbase[r] = g->h_boff[b];
+    vt += e - b;
+    bt += g->h_boff[e] - g->h_boff[b];
+  }
+  vpre[nranges] = (uint32_t)vt;
+  bpre[nranges] = (uint32_t)bt;
+  vbase[nranges] = bbase[nranges] = 0;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(w->timer.start(s, ms_out != nullptr));
+  if (nranges == 0) return w->timer.stop(ms_out);
+  MK_CHECK(w->ranges.reserve(host.size(), &g->device_bytes));
+  MK_CUDA(cudaMemcpyAsync(w->ranges.ptr, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s));
+  // the host copy must outlive the asynchronous transfer
+  MK_CUDA(cudaStreamSynchronize(s));
+  const uint32_t *dv = w->ranges.ptr, *dvb = dv + nranges + 1;
+  const uint32_t *db = dvb + nranges + 1, *dbb = db + nranges + 1;
+  k_uf_init_ranges<<<flat_grid(vt, g->device), 256, 0, s>>>(w->parent, dv, dvb, nranges);
+  const int blocks = (int)std::min<uint64_t>(bt * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  if (g->weighted)
+    k_uf_edges_ranges<true><<<blocks, 256, 0, s>>>(g->view(), w->parent, db, dbb, nranges, w->err);
+  else
+    k_uf_edges_ranges<false><<<blocks, 256, 0, s>>>(g->view(), w->parent, db, dbb, nranges, w->err);
+  k_uf_compress_ranges<<<flat_grid(vt, g->device), 256, 0, s>>>(w->parent, dv, dvb, nranges);
+  MK_CUDA(cudaGetLastError());
+  return w->timer.stop(ms_out);
+}
+
 mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d_dst,
                              uint32_t n, void *stream, float *ms_out) {
   if (!w) return fail(MK_ERR_INVALID, "mk_wcc_incremental: null handle");
@@ -282,6 +382,7 @@ mk_status mk_wcc_destroy(mk_wcc *w) {
   cudaFree(w->aff_labels);
   cudaFree(w->aff_vertices);
   cudaFree(w->err);
+  w->ranges.release();
   delete w;
   return MK_OK;
 }

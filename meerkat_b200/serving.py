@@ -12,10 +12,13 @@ queue -- are served by coalesced launches:
   WCC queries                           one subset union-find pass
 
 PageRank pulls over in-edges and triangle counting needs the symmetric
-graph, so those requests run on per-graph views (a reverse graph, a
-symmetric graph) built on first use from a CSR export of the member and kept
-current by replaying every later update of that graph on them.  Views are
-admitted under a device-memory budget and evicted least-recently-used.
+graph, so those requests run on per-graph views (a reverse graph for
+PageRank, a symmetric graph for TC) built on first use from a CSR export of
+the member and kept current by replaying every later update of that graph on
+them.  Views are admitted under a device-memory budget and evicted
+least-recently-used.  These heavy requests run one per round after the
+coalesced fast work, so a triangle count does not hold up the updates and
+traversals of other graphs.
 
 Each graph's requests are served in arrival order, so every request sees
 exactly the updates of its graph that arrived before it, whether it shares
@@ -52,6 +55,7 @@ class Request:
     lo: int = 0             # payload slice [lo, hi) of the update pool
     hi: int = 0
     done: float = -1.0      # completion time (seconds after the start)
+    service: float = 0.0    # seconds of the round that served it
     result: object = None   # query answer when results are recorded
 
 
@@ -76,7 +80,7 @@ def make_graph_sizes(num_graphs: int, scale_lo: int, scale_hi: int, edge_factor:
 
 
 def build_set(nv, ne, seed: int, device: int = 0, w_lo: int = 1, w_hi: int = 1000,
-              pool_fraction: float = 0.125):
+              pool_fraction: float = 0.0625):
     """The resident graph set (R-MAT members generated on the device) and the
     generated edges (kept for sampling delete payloads)."""
     import torch
@@ -89,7 +93,10 @@ def build_set(nv, ne, seed: int, device: int = 0, w_lo: int = 1, w_hi: int = 100
     gs = GraphSet(nv, degree_hints=[hints[voff[m]:voff[m + 1]] for m in range(len(nv))],
                   weighted=True, device=device,
                   pool_slabs=int(buckets_est * pool_fraction) + (1 << 23))
-    gs.graph.InsertEdges(src, dst, vals=w)
+    # load in slices so the per-batch scratch stays small
+    step = 1 << 27
+    for a in range(0, src.numel(), step):
+        gs.graph.InsertEdges(src[a:a + step], dst[a:a + step], vals=w[a:a + step])
     if gs.graph.sync() != 0:
         raise RuntimeError("device error while loading the graph set")
     return gs, (src, dst, w)
@@ -162,38 +169,63 @@ def make_requests(wl: Workload, edges, n: int, rate: float, seed: int, device: i
     return wl.requests[base:]
 
 
-class _View:
-    """Reverse and symmetric copies of one member, for PageRank and TC."""
+HEAVY_KINDS = (PAGERANK_Q, TC_Q)
 
-    def __init__(self, gs: GraphSet, g: int, device: int):
+
+class _View:
+    """A copy of one member for the queries the union graph cannot answer:
+    kind "rev" (in-edges, PageRank) or "sym" (both directions, triangles)."""
+
+    def __init__(self, gs: GraphSet, g: int, kind: str, device: int):
         import torch
         lo, hi = int(gs.offsets[g]), int(gs.offsets[g + 1])
         n = hi - lo
-        self.n = n
+        self.n, self.kind = n, kind
         rp, col, _ = gs.graph.export_csr_range_device(lo, hi)
         rows = torch.repeat_interleave(torch.arange(n, device=col.device, dtype=torch.int32),
                                        (rp[1:] - rp[:-1]))
         cols = col - lo
-        indeg = torch.bincount(cols.long(), minlength=n).to(torch.int32).cpu().numpy().view(np.uint32)
-        outdeg = (rp[1:] - rp[:-1]).to(torch.int32).cpu().numpy().view(np.uint32)
         e = int(cols.numel())
-        self.rev = DynamicGraph(n, degree_hints=indeg, reverse=True, device=device,
-                                pool_slabs=max(4096, (n + e // 20) // 4))
-        self.rev.InsertEdges(rows, cols)
-        self.sym = DynamicGraph(n, degree_hints=indeg + outdeg, device=device,
-                                pool_slabs=max(4096, (n + e // 10) // 4))
-        self.sym.InsertEdges(torch.cat([rows, cols]), torch.cat([cols, rows]))
-        if self.rev.sync() != 0 or self.sym.sync() != 0:
+        indeg = torch.bincount(cols.long(), minlength=n).to(torch.int32).cpu().numpy().view(np.uint32)
+        if kind == "rev":
+            self.graph = DynamicGraph(n, degree_hints=indeg, reverse=True, device=device,
+                                      pool_slabs=max(4096, (n + e // 20) // 4))
+            self.graph.InsertEdges(rows, cols)
+        else:
+            outdeg = (rp[1:] - rp[:-1]).to(torch.int32).cpu().numpy().view(np.uint32)
+            self.graph = DynamicGraph(n, degree_hints=indeg + outdeg, device=device,
+                                      pool_slabs=max(4096, (n + e // 10) // 4))
+            self.graph.InsertEdges(torch.cat([rows, cols]), torch.cat([cols, rows]))
+        del rp, col, rows, cols
+        if self.graph.sync() != 0:
             raise RuntimeError("device error while building a view")
-        self.pr = PageRank(self.rev, 0.85, 1e-6, n, max_iter=200)
-        self.tc = TC(self.sym, n)
-        # graphs, PageRank vectors, TC's oriented copy of the symmetric edges
-        self.bytes = (self.rev.info()["device_bytes"] + self.sym.info()["device_bytes"] + 28 * n
-                      + 8 * e)
+        if kind == "rev":
+            self.algo = PageRank(self.graph, 0.85, 1e-6, n, max_iter=200)
+            extra = 28 * n  # rank, contribution and degree vectors, work items
+        else:
+            self.algo = TC(self.graph, n)
+            extra = 8 * n + 4 * e  # oriented copy of the symmetric edges
+        self.bytes = self.graph.info()["device_bytes"] + extra
+
+    def apply(self, kind: int, u, w_, reverse_found=None):
+        """Replays one update of the member (local ids) on the view."""
+        import torch
+        if self.kind == "rev":
+            if kind == INSERT:
+                self.graph.InsertEdges(u, w_)
+            else:
+                self.graph.DeleteEdges(u, w_)
+        elif kind == INSERT:
+            self.graph.InsertEdges(torch.cat([u, w_]), torch.cat([w_, u]))
+        else:
+            # the undirected edge goes only when neither direction is left
+            keep = reverse_found == 0
+            uu, ww = u[keep], w_[keep]
+            self.graph.DeleteEdges(torch.cat([uu, ww]), torch.cat([ww, uu]))
 
     def close(self):
-        for o in (self.pr, self.tc, self.rev, self.sym):
-            o.close()
+        self.algo.close()
+        self.graph.close()
 
 
 class GraphServer:
@@ -210,7 +242,7 @@ class GraphServer:
         self.bfs = BFS(self.G, first)
         self.sssp = SSSP(self.G, first)
         self.wcc = WCC(self.G)
-        self.views: "collections.OrderedDict[int, _View]" = collections.OrderedDict()
+        self.views: "collections.OrderedDict[tuple, _View]" = collections.OrderedDict()
         V = gs.num_vertices
         info = self.G.info()
         # graph + two traversals (dist, stamp, bitmap, two frontiers, list) + WCC
@@ -224,21 +256,24 @@ class GraphServer:
     def view_bytes(self) -> int:
         return sum(v.bytes for v in self.views.values())
 
-    def _view(self, g: int) -> _View:
-        v = self.views.get(g)
+    def _view(self, g: int, kind: str) -> _View:
+        key = (g, kind)
+        v = self.views.get(key)
         if v is not None:
-            self.views.move_to_end(g)
+            self.views.move_to_end(key)
             return v
-        n = int(self.off[g + 1] - self.off[g])
-        est = 3 * 128 * (n + int(self.G.count_edges(int(self.off[g]), int(self.off[g + 1]))) // 10)
+        lo, hi = int(self.off[g]), int(self.off[g + 1])
+        n, e = hi - lo, int(self.G.count_edges(lo, hi))
+        mult = 1 if kind == "rev" else 2
+        est = 128 * (n + mult * e // 15) + 32 * n + 4 * e
         while self.views and self.resident + self.view_bytes() + est > self.budget:
             _, old = self.views.popitem(last=False)
             old.close()
             self.view_evictions += 1
         if self.resident + est > self.budget:
-            raise MemoryError(f"graph {g}: a view does not fit the budget")
-        v = _View(self.gs, g, self.device)
-        self.views[g] = v
+            raise MemoryError(f"graph {g}: a {kind} view does not fit the budget")
+        v = _View(self.gs, g, kind, self.device)
+        self.views[key] = v
         self.view_builds += 1
         # the estimate was short: evict older views until the real size fits
         while len(self.views) > 1 and self.resident + self.view_bytes() > self.budget:
@@ -247,10 +282,11 @@ class GraphServer:
             self.view_evictions += 1
         return v
 
-    # ---- one scheduling round: at most one request per graph ----
-    def serve_round(self, reqs: List[Request], wl: Workload) -> None:
+    # ---- a coalesced round of fast requests: at most one per graph ----
+    def serve_fast(self, reqs: List[Request], wl: Workload) -> None:
         import torch
         assert len({r.graph for r in reqs}) == len(reqs), "one request per graph per round"
+        assert all(r.kind not in HEAVY_KINDS for r in reqs)
         dels = [r for r in reqs if r.kind == DELETE]
         inss = [r for r in reqs if r.kind == INSERT]
         P_s, P_d, P_w = wl.pool_src, wl.pool_dst, wl.pool_w
@@ -265,23 +301,17 @@ class GraphServer:
             self.G.InsertEdges(is_, id_, vals=iw)
         # keep cached views current (per graph: the same batch, local ids)
         for r in dels + inss:
-            v = self.views.get(r.graph)
-            if v is None:
+            views = [v for k, v in self.views.items() if k[0] == r.graph]
+            if not views:
                 continue
             base = int(self.off[r.graph])
             u, w_ = P_s[r.lo:r.hi] - base, P_d[r.lo:r.hi] - base
-            if r.kind == INSERT:
-                v.rev.InsertEdges(u, w_)
-                v.sym.InsertEdges(torch.cat([u, w_]), torch.cat([w_, u]))
-            else:
-                v.rev.DeleteEdges(u, w_)
-                # the undirected edge goes only when neither direction is left
+            found = None
+            if r.kind == DELETE and any(v.kind == "sym" for v in views):
                 found = torch.zeros(u.numel(), dtype=torch.uint8, device=u.device)
                 self.G.SearchEdges(P_d[r.lo:r.hi], P_s[r.lo:r.hi], found)
-                keep = found == 0
-                uu, ww = u[keep], w_[keep]
-                v.sym.DeleteEdges(torch.cat([uu, ww]), torch.cat([ww, uu]))
-        # queries
+            for v in views:
+                v.apply(r.kind, u, w_, found)
         bfs = [r for r in reqs if r.kind == BFS_Q]
         sssp = [r for r in reqs if r.kind == SSSP_Q]
         wccs = [r for r in reqs if r.kind == WCC_Q]
@@ -290,19 +320,8 @@ class GraphServer:
                 trav.set_sources([int(self.off[r.graph]) + r.source for r in rs])
                 trav.Static(timed=False)
         if wccs:
-            flags = np.zeros(self.gs.num_graphs, dtype=np.uint8)
-            flags[[r.graph for r in wccs]] = 1
-            self.wcc.StaticSubset(self.gs.select_bits(flags), timed=False)
-        for r in reqs:
-            if r.kind == PAGERANK_Q:
-                v = self._view(r.graph)
-                v.pr.StaticRecount(timed=False)
-                if self.record:
-                    r.result = v.pr.Values()
-            elif r.kind == TC_Q:
-                v = self._view(r.graph)
-                v.tc.Static(timed=False)
-                r.result = v.tc.GetCount()
+            self.wcc.StaticRanges([(int(self.off[r.graph]), int(self.off[r.graph + 1]))
+                                   for r in wccs], timed=False)
         if self.record:
             self._record(bfs, self.bfs)
             self._record(sssp, self.sssp)
@@ -311,6 +330,27 @@ class GraphServer:
                 for r in wccs:
                     lo, hi = int(self.off[r.graph]), int(self.off[r.graph + 1])
                     r.result = (lab[lo:hi] - lo).astype(np.uint32)
+
+    # ---- one PageRank or triangle-count request on its graph's view ----
+    def serve_heavy(self, r: Request) -> None:
+        if r.kind == PAGERANK_Q:
+            v = self._view(r.graph, "rev")
+            v.algo.StaticRecount(timed=False)
+            if self.record:
+                r.result = v.algo.Values()
+        else:
+            v = self._view(r.graph, "sym")
+            v.algo.Static(timed=False)
+            r.result = v.algo.GetCount()
+
+    def serve_round(self, reqs: List[Request], wl: Workload) -> None:
+        """Fast requests as one coalesced round, then the heavy ones in order."""
+        fast = [r for r in reqs if r.kind not in HEAVY_KINDS]
+        if fast:
+            self.serve_fast(fast, wl)
+        for r in reqs:
+            if r.kind in HEAVY_KINDS:
+                self.serve_heavy(r)
 
     def _record(self, rs, trav):
         if not rs:
@@ -328,10 +368,12 @@ class GraphServer:
     def run(self, reqs: List[Request], wl: Workload, mode: str = "coalesced",
             max_round: int = 0) -> dict:
         """Serves `reqs` (sorted by arrival) against the wall clock: a request
-        is admitted once its arrival time has passed; each round takes the
-        head request of every graph with a pending one ("coalesced", at most
-        max_round of them if > 0) or the single oldest request ("alone"), runs
-        it and waits for the GPU.  Returns latency and throughput figures."""
+        is admitted once its arrival time has passed.  "coalesced": each round
+        takes the head request of every graph with a pending one, runs the fast
+        heads (at most max_round if > 0) as one coalesced segment and then the
+        oldest heavy head (PageRank / TC) as a second segment.  "alone": each
+        round runs the single oldest request.  A request completes when the
+        GPU has finished its segment.  Returns latency and throughput."""
         import torch
         assert mode in ("coalesced", "alone")
         queues: Dict[int, collections.deque] = collections.defaultdict(collections.deque)
@@ -350,35 +392,49 @@ class GraphServer:
                 if wait > 0.0005:
                     time.sleep(wait - 0.0003)
                 continue
+            segments = []  # (kind of segment, requests)
             if mode == "alone":
                 r = fifo.popleft()
                 queues[r.graph].popleft()
-                batch = [r]
+                segments.append(("heavy" if r.kind in HEAVY_KINDS else "fast", [r]))
             else:
                 heads = sorted((q[0] for q in queues.values() if q), key=lambda r: r.arrival)
+                fast = [r for r in heads if r.kind not in HEAVY_KINDS]
+                heavy = [r for r in heads if r.kind in HEAVY_KINDS]
                 if max_round > 0:
-                    heads = heads[:max_round]
-                batch = []
-                for r in heads:
-                    queues[r.graph].popleft()
-                    batch.append(r)
-            self.serve_round(batch, wl)
-            torch.cuda.synchronize(self.device)
-            done = time.perf_counter() - t0
-            for r in batch:
-                r.done = done
-            served += len(batch)
-            rounds += 1
+                    fast = fast[:max_round]
+                if fast:
+                    segments.append(("fast", fast))
+                if heavy:  # one heavy request per round, oldest first
+                    segments.append(("heavy", heavy[:1]))
+                for _, rs in segments:
+                    for r in rs:
+                        queues[r.graph].popleft()
+            for kind, rs in segments:
+                start = time.perf_counter() - t0
+                if kind == "fast":
+                    self.serve_fast(rs, wl)
+                else:
+                    self.serve_heavy(rs[0])
+                torch.cuda.synchronize(self.device)
+                done = time.perf_counter() - t0
+                for r in rs:
+                    r.done = done
+                    r.service = done - start
+                served += len(rs)
+                rounds += 1
         self.check()
         lat = np.array([r.done - r.arrival for r in reqs]) * 1000.0
         span = max(r.done for r in reqs) - min(r.arrival for r in reqs) if reqs else 0.0
         by_kind = {}
         for k in range(len(KIND_NAMES)):
             sel = [r.done - r.arrival for r in reqs if r.kind == k]
+            svc = [r.service for r in reqs if r.kind == k]
             if sel:
                 by_kind[KIND_NAMES[k]] = {"n": len(sel),
                                           "p50_ms": float(np.percentile(sel, 50) * 1000.0),
-                                          "p99_ms": float(np.percentile(sel, 99) * 1000.0)}
+                                          "p99_ms": float(np.percentile(sel, 99) * 1000.0),
+                                          "service_p50_ms": float(np.percentile(svc, 50) * 1000.0)}
         return {"mode": mode, "requests": n, "rounds": rounds,
                 "p50_ms": float(np.percentile(lat, 50)) if n else 0.0,
                 "p99_ms": float(np.percentile(lat, 99)) if n else 0.0,

@@ -195,3 +195,28 @@ def test_multi_source_rejects_bad_sources():
         mk.BFS(S.graph, [1, 1])
     with pytest.raises(mk.MeerkatError):
         mk.SSSP(S.graph, [3, 20])
+
+
+def test_wcc_ranges_touch_only_their_members():
+    mem = members(n=8, seed=60)
+    S, oracles = build_set(mem)
+    off = S.offsets.astype(np.int64)
+    wcc = mk.WCC(S.graph)
+    wcc.Static()
+    before = wcc.Labels()
+    # delete a third of member 1's and member 5's edges, recompute only those
+    for m in (1, 5):
+        V, s, d, _ = mem[m]
+        es = mk.EdgeSet(V, s, d)
+        ds, dd = es.sample_present(len(s) // 3, seed=7 + m)
+        S.graph.DeleteEdges(to_dev(ds + off[m]), to_dev(dd + off[m]))
+        oracles[m].delete(ds, dd)
+    assert S.graph.sync() == 0
+    wcc.StaticRanges([(off[1], off[2]), (off[5], off[6])])
+    lab = wcc.Labels()
+    for m, O in enumerate(oracles):
+        lo, hi = off[m], off[m + 1]
+        if m in (1, 5):
+            np.testing.assert_array_equal(lab[lo:hi].astype(np.int64) - lo, O.wcc())
+        else:
+            np.testing.assert_array_equal(lab[lo:hi], before[lo:hi])
