@@ -374,6 +374,24 @@ mk_status mk_gen_set_batches(const uint32_t *d_vertex_offsets, uint32_t num_grap
                              uint32_t *d_ins_dst, uint32_t *d_ins_w, void *stream);
 
 /* ------------------------------------------------------------------------
+ * The reference drivers' text formats (host only; no GPU needed):
+ *   graph file "V E" then E pairs "u v"                 (src/BFS.cu:27-36)
+ *   batch file "<prefix>.batch.<i>": "n" then n pairs  (src/BFS.cu:76-91)
+ * Whitespace-separated unsigned decimals.  Pass NULL arrays first to read
+ * only the header; a short file, a malformed token or (graph files) an id
+ * >= V is MK_ERR_INVALID with the line in mk_last_error_string().
+ * ---------------------------------------------------------------------- */
+mk_status mk_read_edge_list(const char *path, uint32_t *h_num_vertices,
+                            uint64_t *h_num_edges, uint32_t *h_src, uint32_t *h_dst);
+mk_status mk_read_batch_file(const char *path, uint64_t *h_num_edges,
+                             uint32_t *h_src, uint32_t *h_dst);
+mk_status mk_write_edge_list(const char *path, uint32_t num_vertices,
+                             uint64_t num_edges, const uint32_t *h_src,
+                             const uint32_t *h_dst);
+mk_status mk_write_batch_file(const char *path, uint64_t num_edges,
+                              const uint32_t *h_src, const uint32_t *h_dst);
+
+/* ------------------------------------------------------------------------
  * Synthetic inputs (host only; no GPU needed).  Seeded and deterministic.
  * ---------------------------------------------------------------------- */
 /* R-MAT: exactly num_edges distinct directed edges without self-loops over

@@ -301,6 +301,35 @@ class WCC {
   mk_wcc *w_ = nullptr;
 };
 
+// The reference drivers' input files (src/BFS.cu:27-36, :76-91): a graph
+// file "V E" + E pairs, and update batches "<prefix>.batch.<i>".
+struct EdgeList {
+  uint32_t num_vertices = 0;
+  std::vector<uint32_t> src, dst;
+};
+
+inline EdgeList ReadGraphFile(const std::string &path) {
+  EdgeList e;
+  uint64_t n = 0;
+  check(mk_read_edge_list(path.c_str(), &e.num_vertices, &n, nullptr, nullptr), "ReadGraphFile");
+  e.src.resize(n);
+  e.dst.resize(n);
+  check(mk_read_edge_list(path.c_str(), &e.num_vertices, &n, e.src.data(), e.dst.data()),
+        "ReadGraphFile");
+  return e;
+}
+
+inline EdgeList ReadBatchFile(const std::string &prefix, uint32_t index) {
+  const std::string path = prefix + ".batch." + std::to_string(index);
+  EdgeList e;
+  uint64_t n = 0;
+  check(mk_read_batch_file(path.c_str(), &n, nullptr, nullptr), "ReadBatchFile");
+  e.src.resize(n);
+  e.dst.resize(n);
+  check(mk_read_batch_file(path.c_str(), &n, e.src.data(), e.dst.data()), "ReadBatchFile");
+  return e;
+}
+
 }  // namespace meerkat
 
 #ifndef MEERKAT_COMPAT_NO_GLOBAL_NAMES

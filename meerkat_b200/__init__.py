@@ -19,7 +19,8 @@ import numpy as np
 from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
 __all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "TC", "WCC", "EdgeSet",
-           "gen_rmat", "gen_grid", "gen_rmat_members", "MeerkatError", "MK_INF", "lib", "version"]
+           "gen_rmat", "gen_grid", "gen_rmat_members", "read_edge_list", "read_batch",
+           "write_edge_list", "write_batch", "MeerkatError", "MK_INF", "lib", "version"]
 
 
 def version() -> str:
@@ -618,6 +619,47 @@ def gen_rmat_members(vertex_offsets, edges_per_graph, a=0.57, b=0.19, c=0.19, se
         torch.cuda.synchronize(dev)
         del keep
     return src[:E], dst[:E], (w[:E] if w is not None else None)
+
+
+# ---------------------------------------------------------------------------
+# the reference drivers' text formats (host only)
+# ---------------------------------------------------------------------------
+def read_edge_list(path):
+    """Graph file "V E" + E pairs (src/BFS.cu:27-36) -> (V, src, dst)."""
+    p = str(path).encode()
+    V, E = C.c_uint32(0), C.c_uint64(0)
+    check(lib().mk_read_edge_list(p, C.byref(V), C.byref(E), None, None), "mk_read_edge_list")
+    src = np.empty(E.value, dtype=np.uint32)
+    dst = np.empty(E.value, dtype=np.uint32)
+    check(lib().mk_read_edge_list(p, C.byref(V), C.byref(E), src.ctypes.data, dst.ctypes.data),
+          "mk_read_edge_list")
+    return V.value, src, dst
+
+
+def read_batch(path):
+    """Batch file "n" + n pairs (src/BFS.cu:76-91) -> (src, dst)."""
+    p = str(path).encode()
+    n = C.c_uint64(0)
+    check(lib().mk_read_batch_file(p, C.byref(n), None, None), "mk_read_batch_file")
+    src = np.empty(n.value, dtype=np.uint32)
+    dst = np.empty(n.value, dtype=np.uint32)
+    check(lib().mk_read_batch_file(p, C.byref(n), src.ctypes.data, dst.ctypes.data),
+          "mk_read_batch_file")
+    return src, dst
+
+
+def write_edge_list(path, num_vertices: int, src, dst) -> None:
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    check(lib().mk_write_edge_list(str(path).encode(), int(num_vertices), len(s), s.ctypes.data,
+                                   d.ctypes.data), "mk_write_edge_list")
+
+
+def write_batch(path, src, dst) -> None:
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    check(lib().mk_write_batch_file(str(path).encode(), len(s), s.ctypes.data, d.ctypes.data),
+          "mk_write_batch_file")
 
 
 # ---------------------------------------------------------------------------

@@ -13,12 +13,13 @@ from oracle import OracleGraph
 
 ROOT = Path(__file__).resolve().parent.parent
 SRC = ROOT / "tests" / "cpp" / "drop_in_driver.cpp"
+FILE_DRIVER = ROOT / "tests" / "cpp" / "bfs_file_driver.cpp"
 
 
-def build_driver(tmp_path) -> Path:
-    exe = tmp_path / "drop_in_driver"
+def build_driver(tmp_path, src=SRC) -> Path:
+    exe = tmp_path / src.stem
     cmd = ["/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++", "-std=c++17", "-O2",
-           f"-I{ROOT / 'include'}", "-I/usr/local/cuda/include", str(SRC), "-o", str(exe),
+           f"-I{ROOT / 'include'}", "-I/usr/local/cuda/include", str(src), "-o", str(exe),
            f"-L{LIB_PATH.parent}", "-lmeerkat_b200", f"-Wl,-rpath,{LIB_PATH.parent}",
            "-L/usr/local/cuda/lib64", "-lcudart", "-Wl,-rpath,/usr/local/cuda/lib64"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -29,6 +30,36 @@ def build_driver(tmp_path) -> Path:
 def test_shim_compiles_and_links(tmp_path):
     exe = build_driver(tmp_path)
     assert exe.exists()
+    assert build_driver(tmp_path, FILE_DRIVER).exists()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("op", ["0", "1"])
+def test_reference_file_workflow_matches_oracle(tmp_path, op):
+    """The reference's BFS driver workflow: graph file + <prefix>.batch.<i>
+    files in its text formats, update then Incremental/Decremental."""
+    exe = build_driver(tmp_path, FILE_DRIVER)
+    V = 1 << 11
+    s, d, _ = mk.gen_rmat(11, 12000, seed=9)
+    mk.write_edge_list(tmp_path / "g.txt", V, s, d)
+    es = mk.EdgeSet(V, s, d)
+    O = OracleGraph(V)
+    O.insert(s, d)
+    for i in range(3):
+        if op == "0":
+            bs, bd = es.sample_absent(700, seed=20 + i)
+            O.insert(bs, bd)
+        else:
+            bs, bd = es.sample_present(700, seed=20 + i)
+            O.delete(bs, bd)
+        mk.write_batch(tmp_path / f"upd.batch.{i}", bs, bd)
+    r = subprocess.run([str(exe), str(tmp_path / "g.txt"), op, str(tmp_path / "upd"), "3"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert lines[0].startswith(str(tmp_path / "g.txt")) and lines[0].count(",") == 4
+    got = np.array(list(map(int, lines[1:])), dtype=np.uint32)
+    np.testing.assert_array_equal(got, O.bfs(0))
 
 
 @pytest.mark.gpu
