@@ -568,7 +568,7 @@ def main():
     ap.add_argument("--scale", type=int, default=22,
                     help="R-MAT scale (22 = the benchmark config; smaller only for profiling)")
     ap.add_argument("--batch", type=int, default=500_000, help="edges per sub-batch")
-    ap.add_argument("--update-kernel", default="auto", choices=["auto", "0", "1"],
+    ap.add_argument("--update-kernel", default="auto", choices=["auto", "0", "1", "2"],
                     help="auto = autotune on the first batches; 0/1 pins a variant")
     ap.add_argument("--workload", default="updates", choices=["updates", "batched", "serving"],
                     help="updates = the headline mixed-batch benchmark; batched = many small "
@@ -619,7 +619,7 @@ def main():
     dev = torch.device(f"cuda:{local}")
     W, K, A = args.warmup, args.steps, args.algo_batches
     from meerkat_b200.autotune import VARIANTS, tune_updates
-    T = len(VARIANTS)
+    T = 2 * len(VARIANTS)  # two tuning rounds
     graph, batches = make_workload(T + W + 2 * K + A + 2)
     s, d, w = graph
     V = 1 << SCALE
@@ -638,9 +638,9 @@ def main():
 
     stream = torch.cuda.current_stream(dev)
     # autotune the update kernel on the first T batches (they are real updates)
-    variants = VARIANTS if args.update_kernel == "auto" else [(int(args.update_kernel), 0)] * T
+    variants = VARIANTS if args.update_kernel == "auto" else [(int(args.update_kernel), 0)] * 4
     tuning = tune_updates(G, [tuple(todev(x) for x in b) for b in batches[:T]], variants=variants,
-                          stream=stream)
+                          stream=stream, rounds=2)
     log(f"[bench] tuning: {tuning}")
     batches = batches[T:]
     dbatches = [tuple(todev(x) for x in b) for b in batches[:W + K]]

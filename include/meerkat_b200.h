@@ -170,7 +170,8 @@ mk_status mk_graph_reserve_batch(mk_graph *g, uint32_t n);
  * meerkat_b200/autotune.py measures the variants on live batches. */
 typedef struct mk_tuning {
   uint32_t update_kernel;        /* 0 = warp-staged (TMA bulk copies into shared
-                                    memory), 1 = one lane per edge             */
+                                    memory), 1 = one lane per edge,
+                                    2 = warp-cooperative coalesced slab loads  */
   uint32_t update_blocks_per_sm; /* resident blocks per SM, 0 = automatic     */
   uint32_t frontier_chunk;       /* buckets per BFS/SSSP frontier work item,
                                     1..1024, 0 = 4                            */

@@ -231,6 +231,7 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
 // A staged slab that went stale only costs step 4: inside one insert call key
 // words only move EMPTY -> key, inside one delete call only key -> TOMBSTONE.
 constexpr int kUpdWarps = 4;  // warps per block
+constexpr int kCoopBlock = 256;  // threads per block of the warp-cooperative kernel
 constexpr size_t kStageStride = 9;  // uint4 per staged slab: 128 B + 16 B pad
 constexpr size_t kUpdSmem = (size_t)kUpdWarps * 2 * 32 * kStageStride * 16;  // 2 stages x 32 slabs per warp
 
@@ -372,6 +373,130 @@ __device__ uint32_t lane_delete_chain(const GraphView &g, uint32_t s, uint4 (&q)
   return 0;
 }
 
+// Batch record of one edge, loaded ahead of use.
+struct UpdRaw {
+  uint32_t u, v, wt;
+  uint32_t present;  // e < n
+};
+// Bucket offsets of a record's source, loaded ahead of use.
+struct UpdOff {
+  uint32_t b0, b1;
+  uint32_t ok;  // in range and not a self-loop
+};
+
+template <bool kWeighted, bool kInsert>
+__device__ __forceinline__ UpdRaw upd_load(const uint32_t *__restrict__ src,
+                                           const uint32_t *__restrict__ dst,
+                                           const uint32_t *__restrict__ w, uint32_t n, uint64_t e,
+                                           unsigned long long stream_pol) {
+  UpdRaw r{0u, 0u, 0u, 0u};
+  if (e < n) {
+    r.u = ld_stream_u32(src + e, stream_pol);
+    r.v = ld_stream_u32(dst + e, stream_pol);
+    if (kWeighted && kInsert && w) r.wt = ld_stream_u32(w + e, stream_pol);
+    r.present = 1u;
+  }
+  return r;
+}
+
+__device__ __forceinline__ UpdOff upd_offsets(const GraphView &g, UpdRaw &r,
+                                              unsigned long long keep_pol) {
+  UpdOff o{0u, 0u, 0u};
+  if (!r.present) return o;
+  if (g.reverse) {
+    const uint32_t t = r.u;
+    r.u = r.v;
+    r.v = t;
+  }
+  if (r.u >= g.V || r.v >= g.V) {
+    atomicOr(g.err, kErrInvalidId);
+    return o;
+  }
+  if (r.u == r.v) return o;
+  o.b0 = ld_hint_u32(g.boff + r.u, keep_pol);
+  o.b1 = ld_hint_u32(g.boff + r.u + 1, keep_pol);
+  o.ok = 1u;
+  return o;
+}
+
+// A lane's decision for its edge, committed one iteration later.
+struct UpdPending {
+  uint32_t head, u, v, wt;
+  uint32_t word;  // slot word the CAS targets
+  uint32_t old;   // value the CAS returned
+  uint32_t kind;  // 0 done (not applied), 1 CAS issued, 2 walk the chain
+};
+
+// Decides from the staged head slab and issues the one CAS of the fast path
+// without waiting for its result.
+template <bool kWeighted, bool kInsert>
+__device__ __forceinline__ UpdPending upd_decide_probe(const GraphView &g, const LaneProbe &pr,
+                                                       uint32_t head, const UpdRaw &r) {
+  UpdPending p{head, r.u, r.v, r.wt, 0u, 0u, 0u};
+  uint32_t *slab = reinterpret_cast<uint32_t *>(g.slabs + 8ull * head);
+  if (kInsert) {
+    if (pr.found_word < 32) {
+      if (kWeighted) atomicMin(slab + pr.found_word + 1, r.wt);  // live edge: upsert-min
+    } else if (pr.empty_word < 32) {
+      p.word = pr.empty_word;
+      p.old = atomicCAS(slab + pr.empty_word, kEmptyKey, r.v);
+      p.kind = 1;
+    } else {
+      p.kind = 2;
+    }
+  } else {
+    if (pr.found_word < 32) {
+      p.word = pr.found_word;
+      p.old = atomicCAS(slab + pr.found_word, r.v, kTombKey);
+      p.kind = 1;
+    } else if (pr.next != kNoSlab) {
+      p.kind = 2;
+    }
+  }
+  return p;
+}
+
+template <bool kWeighted, bool kInsert>
+__device__ __forceinline__ UpdPending upd_decide(const GraphView &g, const uint4 (&q)[8],
+                                                 uint32_t head, const UpdRaw &r) {
+  return upd_decide_probe<kWeighted, kInsert>(g, lane_probe<kWeighted>(q, r.v), head, r);
+}
+
+// Reads the CAS result (or walks the chain) and returns whether the edge
+// was applied.
+template <bool kWeighted, bool kInsert>
+__device__ __forceinline__ uint32_t upd_finish(const GraphView &g, const UpdPending &p) {
+  if (p.kind == 0) return 0u;
+  uint32_t *slab = reinterpret_cast<uint32_t *>(g.slabs + 8ull * p.head);
+  if (p.kind == 1) {
+    if (!kInsert) return p.old == p.v ? 1u : 0u;
+    if (p.old == kEmptyKey || p.old == p.v) {
+      // a never-used value word is EMPTY, so atomicMin keeps the minimum over
+      // every concurrent copy
+      if (kWeighted) atomicMin(slab + p.word + 1, p.wt);
+      return p.old == kEmptyKey ? 1u : 0u;
+    }
+  }
+  // lost the slot to another key, or the chain continues: walk it
+  uint4 q[8];
+  lane_load_slab(g, p.head, q);
+  return kInsert ? lane_insert_chain<kWeighted>(g, p.head, q, p.v, p.wt)
+                 : lane_delete_chain<kWeighted>(g, p.head, q, p.v);
+}
+
+// Warp-staged update kernel.  Each warp walks groups of 32 edges through a
+// software pipeline, one group per step per iteration:
+//   load    the batch records of group i+3 (streamed, evict-first);
+//   offsets the bucket offsets of group i+2's sources (evict-last: the
+//           per-vertex arrays stay in L2 under the slab traffic);
+//   stage   group i+1's head slabs: one 128-byte cp.async.bulk per lane into
+//           the warp's shared-memory stage, completing on its mbarrier;
+//   decide  group i: each lane decides from its staged slab and issues its
+//           one CAS without waiting for the result;
+//   finish  group i-1: the CAS results are read (weighted inserts then
+//           atomicMin the value word; a lost race walks the chain).
+// Every result a step consumes was requested one iteration earlier, so a
+// warp waits about one memory latency per group.
 template <bool kWeighted, bool kInsert>
 __global__ void __launch_bounds__(kUpdWarps * 32)
     k_update(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
@@ -381,8 +506,10 @@ __global__ void __launch_bounds__(kUpdWarps * 32)
   __shared__ __align__(8) uint64_t bars[kUpdWarps][2];
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t wib = threadIdx.x >> 5;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint64_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint64_t ngroups = ((uint64_t)n + 31) / 32;
+  if (warp >= ngroups) return;
   // [stage][lane] slabs of kStageStride uint4 (144 B: conflict-free lane reads)
   uint4 *wst = stage_smem + (size_t)wib * 2 * 32 * kStageStride;
   if (lane == 0) {
@@ -391,64 +518,169 @@ __global__ void __launch_bounds__(kUpdWarps * 32)
     mbar_init_fence();
   }
   __syncwarp();
-  const unsigned long long pol = l2_policy_evict_last();
+  const unsigned long long keep = l2_policy_evict_last();
+  const unsigned long long once = l2_policy_evict_first();
   uint32_t parity[2] = {0u, 0u};
   uint32_t mine = 0;
 
-  // stage the head slab of this lane's edge into stage st
-  auto issue = [&](const UpdEdge &E, uint32_t st) {
-    const uint32_t valid = __ballot_sync(0xFFFFFFFFu, E.head != kNoSlab);
+  auto edge_of = [&](uint64_t k) { return (warp + k * nwarps) * 32 + lane; };
+  auto group_ok = [&](uint64_t k) { return warp + k * nwarps < ngroups; };
+  // stage the head slab of this lane's edge (head == kNoSlab: nothing)
+  auto stage = [&](uint32_t head, uint32_t st) {
+    const uint32_t valid = __ballot_sync(0xFFFFFFFFu, head != kNoSlab);
     fence_proxy_async_smem();  // this warp's earlier reads of the buffer come first
     __syncwarp();
     if (lane == 0) mbar_arrive_expect_tx(&bars[wib][st], 128u * __popc(valid));
     __syncwarp();
-    if (E.head != kNoSlab)
-      bulk_load_hint(wst + ((size_t)st * 32 + lane) * kStageStride, g.slabs + 8ull * E.head, 128u,
-                     &bars[wib][st], pol);
+    if (head != kNoSlab)
+      bulk_load(wst + ((size_t)st * 32 + lane) * kStageStride, g.slabs + 8ull * head, 128u,
+                &bars[wib][st]);
+  };
+  auto head_of = [&](const UpdRaw &r, const UpdOff &o) {
+    return o.ok ? o.b0 + bucket_of(r.v, o.b1 - o.b0) : kNoSlab;
+  };
+  auto finish = [&](const UpdPending &p, uint64_t e) {
+    const uint32_t app = upd_finish<kWeighted, kInsert>(g, p);
+    if (app) {
+      red_add_hint_u32(g.deg + p.u, kInsert ? 1u : 0xFFFFFFFFu, keep);
+      ++mine;
+    }
+    if (e < n) applied[e] = (uint8_t)app;
   };
 
-  uint64_t base = (uint64_t)warp * 32;
-  if (base >= n) return;
-  UpdEdge cur = upd_resolve<kWeighted, kInsert>(g, src, dst, w, n, base + lane, applied);
+  // prologue: group 0 staged, group 1's offsets and group 2's records in flight
+  UpdRaw r0 = upd_load<kWeighted, kInsert>(src, dst, w, n, edge_of(0), once);
+  UpdRaw r1 = group_ok(1) ? upd_load<kWeighted, kInsert>(src, dst, w, n, edge_of(1), once)
+                          : UpdRaw{0u, 0u, 0u, 0u};
+  UpdRaw r2 = group_ok(2) ? upd_load<kWeighted, kInsert>(src, dst, w, n, edge_of(2), once)
+                          : UpdRaw{0u, 0u, 0u, 0u};
+  UpdOff o0 = upd_offsets(g, r0, keep);
+  UpdOff o1 = upd_offsets(g, r1, keep);
+  uint32_t head0 = head_of(r0, o0);
+  stage(head0, 0);
   uint32_t st = 0;
-  issue(cur, st);
-  for (;;) {
-    const uint64_t nbase = base + (uint64_t)nwarps * 32;
-    const bool has_next = nbase < n;
-    UpdEdge nxt{0u, 0u, 0u, kNoSlab};
-    if (has_next) {
-      nxt = upd_resolve<kWeighted, kInsert>(g, src, dst, w, n, nbase + lane, applied);
-      issue(nxt, st ^ 1u);
+  UpdPending prev{kNoSlab, 0u, 0u, 0u, 0u, 0u, 0u};
+  uint64_t prev_e = ~0ull;
+  for (uint64_t k = 0;; ++k) {
+    const bool has1 = group_ok(k + 1);
+    uint32_t head1 = kNoSlab;
+    if (has1) {
+      head1 = head_of(r1, o1);
+      stage(head1, st ^ 1u);
     }
+    UpdOff o2{0u, 0u, 0u};
+    if (group_ok(k + 2)) o2 = upd_offsets(g, r2, keep);
+    UpdRaw r3{0u, 0u, 0u, 0u};
+    if (group_ok(k + 3)) r3 = upd_load<kWeighted, kInsert>(src, dst, w, n, edge_of(k + 3), once);
+    if (k) finish(prev, prev_e);
+
+    // decide group k from its staged slab
     const bool ready = mbar_wait(&bars[wib][st], parity[st], g.err);
     parity[st] ^= 1u;
-    if (cur.head != kNoSlab) {
-      // the lane decides alone from its staged slab, then commits
+    UpdPending cur{kNoSlab, 0u, 0u, 0u, 0u, 0u, 0u};
+    if (head0 != kNoSlab) {
       uint4 q[8];
       const uint4 *sp = wst + ((size_t)st * 32 + lane) * kStageStride;
       if (ready) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) q[j] = sp[j];
       } else {
-        lane_load_slab(g, cur.head, q);
+        lane_load_slab(g, head0, q);
       }
-      const uint32_t app = kInsert ? lane_insert_chain<kWeighted>(g, cur.head, q, cur.v, cur.wt)
-                                   : lane_delete_chain<kWeighted>(g, cur.head, q, cur.v);
-      applied[base + lane] = (uint8_t)app;
-      if (app) {
-        if (kInsert)
-          atomicAdd(g.deg + cur.u, 1u);
-        else
-          atomicSub(g.deg + cur.u, 1u);
-        ++mine;
-      }
+      cur = upd_decide<kWeighted, kInsert>(g, q, head0, r0);
     }
-    if (!has_next) break;
+    prev = cur;
+    prev_e = edge_of(k);
+    if (!has1) break;
     __syncwarp();
-    cur = nxt;
-    base = nbase;
+    r0 = r1;
+    head0 = head1;
+    r1 = r2;
+    o1 = o2;
+    r2 = r3;
     st ^= 1u;
   }
+  finish(prev, prev_e);
+  mine = __reduce_add_sync(0xFFFFFFFFu, mine);
+  if (lane == 0 && mine) atomicAdd(count, (unsigned long long)mine);
+}
+
+// Warp-cooperative update kernel (no shared memory, no bulk copies): a warp
+// loads the head slabs of its 32 edges as 32 coalesced 128-byte loads (lane
+// l holds word l of every slab), then decides edge j from slab j with two
+// ballots (key found / first EMPTY word) and one shuffle (next-slab word);
+// lane j commits its own edge with one CAS.  Batch records and bucket
+// offsets are prefetched one group ahead, CAS results read one group later.
+template <bool kWeighted, bool kInsert>
+__global__ void __launch_bounds__(kCoopBlock, 3)
+    k_update_coop(GraphView g, const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                  const uint32_t *__restrict__ w, uint32_t n, uint8_t *__restrict__ applied,
+                  unsigned long long *count) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint64_t ngroups = ((uint64_t)n + 31) / 32;
+  if (warp >= ngroups) return;
+  const unsigned long long keep = l2_policy_evict_last();
+  const unsigned long long once = l2_policy_evict_first();
+  const uint32_t *words = reinterpret_cast<const uint32_t *>(g.slabs);
+  // key words: set slabs 0..30, map slabs the even words 0..28
+  const bool keylane = kWeighted ? ((lane & 1u) == 0 && lane < 30) : (lane < 31);
+  uint32_t mine = 0;
+  auto edge_of = [&](uint64_t k) { return (warp + k * nwarps) * 32 + lane; };
+  auto group_ok = [&](uint64_t k) { return warp + k * nwarps < ngroups; };
+  auto finish = [&](const UpdPending &p, uint64_t e) {
+    const uint32_t app = upd_finish<kWeighted, kInsert>(g, p);
+    if (app) {
+      red_add_hint_u32(g.deg + p.u, kInsert ? 1u : 0xFFFFFFFFu, keep);
+      ++mine;
+    }
+    if (e < n) applied[e] = (uint8_t)app;
+  };
+
+  UpdRaw r0 = upd_load<kWeighted, kInsert>(src, dst, w, n, edge_of(0), once);
+  UpdRaw r1 = group_ok(1) ? upd_load<kWeighted, kInsert>(src, dst, w, n, edge_of(1), once)
+                          : UpdRaw{0u, 0u, 0u, 0u};
+  UpdOff o0 = upd_offsets(g, r0, keep);
+  UpdPending prev{kNoSlab, 0u, 0u, 0u, 0u, 0u, 0u};
+  uint64_t prev_e = ~0ull;
+  for (uint64_t k = 0;; ++k) {
+    const bool has1 = group_ok(k + 1);
+    UpdOff o1{0u, 0u, 0u};
+    if (has1) o1 = upd_offsets(g, r1, keep);
+    UpdRaw r2{0u, 0u, 0u, 0u};
+    if (group_ok(k + 2)) r2 = upd_load<kWeighted, kInsert>(src, dst, w, n, edge_of(k + 2), once);
+    const uint32_t head0 = o0.ok ? o0.b0 + bucket_of(r0.v, o0.b1 - o0.b0) : kNoSlab;
+    uint32_t wv[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t h = __shfl_sync(0xFFFFFFFFu, head0, j);
+      wv[j] = h != kNoSlab ? __ldcg(words + (size_t)h * 32 + lane) : kEmptyKey;
+    }
+    if (k) finish(prev, prev_e);
+    LaneProbe pr{32u, 32u, kNoSlab};
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t vj = __shfl_sync(0xFFFFFFFFu, r0.v, j);
+      const uint32_t hit = __ballot_sync(0xFFFFFFFFu, keylane && wv[j] == vj);
+      const uint32_t emp = __ballot_sync(0xFFFFFFFFu, keylane && wv[j] == kEmptyKey);
+      const uint32_t nx = __shfl_sync(0xFFFFFFFFu, wv[j], 31);
+      if (lane == (uint32_t)j) {
+        pr.found_word = hit ? (uint32_t)__ffs(hit) - 1u : 32u;
+        pr.empty_word = emp ? (uint32_t)__ffs(emp) - 1u : 32u;
+        pr.next = nx;
+      }
+    }
+    UpdPending cur{kNoSlab, 0u, 0u, 0u, 0u, 0u, 0u};
+    if (head0 != kNoSlab) cur = upd_decide_probe<kWeighted, kInsert>(g, pr, head0, r0);
+    prev = cur;
+    prev_e = edge_of(k);
+    if (!has1) break;
+    r0 = r1;
+    o0 = o1;
+    r1 = r2;
+  }
+  finish(prev, prev_e);
   mine = __reduce_add_sync(0xFFFFFFFFu, mine);
   if (lane == 0 && mine) atomicAdd(count, (unsigned long long)mine);
 }
@@ -741,6 +973,24 @@ static int lane_grid(uint32_t n, const mk_graph *g) {
   return (int)blocks;
 }
 
+// Warp-cooperative kernel: one warp per group of 32 edges, capped at the
+// resident count (or update_blocks_per_sm blocks per SM when set).
+template <class K>
+static int coop_grid(uint32_t n, const mk_graph *g, K kernel) {
+  const uint64_t groups = ((uint64_t)n + 31) / 32;
+  uint64_t blocks = (groups + kCoopBlock / 32 - 1) / (kCoopBlock / 32);
+  uint32_t per_sm = g->tuning.update_blocks_per_sm;
+  if (per_sm == 0) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kCoopBlock, 0);
+    per_sm = occ > 0 ? (uint32_t)occ : 1u;
+  }
+  const uint64_t cap = (uint64_t)device_sm_count(g->device) * per_sm;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (int)blocks;
+}
+
 // Opts a kernel into kUpdSmem of dynamic shared memory, once per device.
 template <class K>
 static mk_status set_update_smem(K kernel) {
@@ -913,7 +1163,14 @@ mk_status mk_graph_insert_edges(mk_graph *g, const uint32_t *d_src,
   if (n == 0) return MK_OK;
   GraphView v = g->view();
   int blocks = update_grid(n, g->device);
-  if (g->tuning.update_kernel == 1) {
+  if (g->tuning.update_kernel == 2) {
+    if (g->weighted)
+      k_update_coop<true, true><<<coop_grid(n, g, k_update_coop<true, true>), kCoopBlock, 0, s>>>(
+          v, d_src, d_dst, d_w, n, g->applied.ptr, g->counters);
+    else
+      k_update_coop<false, true><<<coop_grid(n, g, k_update_coop<false, true>), kCoopBlock, 0, s>>>(
+          v, d_src, d_dst, nullptr, n, g->applied.ptr, g->counters);
+  } else if (g->tuning.update_kernel == 1) {
     if (g->weighted)
       k_update_lane<true, true><<<lane_grid(n, g), 256, 0, s>>>(v, d_src, d_dst, d_w, n,
                                                                 g->applied.ptr, g->counters);
@@ -944,7 +1201,14 @@ mk_status mk_graph_delete_edges(mk_graph *g, const uint32_t *d_src,
   if (n == 0) return MK_OK;
   GraphView v = g->view();
   int blocks = update_grid(n, g->device);
-  if (g->tuning.update_kernel == 1) {
+  if (g->tuning.update_kernel == 2) {
+    if (g->weighted)
+      k_update_coop<true, false><<<coop_grid(n, g, k_update_coop<true, false>), kCoopBlock, 0, s>>>(
+          v, d_src, d_dst, nullptr, n, g->applied.ptr, g->counters);
+    else
+      k_update_coop<false, false><<<coop_grid(n, g, k_update_coop<false, false>), kCoopBlock, 0, s>>>(
+          v, d_src, d_dst, nullptr, n, g->applied.ptr, g->counters);
+  } else if (g->tuning.update_kernel == 1) {
     if (g->weighted)
       k_update_lane<true, false><<<lane_grid(n, g), 256, 0, s>>>(v, d_src, d_dst, nullptr, n,
                                                                  g->applied.ptr, g->counters);
@@ -984,7 +1248,7 @@ mk_status mk_graph_search_edges(mk_graph *g, const uint32_t *d_src,
 
 mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t) {
   if (!g || !t) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: null argument");
-  if (t->update_kernel > 1) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_kernel must be 0 or 1");
+  if (t->update_kernel > 2) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_kernel must be 0, 1 or 2");
   if (t->update_blocks_per_sm > 32) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_blocks_per_sm > 32");
   if (t->frontier_chunk > 1024) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: frontier_chunk > 1024");
   g->tuning = *t;

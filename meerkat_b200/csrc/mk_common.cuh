@@ -202,12 +202,36 @@ __device__ __forceinline__ void bulk_load(void *dst_smem, const void *src_gmem, 
       "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-// L2 policy that keeps lines resident (used for slabs that are about to be
-// updated with an atomic right after the bulk copy).
+// L2 policies: evict_last for small arrays read on every edge (bucket
+// offsets, degrees), evict_first for data streamed once (batch arrays).
 __device__ __forceinline__ unsigned long long l2_policy_evict_last() {
   unsigned long long pol;
   asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
   return pol;
+}
+__device__ __forceinline__ unsigned long long l2_policy_evict_first() {
+  unsigned long long pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// Loads issued where they stand (volatile: the compiler keeps their order
+// against the other asm, so a prefetch is not sunk to its use).
+__device__ __forceinline__ uint32_t ld_hint_u32(const uint32_t *p, unsigned long long pol) {
+  uint32_t v;
+  asm volatile("ld.global.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t *p, unsigned long long pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+               : "=r"(v)
+               : "l"(p), "l"(pol));
+  return v;
+}
+// Fire-and-forget add with an L2 policy (degree counters).
+__device__ __forceinline__ void red_add_hint_u32(uint32_t *p, uint32_t v, unsigned long long pol) {
+  asm volatile("red.global.add.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol)
+               : "memory");
 }
 // Bulk copy global -> shared with an L2 cache policy (no multicast).
 __device__ __forceinline__ void bulk_load_hint(void *dst_smem, const void *src_gmem, uint32_t bytes,

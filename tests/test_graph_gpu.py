@@ -20,7 +20,7 @@ def rmat12():
     return mk.gen_rmat(12, 60000, seed=11, w_lo=1, w_hi=64)
 
 
-VARIANTS = [0, 1]  # update kernels: warp-staged TMA, lane per edge
+VARIANTS = [0, 1, 2]  # update kernels: warp-staged TMA, lane per edge, warp-cooperative
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
