@@ -764,6 +764,9 @@ def main():
     upd_ms = ms / K  # device time of one delete + insert pair (graph replay)
     achieved = upd_bytes / (upd_ms / 1000.0) / 1e9
     traffic = profile_traffic()
+    # the same random-line pattern without decision logic, on a buffer the
+    # size of the slab pool: what the memory system gives this access pattern
+    ceiling = mk.probe_random_rmw(int(info["pool_capacity"]) * 128, V, 2 * HALF, device=local)
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(graph, batches[W:W + K], max_batches=3)
@@ -791,7 +794,13 @@ def main():
                          "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak,
                          "algorithmic_bytes_per_step": upd_bytes,
-                         "traffic": traffic},
+                         "traffic": traffic,
+                         "pattern_ceiling": {
+                             "what": "mk_probe_random_rmw: random 128-B line read + CAS + random "
+                                     "4-B read and add per operation, no decision logic, "
+                                     f"{2 * HALF} operations on a {int(info['pool_capacity']) * 128 >> 20} MiB buffer",
+                             **ceiling,
+                             "frac": (upd_per_step / (ms / K / 1000.0)) / ceiling["update_pattern_per_s"]}},
             "host_driven_delete_ms": statistics.mean(del_ms),
             "host_driven_insert_ms": statistics.mean(ins_ms),
             "tuning": tuning,

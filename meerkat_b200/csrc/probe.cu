@@ -1,0 +1,101 @@
+// probe.cu -- ceiling of the update path's memory pattern on this device.
+//
+// The update kernels touch, per edge, one random 128-byte slab line (read,
+// then a CAS on one of its words), one random word of the bucket-offset
+// array (read) and one random word of the degree array (add).  A copy kernel
+// measures sequential bandwidth, which random line traffic cannot reach; this
+// probe replays the same pattern with no decision logic so the update
+// kernels can be judged against what the memory system delivers for it.
+//
+//   mode 0  random 128-byte line reads
+//   mode 1  mode 0 + one CAS per line (the slab read-modify-write)
+//   mode 2  mode 1 + a random 4-byte read and a random 4-byte add on two
+//           per-vertex arrays of `small_words` words each
+//
+// Warp-cooperative: a warp reads the lines of its 32 operations as 32
+// coalesced loads, lane j then issues operation j's CAS / add.  Lines and
+// words are chosen by a counter-based hash of (seed, operation).
+#include <cuda_runtime.h>
+
+#include "mk_internal.h"
+
+namespace mk {
+namespace {
+
+__device__ __forceinline__ unsigned long long probe_mix(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+__global__ void __launch_bounds__(256) k_probe_rmw(uint32_t *__restrict__ lines, uint64_t nlines,
+                                                   uint32_t *__restrict__ small_a,
+                                                   uint32_t *__restrict__ small_b,
+                                                   uint32_t small_words, uint64_t nops,
+                                                   uint32_t mode, unsigned long long seed,
+                                                   unsigned long long *sink) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  unsigned long long acc = 0;
+  for (uint64_t base = warp * 32; base < nops; base += nwarps * 32) {
+    const uint64_t op = base + lane;
+    const unsigned long long h = probe_mix(seed ^ op);
+    const uint64_t line = op < nops ? h % nlines : ~0ull;
+    uint32_t v[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t lj = __shfl_sync(0xFFFFFFFFu, line, j);
+      v[j] = lj != ~0ull ? __ldcg(lines + lj * 32 + lane) : 0u;
+    }
+    uint32_t mine = 0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t w5 = __shfl_sync(0xFFFFFFFFu, v[j], 5);
+      if (lane == (uint32_t)j) mine = w5;
+      acc += v[j];
+    }
+    if (line != ~0ull && mode >= 1) {
+      uint32_t *p = lines + line * 32 + 5;
+      acc += atomicCAS(p, mine, mine + 1u);
+    }
+    if (line != ~0ull && mode >= 2) {
+      const uint32_t i = (uint32_t)(h >> 32) % small_words;
+      const uint32_t k = (uint32_t)(probe_mix(h) % small_words);
+      acc += __ldcg(small_a + i);
+      atomicAdd(small_b + k, 1u);
+    }
+  }
+  if (acc == 0x5EEDull) atomicAdd(sink, acc);  // keeps the loads live
+}
+
+}  // namespace
+}  // namespace mk
+
+using namespace mk;
+
+extern "C" mk_status mk_probe_random_rmw(void *d_lines, uint64_t line_count, void *d_small_a,
+                                         void *d_small_b, uint32_t small_words, uint64_t num_ops,
+                                         uint32_t mode, uint64_t seed, void *d_sink, void *stream,
+                                         float *ms_out) {
+  if (!d_lines || !line_count || !d_sink || mode > 2 ||
+      (mode == 2 && (!d_small_a || !d_small_b || !small_words)))
+    return fail(MK_ERR_INVALID, "mk_probe_random_rmw: bad argument");
+  int dev = 0;
+  MK_CUDA(cudaGetDevice(&dev));
+  cudaStream_t s = as_stream(stream);
+  Timer t;
+  MK_CHECK(t.start(s, ms_out != nullptr));
+  int per_sm = 0;
+  MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_rmw, 256, 0));
+  const uint64_t want = (num_ops + 255) / 256;
+  const uint64_t cap = (uint64_t)device_sm_count(dev) * (per_sm > 0 ? per_sm : 1);
+  const int blocks = (int)(want < cap ? (want ? want : 1) : cap);
+  k_probe_rmw<<<blocks, 256, 0, s>>>(static_cast<uint32_t *>(d_lines), line_count,
+                                     static_cast<uint32_t *>(d_small_a),
+                                     static_cast<uint32_t *>(d_small_b), small_words, num_ops,
+                                     mode, seed, static_cast<unsigned long long *>(d_sink));
+  MK_CUDA(cudaGetLastError());
+  return t.stop(ms_out);
+}
