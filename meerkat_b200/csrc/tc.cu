@@ -145,37 +145,77 @@ __device__ __forceinline__ bool set_contains_cg(const uint32_t *set, uint32_t ca
   }
 }
 
+constexpr uint32_t kTcChunk = 32;  // N+(u) entries per work item
+
+// Work items of the forward algorithm: (u, chunk c) covers N+(u)[32c, 32c+32).
+// Per-vertex work is heavy-tailed (a hub's neighbours have long N+ lists),
+// so vertices are split into chunks and handed out dynamically.  Vertices
+// with N+(u) larger than kTcSmallMax go to the big list instead.
+__global__ void k_tc_item_count(uint32_t V, const unsigned long long *__restrict__ orow,
+                                uint32_t *__restrict__ icnt, uint32_t *big_list, uint32_t *big_n) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < V; u += gridDim.x * blockDim.x) {
+    const uint32_t du = (uint32_t)(orow[u + 1] - orow[u]);
+    uint32_t c = 0;
+    if (du >= 2) {  // a triangle needs two oriented edges out of u
+      if (du > kTcSmallMax)
+        big_list[atomicAdd(big_n, 1u)] = u;
+      else
+        c = (du + kTcChunk - 1) / kTcChunk;
+    }
+    icnt[u] = c;
+  }
+}
+
+__global__ void k_tc_item_fill(uint32_t V, const uint32_t *__restrict__ icnt,
+                               const unsigned long long *__restrict__ ioff,
+                               unsigned long long *__restrict__ items) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < V; u += gridDim.x * blockDim.x) {
+    const uint32_t c = icnt[u];
+    const unsigned long long b = ioff[u];
+    for (uint32_t j = 0; j < c; ++j) items[b + j] = ((unsigned long long)j << 32) | u;
+  }
+}
+
+// Persistent warps take work items from a global counter.  For item (u, c)
+// the warp stages N+(u) in a shared-memory hash set and streams N+(v) for the
+// item's 32 neighbours v with coalesced reads, probing the set.
 __global__ void __launch_bounds__(kTcWarps * 32)
-    k_tc_small(uint32_t V, const unsigned long long *__restrict__ orow,
-               const uint32_t *__restrict__ ocol, unsigned long long *count,
-               uint32_t *big_list, uint32_t *big_n) {
+    k_tc_small(const unsigned long long *__restrict__ orow, const uint32_t *__restrict__ ocol,
+               const unsigned long long *__restrict__ items, const unsigned long long *nitems_p,
+               uint32_t *next, unsigned long long *count) {
   __shared__ uint32_t sets[kTcWarps][kTcSetCap];
   const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   uint32_t *set = sets[wib];
+  const unsigned long long nitems = *nitems_p;
   unsigned long long c = 0;
-  for (uint32_t u = warp; u < V; u += nwarps) {
+  uint32_t have_u = 0xFFFFFFFFu;  // vertex whose set is staged
+  uint32_t cap = 64;
+  for (;;) {
+    uint32_t it = 0;
+    if (lane == 0) it = atomicAdd(next, 1u);
+    it = __shfl_sync(0xFFFFFFFFu, it, 0);
+    if (it >= nitems) break;
+    const unsigned long long item = items[it];
+    const uint32_t u = (uint32_t)item, chunk = (uint32_t)(item >> 32);
     const unsigned long long r0 = orow[u], r1 = orow[u + 1];
     const uint32_t du = (uint32_t)(r1 - r0);
-    if (du < 2) continue;  // a triangle needs two oriented edges out of u
-    if (du > kTcSmallMax) {
-      if (lane == 0) big_list[atomicAdd(big_n, 1u)] = u;
-      continue;
+    if (u != have_u) {
+      __syncwarp();
+      cap = 64;
+      while (cap < 2 * du) cap <<= 1;
+      for (uint32_t i = lane; i < cap; i += 32) set[i] = kEmptyKey;
+      __syncwarp();
+      for (uint32_t i = lane; i < du; i += 32) set_insert(set, cap - 1, ocol[r0 + i]);
+      __syncwarp();
+      have_u = u;
     }
-    uint32_t cap = 64;
-    while (cap < 2 * du) cap <<= 1;
-    for (uint32_t i = lane; i < cap; i += 32) set[i] = kEmptyKey;
-    __syncwarp();
-    for (uint32_t i = lane; i < du; i += 32) set_insert(set, cap - 1, ocol[r0 + i]);
-    __syncwarp();
-    for (uint32_t i = 0; i < du; ++i) {
+    const uint32_t i0 = chunk * kTcChunk, i1 = min(du, i0 + kTcChunk);
+    for (uint32_t i = i0; i < i1; ++i) {
       const uint32_t v = ocol[r0 + i];
       const unsigned long long s0 = orow[v], s1 = orow[v + 1];
       for (unsigned long long j = s0 + lane; j < s1; j += 32)
         c += set_contains(set, cap - 1, ocol[j]);
     }
-    __syncwarp();
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
@@ -388,7 +428,7 @@ struct mk_tc {
   unsigned long long *dcount = nullptr;  // [0] count, [1] scratch accumulator
   uint32_t *small = nullptr;             // [0] big_n
   DevBuf<uint32_t> ocnt, ocol, big_list, big_scratch, bcnt, bfill, bcol, pidx;
-  DevBuf<unsigned long long> orow, tmp, brow, pkeys, bpos;
+  DevBuf<unsigned long long> orow, tmp, brow, pkeys, bpos, items;
   Timer timer;
 };
 
@@ -424,10 +464,22 @@ static mk_status tc_static(mk_tc *t, cudaStream_t s) {
     k_orient_fill<false><<<blocks, 256, 0, s>>>(gv, t->bpos.ptr, t->ocol.ptr);
   MK_CHECK(t->big_list.reserve(V, &acc));
   MK_CUDA(cudaMemsetAsync(t->dcount, 0, 8, s));
-  MK_CUDA(cudaMemsetAsync(t->small, 0, 4, s));
-  int sblocks = std::min<uint64_t>((uint64_t)V / kTcWarps + 1, (uint64_t)device_sm_count(g->device) * 4);
-  k_tc_small<<<sblocks, kTcWarps * 32, 0, s>>>(V, t->orow.ptr, t->ocol.ptr, t->dcount,
-                                              t->big_list.ptr, t->small);
+  MK_CUDA(cudaMemsetAsync(t->small, 0, 8, s));  // [0] big count, [1] work-item counter
+  // work items (the orientation scratch is free again: ocnt >= V words,
+  // bpos >= V + 1)
+  const int vb = (int)std::min<uint64_t>((uint64_t)V / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  k_tc_item_count<<<vb, 256, 0, s>>>(V, t->orow.ptr, t->ocnt.ptr, t->big_list.ptr, t->small);
+  MK_CHECK(scan_u32_to_u64(t->ocnt.ptr, t->bpos.ptr, V, t->tmp, s));
+  unsigned long long nitems = 0;
+  MK_CUDA(cudaMemcpyAsync(&nitems, t->bpos.ptr + V, 8, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  MK_CHECK(t->items.reserve(std::max<unsigned long long>(nitems, 1), &acc));
+  k_tc_item_fill<<<vb, 256, 0, s>>>(V, t->ocnt.ptr, t->bpos.ptr, t->items.ptr);
+  int per_sm = 0;
+  MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_small, kTcWarps * 32, 0));
+  const int sblocks = device_sm_count(g->device) * std::max(per_sm, 1);
+  k_tc_small<<<sblocks, kTcWarps * 32, 0, s>>>(t->orow.ptr, t->ocol.ptr, t->items.ptr,
+                                              t->bpos.ptr + V, t->small + 1, t->dcount);
   // big vertices: one block each, global-memory set
   uint32_t nbig = 0;
   MK_CUDA(cudaMemcpyAsync(&nbig, t->small, 4, cudaMemcpyDeviceToHost, s));
@@ -570,6 +622,7 @@ mk_status mk_tc_destroy(mk_tc *t) {
   t->brow.release();
   t->pkeys.release();
   t->bpos.release();
+  t->items.release();
   delete t;
   return MK_OK;
 }
