@@ -562,10 +562,12 @@ def run_serving(args, rank, world, local):
     srv.run(warm, wl, mode="coalesced")
     clocks = Clocks(local)
     table = []
-    for rate, reqs in blocks:
+    for j, (rate, reqs) in enumerate(blocks):
         row = {"offered_rps": rate}
-        for mode in ("coalesced", "alone"):
+        # both modes start with no cached view; the order alternates by rate
+        for mode in (("coalesced", "alone") if j % 2 == 0 else ("alone", "coalesced")):
             rs = [S.Request(r.rid, r.graph, r.kind, r.arrival, r.source, r.lo, r.hi) for r in reqs]
+            srv.reset_views()
             t1 = time.time()
             out = srv.run(rs, wl, mode=mode)
             log(f"[serving] {rate:.0f} rps {mode}: p50 {out['p50_ms']:.2f} ms p99 "

@@ -266,6 +266,22 @@ mk_status mk_pagerank_stats(mk_pagerank *p, uint32_t *h_iters,
                             float *h_delta);
 mk_status mk_pagerank_destroy(mk_pagerank *p);
 
+/* PageRank of one vertex range of an OUT-edge graph (a graph-set member),
+ * push form, FP64 accumulation: no reverse graph needed.  Same formula,
+ * start and stopping rule as above with N = v_end - v_begin; out-degrees are
+ * the graph's live degrees.  The range must be closed under out-edges.
+ * No counterpart in the reference (whose PageRank needs the reverse graph). */
+typedef struct mk_pagerank_range mk_pagerank_range;
+mk_status mk_pagerank_range_create(mk_graph *g, uint32_t max_vertices,
+                                   mk_pagerank_range **out);
+mk_status mk_pagerank_range_run(mk_pagerank_range *p, uint32_t v_begin, uint32_t v_end,
+                                float damping, float tol, uint32_t max_iter,
+                                void *stream, float *ms_out);
+/* The last run's v_end - v_begin values (host). */
+mk_status mk_pagerank_range_values(mk_pagerank_range *p, float *h_out);
+mk_status mk_pagerank_range_stats(mk_pagerank_range *p, uint32_t *h_iters, float *h_delta);
+mk_status mk_pagerank_range_destroy(mk_pagerank_range *p);
+
 /* ------------------------------------------------------------------------
  * Triangle counting on a symmetric graph (replaces TC<AllocPolicy>,
  * include/Algorithms/TC.cuh:9-40).

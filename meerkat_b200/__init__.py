@@ -18,7 +18,8 @@ import numpy as np
 
 from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
-__all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "TC", "WCC", "EdgeSet",
+__all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "PageRankRange", "TC", "WCC",
+           "EdgeSet",
            "gen_rmat", "gen_grid", "gen_rmat_members", "read_edge_list", "read_batch",
            "write_edge_list", "write_batch", "MeerkatError", "MK_INF", "lib", "version"]
 
@@ -383,6 +384,47 @@ class PageRank(_Timed):
         it = C.c_uint32(0)
         dl = C.c_float(0)
         check(lib().mk_pagerank_stats(self._h, C.byref(it), C.byref(dl)), "mk_pagerank_stats")
+        return it.value, dl.value
+
+
+class PageRankRange(_Timed):
+    """PageRank of one vertex range (a GraphSet member) of an out-edge graph,
+    push form: no reverse graph needed (mk_pagerank_range_*)."""
+
+    def __init__(self, G: DynamicGraph, max_vertices: int):
+        self.G = G
+        h = C.c_void_p()
+        check(lib().mk_pagerank_range_create(G.handle, int(max_vertices), C.byref(h)),
+              "mk_pagerank_range_create")
+        self._h = h
+        self._n = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_pagerank_range_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Run(self, v_begin: int, v_end: int, damping: float = 0.85, tol: float = 1e-6,
+            max_iter: int = 200, stream=None, timed=True):
+        self._n = int(v_end) - int(v_begin)
+        return self._call(lib().mk_pagerank_range_run, self._h, int(v_begin), int(v_end),
+                          float(damping), float(tol), int(max_iter), _stream(stream), timed=timed)
+
+    def Values(self) -> np.ndarray:
+        out = np.zeros(self._n, dtype=np.float32)
+        check(lib().mk_pagerank_range_values(self._h, out.ctypes.data), "mk_pagerank_range_values")
+        return out
+
+    def stats(self):
+        it = C.c_uint32(0)
+        dl = C.c_float(0)
+        check(lib().mk_pagerank_range_stats(self._h, C.byref(it), C.byref(dl)), "stats")
         return it.value, dl.value
 
 

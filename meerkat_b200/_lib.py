@@ -83,6 +83,12 @@ SIGNATURES = [
     ("mk_pagerank_values_device", _S, [vp, C.POINTER(vp)]),
     ("mk_pagerank_stats", _S, [vp, u32p, f32p]),
     ("mk_pagerank_destroy", _S, [vp]),
+    ("mk_pagerank_range_create", _S, [vp, C.c_uint32, C.POINTER(vp)]),
+    ("mk_pagerank_range_run", _S, [vp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_uint32,
+                                   vp, f32p]),
+    ("mk_pagerank_range_values", _S, [vp, vp]),
+    ("mk_pagerank_range_stats", _S, [vp, u32p, f32p]),
+    ("mk_pagerank_range_destroy", _S, [vp]),
     ("mk_tc_create", _S, [vp, C.POINTER(vp)]),
     ("mk_tc_static", _S, [vp, vp, f32p]),
     ("mk_tc_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),

@@ -11,14 +11,14 @@ queue -- are served by coalesced launches:
                                         (one source per queried graph)
   WCC queries                           one subset union-find pass
 
-PageRank pulls over in-edges and triangle counting needs the symmetric
-graph, so those requests run on per-graph views (a reverse graph for
-PageRank, a symmetric graph for TC) built on first use from a CSR export of
-the member and kept current by replaying every later update of that graph on
+PageRank runs on the member's out-edges directly (push form,
+mk_pagerank_range_*).  Triangle counting needs the symmetric graph, so TC
+requests run on per-graph views built on first use from a CSR export of the
+member and kept current by replaying every later update of that graph on
 them.  Views are admitted under a device-memory budget and evicted
-least-recently-used.  These heavy requests run one per round after the
-coalesced fast work, so a triangle count does not hold up the updates and
-traversals of other graphs.
+least-recently-used.  These heavy requests run after the coalesced fast
+work of their round, one segment each, so a triangle count does not hold up
+the updates and traversals of other graphs in that round.
 
 Each graph's requests are served in arrival order, so every request sees
 exactly the updates of its graph that arrived before it, whether it shares
@@ -38,7 +38,8 @@ from typing import Dict, List, Optional
 
 import numpy as np
 
-from . import BFS, SSSP, TC, WCC, DynamicGraph, GraphSet, PageRank, gen_rmat_members
+from . import (BFS, SSSP, TC, WCC, DynamicGraph, GraphSet, PageRank, PageRankRange,
+               gen_rmat_members)
 
 INSERT, DELETE, BFS_Q, SSSP_Q, PAGERANK_Q, TC_Q, WCC_Q = range(7)
 KIND_NAMES = ["insert", "delete", "bfs", "sssp", "pagerank", "tc", "wcc"]
@@ -242,16 +243,25 @@ class GraphServer:
         self.bfs = BFS(self.G, first)
         self.sssp = SSSP(self.G, first)
         self.wcc = WCC(self.G)
+        sizes = np.diff(self.off)
+        self.prr = PageRankRange(self.G, int(sizes.max()))
         self.views: "collections.OrderedDict[tuple, _View]" = collections.OrderedDict()
         V = gs.num_vertices
         info = self.G.info()
         # graph + two traversals (dist, stamp, bitmap, two frontiers, list) + WCC
+        # + range PageRank (two FP64 vectors and an FP32 copy of the largest member)
         trav = 8 * V + 4 * V + V // 8 + 2 * 8 * (info["num_buckets"] + 64) + 4 * V
-        self.resident = info["device_bytes"] + 2 * trav + 4 * V + V // 4
+        self.resident = info["device_bytes"] + 2 * trav + 4 * V + V // 4 + 20 * int(sizes.max())
         if self.resident > self.budget:
             raise MemoryError(f"resident set {self.resident} B exceeds the budget {self.budget} B")
         self.view_builds = 0
         self.view_evictions = 0
+
+    def reset_views(self) -> None:
+        """Drops every cached view (a run that must start cold)."""
+        for v in self.views.values():
+            v.close()
+        self.views.clear()
 
     def view_bytes(self) -> int:
         return sum(v.bytes for v in self.views.values())
@@ -334,10 +344,11 @@ class GraphServer:
     # ---- one PageRank or triangle-count request on its graph's view ----
     def serve_heavy(self, r: Request) -> None:
         if r.kind == PAGERANK_Q:
-            v = self._view(r.graph, "rev")
-            v.algo.StaticRecount(timed=False)
+            # PageRank on the member's out-edges: no view to build
+            self.prr.Run(int(self.off[r.graph]), int(self.off[r.graph + 1]), 0.85, 1e-6, 200,
+                         timed=False)
             if self.record:
-                r.result = v.algo.Values()
+                r.result = self.prr.Values()
         else:
             v = self._view(r.graph, "sym")
             v.algo.Static(timed=False)
@@ -370,8 +381,9 @@ class GraphServer:
         """Serves `reqs` (sorted by arrival) against the wall clock: a request
         is admitted once its arrival time has passed.  "coalesced": each round
         takes the head request of every graph with a pending one, runs the fast
-        heads (at most max_round if > 0) as one coalesced segment and then the
-        oldest heavy head (PageRank / TC) as a second segment.  "alone": each
+        heads (at most max_round if > 0) as coalesced segments by kind (updates,
+        then BFS and WCC, then SSSP) and then the
+        heavy heads (PageRank / TC) one segment each.  "alone": each
         round runs the single oldest request.  A request completes when the
         GPU has finished its segment.  Returns latency and throughput."""
         import torch
@@ -379,6 +391,7 @@ class GraphServer:
         queues: Dict[int, collections.deque] = collections.defaultdict(collections.deque)
         fifo = collections.deque()
         i, served, rounds, n = 0, 0, 0, len(reqs)
+        builds0, evictions0 = self.view_builds, self.view_evictions
         t0 = time.perf_counter() - (reqs[0].arrival if reqs else 0.0)
         while served < n:
             now = time.perf_counter() - t0
@@ -403,10 +416,14 @@ class GraphServer:
                 heavy = [r for r in heads if r.kind in HEAVY_KINDS]
                 if max_round > 0:
                     fast = fast[:max_round]
-                if fast:
-                    segments.append(("fast", fast))
-                if heavy:  # one heavy request per round, oldest first
-                    segments.append(("heavy", heavy[:1]))
+                # cheap kinds first, each kind group its own segment, so an
+                # update does not wait for the round's traversals
+                for kinds in ((INSERT, DELETE), (BFS_Q, WCC_Q), (SSSP_Q,)):
+                    seg = [r for r in fast if r.kind in kinds]
+                    if seg:
+                        segments.append(("fast", seg))
+                for r in heavy:  # each heavy request its own segment, oldest first
+                    segments.append(("heavy", [r]))
                 for _, rs in segments:
                     for r in rs:
                         queues[r.graph].popleft()
@@ -440,12 +457,12 @@ class GraphServer:
                 "p99_ms": float(np.percentile(lat, 99)) if n else 0.0,
                 "mean_ms": float(lat.mean()) if n else 0.0,
                 "throughput_rps": n / span if span > 0 else 0.0,
-                "by_kind": by_kind, "view_builds": self.view_builds,
-                "view_evictions": self.view_evictions}
+                "by_kind": by_kind, "view_builds": self.view_builds - builds0,
+                "view_evictions": self.view_evictions - evictions0}
 
     def close(self):
         for v in self.views.values():
             v.close()
         self.views.clear()
-        for o in (self.bfs, self.sssp, self.wcc):
+        for o in (self.bfs, self.sssp, self.wcc, self.prr):
             o.close()

@@ -220,3 +220,28 @@ def test_wcc_ranges_touch_only_their_members():
             np.testing.assert_array_equal(lab[lo:hi].astype(np.int64) - lo, O.wcc())
         else:
             np.testing.assert_array_equal(lab[lo:hi], before[lo:hi])
+
+
+def test_range_pagerank_matches_each_member():
+    mem = members(n=6, seed=70)
+    S, oracles = build_set(mem)
+    off = S.offsets.astype(np.int64)
+    prr = mk.PageRankRange(S.graph, int(np.diff(off).max()))
+    for m, O in enumerate(oracles):
+        prr.Run(off[m], off[m + 1], 0.85, 1e-6, 500)
+        want, _ = O.pagerank(0.85, 1e-14)
+        got = prr.Values().astype(np.float64)
+        assert len(got) == off[m + 1] - off[m]
+        assert np.abs(got - want).sum() <= 1e-6, m
+    # after an update of one member, its ranks follow (live out-degrees)
+    V, s, d, _ = mem[2]
+    es = mk.EdgeSet(V, s, d)
+    ds, dd = es.sample_present(len(s) // 4, seed=3)
+    S.graph.DeleteEdges(to_dev(ds + off[2]), to_dev(dd + off[2]))
+    assert S.graph.sync() == 0
+    oracles[2].delete(ds, dd)
+    prr.Run(off[2], off[3], 0.85, 1e-6, 500)
+    want, _ = oracles[2].pagerank(0.85, 1e-14)
+    assert np.abs(prr.Values().astype(np.float64) - want).sum() <= 1e-6
+    with pytest.raises(mk.MeerkatError):
+        prr.Run(0, off[-1])  # larger than max_vertices

@@ -105,7 +105,7 @@ def test_views_are_evicted_under_a_small_budget():
     reqs = S.make_requests(wl, edges, 40, rate=1e7, seed=7,
                            mix=(0.1, 0.1, 0, 0, 0.4, 0.4, 0), upd_lo=10, upd_hi=500)
     srv = S.GraphServer(gs, budget_bytes=1 << 40, record=True)
-    srv.budget = srv.resident + (4 << 20)  # room for about one view
+    srv.budget = srv.resident + (1 << 20)  # room for about one view
     r = srv.run(reqs, wl, mode="coalesced")
     assert r["view_builds"] >= 2 and r["view_evictions"] >= 1
     assert srv.resident + srv.view_bytes() <= srv.budget
