@@ -22,9 +22,13 @@ Reported:
              per step, CUDA-graph replay) against the per-graph launch
              sequence on the same members and batches, with every member's
              answer checked equal in both arms
+  serving    64 resident R-MAT graphs (scales 18-23) under a 120 GB budget,
+             open-loop Poisson requests at two offered rates, served with
+             continuous batching and one request at a time (p50 / p99)
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload batched [--graphs G]   # the batched comparison alone
+    python bench.py --workload serving [--serving-rates R1,R2,...]   # the serving sweep alone
 """
 from __future__ import annotations
 
@@ -524,28 +528,22 @@ def batched_compare(num_graphs, K, W, rank, world, local):
     return out
 
 
-def run_serving(args, rank, world, local):
+def serving_compare(num_graphs, scales, rates, N, budget_gb, rank, world, local):
     """Open-loop serving: G resident R-MAT graphs (scales uniform in the given
     range, edge factor 16, weights U[1,1000]) in one graph set under a device
     memory budget; Poisson arrivals at each offered rate; mix 50% updates
     (log-uniform 1K-1M edges, half inserts, half deletes), 30% BFS/SSSP, 10%
     PageRank, 10% TC/WCC.  Each rate is served twice with the same request
     log: coalesced (continuous batching, one request per graph per round) and
-    alone (one request per round: the plain per-request launch sequence)."""
+    alone (one request per round: the plain per-request launch sequence).
+    Returns the summary (rank 0 reports it)."""
     import torch
 
     from meerkat_b200 import serving as S
-    from meerkat_b200.build import build
-    if rank == 0:
-        build()
-    barrier(world)
-    torch.cuda.set_device(local)
     seed = SEED + 7 + rank
-    lo_s, hi_s = (int(x) for x in args.serving_scales.split(","))
-    rates = [float(x) for x in args.serving_rates.split(",")]
-    N = args.serving_requests
+    lo_s, hi_s = scales
     t0 = time.time()
-    nv, ne = S.make_graph_sizes(args.serving_graphs, lo_s, hi_s, 16, seed)
+    nv, ne = S.make_graph_sizes(num_graphs, lo_s, hi_s, 16, seed)
     gs, edges = S.build_set(nv, ne, seed, device=local)
     log(f"[serving] {len(nv)} graphs, {int(nv.sum())} vertices, {int(ne.sum())} edges loaded "
         f"in {time.time() - t0:.1f}s: {gs.graph.info()}")
@@ -558,7 +556,7 @@ def run_serving(args, rank, world, local):
     del edges
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
-    srv = S.GraphServer(gs, budget_bytes=int(args.serving_budget_gb * 1e9), device=local)
+    srv = S.GraphServer(gs, budget_bytes=int(budget_gb * 1e9), device=local)
     srv.run(warm, wl, mode="coalesced")
     clocks = Clocks(local)
     table = []
@@ -576,28 +574,52 @@ def run_serving(args, rank, world, local):
             row[mode] = out
         table.append(row)
     clk = clocks.stop()
-    top = table[-1]
+    out = {
+        "workload": f"serving_{len(nv)}_graphs",
+        "graphs": f"{len(nv)} R-MAT graphs, scales U{{{lo_s}..{hi_s}}}, edge factor 16, "
+                  "weights U[1,1000]",
+        "vertices": int(nv.sum()), "edges": int(ne.sum()),
+        "mix": "25% insert, 25% delete (1K-1M edges, log-uniform), 15% BFS, 15% SSSP, "
+               "10% PageRank, 5% TC, 5% WCC; graph uniform",
+        "arrivals": "open-loop Poisson", "requests_per_rate": N, "budget_gb": budget_gb,
+        "rates": table, "clocks": clk, "warmup_requests": len(warm),
+        "resident_bytes": srv.resident, "view_bytes": srv.view_bytes(),
+    }
+    srv.close()
+    gs.close()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_serving(args, rank, world, local):
+    import torch
+
+    from meerkat_b200.build import build
+    if rank == 0:
+        build()
+    barrier(world)
+    torch.cuda.set_device(local)
+    scales = tuple(int(x) for x in args.serving_scales.split(","))
+    rates = [float(x) for x in args.serving_rates.split(",")]
+    r = serving_compare(args.serving_graphs, scales, rates, args.serving_requests,
+                        args.serving_budget_gb, rank, world, local)
+    top = r["rates"][-1]
     if rank == 0:
         line = {
             "metric": "serving throughput at the highest offered rate (coalesced)",
             "value": top["coalesced"]["throughput_rps"], "unit": "requests/s", "n_gpus": world,
-            "steps": len(rates), "warmup": len(warm), "ms_per_step": top["coalesced"]["p50_ms"],
+            "steps": len(rates), "warmup": r["warmup_requests"],
+            "ms_per_step": top["coalesced"]["p50_ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic",
-            "config": {"workload": f"serving_{len(nv)}_graphs",
-                       "graphs": f"{len(nv)} R-MAT graphs, scales U{{{lo_s}..{hi_s}}}, edge factor "
-                                 "16, weights U[1,1000]",
-                       "vertices": int(nv.sum()), "edges": int(ne.sum()),
-                       "mix": "25% insert, 25% delete (1K-1M edges, log-uniform), 15% BFS, "
-                              "15% SSSP, 10% PageRank, 5% TC, 5% WCC; graph uniform",
-                       "arrivals": "open-loop Poisson", "requests_per_rate": N,
-                       "budget_gb": args.serving_budget_gb},
+            "config": {k: r[k] for k in ("workload", "graphs", "vertices", "edges", "mix",
+                                         "arrivals", "requests_per_rate", "budget_gb")},
             "p50_ms": top["coalesced"]["p50_ms"], "p99_ms": top["coalesced"]["p99_ms"],
-            "rates": table, "clocks": clk,
-            "resident_bytes": srv.resident, "view_bytes": srv.view_bytes(),
+            "rates": r["rates"], "clocks": r["clocks"],
+            "resident_bytes": r["resident_bytes"], "view_bytes": r["view_bytes"],
         }
         print(json.dumps(line), flush=True)
-    srv.close()
     barrier(world)
     if world > 1:
         import torch.distributed as dist
@@ -659,6 +681,10 @@ def main():
     ap.add_argument("--serving-rates", default="25,50,100,200,400", help="offered req/s")
     ap.add_argument("--serving-requests", type=int, default=300, help="requests per rate")
     ap.add_argument("--serving-budget-gb", type=float, default=120.0)
+    ap.add_argument("--serving-in-line", default="20,160",
+                    help="updates workload: offered rates of the serving comparison attached to "
+                         "the line ('' = skip)")
+    ap.add_argument("--serving-in-line-requests", type=int, default=150)
     args = ap.parse_args()
     if args.workload == "serving":
         rank, world, local = dist_setup(args.gpus)
@@ -861,6 +887,19 @@ def main():
             "plain_ms_per_step", "plain_cuda_graph_ms_per_step", "batched_updates_per_s",
             "updates_per_step", "vertices", "edges", "gpu_launches_per_step",
             "plain_launches_per_step", "queries", "tuning", "equality", "clocks", "steps")}
+    serving = None
+    if args.serving_in_line:
+        rates = [float(x) for x in args.serving_in_line.split(",")]
+        scales = tuple(int(x) for x in args.serving_scales.split(","))
+        r = serving_compare(args.serving_graphs, scales, rates, args.serving_in_line_requests,
+                            args.serving_budget_gb, rank, world, local)
+        serving = {k: r[k] for k in ("workload", "vertices", "edges", "requests_per_rate",
+                                     "budget_gb", "clocks")}
+        serving["rates"] = [
+            {"offered_rps": row["offered_rps"],
+             **{m: {k: row[m][k] for k in ("p50_ms", "p99_ms", "throughput_rps", "rounds",
+                                          "view_builds")} for m in ("coalesced", "alone")}}
+            for row in r["rates"]]
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
@@ -895,6 +934,8 @@ def main():
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         if batched is not None:
             line["batched"] = batched
+        if serving is not None:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     barrier(world)
     if world > 1:
