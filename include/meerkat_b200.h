@@ -114,6 +114,10 @@ mk_status mk_graph_search_edges(mk_graph *g, const uint32_t *d_src,
 mk_status mk_graph_sync(mk_graph *g, void *stream, uint32_t *h_deverr);
 /* Number of batch edges the last insert/delete actually applied (synchronises). */
 mk_status mk_graph_last_applied(mk_graph *g, uint64_t *h_count);
+/* Stream-ordered copy of the same count into h_count (pinned host memory for
+ * a truly asynchronous copy): it lands once the update before it on `stream`
+ * has finished.  No counterpart in the reference. */
+mk_status mk_graph_last_applied_async(mk_graph *g, uint64_t *h_count, void *stream);
 /* Device pointer to the per-edge applied flags (uint8, one per batch entry)
  * of the last insert/delete; valid until the next update call. */
 mk_status mk_graph_last_applied_flags(mk_graph *g, const uint8_t **d_flags,

@@ -169,6 +169,11 @@ class DynamicGraph:
         check(lib().mk_graph_last_applied(self._h, C.byref(c)), "mk_graph_last_applied")
         return c.value
 
+    def last_applied_async(self, host_ptr: int, stream=None) -> None:
+        """Stream-ordered copy of the applied count to host_ptr (pinned u64)."""
+        check(lib().mk_graph_last_applied_async(self._h, host_ptr, _stream(stream)),
+              "mk_graph_last_applied_async")
+
     def degrees_into(self, out, stream=None):
         check(lib().mk_graph_degrees(self._h, _ptr(out), _stream(stream)), "mk_graph_degrees")
 

@@ -49,6 +49,7 @@ SIGNATURES = [
     ("mk_graph_search_edges", _S, [vp, vp, vp, C.c_uint32, vp, vp, vp]),
     ("mk_graph_sync", _S, [vp, vp, u32p]),
     ("mk_graph_last_applied", _S, [vp, u64p]),
+    ("mk_graph_last_applied_async", _S, [vp, vp, vp]),
     ("mk_graph_last_applied_flags", _S, [vp, C.POINTER(vp), u32p]),
     ("mk_graph_degrees", _S, [vp, vp, vp]),
     ("mk_graph_bucket_layout", _S, [vp, vp, vp]),

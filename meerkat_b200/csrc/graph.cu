@@ -1284,6 +1284,13 @@ mk_status mk_graph_last_applied(mk_graph *g, uint64_t *h_count) {
   return MK_OK;
 }
 
+mk_status mk_graph_last_applied_async(mk_graph *g, uint64_t *h_count, void *stream) {
+  if (!g || !h_count) return fail(MK_ERR_INVALID, "mk_graph_last_applied_async: null argument");
+  DeviceGuard dg(g->device);
+  MK_CUDA(cudaMemcpyAsync(h_count, g->counters, 8, cudaMemcpyDeviceToHost, as_stream(stream)));
+  return MK_OK;
+}
+
 mk_status mk_graph_last_applied_flags(mk_graph *g, const uint8_t **d_flags,
                                       uint32_t *n) {
   if (!g) return fail(MK_ERR_INVALID, "mk_graph_last_applied_flags: null graph");
