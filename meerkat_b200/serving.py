@@ -38,8 +38,7 @@ from typing import Dict, List, Optional
 
 import numpy as np
 
-from . import (BFS, SSSP, TC, WCC, DynamicGraph, GraphSet, PageRank, PageRankRange,
-               gen_rmat_members)
+from . import BFS, SSSP, TC, WCC, DynamicGraph, GraphSet, PageRankRange, gen_rmat_members
 
 INSERT, DELETE, BFS_Q, SSSP_Q, PAGERANK_Q, TC_Q, WCC_Q = range(7)
 KIND_NAMES = ["insert", "delete", "bfs", "sssp", "pagerank", "tc", "wcc"]
@@ -174,49 +173,35 @@ HEAVY_KINDS = (PAGERANK_Q, TC_Q)
 
 
 class _View:
-    """A copy of one member for the queries the union graph cannot answer:
-    kind "rev" (in-edges, PageRank) or "sym" (both directions, triangles)."""
+    """The symmetric copy of one member, for triangle counting (the union
+    graph holds out-edges only)."""
 
-    def __init__(self, gs: GraphSet, g: int, kind: str, device: int):
+    def __init__(self, gs: GraphSet, g: int, device: int):
         import torch
         lo, hi = int(gs.offsets[g]), int(gs.offsets[g + 1])
         n = hi - lo
-        self.n, self.kind = n, kind
+        self.n = n
         rp, col, _ = gs.graph.export_csr_range_device(lo, hi)
         rows = torch.repeat_interleave(torch.arange(n, device=col.device, dtype=torch.int32),
                                        (rp[1:] - rp[:-1]))
         cols = col - lo
         e = int(cols.numel())
         indeg = torch.bincount(cols.long(), minlength=n).to(torch.int32).cpu().numpy().view(np.uint32)
-        if kind == "rev":
-            self.graph = DynamicGraph(n, degree_hints=indeg, reverse=True, device=device,
-                                      pool_slabs=max(4096, (n + e // 20) // 4))
-            self.graph.InsertEdges(rows, cols)
-        else:
-            outdeg = (rp[1:] - rp[:-1]).to(torch.int32).cpu().numpy().view(np.uint32)
-            self.graph = DynamicGraph(n, degree_hints=indeg + outdeg, device=device,
-                                      pool_slabs=max(4096, (n + e // 10) // 4))
-            self.graph.InsertEdges(torch.cat([rows, cols]), torch.cat([cols, rows]))
+        outdeg = (rp[1:] - rp[:-1]).to(torch.int32).cpu().numpy().view(np.uint32)
+        self.graph = DynamicGraph(n, degree_hints=indeg + outdeg, device=device,
+                                  pool_slabs=max(4096, (n + e // 10) // 4))
+        self.graph.InsertEdges(torch.cat([rows, cols]), torch.cat([cols, rows]))
         del rp, col, rows, cols
         if self.graph.sync() != 0:
             raise RuntimeError("device error while building a view")
-        if kind == "rev":
-            self.algo = PageRank(self.graph, 0.85, 1e-6, n, max_iter=200)
-            extra = 28 * n  # rank, contribution and degree vectors, work items
-        else:
-            self.algo = TC(self.graph, n)
-            extra = 8 * n + 4 * e  # oriented copy of the symmetric edges
-        self.bytes = self.graph.info()["device_bytes"] + extra
+        self.tc = TC(self.graph, n)
+        # the graph, plus TC's oriented copy of the symmetric edges
+        self.bytes = self.graph.info()["device_bytes"] + 8 * n + 4 * e
 
-    def apply(self, kind: int, u, w_, reverse_found=None):
+    def apply(self, kind: int, u, w_, reverse_found):
         """Replays one update of the member (local ids) on the view."""
         import torch
-        if self.kind == "rev":
-            if kind == INSERT:
-                self.graph.InsertEdges(u, w_)
-            else:
-                self.graph.DeleteEdges(u, w_)
-        elif kind == INSERT:
+        if kind == INSERT:
             self.graph.InsertEdges(torch.cat([u, w_]), torch.cat([w_, u]))
         else:
             # the undirected edge goes only when neither direction is left
@@ -225,7 +210,7 @@ class _View:
             self.graph.DeleteEdges(torch.cat([uu, ww]), torch.cat([ww, uu]))
 
     def close(self):
-        self.algo.close()
+        self.tc.close()
         self.graph.close()
 
 
@@ -245,7 +230,7 @@ class GraphServer:
         self.wcc = WCC(self.G)
         sizes = np.diff(self.off)
         self.prr = PageRankRange(self.G, int(sizes.max()))
-        self.views: "collections.OrderedDict[tuple, _View]" = collections.OrderedDict()
+        self.views: "collections.OrderedDict[int, _View]" = collections.OrderedDict()
         V = gs.num_vertices
         info = self.G.info()
         # graph + two traversals (dist, stamp, bitmap, two frontiers, list) + WCC
@@ -266,24 +251,22 @@ class GraphServer:
     def view_bytes(self) -> int:
         return sum(v.bytes for v in self.views.values())
 
-    def _view(self, g: int, kind: str) -> _View:
-        key = (g, kind)
-        v = self.views.get(key)
+    def _view(self, g: int) -> _View:
+        v = self.views.get(g)
         if v is not None:
-            self.views.move_to_end(key)
+            self.views.move_to_end(g)
             return v
         lo, hi = int(self.off[g]), int(self.off[g + 1])
         n, e = hi - lo, int(self.G.count_edges(lo, hi))
-        mult = 1 if kind == "rev" else 2
-        est = 128 * (n + mult * e // 15) + 32 * n + 4 * e
+        est = 128 * (n + 2 * e // 15) + 8 * n + 4 * e
         while self.views and self.resident + self.view_bytes() + est > self.budget:
             _, old = self.views.popitem(last=False)
             old.close()
             self.view_evictions += 1
         if self.resident + est > self.budget:
-            raise MemoryError(f"graph {g}: a {kind} view does not fit the budget")
-        v = _View(self.gs, g, kind, self.device)
-        self.views[key] = v
+            raise MemoryError(f"graph {g}: its symmetric view does not fit the budget")
+        v = _View(self.gs, g, self.device)
+        self.views[g] = v
         self.view_builds += 1
         # the estimate was short: evict older views until the real size fits
         while len(self.views) > 1 and self.resident + self.view_bytes() > self.budget:
@@ -311,17 +294,16 @@ class GraphServer:
             self.G.InsertEdges(is_, id_, vals=iw)
         # keep cached views current (per graph: the same batch, local ids)
         for r in dels + inss:
-            views = [v for k, v in self.views.items() if k[0] == r.graph]
-            if not views:
+            v = self.views.get(r.graph)
+            if v is None:
                 continue
             base = int(self.off[r.graph])
             u, w_ = P_s[r.lo:r.hi] - base, P_d[r.lo:r.hi] - base
             found = None
-            if r.kind == DELETE and any(v.kind == "sym" for v in views):
+            if r.kind == DELETE:
                 found = torch.zeros(u.numel(), dtype=torch.uint8, device=u.device)
                 self.G.SearchEdges(P_d[r.lo:r.hi], P_s[r.lo:r.hi], found)
-            for v in views:
-                v.apply(r.kind, u, w_, found)
+            v.apply(r.kind, u, w_, found)
         bfs = [r for r in reqs if r.kind == BFS_Q]
         sssp = [r for r in reqs if r.kind == SSSP_Q]
         wccs = [r for r in reqs if r.kind == WCC_Q]
@@ -341,7 +323,7 @@ class GraphServer:
                     lo, hi = int(self.off[r.graph]), int(self.off[r.graph + 1])
                     r.result = (lab[lo:hi] - lo).astype(np.uint32)
 
-    # ---- one PageRank or triangle-count request on its graph's view ----
+    # ---- one PageRank (on the member itself) or triangle-count (on its view) request ----
     def serve_heavy(self, r: Request) -> None:
         if r.kind == PAGERANK_Q:
             # PageRank on the member's out-edges: no view to build
@@ -350,9 +332,9 @@ class GraphServer:
             if self.record:
                 r.result = self.prr.Values()
         else:
-            v = self._view(r.graph, "sym")
-            v.algo.Static(timed=False)
-            r.result = v.algo.GetCount()
+            v = self._view(r.graph)
+            v.tc.Static(timed=False)
+            r.result = v.tc.GetCount()
 
     def serve_round(self, reqs: List[Request], wl: Workload) -> None:
         """Fast requests as one coalesced round, then the heavy ones in order."""
