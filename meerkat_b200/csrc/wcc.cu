@@ -128,6 +128,70 @@ __global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, 
   }
 }
 
+// ---- static pass with the largest component skipped ----
+// Each vertex is first linked to up to two out-neighbours from its first
+// head slab; after compression most vertices of the largest component point
+// at its root.  The full pass then skips every edge whose endpoints both
+// point at that root (they are connected already), so on graphs with a giant
+// component most edges cost one read instead of two finds.  Skipping only
+// edges between vertices already connected keeps the result exact.
+constexpr uint32_t kUfSamples = 1024;
+
+template <bool kW>
+__global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.V; u += gridDim.x * blockDim.x) {
+    if (g.deg[u] == 0) continue;
+    if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(g.slabs + 8ull * g.boff[u]);
+    const uint32_t k0 = w[0], k1 = kW ? w[2] : w[1];
+    if (k0 < kTombKey && k0 != u) uf_union(p, u, k0, err);
+    if (k1 < kTombKey && k1 != u) uf_union(p, u, k1, err);
+  }
+}
+
+// One block: the most frequent root among kUfSamples strided vertices.
+__global__ void k_uf_giant(const uint32_t *p, uint32_t V, uint32_t *giant) {
+  __shared__ uint32_t smp[kUfSamples];
+  __shared__ unsigned long long best;
+  for (uint32_t i = threadIdx.x; i < kUfSamples; i += blockDim.x)
+    smp[i] = __ldcg(p + (uint32_t)(((unsigned long long)i * V) / kUfSamples));
+  if (threadIdx.x == 0) best = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < kUfSamples; i += blockDim.x) {
+    uint32_t c = 0;
+    for (uint32_t j = 0; j < kUfSamples; ++j) c += smp[j] == smp[i];
+    atomicMax(&best, ((unsigned long long)c << 32) | smp[i]);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *giant = (uint32_t)best;
+}
+
+template <bool kW>
+__global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bits,
+                                const uint32_t *giant_p, uint32_t *err) {
+  const Lanes L = lanes();
+  const uint32_t giant = *giant_p;
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
+    const uint32_t u = g.bowner[b];
+    if (g.deg[u] == 0) continue;
+    if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
+    const bool u_giant = __ldcg(p + u) == giant;
+    walk_bucket(g, L, b, [&](const uint4 &q) {
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+      for (int j = 0; j < keys_per_lane<kW>(); ++j) {
+        const uint32_t v = k[j];
+        if (v >= kTombKey || v == u) continue;
+        if (u_giant && __ldcg(p + v) == giant) continue;
+        uf_union(p, u, v, err);
+      }
+    });
+  }
+}
+
 // ---- vertex-range variants: only the listed ranges are touched ----
 // Ranges are given as prefix sums: range r covers the global indices
 // [pre[r], pre[r+1]) of a concatenation, starting at base[r].
@@ -193,6 +257,7 @@ struct mk_wcc {
   uint32_t *aff_labels = nullptr;
   uint32_t *aff_vertices = nullptr;
   uint32_t *err = nullptr;
+  uint32_t *giant = nullptr;  // root of the sampled largest component
   DevBuf<uint32_t> ranges;  // vpre, vbase, bpre, bbase of the last range call
   Timer timer;
 };
@@ -212,13 +277,34 @@ static mk_status wcc_edges(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
   return MK_OK;
 }
 
+// Unions of the out-edges of the selected vertices (all if sel is null), whose
+// parents start reset: sample two neighbours each, compress, find the largest
+// component, then every remaining edge that does not join two vertices of it.
+static mk_status wcc_link(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
+  mk_graph *g = w->g;
+  const int fg = flat_grid(g->V, g->device);
+  const GraphView v = g->view();
+  if (g->weighted)
+    k_uf_sample<true><<<fg, 256, 0, s>>>(v, w->parent, sel, w->err);
+  else
+    k_uf_sample<false><<<fg, 256, 0, s>>>(v, w->parent, sel, w->err);
+  k_uf_compress<<<fg, 256, 0, s>>>(w->parent, g->V, sel);
+  k_uf_giant<<<1, 1024, 0, s>>>(w->parent, g->V, w->giant);
+  const int blocks = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1,
+                                             (uint64_t)device_sm_count(g->device) * 8);
+  if (g->weighted)
+    k_uf_edges_skip<true><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->giant, w->err);
+  else
+    k_uf_edges_skip<false><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->giant, w->err);
+  k_uf_compress<<<fg, 256, 0, s>>>(w->parent, g->V, sel);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
 static mk_status wcc_static(mk_wcc *w, cudaStream_t s) {
   mk_graph *g = w->g;
   k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V);
-  MK_CHECK(wcc_edges(w, nullptr, s));
-  k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, nullptr);
-  MK_CUDA(cudaGetLastError());
-  return MK_OK;
+  return wcc_link(w, nullptr, s);
 }
 
 static bool batch_matches(const mk_graph *g, const uint32_t *d_src, const uint32_t *d_dst,
@@ -238,6 +324,7 @@ mk_status mk_wcc_create(mk_graph *g, mk_wcc **out) {
   if (e == cudaSuccess) e = cudaMalloc(&w->aff_labels, words * 4);
   if (e == cudaSuccess) e = cudaMalloc(&w->aff_vertices, words * 4);
   if (e == cudaSuccess) e = cudaMalloc(&w->err, 4);
+  if (e == cudaSuccess) e = cudaMalloc(&w->giant, 4);
   if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4);
   if (e != cudaSuccess) {
     mk_wcc_destroy(w);
@@ -351,9 +438,7 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d
     MK_CUDA(cudaMemsetAsync(w->aff_vertices, 0, words * 4, s));
     k_uf_mark<<<(n + 255) / 256, 256, 0, s>>>(d_src, g->applied.ptr, n, g->V, w->parent, w->aff_labels);
     k_uf_reset<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, w->aff_labels, w->aff_vertices);
-    MK_CHECK(wcc_edges(w, w->aff_vertices, s));
-    k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, w->aff_vertices);
-    MK_CUDA(cudaGetLastError());
+    MK_CHECK(wcc_link(w, w->aff_vertices, s));
   }
   return w->timer.stop(ms_out);
 }
@@ -382,6 +467,7 @@ mk_status mk_wcc_destroy(mk_wcc *w) {
   cudaFree(w->aff_labels);
   cudaFree(w->aff_vertices);
   cudaFree(w->err);
+  cudaFree(w->giant);
   w->ranges.release();
   delete w;
   return MK_OK;
