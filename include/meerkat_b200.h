@@ -179,7 +179,10 @@ typedef struct mk_tuning {
   uint32_t update_blocks_per_sm; /* resident blocks per SM, 0 = automatic     */
   uint32_t frontier_chunk;       /* buckets per BFS/SSSP frontier work item,
                                     1..1024, 0 = 4                            */
-  uint32_t reserved;
+  uint32_t sssp_delta;           /* static SSSP near-far step: relaxations to
+                                    distances >= threshold wait on a far list
+                                    until the near frontier drains; 0 = off
+                                    (plain level-synchronous)                  */
 } mk_tuning;
 mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t);
 mk_status mk_graph_get_tuning(mk_graph *g, mk_tuning *t);

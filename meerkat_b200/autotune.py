@@ -113,3 +113,20 @@ def tune_frontier_chunk(G, traversal, chunks: Sequence[int] = CHUNKS, repeats: i
     best = min(trials, key=lambda t: t["static_ms"])
     G.set_tuning(frontier_chunk=best["frontier_chunk"])
     return {"best": best["frontier_chunk"], "trials": trials}
+
+
+# static SSSP near-far steps (0 = plain level-synchronous)
+SSSP_DELTAS: Tuple[int, ...] = (0, 128, 512, 2048, 8192)
+
+
+def tune_sssp_delta(G, sssp, deltas: Sequence[int] = SSSP_DELTAS, repeats: int = 2) -> dict:
+    """Times sssp.Static() (idempotent) once per near-far step, keeps the
+    fastest on G.  Returns {"best": delta, "trials": [...]}."""
+    trials: List[dict] = []
+    for dl in deltas:
+        G.set_tuning(sssp_delta=dl)
+        t = min(sssp.Static() for _ in range(max(1, repeats)))
+        trials.append({"sssp_delta": int(dl), "static_ms": t})
+    best = min(trials, key=lambda t: t["static_ms"])
+    G.set_tuning(sssp_delta=best["sssp_delta"])
+    return {"best": best["sssp_delta"], "trials": trials}

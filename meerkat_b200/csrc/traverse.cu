@@ -47,12 +47,15 @@ enum Ctl : int {
   kBar0 = 0,      // barrier arrival
   kBar1 = 1,      // barrier generation
   kErr = 2,       // sticky error bits
+  kThr = 3,       // near-far SSSP: distance threshold of the near frontier
   kSz0 = 4,       // frontier sizes kSz0 + (level % 3)
   kInvCount = 8,  // invalidated vertices so far (append cursor of inv_list)
   kLevels = 9,    // relaxation levels run by the last call
   kDSz0 = 10,     // invalidation frontier sizes kDSz0 + (level % 3)
+  kFarN0 = 13,    // near-far SSSP: far list sizes kFarN0 + (list 0 / 1)
   kRound = 15,    // stamp base, persists across calls
-  kCtlWords = 16
+  kFarMin0 = 16,  // near-far SSSP: smallest distance on far list 0 / 1 (set in-kernel)
+  kCtlWords = 20
 };
 
 struct TravArgs {
@@ -72,6 +75,9 @@ struct TravArgs {
   uint32_t nsources;
   uint32_t chunk;           // buckets per frontier work item
   uint32_t mode;
+  uint32_t delta;           // near-far SSSP step (0: plain level-synchronous)
+  uint32_t *far0, *far1;    // far lists (vertex ids), one is appended at a time
+  uint32_t *fbits;          // bit per vertex: on a far list
   unsigned long long limit_ns;
 };
 
@@ -141,24 +147,52 @@ __device__ __forceinline__ unsigned long long ld_dist(const unsigned long long *
   return __ldcg(p);
 }
 
+// Near-far split of static SSSP: an improved vertex whose new distance is
+// below `thr` joins the next level; otherwise it goes (once) onto the far
+// list, which is drained when the near frontier runs dry.  thr = kNoFar
+// sends everything to the next level.
+constexpr uint32_t kNoFar = 0xFFFFFFFFu;
+struct NearFar {
+  uint32_t thr;
+  uint32_t *far;   // list being appended
+  uint32_t *farn;  // its size
+};
+
+__device__ __forceinline__ void far_push(const TravArgs &a, const NearFar &nf, uint32_t v) {
+  const uint32_t m = 1u << (v & 31);
+  if ((atomicOr(a.fbits + (v >> 5), m) & m) == 0) nf.far[atomicAdd(nf.farn, 1u)] = v;
+}
+
+// Pushes v, whose distance just improved to nd, to the next level or the far list.
+__device__ __forceinline__ void push_improved(const TravArgs &a, const BlockQueue &Q,
+                                              const NearFar &nf, uint32_t v,
+                                              unsigned long long nd, uint32_t stamp_next,
+                                              unsigned long long *gfr, uint32_t *gsz) {
+  if (nd < nf.thr) {
+    if (atomicExch(a.stamp + v, stamp_next) != stamp_next) push_vertex(a, Q, v, gfr, gsz);
+  } else {
+    far_push(a, nf, v);
+  }
+}
+
 // Relaxes v with candidate distance nd via parent u; pushes v on improvement.
-__device__ __forceinline__ void relax(const TravArgs &a, const BlockQueue &Q, uint32_t v,
-                                      unsigned long long nd, uint32_t u, uint32_t stamp_next,
-                                      unsigned long long *gfr, uint32_t *gsz) {
+__device__ __forceinline__ void relax(const TravArgs &a, const BlockQueue &Q, const NearFar &nf,
+                                      uint32_t v, unsigned long long nd, uint32_t u,
+                                      uint32_t stamp_next, unsigned long long *gfr,
+                                      uint32_t *gsz) {
   if (nd >= kInf) return;
   unsigned long long cur = ld_dist(a.dist + v);
   if (nd >= pack_hi(cur)) return;
   unsigned long long cand = pack((uint32_t)nd, u);
   unsigned long long old = atomicMin(a.dist + v, cand);
-  if (pack_hi(old) > nd) {
-    if (atomicExch(a.stamp + v, stamp_next) != stamp_next) push_vertex(a, Q, v, gfr, gsz);
-  }
+  if (pack_hi(old) > nd) push_improved(a, Q, nf, v, nd, stamp_next, gfr, gsz);
 }
 
 // Relaxes the live out-neighbours held by one slab quarter.
 template <bool kW, bool kUseW>
 __device__ __forceinline__ void relax_slab(const TravArgs &a, const Lanes &L,
-                                           const BlockQueue &Q, const uint4 &q, uint32_t u,
+                                           const BlockQueue &Q, const NearFar &nf,
+                                           const uint4 &q, uint32_t u,
                                            uint32_t du, uint32_t stamp_next,
                                            unsigned long long *gfr, uint32_t *gsz,
                                            bool only_invalid) {
@@ -170,7 +204,7 @@ __device__ __forceinline__ void relax_slab(const TravArgs &a, const Lanes &L,
     if (v < kTombKey && v != u) {
       if (only_invalid && !inval_test(a.inval, v)) continue;
       unsigned long long nd = (unsigned long long)du + (kUseW ? w[i] : 1u);
-      relax(a, Q, v, nd, u, stamp_next, gfr, gsz);
+      relax(a, Q, nf, v, nd, u, stamp_next, gfr, gsz);
     }
   }
 }
@@ -179,7 +213,8 @@ __device__ __forceinline__ void relax_slab(const TravArgs &a, const Lanes &L,
 // loaded before any is used, so a lane keeps up to 16 loads in flight.
 template <bool kW, bool kUseW>
 __device__ __forceinline__ void relax_slabs4(const TravArgs &a, const Lanes &L,
-                                             const BlockQueue &Q, const uint4 (&q)[4], uint32_t nq,
+                                             const BlockQueue &Q, const NearFar &nf,
+                                             const uint4 (&q)[4], uint32_t nq,
                                              uint32_t u, uint32_t du, uint32_t stamp_next,
                                              unsigned long long *gfr, uint32_t *gsz) {
   constexpr int KP = keys_per_lane<kW>();
@@ -205,8 +240,7 @@ __device__ __forceinline__ void relax_slabs4(const TravArgs &a, const Lanes &L,
       const unsigned long long nd = (unsigned long long)du + (kUseW ? w[j][i] : 1u);
       if (nd >= kInf || nd >= pack_hi(cur[j][i])) continue;
       const unsigned long long old = atomicMin(a.dist + v, pack((uint32_t)nd, u));
-      if (pack_hi(old) > nd && atomicExch(a.stamp + v, stamp_next) != stamp_next)
-        push_vertex(a, Q, v, gfr, gsz);
+      if (pack_hi(old) > nd) push_improved(a, Q, nf, v, nd, stamp_next, gfr, gsz);
     }
   }
 }
@@ -215,7 +249,8 @@ __device__ __forceinline__ void relax_slabs4(const TravArgs &a, const Lanes &L,
 // relaxation), overflow chains slab by slab.
 template <bool kW, bool kUseW>
 __device__ __forceinline__ void expand_range(const TravArgs &a, const Lanes &L,
-                                             const BlockQueue &Q, uint32_t u, uint32_t du,
+                                             const BlockQueue &Q, const NearFar &nf, uint32_t u,
+                                             uint32_t du,
                                              uint32_t b0, uint32_t b1, uint32_t stamp_next,
                                              unsigned long long *gfr, uint32_t *gsz) {
   for (uint32_t b = b0; b < b1; b += 4) {
@@ -225,13 +260,13 @@ __device__ __forceinline__ void expand_range(const TravArgs &a, const Lanes &L,
     for (int j = 0; j < 4; ++j)
       q[j] = ((uint32_t)j < nq) ? ld_slab_ro(a.g.slabs + 8ull * (b + j) + L.gl)
                                 : make_uint4(kEmptyKey, kEmptyKey, kEmptyKey, kNoSlab);
-    relax_slabs4<kW, kUseW>(a, L, Q, q, nq, u, du, stamp_next, gfr, gsz);
+    relax_slabs4<kW, kUseW>(a, L, Q, nf, q, nq, u, du, stamp_next, gfr, gsz);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       uint32_t s = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
       while (s != kNoSlab) {
         const uint4 r = ld_slab_ro(a.g.slabs + 8ull * s + L.gl);
-        relax_slab<kW, kUseW>(a, L, Q, r, u, du, stamp_next, gfr, gsz, false);
+        relax_slab<kW, kUseW>(a, L, Q, nf, r, u, du, stamp_next, gfr, gsz, false);
         s = __shfl_sync(L.gmask, r.w, L.gbase + 7);
       }
     }
@@ -271,6 +306,14 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   uint32_t *err = ctl + kErr;
   unsigned long long *fr[2] = {a.fr0, a.fr1};
   const uint32_t round = ld_acquire_u32(ctl + kRound);
+  const bool nearfar = kUseW && a.mode == kStatic && a.delta != 0 && a.far0 != nullptr;
+  const NearFar all_near{kNoFar, nullptr, nullptr};
+  uint32_t fb = 0;  // far list being appended
+  if (nearfar && tid == 0) {
+    ctl[kThr] = a.delta;
+    ctl[kFarMin0] = kNoFar;
+    ctl[kFarMin0 + 1] = kNoFar;
+  }
 
   // ---- seeding (level -1 pushes into fr[0] / sz[0]) ----
   if (a.mode == kStatic) {
@@ -305,7 +348,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       if (!present) continue;
       if (L.gl == 0) {
         unsigned long long nd = (unsigned long long)ds + (kUseW ? wv : 1u);
-        relax(a, Q, d, nd, s, round + 1, a.fr0, ctl + kSz0);
+        relax(a, Q, all_near, d, nd, s, round + 1, a.fr0, ctl + kSz0);
       }
     }
   } else {  // kDecremental
@@ -368,7 +411,8 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
         pu = __shfl_sync(L.gmask, pu, L.gbase);
         if (pu == kInfInf) continue;
         walk_bucket(a.g, L, b, [&](const uint4 &q) {
-          relax_slab<kW, kUseW>(a, L, Q, q, u, pack_hi(pu), round + 1, a.fr0, ctl + kSz0, true);
+          relax_slab<kW, kUseW>(a, L, Q, all_near, q, u, pack_hi(pu), round + 1, a.fr0, ctl + kSz0,
+                                true);
         });
       }
     }
@@ -377,23 +421,61 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
 
   // ---- relaxation levels ----
+  // A level expands the frontier; with near-far SSSP, a level whose frontier
+  // is empty instead drains the far list: the threshold moves to the far
+  // list's smallest distance plus delta, vertices below it join the next
+  // level and the rest move to the other far list.
   uint32_t lv = 0;
   for (;; ++lv) {
     const uint32_t n = ld_acquire_u32(ctl + kSz0 + (lv % 3));
-    if (n == 0) break;
+    uint32_t nfar = 0;
+    if (n == 0) {
+      if (!nearfar) break;
+      nfar = ld_acquire_u32(ctl + kFarN0 + fb);
+      if (nfar == 0) break;
+    }
     if (tid == 0) ctl[kSz0 + ((lv + 2) % 3)] = 0;
     const unsigned long long *cur = fr[lv & 1];
     unsigned long long *nxt = fr[(lv + 1) & 1];
     uint32_t *nsz = ctl + kSz0 + ((lv + 1) % 3);
     const uint32_t stamp_next = round + 2 + lv;
-    for (uint32_t i = group; i < n; i += ngroups) {
-      uint32_t u, b0, b1;
-      item_range(a.g, __ldcg(cur + i), a.chunk, u, b0, b1);
-      unsigned long long pu = 0;
-      if (L.gl == 0) pu = ld_dist(a.dist + u);
-      pu = __shfl_sync(L.gmask, pu, L.gbase);
-      if (pu == kInfInf) continue;
-      expand_range<kW, kUseW>(a, L, Q, u, pack_hi(pu), b0, b1, stamp_next, nxt, nsz);
+    const uint32_t thr = nearfar ? ld_acquire_u32(ctl + kThr) : kNoFar;
+    if (n) {
+      const NearFar nf = nearfar ? NearFar{thr, fb ? a.far1 : a.far0, ctl + kFarN0 + fb} : all_near;
+      for (uint32_t i = group; i < n; i += ngroups) {
+        uint32_t u, b0, b1;
+        item_range(a.g, __ldcg(cur + i), a.chunk, u, b0, b1);
+        unsigned long long pu = 0;
+        if (L.gl == 0) pu = ld_dist(a.dist + u);
+        pu = __shfl_sync(L.gmask, pu, L.gbase);
+        if (pu == kInfInf) continue;
+        expand_range<kW, kUseW>(a, L, Q, nf, u, pack_hi(pu), b0, b1, stamp_next, nxt, nsz);
+      }
+    } else {
+      const uint32_t *fc = fb ? a.far1 : a.far0;
+      uint32_t *fo = fb ? a.far0 : a.far1;
+      for (uint32_t i = tid; i < nfar; i += nthreads)
+        atomicMin(ctl + kFarMin0 + fb, pack_hi(ld_dist(a.dist + __ldcg(fc + i))));
+      if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+      const uint32_t lo = max(thr, ld_acquire_u32(ctl + kFarMin0 + fb));
+      const uint32_t nthr = lo > kNoFar - a.delta ? kNoFar : lo + a.delta;
+      for (uint32_t i = tid; i < nfar; i += nthreads) {
+        const uint32_t v = __ldcg(fc + i);
+        const uint32_t d = pack_hi(ld_dist(a.dist + v));
+        if (d < nthr) {
+          atomicAnd(a.fbits + (v >> 5), ~(1u << (v & 31)));
+          if (atomicExch(a.stamp + v, stamp_next) != stamp_next) push_vertex(a, Q, v, nxt, nsz);
+        } else {
+          fo[atomicAdd(ctl + kFarN0 + (fb ^ 1u), 1u)] = v;
+        }
+      }
+      if (tid == 0) {
+        ctl[kThr] = nthr;
+        ctl[kFarN0 + fb] = 0;
+        // the other list's minimum is read by the next drain, not this one
+        ctl[kFarMin0 + (fb ^ 1u)] = kNoFar;
+      }
+      fb ^= 1u;
     }
     queue_flush(Q, nxt, nsz, a.pushed, &base_s);
     if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
@@ -429,6 +511,7 @@ struct mk_traversal {
   uint32_t *inv_list = nullptr;
   uint32_t *ctl = nullptr;
   unsigned long long *pushed = nullptr;
+  uint32_t *far0 = nullptr, *far1 = nullptr, *fbits = nullptr;  // near-far SSSP
   Timer timer;
 };
 
@@ -478,6 +561,11 @@ static mk_status trav_create(mk_graph *g, const uint32_t *h_sources, uint32_t ns
   A((void **)&t->ctl, kCtlWords * 4);
   A((void **)&t->pushed, 8);
   A((void **)&t->sources, (size_t)nsrc * 4);
+  if (sssp) {  // far lists: a vertex is on at most one of them at a time
+    A((void **)&t->far0, V * 4 + 16);
+    A((void **)&t->far1, V * 4 + 16);
+    A((void **)&t->fbits, (V + 31) / 32 * 4);
+  }
   if (e == cudaSuccess)
     e = cudaMemcpy(t->sources, h_sources, (size_t)nsrc * 4, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(t->dist, 0xFF, V * 8);
@@ -511,6 +599,8 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   if (n && (!bs || !bd)) return fail(MK_ERR_INVALID, "traversal: null batch");
   MK_CHECK(t->timer.start(s, ms_out != nullptr));
   if (mode == kStatic) MK_CUDA(cudaMemsetAsync(t->dist, 0xFF, (size_t)g->V * 8, s));
+  const uint32_t delta = (t->sssp && mode == kStatic && t->far0) ? g->tuning.sssp_delta : 0u;
+  if (delta) MK_CUDA(cudaMemsetAsync(t->fbits, 0, ((size_t)g->V + 31) / 32 * 4, s));
   // clear everything but the persistent round counter
   MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
   MK_CUDA(cudaMemsetAsync(t->pushed, 0, 8, s));
@@ -530,6 +620,10 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   a.sources = t->sources;
   a.nsources = t->nsources;
   a.chunk = g->tuning.frontier_chunk ? g->tuning.frontier_chunk : kDefaultChunk;
+  a.delta = delta;
+  a.far0 = t->far0;
+  a.far1 = t->far1;
+  a.fbits = t->fbits;
   a.mode = mode;
   a.limit_ns = 4000000000ull;
   const void *fn;
@@ -660,6 +754,9 @@ mk_status mk_traversal_destroy(mk_traversal *t) {
   cudaFree(t->ctl);
   cudaFree(t->pushed);
   cudaFree(t->sources);
+  cudaFree(t->far0);
+  cudaFree(t->far1);
+  cudaFree(t->fbits);
   delete t;
   return MK_OK;
 }

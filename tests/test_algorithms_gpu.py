@@ -298,3 +298,29 @@ def test_wcc_labels_are_roots_on_deep_trees():
     for _ in range(8):
         wcc.Static()
         np.testing.assert_array_equal(wcc.Labels(), want)
+
+
+@pytest.mark.parametrize("delta", [1, 50, 700, 100000])
+def test_sssp_near_far_static_matches_oracle(delta):
+    """Static SSSP with the near-far split (sssp_delta) on a skewed graph and
+    a high-diameter grid: same distances as the oracle, valid parents, and
+    the dynamic calls that follow still agree."""
+    for V, (s, d, w) in ((1 << 13, mk.gen_rmat(13, 90000, seed=23, w_lo=1, w_hi=1000)),
+                         (64 * 64, mk.gen_grid(64, 100, seed=8, w_lo=1, w_hi=1000))):
+        G, O = make_pair(V, s, d, w, weighted=True)
+        G.set_tuning(sssp_delta=delta)
+        src = int(np.argmax(np.bincount(s, minlength=V)))
+        sssp = mk.SSSP(G, src, V)
+        sssp.Static()
+        np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
+        assert O.check_parents(src, sssp.packed(), weighted=True) == 0
+        es = mk.EdgeSet(V, s, d)
+        ds, dd = es.sample_present(len(s) // 10, seed=delta % 97)
+        tds, tdd = to_dev(ds), to_dev(dd)
+        G.DeleteEdges(tds, tdd)
+        O.delete(ds, dd)
+        sssp.Decremental(tds, tdd)
+        np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
+        sssp.Static()  # near-far again on the changed graph
+        np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
+        assert O.check_parents(src, sssp.packed(), weighted=True) == 0
