@@ -629,6 +629,110 @@ def run_serving(args, rank, world, local):
     return 0
 
 
+def grid_stress(side, nbatch, batch, rank, world, local):
+    """High-diameter decremental stress: side x side 4-neighbour grid, both
+    directions, plus 1% random long-range shortcut edges, weights U[1,1000].
+    nbatch delete-only batches of `batch` edges, 80% drawn from the current
+    SSSP tree and 20% from the generated edges, then nbatch insert batches of
+    `batch` random local edges (Chebyshev radius <= 2).  After each batch:
+    decremental / incremental BFS, SSSP (from the centre) and WCC, ms each.
+    At the end the maintained BFS levels, SSSP distances and WCC labels must
+    equal a fresh static recompute on the final graph."""
+    import torch
+
+    import meerkat_b200 as mk
+    dev = torch.device(f"cuda:{local}")
+    V = side * side
+    grid_edges = 4 * side * (side - 1)
+    t0 = time.time()
+    s, d, w = mk.gen_grid(side, grid_edges // 100, seed=SEED + 21 + rank, w_lo=1, w_hi=1000)
+    E = len(s)
+
+    def todev(a):
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).to(dev)
+
+    G = mk.DynamicGraph(V, degree_hints=np.bincount(s, minlength=V).astype(np.uint32),
+                        weighted=True, device=local)
+    G.InsertEdges(todev(s), todev(d), vals=todev(w))
+    assert G.sync() == 0
+    log(f"[grid] {side}x{side}: {V} vertices, {E} edges in {time.time() - t0:.1f}s")
+    src = (side // 2) * side + side // 2
+    bfs, sssp, wcc = mk.BFS(G, src, V), mk.SSSP(G, src, V), mk.WCC(G)
+    from meerkat_b200.autotune import tune_sssp_delta
+    nf = tune_sssp_delta(G, sssp, deltas=(0, 4096, 16384, 65536))
+    # deletes aimed at the SSSP tree cut off large subtrees: recompute from the
+    # centre once 0.5% of the vertices are invalidated instead of repairing
+    G.set_tuning(recompute_permille=5)
+    static = {"bfs_ms": min(bfs.Static() for _ in range(2)),
+              "sssp_ms": min(sssp.Static() for _ in range(2)),
+              "wcc_ms": min(wcc.Static() for _ in range(2))}
+    static["bfs_levels"], _ = bfs.stats()
+    static["sssp_levels"], _ = sssp.stats()
+    rng = np.random.default_rng(SEED + 22 + rank)
+    rec = {k: [] for k in ("update_ms", "bfs_ms", "sssp_ms", "wcc_ms")}
+    dec, inc = {k: [] for k in rec}, {k: [] for k in rec}
+    INFINF = np.uint64(2**64 - 1)
+    for b in range(nbatch):
+        packed = sssp.packed()
+        par = (packed & np.uint64(0xFFFFFFFF)).astype(np.int64)
+        tree = np.flatnonzero((packed != INFINF) & (par != np.arange(V)))
+        nt = min(len(tree), int(0.8 * batch))
+        pick = rng.choice(tree, size=nt, replace=False)
+        ridx = rng.integers(0, E, batch - nt)
+        ds = np.concatenate([par[pick], s[ridx]]).astype(np.uint32)
+        dd = np.concatenate([pick, d[ridx]]).astype(np.uint32)
+        tds, tdd = todev(ds), todev(dd)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        G.DeleteEdges(tds, tdd)
+        e1.record()
+        e1.synchronize()
+        dec["update_ms"].append(e0.elapsed_time(e1))
+        dec["bfs_ms"].append(bfs.Decremental(tds, tdd))
+        dec["sssp_ms"].append(sssp.Decremental(tds, tdd))
+        dec["wcc_ms"].append(wcc.Decremental(tds, tdd))
+    for b in range(nbatch):
+        u = rng.integers(0, V, batch)
+        dx = rng.integers(-2, 3, batch)
+        dy = rng.integers(-2, 3, batch)
+        r, c = u // side + dy, u % side + dx
+        ok = (r >= 0) & (r < side) & (c >= 0) & (c < side) & ((dx != 0) | (dy != 0))
+        r, c, u = np.where(ok, r, u // side), np.where(ok, c, u % side), u
+        v = (r * side + c).astype(np.uint32)
+        tis, tid, tiw = todev(u), todev(v), todev(rng.integers(1, 1001, batch))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        G.InsertEdges(tis, tid, vals=tiw)
+        e1.record()
+        e1.synchronize()
+        inc["update_ms"].append(e0.elapsed_time(e1))
+        inc["bfs_ms"].append(bfs.Incremental(tis, tid))
+        inc["sssp_ms"].append(sssp.Incremental(tis, tid, wgt=tiw))
+        inc["wcc_ms"].append(wcc.Incremental(tis, tid))
+    assert G.sync() == 0
+    # full-size check: the maintained answers equal a fresh recompute
+    got = (bfs.Distances(), sssp.Distances(), wcc.Labels())
+    fb, fs, fw = mk.BFS(G, src, V), mk.SSSP(G, src, V), mk.WCC(G)
+    fb.Static(), fs.Static(), fw.Static()
+    same = {"bfs": bool(np.array_equal(got[0], fb.Distances())),
+            "sssp": bool(np.array_equal(got[1], fs.Distances())),
+            "wcc": bool(np.array_equal(got[2], fw.Labels()))}
+    comps = int(len(np.unique(got[2])))
+    for o in (fb, fs, fw, bfs, sssp, wcc):
+        o.close()
+    G.close()
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    assert all(same.values()), same
+    p50 = lambda xs: statistics.median(xs) if xs else None
+    return {"workload": f"grid{side}_decremental_stress", "vertices": V, "edges": E,
+            "tuning": {"sssp_delta": nf["best"], "recompute_permille": 5},
+            "batches": nbatch, "batch": batch, "source": src, "static": static,
+            "decremental_p50_ms": {k: p50(v) for k, v in dec.items()},
+            "incremental_p50_ms": {k: p50(v) for k, v in inc.items()},
+            "components_after": comps, "matches_static_recompute": same}
+
+
 def run_batched(args, rank, world, local):
     import torch
     from meerkat_b200.build import build
@@ -687,6 +791,9 @@ def main():
                     help="updates workload: offered rates of the serving comparison attached to "
                          "the line ('' = skip)")
     ap.add_argument("--serving-in-line-requests", type=int, default=150)
+    ap.add_argument("--grid-side", type=int, default=4096,
+                    help="updates workload: side of the grid decremental stress run attached to "
+                         "the line (0 = skip)")
     args = ap.parse_args()
     if args.workload == "serving":
         rank, world, local = dist_setup(args.gpus)
@@ -913,6 +1020,9 @@ def main():
             "plain_ms_per_step", "plain_cuda_graph_ms_per_step", "batched_updates_per_s",
             "updates_per_step", "vertices", "edges", "gpu_launches_per_step",
             "plain_launches_per_step", "queries", "tuning", "equality", "clocks", "steps")}
+    grid = None
+    if args.grid_side > 0:
+        grid = grid_stress(args.grid_side, 10, 500_000, rank, world, local)
     serving = None
     if args.serving_in_line:
         rates = [float(x) for x in args.serving_in_line.split(",")]
@@ -962,6 +1072,8 @@ def main():
             line["batched"] = batched
         if serving is not None:
             line["serving"] = serving
+        if grid is not None:
+            line["grid"] = grid
         print(json.dumps(line), flush=True)
     barrier(world)
     if world > 1:

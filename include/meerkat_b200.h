@@ -183,6 +183,11 @@ typedef struct mk_tuning {
                                     distances >= threshold wait on a far list
                                     until the near frontier drains; 0 = off
                                     (plain level-synchronous)                  */
+  uint32_t recompute_permille;   /* decremental BFS/SSSP: once this share of
+                                    the vertices (per mille) is invalidated,
+                                    recompute from the sources instead of
+                                    repairing; 0 = never                       */
+  uint32_t reserved[3];
 } mk_tuning;
 mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t);
 mk_status mk_graph_get_tuning(mk_graph *g, mk_tuning *t);

@@ -141,22 +141,25 @@ class DynamicGraph:
     def set_tuning(self, update_kernel: Optional[int] = None,
                    update_blocks_per_sm: Optional[int] = None,
                    frontier_chunk: Optional[int] = None,
-                   sssp_delta: Optional[int] = None) -> None:
+                   sssp_delta: Optional[int] = None,
+                   recompute_permille: Optional[int] = None) -> None:
         """Sets the given kernel knobs; the others keep their values."""
         cur = self.get_tuning()
         for k, v in (("update_kernel", update_kernel), ("update_blocks_per_sm", update_blocks_per_sm),
-                     ("frontier_chunk", frontier_chunk), ("sssp_delta", sssp_delta)):
+                     ("frontier_chunk", frontier_chunk), ("sssp_delta", sssp_delta),
+                     ("recompute_permille", recompute_permille)):
             if v is not None:
                 cur[k] = int(v)
         t = Tuning(cur["update_kernel"], cur["update_blocks_per_sm"], cur["frontier_chunk"],
-                   cur["sssp_delta"])
+                   cur["sssp_delta"], cur["recompute_permille"])
         check(lib().mk_graph_set_tuning(self._h, C.byref(t)), "mk_graph_set_tuning")
 
     def get_tuning(self) -> dict:
         t = Tuning()
         check(lib().mk_graph_get_tuning(self._h, C.byref(t)), "mk_graph_get_tuning")
         return {"update_kernel": t.update_kernel, "update_blocks_per_sm": t.update_blocks_per_sm,
-                "frontier_chunk": t.frontier_chunk, "sssp_delta": t.sssp_delta}
+                "frontier_chunk": t.frontier_chunk, "sssp_delta": t.sssp_delta,
+                "recompute_permille": t.recompute_permille}
 
     def reserve_batch(self, n: int) -> None:
         check(lib().mk_graph_reserve_batch(self._h, int(n)), "mk_graph_reserve_batch")

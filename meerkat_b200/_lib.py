@@ -34,7 +34,8 @@ class GraphInfo(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("update_kernel", C.c_uint32), ("update_blocks_per_sm", C.c_uint32),
-                ("frontier_chunk", C.c_uint32), ("sssp_delta", C.c_uint32)]
+                ("frontier_chunk", C.c_uint32), ("sssp_delta", C.c_uint32),
+                ("recompute_permille", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 # (name, restype, argtypes); every function returns mk_status unless noted

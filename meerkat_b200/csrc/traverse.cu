@@ -76,6 +76,7 @@ struct TravArgs {
   uint32_t chunk;           // buckets per frontier work item
   uint32_t mode;
   uint32_t delta;           // near-far SSSP step (0: plain level-synchronous)
+  uint32_t recompute_inv;   // decremental: invalidated vertices from which to recompute (0: never)
   uint32_t *far0, *far1;    // far lists (vertex ids), one is appended at a time
   uint32_t *fbits;          // bit per vertex: on a far list
   unsigned long long limit_ns;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   uint32_t *err = ctl + kErr;
   unsigned long long *fr[2] = {a.fr0, a.fr1};
   const uint32_t round = ld_acquire_u32(ctl + kRound);
-  const bool nearfar = kUseW && a.mode == kStatic && a.delta != 0 && a.far0 != nullptr;
+  bool nearfar = kUseW && a.mode == kStatic && a.delta != 0 && a.far0 != nullptr;
   const NearFar all_near{kNoFar, nullptr, nullptr};
   uint32_t fb = 0;  // far list being appended
   if (nearfar && tid == 0) {
@@ -373,9 +374,18 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
     // D2: invalidate whole subtrees along tree edges, level by level.  Sizes
     // rotate over three counters so no block reads a counter that another
     // block is already filling for the next level.
+    // The running total of the level sizes (each read after a barrier, the
+    // same in every thread) stops the walk early once a recompute is due.
+    uint64_t walked = 0;
+    bool restart = false;
     for (uint32_t dl = 0;; ++dl) {
       const uint32_t n = ld_acquire_u32(ctl + kDSz0 + (dl % 3));
       if (n == 0) break;
+      walked += n;
+      if (a.recompute_inv && walked >= a.recompute_inv) {
+        restart = true;
+        break;
+      }
       if (tid == 0) ctl[kDSz0 + ((dl + 2) % 3)] = 0;
       const unsigned long long *cur = fr[dl & 1];
       unsigned long long *nxt = fr[(dl + 1) & 1];
@@ -400,9 +410,31 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
     }
     const uint32_t hi = ld_acquire_u32(ctl + kInvCount);
-    // D3: re-seed invalidated vertices from valid in-neighbours: one sweep
-    // over all buckets (balanced by construction)
-    if (hi > 0) {
+    if (restart) {
+      // Most of the tree is gone: a recompute from the sources costs less
+      // than re-seeding and repairing this many vertices.  The invalidation
+      // bits are cleared in the epilogue as usual.
+      for (uint32_t v = tid; v < a.g.V; v += nthreads) a.dist[v] = kInfInf;
+      if (tid == 0) {
+        ctl[kThr] = a.delta;
+        ctl[kFarMin0] = kNoFar;
+        ctl[kFarMin0 + 1] = kNoFar;
+      }
+      if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+      for (uint32_t i = tid; i < a.nsources; i += nthreads) {
+        const uint32_t src = a.sources[i];
+        a.dist[src] = pack(0, src);
+        a.stamp[src] = round + 1;
+        const uint32_t nb = a.g.boff[src + 1] - a.g.boff[src];
+        const uint32_t k = max(1u, (nb + a.chunk - 1) / a.chunk);
+        const uint32_t base = atomicAdd(ctl + kSz0, k);
+        for (uint32_t j = 0; j < k; ++j) a.fr0[base + j] = item(src, j);
+        atomicAdd(a.pushed, 1ull);
+      }
+      nearfar = kUseW && a.delta != 0 && a.far0 != nullptr;
+    } else if (hi > 0) {
+      // D3: re-seed invalidated vertices from valid in-neighbours: one sweep
+      // over all buckets (balanced by construction)
       for (uint32_t b = group; b < a.g.nbuckets; b += ngroups) {
         const uint32_t u = a.g.bowner[b];
         if (a.g.deg[u] == 0 || inval_test(a.inval, u)) continue;
@@ -599,7 +631,7 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   if (n && (!bs || !bd)) return fail(MK_ERR_INVALID, "traversal: null batch");
   MK_CHECK(t->timer.start(s, ms_out != nullptr));
   if (mode == kStatic) MK_CUDA(cudaMemsetAsync(t->dist, 0xFF, (size_t)g->V * 8, s));
-  const uint32_t delta = (t->sssp && mode == kStatic && t->far0) ? g->tuning.sssp_delta : 0u;
+  const uint32_t delta = (t->sssp && mode != kIncremental && t->far0) ? g->tuning.sssp_delta : 0u;
   if (delta) MK_CUDA(cudaMemsetAsync(t->fbits, 0, ((size_t)g->V + 31) / 32 * 4, s));
   // clear everything but the persistent round counter
   MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
@@ -621,6 +653,9 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   a.nsources = t->nsources;
   a.chunk = g->tuning.frontier_chunk ? g->tuning.frontier_chunk : kDefaultChunk;
   a.delta = delta;
+  a.recompute_inv = g->tuning.recompute_permille
+                        ? (uint32_t)std::max<uint64_t>(1, (uint64_t)g->V * g->tuning.recompute_permille / 1000)
+                        : 0u;
   a.far0 = t->far0;
   a.far1 = t->far1;
   a.fbits = t->fbits;

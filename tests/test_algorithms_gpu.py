@@ -89,8 +89,10 @@ def test_golden_fixture_through_the_abi(gold):
     check("del_")
 
 
-def _traversal_rounds(V, s, d, w, rounds, batch, seed, hints="exact"):
+def _traversal_rounds(V, s, d, w, rounds, batch, seed, hints="exact", tuning=None):
     G, O = make_pair(V, s, d, w, weighted=True, hints=hints)
+    if tuning:
+        G.set_tuning(**tuning)
     es = mk.EdgeSet(V, s, d)
     src = int(np.argmax(np.bincount(s, minlength=V)))
     bfs, sssp = mk.BFS(G, src, V), mk.SSSP(G, src, V)
@@ -324,3 +326,18 @@ def test_sssp_near_far_static_matches_oracle(delta):
         sssp.Static()  # near-far again on the changed graph
         np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
         assert O.check_parents(src, sssp.packed(), weighted=True) == 0
+
+
+@pytest.mark.parametrize("tuning", [{"recompute_permille": 0},
+                                    {"recompute_permille": 1},
+                                    {"recompute_permille": 1, "sssp_delta": 300}])
+def test_decremental_recompute_fallback(tuning):
+    """Decremental BFS/SSSP either repair the invalidated subtrees or, past the
+    recompute threshold, recompute from the source (with or without the
+    near-far split): the answers are the oracle's either way."""
+    side = 48
+    s, d, w = mk.gen_grid(side, 60, seed=12, w_lo=1, w_hi=1000)
+    _traversal_rounds(side * side, s, d, w, rounds=3, batch=500, seed=13, tuning=tuning)
+    V = 1 << 12
+    s, d, w = mk.gen_rmat(12, 40000, seed=14, w_lo=1, w_hi=1000)
+    _traversal_rounds(V, s, d, w, rounds=2, batch=1500, seed=15, tuning=tuning)
