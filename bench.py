@@ -234,6 +234,20 @@ def more_queries(mk, G, V, dev, seed):
     indeg = torch.bincount(col.long(), minlength=V).to(torch.int32).cpu().numpy().view(np.uint32)
     Gr = mk.DynamicGraph(V, degree_hints=indeg, reverse=True, device=dev.index or 0)
     Gr.InsertEdges(rows, col)
+    # direction-optimizing static BFS: the reverse copy lets large levels pull
+    from meerkat_b200.autotune import tune_bfs_pull
+    src_bfs = int(torch.argmax(rp[1:] - rp[:-1]))
+    bfs_push = mk.BFS(G, src_bfs, V)
+    t_push = min(bfs_push.Static() for _ in range(2))
+    bfs_pull = mk.BFS(G, src_bfs, V)
+    bfs_pull.set_reverse(Gr)
+    pull = tune_bfs_pull(G, bfs_pull)
+    same = bool(np.array_equal(bfs_push.Distances(), bfs_pull.Distances()))
+    out["bfs_pull"] = {"push_only_ms": t_push, "best_ms": min(x["static_ms"] for x in pull["trials"]),
+                       "pull_permille": pull["best"], "trials": pull["trials"], "same_levels": same}
+    bfs_push.close()
+    bfs_pull.close()
+    G.set_tuning(pull_permille=0)
     pr = mk.PageRank(Gr, 0.85, 1e-6, V, max_iter=200)
     t = pr.Static()
     it, _ = pr.stats()
@@ -277,7 +291,8 @@ def more_queries(mk, G, V, dev, seed):
     torch.cuda.empty_cache()
     peak = measured_peak()[0]
     for k in out:
-        out[k]["static_frac"] = out[k]["static_gbs"] / peak
+        if "static_gbs" in out[k]:
+            out[k]["static_frac"] = out[k]["static_gbs"] / peak
     return out
 
 

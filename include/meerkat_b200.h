@@ -187,7 +187,11 @@ typedef struct mk_tuning {
                                     the vertices (per mille) is invalidated,
                                     recompute from the sources instead of
                                     repairing; 0 = never                       */
-  uint32_t reserved[3];
+  uint32_t pull_permille;        /* static BFS with a reverse graph attached
+                                    (mk_traversal_set_reverse): a level whose
+                                    frontier holds this share of the vertices
+                                    (per mille) is pulled bottom-up; 0 = never */
+  uint32_t reserved[2];
 } mk_tuning;
 mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t);
 mk_status mk_graph_get_tuning(mk_graph *g, mk_tuning *t);
@@ -219,6 +223,11 @@ mk_status mk_sssp_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t 
  * one multi-source query per round with one resident traversal.  No
  * counterpart in the reference. */
 mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, uint32_t n);
+/* Attaches the reverse graph (in-edges) of the same edge set to a BFS, for
+ * pull levels of static calls (tuning.pull_permille); the caller keeps both
+ * graphs updated with the same batches.  NULL detaches.  No counterpart in
+ * the reference. */
+mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev);
 /* float Static(EdgesN) (BFSImpl.cuh:590-662, SSSPImpl.cuh:607-690). */
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out);
 /* float Incremental(src*, dst*, n) (BFSImpl.cuh:664-753, SSSPImpl.cuh:692-785).

@@ -142,16 +142,17 @@ class DynamicGraph:
                    update_blocks_per_sm: Optional[int] = None,
                    frontier_chunk: Optional[int] = None,
                    sssp_delta: Optional[int] = None,
-                   recompute_permille: Optional[int] = None) -> None:
+                   recompute_permille: Optional[int] = None,
+                   pull_permille: Optional[int] = None) -> None:
         """Sets the given kernel knobs; the others keep their values."""
         cur = self.get_tuning()
         for k, v in (("update_kernel", update_kernel), ("update_blocks_per_sm", update_blocks_per_sm),
                      ("frontier_chunk", frontier_chunk), ("sssp_delta", sssp_delta),
-                     ("recompute_permille", recompute_permille)):
+                     ("recompute_permille", recompute_permille), ("pull_permille", pull_permille)):
             if v is not None:
                 cur[k] = int(v)
         t = Tuning(cur["update_kernel"], cur["update_blocks_per_sm"], cur["frontier_chunk"],
-                   cur["sssp_delta"], cur["recompute_permille"])
+                   cur["sssp_delta"], cur["recompute_permille"], cur["pull_permille"])
         check(lib().mk_graph_set_tuning(self._h, C.byref(t)), "mk_graph_set_tuning")
 
     def get_tuning(self) -> dict:
@@ -159,7 +160,7 @@ class DynamicGraph:
         check(lib().mk_graph_get_tuning(self._h, C.byref(t)), "mk_graph_get_tuning")
         return {"update_kernel": t.update_kernel, "update_blocks_per_sm": t.update_blocks_per_sm,
                 "frontier_chunk": t.frontier_chunk, "sssp_delta": t.sssp_delta,
-                "recompute_permille": t.recompute_permille}
+                "recompute_permille": t.recompute_permille, "pull_permille": t.pull_permille}
 
     def reserve_batch(self, n: int) -> None:
         check(lib().mk_graph_reserve_batch(self._h, int(n)), "mk_graph_reserve_batch")
@@ -297,6 +298,12 @@ class _Traversal(_Timed):
         self.source = self.sources
         check(lib().mk_traversal_set_sources(self._h, self.sources.ctypes.data_as(
             C.POINTER(C.c_uint32)), len(self.sources)), "mk_traversal_set_sources")
+
+    def set_reverse(self, G_rev: Optional[DynamicGraph]) -> None:
+        """Attaches the reverse graph of the same edges (BFS pull levels)."""
+        self._rev = G_rev
+        check(lib().mk_traversal_set_reverse(self._h, G_rev.handle if G_rev is not None else None),
+              "mk_traversal_set_reverse")
 
     def Static(self, edges_n=None, stream=None, timed=True):
         return self._call(lib().mk_traversal_static, self._h, _stream(stream), timed=timed)

@@ -35,7 +35,8 @@ class GraphInfo(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("update_kernel", C.c_uint32), ("update_blocks_per_sm", C.c_uint32),
                 ("frontier_chunk", C.c_uint32), ("sssp_delta", C.c_uint32),
-                ("recompute_permille", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("recompute_permille", C.c_uint32), ("pull_permille", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 # (name, restype, argtypes); every function returns mk_status unless noted
@@ -68,6 +69,7 @@ SIGNATURES = [
     ("mk_bfs_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
     ("mk_sssp_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
     ("mk_traversal_set_sources", _S, [vp, u32p, C.c_uint32]),
+    ("mk_traversal_set_reverse", _S, [vp, vp]),
     ("mk_traversal_static", _S, [vp, vp, f32p]),
     ("mk_traversal_incremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_traversal_decremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),

@@ -130,3 +130,20 @@ def tune_sssp_delta(G, sssp, deltas: Sequence[int] = SSSP_DELTAS, repeats: int =
     best = min(trials, key=lambda t: t["static_ms"])
     G.set_tuning(sssp_delta=best["sssp_delta"])
     return {"best": best["sssp_delta"], "trials": trials}
+
+
+# static BFS pull thresholds, per mille of the vertices (0 = never pull)
+PULL_PERMILLE: Tuple[int, ...] = (0, 5, 20, 50, 150)
+
+
+def tune_bfs_pull(G, bfs, perms: Sequence[int] = PULL_PERMILLE, repeats: int = 2) -> dict:
+    """Times bfs.Static() (a BFS with a reverse graph attached) once per pull
+    threshold, keeps the fastest on G.  Returns {"best": ..., "trials": [...]}."""
+    trials: List[dict] = []
+    for pm in perms:
+        G.set_tuning(pull_permille=pm)
+        t = min(bfs.Static() for _ in range(max(1, repeats)))
+        trials.append({"pull_permille": int(pm), "static_ms": t})
+    best = min(trials, key=lambda t: t["static_ms"])
+    G.set_tuning(pull_permille=best["pull_permille"])
+    return {"best": best["pull_permille"], "trials": trials}

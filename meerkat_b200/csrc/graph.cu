@@ -1252,6 +1252,7 @@ mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t) {
   if (t->update_blocks_per_sm > 32) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: update_blocks_per_sm > 32");
   if (t->frontier_chunk > 1024) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: frontier_chunk > 1024");
   if (t->recompute_permille > 1000) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: recompute_permille > 1000");
+  if (t->pull_permille > 1000) return fail(MK_ERR_INVALID, "mk_graph_set_tuning: pull_permille > 1000");
   g->tuning = *t;
   return MK_OK;
 }

@@ -122,7 +122,7 @@ struct mk_graph {
   const uint32_t *last_dst = nullptr;
   int last_op = 0;  // 1 insert, 2 delete
   size_t device_bytes = 0;
-  mk_tuning tuning = {0u, 0u, 0u, 0u, 100u, {0u, 0u, 0u}};
+  mk_tuning tuning = {0u, 0u, 0u, 0u, 100u, 0u, {0u, 0u}};
 
   mk::GraphView view() const {
     mk::GraphView v;

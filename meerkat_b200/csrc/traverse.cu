@@ -77,6 +77,8 @@ struct TravArgs {
   uint32_t mode;
   uint32_t delta;           // near-far SSSP step (0: plain level-synchronous)
   uint32_t recompute_inv;   // decremental: invalidated vertices from which to recompute (0: never)
+  GraphView rg;             // in-edges of the same graph (static BFS pull levels), rg.V == 0: none
+  uint32_t pull_items;      // static BFS: frontier size from which a level is pulled (0: never)
   uint32_t *far0, *far1;    // far lists (vertex ids), one is appended at a time
   uint32_t *fbits;          // bit per vertex: on a far list
   unsigned long long limit_ns;
@@ -290,6 +292,49 @@ __device__ __forceinline__ bool is_source(unsigned long long p, uint32_t v) {
   return p == pack(0, v);
 }
 
+// Bottom-up BFS level: every unvisited vertex walks its in-edges (in the
+// reverse graph) until it meets a vertex on level lvl; it then takes level
+// lvl + 1 with that parent and joins the next frontier.  One 8-lane group per
+// vertex, stopping at the first slab that holds a parent.
+template <bool kRW>
+__device__ __forceinline__ void pull_level(const TravArgs &a, const Lanes &L, const BlockQueue &Q,
+                                           uint32_t group, uint32_t ngroups, uint32_t lvl,
+                                           uint32_t stamp_next, unsigned long long *nxt,
+                                           uint32_t *nsz) {
+  const GraphView &rg = a.rg;
+  for (uint32_t v = group; v < rg.V; v += ngroups) {
+    unsigned long long pv = 0;
+    if (L.gl == 0) pv = ld_dist(a.dist + v);
+    pv = __shfl_sync(L.gmask, pv, L.gbase);
+    if (pv != kInfInf) continue;
+    uint32_t parent = kNoSlab;
+    for (uint32_t b = rg.boff[v]; b < rg.boff[v + 1] && parent == kNoSlab; ++b) {
+      uint32_t s = b;
+      for (uint32_t hop = 0; s != kNoSlab && hop < (1u << 24); ++hop) {
+        const uint4 q = ld_slab_ro(rg.slabs + 8ull * s + L.gl);
+        uint32_t k[4], w[4];
+        lane_keys<kRW>(q, L.gl, k, w);
+        uint32_t mine = kNoSlab;
+#pragma unroll
+        for (int j = 0; j < keys_per_lane<kRW>(); ++j)
+          if (mine == kNoSlab && k[j] < kTombKey && k[j] != v &&
+              pack_hi(ld_dist(a.dist + k[j])) == lvl)
+            mine = k[j];
+        const uint32_t hit = __ballot_sync(L.gmask, mine != kNoSlab) >> L.gbase;
+        if (hit) {
+          parent = __shfl_sync(L.gmask, mine, L.gbase + __ffs(hit) - 1);
+          break;
+        }
+        s = __shfl_sync(L.gmask, q.w, L.gbase + 7);
+      }
+    }
+    if (parent != kNoSlab && L.gl == 0) {
+      a.dist[v] = pack(lvl + 1, parent);
+      if (atomicExch(a.stamp + v, stamp_next) != stamp_next) push_vertex(a, Q, v, nxt, nsz);
+    }
+  }
+}
+
 template <bool kW, bool kUseW>
 __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   __shared__ unsigned long long q_s[kQueueCap];
@@ -472,7 +517,13 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
     uint32_t *nsz = ctl + kSz0 + ((lv + 1) % 3);
     const uint32_t stamp_next = round + 2 + lv;
     const uint32_t thr = nearfar ? ld_acquire_u32(ctl + kThr) : kNoFar;
-    if (n) {
+    if (n && !kUseW && a.mode == kStatic && a.pull_items && n >= a.pull_items) {
+      // large BFS frontier: pull this level from the unvisited side
+      if (a.rg.weighted)
+        pull_level<true>(a, L, Q, group, ngroups, lv, stamp_next, nxt, nsz);
+      else
+        pull_level<false>(a, L, Q, group, ngroups, lv, stamp_next, nxt, nsz);
+    } else if (n) {
       const NearFar nf = nearfar ? NearFar{thr, fb ? a.far1 : a.far0, ctl + kFarN0 + fb} : all_near;
       for (uint32_t i = group; i < n; i += ngroups) {
         uint32_t u, b0, b1;
@@ -544,6 +595,7 @@ struct mk_traversal {
   uint32_t *ctl = nullptr;
   unsigned long long *pushed = nullptr;
   uint32_t *far0 = nullptr, *far1 = nullptr, *fbits = nullptr;  // near-far SSSP
+  mk_graph *rev = nullptr;  // in-edges of the same graph, for pull levels (BFS)
   Timer timer;
 };
 
@@ -653,6 +705,11 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   a.nsources = t->nsources;
   a.chunk = g->tuning.frontier_chunk ? g->tuning.frontier_chunk : kDefaultChunk;
   a.delta = delta;
+  a.rg = t->rev ? t->rev->view() : GraphView{};
+  if (!t->rev) a.rg.V = 0;
+  a.pull_items = (t->rev && g->tuning.pull_permille)
+                     ? (uint32_t)std::max<uint64_t>(1, (uint64_t)g->V * g->tuning.pull_permille / 1000)
+                     : 0u;
   a.recompute_inv = g->tuning.recompute_permille
                         ? (uint32_t)std::max<uint64_t>(1, (uint64_t)g->V * g->tuning.recompute_permille / 1000)
                         : 0u;
@@ -711,6 +768,18 @@ mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, u
   MK_CUDA(cudaMemcpy(t->sources, h_sources, (size_t)n * 4, cudaMemcpyHostToDevice));
   t->nsources = n;
   t->has_static = false;
+  return MK_OK;
+}
+
+mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_traversal_set_reverse: null handle");
+  if (g_rev) {
+    if (t->sssp) return fail(MK_ERR_INVALID, "mk_traversal_set_reverse: BFS only");
+    if (!g_rev->reverse || g_rev->V != t->g->V || g_rev->device != t->g->device)
+      return fail(MK_ERR_INVALID,
+                  "mk_traversal_set_reverse: needs a reverse graph of the same size on the same device");
+  }
+  t->rev = g_rev;
   return MK_OK;
 }
 

@@ -341,3 +341,31 @@ def test_decremental_recompute_fallback(tuning):
     V = 1 << 12
     s, d, w = mk.gen_rmat(12, 40000, seed=14, w_lo=1, w_hi=1000)
     _traversal_rounds(V, s, d, w, rounds=2, batch=1500, seed=15, tuning=tuning)
+
+
+@pytest.mark.parametrize("pull", [1, 50])
+def test_bfs_pull_levels_match_oracle(pull):
+    """Static BFS with a reverse graph attached pulls its large levels
+    bottom-up: same levels as the oracle, valid parents, before and after an
+    update applied to both graphs."""
+    for V, (s, d, w) in ((1 << 13, mk.gen_rmat(13, 100000, seed=31, w_lo=1, w_hi=9)),
+                         (64 * 64, mk.gen_grid(64, 100, seed=9, w_lo=1, w_hi=9))):
+        G, O = make_pair(V, s, d, w, weighted=True)
+        Gr, _ = make_pair(V, s, d, reverse=True)
+        G.set_tuning(pull_permille=pull)
+        src = int(np.argmax(np.bincount(s, minlength=V)))
+        bfs = mk.BFS(G, src, V)
+        bfs.set_reverse(Gr)
+        bfs.Static()
+        np.testing.assert_array_equal(bfs.Distances(), O.bfs(src))
+        assert O.check_parents(src, bfs.packed(), weighted=False) == 0
+        es = mk.EdgeSet(V, s, d)
+        ds, dd = es.sample_present(len(s) // 5, seed=pull)
+        for g in (G, Gr):
+            g.DeleteEdges(to_dev(ds), to_dev(dd))
+        O.delete(ds, dd)
+        bfs.Static()
+        np.testing.assert_array_equal(bfs.Distances(), O.bfs(src))
+        assert O.check_parents(src, bfs.packed(), weighted=False) == 0
+        with pytest.raises(mk.MeerkatError):
+            mk.SSSP(G, src, V).set_reverse(Gr)
