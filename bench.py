@@ -995,18 +995,62 @@ def main():
         bfs, sssp = mk.BFS(G, src_v, V), mk.SSSP(G, src_v, V)
         algo["bfs_static_ms"] = bfs.Static()
         algo["sssp_static_ms"] = sssp.Static()
-        rec = {k: [] for k in ("bfs_dec_ms", "sssp_dec_ms", "bfs_inc_ms", "sssp_inc_ms")}
+        # a weighted reverse copy of the same edges, kept in step with G, lets a
+        # second pair of traversals re-seed decremental calls from in-edges
+        rp_, col_, w_ = G.export_csr_range_device(0, V, weights=True)
+        rows_ = torch.repeat_interleave(torch.arange(V, device=dev, dtype=torch.int32),
+                                        rp_[1:] - rp_[:-1])
+        indeg_ = torch.bincount(col_.long(), minlength=V).to(torch.int32).cpu().numpy().view(np.uint32)
+        Gr = mk.DynamicGraph(V, degree_hints=indeg_, weighted=True, reverse=True, device=local)
+        Gr.InsertEdges(rows_, col_, vals=w_)
+        assert Gr.sync() == 0
+        del rp_, col_, w_, rows_
+        bfs_r, sssp_r = mk.BFS(G, src_v, V), mk.SSSP(G, src_v, V)
+        bfs_r.set_reverse(Gr)
+        sssp_r.set_reverse(Gr)
+        bfs_r.Static()
+        sssp_r.Static()
+        rec = {k: [] for k in ("bfs_dec_ms", "sssp_dec_ms", "bfs_inc_ms", "sssp_inc_ms",
+                               "bfs_dec_rev_ms", "sssp_dec_rev_ms")}
+        gbs = {k: [] for k in rec}
+
+        def timed_dynamic(key, trav, s_bytes, call):
+            # algorithmic bytes: sum over vertices whose distance changed of
+            # 8 + (s + 8) x out-degree (a lower bound: vertices invalidated
+            # and restored to the same distance are not counted)
+            before = trav.Distances()
+            ms = call()
+            changed = np.flatnonzero(trav.Distances() != before)
+            deg = G.degrees().astype(np.int64)
+            nbytes = int(8 * len(changed) + (s_bytes + 8) * deg[changed].sum())
+            rec[key].append(ms)
+            gbs[key].append(nbytes / (ms / 1e3) / 1e9)
+
         for b in batches[W + 2 * K + 2:W + 2 * K + 2 + A]:
             ds, dd, is_, id_, iw = (todev(x) for x in b)
             G.DeleteEdges(ds, dd)
-            rec["bfs_dec_ms"].append(bfs.Decremental(ds, dd))
-            rec["sssp_dec_ms"].append(sssp.Decremental(ds, dd))
+            Gr.DeleteEdges(ds, dd)
+            timed_dynamic("bfs_dec_ms", bfs, 4, lambda: bfs.Decremental(ds, dd))
+            timed_dynamic("sssp_dec_ms", sssp, 8, lambda: sssp.Decremental(ds, dd))
+            timed_dynamic("bfs_dec_rev_ms", bfs_r, 4, lambda: bfs_r.Decremental(ds, dd))
+            timed_dynamic("sssp_dec_rev_ms", sssp_r, 8, lambda: sssp_r.Decremental(ds, dd))
             G.InsertEdges(is_, id_, vals=iw)
-            rec["bfs_inc_ms"].append(bfs.Incremental(is_, id_))
-            rec["sssp_inc_ms"].append(sssp.Incremental(is_, id_, wgt=iw))
+            Gr.InsertEdges(is_, id_, vals=iw)
+            timed_dynamic("bfs_inc_ms", bfs, 4, lambda: bfs.Incremental(is_, id_))
+            timed_dynamic("sssp_inc_ms", sssp, 8, lambda: sssp.Incremental(is_, id_, wgt=iw))
+            bfs_r.Incremental(is_, id_, timed=False)
+            sssp_r.Incremental(is_, id_, wgt=iw, timed=False)
+        assert np.array_equal(bfs.Distances(), bfs_r.Distances())
+        assert np.array_equal(sssp.Distances(), sssp_r.Distances())
+        for o in (bfs_r, sssp_r, Gr):
+            o.close()
         assert G.sync() == 0
+        peak_q = measured_peak()[0]
         for k, v in rec.items():
             algo[k + "_p50"] = statistics.median(v)
+            g = statistics.median(gbs[k])
+            algo[k.replace("_ms", "_gbs") + "_p50"] = g
+            algo[k.replace("_ms", "_frac") + "_p50"] = g / peak_q
         algo["source"] = src_v
         bfs.close()
         sssp.close()

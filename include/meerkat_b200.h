@@ -223,10 +223,12 @@ mk_status mk_sssp_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t 
  * one multi-source query per round with one resident traversal.  No
  * counterpart in the reference. */
 mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, uint32_t n);
-/* Attaches the reverse graph (in-edges) of the same edge set to a BFS, for
- * pull levels of static calls (tuning.pull_permille); the caller keeps both
- * graphs updated with the same batches.  NULL detaches.  No counterpart in
- * the reference. */
+/* Attaches the reverse graph (in-edges) of the same edge set (for SSSP:
+ * weighted, with the same weights): static BFS pulls large levels
+ * (tuning.pull_permille), and decremental BFS/SSSP re-seed invalidated
+ * vertices from their own in-edges instead of sweeping every bucket.  The
+ * caller keeps both graphs updated with the same batches.  NULL detaches.
+ * No counterpart in the reference. */
 mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev);
 /* float Static(EdgesN) (BFSImpl.cuh:590-662, SSSPImpl.cuh:607-690). */
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out);

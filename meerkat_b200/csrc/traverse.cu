@@ -335,6 +335,46 @@ __device__ __forceinline__ void pull_level(const TravArgs &a, const Lanes &L, co
   }
 }
 
+// Decremental re-seed by pull: every invalidated vertex takes the best
+// distance offered by its in-neighbours that are still valid (reverse graph;
+// its weights when SSSP), instead of a sweep over every bucket of the graph.
+template <bool kRW, bool kUseW>
+__device__ __forceinline__ void pull_reseed(const TravArgs &a, const Lanes &L, const BlockQueue &Q,
+                                            uint32_t group, uint32_t ngroups, uint32_t ninv,
+                                            uint32_t stamp_next, unsigned long long *gfr,
+                                            uint32_t *gsz) {
+  const GraphView &rg = a.rg;
+  for (uint32_t i = group; i < ninv; i += ngroups) {
+    const uint32_t v = __ldcg(a.inv_list + i);
+    unsigned long long best = kInfInf;  // pack(candidate distance, parent)
+    for (uint32_t b = rg.boff[v]; b < rg.boff[v + 1]; ++b) {
+      uint32_t s = b;
+      for (uint32_t hop = 0; s != kNoSlab && hop < (1u << 24); ++hop) {
+        const uint4 q = ld_slab_ro(rg.slabs + 8ull * s + L.gl);
+        uint32_t k[4], w[4];
+        lane_keys<kRW>(q, L.gl, k, w);
+#pragma unroll
+        for (int j = 0; j < keys_per_lane<kRW>(); ++j) {
+          const uint32_t u = k[j];
+          if (u >= kTombKey || u == v || inval_test(a.inval, u)) continue;
+          const unsigned long long pu = ld_dist(a.dist + u);
+          if (pu == kInfInf) continue;
+          const unsigned long long nd = (unsigned long long)pack_hi(pu) + (kUseW ? w[j] : 1u);
+          if (nd < kInf) best = min(best, pack((uint32_t)nd, u));
+        }
+        s = __shfl_sync(L.gmask, q.w, L.gbase + 7);
+      }
+    }
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(L.gmask, best, o, 8));
+    if (L.gl == 0 && best != kInfInf) {
+      const unsigned long long old = atomicMin(a.dist + v, best);
+      if (old > best && atomicExch(a.stamp + v, stamp_next) != stamp_next)
+        push_vertex(a, Q, v, gfr, gsz);
+    }
+  }
+}
+
 template <bool kW, bool kUseW>
 __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   __shared__ unsigned long long q_s[kQueueCap];
@@ -477,6 +517,12 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
         atomicAdd(a.pushed, 1ull);
       }
       nearfar = kUseW && a.delta != 0 && a.far0 != nullptr;
+    } else if (hi > 0 && a.rg.V) {
+      // D3 with the reverse graph: pull from each invalidated vertex's in-edges
+      if (a.rg.weighted)
+        pull_reseed<true, kUseW>(a, L, Q, group, ngroups, hi, round + 1, a.fr0, ctl + kSz0);
+      else
+        pull_reseed<false, kUseW>(a, L, Q, group, ngroups, hi, round + 1, a.fr0, ctl + kSz0);
     } else if (hi > 0) {
       // D3: re-seed invalidated vertices from valid in-neighbours: one sweep
       // over all buckets (balanced by construction)
@@ -774,7 +820,8 @@ mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, u
 mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev) {
   if (!t) return fail(MK_ERR_INVALID, "mk_traversal_set_reverse: null handle");
   if (g_rev) {
-    if (t->sssp) return fail(MK_ERR_INVALID, "mk_traversal_set_reverse: BFS only");
+    if (t->sssp && !g_rev->weighted)
+      return fail(MK_ERR_INVALID, "mk_traversal_set_reverse: SSSP needs a weighted reverse graph");
     if (!g_rev->reverse || g_rev->V != t->g->V || g_rev->device != t->g->device)
       return fail(MK_ERR_INVALID,
                   "mk_traversal_set_reverse: needs a reverse graph of the same size on the same device");

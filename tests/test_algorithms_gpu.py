@@ -368,4 +368,52 @@ def test_bfs_pull_levels_match_oracle(pull):
         np.testing.assert_array_equal(bfs.Distances(), O.bfs(src))
         assert O.check_parents(src, bfs.packed(), weighted=False) == 0
         with pytest.raises(mk.MeerkatError):
-            mk.SSSP(G, src, V).set_reverse(Gr)
+            mk.SSSP(G, src, V).set_reverse(Gr)  # SSSP needs a weighted reverse graph
+
+
+def test_decremental_reseed_from_reverse_graph():
+    """Decremental BFS/SSSP with a reverse graph attached re-seed invalidated
+    vertices from their own in-edges (weighted reverse copy for SSSP): the
+    oracle's answers after every delete and insert batch, including deletes
+    of shortest-path-tree edges."""
+    for V, (s, d, w) in ((1 << 12, mk.gen_rmat(12, 50000, seed=41, w_lo=1, w_hi=1000)),
+                         (48 * 48, mk.gen_grid(48, 60, seed=42, w_lo=1, w_hi=1000))):
+        G, O = make_pair(V, s, d, w, weighted=True)
+        Gr, _ = make_pair(V, s, d, w, weighted=True, reverse=True)
+        G.set_tuning(recompute_permille=0)  # always repair, never recompute
+        src = int(np.argmax(np.bincount(s, minlength=V)))
+        bfs, sssp = mk.BFS(G, src, V), mk.SSSP(G, src, V)
+        bfs.set_reverse(Gr)
+        sssp.set_reverse(Gr)
+        bfs.Static()
+        sssp.Static()
+        es = mk.EdgeSet(V, s, d)
+        rng = np.random.default_rng(43)
+        for r in range(3):
+            ds, dd = es.sample_present(len(s) // 20, seed=50 + r)
+            par = (sssp.packed() & np.uint64(0xFFFFFFFF)).astype(np.int64)
+            dist = sssp.Distances()
+            tree = np.flatnonzero((dist != mk.MK_INF) & (par != np.arange(V)))
+            pick = rng.choice(tree, size=min(len(tree), 200), replace=False)
+            ds = np.concatenate([ds, par[pick]]).astype(np.uint32)
+            dd = np.concatenate([dd, pick]).astype(np.uint32)
+            for g in (G, Gr):
+                g.DeleteEdges(to_dev(ds), to_dev(dd))
+            O.delete(ds, dd)
+            bfs.Decremental(to_dev(ds), to_dev(dd))
+            sssp.Decremental(to_dev(ds), to_dev(dd))
+            np.testing.assert_array_equal(bfs.Distances(), O.bfs(src))
+            np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
+            assert O.check_parents(src, sssp.packed(), weighted=True) == 0
+            is_, id_ = es.sample_absent(len(s) // 20, seed=60 + r)
+            iw = rng.integers(1, 1001, len(is_)).astype(np.uint32)
+            for g in (G, Gr):
+                g.InsertEdges(to_dev(is_), to_dev(id_), vals=to_dev(iw))
+            O.insert(is_, id_, iw)
+            bfs.Incremental(to_dev(is_), to_dev(id_))
+            sssp.Incremental(to_dev(is_), to_dev(id_), wgt=to_dev(iw))
+            np.testing.assert_array_equal(bfs.Distances(), O.bfs(src))
+            np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
+        with pytest.raises(mk.MeerkatError):
+            Gu, _ = make_pair(V, s, d, reverse=True)  # unweighted reverse
+            mk.SSSP(G, src, V).set_reverse(Gu)
