@@ -511,10 +511,28 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         else:
             mism["wcc"] += int(not np.array_equal(a.Labels().astype(np.int64), l_union[lo:hi] - lo))
     assert mism == {"bfs": 0, "wcc": 0}, mism
+    # phase split of the batched step: two more steps (a batch and its
+    # inverse, so the set stays on the same state) with events between phases
+    phases = {"update": 0.0, "bfs": 0.0, "wcc": 0.0}
+    for i in range(2):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(stream)
+        br.update(*both[(Wb + K + i) % 2])
+        ev[1].record(stream)
+        if br.bfs is not None:
+            br.bfs.Static(timed=False)
+        ev[2].record(stream)
+        if br.wcc is not None:
+            br.wcc.StaticPrepared(timed=False)
+        ev[3].record(stream)
+        ev[3].synchronize()
+        for k, (x, y) in zip(phases, [(0, 1), (1, 2), (2, 3)]):
+            phases[k] += ev[x].elapsed_time(ev[y]) / 2
     out = {
         "speedup_vs_plain": plain_ms / batched_ms,
         "speedup_vs_plain_cuda_graph": plain_graph_ms / batched_ms,
         "batched_ms_per_step": batched_ms, "plain_ms_per_step": plain_ms,
+        "batched_phases_ms": phases,
         "plain_cuda_graph_ms_per_step": plain_graph_ms, "plain_capture_s": cap_s,
         "steps": K, "warmup": Wb,
         "workload": f"batched_{Gn}_graphs",

@@ -346,6 +346,17 @@ mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stre
  * reference. */
 mk_status mk_wcc_static_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges,
                                uint32_t nranges, void *stream, float *ms_out);
+/* The two halves of mk_wcc_static_ranges.  prepare uploads the range table
+ * (blocking: it waits for the device, since queued work may read the
+ * previous table); static_prepared runs on it and issues only asynchronous
+ * work on `stream`, so it can be captured into a CUDA graph (a later prepare
+ * invalidates such a capture).  Ranges of at most 65,536 vertices are each
+ * solved by one CTA with the parent array in shared memory; larger ones by
+ * the device-wide pass.  A key outside its range sets MK_DEVERR_INVALID_ID
+ * on the graph.  No counterpart in the reference. */
+mk_status mk_wcc_prepare_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges,
+                                uint32_t nranges);
+mk_status mk_wcc_static_prepared(mk_wcc *w, void *stream, float *ms_out);
 mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src,
                              const uint32_t *d_dst, uint32_t n, void *stream,
                              float *ms_out);

@@ -16,12 +16,14 @@ from typing import Optional
 
 import numpy as np
 
-from ._lib import (MK_INF, GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
+from ._lib import (DEVERR_INVALID_ID, DEVERR_OOM, DEVERR_OVERFLOW, DEVERR_TIMEOUT, MK_INF,
+                   GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
 __all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "PageRankRange", "TC", "WCC",
            "EdgeSet",
            "gen_rmat", "gen_grid", "gen_rmat_members", "read_edge_list", "read_batch",
-           "write_edge_list", "write_batch", "MeerkatError", "MK_INF", "lib", "version"]
+           "write_edge_list", "write_batch", "MeerkatError", "MK_INF", "DEVERR_INVALID_ID",
+           "DEVERR_OOM", "DEVERR_TIMEOUT", "DEVERR_OVERFLOW", "lib", "version"]
 
 
 def version() -> str:
@@ -512,6 +514,19 @@ class WCC(_Timed):
         return self._call(lib().mk_wcc_static_ranges, self._h,
                           r.ctypes.data_as(C.POINTER(C.c_uint32)), len(r) // 2, _stream(stream),
                           timed=timed)
+
+    def PrepareRanges(self, ranges):
+        """Uploads a vertex-range table [(begin, end), ...] for StaticPrepared
+        (blocking).  Ranges of at most 65,536 vertices are each solved by one
+        CTA in shared memory; larger ones by the device-wide pass."""
+        r = np.ascontiguousarray(np.asarray(ranges, dtype=np.uint32).reshape(-1))
+        check(lib().mk_wcc_prepare_ranges(self._h, r.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                          len(r) // 2), "mk_wcc_prepare_ranges")
+
+    def StaticPrepared(self, stream=None, timed=True):
+        """StaticRanges over the prepared table; only asynchronous work on the
+        stream, so it can be captured into a CUDA graph."""
+        return self._call(lib().mk_wcc_static_prepared, self._h, _stream(stream), timed=timed)
 
     def StaticSubset(self, sel_bits, stream=None, timed=True):
         """Recomputes the labels of the vertices whose bit is set in the device

@@ -17,6 +17,8 @@ MK_OK, MK_ERR_INVALID, MK_ERR_OOM, MK_ERR_TIMEOUT, MK_ERR_CUDA, MK_ERR_STATE = r
 STATUS_NAMES = {0: "MK_OK", 1: "MK_ERR_INVALID", 2: "MK_ERR_OOM", 3: "MK_ERR_TIMEOUT",
                 4: "MK_ERR_CUDA", 5: "MK_ERR_STATE"}
 MK_INF = 0xFFFFFFFF
+# sticky device error bits returned by DynamicGraph.sync() (MK_DEVERR_*)
+DEVERR_INVALID_ID, DEVERR_OOM, DEVERR_TIMEOUT, DEVERR_OVERFLOW = 0x1, 0x2, 0x4, 0x8
 
 
 class GraphDesc(C.Structure):
@@ -103,6 +105,8 @@ SIGNATURES = [
     ("mk_wcc_static", _S, [vp, vp, f32p]),
     ("mk_wcc_static_subset", _S, [vp, vp, vp, f32p]),
     ("mk_wcc_static_ranges", _S, [vp, u32p, C.c_uint32, vp, f32p]),
+    ("mk_wcc_prepare_ranges", _S, [vp, u32p, C.c_uint32]),
+    ("mk_wcc_static_prepared", _S, [vp, vp, f32p]),
     ("mk_wcc_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_decremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_labels", _S, [vp, vp]),

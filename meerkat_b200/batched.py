@@ -12,7 +12,8 @@ members in one GraphSet and issues, per step,
 
   one delete launch and one insert launch for every member's batch,
   one multi-source BFS (one source per BFS-queried member), and
-  one subset WCC pass over the WCC-queried members,
+  one WCC launch over the WCC-queried members (a member of at most 65,536
+  vertices is solved by one CTA with its union-find in shared memory),
 
 each member's results being those of the member alone.  The step can be
 captured into a CUDA graph and replayed; the autotuner picks the update
@@ -29,6 +30,7 @@ import numpy as np
 from . import BFS, WCC, DynamicGraph, GraphSet
 
 QUERY_BFS, QUERY_WCC = 0, 1
+WCC_LOCAL_MAX = 1 << 16  # vertices of a member that one CTA solves in shared memory
 
 
 @dataclass
@@ -103,9 +105,10 @@ class BatchedRunner:
         self.sources_global = glob
         self.bfs = BFS(self.G, glob) if len(glob) else None
         self.wcc = WCC(self.G) if len(self.wcc_members) else None
-        flags = np.zeros(gs.num_graphs, dtype=np.uint8)
-        flags[self.wcc_members] = 1
-        self.sel = gs.select_bits(flags)
+        sizes = off[self.wcc_members + 1] - off[self.wcc_members]
+        self._wcc_large = int((sizes > WCC_LOCAL_MAX).sum())
+        if self.wcc is not None:
+            self.wcc.PrepareRanges(np.stack([off[self.wcc_members], off[self.wcc_members + 1]], 1))
 
     def update(self, ds, dd, is_, id_, iw, stream=None):
         self.G.DeleteEdges(ds, dd, stream=stream)
@@ -115,15 +118,18 @@ class BatchedRunner:
         if self.bfs is not None:
             self.bfs.Static(stream=stream, timed=False)
         if self.wcc is not None:
-            self.wcc.StaticSubset(self.sel, stream=stream, timed=False)
+            self.wcc.StaticPrepared(stream=stream, timed=False)
 
     def step(self, batch, stream=None):
         self.update(*batch, stream=stream)
         self.query(stream=stream)
 
     def launches_per_step(self) -> int:
-        # delete, insert; BFS: 2 memsets + 1 cooperative kernel; WCC: 3 kernels
-        return 2 + (1 if self.bfs is not None else 0) + (3 if self.wcc is not None else 0)
+        # kernels: delete, insert; BFS: 1 cooperative kernel (plus 2 memsets);
+        # WCC: 1 shared-memory kernel (plus 1 memset), and 5 device-wide
+        # kernels when some member is larger than shared memory holds
+        wcc = (1 + (5 if self._wcc_large else 0)) if self.wcc is not None else 0
+        return 2 + (1 if self.bfs is not None else 0) + wcc
 
     def member_bfs(self, m_index: int, dist: Optional[np.ndarray] = None) -> np.ndarray:
         """BFS levels of the i-th BFS member (slice of the union result)."""

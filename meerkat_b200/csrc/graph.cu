@@ -1273,7 +1273,10 @@ mk_status mk_graph_sync(mk_graph *g, void *stream, uint32_t *h_deverr) {
   if (h_deverr) *h_deverr = err;
   if (err & kErrTimeout) return fail(MK_ERR_TIMEOUT, "device wait or probe limit exceeded");
   if (err & kErrOom) return fail(MK_ERR_OOM, "slab pool exhausted");
-  if (err & kErrInvalidId) return fail(MK_ERR_INVALID, "batch holds a vertex id >= num_vertices");
+  if (err & kErrInvalidId)
+    return fail(MK_ERR_INVALID,
+                "vertex id out of range: a batch id >= num_vertices, or an edge leaving the "
+                "vertex range of a range call");
   return MK_OK;
 }
 

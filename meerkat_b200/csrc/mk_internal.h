@@ -39,6 +39,7 @@ struct DevBuf {
     if (n <= cap) return MK_OK;
     size_t want = cap ? cap : 1024;
     while (want < n) want *= 2;
+    const size_t old = cap;
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     cap = 0;
@@ -47,7 +48,7 @@ struct DevBuf {
       ptr = nullptr;
       return cuda_fail(e, "cudaMalloc(scratch)");
     }
-    if (bytes_acc) *bytes_acc += (want - cap) * sizeof(T);
+    if (bytes_acc) *bytes_acc += (want - old) * sizeof(T);
     cap = want;
     return MK_OK;
   }

@@ -5,8 +5,10 @@
 // union that hooks the larger root under the smaller one with a CAS
 // (UnionAsync, :194-215), so every root is the minimum vertex id of its tree.
 // This build adds the entry points:
-//   static       every vertex is its own parent, every live edge is a union,
-//                then every vertex is compressed to its root;
+//   static       every vertex is its own parent; two sampled out-edges per
+//                vertex are unions, then every live edge whose endpoints do
+//                not share a parent yet; then every vertex is compressed to
+//                its root;
 //   incremental  union of the edges the last insert applied, then compress;
 //   decremental  union-find cannot split, so every component that lost an
 //                edge is reset and rebuilt from its vertices' out-edges (an
@@ -69,27 +71,6 @@ __global__ void k_uf_init(uint32_t *p, uint32_t V, const uint32_t *sel_bits = nu
   }
 }
 
-// Union every out-edge of the vertices selected by `sel` (all if null); one
-// group per bucket so hubs do not serialise the pass.
-template <bool kW>
-__global__ void k_uf_edges(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
-  const Lanes L = lanes();
-  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
-    const uint32_t u = g.bowner[b];
-    if (g.deg[u] == 0) continue;
-    if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
-    walk_bucket(g, L, b, [&](const uint4 &q) {
-      uint32_t k[4], w[4];
-      lane_keys<kW>(q, L.gl, k, w);
-#pragma unroll
-      for (int i = 0; i < keys_per_lane<kW>(); ++i)
-        if (k[i] < kTombKey && k[i] != u) uf_union(p, u, k[i], err);
-    });
-  }
-}
-
 __global__ void k_uf_batch(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
                            const uint8_t *__restrict__ applied, uint32_t n, uint32_t V,
                            uint32_t *p, uint32_t *err) {
@@ -128,15 +109,14 @@ __global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, 
   }
 }
 
-// ---- static pass with the largest component skipped ----
-// Each vertex is first linked to up to two out-neighbours from its first
-// head slab; after compression most vertices of the largest component point
-// at its root.  The full pass then skips every edge whose endpoints both
-// point at that root (they are connected already), so on graphs with a giant
-// component most edges cost one read instead of two finds.  Skipping only
-// edges between vertices already connected keeps the result exact.
-constexpr uint32_t kUfSamples = 1024;
-
+// ---- sampled linking, then a pass that skips already-connected edges ----
+// Each vertex is first linked to up to two out-neighbours from its first head
+// slab; after compression most vertices of every large component point at its
+// root.  The full pass then skips every edge whose endpoints already have the
+// same parent (they are connected), so on graphs with big components most
+// edges cost two reads instead of two finds and a CAS.  Skipping only edges
+// between vertices already connected keeps the result exact, and it works for
+// every component at once (the members of a graph set included).
 template <bool kW>
 __global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.V; u += gridDim.x * blockDim.x) {
@@ -149,46 +129,35 @@ __global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, 
   }
 }
 
-// One block: the most frequent root among kUfSamples strided vertices.
-__global__ void k_uf_giant(const uint32_t *p, uint32_t V, uint32_t *giant) {
-  __shared__ uint32_t smp[kUfSamples];
-  __shared__ unsigned long long best;
-  for (uint32_t i = threadIdx.x; i < kUfSamples; i += blockDim.x)
-    smp[i] = __ldcg(p + (uint32_t)(((unsigned long long)i * V) / kUfSamples));
-  if (threadIdx.x == 0) best = 0;
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < kUfSamples; i += blockDim.x) {
-    uint32_t c = 0;
-    for (uint32_t j = 0; j < kUfSamples; ++j) c += smp[j] == smp[i];
-    atomicMax(&best, ((unsigned long long)c << 32) | smp[i]);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) *giant = (uint32_t)best;
+// Unions of the out-edges of bucket b (owner u) whose endpoints do not share
+// a parent yet.
+template <bool kW>
+__device__ __forceinline__ void link_bucket_skip(const GraphView &g, const Lanes &L, uint32_t *p,
+                                                 uint32_t b, uint32_t u, uint32_t *err) {
+  const uint32_t pu = __ldcg(p + u);
+  walk_bucket(g, L, b, [&](const uint4 &q) {
+    uint32_t k[4], w[4];
+    lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+    for (int j = 0; j < keys_per_lane<kW>(); ++j) {
+      const uint32_t v = k[j];
+      if (v >= kTombKey || v == u) continue;
+      if (__ldcg(p + v) == pu) continue;
+      uf_union(p, u, v, err);
+    }
+  });
 }
 
 template <bool kW>
-__global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bits,
-                                const uint32_t *giant_p, uint32_t *err) {
+__global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
   const Lanes L = lanes();
-  const uint32_t giant = *giant_p;
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
   for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
     const uint32_t u = g.bowner[b];
     if (g.deg[u] == 0) continue;
     if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
-    const bool u_giant = __ldcg(p + u) == giant;
-    walk_bucket(g, L, b, [&](const uint4 &q) {
-      uint32_t k[4], w[4];
-      lane_keys<kW>(q, L.gl, k, w);
-#pragma unroll
-      for (int j = 0; j < keys_per_lane<kW>(); ++j) {
-        const uint32_t v = k[j];
-        if (v >= kTombKey || v == u) continue;
-        if (u_giant && __ldcg(p + v) == giant) continue;
-        uf_union(p, u, v, err);
-      }
-    });
+    link_bucket_skip<kW>(g, L, p, b, u, err);
   }
 }
 
@@ -218,6 +187,20 @@ __global__ void k_uf_init_ranges(uint32_t *p, const uint32_t *vpre, const uint32
 }
 
 template <bool kW>
+__global__ void k_uf_sample_ranges(GraphView g, uint32_t *p, const uint32_t *vpre,
+                                   const uint32_t *vbase, uint32_t nr, uint32_t *err) {
+  const uint32_t total = vpre[nr];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const uint32_t u = range_at(vpre, nr, i, vbase);
+    if (g.deg[u] == 0) continue;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(g.slabs + 8ull * g.boff[u]);
+    const uint32_t k0 = w[0], k1 = kW ? w[2] : w[1];
+    if (k0 < kTombKey && k0 != u) uf_union(p, u, k0, err);
+    if (k1 < kTombKey && k1 != u) uf_union(p, u, k1, err);
+  }
+}
+
+template <bool kW>
 __global__ void k_uf_edges_ranges(GraphView g, uint32_t *p, const uint32_t *bpre,
                                   const uint32_t *bbase, uint32_t nr, uint32_t *err) {
   const Lanes L = lanes();
@@ -228,13 +211,7 @@ __global__ void k_uf_edges_ranges(GraphView g, uint32_t *p, const uint32_t *bpre
     const uint32_t b = range_at(bpre, nr, i, bbase);
     const uint32_t u = g.bowner[b];
     if (g.deg[u] == 0) continue;
-    walk_bucket(g, L, b, [&](const uint4 &q) {
-      uint32_t k[4], w[4];
-      lane_keys<kW>(q, L.gl, k, w);
-#pragma unroll
-      for (int j = 0; j < keys_per_lane<kW>(); ++j)
-        if (k[j] < kTombKey && k[j] != u) uf_union(p, u, k[j], err);
-    });
+    link_bucket_skip<kW>(g, L, p, b, u, err);
   }
 }
 
@@ -247,6 +224,115 @@ __global__ void k_uf_compress_ranges(uint32_t *p, const uint32_t *vpre, const ui
   }
 }
 
+// ---- ranges held in shared memory ----
+// A range of at most kLocalMax vertices (a member of a graph set) is solved
+// by one CTA: its parent array lives in shared memory as 16-bit local ids, so
+// every find, halving store and hooking CAS stays on chip, and device memory
+// sees one pass over the range's slabs and one write of its labels.  CTAs
+// take ranges from a counter, largest first.  The union rule is the one of
+// the global kernels (larger root under smaller), so labels are again the
+// minimum vertex id of each component.
+constexpr uint32_t kLocalMax = 1u << 16;
+constexpr int kMemberThreads = 1024;
+constexpr uint32_t kMemberHeads = 4;  // head slabs a group loads together
+
+__device__ __forceinline__ uint32_t ls_find(uint16_t *p, uint32_t x) {
+  volatile uint16_t *vp = p;
+  for (uint32_t it = 0; it < kUfLimit; ++it) {
+    const uint32_t px = vp[x];
+    if (px == x) return x;
+    const uint32_t gx = vp[px];
+    if (px != gx) vp[x] = (uint16_t)gx;  // x is not a root: only halving writes it
+    x = gx;
+  }
+  return x;
+}
+
+__device__ __forceinline__ uint32_t ls_root(const uint16_t *p, uint32_t x) {
+  const volatile uint16_t *vp = p;
+  for (uint32_t it = 0; it < kUfLimit; ++it) {
+    const uint32_t px = vp[x];
+    if (px == x) return x;
+    x = px;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void ls_union(uint16_t *p, uint32_t a, uint32_t b, uint32_t *err) {
+  for (uint32_t it = 0; it < kUfLimit; ++it) {
+    const uint32_t ra = ls_find(p, a), rb = ls_find(p, b);
+    if (ra == rb) return;
+    const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+    if (atomicCAS(reinterpret_cast<unsigned short *>(p + hi), (unsigned short)hi,
+                  (unsigned short)lo) == (unsigned short)hi)
+      return;
+  }
+  atomicOr(err, kErrTimeout);
+}
+
+// rng[r] = (first vertex, end vertex, first bucket, end bucket), at most
+// kLocalMax vertices each.  A key outside its range (a range that is not
+// closed under edges) is skipped and reported as MK_DEVERR_INVALID_ID.
+template <bool kW>
+__global__ void __launch_bounds__(kMemberThreads, 1)
+    k_uf_members(GraphView g, const uint4 *__restrict__ rng, uint32_t nr, uint32_t *counter,
+                 uint32_t *__restrict__ labels, uint32_t *err) {
+  extern __shared__ uint16_t sp[];
+  __shared__ uint32_t s_range;
+  const Lanes L = lanes();
+  const uint32_t group = threadIdx.x >> 3, ngroups = blockDim.x >> 3;
+  for (;;) {
+    if (threadIdx.x == 0) s_range = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t r = s_range;
+    if (r >= nr) break;
+    const uint4 R = rng[r];
+    const uint32_t lo = R.x, n = R.y - R.x;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sp[i] = (uint16_t)i;
+    __syncthreads();
+    for (uint32_t b = R.z + group * kMemberHeads; b < R.w; b += ngroups * kMemberHeads) {
+      const uint32_t m = min(kMemberHeads, R.w - b);
+      uint4 q[kMemberHeads];
+      uint32_t own[kMemberHeads];
+#pragma unroll
+      for (uint32_t j = 0; j < kMemberHeads; ++j)
+        if (j < m) {
+          q[j] = ld_slab_ro(g.slabs + 8ull * (b + j) + L.gl);
+          own[j] = __ldg(g.bowner + b + j) - lo;
+        }
+#pragma unroll
+      for (uint32_t j = 0; j < kMemberHeads; ++j) {
+        if (j >= m) continue;
+        const uint32_t u = own[j];
+        auto link = [&](const uint4 x) {
+          uint32_t k[4], w[4];
+          lane_keys<kW>(x, L.gl, k, w);
+#pragma unroll
+          for (int t = 0; t < keys_per_lane<kW>(); ++t) {
+            if (k[t] >= kTombKey) continue;
+            const uint32_t v = k[t] - lo;
+            if (v >= n || u >= n) {
+              atomicOr(err, kErrInvalidId);
+              continue;
+            }
+            if (v != u) ls_union(sp, u, v, err);
+          }
+        };
+        link(q[j]);
+        uint32_t nx = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
+        while (nx != kNoSlab) {
+          const uint4 x = ld_slab_ro(g.slabs + 8ull * nx + L.gl);
+          link(x);
+          nx = __shfl_sync(L.gmask, x.w, L.gbase + 7);
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) labels[lo + i] = lo + ls_root(sp, i);
+    __syncthreads();  // sp and s_range are reused by the next range
+  }
+}
+
 }  // namespace mk
 
 using namespace mk;
@@ -256,9 +342,14 @@ struct mk_wcc {
   uint32_t *parent = nullptr;
   uint32_t *aff_labels = nullptr;
   uint32_t *aff_vertices = nullptr;
-  uint32_t *err = nullptr;
-  uint32_t *giant = nullptr;  // root of the sampled largest component
-  DevBuf<uint32_t> ranges;  // vpre, vbase, bpre, bbase of the last range call
+  uint32_t *err = nullptr;  // the graph's sticky device error word
+  // prepared range table: counter word, then uint4 (lo, hi, b0, b1) per small
+  // range (largest first), then vpre, vbase, bpre, bbase of the large ranges
+  DevBuf<uint32_t> ranges;
+  uint32_t n_small = 0, n_large = 0, small_max = 0;
+  uint64_t large_vt = 0, large_bt = 0;
+  int small_grid = 0;
+  bool prepared = false;
   Timer timer;
 };
 
@@ -266,20 +357,9 @@ static int flat_grid(uint64_t n, int device) {
   return (int)std::min<uint64_t>(n / 256 + 1, (uint64_t)device_sm_count(device) * 8);
 }
 
-static mk_status wcc_edges(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
-  mk_graph *g = w->g;
-  int blocks = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
-  if (g->weighted)
-    k_uf_edges<true><<<blocks, 256, 0, s>>>(g->view(), w->parent, sel, w->err);
-  else
-    k_uf_edges<false><<<blocks, 256, 0, s>>>(g->view(), w->parent, sel, w->err);
-  MK_CUDA(cudaGetLastError());
-  return MK_OK;
-}
-
 // Unions of the out-edges of the selected vertices (all if sel is null), whose
-// parents start reset: sample two neighbours each, compress, find the largest
-// component, then every remaining edge that does not join two vertices of it.
+// parents start reset: sample two neighbours each, compress, then every edge
+// whose endpoints do not share a parent yet.
 static mk_status wcc_link(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
   mk_graph *g = w->g;
   const int fg = flat_grid(g->V, g->device);
@@ -289,13 +369,12 @@ static mk_status wcc_link(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
   else
     k_uf_sample<false><<<fg, 256, 0, s>>>(v, w->parent, sel, w->err);
   k_uf_compress<<<fg, 256, 0, s>>>(w->parent, g->V, sel);
-  k_uf_giant<<<1, 1024, 0, s>>>(w->parent, g->V, w->giant);
   const int blocks = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1,
                                              (uint64_t)device_sm_count(g->device) * 8);
   if (g->weighted)
-    k_uf_edges_skip<true><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->giant, w->err);
+    k_uf_edges_skip<true><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->err);
   else
-    k_uf_edges_skip<false><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->giant, w->err);
+    k_uf_edges_skip<false><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->err);
   k_uf_compress<<<fg, 256, 0, s>>>(w->parent, g->V, sel);
   MK_CUDA(cudaGetLastError());
   return MK_OK;
@@ -323,9 +402,7 @@ mk_status mk_wcc_create(mk_graph *g, mk_wcc **out) {
   cudaError_t e = cudaMalloc(&w->parent, V * 4);
   if (e == cudaSuccess) e = cudaMalloc(&w->aff_labels, words * 4);
   if (e == cudaSuccess) e = cudaMalloc(&w->aff_vertices, words * 4);
-  if (e == cudaSuccess) e = cudaMalloc(&w->err, 4);
-  if (e == cudaSuccess) e = cudaMalloc(&w->giant, 4);
-  if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4);
+  w->err = g->err_word();
   if (e != cudaSuccess) {
     mk_wcc_destroy(w);
     return cuda_fail(e, "mk_wcc_create");
@@ -357,8 +434,106 @@ mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stre
   cudaStream_t s = as_stream(stream);
   MK_CHECK(w->timer.start(s, ms_out != nullptr));
   k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, d_sel_bits);
-  MK_CHECK(wcc_edges(w, d_sel_bits, s));
-  k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, d_sel_bits);
+  MK_CHECK(wcc_link(w, d_sel_bits, s));
+  return w->timer.stop(ms_out);
+}
+
+mk_status mk_wcc_prepare_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges, uint32_t nranges) {
+  if (!w || (nranges && !h_vertex_ranges))
+    return fail(MK_ERR_INVALID, "mk_wcc_prepare_ranges: null argument");
+  mk_graph *g = w->g;
+  std::vector<uint32_t> small_ids, large_ids;
+  for (uint32_t r = 0; r < nranges; ++r) {
+    const uint32_t b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
+    if (b >= e || e > g->V) return fail(MK_ERR_INVALID, "mk_wcc_prepare_ranges: bad vertex range");
+    (e - b <= kLocalMax ? small_ids : large_ids).push_back(r);
+  }
+  auto len = [&](uint32_t r) { return h_vertex_ranges[2 * r + 1] - h_vertex_ranges[2 * r]; };
+  std::stable_sort(small_ids.begin(), small_ids.end(),
+                   [&](uint32_t a, uint32_t b) { return len(a) > len(b); });
+  const size_t ns = small_ids.size(), nl = large_ids.size();
+  std::vector<uint32_t> host(4 + 4 * ns + 4 * (nl + 1), 0u);
+  uint32_t *sm = host.data() + 4;
+  for (size_t i = 0; i < ns; ++i) {
+    const uint32_t r = small_ids[i], b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
+    sm[4 * i + 0] = b;
+    sm[4 * i + 1] = e;
+    sm[4 * i + 2] = g->h_boff[b];
+    sm[4 * i + 3] = g->h_boff[e];
+  }
+  uint32_t *vpre = sm + 4 * ns, *vbase = vpre + nl + 1, *bpre = vbase + nl + 1, *bbase = bpre + nl + 1;
+  uint64_t vt = 0, bt = 0;
+  for (size_t i = 0; i < nl; ++i) {
+    const uint32_t r = large_ids[i], b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
+    vpre[i] = (uint32_t)vt;
+    vbase[i] = b;
+    bpre[i] = (uint32_t)bt;
+    bbase[i] = g->h_boff[b];
+    vt += e - b;
+    bt += g->h_boff[e] - g->h_boff[b];
+  }
+  vpre[nl] = (uint32_t)vt;
+  bpre[nl] = (uint32_t)bt;
+  DeviceGuard dg(g->device);
+  // queued work may still read the previous table
+  MK_CUDA(cudaDeviceSynchronize());
+  w->prepared = false;
+  MK_CHECK(w->ranges.reserve(host.size(), &g->device_bytes));
+  MK_CUDA(cudaMemcpy(w->ranges.ptr, host.data(), host.size() * 4, cudaMemcpyHostToDevice));
+  w->n_small = (uint32_t)ns;
+  w->n_large = (uint32_t)nl;
+  w->small_max = ns ? len(small_ids[0]) : 0;
+  w->large_vt = vt;
+  w->large_bt = bt;
+  w->small_grid = 0;
+  if (ns) {
+    const size_t smem = ((size_t)w->small_max * 2 + 15) & ~(size_t)15;
+    auto kern = g->weighted ? k_uf_members<true> : k_uf_members<false>;
+    MK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kLocalMax * 2)));
+    int per_sm = 0;
+    MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMemberThreads, smem));
+    w->small_grid = (int)std::min<uint64_t>(ns, (uint64_t)device_sm_count(g->device) * std::max(per_sm, 1));
+  }
+  w->prepared = true;
+  return MK_OK;
+}
+
+mk_status mk_wcc_static_prepared(mk_wcc *w, void *stream, float *ms_out) {
+  if (!w) return fail(MK_ERR_INVALID, "mk_wcc_static_prepared: null handle");
+  if (!w->prepared) return fail(MK_ERR_INVALID, "mk_wcc_static_prepared: no prepared ranges");
+  mk_graph *g = w->g;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(w->timer.start(s, ms_out != nullptr));
+  const GraphView v = g->view();
+  uint32_t *counter = w->ranges.ptr;
+  const uint32_t ns = w->n_small, nl = w->n_large;
+  if (ns) {
+    const size_t smem = ((size_t)w->small_max * 2 + 15) & ~(size_t)15;
+    const uint4 *rng = reinterpret_cast<const uint4 *>(w->ranges.ptr + 4);
+    MK_CUDA(cudaMemsetAsync(counter, 0, 4, s));
+    if (g->weighted)
+      k_uf_members<true><<<w->small_grid, kMemberThreads, smem, s>>>(v, rng, ns, counter, w->parent, w->err);
+    else
+      k_uf_members<false><<<w->small_grid, kMemberThreads, smem, s>>>(v, rng, ns, counter, w->parent, w->err);
+  }
+  if (nl) {
+    const uint32_t *dv = w->ranges.ptr + 4 + 4 * (size_t)ns, *dvb = dv + nl + 1;
+    const uint32_t *db = dvb + nl + 1, *dbb = db + nl + 1;
+    const int fg = flat_grid(w->large_vt, g->device);
+    k_uf_init_ranges<<<fg, 256, 0, s>>>(w->parent, dv, dvb, nl);
+    if (g->weighted)
+      k_uf_sample_ranges<true><<<fg, 256, 0, s>>>(v, w->parent, dv, dvb, nl, w->err);
+    else
+      k_uf_sample_ranges<false><<<fg, 256, 0, s>>>(v, w->parent, dv, dvb, nl, w->err);
+    k_uf_compress_ranges<<<fg, 256, 0, s>>>(w->parent, dv, dvb, nl);
+    const int blocks = (int)std::min<uint64_t>(w->large_bt * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+    if (g->weighted)
+      k_uf_edges_ranges<true><<<blocks, 256, 0, s>>>(v, w->parent, db, dbb, nl, w->err);
+    else
+      k_uf_edges_ranges<false><<<blocks, 256, 0, s>>>(v, w->parent, db, dbb, nl, w->err);
+    k_uf_compress_ranges<<<fg, 256, 0, s>>>(w->parent, dv, dvb, nl);
+  }
   MK_CUDA(cudaGetLastError());
   return w->timer.stop(ms_out);
 }
@@ -367,43 +542,8 @@ mk_status mk_wcc_static_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges, uint3
                                void *stream, float *ms_out) {
   if (!w || (nranges && !h_vertex_ranges))
     return fail(MK_ERR_INVALID, "mk_wcc_static_ranges: null argument");
-  mk_graph *g = w->g;
-  std::vector<uint32_t> host(4 * ((size_t)nranges + 1));
-  uint32_t *vpre = host.data(), *vbase = vpre + nranges + 1;
-  uint32_t *bpre = vbase + nranges + 1, *bbase = bpre + nranges + 1;
-  uint64_t vt = 0, bt = 0;
-  for (uint32_t r = 0; r < nranges; ++r) {
-    const uint32_t b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
-    if (b >= e || e > g->V) return fail(MK_ERR_INVALID, "mk_wcc_static_ranges: bad vertex range");
-    vpre[r] = (uint32_t)vt;
-    vbase[r] = b;
-    bpre[r] = (uint32_t)bt;
-    bbase[r] = g->h_boff[b];
-    vt += e - b;
-    bt += g->h_boff[e] - g->h_boff[b];
-  }
-  vpre[nranges] = (uint32_t)vt;
-  bpre[nranges] = (uint32_t)bt;
-  vbase[nranges] = bbase[nranges] = 0;
-  DeviceGuard dg(g->device);
-  cudaStream_t s = as_stream(stream);
-  MK_CHECK(w->timer.start(s, ms_out != nullptr));
-  if (nranges == 0) return w->timer.stop(ms_out);
-  MK_CHECK(w->ranges.reserve(host.size(), &g->device_bytes));
-  MK_CUDA(cudaMemcpyAsync(w->ranges.ptr, host.data(), host.size() * 4, cudaMemcpyHostToDevice, s));
-  // the host copy must outlive the asynchronous transfer
-  MK_CUDA(cudaStreamSynchronize(s));
-  const uint32_t *dv = w->ranges.ptr, *dvb = dv + nranges + 1;
-  const uint32_t *db = dvb + nranges + 1, *dbb = db + nranges + 1;
-  k_uf_init_ranges<<<flat_grid(vt, g->device), 256, 0, s>>>(w->parent, dv, dvb, nranges);
-  const int blocks = (int)std::min<uint64_t>(bt * 8 / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
-  if (g->weighted)
-    k_uf_edges_ranges<true><<<blocks, 256, 0, s>>>(g->view(), w->parent, db, dbb, nranges, w->err);
-  else
-    k_uf_edges_ranges<false><<<blocks, 256, 0, s>>>(g->view(), w->parent, db, dbb, nranges, w->err);
-  k_uf_compress_ranges<<<flat_grid(vt, g->device), 256, 0, s>>>(w->parent, dv, dvb, nranges);
-  MK_CUDA(cudaGetLastError());
-  return w->timer.stop(ms_out);
+  MK_CHECK(mk_wcc_prepare_ranges(w, h_vertex_ranges, nranges));
+  return mk_wcc_static_prepared(w, stream, ms_out);
 }
 
 mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d_dst,
@@ -466,8 +606,6 @@ mk_status mk_wcc_destroy(mk_wcc *w) {
   cudaFree(w->parent);
   cudaFree(w->aff_labels);
   cudaFree(w->aff_vertices);
-  cudaFree(w->err);
-  cudaFree(w->giant);
   w->ranges.release();
   delete w;
   return MK_OK;

@@ -245,3 +245,74 @@ def test_range_pagerank_matches_each_member():
     assert np.abs(prr.Values().astype(np.float64) - want).sum() <= 1e-6
     with pytest.raises(mk.MeerkatError):
         prr.Run(0, off[-1])  # larger than max_vertices
+
+
+def _random_member(V, E, rng):
+    s = rng.integers(0, V, E).astype(np.uint32)
+    d = rng.integers(0, V, E).astype(np.uint32)
+    keep = s != d
+    return s[keep], d[keep], rng.integers(1, 65, keep.sum()).astype(np.uint32)
+
+
+def test_wcc_prepared_ranges_shared_memory_and_device_wide_members():
+    """Members up to 65,536 vertices run in shared memory, larger ones through
+    the device-wide pass; both must give each member's own labels, also when
+    the prepared call is captured into a CUDA graph and replayed after an
+    update."""
+    import torch
+    rng = np.random.default_rng(91)
+    sizes = [65536, 70000, 3, 1, 20000, 1024, 4096]
+    mem = []
+    for m, V in enumerate(sizes):
+        if m == 5:  # no edges at all
+            s = d = w = np.zeros(0, np.uint32)
+        elif m == 6:  # one long path in a shuffled order: deep union trees
+            perm = rng.permutation(V).astype(np.uint32)
+            s, d = perm[:-1], perm[1:]
+            w = np.ones(V - 1, np.uint32)
+        else:  # sparse: many components
+            s, d, w = _random_member(V, max(1, int(V * 0.6)), rng)
+        mem.append((V, s, d, w))
+    S, oracles = build_set(mem)
+    off = S.offsets.astype(np.int64)
+    wcc = mk.WCC(S.graph)
+    ranges = [(off[m], off[m + 1]) for m in range(len(sizes))]
+    wcc.PrepareRanges(ranges)
+    wcc.StaticPrepared()
+    assert S.graph.sync() == 0
+
+    def check():
+        lab = wcc.Labels().astype(np.int64)
+        for m, O in enumerate(oracles):
+            np.testing.assert_array_equal(lab[off[m]:off[m + 1]] - off[m], O.wcc(), err_msg=str(m))
+    check()
+    # capture, update two members (one per path), replay
+    cs = torch.cuda.Stream()
+    cs.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=cs):
+        wcc.StaticPrepared(stream=cs, timed=False)
+    torch.cuda.synchronize()
+    for m in (1, 6):
+        V, s, d, _ = mem[m]
+        pick = rng.choice(len(s), size=len(s) // 5, replace=False)
+        S.graph.DeleteEdges(to_dev(s[pick] + off[m]), to_dev(d[pick] + off[m]))
+        oracles[m].delete(s[pick], d[pick])
+    assert S.graph.sync() == 0
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    assert S.graph.sync() == 0
+    check()
+    del g
+
+
+def test_wcc_range_not_closed_under_edges_is_reported():
+    S = mk.GraphSet([100, 100])
+    # an edge from member 0 into member 1 breaks the closure of member 0
+    S.graph.InsertEdges(to_dev(np.array([5, 7], np.uint32)), to_dev(np.array([150, 8], np.uint32)))
+    assert S.graph.sync() == 0
+    wcc = mk.WCC(S.graph)
+    wcc.StaticRanges([(0, 100)])
+    with pytest.raises(mk.MeerkatError, match="vertex range"):
+        S.graph.sync()
