@@ -520,7 +520,7 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         br.update(*both[(Wb + K + i) % 2])
         ev[1].record(stream)
         if br.bfs is not None:
-            br.bfs.Static(timed=False)
+            br.bfs.StaticMembers(timed=False)
         ev[2].record(stream)
         if br.wcc is not None:
             br.wcc.StaticPrepared(timed=False)

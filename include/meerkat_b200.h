@@ -232,6 +232,22 @@ mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, u
 mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev);
 /* float Static(EdgesN) (BFSImpl.cuh:590-662, SSSPImpl.cuh:607-690). */
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out);
+/* Static BFS of a multi-source traversal whose sources each lie in their own
+ * vertex range, each range closed under edges (members of a graph set):
+ * range i = [r[2i], r[2i+1]) holds source i.  prepare uploads the table
+ * (blocking; it waits for the device, since queued work may read the
+ * previous table); static_members runs it and issues only asynchronous work
+ * on `stream`, so it can be captured into a CUDA graph.  A range of at most
+ * 65,535 vertices is solved by one CTA with its BFS state in shared memory;
+ * larger ones by the device-wide kernel.  The distances of every vertex are
+ * those mk_traversal_static gives and the parents form a valid BFS tree
+ * (parents are not unique: of several equal-distance parents, the device-wide
+ * kernel keeps the first to arrive, the member kernel the smallest id); an
+ * edge leaving its range sets MK_DEVERR_INVALID_ID on the graph.  BFS only.
+ * No counterpart in the reference. */
+mk_status mk_bfs_prepare_members(mk_traversal *t, const uint32_t *h_vertex_ranges,
+                                 uint32_t nranges);
+mk_status mk_bfs_static_members(mk_traversal *t, void *stream, float *ms_out);
 /* float Incremental(src*, dst*, n) (BFSImpl.cuh:664-753, SSSPImpl.cuh:692-785).
  * d_w is accepted for the SSSP signature and ignored: the stored weight of
  * each edge is used. */

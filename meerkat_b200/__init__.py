@@ -345,6 +345,21 @@ class BFS(_Traversal):
     """BFS<AllocPolicy>(G, SourceVertex, VertexN) (include/Algorithms/BFS.cuh:13-69)."""
     _create = "mk_bfs_create"
 
+    def PrepareMembers(self, ranges):
+        """Uploads one vertex range [(begin, end), ...] per source, in source
+        order, for StaticMembers (blocking).  Each range holds its source and
+        is closed under edges (a GraphSet member)."""
+        r = np.ascontiguousarray(np.asarray(ranges, dtype=np.uint32).reshape(-1))
+        check(lib().mk_bfs_prepare_members(self._h, r.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                           len(r) // 2), "mk_bfs_prepare_members")
+
+    def StaticMembers(self, stream=None, timed=True):
+        """Static BFS over the prepared ranges: the distances of Static (and
+        a valid BFS tree), with a range of at most 65,535 vertices solved by
+        one CTA in shared memory.  Only asynchronous work on the stream
+        (capturable)."""
+        return self._call(lib().mk_bfs_static_members, self._h, _stream(stream), timed=timed)
+
 
 class SSSP(_Traversal):
     """SSSP<AllocPolicy>(G, SourceVertex, VertexN) (include/Algorithms/SSSP.cuh:11-69)."""

@@ -73,6 +73,8 @@ SIGNATURES = [
     ("mk_traversal_set_sources", _S, [vp, u32p, C.c_uint32]),
     ("mk_traversal_set_reverse", _S, [vp, vp]),
     ("mk_traversal_static", _S, [vp, vp, f32p]),
+    ("mk_bfs_prepare_members", _S, [vp, u32p, C.c_uint32]),
+    ("mk_bfs_static_members", _S, [vp, vp, f32p]),
     ("mk_traversal_incremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_traversal_decremental", _S, [vp, vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_traversal_distances", _S, [vp, vp]),

@@ -11,7 +11,9 @@ member's work is far too small to fill the GPU.  The batched runner keeps all
 members in one GraphSet and issues, per step,
 
   one delete launch and one insert launch for every member's batch,
-  one multi-source BFS (one source per BFS-queried member), and
+  one multi-source BFS (one source per BFS-queried member; a member of at
+  most 65,535 vertices is traversed by one CTA with its state in shared
+  memory), and
   one WCC launch over the WCC-queried members (a member of at most 65,536
   vertices is solved by one CTA with its union-find in shared memory),
 
@@ -31,6 +33,7 @@ from . import BFS, WCC, DynamicGraph, GraphSet
 
 QUERY_BFS, QUERY_WCC = 0, 1
 WCC_LOCAL_MAX = 1 << 16  # vertices of a member that one CTA solves in shared memory
+BFS_LOCAL_MAX = (1 << 16) - 1
 
 
 @dataclass
@@ -104,6 +107,10 @@ class BatchedRunner:
         glob = (off[self.bfs_members] + sources_local.astype(np.int64)).astype(np.uint32)
         self.sources_global = glob
         self.bfs = BFS(self.G, glob) if len(glob) else None
+        if self.bfs is not None:
+            self.bfs.PrepareMembers(np.stack([off[self.bfs_members], off[self.bfs_members + 1]], 1))
+        bsz = off[self.bfs_members + 1] - off[self.bfs_members]
+        self._bfs_large = int((bsz > BFS_LOCAL_MAX).sum())
         self.wcc = WCC(self.G) if len(self.wcc_members) else None
         sizes = off[self.wcc_members + 1] - off[self.wcc_members]
         self._wcc_large = int((sizes > WCC_LOCAL_MAX).sum())
@@ -116,7 +123,7 @@ class BatchedRunner:
 
     def query(self, stream=None):
         if self.bfs is not None:
-            self.bfs.Static(stream=stream, timed=False)
+            self.bfs.StaticMembers(stream=stream, timed=False)
         if self.wcc is not None:
             self.wcc.StaticPrepared(stream=stream, timed=False)
 
@@ -125,11 +132,13 @@ class BatchedRunner:
         self.query(stream=stream)
 
     def launches_per_step(self) -> int:
-        # kernels: delete, insert; BFS: 1 cooperative kernel (plus 2 memsets);
-        # WCC: 1 shared-memory kernel (plus 1 memset), and 5 device-wide
-        # kernels when some member is larger than shared memory holds
+        # kernels: delete, insert; BFS: 1 shared-memory kernel (plus 2
+        # memsets) and the cooperative device-wide kernel when some member is
+        # larger than shared memory holds; WCC: 1 shared-memory kernel (plus 1
+        # memset), and 5 device-wide kernels for such members
+        bfs = (1 + (1 if self._bfs_large else 0)) if self.bfs is not None else 0
         wcc = (1 + (5 if self._wcc_large else 0)) if self.wcc is not None else 0
-        return 2 + (1 if self.bfs is not None else 0) + wcc
+        return 2 + bfs + wcc
 
     def member_bfs(self, m_index: int, dist: Optional[np.ndarray] = None) -> np.ndarray:
         """BFS levels of the i-th BFS member (slice of the union result)."""

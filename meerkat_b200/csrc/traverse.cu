@@ -621,6 +621,146 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   }
 }
 
+
+// ---- static BFS of ranges held in shared memory ----
+// One CTA per range (a member of a graph set that holds one source): the
+// member's BFS state lives in shared memory -- a 16-bit parent per vertex
+// (0xFFFF: not reached) and a visited bitmap -- and its levels are separated
+// by block barriers instead of grid barriers.  A level's frontier is a list
+// of work items (vertex, chunk of buckets) in the range's slice of a device
+// array, so a hub's buckets spread over many 8-lane groups.  A newly reached
+// vertex keeps the smallest-id frontier vertex with an edge to it as its
+// parent (a 16-bit CAS minimum).  Distances equal the device-wide kernel's;
+// parents form a valid BFS tree, as there, where (as in the reference,
+// BFSImpl.cuh:311-314) the first of several equal-distance parents stays.
+// After each level the newly reached vertices get their packed word in
+// device memory, their visited bit and their work items.
+constexpr uint32_t kMemLocalMax = 65535;  // 0xFFFF marks "not reached"
+constexpr int kMemThreads = 1024;
+constexpr uint32_t kMemChunk = 4;  // buckets per work item (head slabs loaded together)
+
+// Buckets per work item of a vertex with nb buckets: the chunk index must fit
+// 16 bits.
+__device__ __forceinline__ uint32_t mem_chunk(uint32_t nb) {
+  return nb > 65536u * kMemChunk ? (nb + 65535u) / 65536u : kMemChunk;
+}
+
+// Lowers *p to v if v is smaller; true if this call replaced 0xFFFF.  Every
+// failed CAS means another thread lowered *p, so the loop ends within 65,536
+// rounds.
+__device__ __forceinline__ bool cas_min16_first(uint16_t *p, uint32_t v) {
+  volatile unsigned short *vp = p;
+  unsigned short cur = *vp;
+  for (uint32_t it = 0; it <= 65536u; ++it) {
+    if (v >= cur) return false;
+    const unsigned short prev =
+        atomicCAS(reinterpret_cast<unsigned short *>(p), cur, (unsigned short)v);
+    if (prev == cur) return cur == 0xFFFFu;
+    cur = prev;
+  }
+  return false;
+}
+
+// rng[r] = (first vertex, end vertex, first bucket, end bucket) of a range of
+// at most kMemLocalMax vertices, src[r] its source (global id).  items holds
+// one word per bucket of the graph, found one per vertex; range r uses their
+// slices [b0, b1) and [lo, hi).  dist must already hold INFINF.
+template <bool kW>
+__global__ void __launch_bounds__(kMemThreads, 1)
+    k_bfs_members(GraphView g, const uint4 *__restrict__ rng, const uint32_t *__restrict__ src,
+                  uint32_t nr, uint32_t *counter, unsigned long long *__restrict__ dist,
+                  uint32_t *__restrict__ items, uint32_t *__restrict__ found, uint32_t *err) {
+  extern __shared__ uint32_t smem[];
+  __shared__ uint32_t s_range, s_nfound, s_nitems;
+  const Lanes L = lanes();
+  const uint32_t group = threadIdx.x >> 3, ngroups = blockDim.x >> 3;
+  for (;;) {
+    if (threadIdx.x == 0) s_range = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t r = s_range;
+    if (r >= nr) break;
+    const uint4 R = rng[r];
+    const uint32_t lo = R.x, n = R.y - R.x, s0 = src[r] - lo;
+    const uint32_t nw = (n + 31) >> 5;
+    uint32_t *vis = smem;
+    uint16_t *par = reinterpret_cast<uint16_t *>(smem + nw);
+    uint32_t *q = items + R.z;  // capacity R.w - R.z: a vertex's items never exceed its buckets
+    uint32_t *fl = found + lo;  // capacity n: a vertex is reached once
+    for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x) vis[i] = 0u;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) par[i] = 0xFFFFu;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      par[s0] = (uint16_t)s0;
+      fl[0] = s0;
+      s_nfound = 1;
+      s_nitems = 0;
+    }
+    __syncthreads();
+    uint32_t fbeg = 0, ibeg = 0;
+    for (uint32_t level = 0; level <= n; ++level) {
+      // vertices reached at `level`: packed word, visited bit, work items
+      const uint32_t fend = s_nfound;
+      for (uint32_t i = fbeg + threadIdx.x; i < fend; i += blockDim.x) {
+        const uint32_t v = fl[i], gv = lo + v;
+        dist[gv] = pack(level, lo + par[v]);
+        atomicOr(vis + (v >> 5), 1u << (v & 31));
+        if (g.deg[gv] == 0) continue;
+        const uint32_t nb = g.boff[gv + 1] - g.boff[gv];
+        const uint32_t cs = mem_chunk(nb), nc = (nb + cs - 1) / cs;
+        const uint32_t pos = atomicAdd(&s_nitems, nc);
+        for (uint32_t c = 0; c < nc; ++c) q[pos + c] = v | (c << 16);
+      }
+      __syncthreads();
+      const uint32_t iend = s_nitems;
+      if (iend == ibeg) break;
+      // expand the items of `level`
+      for (uint32_t it = ibeg + group; it < iend; it += ngroups) {
+        const uint32_t item = q[it];
+        const uint32_t u = item & 0xFFFFu, gu = lo + u;
+        const uint32_t ub0 = g.boff[gu], nb = g.boff[gu + 1] - ub0, cs = mem_chunk(nb);
+        const uint32_t bb = ub0 + (item >> 16) * cs, be = min(bb + cs, ub0 + nb);
+        auto relax = [&](const uint4 x) {
+          uint32_t k[4], w[4];
+          lane_keys<kW>(x, L.gl, k, w);
+#pragma unroll
+          for (int t = 0; t < keys_per_lane<kW>(); ++t) {
+            if (k[t] >= kTombKey) continue;
+            const uint32_t v = k[t] - lo;
+            if (v >= n) {
+              atomicOr(err, kErrInvalidId);
+              continue;
+            }
+            if ((vis[v >> 5] >> (v & 31)) & 1u) continue;
+            if (cas_min16_first(par + v, u)) fl[atomicAdd(&s_nfound, 1u)] = v;
+          }
+        };
+        for (uint32_t b = bb; b < be; b += kMemChunk) {
+          const uint32_t m = min(kMemChunk, be - b);
+          uint4 hq[kMemChunk];
+#pragma unroll
+          for (uint32_t j = 0; j < kMemChunk; ++j)
+            if (j < m) hq[j] = ld_slab_ro(g.slabs + 8ull * (b + j) + L.gl);
+#pragma unroll
+          for (uint32_t j = 0; j < kMemChunk; ++j) {
+            if (j >= m) continue;
+            relax(hq[j]);
+            uint32_t nx = __shfl_sync(L.gmask, hq[j].w, L.gbase + 7);
+            while (nx != kNoSlab) {
+              const uint4 x = ld_slab_ro(g.slabs + 8ull * nx + L.gl);
+              relax(x);
+              nx = __shfl_sync(L.gmask, x.w, L.gbase + 7);
+            }
+          }
+        }
+      }
+      fbeg = fend;
+      ibeg = iend;
+      __syncthreads();
+    }
+    __syncthreads();  // shared memory and s_range are reused by the next range
+  }
+}
+
 }  // namespace mk
 
 using namespace mk;
@@ -642,6 +782,14 @@ struct mk_traversal {
   unsigned long long *pushed = nullptr;
   uint32_t *far0 = nullptr, *far1 = nullptr, *fbits = nullptr;  // near-far SSSP
   mk_graph *rev = nullptr;  // in-edges of the same graph, for pull levels (BFS)
+  std::vector<uint32_t> h_sources;
+  // prepared member table (BFS): counter word, uint4 (lo, hi, b0, b1) per
+  // small range (largest first), their sources, then the sources whose
+  // range is too large for shared memory
+  DevBuf<uint32_t> members;
+  uint32_t n_small = 0, n_large = 0, small_max = 0;
+  int small_grid = 0;
+  bool members_prepared = false;
   Timer timer;
 };
 
@@ -674,6 +822,7 @@ static mk_status trav_create(mk_graph *g, const uint32_t *h_sources, uint32_t ns
   t->nsources = nsrc;
   t->src_cap = nsrc;
   t->sssp = sssp;
+  t->h_sources.assign(h_sources, h_sources + nsrc);
   const size_t V = g->V;
   cudaError_t e = cudaSuccess;
   auto A = [&](void **p, size_t bytes) {
@@ -720,14 +869,10 @@ static mk_status trav_create(mk_graph *g, const uint32_t *h_sources, uint32_t ns
   return MK_OK;
 }
 
-static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
-                             const uint32_t *bd, uint32_t n, void *stream,
-                             float *ms_out) {
+// Issues one traversal launch (sources: t's own, or the given device list).
+static mk_status trav_issue(mk_traversal *t, uint32_t mode, const uint32_t *bs, const uint32_t *bd,
+                            uint32_t n, cudaStream_t s, const uint32_t *srcs, uint32_t nsrc) {
   mk_graph *g = t->g;
-  DeviceGuard dg(g->device);
-  cudaStream_t s = as_stream(stream);
-  if (n && (!bs || !bd)) return fail(MK_ERR_INVALID, "traversal: null batch");
-  MK_CHECK(t->timer.start(s, ms_out != nullptr));
   if (mode == kStatic) MK_CUDA(cudaMemsetAsync(t->dist, 0xFF, (size_t)g->V * 8, s));
   const uint32_t delta = (t->sssp && mode != kIncremental && t->far0) ? g->tuning.sssp_delta : 0u;
   if (delta) MK_CUDA(cudaMemsetAsync(t->fbits, 0, ((size_t)g->V + 31) / 32 * 4, s));
@@ -747,8 +892,8 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   a.bsrc = bs;
   a.bdst = bd;
   a.bn = n;
-  a.sources = t->sources;
-  a.nsources = t->nsources;
+  a.sources = srcs ? srcs : t->sources;
+  a.nsources = srcs ? nsrc : t->nsources;
   a.chunk = g->tuning.frontier_chunk ? g->tuning.frontier_chunk : kDefaultChunk;
   a.delta = delta;
   a.rg = t->rev ? t->rev->view() : GraphView{};
@@ -772,6 +917,17 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   if (t->nblocks == 0) t->nblocks = persistent_blocks(fn, kTravBlock, 0, g->device);
   void *args[] = {&a};
   MK_CUDA(cudaLaunchCooperativeKernel(fn, dim3(t->nblocks), dim3(kTravBlock), args, 0, s));
+  return MK_OK;
+}
+
+static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
+                             const uint32_t *bd, uint32_t n, void *stream,
+                             float *ms_out) {
+  DeviceGuard dg(t->g->device);
+  cudaStream_t s = as_stream(stream);
+  if (n && (!bs || !bd)) return fail(MK_ERR_INVALID, "traversal: null batch");
+  MK_CHECK(t->timer.start(s, ms_out != nullptr));
+  MK_CHECK(trav_issue(t, mode, bs, bd, n, s, nullptr, 0));
   MK_CHECK(t->timer.stop(ms_out));
   if (mode == kStatic) t->has_static = true;
   return MK_OK;
@@ -813,7 +969,9 @@ mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, u
   MK_CUDA(cudaDeviceSynchronize());
   MK_CUDA(cudaMemcpy(t->sources, h_sources, (size_t)n * 4, cudaMemcpyHostToDevice));
   t->nsources = n;
+  t->h_sources.assign(h_sources, h_sources + n);
   t->has_static = false;
+  t->members_prepared = false;
   return MK_OK;
 }
 
@@ -833,6 +991,105 @@ mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev) {
 mk_status mk_traversal_static(mk_traversal *t, void *stream, float *ms_out) {
   if (!t) return fail(MK_ERR_INVALID, "mk_traversal_static: null handle");
   return trav_launch(t, kStatic, nullptr, nullptr, 0, stream, ms_out);
+}
+
+mk_status mk_bfs_prepare_members(mk_traversal *t, const uint32_t *h_vertex_ranges,
+                                 uint32_t nranges) {
+  const char *what = "mk_bfs_prepare_members";
+  if (!t || (nranges && !h_vertex_ranges)) return fail(MK_ERR_INVALID, std::string(what) + ": null argument");
+  if (t->sssp) return fail(MK_ERR_INVALID, std::string(what) + ": BFS only");
+  if (nranges != t->nsources)
+    return fail(MK_ERR_INVALID, std::string(what) + ": need one range per source");
+  mk_graph *g = t->g;
+  std::vector<uint32_t> small_ids, large_src;
+  std::vector<std::pair<uint32_t, uint32_t>> spans;
+  for (uint32_t r = 0; r < nranges; ++r) {
+    const uint32_t b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
+    if (b >= e || e > g->V) return fail(MK_ERR_INVALID, std::string(what) + ": bad vertex range");
+    if (t->h_sources[r] < b || t->h_sources[r] >= e)
+      return fail(MK_ERR_INVALID, std::string(what) + ": source outside its range");
+    spans.emplace_back(b, e);
+    if (e - b <= kMemLocalMax)
+      small_ids.push_back(r);
+    else
+      large_src.push_back(t->h_sources[r]);
+  }
+  std::sort(spans.begin(), spans.end());
+  for (size_t i = 1; i < spans.size(); ++i)
+    if (spans[i].first < spans[i - 1].second)
+      return fail(MK_ERR_INVALID, std::string(what) + ": overlapping ranges");
+  auto len = [&](uint32_t r) { return h_vertex_ranges[2 * r + 1] - h_vertex_ranges[2 * r]; };
+  std::stable_sort(small_ids.begin(), small_ids.end(),
+                   [&](uint32_t a, uint32_t b) { return len(a) > len(b); });
+  const size_t ns = small_ids.size(), nl = large_src.size();
+  std::vector<uint32_t> host(4 + 5 * ns + nl, 0u);
+  uint32_t *tab = host.data() + 4, *ssrc = tab + 4 * ns, *lsrc = ssrc + ns;
+  for (size_t i = 0; i < ns; ++i) {
+    const uint32_t r = small_ids[i], b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
+    tab[4 * i + 0] = b;
+    tab[4 * i + 1] = e;
+    tab[4 * i + 2] = g->h_boff[b];
+    tab[4 * i + 3] = g->h_boff[e];
+    ssrc[i] = t->h_sources[r];
+  }
+  std::copy(large_src.begin(), large_src.end(), lsrc);
+  DeviceGuard dg(g->device);
+  // queued work may still read the previous table
+  MK_CUDA(cudaDeviceSynchronize());
+  t->members_prepared = false;
+  MK_CHECK(t->members.reserve(host.size(), &g->device_bytes));
+  MK_CUDA(cudaMemcpy(t->members.ptr, host.data(), host.size() * 4, cudaMemcpyHostToDevice));
+  t->n_small = (uint32_t)ns;
+  t->n_large = (uint32_t)nl;
+  t->small_max = ns ? len(small_ids[0]) : 0;
+  t->small_grid = 0;
+  if (ns) {
+    const size_t smem = (((size_t)t->small_max + 31) / 32) * 4 + (((size_t)t->small_max * 2 + 15) & ~(size_t)15);
+    auto kern = g->weighted ? k_bfs_members<true> : k_bfs_members<false>;
+    const int most = (int)((kMemLocalMax + 31) / 32 * 4 + ((kMemLocalMax * 2 + 15) & ~15u));
+    MK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+    int per_sm = 0;
+    MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMemThreads, smem));
+    t->small_grid = (int)std::min<uint64_t>(ns, (uint64_t)device_sm_count(g->device) * std::max(per_sm, 1));
+  }
+  t->members_prepared = true;
+  return MK_OK;
+}
+
+mk_status mk_bfs_static_members(mk_traversal *t, void *stream, float *ms_out) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_bfs_static_members: null handle");
+  if (!t->members_prepared) return fail(MK_ERR_INVALID, "mk_bfs_static_members: no prepared ranges");
+  mk_graph *g = t->g;
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(t->timer.start(s, ms_out != nullptr));
+  const uint32_t ns = t->n_small, nl = t->n_large;
+  uint32_t *counter = t->members.ptr;
+  const uint4 *tab = reinterpret_cast<const uint4 *>(counter + 4);
+  const uint32_t *ssrc = counter + 4 + 4 * (size_t)ns, *lsrc = ssrc + ns;
+  if (nl) {
+    // ranges too large for shared memory: the device-wide kernel from their
+    // sources (it also resets every distance)
+    MK_CHECK(trav_issue(t, kStatic, nullptr, nullptr, 0, s, lsrc, nl));
+  } else {
+    MK_CUDA(cudaMemsetAsync(t->dist, 0xFF, (size_t)g->V * 8, s));
+    MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
+  }
+  if (ns) {
+    const size_t smem = (((size_t)t->small_max + 31) / 32) * 4 + (((size_t)t->small_max * 2 + 15) & ~(size_t)15);
+    MK_CUDA(cudaMemsetAsync(counter, 0, 4, s));
+    uint32_t *items = reinterpret_cast<uint32_t *>(t->fr0);
+    if (g->weighted)
+      k_bfs_members<true><<<t->small_grid, kMemThreads, smem, s>>>(g->view(), tab, ssrc, ns, counter, t->dist,
+                                                                   items, t->inv_list, g->err_word());
+    else
+      k_bfs_members<false><<<t->small_grid, kMemThreads, smem, s>>>(g->view(), tab, ssrc, ns, counter, t->dist,
+                                                                    items, t->inv_list, g->err_word());
+    MK_CUDA(cudaGetLastError());
+  }
+  MK_CHECK(t->timer.stop(ms_out));
+  t->has_static = true;
+  return MK_OK;
 }
 
 mk_status mk_traversal_incremental(mk_traversal *t, const uint32_t *d_src,
@@ -908,6 +1165,7 @@ mk_status mk_traversal_destroy(mk_traversal *t) {
   cudaFree(t->far0);
   cudaFree(t->far1);
   cudaFree(t->fbits);
+  t->members.release();
   delete t;
   return MK_OK;
 }

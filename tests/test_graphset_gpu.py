@@ -316,3 +316,106 @@ def test_wcc_range_not_closed_under_edges_is_reported():
     wcc.StaticRanges([(0, 100)])
     with pytest.raises(mk.MeerkatError, match="vertex range"):
         S.graph.sync()
+
+
+def test_bfs_static_members_equals_device_wide_static():
+    """The shared-memory member BFS gives the distances of the device-wide
+    static BFS and a valid BFS tree (parents are not unique: the reference's
+    relaxation keeps the first of equal-distance parents, BFSImpl.cuh:311-314),
+    for members at the shared-memory limit, above it (device-wide path), tiny,
+    edgeless and deep; the dynamic calls that follow it stay exact; a captured
+    replay after an update matches a fresh static run."""
+    import torch
+    rng = np.random.default_rng(92)
+    sizes = [65535, 70000, 3, 1, 20000, 1024, 4096, 300]
+    mem = []
+    for m, V in enumerate(sizes):
+        if m == 5:
+            s = d = w = np.zeros(0, np.uint32)
+        elif m == 6:  # a shuffled path: 4095 levels
+            perm = rng.permutation(V).astype(np.uint32)
+            s, d = perm[:-1], perm[1:]
+            w = np.ones(V - 1, np.uint32)
+        else:
+            s, d, w = _random_member(V, max(1, int(V * 3)), rng)
+        mem.append((V, s, d, w))
+    S, oracles = build_set(mem)
+    off = S.offsets.astype(np.int64)
+    src_local = []
+    for m, (V, s, d, _) in enumerate(mem):
+        if m == 6:
+            src_local.append(int(s[0]))  # the head of the path
+        else:
+            src_local.append(int(np.argmax(np.bincount(s, minlength=V))) if len(s) else 0)
+    sources = [int(off[m] + v) for m, v in enumerate(src_local)]
+    ranges = [(off[m], off[m + 1]) for m in range(len(sizes))]
+    bfs = mk.BFS(S.graph, sources)
+    bfs.Static()
+    want = bfs.Distances()
+    bfs.PrepareMembers(ranges)
+    bfs.StaticMembers()
+    assert S.graph.sync() == 0
+    dist = bfs.Distances()
+    np.testing.assert_array_equal(dist, want)
+    packed = bfs.packed()
+    for m, O in enumerate(oracles):
+        np.testing.assert_array_equal(dist[off[m]:off[m + 1]], O.bfs(src_local[m]), err_msg=str(m))
+        assert O.check_parents(src_local[m], local_packed(packed, off[m], off[m + 1]),
+                               weighted=False) == 0, m
+    # a decremental call after the member static: tree edges of two members
+    del_s, del_d = [], []
+    for m in (0, 6):
+        V, s, d, _ = mem[m]
+        lp = local_packed(packed, off[m], off[m + 1])
+        par = (lp & np.uint64(0xFFFFFFFF)).astype(np.int64)
+        tree = np.nonzero((lp != INFINF) & (par != np.arange(V)))[0]
+        pick = rng.choice(tree, size=min(16, len(tree)), replace=False)
+        oracles[m].delete(par[pick].astype(np.uint32), pick.astype(np.uint32))
+        del_s.append(par[pick] + off[m])
+        del_d.append(pick + off[m])
+    tds = to_dev(np.concatenate(del_s).astype(np.uint32))
+    tdd = to_dev(np.concatenate(del_d).astype(np.uint32))
+    S.graph.DeleteEdges(tds, tdd)
+    assert S.graph.sync() == 0
+    bfs.Decremental(tds, tdd)
+    dist = bfs.Distances()
+    for m in (0, 6):
+        np.testing.assert_array_equal(dist[off[m]:off[m + 1]], oracles[m].bfs(src_local[m]))
+    # captured member static, replayed after an insert batch
+    cs = torch.cuda.Stream()
+    cs.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=cs):
+        bfs.StaticMembers(stream=cs, timed=False)
+    torch.cuda.synchronize()
+    V, s, d, _ = mem[4]
+    es = mk.EdgeSet(V, s, d)
+    is_, id_ = es.sample_absent(2000, seed=5)
+    S.graph.InsertEdges(to_dev(is_ + off[4]), to_dev(id_ + off[4]),
+                        vals=to_dev(np.ones(len(is_), np.uint32)))
+    assert S.graph.sync() == 0
+    oracles[4].insert(is_, id_, np.ones(len(is_), np.uint32))
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
+    got = bfs.Distances()
+    del g
+    np.testing.assert_array_equal(got[off[4]:off[5]], oracles[4].bfs(src_local[4]))
+    bfs.Static()
+    np.testing.assert_array_equal(got, bfs.Distances())
+
+
+def test_bfs_prepare_members_rejects_bad_tables():
+    S = mk.GraphSet([10, 10, 10], weighted=True)
+    bfs = mk.BFS(S.graph, [1, 12])
+    with pytest.raises(mk.MeerkatError):
+        bfs.PrepareMembers([(0, 10)])                 # one range per source
+    with pytest.raises(mk.MeerkatError):
+        bfs.PrepareMembers([(0, 10), (20, 30)])       # source 12 outside (20, 30)
+    with pytest.raises(mk.MeerkatError):
+        bfs.PrepareMembers([(0, 15), (10, 20)])       # overlapping
+    with pytest.raises(mk.MeerkatError):
+        bfs.StaticMembers()                           # nothing prepared
+    sssp = mk.SSSP(S.graph, [1])
+    with pytest.raises((mk.MeerkatError, AttributeError)):
+        sssp.PrepareMembers([(0, 10)])
