@@ -1396,6 +1396,41 @@ mk_status mk_graph_export_csr_range(mk_graph *g, uint32_t v_begin, uint32_t v_en
   return MK_OK;
 }
 
+}  // extern "C"
+
+namespace mk {
+
+mk_status export_csr_grow(mk_graph *g, DevBuf<unsigned long long> &row_ptr, DevBuf<uint32_t> &col,
+                          cudaStream_t s, uint64_t *h_edges, size_t *bytes_acc) {
+  const uint32_t nb = (uint32_t)g->num_buckets;
+  MK_CHECK(g->bucket_cnt.reserve(nb, &g->device_bytes));
+  MK_CHECK(g->bucket_pos.reserve((size_t)nb + 1, &g->device_bytes));
+  MK_CHECK(row_ptr.reserve((size_t)g->V + 1, bytes_acc));
+  GraphView v = g->view();
+  const int blocks = group_grid(nb, g->device);
+  if (g->weighted)
+    k_bucket_live<true><<<blocks, 256, 0, s>>>(v, g->bucket_cnt.ptr);
+  else
+    k_bucket_live<false><<<blocks, 256, 0, s>>>(v, g->bucket_cnt.ptr);
+  MK_CHECK(scan_u32_to_u64(g->bucket_cnt.ptr, g->bucket_pos.ptr, nb, g->scan_tmp, s));
+  unsigned long long total = 0;
+  MK_CUDA(cudaMemcpyAsync(&total, g->bucket_pos.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  MK_CHECK(col.reserve(std::max<unsigned long long>(total, 1), bytes_acc));
+  k_rows_from_buckets<<<(g->V + 256) / 256, 256, 0, s>>>(g->boff, g->V, nb, g->bucket_pos.ptr, row_ptr.ptr);
+  if (g->weighted)
+    k_bucket_fill<true><<<blocks, 256, 0, s>>>(v, g->bucket_pos.ptr, col.ptr, nullptr);
+  else
+    k_bucket_fill<false><<<blocks, 256, 0, s>>>(v, g->bucket_pos.ptr, col.ptr, nullptr);
+  MK_CUDA(cudaGetLastError());
+  *h_edges = total;
+  return MK_OK;
+}
+
+}  // namespace mk
+
+extern "C" {
+
 mk_status mk_graph_export_csr(mk_graph *g, uint64_t *d_row_ptr, uint32_t *d_col,
                               uint32_t *d_w, void *stream) {
   if (!g || !d_row_ptr || !d_col) return fail(MK_ERR_INVALID, "mk_graph_export_csr: null argument");

@@ -92,6 +92,12 @@ mk_status scan_u32_to_u64(const uint32_t *d_in, unsigned long long *d_out,
                           uint32_t n, DevBuf<unsigned long long> &tmp,
                           cudaStream_t s);
 
+// CSR (row offsets, column ids in slab order) of the whole graph into
+// buffers that grow to fit; the live edge count comes back to the host
+// between the count and the fill (the call synchronises the stream).
+mk_status export_csr_grow(mk_graph *g, DevBuf<unsigned long long> &row_ptr, DevBuf<uint32_t> &col,
+                          cudaStream_t s, uint64_t *h_edges, size_t *bytes_acc);
+
 // Number of co-resident blocks for a persistent cooperative launch.
 int persistent_blocks(const void *kernel, int block, size_t smem, int device);
 

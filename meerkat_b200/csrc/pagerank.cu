@@ -9,15 +9,26 @@
 //                 from the previous ranks after adjusting out-degrees
 //                 (PageRankImpl.cuh:222-251).
 //
-// B200 design: the whole solve is one cooperative launch.  Each iteration
-// is one pull pass over fixed work items (chunks of up to 32 buckets of one
-// vertex, 8-lane group per item, 16-byte slab loads, 4-byte gathers of c[]
-// which stays L2 resident) that also writes the next contributions and
-// accumulates |delta| and the dangling mass.  A vertex with one item is
-// finished in that pass; hubs with several items combine the item partials
-// in a second, fixed-order pass.  Bounded grid barriers separate the passes.  All sums are Kahan-compensated FP32 in
-// a fixed order (per-lane, 8-lane butterfly, per-block tree, per-grid fixed
-// order), so a solve is deterministic for a given slab layout.
+// B200 design: a solve first compacts the reverse graph into CSR (column ids
+// in slab order; the graph does not change during a solve), then runs as one
+// cooperative launch.  Slab buckets of low-degree vertices are mostly empty
+// 128-byte lines, so a pull straight over the slabs reads several times the
+// edge bytes and is latency bound; over CSR every iteration streams 4 bytes
+// per edge (evict-first, so c[] and the ranks stay in L2) plus 4-byte gathers
+// of c[].  An iteration is one pull pass that also writes the next
+// contributions and accumulates |delta| and the dangling mass:
+//   * vertices of in-degree <= kPrFlat: a warp takes 32 consecutive ones and
+//     walks the concatenation of their rows 32 edges per step (coalesced
+//     column loads, several steps in flight), a segmented warp scan giving
+//     each vertex its share of every step;
+//   * hubs (in-degree > kPrFlat) are split into work items of kPrChunk
+//     in-edges, one warp per item, and combine their item partials in a
+//     second, fixed-order pass.
+// Item and multi-item lists are built per solve by scans, not atomics.
+// Bounded grid barriers separate the passes.  All sums are Kahan-compensated
+// FP32 in a fixed order (segmented warp scans, per-lane, warp butterfly,
+// per-block tree, per-grid fixed order), so a solve is deterministic for a
+// given slab layout.
 //
 // Stopping rule: `tol` is read as the L1 error target.  The iteration is a
 // d-contraction in L1, so after a step with change delta the remaining error
@@ -59,13 +70,14 @@ __device__ __forceinline__ Kahan shfl_xor_kahan(const Kahan &k, uint32_t mask, i
 enum PrCtl : int { kPBar0 = 0, kPBar1 = 1, kPErr = 2, kPIters = 3, kPCur = 4, kPCtlWords = 8 };
 
 struct PrArgs {
-  GraphView g;       // reverse graph
-  const uint32_t *item_b0;   // first bucket of each work item (items of a vertex are contiguous)
-  const uint32_t *item_off;  // V+1: items of vertex u are [item_off[u], item_off[u+1])
-  const uint32_t *multi;     // vertices with more than one item
-  uint32_t nitems;
-  uint32_t nmulti;
-  float *ipart;      // per-item Kahan partials (s, c) = 2 * nitems
+  uint32_t V;
+  const unsigned long long *rp;    // V+1 CSR row offsets of the reverse graph
+  const uint32_t *col;             // in-neighbours, row by row
+  const unsigned long long *ioff;  // V+1: items of vertex u are [ioff[u], ioff[u+1]); ioff[V] = items
+  const uint32_t *item_v;          // vertex of each item (items of a vertex are contiguous)
+  const unsigned long long *moff;  // V+1: moff[V] = vertices with several items
+  const uint32_t *multi;           // those vertices, in increasing id order
+  float *ipart;      // per-item Kahan partials (s, c) = 2 * items
   float *pr0, *pr1;
   float *c0, *c1;
   const uint32_t *outdeg;
@@ -140,38 +152,35 @@ __device__ __forceinline__ float grid_total(const float *p) {
   return r;
 }
 
-constexpr uint32_t kPrChunk = 32;  // buckets per work item
+constexpr uint32_t kPrFlat = 256;   // in-degree up to which the flat pass sums a vertex
+constexpr uint32_t kPrChunk = 256;  // in-edges per work item of a hub (in-degree > kPrFlat)
+constexpr int kPrSteps = 4;         // 32-edge steps of the flat pass whose loads are in flight together
 
-// Kahan sum of contributions over buckets [b0, b1) (group-cooperative).
-template <bool kW>
-__device__ __forceinline__ Kahan pull_range(const GraphView &g, const Lanes &L, uint32_t b0,
-                                            uint32_t b1, const float *__restrict__ c) {
-  Kahan acc;
-  walk_buckets(g, L, b0, b1, [&](const uint4 &q) {
-    uint32_t k[4], w[4];
-    lane_keys<kW>(q, L.gl, k, w);
+// Segmented inclusive sum across the warp: lanes with equal keys form
+// contiguous runs, and each lane ends with the sum of its run up to itself
+// (a fixed tree order).
+__device__ __forceinline__ float seg_scan(float v, uint32_t key, uint32_t lane) {
 #pragma unroll
-    for (int i = 0; i < keys_per_lane<kW>(); ++i)
-      if (k[i] < kTombKey) acc.add(__ldcg(c + k[i]));  // c is rewritten every iteration
-  });
-#pragma unroll
-  for (int o = 4; o > 0; o >>= 1) acc.merge(shfl_xor_kahan(acc, L.gmask, o));
-  return acc;
+  for (int s = 1; s < 32; s <<= 1) {
+    const float y = __shfl_up_sync(0xFFFFFFFFu, v, s);
+    const uint32_t ky = __shfl_up_sync(0xFFFFFFFFu, key, s);
+    if (lane >= (uint32_t)s && ky == key) v += y;
+  }
+  return v;
 }
 
-template <bool kW>
 __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
-  const Lanes L = lanes();
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t nthreads = gridDim.x * blockDim.x;
-  const uint32_t group = tid >> 3;
-  const uint32_t ngroups = nthreads >> 3;
-  const uint32_t V = a.g.V;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t wid = tid >> 5, nwarps = nthreads >> 5;
+  const uint32_t V = a.V;
   const uint32_t nb = gridDim.x;
-  float *pr[2] = {a.pr0, a.pr1};
-  float *cb[2] = {a.c0, a.c1};
+  auto pr = [&](uint32_t k) { return k ? a.pr1 : a.pr0; };
+  auto cb = [&](uint32_t k) { return k ? a.c1 : a.c0; };
   auto part = [&](uint32_t parity, uint32_t kind) { return a.part + ((parity * 2 + kind) * 2) * nb; };
   uint32_t cur = a.cur;
+  const unsigned long long nitems = a.ioff[V], nmulti = a.moff[V];
   const float d = a.damping;
   const float invV = 1.0f / (float)V;
 
@@ -180,8 +189,8 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
     Kahan dang, zero;
     for (uint32_t u = tid; u < V; u += nthreads) {
       uint32_t od = a.outdeg[u];
-      float p = pr[cur][u];
-      cb[cur][u] = od ? p / (float)od : 0.0f;
+      float p = pr(cur)[u];
+      cb(cur)[u] = od ? p / (float)od : 0.0f;
       if (!od) dang.add(p);
     }
     block_reduce2(dang, zero, part(0, 0), part(0, 1));
@@ -193,12 +202,12 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
     const uint32_t rp = it & 1u, wp = rp ^ 1u;
     const float dangling = grid_total(part(rp, 0));
     const float base = (1.0f - d) * invV + d * (dangling * invV);
-    const float *c = cb[cur];
-    const float *pold = pr[cur];
-    float *pnew = pr[cur ^ 1];
-    float *cnew = cb[cur ^ 1];
+    const float *c = cb(cur);
+    const float *pold = pr(cur);
+    float *pnew = pr(cur ^ 1);
+    float *cnew = cb(cur ^ 1);
     Kahan kd, kdang;
-    auto finalize = [&](uint32_t u, float sum) {  // lane 0 of a group
+    auto finalize = [&](uint32_t u, float sum) {
       float nv = base + d * sum;
       pnew[u] = nv;
       kd.add(fabsf(nv - __ldcg(pold + u)));
@@ -206,37 +215,103 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
       cnew[u] = od ? nv / (float)od : 0.0f;
       if (!od) kdang.add(nv);
     };
-    // pass A: every work item; a vertex with a single item is finished here
-    for (uint32_t i = group; i < a.nitems; i += ngroups) {
-      const uint32_t b0 = a.item_b0[i];
-      const uint32_t u = a.g.bowner[b0];
-      const uint32_t b1 = min(a.g.boff[u + 1], b0 + kPrChunk);
-      Kahan acc = pull_range<kW>(a.g, L, b0, b1, c);
-      if (L.gl == 0) {
-        if (a.item_off[u + 1] - a.item_off[u] == 1) {
-          finalize(u, acc.value());
-        } else {
-          a.ipart[2 * i] = acc.s;
-          a.ipart[2 * i + 1] = acc.c;
+    // pass A, flat: a warp takes 32 consecutive vertices and walks the
+    // concatenation of their in-edge rows (hubs excluded) 32 edges per step,
+    // kPrSteps steps with their loads in flight together; a segmented scan
+    // hands every vertex the sum of its part of each step
+    for (uint32_t vb = wid * 32u; vb < V; vb += nwarps * 32u) {
+      const uint32_t u = vb + lane;
+      unsigned long long j0 = 0;
+      uint32_t dl = 0;
+      bool mine = false;
+      if (u < V) {
+        j0 = a.rp[u];
+        const unsigned long long dd = a.rp[u + 1] - j0;
+        mine = dd <= kPrFlat;
+        dl = mine ? (uint32_t)dd : 0u;
+      }
+      uint32_t incl = dl;
+#pragma unroll
+      for (int s2 = 1; s2 < 32; s2 <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, s2);
+        if (lane >= (uint32_t)s2) incl += y;
+      }
+      const uint32_t off = incl - dl;
+      const uint32_t T = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      const unsigned long long basej = j0 - off;  // edge x of the run of lane l is col[basej(l) + x]
+      Kahan acc;
+      for (uint32_t t0 = 0; t0 < T; t0 += 32u * kPrSteps) {
+        uint32_t own[kPrSteps], kc[kPrSteps];
+        float val[kPrSteps];
+#pragma unroll
+        for (int q = 0; q < kPrSteps; ++q) {
+          const uint32_t x = t0 + 32u * q + lane;
+          uint32_t lo = 0;  // last lane whose run starts at or before x
+#pragma unroll
+          for (int st = 16; st > 0; st >>= 1) {
+            const uint32_t cand = lo + (uint32_t)st;
+            if (__shfl_sync(0xFFFFFFFFu, off, cand) <= x) lo = cand;
+          }
+          const unsigned long long bj = __shfl_sync(0xFFFFFFFFu, basej, lo);
+          own[q] = x < T ? lo : 32u;
+          kc[q] = x < T ? __ldcs(a.col + (bj + x)) : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < kPrSteps; ++q) val[q] = own[q] < 32u ? __ldca(c + kc[q]) : 0.0f;
+#pragma unroll
+        for (int q = 0; q < kPrSteps; ++q) {
+          const float sv = seg_scan(val[q], own[q], lane);
+          const uint32_t sb = t0 + 32u * q;
+          const bool hit = dl && off < sb + 32u && off + dl > sb;
+          const uint32_t last = hit ? min(off + dl, sb + 32u) - 1u - sb : 0u;
+          const float tot = __shfl_sync(0xFFFFFFFFu, sv, last);
+          if (hit) acc.add(tot);
         }
       }
+      if (mine) finalize(u, acc.value());
     }
-    if (a.nmulti) {
+    // pass A, hubs: one warp per work item of kPrChunk in-edges
+    for (unsigned long long i = wid; i < nitems; i += nwarps) {
+      const uint32_t u = a.item_v[i];
+      const unsigned long long j0 = a.rp[u] + (i - a.ioff[u]) * kPrChunk;
+      const unsigned long long j1 = min(j0 + kPrChunk, a.rp[u + 1]);
+      constexpr int kPer = (int)(kPrChunk / 32);
+      uint32_t kc[kPer];
+      float x[kPer];
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) {
+        const unsigned long long j = j0 + 32u * q + lane;
+        kc[q] = j < j1 ? __ldcs(a.col + j) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < kPer; ++q) x[q] = (j0 + 32u * q + lane < j1) ? __ldca(c + kc[q]) : 0.0f;
+      Kahan acc;
+#pragma unroll
+      for (int q = 0; q < kPer; ++q)
+        if (j0 + 32u * q + lane < j1) acc.add(x[q]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc.merge(shfl_xor_kahan(acc, 0xFFFFFFFFu, o));
+      if (lane == 0) {
+        a.ipart[2 * i] = acc.s;
+        a.ipart[2 * i + 1] = acc.c;
+      }
+    }
+    if (nmulti) {
       if (!grid_barrier(a.ctl + kPBar0, a.ctl + kPErr, a.limit_ns)) return;
-      // pass B: vertices with several items combine their partials in order
-      for (uint32_t m = group; m < a.nmulti; m += ngroups) {
+      // pass B: every hub combines its item partials in order
+      for (unsigned long long m = wid; m < nmulti; m += nwarps) {
         const uint32_t u = a.multi[m];
-        const uint32_t i0 = a.item_off[u], i1 = a.item_off[u + 1];
+        const unsigned long long i0 = a.ioff[u], i1 = a.ioff[u + 1];
         Kahan acc;
-        for (uint32_t i = i0 + L.gl; i < i1; i += 8) {
+        for (unsigned long long i = i0 + lane; i < i1; i += 32) {
           Kahan t;
           t.s = __ldcg(a.ipart + 2 * i);
           t.c = __ldcg(a.ipart + 2 * i + 1);
           acc.merge(t);
         }
 #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) acc.merge(shfl_xor_kahan(acc, L.gmask, o));
-        if (L.gl == 0) finalize(u, acc.value());
+        for (int o = 16; o > 0; o >>= 1) acc.merge(shfl_xor_kahan(acc, 0xFFFFFFFFu, o));
+        if (lane == 0) finalize(u, acc.value());
       }
     }
     block_reduce2(kdang, kd, part(wp, 0), part(wp, 1));
@@ -278,6 +353,30 @@ __global__ void k_outdeg_count(GraphView g, uint32_t *outdeg) {
   }
 }
 
+// work items per vertex: ceil(in-degree / kPrChunk) for a hub (in-degree
+// above kPrFlat, so at least two items), else 0; flag = hub
+__global__ void k_pr_item_counts(const unsigned long long *__restrict__ rp, uint32_t V,
+                                 uint32_t *__restrict__ cnt, uint32_t *__restrict__ mflag) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < V; u += gridDim.x * blockDim.x) {
+    const unsigned long long d = rp[u + 1] - rp[u];
+    const uint32_t c = d > kPrFlat ? (uint32_t)((d + kPrChunk - 1) / kPrChunk) : 0u;
+    cnt[u] = c;
+    mflag[u] = c > 1 ? 1u : 0u;
+  }
+}
+
+__global__ void k_pr_item_fill(const uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ ioff,
+                               const unsigned long long *__restrict__ moff, uint32_t V,
+                               uint32_t *__restrict__ item_v, uint32_t *__restrict__ multi) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < V; u += gridDim.x * blockDim.x) {
+    const uint32_t c = cnt[u];
+    if (!c) continue;
+    const unsigned long long o = ioff[u];
+    for (uint32_t j = 0; j < c; ++j) item_v[o + j] = u;
+    if (c > 1) multi[moff[u]] = u;
+  }
+}
+
 __global__ void k_fill(float *p, uint32_t n, float v) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
@@ -294,9 +393,10 @@ struct mk_pagerank {
   uint32_t *outdeg = nullptr;
   float *part = nullptr;
   float *delta = nullptr;
-  uint32_t *item_b0 = nullptr, *item_off = nullptr, *multi = nullptr;
-  float *ipart = nullptr;
-  uint32_t nitems = 0, nmulti = 0;
+  // per-solve CSR of the reverse graph and its work items
+  DevBuf<unsigned long long> rp, ioff, moff, scan_tmp;
+  DevBuf<uint32_t> col, cnt, mflag, item_v, multi;
+  DevBuf<float> ipart;
   uint32_t *ctl = nullptr;
   uint32_t cur = 0;  // host mirror of the buffer with the latest ranks
   int nblocks = 0;
@@ -315,9 +415,36 @@ static mk_status pr_recount_outdeg(mk_pagerank *p, cudaStream_t s) {
   return MK_OK;
 }
 
+// CSR of the reverse graph and the work items of this solve.
+static mk_status pr_prepare(mk_pagerank *p, cudaStream_t s) {
+  mk_graph *g = p->g;
+  const uint32_t V = g->V;
+  uint64_t E = 0;
+  MK_CHECK(export_csr_grow(g, p->rp, p->col, s, &E, nullptr));
+  MK_CHECK(p->cnt.reserve(V));
+  MK_CHECK(p->mflag.reserve(V));
+  MK_CHECK(p->ioff.reserve((size_t)V + 1));
+  MK_CHECK(p->moff.reserve((size_t)V + 1));
+  // a vertex with items has more than kPrFlat in-edges, and
+  // ceil(d / kPrChunk) <= d / kPrChunk + 1
+  const size_t heavy_cap = E / (kPrFlat + 1) + 1;
+  const size_t item_cap = E / kPrChunk + heavy_cap;
+  MK_CHECK(p->item_v.reserve(item_cap));
+  MK_CHECK(p->multi.reserve(heavy_cap));
+  MK_CHECK(p->ipart.reserve(2 * item_cap));
+  const int fb = (int)std::min<uint64_t>((uint64_t)V / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  k_pr_item_counts<<<fb, 256, 0, s>>>(p->rp.ptr, V, p->cnt.ptr, p->mflag.ptr);
+  MK_CHECK(scan_u32_to_u64(p->cnt.ptr, p->ioff.ptr, V, p->scan_tmp, s));
+  MK_CHECK(scan_u32_to_u64(p->mflag.ptr, p->moff.ptr, V, p->scan_tmp, s));
+  k_pr_item_fill<<<fb, 256, 0, s>>>(p->cnt.ptr, p->ioff.ptr, p->moff.ptr, V, p->item_v.ptr, p->multi.ptr);
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
+}
+
 static mk_status pr_solve(mk_pagerank *p, cudaStream_t s) {
   mk_graph *g = p->g;
-  const void *fn = g->weighted ? (const void *)k_pagerank<true> : (const void *)k_pagerank<false>;
+  MK_CHECK(pr_prepare(p, s));
+  const void *fn = (const void *)k_pagerank;
   if (p->nblocks == 0) {
     p->nblocks = persistent_blocks(fn, kPrBlock, 0, g->device);
     cudaError_t e = cudaMalloc(&p->part, (size_t)p->nblocks * 8 * sizeof(float));
@@ -325,13 +452,14 @@ static mk_status pr_solve(mk_pagerank *p, cudaStream_t s) {
   }
   MK_CUDA(cudaMemsetAsync(p->ctl, 0, kPCtlWords * 4, s));
   PrArgs a;
-  a.g = g->view();
-  a.item_b0 = p->item_b0;
-  a.item_off = p->item_off;
-  a.multi = p->multi;
-  a.nitems = p->nitems;
-  a.nmulti = p->nmulti;
-  a.ipart = p->ipart;
+  a.V = g->V;
+  a.rp = p->rp.ptr;
+  a.col = p->col.ptr;
+  a.ioff = p->ioff.ptr;
+  a.item_v = p->item_v.ptr;
+  a.moff = p->moff.ptr;
+  a.multi = p->multi.ptr;
+  a.ipart = p->ipart.ptr;
   a.pr0 = p->pr0;
   a.pr1 = p->pr1;
   a.c0 = p->c0;
@@ -382,24 +510,6 @@ mk_status mk_pagerank_create(mk_graph *g_rev, float damping, float tol,
   A((void **)&p->outdeg, V * 4);
   A((void **)&p->delta, 4);
   A((void **)&p->ctl, kPCtlWords * 4);
-  // fixed work items: chunks of kPrChunk buckets, contiguous per vertex
-  std::vector<uint32_t> ib0, ioff(V + 1), mul;
-  for (uint32_t u = 0; u < V; ++u) {
-    ioff[u] = (uint32_t)ib0.size();
-    const uint32_t lo = g_rev->h_boff[u], hi = g_rev->h_boff[u + 1];
-    for (uint32_t b = lo; b < hi; b += kPrChunk) ib0.push_back(b);
-    if (hi - lo > kPrChunk) mul.push_back(u);
-  }
-  ioff[V] = (uint32_t)ib0.size();
-  p->nitems = (uint32_t)ib0.size();
-  p->nmulti = (uint32_t)mul.size();
-  A((void **)&p->item_b0, ib0.size() * 4);
-  A((void **)&p->item_off, ioff.size() * 4);
-  A((void **)&p->multi, std::max<size_t>(mul.size(), 1) * 4);
-  A((void **)&p->ipart, ib0.size() * 8);
-  if (e == cudaSuccess) e = cudaMemcpy(p->item_b0, ib0.data(), ib0.size() * 4, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(p->item_off, ioff.data(), ioff.size() * 4, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && !mul.empty()) e = cudaMemcpy(p->multi, mul.data(), mul.size() * 4, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     mk_pagerank_destroy(p);
     return cuda_fail(e, "mk_pagerank_create");
@@ -524,10 +634,16 @@ mk_status mk_pagerank_destroy(mk_pagerank *p) {
   cudaFree(p->part);
   cudaFree(p->delta);
   cudaFree(p->ctl);
-  cudaFree(p->item_b0);
-  cudaFree(p->item_off);
-  cudaFree(p->multi);
-  cudaFree(p->ipart);
+  p->rp.release();
+  p->ioff.release();
+  p->moff.release();
+  p->scan_tmp.release();
+  p->col.release();
+  p->cnt.release();
+  p->mflag.release();
+  p->item_v.release();
+  p->multi.release();
+  p->ipart.release();
   delete p;
   return MK_OK;
 }
