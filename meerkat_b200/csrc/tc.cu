@@ -145,7 +145,8 @@ __device__ __forceinline__ bool set_contains_cg(const uint32_t *set, uint32_t ca
   }
 }
 
-constexpr uint32_t kTcChunk = 32;  // N+(u) entries per work item
+constexpr uint32_t kTcChunk = 32;  // N+(u) entries per work item (one per lane)
+constexpr int kTcSteps = 4;        // 32-entry probe steps with their loads in flight together
 
 // Work items of the forward algorithm: (u, chunk c) covers N+(u)[32c, 32c+32).
 // Per-vertex work is heavy-tailed (a hub's neighbours have long N+ lists),
@@ -177,8 +178,9 @@ __global__ void k_tc_item_fill(uint32_t V, const uint32_t *__restrict__ icnt,
 }
 
 // Persistent warps take work items from a global counter.  For item (u, c)
-// the warp stages N+(u) in a shared-memory hash set and streams N+(v) for the
-// item's 32 neighbours v with coalesced reads, probing the set.
+// the warp stages N+(u) in a shared-memory hash set and streams the N+(v)
+// lists of the item's 32 neighbours v as one concatenated range with
+// coalesced reads, probing the set.
 __global__ void __launch_bounds__(kTcWarps * 32)
     k_tc_small(const unsigned long long *__restrict__ orow, const uint32_t *__restrict__ ocol,
                const unsigned long long *__restrict__ items, const unsigned long long *nitems_p,
@@ -209,12 +211,43 @@ __global__ void __launch_bounds__(kTcWarps * 32)
       __syncwarp();
       have_u = u;
     }
-    const uint32_t i0 = chunk * kTcChunk, i1 = min(du, i0 + kTcChunk);
-    for (uint32_t i = i0; i < i1; ++i) {
-      const uint32_t v = ocol[r0 + i];
-      const unsigned long long s0 = orow[v], s1 = orow[v + 1];
-      for (unsigned long long j = s0 + lane; j < s1; j += 32)
-        c += set_contains(set, cap - 1, ocol[j]);
+    // the item's (up to 32) neighbours v, one per lane; their N+(v) lists
+    // are walked as one concatenated range, 32 entries per step and
+    // kTcSteps steps of loads in flight, so short lists do not idle lanes
+    const uint32_t i0 = chunk * kTcChunk, m = min(du, i0 + kTcChunk) - i0;
+    unsigned long long s0 = 0;
+    uint32_t len = 0;
+    if (lane < m) {
+      const uint32_t v = ocol[r0 + i0 + lane];
+      s0 = orow[v];
+      len = (uint32_t)(orow[v + 1] - s0);
+    }
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    const uint32_t off = incl - len;
+    const uint32_t T = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    const unsigned long long basej = s0 - off;  // entry x of lane l's list is ocol[basej(l) + x]
+    for (uint32_t x0 = 0; x0 < T; x0 += 32u * kTcSteps) {
+      uint32_t key[kTcSteps];
+#pragma unroll
+      for (int q = 0; q < kTcSteps; ++q) {
+        const uint32_t x = x0 + 32u * q + lane;
+        uint32_t lo = 0;  // last lane whose list starts at or before x
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1) {
+          const uint32_t cand = lo + (uint32_t)st;
+          if (__shfl_sync(0xFFFFFFFFu, off, cand) <= x) lo = cand;
+        }
+        const unsigned long long bj = __shfl_sync(0xFFFFFFFFu, basej, lo);
+        key[q] = x < T ? ocol[bj + x] : kEmptyKey;
+      }
+#pragma unroll
+      for (int q = 0; q < kTcSteps; ++q)
+        if (key[q] != kEmptyKey) c += set_contains(set, cap - 1, key[q]);
     }
   }
 #pragma unroll
