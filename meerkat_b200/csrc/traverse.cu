@@ -264,14 +264,19 @@ __device__ __forceinline__ void expand_range(const TravArgs &a, const Lanes &L,
       q[j] = ((uint32_t)j < nq) ? ld_slab_ro(a.g.slabs + 8ull * (b + j) + L.gl)
                                 : make_uint4(kEmptyKey, kEmptyKey, kEmptyKey, kNoSlab);
     relax_slabs4<kW, kUseW>(a, L, Q, nf, q, nq, u, du, stamp_next, gfr, gsz);
+    // overflow chains level by level: the next slabs of all running chains
+    // are loaded together (a finished chain contributes an empty slab)
+    uint32_t nx[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      uint32_t s = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
-      while (s != kNoSlab) {
-        const uint4 r = ld_slab_ro(a.g.slabs + 8ull * s + L.gl);
-        relax_slab<kW, kUseW>(a, L, Q, nf, r, u, du, stamp_next, gfr, gsz, false);
-        s = __shfl_sync(L.gmask, r.w, L.gbase + 7);
-      }
+    for (int j = 0; j < 4; ++j) nx[j] = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
+    while ((nx[0] & nx[1] & nx[2] & nx[3]) != kNoSlab) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        q[j] = nx[j] != kNoSlab ? ld_slab_ro(a.g.slabs + 8ull * nx[j] + L.gl)
+                                : make_uint4(kEmptyKey, kEmptyKey, kEmptyKey, kNoSlab);
+      relax_slabs4<kW, kUseW>(a, L, Q, nf, q, 4u, u, du, stamp_next, gfr, gsz);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) nx[j] = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
     }
   }
 }
@@ -734,24 +739,8 @@ __global__ void __launch_bounds__(kMemThreads, 1)
             if (cas_min16_first(par + v, u)) fl[atomicAdd(&s_nfound, 1u)] = v;
           }
         };
-        for (uint32_t b = bb; b < be; b += kMemChunk) {
-          const uint32_t m = min(kMemChunk, be - b);
-          uint4 hq[kMemChunk];
-#pragma unroll
-          for (uint32_t j = 0; j < kMemChunk; ++j)
-            if (j < m) hq[j] = ld_slab_ro(g.slabs + 8ull * (b + j) + L.gl);
-#pragma unroll
-          for (uint32_t j = 0; j < kMemChunk; ++j) {
-            if (j >= m) continue;
-            relax(hq[j]);
-            uint32_t nx = __shfl_sync(L.gmask, hq[j].w, L.gbase + 7);
-            while (nx != kNoSlab) {
-              const uint4 x = ld_slab_ro(g.slabs + 8ull * nx + L.gl);
-              relax(x);
-              nx = __shfl_sync(L.gmask, x.w, L.gbase + 7);
-            }
-          }
-        }
+        for (uint32_t b = bb; b < be; b += kMemChunk)
+          walk4_levels(g, L, b, min(kMemChunk, be - b), [&](uint32_t, const uint4 x) { relax(x); });
       }
       fbeg = fend;
       ibeg = iend;

@@ -292,40 +292,24 @@ __global__ void __launch_bounds__(kMemberThreads, 1)
     __syncthreads();
     for (uint32_t b = R.z + group * kMemberHeads; b < R.w; b += ngroups * kMemberHeads) {
       const uint32_t m = min(kMemberHeads, R.w - b);
-      uint4 q[kMemberHeads];
       uint32_t own[kMemberHeads];
 #pragma unroll
-      for (uint32_t j = 0; j < kMemberHeads; ++j)
-        if (j < m) {
-          q[j] = ld_slab_ro(g.slabs + 8ull * (b + j) + L.gl);
-          own[j] = __ldg(g.bowner + b + j) - lo;
-        }
+      for (uint32_t j = 0; j < kMemberHeads; ++j) own[j] = j < m ? __ldg(g.bowner + b + j) - lo : 0u;
+      walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 x) {
+        const uint32_t u = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
+        uint32_t k[4], w[4];
+        lane_keys<kW>(x, L.gl, k, w);
 #pragma unroll
-      for (uint32_t j = 0; j < kMemberHeads; ++j) {
-        if (j >= m) continue;
-        const uint32_t u = own[j];
-        auto link = [&](const uint4 x) {
-          uint32_t k[4], w[4];
-          lane_keys<kW>(x, L.gl, k, w);
-#pragma unroll
-          for (int t = 0; t < keys_per_lane<kW>(); ++t) {
-            if (k[t] >= kTombKey) continue;
-            const uint32_t v = k[t] - lo;
-            if (v >= n || u >= n) {
-              atomicOr(err, kErrInvalidId);
-              continue;
-            }
-            if (v != u) ls_union(sp, u, v, err);
+        for (int t = 0; t < keys_per_lane<kW>(); ++t) {
+          if (k[t] >= kTombKey) continue;
+          const uint32_t v = k[t] - lo;
+          if (v >= n || u >= n) {
+            atomicOr(err, kErrInvalidId);
+            continue;
           }
-        };
-        link(q[j]);
-        uint32_t nx = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
-        while (nx != kNoSlab) {
-          const uint4 x = ld_slab_ro(g.slabs + 8ull * nx + L.gl);
-          link(x);
-          nx = __shfl_sync(L.gmask, x.w, L.gbase + 7);
+          if (v != u) ls_union(sp, u, v, err);
         }
-      }
+      });
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) labels[lo + i] = lo + ls_root(sp, i);
