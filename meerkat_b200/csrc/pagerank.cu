@@ -129,27 +129,51 @@ __device__ __forceinline__ void block_reduce2(Kahan a, Kahan b, float *pa, float
   __syncthreads();
 }
 
-// Fixed-order grid reduction of one partial array (done redundantly by every
-// block's warp 0, so every block sees the same value).
-__device__ __forceinline__ float grid_total(const float *p) {
-  __shared__ float res;
-  uint32_t nb = gridDim.x;
+// Fixed-order grid reductions of two partial arrays at once (done
+// redundantly by every block's warp 0, so every block sees the same values);
+// each lane has four blocks' partials in flight at a time.
+__device__ __forceinline__ void grid_totals(const float *p, const float *q, float &tp, float &tq) {
+  __shared__ float res[2];
+  const uint32_t nb = gridDim.x;
   if (threadIdx.x < 32) {
-    Kahan k;
-    for (uint32_t i = threadIdx.x; i < nb; i += 32) {
-      Kahan t;
-      t.s = __ldcg(p + i);
-      t.c = __ldcg(p + nb + i);
-      k.merge(t);
+    Kahan kp, kq;
+    for (uint32_t i0 = threadIdx.x; i0 < nb; i0 += 128) {
+      float ps[4], pc[4], qs[4], qc[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint32_t i = i0 + 32u * r;
+        const bool ok = i < nb;
+        ps[r] = ok ? __ldcg(p + i) : 0.f;
+        pc[r] = ok ? __ldcg(p + nb + i) : 0.f;
+        qs[r] = ok ? __ldcg(q + i) : 0.f;
+        qc[r] = ok ? __ldcg(q + nb + i) : 0.f;
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (i0 + 32u * r >= nb) continue;
+        Kahan t;
+        t.s = ps[r];
+        t.c = pc[r];
+        kp.merge(t);
+        t.s = qs[r];
+        t.c = qc[r];
+        kq.merge(t);
+      }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) k.merge(shfl_xor_kahan(k, 0xFFFFFFFFu, o));
-    if (threadIdx.x == 0) res = k.value();
+    for (int o = 16; o > 0; o >>= 1) {
+      kp.merge(shfl_xor_kahan(kp, 0xFFFFFFFFu, o));
+      kq.merge(shfl_xor_kahan(kq, 0xFFFFFFFFu, o));
+    }
+    if (threadIdx.x == 0) {
+      res[0] = kp.value();
+      res[1] = kq.value();
+    }
   }
   __syncthreads();
-  float r = res;
+  tp = res[0];
+  tq = res[1];
   __syncthreads();
-  return r;
 }
 
 constexpr uint32_t kPrFlat = 256;   // in-degree up to which the flat pass sums a vertex
@@ -197,10 +221,10 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
     if (!grid_barrier(a.ctl + kPBar0, a.ctl + kPErr, a.limit_ns)) return;
   }
   uint32_t it = 0;
-  float delta = 0.f;
+  float delta = 0.f, dangling = 0.f, unused = 0.f;
+  grid_totals(part(0, 0), part(0, 1), dangling, unused);
   while (it < a.max_iter) {
     const uint32_t rp = it & 1u, wp = rp ^ 1u;
-    const float dangling = grid_total(part(rp, 0));
     const float base = (1.0f - d) * invV + d * (dangling * invV);
     const float *c = cb(cur);
     const float *pold = pr(cur);
@@ -316,7 +340,8 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
     }
     block_reduce2(kdang, kd, part(wp, 0), part(wp, 1));
     if (!grid_barrier(a.ctl + kPBar0, a.ctl + kPErr, a.limit_ns)) return;
-    delta = grid_total(part(wp, 1));
+    // this iteration's |delta| and the next one's dangling mass in one pass
+    grid_totals(part(wp, 1), part(wp, 0), delta, dangling);
     cur ^= 1u;
     ++it;
     if (delta <= a.stop_delta) break;

@@ -114,35 +114,48 @@ constexpr int kTcWarps = 4;           // warps per block in the small kernel (32
 constexpr int kTcSetCap = 2048;       // per-warp shared hash capacity (entries)
 constexpr uint32_t kTcSmallMax = 1024;  // N+(u) handled by one warp
 
-__device__ __forceinline__ void set_insert(uint32_t *set, uint32_t cap_mask, uint32_t key) {
-  uint32_t h = mix32(key) & cap_mask;
-  while (true) {
+// Open-addressing sets of capacity 2^k (k >= 6), at most half full, with
+// Fibonacci hashing: the slot is the top k bits of key * 2654435769 (one
+// multiply and one shift per probe; the sets are probed far more often than
+// built).  shift = 32 - k.  Probes are bounded by the capacity.
+__device__ __forceinline__ uint32_t set_slot(uint32_t key, uint32_t shift) {
+  return (key * 2654435769u) >> shift;
+}
+
+__device__ __forceinline__ void set_insert(uint32_t *set, uint32_t cap_mask, uint32_t shift,
+                                           uint32_t key) {
+  uint32_t h = set_slot(key, shift);
+  for (uint32_t it = 0; it <= cap_mask; ++it) {
     uint32_t old = atomicCAS(set + h, kEmptyKey, key);
     if (old == kEmptyKey || old == key) return;
     h = (h + 1) & cap_mask;
   }
 }
 
-__device__ __forceinline__ bool set_contains(const uint32_t *set, uint32_t cap_mask, uint32_t key) {
-  uint32_t h = mix32(key) & cap_mask;
-  while (true) {
+__device__ __forceinline__ bool set_contains(const uint32_t *set, uint32_t cap_mask, uint32_t shift,
+                                             uint32_t key) {
+  uint32_t h = set_slot(key, shift);
+  for (uint32_t it = 0; it <= cap_mask; ++it) {
     uint32_t k = set[h];
     if (k == key) return true;
     if (k == kEmptyKey) return false;
     h = (h + 1) & cap_mask;
   }
+  return false;
 }
 
 // Same probe for a set in global memory, read through L2 (the set is
 // rebuilt for every vertex, so L1 may hold stale lines).
-__device__ __forceinline__ bool set_contains_cg(const uint32_t *set, uint32_t cap_mask, uint32_t key) {
-  uint32_t h = mix32(key) & cap_mask;
-  while (true) {
+__device__ __forceinline__ bool set_contains_cg(const uint32_t *set, uint32_t cap_mask,
+                                                uint32_t shift, uint32_t key) {
+  uint32_t h = set_slot(key, shift);
+  for (uint32_t it = 0; it <= cap_mask; ++it) {
     uint32_t k = __ldcg(set + h);
     if (k == key) return true;
     if (k == kEmptyKey) return false;
     h = (h + 1) & cap_mask;
   }
+  return false;
 }
 
 constexpr uint32_t kTcChunk = 32;  // N+(u) entries per work item (one per lane)
@@ -153,14 +166,16 @@ constexpr int kTcSteps = 4;        // 32-entry probe steps with their loads in f
 // so vertices are split into chunks and handed out dynamically.  Vertices
 // with N+(u) larger than kTcSmallMax go to the big list instead.
 __global__ void k_tc_item_count(uint32_t V, const unsigned long long *__restrict__ orow,
-                                uint32_t *__restrict__ icnt, uint32_t *big_list, uint32_t *big_n) {
+                                uint32_t *__restrict__ icnt, uint32_t *big_list, uint32_t *big_n,
+                                uint32_t *big_max) {
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < V; u += gridDim.x * blockDim.x) {
     const uint32_t du = (uint32_t)(orow[u + 1] - orow[u]);
     uint32_t c = 0;
     if (du >= 2) {  // a triangle needs two oriented edges out of u
-      if (du > kTcSmallMax)
+      if (du > kTcSmallMax) {
         big_list[atomicAdd(big_n, 1u)] = u;
-      else
+        atomicMax(big_max, du);
+      } else
         c = (du + kTcChunk - 1) / kTcChunk;
     }
     icnt[u] = c;
@@ -207,13 +222,14 @@ __global__ void __launch_bounds__(kTcWarps * 32)
       while (cap < 2 * du) cap <<= 1;
       for (uint32_t i = lane; i < cap; i += 32) set[i] = kEmptyKey;
       __syncwarp();
-      for (uint32_t i = lane; i < du; i += 32) set_insert(set, cap - 1, ocol[r0 + i]);
+      for (uint32_t i = lane; i < du; i += 32) set_insert(set, cap - 1, __clz(cap) + 1, ocol[r0 + i]);
       __syncwarp();
       have_u = u;
     }
     // the item's (up to 32) neighbours v, one per lane; their N+(v) lists
     // are walked as one concatenated range, 32 entries per step and
     // kTcSteps steps of loads in flight, so short lists do not idle lanes
+    const uint32_t shift = __clz(cap) + 1;
     const uint32_t i0 = chunk * kTcChunk, m = min(du, i0 + kTcChunk) - i0;
     unsigned long long s0 = 0;
     uint32_t len = 0;
@@ -247,7 +263,7 @@ __global__ void __launch_bounds__(kTcWarps * 32)
       }
 #pragma unroll
       for (int q = 0; q < kTcSteps; ++q)
-        if (key[q] != kEmptyKey) c += set_contains(set, cap - 1, key[q]);
+        if (key[q] != kEmptyKey) c += set_contains(set, cap - 1, shift, key[q]);
     }
   }
 #pragma unroll
@@ -271,13 +287,14 @@ __global__ void k_tc_big(const unsigned long long *__restrict__ orow,
     while (cp < 2 * du && cp < cap) cp <<= 1;
     for (uint32_t i = threadIdx.x; i < cp; i += blockDim.x) set[i] = kEmptyKey;
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < du; i += blockDim.x) set_insert(set, cp - 1, ocol[r0 + i]);
+    const uint32_t shift = __clz(cp) + 1;
+    for (uint32_t i = threadIdx.x; i < du; i += blockDim.x) set_insert(set, cp - 1, shift, ocol[r0 + i]);
     __syncthreads();
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (uint32_t i = warp; i < du; i += nw) {
       const uint32_t v = ocol[r0 + i];
       const unsigned long long s0 = orow[v], s1 = orow[v + 1];
-      for (unsigned long long j = s0 + lane; j < s1; j += 32) c += set_contains_cg(set, cp - 1, ocol[j]);
+      for (unsigned long long j = s0 + lane; j < s1; j += 32) c += set_contains_cg(set, cp - 1, shift, ocol[j]);
     }
     __syncthreads();
   }
@@ -497,14 +514,18 @@ static mk_status tc_static(mk_tc *t, cudaStream_t s) {
     k_orient_fill<false><<<blocks, 256, 0, s>>>(gv, t->bpos.ptr, t->ocol.ptr);
   MK_CHECK(t->big_list.reserve(V, &acc));
   MK_CUDA(cudaMemsetAsync(t->dcount, 0, 8, s));
-  MK_CUDA(cudaMemsetAsync(t->small, 0, 8, s));  // [0] big count, [1] work-item counter
+  // [0] big count, [1] work-item counter, [2] largest big oriented degree
+  MK_CUDA(cudaMemsetAsync(t->small, 0, 16, s));
   // work items (the orientation scratch is free again: ocnt >= V words,
   // bpos >= V + 1)
   const int vb = (int)std::min<uint64_t>((uint64_t)V / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
-  k_tc_item_count<<<vb, 256, 0, s>>>(V, t->orow.ptr, t->ocnt.ptr, t->big_list.ptr, t->small);
+  k_tc_item_count<<<vb, 256, 0, s>>>(V, t->orow.ptr, t->ocnt.ptr, t->big_list.ptr, t->small,
+                                     t->small + 2);
   MK_CHECK(scan_u32_to_u64(t->ocnt.ptr, t->bpos.ptr, V, t->tmp, s));
   unsigned long long nitems = 0;
+  uint32_t hs[4] = {0, 0, 0, 0};  // [0] big vertices, [2] their largest oriented degree
   MK_CUDA(cudaMemcpyAsync(&nitems, t->bpos.ptr + V, 8, cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaMemcpyAsync(hs, t->small, 16, cudaMemcpyDeviceToHost, s));
   MK_CUDA(cudaStreamSynchronize(s));
   MK_CHECK(t->items.reserve(std::max<unsigned long long>(nitems, 1), &acc));
   k_tc_item_fill<<<vb, 256, 0, s>>>(V, t->ocnt.ptr, t->bpos.ptr, t->items.ptr);
@@ -514,15 +535,10 @@ static mk_status tc_static(mk_tc *t, cudaStream_t s) {
   k_tc_small<<<sblocks, kTcWarps * 32, 0, s>>>(t->orow.ptr, t->ocol.ptr, t->items.ptr,
                                               t->bpos.ptr + V, t->small + 1, t->dcount);
   // big vertices: one block each, global-memory set
-  uint32_t nbig = 0;
-  MK_CUDA(cudaMemcpyAsync(&nbig, t->small, 4, cudaMemcpyDeviceToHost, s));
-  MK_CUDA(cudaStreamSynchronize(s));
+  const uint32_t nbig = hs[0];
   if (nbig) {
-    // capacity: next power of two >= 2 * max oriented degree
-    std::vector<unsigned long long> rows((size_t)V + 1);
-    MK_CUDA(cudaMemcpy(rows.data(), t->orow.ptr, rows.size() * 8, cudaMemcpyDeviceToHost));
-    uint32_t mx = 0;
-    for (uint32_t u = 0; u < V; ++u) mx = std::max<uint32_t>(mx, (uint32_t)(rows[u + 1] - rows[u]));
+    // capacity: next power of two >= 2 * largest oriented degree of a big vertex
+    const uint32_t mx = hs[2];
     uint32_t cap = 64;
     while (cap < 2ull * mx) cap <<= 1;
     int bb = std::min<uint32_t>(nbig, (uint32_t)device_sm_count(g->device) * 2);
