@@ -38,7 +38,6 @@ constexpr uint32_t kErrOom = 0x2u;
 constexpr uint32_t kErrTimeout = 0x4u;
 constexpr uint32_t kErrOverflow = 0x8u;
 
-constexpr int kGroup = 8;  // lanes per slab probe (8 x 16 B = 128 B)
 
 // Device view of one dynamic graph.  Passed by value to kernels.
 struct GraphView {
@@ -82,9 +81,6 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t key, uint32_t nb) {
   return __umulhi(mix32(key), nb);
 }
 
-// 16-byte slab load that bypasses L1 (L2 is the coherence point for the
-// concurrent CAS traffic of the update kernels).
-__device__ __forceinline__ uint4 ld_slab_cg(const uint4 *p) { return __ldcg(p); }
 // Read-only slab load for traversals (graph is not mutated during them).
 __device__ __forceinline__ uint4 ld_slab_ro(const uint4 *p) { return __ldg(p); }
 
@@ -97,12 +93,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
   uint32_t v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 
@@ -232,15 +222,6 @@ __device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t *p, unsigned lo
 __device__ __forceinline__ void red_add_hint_u32(uint32_t *p, uint32_t v, unsigned long long pol) {
   asm volatile("red.global.add.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol)
                : "memory");
-}
-// Bulk copy global -> shared with an L2 cache policy (no multicast).
-__device__ __forceinline__ void bulk_load_hint(void *dst_smem, const void *src_gmem, uint32_t bytes,
-                                               uint64_t *bar, unsigned long long policy) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
-      "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst_smem)),
-      "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
-      : "memory");
 }
 // Orders this thread's earlier generic-proxy shared accesses before later
 // async-proxy (TMA) writes to the same buffer.

@@ -45,12 +45,6 @@ __device__ __forceinline__ void probe_slab(const uint4 &q, uint32_t key,
   next = __shfl_sync(L.gmask, q.w, L.gbase + 7);
 }
 
-// Word index of key slot `slot`.
-template <bool kWeighted>
-__device__ __forceinline__ uint32_t slot_word(uint32_t slot) {
-  return kWeighted ? 2 * slot : slot;
-}
-
 // Group-cooperative membership test of (u, v) (u = the vertex whose table is
 // probed).  Returns found; *val gets the stored value for map slabs.
 template <bool kWeighted>
