@@ -161,8 +161,9 @@ def make_workload(n_batches: int):
     return (s, d, w), batches
 
 
-def cpu_baseline(graph, batches, max_batches=3):
-    """The oracle (C, OpenMP, one thread per host core) applying mixed batches."""
+def cpu_baseline(graph, batches, max_batches=3, warmup=0):
+    """The oracle (C, OpenMP, one thread per host core) applying mixed batches:
+    `warmup` untimed batches, then up to `max_batches` timed ones."""
     from oracle import OracleGraph
     s, d, w = graph
     T = os.cpu_count() or 1
@@ -170,9 +171,12 @@ def cpu_baseline(graph, batches, max_batches=3):
     t0 = time.time()
     O.insert(s, d, w)
     log(f"[bench] oracle load {time.time() - t0:.1f}s on {T} threads")
+    for (ds, dd, is_, id_, iw) in batches[:warmup]:
+        O.delete(ds, dd)
+        O.insert(is_, id_, iw)
     times = []
     applied = 0
-    for (ds, dd, is_, id_, iw) in batches[:max_batches]:
+    for (ds, dd, is_, id_, iw) in batches[warmup:warmup + max_batches]:
         t0 = time.perf_counter()
         n1, _ = O.delete(ds, dd)
         n2, _ = O.insert(is_, id_, iw)
@@ -331,12 +335,13 @@ def run_reference(args, rank, world):
     the host cores on the same config and metric."""
     if rank != 0:
         return 0
-    graph, batches = make_workload(args.steps + args.warmup)
-    cb = cpu_baseline(graph, batches, max_batches=min(len(batches), max(args.steps, 1)))
+    K = max(args.steps, 1)
+    graph, batches = make_workload(K + args.warmup)
+    cb = cpu_baseline(graph, batches, max_batches=K, warmup=args.warmup)
     v = cb["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC,
-            "n_gpus": args.gpus, "steps": min(len(batches), args.steps), "warmup": 0,
-            "ms_per_step": 1000.0 * cb["seconds"] / max(1, min(len(batches), args.steps)),
+            "n_gpus": args.gpus, "steps": K, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * cb["seconds"] / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "config": config_block(args.gpus),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
