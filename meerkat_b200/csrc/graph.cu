@@ -439,7 +439,16 @@ __device__ __forceinline__ UpdPending upd_decide_probe(const GraphView &g, const
       if (kWeighted) atomicMin(slab + pr.found_word + 1, r.wt);  // live edge: upsert-min
     } else if (pr.empty_word < 32) {
       p.word = pr.empty_word;
-      p.old = atomicCAS(slab + pr.empty_word, kEmptyKey, r.v);
+      if (kWeighted) {
+        // key and weight share one 8-byte pair (key word even): one 64-bit
+        // CAS installs both.  A never-used slot is EMPTY in both words; a key
+        // placed by the two-step chain walk (key CAS, then atomicMin) makes
+        // this CAS fail and return that key.
+        unsigned long long *pw = reinterpret_cast<unsigned long long *>(slab + pr.empty_word);
+        p.old = (uint32_t)atomicCAS(pw, ~0ull, ((unsigned long long)r.wt << 32) | r.v);
+      } else {
+        p.old = atomicCAS(slab + pr.empty_word, kEmptyKey, r.v);
+      }
       p.kind = 1;
     } else {
       p.kind = 2;
@@ -471,9 +480,10 @@ __device__ __forceinline__ uint32_t upd_finish(const GraphView &g, const UpdPend
   if (p.kind == 1) {
     if (!kInsert) return p.old == p.v ? 1u : 0u;
     if (p.old == kEmptyKey || p.old == p.v) {
-      // a never-used value word is EMPTY, so atomicMin keeps the minimum over
-      // every concurrent copy
-      if (kWeighted) atomicMin(slab + p.word + 1, p.wt);
+      // the pair CAS wrote the weight with the key; a copy that found the key
+      // already placed keeps the minimum (the value word of a never-used
+      // slot is EMPTY, so atomicMin is exact under any interleaving)
+      if (kWeighted && p.old == p.v) atomicMin(slab + p.word + 1, p.wt);
       return p.old == kEmptyKey ? 1u : 0u;
     }
   }
@@ -493,8 +503,9 @@ __device__ __forceinline__ uint32_t upd_finish(const GraphView &g, const UpdPend
 //           the warp's shared-memory stage, completing on its mbarrier;
 //   decide  group i: each lane decides from its staged slab and issues its
 //           one CAS without waiting for the result;
-//   finish  group i-1: the CAS results are read (weighted inserts then
-//           atomicMin the value word; a lost race walks the chain).
+//   finish  group i-1: the CAS results are read (a weighted insert that
+//           met its own key placed concurrently atomicMins the value word;
+//           a lost race walks the chain).
 // Every result a step consumes was requested one iteration earlier, so a
 // warp waits about one memory latency per group.
 template <bool kWeighted, bool kInsert>
