@@ -38,6 +38,19 @@ def test_python_bindings_cover_the_header():
     assert set(declared_symbols()) <= bound
 
 
+def test_python_bindings_match_the_header_arity():
+    """Every ctypes prototype takes as many arguments as the C declaration."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(mk_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = m.group(2).strip()
+        protos[m.group(1)] = 0 if params in ("", "void") else len(params.split(","))
+    assert len(protos) > 40
+    bad = [(name, protos[name], len(args)) for name, _, args in SIGNATURES
+           if name in protos and protos[name] != len(args)]
+    assert not bad, bad
+
+
 def test_version_string():
     assert "sm_100a" in mk.version()
 
