@@ -320,11 +320,17 @@ __device__ uint32_t lane_insert_chain(const GraphView &g, uint32_t s, uint4 (&q)
     }
     if (p.empty_word < 32) {
       uint32_t *wp = reinterpret_cast<uint32_t *>(g.slabs + 8ull * s) + p.empty_word;
-      const uint32_t old = atomicCAS(wp, kEmptyKey, v);
+      // weighted: one 64-bit CAS installs key and weight together (the pair
+      // of a never-used slot is EMPTY in both words)
+      const uint32_t old =
+          kWeighted ? (uint32_t)atomicCAS(reinterpret_cast<unsigned long long *>(wp), ~0ull,
+                                          ((unsigned long long)wt << 32) | v)
+                    : atomicCAS(wp, kEmptyKey, v);
       if (old == kEmptyKey || old == v) {
-        // the value word of a never-used slot is EMPTY (0xFFFFFFFF), so
-        // atomicMin leaves the minimum over every concurrent copy
-        if (kWeighted) atomicMin(wp + 1, wt);
+        // a copy that found its key already placed keeps the minimum weight
+        // (the value word of a never-used slot is EMPTY, so atomicMin is
+        // exact under any interleaving)
+        if (kWeighted && old == v) atomicMin(wp + 1, wt);
         return old == kEmptyKey ? 1u : 0u;
       }
       continue;
