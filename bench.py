@@ -123,11 +123,14 @@ class Clocks:
         self.samples.append((time.perf_counter(), sm, r))
 
     def _run(self):
+        # 2 ms between samples: enough to see the clocks of a sub-second
+        # region without holding the GIL against the host-issued arms
         while not self.stop_flag.is_set():
             try:
                 self._sample()
             except Exception:
                 break
+            time.sleep(0.002)
 
     def stop(self):
         if self.N is None:
@@ -141,6 +144,44 @@ class Clocks:
         sm = [x for _, x, _ in self.samples]
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz,
                 "reasons": sorted(names), "samples": len(sm), "source": "nvml"}
+
+
+def probe_random_rmw(line_bytes: int, small_words: int, num_ops: int, repeats: int = 5,
+                     device: int = 0) -> dict:
+    """Operations per second of the update path's memory pattern (random
+    128-B line read; + CAS; + a random 4-B read and add) for modes 0, 1, 2,
+    best of `repeats` launches each, on a fresh buffer of line_bytes bytes.
+    Runs the benchmark-only libmk_bench_probe.so."""
+    import ctypes as C
+
+    import torch
+    from meerkat_b200.build import build_bench_probe
+    L = C.CDLL(str(build_bench_probe()))
+    vp = C.c_void_p
+    f = L.mkb_probe_random_rmw
+    f.restype = C.c_int
+    f.argtypes = [vp, C.c_uint64, vp, vp, C.c_uint32, C.c_uint64, C.c_uint32, C.c_uint64, vp, vp,
+                  C.POINTER(C.c_float)]
+    dev = f"cuda:{device}"
+    lines = torch.zeros(line_bytes // 4, dtype=torch.int32, device=dev)
+    a = torch.zeros(small_words, dtype=torch.int32, device=dev)
+    b = torch.zeros(small_words, dtype=torch.int32, device=dev)
+    sink = torch.zeros(1, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize(dev)
+    out = {}
+    for mode in (0, 1, 2):
+        best = None
+        for r in range(repeats):
+            ms = C.c_float(0.0)
+            rc = f(lines.data_ptr(), line_bytes // 128, a.data_ptr(), b.data_ptr(), small_words,
+                   num_ops, mode, 1000 + r, sink.data_ptr(), None, C.byref(ms))
+            if rc != 0:
+                raise RuntimeError(f"mkb_probe_random_rmw failed ({rc})")
+            best = ms.value if best is None else min(best, ms.value)
+        out[mode] = num_ops / (best / 1000.0)
+    del lines, a, b, sink
+    torch.cuda.empty_cache()
+    return {"read_lines_per_s": out[0], "read_cas_per_s": out[1], "update_pattern_per_s": out[2]}
 
 
 def make_workload(n_batches: int):
@@ -1120,7 +1161,7 @@ def main():
     traffic = profile_traffic()
     # the same random-line pattern without decision logic, on a buffer the
     # size of the slab pool: what the memory system gives this access pattern
-    ceiling = mk.probe_random_rmw(int(info["pool_capacity"]) * 128, V, 2 * HALF, device=local)
+    ceiling = probe_random_rmw(int(info["pool_capacity"]) * 128, V, 2 * HALF, device=local)
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(graph, batches[W:W + K], max_batches=3)
@@ -1174,7 +1215,7 @@ def main():
                          "algorithmic_bytes_per_step": upd_bytes,
                          "traffic": traffic,
                          "pattern_ceiling": {
-                             "what": "mk_probe_random_rmw: random 128-B line read + CAS + random "
+                             "what": "benchmark probe: random 128-B line read + CAS + random "
                                      "4-B read and add per operation, no decision logic, "
                                      f"{2 * HALF} operations on a {int(info['pool_capacity']) * 128 >> 20} MiB buffer",
                              **ceiling,

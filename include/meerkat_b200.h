@@ -441,20 +441,6 @@ mk_status mk_gen_set_batches(const uint32_t *d_vertex_offsets, uint32_t num_grap
                              uint32_t *d_ins_dst, uint32_t *d_ins_w, void *stream);
 
 /* ------------------------------------------------------------------------
- * Device probe (no counterpart in the reference): the update path's memory
- * pattern without its decision logic, to state the ceiling the update
- * kernels run against.  num_ops operations on random 128-byte lines of
- * d_lines (line_count lines): mode 0 reads the line, mode 1 also CASes one
- * of its words, mode 2 also reads one random word of d_small_a and adds to
- * one random word of d_small_b (small_words words each).  d_sink: one
- * zeroed u64.  Times the launch when ms_out is non-NULL.
- * ---------------------------------------------------------------------- */
-mk_status mk_probe_random_rmw(void *d_lines, uint64_t line_count, void *d_small_a,
-                              void *d_small_b, uint32_t small_words, uint64_t num_ops,
-                              uint32_t mode, uint64_t seed, void *d_sink, void *stream,
-                              float *ms_out);
-
-/* ------------------------------------------------------------------------
  * The reference drivers' text formats (host only; no GPU needed):
  *   graph file "V E" then E pairs "u v"                 (src/BFS.cu:27-36)
  *   batch file "<prefix>.batch.<i>": "n" then n pairs  (src/BFS.cu:76-91)

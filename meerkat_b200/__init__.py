@@ -710,33 +710,6 @@ def gen_rmat_members(vertex_offsets, edges_per_graph, a=0.57, b=0.19, c=0.19, se
     return src[:E], dst[:E], (w[:E] if w is not None else None)
 
 
-def probe_random_rmw(line_bytes: int, small_words: int, num_ops: int, repeats: int = 5,
-                     device: int = 0) -> dict:
-    """Operations per second of the update path's memory pattern (see
-    mk_probe_random_rmw) for modes 0, 1, 2, best of `repeats` launches each,
-    on a fresh buffer of line_bytes bytes."""
-    import torch
-    dev = f"cuda:{device}"
-    lines = torch.zeros(line_bytes // 4, dtype=torch.int32, device=dev)
-    a = torch.zeros(small_words, dtype=torch.int32, device=dev)
-    b = torch.zeros(small_words, dtype=torch.int32, device=dev)
-    sink = torch.zeros(1, dtype=torch.int64, device=dev)
-    out = {}
-    for mode in (0, 1, 2):
-        best = None
-        for r in range(repeats):
-            ms = C.c_float(0.0)
-            check(lib().mk_probe_random_rmw(lines.data_ptr(), line_bytes // 128, a.data_ptr(),
-                                            b.data_ptr(), small_words, num_ops, mode, 1000 + r,
-                                            sink.data_ptr(), None, C.byref(ms)),
-                  "mk_probe_random_rmw")
-            best = ms.value if best is None else min(best, ms.value)
-        out[mode] = num_ops / (best / 1000.0)
-    del lines, a, b, sink
-    torch.cuda.empty_cache()
-    return {"read_lines_per_s": out[0], "read_cas_per_s": out[1], "update_pattern_per_s": out[2]}
-
-
 # ---------------------------------------------------------------------------
 # the reference drivers' text formats (host only)
 # ---------------------------------------------------------------------------

@@ -125,8 +125,6 @@ SIGNATURES = [
                              C.c_uint32, C.c_uint32, vp, vp, vp, vp]),
     ("mk_gen_set_batches", _S, [vp, C.c_uint32, vp, vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32,
                                 vp, vp, vp, vp, vp, vp]),
-    ("mk_probe_random_rmw", _S, [vp, C.c_uint64, vp, vp, C.c_uint32, C.c_uint64, C.c_uint32,
-                                 C.c_uint64, vp, vp, f32p]),
     ("mk_read_edge_list", _S, [C.c_char_p, u32p, u64p, vp, vp]),
     ("mk_read_batch_file", _S, [C.c_char_p, u64p, vp, vp]),
     ("mk_write_edge_list", _S, [C.c_char_p, C.c_uint32, C.c_uint64, vp, vp]),

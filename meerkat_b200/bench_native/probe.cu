@@ -1,5 +1,8 @@
 // probe.cu -- ceiling of the update path's memory pattern on this device.
 //
+// Benchmark-only: built into libmk_bench_probe.so, which bench.py alone
+// loads; it is not part of libmeerkat_b200.so or its public header.
+//
 // The update kernels touch, per edge, one random 128-byte slab line (read,
 // then a CAS on one of its words), one random word of the bucket-offset
 // array (read) and one random word of the degree array (add).  A copy kernel
@@ -16,10 +19,8 @@
 // coalesced loads, lane j then issues operation j's CAS / add.  Lines and
 // words are chosen by a counter-based hash of (seed, operation).
 #include <cuda_runtime.h>
+#include <stdint.h>
 
-#include "mk_internal.h"
-
-namespace mk {
 namespace {
 
 __device__ __forceinline__ unsigned long long probe_mix(unsigned long long x) {
@@ -71,31 +72,42 @@ __global__ void __launch_bounds__(256) k_probe_rmw(uint32_t *__restrict__ lines,
 }
 
 }  // namespace
-}  // namespace mk
 
-using namespace mk;
-
-extern "C" mk_status mk_probe_random_rmw(void *d_lines, uint64_t line_count, void *d_small_a,
-                                         void *d_small_b, uint32_t small_words, uint64_t num_ops,
-                                         uint32_t mode, uint64_t seed, void *d_sink, void *stream,
-                                         float *ms_out) {
-  if (!d_lines || !line_count || !d_sink || mode > 2 ||
+// Returns 0 on success, 1 on a bad argument, 2 on a CUDA error.  Synchronises
+// and writes the launch's device time to *ms_out (CUDA events on `stream`).
+extern "C" int mkb_probe_random_rmw(void *d_lines, uint64_t line_count, void *d_small_a,
+                                    void *d_small_b, uint32_t small_words, uint64_t num_ops,
+                                    uint32_t mode, uint64_t seed, void *d_sink, void *stream,
+                                    float *ms_out) {
+  if (!d_lines || !line_count || !d_sink || !ms_out || mode > 2 ||
       (mode == 2 && (!d_small_a || !d_small_b || !small_words)))
-    return fail(MK_ERR_INVALID, "mk_probe_random_rmw: bad argument");
-  int dev = 0;
-  MK_CUDA(cudaGetDevice(&dev));
-  cudaStream_t s = as_stream(stream);
-  Timer t;
-  MK_CHECK(t.start(s, ms_out != nullptr));
-  int per_sm = 0;
-  MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_rmw, 256, 0));
+    return 1;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 2;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 2;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_rmw, 256, 0) != cudaSuccess)
+    return 2;
   const uint64_t want = (num_ops + 255) / 256;
-  const uint64_t cap = (uint64_t)device_sm_count(dev) * (per_sm > 0 ? per_sm : 1);
+  const uint64_t cap = (uint64_t)sms * (per_sm > 0 ? per_sm : 1);
   const int blocks = (int)(want < cap ? (want ? want : 1) : cap);
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return 2;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return 2;
+  }
+  int rc = 0;
+  cudaEventRecord(e0, s);
   k_probe_rmw<<<blocks, 256, 0, s>>>(static_cast<uint32_t *>(d_lines), line_count,
                                      static_cast<uint32_t *>(d_small_a),
                                      static_cast<uint32_t *>(d_small_b), small_words, num_ops,
                                      mode, seed, static_cast<unsigned long long *>(d_sink));
-  MK_CUDA(cudaGetLastError());
-  return t.stop(ms_out);
+  if (cudaGetLastError() != cudaSuccess) rc = 2;
+  cudaEventRecord(e1, s);
+  if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(ms_out, e0, e1) != cudaSuccess)
+    rc = 2;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
 }

@@ -21,6 +21,9 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libmeerkat_b200.so"
+# benchmark-only probe library (not part of the product library or header)
+BENCH_SRC = PKG / "bench_native" / "probe.cu"
+BENCH_LIB = PKG / "libmk_bench_probe.so"
 INCLUDE = PKG.parent / "include"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -83,12 +86,24 @@ def build(clean: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     return LIB
 
 
+def build_bench_probe() -> Path:
+    """Builds libmk_bench_probe.so (bench.py's memory-pattern probe)."""
+    if BENCH_LIB.exists() and BENCH_LIB.stat().st_mtime >= BENCH_SRC.stat().st_mtime:
+        return BENCH_LIB
+    cmd = [NVCC, *CUFLAGS, "-shared", "-o", str(BENCH_LIB), str(BENCH_SRC), "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {BENCH_SRC.name}:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return BENCH_LIB
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--clean", action="store_true")
     ap.add_argument("--ptxas-v", action="store_true", help="print register / smem usage")
     a = ap.parse_args(argv)
     build(clean=a.clean, verbose=True, ptxas_v=a.ptxas_v)
+    build_bench_probe()
 
 
 if __name__ == "__main__":

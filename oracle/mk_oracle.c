@@ -48,36 +48,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define OK_EMPTY (~0ull)
-#define OK_INF 0xFFFFFFFFu
-
-static inline uint64_t mixk(uint64_t x) {
-  x ^= x >> 33;
-  x *= 0xff51afd7ed558ccdull;
-  x ^= x >> 33;
-  x *= 0xc4ceb9fe1a85ec53ull;
-  x ^= x >> 33;
-  return x;
-}
-
-typedef struct {
-  uint64_t *keys;
-  uint32_t *wt;
-  uint32_t *pos;
-  uint64_t cap, size;
-} omap;
-
-typedef struct {
-  uint32_t *a; /* neighbours */
-  uint32_t n, cap;
-} ivec;
-
-typedef struct og {
-  uint32_t V;
-  int T;
-  omap *shard;
-  ivec *adj;
-} og;
+#include "mk_oracle.h"
 
 static void omap_init(omap *m, uint64_t cap) {
   m->cap = cap;
@@ -134,11 +105,13 @@ static void omap_erase_slot(omap *m, uint64_t p) {
   }
 }
 
-static void ivec_push(ivec *v, uint32_t x) {
+static void ivec_push(ivec *v, uint32_t x, uint32_t w) {
   if (v->n == v->cap) {
     v->cap = v->cap ? v->cap * 2 : 4;
     v->a = (uint32_t *)realloc(v->a, (size_t)v->cap * 4);
+    v->w = (uint32_t *)realloc(v->w, (size_t)v->cap * 4);
   }
+  v->w[v->n] = w;
   v->a[v->n++] = x;
 }
 
@@ -156,7 +129,10 @@ void og_destroy(og *g) {
   if (!g) return;
   for (int t = 0; t < g->T; ++t) omap_free(&g->shard[t]);
   free(g->shard);
-  for (uint32_t i = 0; i < g->V; ++i) free(g->adj[i].a);
+  for (uint32_t i = 0; i < g->V; ++i) {
+    free(g->adj[i].a);
+    free(g->adj[i].w);
+  }
   free(g->adj);
   free(g);
 }
@@ -166,14 +142,17 @@ static int og_insert_one(og *g, omap *m, uint32_t u, uint32_t v, uint32_t w) {
   if ((m->size + 1) * 2 > m->cap) omap_grow(m);
   uint64_t p = omap_slot(m, k);
   if (m->keys[p] == k) { /* live edge: keep the smaller weight (upsert-min) */
-    if (w < m->wt[p]) m->wt[p] = w;
+    if (w < m->wt[p]) {
+      m->wt[p] = w;
+      g->adj[u].w[m->pos[p]] = w;
+    }
     return 0;
   }
   m->keys[p] = k;
   m->wt[p] = w;
   m->pos[p] = g->adj[u].n;
   m->size++;
-  ivec_push(&g->adj[u], v);
+  ivec_push(&g->adj[u], v, w);
   return 1;
 }
 
@@ -185,9 +164,11 @@ static int og_delete_one(og *g, omap *m, uint32_t u, uint32_t v) {
   omap_erase_slot(m, p);
   ivec *a = &g->adj[u];
   uint32_t last = a->a[a->n - 1];
+  uint32_t lastw = a->w[a->n - 1];
   a->n--;
   if (pos < a->n) {
     a->a[pos] = last;
+    a->w[pos] = lastw;
     uint64_t q = omap_slot(m, ((uint64_t)u << 32) | last);
     m->pos[q] = pos;
   }
@@ -335,8 +316,7 @@ int og_sssp(const og *g, uint32_t src, uint32_t *dist) {
     if (dk != d64[u]) continue;
     const ivec *a = &g->adj[u];
     for (uint32_t j = 0; j < a->n; ++j) {
-      uint32_t v = a->a[j], w = 0;
-      og_has_edge(g, (uint32_t)u, v, &w);
+      uint32_t v = a->a[j], w = a->w[j];
       uint64_t nd = dk + w;
       if (nd < d64[v]) {
         d64[v] = nd;
