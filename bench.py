@@ -184,13 +184,21 @@ def probe_random_rmw(line_bytes: int, small_words: int, num_ops: int, repeats: i
     return {"read_lines_per_s": out[0], "read_cas_per_s": out[1], "update_pattern_per_s": out[2]}
 
 
-def make_workload(n_batches: int):
-    import meerkat_b200 as mk
+def make_workload(n_batches: int, source: str = "product"):
+    """The R-MAT graph and `n_batches` mixed batches (delete sub-batch of
+    present edges, insert sub-batch of absent edges with weights).
+    source="oracle" draws the same edges and batches with the oracle's host
+    generators, so the reference arm loads no product code."""
+    if source == "oracle":
+        from oracle import OracleEdgeSet as EdgeSet
+        from oracle import gen_rmat
+    else:
+        from meerkat_b200 import EdgeSet, gen_rmat
     t0 = time.time()
-    s, d, w = mk.gen_rmat(SCALE, EDGES, seed=SEED, w_lo=W_LO, w_hi=W_HI)
-    log(f"[bench] R-MAT s{SCALE}: {len(s)} edges in {time.time() - t0:.1f}s")
+    s, d, w = gen_rmat(SCALE, EDGES, seed=SEED, w_lo=W_LO, w_hi=W_HI)
+    log(f"[bench] R-MAT s{SCALE}: {len(s)} edges in {time.time() - t0:.1f}s ({source} generator)")
     t0 = time.time()
-    es = mk.EdgeSet(1 << SCALE, s, d)
+    es = EdgeSet(1 << SCALE, s, d)
     batches = []
     rng = np.random.default_rng(SEED)
     for b in range(n_batches):
@@ -230,6 +238,114 @@ def cpu_baseline(graph, batches, max_batches=3, warmup=0):
             "seconds": total}
 
 
+def oracle_large(graph, hist, timed_at, A, gpu, algo):
+    """Rank 0, after the GPU work of the updates workload.  The oracle (C,
+    OpenMP, every host core) replays every batch the GPU graph received, in
+    order, and
+
+    * times three mixed batches (the first three of the K timed ones): the
+      CPU baseline of the update half;
+    * times the multithreaded CPU implementation of the query half on the
+      same graph: static BFS / SSSP from the GPU's source before the A query
+      batches, then per batch decremental BFS / SSSP after its deletes and
+      incremental after its inserts; static WCC, PageRank (stopped by the
+      GPU's rule) and triangle counting on the final graph;
+    * checks the GPU's answers at full size: the maintained BFS levels and
+      SSSP distances after the A batches bit-exact against the oracle's BFS
+      and Dijkstra, with valid parents; after the last batch the degrees,
+      the WCC labels and the triangle count exact, and PageRank within L1
+      1e-6 of an FP64 solve run to an L1 change of 1e-11 (the pull solver
+      the CPU tests pin against the oracle's own iteration).
+
+    Returns (cpu_baseline, cpu_queries, parity)."""
+    from oracle import CpuTraversal, OracleGraph, cpu_pagerank, cpu_triangles, cpu_wcc
+    s, d, w = graph
+    T = os.cpu_count() or 1
+    V = 1 << SCALE
+    O = OracleGraph(V, threads=T)
+    t0 = time.time()
+    O.insert(s, d, w)
+    log(f"[oracle] s{SCALE} loaded in {time.time() - t0:.1f}s on {T} threads")
+    nq = len(hist) - A
+    up_times, applied = [], 0
+    t0 = time.time()
+    for i, (ds, dd, is_, id_, iw) in enumerate(hist[:nq]):
+        t1 = time.perf_counter()
+        n1, _ = O.delete(ds, dd)
+        n2, _ = O.insert(is_, id_, iw)
+        if timed_at[0] <= i < timed_at[1]:
+            up_times.append(time.perf_counter() - t1)
+            applied += n1 + n2
+    log(f"[oracle] replayed {nq} mixed batches in {time.time() - t0:.1f}s")
+    cb = {"value": applied / sum(up_times), "unit": METRIC, "cores": T, "kind": "port",
+          "sample": f"{len(up_times)} mixed batches of {2 * HALF} edges on the full R-MAT "
+                    f"s{SCALE} graph (hash-set adjacency, one shard per thread)",
+          "seconds": sum(up_times)}
+
+    def ms(fn):
+        t1 = time.perf_counter()
+        r = fn()
+        return 1000.0 * (time.perf_counter() - t1), r
+
+    src = gpu["source"]
+    cq = {"cores": T, "kind": "port", "source": src}
+    bfs, sssp = CpuTraversal(O, src, False), CpuTraversal(O, src, True)
+    cq["bfs_static_ms"], _ = ms(bfs.static)
+    cq["sssp_static_ms"], _ = ms(sssp.static)
+    rec = {k: [] for k in ("bfs_dec_ms", "sssp_dec_ms", "bfs_inc_ms", "sssp_inc_ms")}
+    inv = {"bfs": [], "sssp": []}
+    for (ds, dd, is_, id_, iw) in hist[nq:]:
+        O.delete(ds, dd)
+        rec["bfs_dec_ms"].append(ms(lambda: bfs.decremental(ds, dd))[0])
+        rec["sssp_dec_ms"].append(ms(lambda: sssp.decremental(ds, dd))[0])
+        inv["bfs"].append(bfs.stats()["invalidated"])
+        inv["sssp"].append(sssp.stats()["invalidated"])
+        O.insert(is_, id_, iw)
+        rec["bfs_inc_ms"].append(ms(lambda: bfs.incremental(is_, id_))[0])
+        rec["sssp_inc_ms"].append(ms(lambda: sssp.incremental(is_, id_))[0])
+    for k, v in rec.items():
+        cq[k + "_p50"] = statistics.median(v)
+    cq["invalidated"] = inv
+    par = {}
+    t0 = time.time()
+    want_b, want_s = O.bfs(src), O.sssp(src)
+    par["bfs"] = bool(np.array_equal(gpu["bfs"], want_b))
+    par["sssp"] = bool(np.array_equal(gpu["sssp"], want_s))
+    par["bfs_bad_parents"] = O.check_parents(src, gpu["bfs_packed"], False)
+    par["sssp_bad_parents"] = O.check_parents(src, gpu["sssp_packed"], True)
+    par["cpu_port_bfs"] = bool(np.array_equal(bfs.distances(), want_b))
+    par["cpu_port_sssp"] = bool(np.array_equal(sssp.distances(), want_s))
+    del bfs, sssp
+    # the 100,000-edge batch of the WCC / PageRank / TC queries: deleted, then
+    # inserted again with weight 0
+    bs, bd = gpu["batch"]
+    O.delete(bs, bd)
+    O.insert(bs, bd, np.zeros(len(bs), dtype=np.uint32))
+    par["degrees"] = bool(np.array_equal(gpu["degrees"], O.degrees()))
+    want_w = O.wcc()
+    par["wcc"] = bool(np.array_equal(gpu["wcc"], want_w))
+    cq["wcc_static_ms"], lab = ms(lambda: cpu_wcc(O))
+    par["cpu_port_wcc"] = bool(np.array_equal(lab, want_w))
+    want_t = O.triangles()
+    par["triangles"] = int(want_t)
+    par["tc"] = int(gpu["triangles"]) == int(want_t)
+    cq["tc_static_ms"], n_t = ms(lambda: cpu_triangles(O))
+    par["cpu_port_tc"] = int(n_t) == int(want_t)
+    # the GPU stops when its L1 change x d / (1 - d) <= tol / 2
+    tol = algo.get("pagerank", {}).get("tol", 1e-6)
+    cq["pagerank_static_ms"], (_, it) = ms(lambda: cpu_pagerank(O, 0.85, tol * 0.5 * 0.15 / 0.85, 1000))
+    cq["pagerank_iterations"] = it
+    ref, _ = cpu_pagerank(O, 0.85, 1e-11, 10000)
+    par["pagerank_l1"] = float(np.abs(gpu["pagerank"].astype(np.float64) - ref).sum())
+    par["pagerank"] = par["pagerank_l1"] <= 1e-6
+    par["ok"] = bool(par["bfs"] and par["sssp"] and par["bfs_bad_parents"] == 0 and
+                     par["sssp_bad_parents"] == 0 and par["degrees"] and par["wcc"] and
+                     par["tc"] and par["pagerank"])
+    log(f"[oracle] parity checks in {time.time() - t0:.1f}s: {par}")
+    del O
+    return cb, cq, par
+
+
 def verify_replay(G, timed_batches, todev, dev):
     """Checks the graph state after the K captured steps against the batches."""
     import torch
@@ -256,9 +372,15 @@ def more_queries(mk, G, V, dev, seed):
     then one decremental and one incremental batch), with the algorithmic
     bytes of each static run: WCC 8 E + 8 V; PageRank 8 E + 16 V per
     iteration; TC 4 x sum over oriented edges of (d+(u) + d+(v)), edges
-    oriented from lower to higher (degree, id) on the symmetric graph."""
+    oriented from lower to higher (degree, id) on the symmetric graph.
+
+    Returns (timings, finals): finals holds the last answers (WCC labels,
+    PageRank values, triangle count) and the host copy of the 100,000-edge
+    batch this function deletes from G and inserts again with weight 0, so
+    the oracle can replay it and check the answers."""
     import torch
     out = {}
+    finals = {}
     g = torch.Generator(device=dev)
     g.manual_seed(seed)
     rp, col, _ = G.export_csr_range_device(0, V)
@@ -274,6 +396,8 @@ def more_queries(mk, G, V, dev, seed):
     out["wcc"]["dec_ms"] = wcc.Decremental(bs, bd)
     G.InsertEdges(bs, bd)  # weight 0 on the re-inserted copies
     out["wcc"]["inc_ms"] = wcc.Incremental(bs, bd)
+    finals["wcc"] = wcc.Labels()
+    finals["batch"] = (bs.cpu().numpy().view(np.uint32).copy(), bd.cpu().numpy().view(np.uint32).copy())
     wcc.close()
     # PageRank on a reverse copy
     indeg = torch.bincount(col.long(), minlength=V).to(torch.int32).cpu().numpy().view(np.uint32)
@@ -303,6 +427,8 @@ def more_queries(mk, G, V, dev, seed):
     out["pagerank"]["dec_ms"] = pr.Decremental(bs, bd)
     Gr.InsertEdges(bs, bd)
     out["pagerank"]["inc_ms"] = pr.Incremental(bs, bd)
+    finals["pagerank"] = pr.Values()
+    out["pagerank"]["tol"] = 1e-6
     pr.close()
     Gr.close()
     # triangles on the symmetric graph
@@ -330,6 +456,7 @@ def more_queries(mk, G, V, dev, seed):
     out["tc"]["dec_ms"] = tc.Decremental(uu, uv)
     Gs.InsertEdges(uu, uv)
     out["tc"]["inc_ms"] = tc.Incremental(uu, uv)
+    finals["triangles"] = tc.GetCount()
     tc.close()
     Gs.close()
     del rp, col, rows, su, sv, key, sdeg, fwd, ou, ov, dplus
@@ -339,6 +466,44 @@ def more_queries(mk, G, V, dev, seed):
     for k in out:
         if "static_gbs" in out[k]:
             out[k]["static_frac"] = out[k]["static_gbs"] / peak
+    return out, finals
+
+
+def line_summary(line):
+    """The headline figures of the updates workload in a few hundred bytes:
+    the update rates, the roofline fraction, the query half of the metric
+    (GPU and CPU ms per call, p50) and the parity verdict per config."""
+    q, cq = line.get("queries", {}), line.get("cpu_queries") or {}
+    r3 = lambda x: None if x is None else float(f"{x:.4g}")
+    keys = [("bfs_static", "bfs_static_ms", "bfs_static_ms"),
+            ("sssp_static", "sssp_static_ms", "sssp_static_ms"),
+            ("bfs_inc", "bfs_inc_ms_p50", "bfs_inc_ms_p50"),
+            ("bfs_dec", "bfs_dec_ms_p50", "bfs_dec_ms_p50"),
+            ("sssp_inc", "sssp_inc_ms_p50", "sssp_inc_ms_p50"),
+            ("sssp_dec", "sssp_dec_ms_p50", "sssp_dec_ms_p50")]
+    gpu_ms = {k: r3(q.get(a)) for k, a, _ in keys}
+    cpu_ms = {k: r3(cq.get(b)) for k, _, b in keys}
+    for k in ("wcc", "pagerank", "tc"):
+        gpu_ms[k + "_static"] = r3(q.get(k, {}).get("static_ms"))
+        cpu_ms[k + "_static"] = r3(cq.get(k + "_static_ms"))
+    out = {"updates_per_s": r3(line["value"]), "e2e_updates_per_s": r3(line["e2e"]["value"]),
+           "roofline_frac": r3(line["roofline"]["frac"]),
+           "cpu_updates_per_s": r3((line.get("cpu_baseline") or {}).get("value")),
+           "cpu_cores": cq.get("cores"), "gpu_ms": gpu_ms, "cpu_ms": cpu_ms,
+           "parity": line.get("parity")}
+    if "batched" in line:
+        out["batched_speedup"] = r3(line["batched"]["speedup_vs_plain"])
+    if "grid" in line:
+        g = line["grid"]
+        out["grid_ms_p50"] = {"bfs_dec": r3(g["decremental_p50_ms"]["bfs_ms"]),
+                              "sssp_dec": r3(g["decremental_p50_ms"]["sssp_ms"]),
+                              "bfs_static": r3(g["static"]["bfs_ms"]),
+                              "sssp_static": r3(g["static"]["sssp_ms"])}
+    if "serving" in line:
+        out["serving"] = [{"rps": row["offered_rps"],
+                           **{m: [r3(row[m]["p50_ms"]), r3(row[m]["p99_ms"]),
+                                  r3(row[m]["throughput_rps"])] for m in ("coalesced", "alone")}}
+                          for row in line["serving"]["rates"]]
     return out
 
 
@@ -373,11 +538,13 @@ def barrier(world):
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU path does not exist (the reference is
     GPU-only and does not build here), so the oracle port stands in, timed on
-    the host cores on the same config and metric."""
+    the host cores on the same config and metric.  Its inputs come from the
+    oracle's host generators (the same edges and batches as the GPU arm's), so
+    this arm loads only the oracle library."""
     if rank != 0:
         return 0
     K = max(args.steps, 1)
-    graph, batches = make_workload(K + args.warmup)
+    graph, batches = make_workload(K + args.warmup, source="oracle")
     cb = cpu_baseline(graph, batches, max_batches=K, warmup=args.warmup)
     v = cb["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC,
@@ -446,6 +613,16 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         plain.append(g)
     torch.cuda.synchronize(dev)
     assert all(g.sync() == 0 for g in plain)
+    # members the oracle checks at the end: the 8 with the most edges and 56
+    # more drawn with a seed; their generated edges, in local ids
+    sample = np.unique(np.concatenate([
+        np.argsort(spec.num_edges)[-8:],
+        np.random.default_rng(spec.seed + 9).choice(Gn, size=min(56, Gn), replace=False)]))
+    base_edges = {}
+    for m in sample.tolist():
+        lo, hi, b0 = int(eoff[m]), int(eoff[m + 1]), int(voff[m])
+        base_edges[m] = tuple(x[lo:hi].cpu().numpy().view(np.uint32) - (b0 if i < 2 else 0)
+                              for i, x in enumerate((src, dst, w)))
     del src, dst, w
     info = gs.graph.info()
     log(f"[batched] union and {Gn} per-graph copies built in {time.time() - t0:.1f}s: {info}")
@@ -558,6 +735,13 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         else:
             mism["wcc"] += int(not np.array_equal(a.Labels().astype(np.int64), l_union[lo:hi] - lo))
     assert mism == {"bfs": 0, "wcc": 0}, mism
+    # the oracle replays the sampled members' batches (a batch and its inverse
+    # alternate, starting with the batch; every update the set received)
+    n_updates = Wb + K + 2  # warm-up and tuner steps, K timed steps, 2 phase-split steps
+    host_local = {m: [tuple(x.cpu().numpy().view(np.uint32) for x in both_local[k][m])
+                      for k in (0, 1)] for m in sample.tolist()}
+    par = batched_oracle_check(sample, base_edges, host_local, n_updates, spec, srcs, voff,
+                               d_union, l_union, gs) if rank == 0 else None
     # phase split of the batched step: two more steps (a batch and its
     # inverse, so the set stays on the same state) with events between phases
     phases = {"update": 0.0, "bfs": 0.0, "wcc": 0.0}
@@ -597,6 +781,7 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         "tuning_trials": {"updates": tuning["trials"], "frontier_chunk": chunk["trials"] if chunk else None},
         "equality": {"members_checked": Gn, "bfs_mismatches": mism["bfs"],
                      "wcc_mismatches": mism["wcc"]},
+        **({"parity": par} if par is not None else {}),
         "clocks": clk,
         "graph": {"buckets": info["num_buckets"], "slabs_used": info["slabs_used"],
                   "device_bytes": info["device_bytes"]},
@@ -607,6 +792,40 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         g.close()
     gs.close()
     torch.cuda.synchronize(dev)
+    return out
+
+
+def batched_oracle_check(sample, base_edges, host_local, n_updates, spec, srcs, voff, d_union,
+                         l_union, gs):
+    """The oracle on a sample of the batched set's members: each member's
+    generated edges and its n_updates alternating batches replayed on the CPU,
+    then its degrees, BFS levels (BFS members, from the member's source) or
+    WCC labels (WCC members) compared bit-exactly with the batched arm's."""
+    from meerkat_b200 import batched as B
+    from oracle import OracleGraph
+    t0 = time.time()
+    deg = gs.graph.degrees()
+    bfs_index = {int(m): i for i, m in enumerate(np.flatnonzero(spec.query == B.QUERY_BFS))}
+    bad = {"degrees": 0, "bfs": 0, "wcc": 0}
+    edges_checked = 0
+    for m in sample.tolist():
+        lo, hi = int(voff[m]), int(voff[m + 1])
+        O = OracleGraph(hi - lo)
+        bs, bd, bw = base_edges[m]
+        O.insert(bs, bd, bw)
+        for i in range(n_updates):
+            ds, dd, is_, id_, iw = host_local[m][i % 2]
+            O.delete(ds, dd)
+            O.insert(is_, id_, iw)
+        edges_checked += O.num_edges()
+        bad["degrees"] += int(not np.array_equal(deg[lo:hi], O.degrees()))
+        if spec.query[m] == B.QUERY_BFS:
+            bad["bfs"] += int(not np.array_equal(d_union[lo:hi], O.bfs(int(srcs[bfs_index[m]]))))
+        else:
+            bad["wcc"] += int(not np.array_equal(l_union[lo:hi] - lo, O.wcc().astype(np.int64)))
+    out = {"members": int(len(sample)), "largest_included": 8, "edges": int(edges_checked),
+           "mismatches": bad, "ok": not any(bad.values())}
+    log(f"[batched] oracle check of {len(sample)} members in {time.time() - t0:.1f}s: {out}")
     return out
 
 
@@ -751,6 +970,8 @@ def grid_stress(side, nbatch, batch, rank, world, local):
     rng = np.random.default_rng(SEED + 22 + rank)
     rec = {k: [] for k in ("update_ms", "bfs_ms", "sssp_ms", "wcc_ms")}
     dec, inc = {k: [] for k in rec}, {k: [] for k in rec}
+    repair = {"bfs": [], "sssp": []}
+    history = []  # host copies of every batch, for the oracle replay
     INFINF = np.uint64(2**64 - 1)
     for b in range(nbatch):
         packed = sssp.packed()
@@ -771,6 +992,9 @@ def grid_stress(side, nbatch, batch, rank, world, local):
         dec["bfs_ms"].append(bfs.Decremental(tds, tdd))
         dec["sssp_ms"].append(sssp.Decremental(tds, tdd))
         dec["wcc_ms"].append(wcc.Decremental(tds, tdd))
+        repair["bfs"].append(bfs.decremental_stats())
+        repair["sssp"].append(sssp.decremental_stats())
+        history.append(("del", ds, dd, None))
     for b in range(nbatch):
         u = rng.integers(0, V, batch)
         dx = rng.integers(-2, 3, batch)
@@ -779,7 +1003,9 @@ def grid_stress(side, nbatch, batch, rank, world, local):
         ok = (r >= 0) & (r < side) & (c >= 0) & (c < side) & ((dx != 0) | (dy != 0))
         r, c, u = np.where(ok, r, u // side), np.where(ok, c, u % side), u
         v = (r * side + c).astype(np.uint32)
-        tis, tid, tiw = todev(u), todev(v), todev(rng.integers(1, 1001, batch))
+        uw = rng.integers(1, 1001, batch).astype(np.uint32)
+        tis, tid, tiw = todev(u), todev(v), todev(uw)
+        history.append(("ins", u.astype(np.uint32), v, uw))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         G.InsertEdges(tis, tid, vals=tiw)
@@ -798,19 +1024,42 @@ def grid_stress(side, nbatch, batch, rank, world, local):
             "sssp": bool(np.array_equal(got[1], fs.Distances())),
             "wcc": bool(np.array_equal(got[2], fw.Labels()))}
     comps = int(len(np.unique(got[2])))
+    gpu_deg = G.degrees()
     for o in (fb, fs, fw, bfs, sssp, wcc):
         o.close()
     G.close()
     torch.cuda.synchronize(dev)
     torch.cuda.empty_cache()
     assert all(same.values()), same
+    # the oracle replays the same batches: the maintained answers bit-exact
+    par = None
+    if rank == 0:
+        from oracle import OracleGraph
+        t0 = time.time()
+        O = OracleGraph(V, threads=os.cpu_count() or 1)
+        O.insert(s, d, w)
+        for op, a, b, c in history:
+            O.delete(a, b) if op == "del" else O.insert(a, b, c)
+        par = {"degrees": bool(np.array_equal(gpu_deg, O.degrees())),
+               "bfs": bool(np.array_equal(got[0], O.bfs(src))),
+               "sssp": bool(np.array_equal(got[1], O.sssp(src))),
+               "wcc": bool(np.array_equal(got[2], O.wcc()))}
+        par["ok"] = all(par.values())
+        del O
+        log(f"[grid] oracle replay and checks in {time.time() - t0:.1f}s: {par}")
     p50 = lambda xs: statistics.median(xs) if xs else None
-    return {"workload": f"grid{side}_decremental_stress", "vertices": V, "edges": E,
-            "tuning": {"sssp_delta": nf["best"], "recompute_permille": 5},
-            "batches": nbatch, "batch": batch, "source": src, "static": static,
-            "decremental_p50_ms": {k: p50(v) for k, v in dec.items()},
-            "incremental_p50_ms": {k: p50(v) for k, v in inc.items()},
-            "components_after": comps, "matches_static_recompute": same}
+    out = {"workload": f"grid{side}_decremental_stress", "vertices": V, "edges": E,
+           "tuning": {"sssp_delta": nf["best"], "recompute_permille": 5},
+           "batches": nbatch, "batch": batch, "source": src, "static": static,
+           "decremental_p50_ms": {k: p50(v) for k, v in dec.items()},
+           "incremental_p50_ms": {k: p50(v) for k, v in inc.items()},
+           "decremental_repair": {k: {"invalidated": [int(x) for x, _ in v],
+                                      "recomputed": [bool(r) for _, r in v]}
+                                  for k, v in repair.items()},
+           "components_after": comps, "matches_static_recompute": same}
+    if par is not None:
+        out["parity"] = par
+    return out
 
 
 def run_batched(args, rank, world, local):
@@ -912,6 +1161,7 @@ def main():
     from meerkat_b200.autotune import VARIANTS, tune_updates
     T = 2 * len(VARIANTS)  # two tuning rounds
     graph, batches = make_workload(T + W + 2 * K + W + A + 2)
+    allb = batches  # every batch G receives, in order (the oracle replays them)
     s, d, w = graph
     V = 1 << SCALE
 
@@ -1110,6 +1360,7 @@ def main():
         rec = {k: [] for k in ("bfs_dec_ms", "sssp_dec_ms", "bfs_inc_ms", "sssp_inc_ms",
                                "bfs_dec_rev_ms", "sssp_dec_rev_ms")}
         gbs = {k: [] for k in rec}
+        repair = {"bfs": [], "sssp": []}  # (invalidated, recomputed) per decremental call
 
         def timed_dynamic(key, trav, s_bytes, call):
             # algorithmic bytes: sum over vertices whose distance changed of
@@ -1129,6 +1380,8 @@ def main():
             Gr.DeleteEdges(ds, dd)
             timed_dynamic("bfs_dec_ms", bfs, 4, lambda: bfs.Decremental(ds, dd))
             timed_dynamic("sssp_dec_ms", sssp, 8, lambda: sssp.Decremental(ds, dd))
+            repair["bfs"].append(bfs.decremental_stats())
+            repair["sssp"].append(sssp.decremental_stats())
             timed_dynamic("bfs_dec_rev_ms", bfs_r, 4, lambda: bfs_r.Decremental(ds, dd))
             timed_dynamic("sssp_dec_rev_ms", sssp_r, 8, lambda: sssp_r.Decremental(ds, dd))
             G.InsertEdges(is_, id_, vals=iw)
@@ -1149,10 +1402,20 @@ def main():
             algo[k.replace("_ms", "_gbs") + "_p50"] = g
             algo[k.replace("_ms", "_frac") + "_p50"] = g / peak_q
         algo["source"] = src_v
+        algo["decremental_repair"] = {
+            k: {"invalidated": [int(x) for x, _ in v], "recomputed": [bool(r) for _, r in v],
+                "invalidated_share_p50": statistics.median(x for x, _ in v) / V}
+            for k, v in repair.items()}
+        # the maintained answers after the A batches, for the oracle check
+        gpu_final = {"source": src_v, "bfs": bfs.Distances(), "sssp": sssp.Distances(),
+                     "bfs_packed": bfs.packed(), "sssp_packed": sssp.packed()}
         bfs.close()
         sssp.close()
         bfs = sssp = None
-        algo.update(more_queries(mk, G, V, dev, SEED + 11))
+        mq, mq_finals = more_queries(mk, G, V, dev, SEED + 11)
+        algo.update(mq)
+        gpu_final.update(mq_finals)
+        gpu_final["degrees"] = G.degrees()
 
     peak, peak_kind = measured_peak()
     upd_bytes = HALF * DEL_BYTES + HALF * INS_BYTES
@@ -1162,9 +1425,15 @@ def main():
     # the same random-line pattern without decision logic, on a buffer the
     # size of the slab pool: what the memory system gives this access pattern
     ceiling = probe_random_rmw(int(info["pool_capacity"]) * 128, V, 2 * HALF, device=local)
-    cb = None
+    cb = cpu_q = parity_large = None
     if rank == 0 and not args.no_cpu_baseline:
-        cb = cpu_baseline(graph, batches[W:W + K], max_batches=3)
+        if A > 0:
+            hist = allb[:T + W + 2 * K + 2 + W + A]
+            timed_at = (T + W, T + W + 3)  # the CPU times the first 3 of the K timed batches
+            cb, cpu_q, parity_large = oracle_large(graph, hist, timed_at, A, gpu_final, algo)
+            del gpu_final
+        else:
+            cb = cpu_baseline(graph, batches[W:W + K], max_batches=3)
     batched = None
     if args.batched_graphs > 0:
         del bfs, sssp
@@ -1175,7 +1444,10 @@ def main():
             "workload", "speedup_vs_plain", "speedup_vs_plain_cuda_graph", "batched_ms_per_step",
             "plain_ms_per_step", "plain_cuda_graph_ms_per_step", "batched_updates_per_s",
             "updates_per_step", "vertices", "edges", "gpu_launches_per_step",
-            "plain_launches_per_step", "queries", "tuning", "equality", "clocks", "steps")}
+            "plain_launches_per_step", "queries", "tuning", "equality", "clocks", "steps")
+            if k in r}
+        if "parity" in r:
+            batched["parity"] = r["parity"]
     grid = None
     if args.grid_side > 0:
         grid = grid_stress(args.grid_side, 10, 500_000, rank, world, local)
@@ -1222,7 +1494,7 @@ def main():
                              "frac": (upd_per_step / (ms / K / 1000.0)) / ceiling["update_pattern_per_s"]}},
             "host_driven_delete_ms": statistics.mean(del_ms),
             "host_driven_insert_ms": statistics.mean(ins_ms),
-            "tuning": tuning,
+            "tuning": tuning["best"],
             "replay_check": verify,
             "replay_host_ms": host_ms,
             "clocks": clk,
@@ -1230,14 +1502,29 @@ def main():
             "graph": {"slabs_used": info["slabs_used"], "buckets": info["num_buckets"],
                       "device_bytes": info["device_bytes"]},
         }
+        if "bfs_pull" in algo:
+            algo["bfs_pull"].pop("trials", None)
         if cb is not None:
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if cpu_q is not None:
+            line["cpu_queries"] = cpu_q
+        parity = {}
+        if parity_large is not None:
+            line["parity_large"] = parity_large
+            parity["large"] = "ok" if parity_large["ok"] else "MISMATCH"
         if batched is not None:
             line["batched"] = batched
+            if "parity" in batched:
+                parity["batched"] = "ok" if batched["parity"]["ok"] else "MISMATCH"
         if serving is not None:
             line["serving"] = serving
         if grid is not None:
             line["grid"] = grid
+            if "parity" in grid:
+                parity["grid"] = "ok" if grid["parity"]["ok"] else "MISMATCH"
+        line["parity"] = parity
+        # a compact digest last, so a reader of the line's tail sees it
+        line["summary"] = line_summary(line)
         print(json.dumps(line), flush=True)
     barrier(world)
     if world > 1:

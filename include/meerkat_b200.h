@@ -158,7 +158,13 @@ mk_status mk_graph_export_csr_range(mk_graph *g, uint32_t v_begin, uint32_t v_en
  *   - The first call on each device looks the array up and may load the
  *     library's device code; make that first call before any stream capture.
  *   - Calls that overlap in time on one device (different streams, or
- *     host threads) race on the shared scratch: order them on one stream. */
+ *     host threads) race on the shared scratch: order them on one stream.
+ *   - The array's device address is looked up once per device and kept; a
+ *     cudaDeviceReset of that device invalidates it, so do not call this
+ *     entry point on a device after resetting it in the same process.
+ *   - Like the plain export it does not read the graph's sticky error word:
+ *     an update that ran out of slab pool drops edges, so check
+ *     mk_graph_sync before exporting. */
 mk_status mk_graph_export_csr_noalloc(mk_graph *g, uint64_t *d_row_ptr,
                                       uint32_t *d_col, uint32_t *d_w,
                                       void *stream);
@@ -191,7 +197,19 @@ typedef struct mk_tuning {
                                     (mk_traversal_set_reverse): a level whose
                                     frontier holds this share of the vertices
                                     (per mille) is pulled bottom-up; 0 = never */
-  uint32_t reserved[2];
+  uint32_t wait_limit_us;        /* limit of every grid-barrier wait of the
+                                    persistent kernels launched on this graph
+                                    (BFS/SSSP traversals; PageRank on this
+                                    reverse graph), microseconds; 0 = 4 s.  A
+                                    wait past it ends the launch: every block
+                                    leaves and MK_ERR_TIMEOUT is reported (by
+                                    a timed call or a PageRank solve at once,
+                                    else by mk_traversal_distances / _stats);
+                                    that call's results stay undefined until
+                                    the next Static.  Replaces the reference's
+                                    unbounded spins
+                                    (include/Util/Lock.cuh:43-56).             */
+  uint32_t reserved;
 } mk_tuning;
 mk_status mk_graph_set_tuning(mk_graph *g, const mk_tuning *t);
 mk_status mk_graph_get_tuning(mk_graph *g, mk_tuning *t);
@@ -267,6 +285,13 @@ mk_status mk_traversal_packed_host(mk_traversal *t, uint64_t *h_out);
 /* Work counters of the last call: levels run and vertices pushed. */
 mk_status mk_traversal_stats(mk_traversal *t, uint32_t *h_levels,
                              uint64_t *h_pushed);
+/* Repair counters of the last call when it was a Decremental: vertices whose
+ * subtree was invalidated (when the call recomputed, the count at which the
+ * invalidation walk stopped, tuning.recompute_permille of V) and whether it
+ * recomputed from the sources (1) instead of repairing (0).  No counterpart
+ * in the reference, whose Decremental (BFSImpl.cuh:755-846) always repairs. */
+mk_status mk_traversal_decremental_stats(mk_traversal *t, uint64_t *h_invalidated,
+                                         uint32_t *h_recomputed);
 mk_status mk_traversal_destroy(mk_traversal *t);
 
 /* ------------------------------------------------------------------------

@@ -145,16 +145,19 @@ class DynamicGraph:
                    frontier_chunk: Optional[int] = None,
                    sssp_delta: Optional[int] = None,
                    recompute_permille: Optional[int] = None,
-                   pull_permille: Optional[int] = None) -> None:
+                   pull_permille: Optional[int] = None,
+                   wait_limit_us: Optional[int] = None) -> None:
         """Sets the given kernel knobs; the others keep their values."""
         cur = self.get_tuning()
         for k, v in (("update_kernel", update_kernel), ("update_blocks_per_sm", update_blocks_per_sm),
                      ("frontier_chunk", frontier_chunk), ("sssp_delta", sssp_delta),
-                     ("recompute_permille", recompute_permille), ("pull_permille", pull_permille)):
+                     ("recompute_permille", recompute_permille), ("pull_permille", pull_permille),
+                     ("wait_limit_us", wait_limit_us)):
             if v is not None:
                 cur[k] = int(v)
         t = Tuning(cur["update_kernel"], cur["update_blocks_per_sm"], cur["frontier_chunk"],
-                   cur["sssp_delta"], cur["recompute_permille"], cur["pull_permille"])
+                   cur["sssp_delta"], cur["recompute_permille"], cur["pull_permille"],
+                   cur["wait_limit_us"])
         check(lib().mk_graph_set_tuning(self._h, C.byref(t)), "mk_graph_set_tuning")
 
     def get_tuning(self) -> dict:
@@ -162,7 +165,8 @@ class DynamicGraph:
         check(lib().mk_graph_get_tuning(self._h, C.byref(t)), "mk_graph_get_tuning")
         return {"update_kernel": t.update_kernel, "update_blocks_per_sm": t.update_blocks_per_sm,
                 "frontier_chunk": t.frontier_chunk, "sssp_delta": t.sssp_delta,
-                "recompute_permille": t.recompute_permille, "pull_permille": t.pull_permille}
+                "recompute_permille": t.recompute_permille, "pull_permille": t.pull_permille,
+                "wait_limit_us": t.wait_limit_us}
 
     def reserve_batch(self, n: int) -> None:
         check(lib().mk_graph_reserve_batch(self._h, int(n)), "mk_graph_reserve_batch")
@@ -339,6 +343,15 @@ class _Traversal(_Timed):
         pushed = C.c_uint64(0)
         check(lib().mk_traversal_stats(self._h, C.byref(lv), C.byref(pushed)), "stats")
         return lv.value, pushed.value
+
+    def decremental_stats(self):
+        """(vertices invalidated, recomputed from the sources) of the last
+        Decremental call."""
+        inv = C.c_uint64(0)
+        rec = C.c_uint32(0)
+        check(lib().mk_traversal_decremental_stats(self._h, C.byref(inv), C.byref(rec)),
+              "mk_traversal_decremental_stats")
+        return int(inv.value), bool(rec.value)
 
 
 class BFS(_Traversal):

@@ -38,7 +38,7 @@ class Tuning(C.Structure):
     _fields_ = [("update_kernel", C.c_uint32), ("update_blocks_per_sm", C.c_uint32),
                 ("frontier_chunk", C.c_uint32), ("sssp_delta", C.c_uint32),
                 ("recompute_permille", C.c_uint32), ("pull_permille", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("wait_limit_us", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 # (name, restype, argtypes); every function returns mk_status unless noted
@@ -80,6 +80,7 @@ SIGNATURES = [
     ("mk_traversal_distances", _S, [vp, vp]),
     ("mk_traversal_packed", _S, [vp, C.POINTER(vp)]),
     ("mk_traversal_packed_host", _S, [vp, vp]),
+    ("mk_traversal_decremental_stats", _S, [vp, u64p, u32p]),
     ("mk_traversal_stats", _S, [vp, u32p, u64p]),
     ("mk_traversal_destroy", _S, [vp]),
     ("mk_pagerank_create", _S, [vp, C.c_float, C.c_float, C.c_uint32, vp, C.POINTER(vp)]),

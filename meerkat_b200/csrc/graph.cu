@@ -539,11 +539,19 @@ __global__ void __launch_bounds__(kUpdWarps * 32)
   const unsigned long long once = l2_policy_evict_first();
   uint32_t parity[2] = {0u, 0u};
   uint32_t mine = 0;
+  // Staging stops for good once a wait gives up (warp-uniform): the rest of
+  // the warp's groups read their slabs from global memory, so no copy is
+  // issued into a stage whose state is unknown; inflight[s] marks a stage
+  // whose copy was issued and not yet seen complete, drained before exit.
+  bool staging = true;
+  uint32_t inflight[2] = {0u, 0u};
 
   auto edge_of = [&](uint64_t k) { return (warp + k * nwarps) * 32 + lane; };
   auto group_ok = [&](uint64_t k) { return warp + k * nwarps < ngroups; };
   // stage the head slab of this lane's edge (head == kNoSlab: nothing)
   auto stage = [&](uint32_t head, uint32_t st) {
+    if (!staging) return;
+    inflight[st] = 1u;
     const uint32_t valid = __ballot_sync(0xFFFFFFFFu, head != kNoSlab);
     fence_proxy_async_smem();  // this warp's earlier reads of the buffer come first
     __syncwarp();
@@ -592,8 +600,16 @@ __global__ void __launch_bounds__(kUpdWarps * 32)
     if (k) finish(prev, prev_e);
 
     // decide group k from its staged slab
-    const bool ready = mbar_wait(&bars[wib][st], parity[st], g.err);
-    parity[st] ^= 1u;
+    bool ready = false;
+    if (staging) {
+      ready = __all_sync(0xFFFFFFFFu, mbar_wait(&bars[wib][st], parity[st], g.err));
+      if (ready) {
+        parity[st] ^= 1u;
+        inflight[st] = 0u;
+      } else {
+        staging = false;  // inflight[st] stays set: its copy may still land
+      }
+    }
     UpdPending cur{kNoSlab, 0u, 0u, 0u, 0u, 0u, 0u};
     if (head0 != kNoSlab) {
       uint4 q[8];
@@ -620,6 +636,11 @@ __global__ void __launch_bounds__(kUpdWarps * 32)
   finish(prev, prev_e);
   mine = __reduce_add_sync(0xFFFFFFFFu, mine);
   if (lane == 0 && mine) atomicAdd(count, (unsigned long long)mine);
+  // after a wait gave up: give the copies still in flight a bounded time to
+  // land before the block's shared memory is released
+#pragma unroll
+  for (int sidx = 0; sidx < 2; ++sidx)
+    if (inflight[sidx]) mbar_wait(&bars[wib][sidx], parity[sidx], g.err);
 }
 
 // Warp-cooperative update kernel (no shared memory, no bulk copies): a warp

@@ -121,19 +121,19 @@ __device__ __forceinline__ bool grid_barrier(uint32_t *bar, uint32_t *err,
       __threadfence();
       atomicAdd(bar + 1, 1u);
     } else {
-      unsigned long long t0 = global_ns();
+      // the clock is read on every spin, so even a limit of a microsecond
+      // is honoured; another block's timeout is noticed within 16 spins
+      const unsigned long long t0 = global_ns();
       uint32_t spins = 0;
       while (ld_acquire_u32(bar + 1) == gen) {
-        if ((++spins & 63u) == 0) {
-          if (global_ns() - t0 > limit_ns) {
-            atomicOr(err, kErrTimeout);
-            ok = 0;
-            break;
-          }
-          if (ld_relaxed_u32(err) & kErrTimeout) {
-            ok = 0;
-            break;
-          }
+        if (global_ns() - t0 > limit_ns) {
+          atomicOr(err, kErrTimeout);
+          ok = 0;
+          break;
+        }
+        if ((++spins & 15u) == 0 && (ld_relaxed_u32(err) & kErrTimeout)) {
+          ok = 0;
+          break;
         }
         __nanosleep(32);
       }

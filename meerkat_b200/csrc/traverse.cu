@@ -53,6 +53,7 @@ enum Ctl : int {
   kLevels = 9,    // relaxation levels run by the last call
   kDSz0 = 10,     // invalidation frontier sizes kDSz0 + (level % 3)
   kFarN0 = 13,    // near-far SSSP: far list sizes kFarN0 + (list 0 / 1)
+  kRestart = 14,  // decremental: 1 when the call recomputed from the sources
   kRound = 15,    // stamp base, persists across calls
   kFarMin0 = 16,  // near-far SSSP: smallest distance on far list 0 / 1 (set in-kernel)
   kCtlWords = 20
@@ -506,6 +507,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       // bits are cleared in the epilogue as usual.
       for (uint32_t v = tid; v < a.g.V; v += nthreads) a.dist[v] = kInfInf;
       if (tid == 0) {
+        ctl[kRestart] = 1u;
         ctl[kThr] = a.delta;
         ctl[kFarMin0] = kNoFar;
         ctl[kFarMin0 + 1] = kNoFar;
@@ -897,7 +899,7 @@ static mk_status trav_issue(mk_traversal *t, uint32_t mode, const uint32_t *bs, 
   a.far1 = t->far1;
   a.fbits = t->fbits;
   a.mode = mode;
-  a.limit_ns = 4000000000ull;
+  a.limit_ns = g->wait_limit_ns();
   const void *fn;
   if (g->weighted)
     fn = t->sssp ? (const void *)k_traverse<true, true> : (const void *)k_traverse<true, false>;
@@ -918,6 +920,11 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   MK_CHECK(t->timer.start(s, ms_out != nullptr));
   MK_CHECK(trav_issue(t, mode, bs, bd, n, s, nullptr, 0));
   MK_CHECK(t->timer.stop(ms_out));
+  if (ms_out) {  // the call has synchronised: report a barrier that gave up
+    uint32_t err = 0;
+    MK_CUDA(cudaMemcpy(&err, t->ctl + kErr, 4, cudaMemcpyDeviceToHost));
+    if (err & kErrTimeout) return fail(MK_ERR_TIMEOUT, "traversal: grid barrier timed out");
+  }
   if (mode == kStatic) t->has_static = true;
   return MK_OK;
 }
@@ -1135,6 +1142,19 @@ mk_status mk_traversal_stats(mk_traversal *t, uint32_t *h_levels, uint64_t *h_pu
   MK_CUDA(cudaMemcpy(&p, t->pushed, 8, cudaMemcpyDeviceToHost));
   if (h_levels) *h_levels = ctl[kLevels];
   if (h_pushed) *h_pushed = p;
+  if (ctl[kErr] & kErrTimeout) return fail(MK_ERR_TIMEOUT, "traversal: grid barrier timed out");
+  return MK_OK;
+}
+
+mk_status mk_traversal_decremental_stats(mk_traversal *t, uint64_t *h_invalidated,
+                                         uint32_t *h_recomputed) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_traversal_decremental_stats: null handle");
+  DeviceGuard dg(t->g->device);
+  MK_CUDA(cudaDeviceSynchronize());
+  uint32_t ctl[kCtlWords];
+  MK_CUDA(cudaMemcpy(ctl, t->ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+  if (h_invalidated) *h_invalidated = ctl[kInvCount];
+  if (h_recomputed) *h_recomputed = ctl[kRestart];
   if (ctl[kErr] & kErrTimeout) return fail(MK_ERR_TIMEOUT, "traversal: grid barrier timed out");
   return MK_OK;
 }

@@ -441,15 +441,22 @@ static void sym_csr(const og *g, uint64_t **rp_out, uint32_t **col_out) {
       col[fill[u]++] = v;
       col[fill[v]++] = u;
     }
-  /* sort + unique each row, compact */
+  /* sort + unique each row in place (rows in parallel), then compact */
+  uint64_t *len = cnt;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t uu = 0; uu < (int64_t)V; ++uu) {
+    uint64_t b = rp[uu], e = rp[uu + 1], k = b;
+    qsort(col + b, e - b, 4, cmp_u32);
+    for (uint64_t i = b; i < e; ++i)
+      if (i == b || col[i] != col[i - 1]) col[k++] = col[i];
+    len[uu] = k - b;
+  }
   uint64_t w = 0;
   for (uint32_t u = 0; u < V; ++u) {
-    uint64_t b = rp[u], e = rp[u + 1];
-    qsort(col + b, e - b, 4, cmp_u32);
-    uint64_t start = w;
-    for (uint64_t i = b; i < e; ++i)
-      if (i == b || col[i] != col[i - 1]) col[w++] = col[i];
-    rp[u] = start;
+    uint64_t b = rp[u];
+    rp[u] = w;
+    memmove(col + w, col + b, (size_t)len[u] * 4);
+    w += len[u];
   }
   rp[V] = w;
   free(cnt);

@@ -183,12 +183,12 @@ def test_tuning_round_trip_and_validation():
     G, _ = make_pair(64, np.array([1], np.uint32), np.array([2], np.uint32))
     assert G.get_tuning() == {"update_kernel": 0, "update_blocks_per_sm": 0, "frontier_chunk": 0,
                               "sssp_delta": 0, "recompute_permille": 100,
-                              "pull_permille": 0}
+                              "pull_permille": 0, "wait_limit_us": 0}
     G.set_tuning(update_kernel=1, update_blocks_per_sm=3)
     G.set_tuning(frontier_chunk=16)  # keeps the other knobs
     assert G.get_tuning() == {"update_kernel": 1, "update_blocks_per_sm": 3, "frontier_chunk": 16,
                               "sssp_delta": 0, "recompute_permille": 100,
-                              "pull_permille": 0}
+                              "pull_permille": 0, "wait_limit_us": 0}
     with pytest.raises(mk.MeerkatError):
         G.set_tuning(update_kernel=7)
     with pytest.raises(mk.MeerkatError):

@@ -97,6 +97,28 @@ def test_noalloc_export_matches_plain_export_on_consecutive_calls(weighted):
     G.close()
 
 
+def test_noalloc_export_at_its_bucket_limit():
+    """A graph of exactly 262,144 buckets: the last tile of the scan and the
+    final row offset sit at the end of the fixed scratch."""
+    V = MAX_BUCKETS  # no hints: one bucket per vertex
+    rng = np.random.default_rng(11)
+    s = rng.integers(0, V, 5000).astype(np.uint32)
+    d = rng.integers(0, V, 5000).astype(np.uint32)
+    s[:3] = V - 1  # rows at the very end of the range
+    d[:3] = np.array([0, 1, 2], np.uint32)
+    G = mk.DynamicGraph(V, weighted=True)
+    G.InsertEdges(to_dev(s), to_dev(d), vals=to_dev(np.arange(5000, dtype=np.uint32) % 97 + 1))
+    assert G.sync() == 0
+    assert G.info()["num_buckets"] == MAX_BUCKETS
+    E = G.info()["num_edges"]
+    for _ in range(2):
+        got = export(G, "mk_graph_export_csr_noalloc")
+        plain = export(G, "mk_graph_export_csr")
+        assert_same(got, plain)
+        assert got[0][-1] == E
+    G.close()
+
+
 def test_noalloc_export_rejects_graphs_beyond_its_scratch():
     G = mk.DynamicGraph(MAX_BUCKETS + 1000)  # one bucket per vertex
     assert G.info()["num_buckets"] > MAX_BUCKETS
