@@ -112,6 +112,12 @@ mk_status mk_graph_search_edges(mk_graph *g, const uint32_t *d_src,
 /* Waits for the graph's work on `stream`, returns MK_OK or the first error and
  * writes the sticky device error bits (MK_DEVERR_*) to *h_deverr if given. */
 mk_status mk_graph_sync(mk_graph *g, void *stream, uint32_t *h_deverr);
+/* Stream-ordered copy of the slabs in use (head + allocated overflow slabs,
+ * mk_graph_info.slabs_used; capacity: pool_capacity) into *h_slabs_used
+ * (pinned host memory for an asynchronous copy).  A server admits inserts
+ * against it: an insert of n edges needs at most n new slabs.  No
+ * counterpart in the reference, which has no OOM reporting. */
+mk_status mk_graph_slabs_used_async(mk_graph *g, uint32_t *h_slabs_used, void *stream);
 /* Number of batch edges the last insert/delete actually applied (synchronises). */
 mk_status mk_graph_last_applied(mk_graph *g, uint64_t *h_count);
 /* Stream-ordered copy of the same count into h_count (pinned host memory for
@@ -241,6 +247,14 @@ mk_status mk_sssp_create_multi(mk_graph *g, const uint32_t *h_sources, uint32_t 
  * one multi-source query per round with one resident traversal.  No
  * counterpart in the reference. */
 mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, uint32_t n);
+/* Stream-ordered form of mk_traversal_set_sources: the new sources reach the
+ * device on `stream`, after the launches queued there before the call, and
+ * the call waits for no other device work (a server issues its rounds
+ * without stalling on another stream).  The traversal must not have work in
+ * flight on any other stream.  Growing past the largest source count seen
+ * synchronises the device once. */
+mk_status mk_traversal_set_sources_async(mk_traversal *t, const uint32_t *h_sources, uint32_t n,
+                                         void *stream);
 /* Attaches the reverse graph (in-edges) of the same edge set (for SSSP:
  * weighted, with the same weights): static BFS pulls large levels
  * (tuning.pull_permille), and decremental BFS/SSSP re-seed invalidated
@@ -366,6 +380,27 @@ mk_status mk_tc_decremental(mk_tc *t, const uint32_t *d_src,
 mk_status mk_tc_count(mk_tc *t, uint64_t *h_count);
 mk_status mk_tc_destroy(mk_tc *t);
 
+/* Triangles of the symmetrised vertex range [v_begin, v_end) of an OUT-edge
+ * graph (a member of a graph set), without a symmetric copy: the member's
+ * edges are exported, each edge probes for its reverse, and the undirected
+ * edges are oriented by (symmetric degree, id) as in mk_tc_static.  The
+ * count equals mk_tc_static's on the member's symmetrised simple graph.
+ * The range must be closed under out-edges (an edge leaving it is skipped
+ * and sets MK_DEVERR_INVALID_ID on the graph).  run synchronises its stream
+ * twice (edge count, work sizes); its scratch grows to the largest range
+ * seen and is kept.  No counterpart in the reference, whose TC<> needs the
+ * symmetric graph (TC.cuh:9-40). */
+typedef struct mk_tc_range mk_tc_range;
+mk_status mk_tc_range_create(mk_graph *g, mk_tc_range **out);
+mk_status mk_tc_range_run(mk_tc_range *t, uint32_t v_begin, uint32_t v_end, void *stream,
+                          float *ms_out);
+/* The last run's count (synchronises). */
+mk_status mk_tc_range_count(mk_tc_range *t, uint64_t *h_count);
+/* Stream-ordered copy of the last run's count into h_count (pinned host
+ * memory for a truly asynchronous copy). */
+mk_status mk_tc_range_count_async(mk_tc_range *t, uint64_t *h_count, void *stream);
+mk_status mk_tc_range_destroy(mk_tc_range *t);
+
 /* ------------------------------------------------------------------------
  * Weakly connected components by lock-free union-find with min-id labels.
  * The reference ships only the device primitives
@@ -398,6 +433,13 @@ mk_status mk_wcc_static_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges,
 mk_status mk_wcc_prepare_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges,
                                 uint32_t nranges);
 mk_status mk_wcc_static_prepared(mk_wcc *w, void *stream, float *ms_out);
+/* Stream-ordered form of mk_wcc_prepare_ranges: the table reaches the device
+ * on `stream` after the launches queued there before the call; no other
+ * device work is waited for.  The WCC handle must not have work in flight on
+ * another stream.  A table larger than any prepared before synchronises the
+ * device once. */
+mk_status mk_wcc_prepare_ranges_async(mk_wcc *w, const uint32_t *h_vertex_ranges,
+                                      uint32_t nranges, void *stream);
 mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src,
                              const uint32_t *d_dst, uint32_t n, void *stream,
                              float *ms_out);

@@ -19,7 +19,8 @@ import numpy as np
 from ._lib import (DEVERR_INVALID_ID, DEVERR_OOM, DEVERR_OVERFLOW, DEVERR_TIMEOUT, MK_INF,
                    GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
-__all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "PageRankRange", "TC", "WCC",
+__all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "PageRankRange", "TC", "TCRange",
+           "WCC",
            "EdgeSet",
            "gen_rmat", "gen_grid", "gen_rmat_members", "read_edge_list", "read_batch",
            "write_edge_list", "write_batch", "MeerkatError", "MK_INF", "DEVERR_INVALID_ID",
@@ -181,6 +182,11 @@ class DynamicGraph:
         check(lib().mk_graph_last_applied(self._h, C.byref(c)), "mk_graph_last_applied")
         return c.value
 
+    def slabs_used_async(self, host_ptr: int, stream=None) -> None:
+        """Stream-ordered copy of the slabs in use to host_ptr (pinned u32)."""
+        check(lib().mk_graph_slabs_used_async(self._h, host_ptr, _stream(stream)),
+              "mk_graph_slabs_used_async")
+
     def last_applied_async(self, host_ptr: int, stream=None) -> None:
         """Stream-ordered copy of the applied count to host_ptr (pinned u64)."""
         check(lib().mk_graph_last_applied_async(self._h, host_ptr, _stream(stream)),
@@ -298,12 +304,20 @@ class _Traversal(_Timed):
         except Exception:
             pass
 
-    def set_sources(self, sources) -> None:
-        """Replaces the source set (distinct vertices); call Static next."""
+    def set_sources(self, sources, stream=None) -> None:
+        """Replaces the source set (distinct vertices); call Static next.
+        With a stream the upload is stream-ordered on it and waits for no
+        other device work (mk_traversal_set_sources_async)."""
         self.sources = np.ascontiguousarray(np.atleast_1d(np.asarray(sources, dtype=np.uint32)))
         self.source = self.sources
-        check(lib().mk_traversal_set_sources(self._h, self.sources.ctypes.data_as(
-            C.POINTER(C.c_uint32)), len(self.sources)), "mk_traversal_set_sources")
+        p = self.sources.ctypes.data_as(C.POINTER(C.c_uint32))
+        if stream is None:
+            check(lib().mk_traversal_set_sources(self._h, p, len(self.sources)),
+                  "mk_traversal_set_sources")
+        else:
+            check(lib().mk_traversal_set_sources_async(self._h, p, len(self.sources),
+                                                       _stream(stream)),
+                  "mk_traversal_set_sources_async")
 
     def set_reverse(self, G_rev: Optional[DynamicGraph]) -> None:
         """Attaches the reverse graph of the same edges (BFS pull levels)."""
@@ -512,6 +526,42 @@ class TC(_Timed):
         return c.value
 
 
+class TCRange(_Timed):
+    """Triangles of one vertex range of an out-edge graph (a graph-set
+    member), symmetrised, without a symmetric copy (mk_tc_range_*)."""
+
+    def __init__(self, G: DynamicGraph):
+        self.G = G
+        h = C.c_void_p()
+        check(lib().mk_tc_range_create(G.handle, C.byref(h)), "mk_tc_range_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mk_tc_range_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def Run(self, v_begin: int, v_end: int, stream=None, timed=True):
+        return self._call(lib().mk_tc_range_run, self._h, int(v_begin), int(v_end),
+                          _stream(stream), timed=timed)
+
+    def GetCount(self) -> int:
+        c = C.c_uint64(0)
+        check(lib().mk_tc_range_count(self._h, C.byref(c)), "mk_tc_range_count")
+        return int(c.value)
+
+    def count_async(self, host_ptr: int, stream=None) -> None:
+        """Stream-ordered copy of the count to host_ptr (pinned, 8 bytes)."""
+        check(lib().mk_tc_range_count_async(self._h, C.c_void_p(host_ptr), _stream(stream)),
+              "mk_tc_range_count_async")
+
+
 class WCC(_Timed):
     """Connected components (new entry points over include/Util/UnionFind.cuh)."""
 
@@ -543,13 +593,18 @@ class WCC(_Timed):
                           r.ctypes.data_as(C.POINTER(C.c_uint32)), len(r) // 2, _stream(stream),
                           timed=timed)
 
-    def PrepareRanges(self, ranges):
+    def PrepareRanges(self, ranges, stream=None):
         """Uploads a vertex-range table [(begin, end), ...] for StaticPrepared
-        (blocking).  Ranges of at most 65,536 vertices are each solved by one
-        CTA in shared memory; larger ones by the device-wide pass."""
+        (blocking; with a stream, stream-ordered on it instead).  Ranges of at
+        most 65,536 vertices are each solved by one CTA in shared memory;
+        larger ones by the device-wide pass."""
         r = np.ascontiguousarray(np.asarray(ranges, dtype=np.uint32).reshape(-1))
-        check(lib().mk_wcc_prepare_ranges(self._h, r.ctypes.data_as(C.POINTER(C.c_uint32)),
-                                          len(r) // 2), "mk_wcc_prepare_ranges")
+        p = r.ctypes.data_as(C.POINTER(C.c_uint32))
+        if stream is None:
+            check(lib().mk_wcc_prepare_ranges(self._h, p, len(r) // 2), "mk_wcc_prepare_ranges")
+        else:
+            check(lib().mk_wcc_prepare_ranges_async(self._h, p, len(r) // 2, _stream(stream)),
+                  "mk_wcc_prepare_ranges_async")
 
     def StaticPrepared(self, stream=None, timed=True):
         """StaticRanges over the prepared table; only asynchronous work on the

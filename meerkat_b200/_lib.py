@@ -52,6 +52,7 @@ SIGNATURES = [
     ("mk_graph_delete_edges", _S, [vp, vp, vp, C.c_uint32, vp]),
     ("mk_graph_search_edges", _S, [vp, vp, vp, C.c_uint32, vp, vp, vp]),
     ("mk_graph_sync", _S, [vp, vp, u32p]),
+    ("mk_graph_slabs_used_async", _S, [vp, vp, vp]),
     ("mk_graph_last_applied", _S, [vp, u64p]),
     ("mk_graph_last_applied_async", _S, [vp, vp, vp]),
     ("mk_graph_last_applied_flags", _S, [vp, C.POINTER(vp), u32p]),
@@ -71,6 +72,7 @@ SIGNATURES = [
     ("mk_bfs_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
     ("mk_sssp_create_multi", _S, [vp, u32p, C.c_uint32, C.POINTER(vp)]),
     ("mk_traversal_set_sources", _S, [vp, u32p, C.c_uint32]),
+    ("mk_traversal_set_sources_async", _S, [vp, vp, C.c_uint32, vp]),
     ("mk_traversal_set_reverse", _S, [vp, vp]),
     ("mk_traversal_static", _S, [vp, vp, f32p]),
     ("mk_bfs_prepare_members", _S, [vp, u32p, C.c_uint32]),
@@ -103,12 +105,18 @@ SIGNATURES = [
     ("mk_tc_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_tc_decremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_tc_count", _S, [vp, u64p]),
+    ("mk_tc_range_create", _S, [vp, C.POINTER(vp)]),
+    ("mk_tc_range_run", _S, [vp, C.c_uint32, C.c_uint32, vp, f32p]),
+    ("mk_tc_range_count", _S, [vp, u64p]),
+    ("mk_tc_range_count_async", _S, [vp, vp, vp]),
+    ("mk_tc_range_destroy", _S, [vp]),
     ("mk_tc_destroy", _S, [vp]),
     ("mk_wcc_create", _S, [vp, C.POINTER(vp)]),
     ("mk_wcc_static", _S, [vp, vp, f32p]),
     ("mk_wcc_static_subset", _S, [vp, vp, vp, f32p]),
     ("mk_wcc_static_ranges", _S, [vp, u32p, C.c_uint32, vp, f32p]),
     ("mk_wcc_prepare_ranges", _S, [vp, u32p, C.c_uint32]),
+    ("mk_wcc_prepare_ranges_async", _S, [vp, vp, C.c_uint32, vp]),
     ("mk_wcc_static_prepared", _S, [vp, vp, f32p]),
     ("mk_wcc_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_decremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),

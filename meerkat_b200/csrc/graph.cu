@@ -91,6 +91,34 @@ mk_status Timer::stop(float *ms_out) {
   return MK_OK;
 }
 
+mk_status PinnedRing::upload(void *d_dst, const void *src, size_t bytes, cudaStream_t s) {
+  Slot &sl = slots[next++ % kSlots];
+  if (sl.used) MK_CUDA(cudaEventSynchronize(sl.done));  // the copy that last read this slot
+  if (sl.cap < bytes) {
+    if (sl.host) cudaFreeHost(sl.host);
+    sl.host = nullptr;
+    sl.cap = 0;
+    const size_t want = std::max<size_t>(bytes, 64 * 1024);
+    MK_CUDA(cudaMallocHost(&sl.host, want));
+    sl.cap = want;
+  }
+  if (!sl.done) MK_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+  std::memcpy(sl.host, src, bytes);
+  MK_CUDA(cudaMemcpyAsync(d_dst, sl.host, bytes, cudaMemcpyHostToDevice, s));
+  MK_CUDA(cudaEventRecord(sl.done, s));
+  sl.used = true;
+  return MK_OK;
+}
+
+void PinnedRing::release() {
+  for (Slot &sl : slots) {
+    if (sl.used) cudaEventSynchronize(sl.done);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.host) cudaFreeHost(sl.host);
+    sl = Slot();
+  }
+}
+
 Timer::~Timer() {
   if (a) cudaEventDestroy(a);
   if (b) cudaEventDestroy(b);
@@ -1315,6 +1343,13 @@ mk_status mk_graph_sync(mk_graph *g, void *stream, uint32_t *h_deverr) {
     return fail(MK_ERR_INVALID,
                 "vertex id out of range: a batch id >= num_vertices, or an edge leaving the "
                 "vertex range of a range call");
+  return MK_OK;
+}
+
+mk_status mk_graph_slabs_used_async(mk_graph *g, uint32_t *h_slabs_used, void *stream) {
+  if (!g || !h_slabs_used) return fail(MK_ERR_INVALID, "mk_graph_slabs_used_async: null argument");
+  DeviceGuard dg(g->device);
+  MK_CUDA(cudaMemcpyAsync(h_slabs_used, g->pool_top, 4, cudaMemcpyDeviceToHost, as_stream(stream)));
   return MK_OK;
 }
 

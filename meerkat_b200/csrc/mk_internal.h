@@ -87,6 +87,25 @@ struct Timer {
   ~Timer();
 };
 
+// Pinned host staging of small host tables (sources, range tables) for
+// stream-ordered uploads: a ring of slots, each reused only once the copy
+// that last read it has finished, so an upload never waits for the device
+// unless the ring wraps onto a copy still queued.
+struct PinnedRing {
+  static constexpr int kSlots = 4;
+  struct Slot {
+    void *host = nullptr;
+    size_t cap = 0;
+    cudaEvent_t done = nullptr;
+    bool used = false;
+  };
+  Slot slots[kSlots];
+  uint32_t next = 0;
+  // Copies `bytes` from src into a slot and queues its copy to d_dst on s.
+  mk_status upload(void *d_dst, const void *src, size_t bytes, cudaStream_t s);
+  void release();
+};
+
 // Exclusive scan of n u32 counts into u64 offsets (out has n+1 entries).
 mk_status scan_u32_to_u64(const uint32_t *d_in, unsigned long long *d_out,
                           uint32_t n, DevBuf<unsigned long long> &tmp,

@@ -469,6 +469,79 @@ __global__ void k_tc_apply(unsigned long long *count, const unsigned long long *
     *count -= *acc;
 }
 
+// ---- triangles of one vertex range of a directed graph -----------------
+// The symmetrised member is never built: its edges come from a CSR export
+// of the member's out-edges, each edge (u, v) probes the slab table of v for
+// the reverse edge (v, u), and the symmetric degree is out + in - reciprocal.
+// An undirected edge present in both directions is kept once (from its
+// smaller endpoint), then oriented by (symmetric degree, id) like the static
+// path, and the same forward algorithm counts.
+
+// rowid[e] = local row of CSR edge e: one warp per row, so hubs are written
+// with coalesced stores.
+__global__ void k_trc_rows(const unsigned long long *__restrict__ rp, uint32_t n,
+                           uint32_t *__restrict__ rowid) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
+  for (uint64_t u = warp; u < n; u += nwarps)
+    for (unsigned long long e = rp[u] + lane; e < rp[u + 1]; e += 32) rowid[e] = (uint32_t)u;
+}
+
+// Per edge (u, v): range check, reverse-edge probe, in-degree and
+// reciprocal counts.  rflag[e] = 1 when (v, u) is present, 0 when not, 2 for
+// an edge leaving the range (skipped; sets kErrInvalidId on the graph).
+template <bool kW>
+__global__ void k_trc_probe(GraphView g, uint32_t lo, uint32_t n, const uint32_t *__restrict__ rowid,
+                            const uint32_t *__restrict__ col, unsigned long long E,
+                            uint8_t *__restrict__ rflag, uint32_t *__restrict__ indeg,
+                            uint32_t *__restrict__ recip) {
+  for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < E;
+       e += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t u = rowid[e], v = col[e];
+    if (v < lo || v - lo >= n) {
+      atomicOr(g.err, kErrInvalidId);
+      rflag[e] = 2;
+      continue;
+    }
+    const bool r = lane_find<kW>(g, v, lo + u);
+    rflag[e] = r ? 1 : 0;
+    atomicAdd(indeg + (v - lo), 1u);
+    if (r) atomicAdd(recip + u, 1u);
+  }
+}
+
+__global__ void k_trc_dsym(const uint32_t *__restrict__ deg, uint32_t lo, uint32_t n,
+                           const uint32_t *__restrict__ indeg, const uint32_t *__restrict__ recip,
+                           uint32_t *__restrict__ dsym) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+    dsym[u] = deg[lo + u] + indeg[u] - recip[u];
+}
+
+// Orientation of the undirected edges: kFill = false counts the oriented
+// degree of each lower-ranked endpoint, kFill = true writes the higher one
+// into its row (positions taken with an atomic per row; the forward
+// algorithm does not need sorted rows).
+template <bool kFill>
+__global__ void k_trc_orient(const uint32_t *__restrict__ rowid, const uint32_t *__restrict__ col,
+                             uint32_t lo, unsigned long long E, const uint8_t *__restrict__ rflag,
+                             const uint32_t *__restrict__ dsym, uint32_t *__restrict__ ocnt,
+                             const unsigned long long *__restrict__ orow, uint32_t *__restrict__ ocol) {
+  for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < E;
+       e += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint8_t f = rflag[e];
+    if (f == 2) continue;
+    const uint32_t u = rowid[e], v = col[e] - lo;
+    if (f == 1 && u > v) continue;  // both directions present: keep (min, max) once
+    const bool ux = rank_less(dsym[u], u, dsym[v], v);
+    const uint32_t x = ux ? u : v, y = ux ? v : u;
+    if (!kFill)
+      atomicAdd(ocnt + x, 1u);
+    else
+      ocol[orow[x] + atomicAdd(ocnt + x, 1u)] = y;
+  }
+}
+
 }  // namespace mk
 
 using namespace mk;
@@ -482,11 +555,20 @@ struct mk_tc {
   Timer timer;
 };
 
+struct mk_tc_range {
+  mk_tc core;  // orow / ocol and the counting scratch; core.g is the directed graph
+  DevBuf<unsigned long long> rp;
+  DevBuf<uint32_t> col, rowid, indeg, recip, dsym;
+  DevBuf<uint8_t> rflag;
+};
+
 static int groups_grid(uint64_t items, int device) {
   uint64_t b = items * 8 / 256 + 1;
   uint64_t cap = (uint64_t)device_sm_count(device) * 8;
   return (int)std::min(b, cap);
 }
+
+static mk_status tc_count_oriented(mk_tc *t, uint32_t V, int device, cudaStream_t s);
 
 static mk_status tc_static(mk_tc *t, cudaStream_t s) {
   mk_graph *g = t->g;
@@ -512,13 +594,22 @@ static mk_status tc_static(mk_tc *t, cudaStream_t s) {
     k_orient_fill<true><<<blocks, 256, 0, s>>>(gv, t->bpos.ptr, t->ocol.ptr);
   else
     k_orient_fill<false><<<blocks, 256, 0, s>>>(gv, t->bpos.ptr, t->ocol.ptr);
+  MK_CUDA(cudaGetLastError());
+  return tc_count_oriented(t, V, g->device, s);
+}
+
+// The forward algorithm on the oriented CSR in t->orow / t->ocol over V
+// vertices; the count lands in t->dcount[0].  t->ocnt (>= V words) and
+// t->bpos (>= V + 1) serve as scratch.
+static mk_status tc_count_oriented(mk_tc *t, uint32_t V, int device, cudaStream_t s) {
+  size_t acc = 0;
   MK_CHECK(t->big_list.reserve(V, &acc));
   MK_CUDA(cudaMemsetAsync(t->dcount, 0, 8, s));
   // [0] big count, [1] work-item counter, [2] largest big oriented degree
   MK_CUDA(cudaMemsetAsync(t->small, 0, 16, s));
   // work items (the orientation scratch is free again: ocnt >= V words,
   // bpos >= V + 1)
-  const int vb = (int)std::min<uint64_t>((uint64_t)V / 256 + 1, (uint64_t)device_sm_count(g->device) * 8);
+  const int vb = (int)std::min<uint64_t>((uint64_t)V / 256 + 1, (uint64_t)device_sm_count(device) * 8);
   k_tc_item_count<<<vb, 256, 0, s>>>(V, t->orow.ptr, t->ocnt.ptr, t->big_list.ptr, t->small,
                                      t->small + 2);
   MK_CHECK(scan_u32_to_u64(t->ocnt.ptr, t->bpos.ptr, V, t->tmp, s));
@@ -531,7 +622,7 @@ static mk_status tc_static(mk_tc *t, cudaStream_t s) {
   k_tc_item_fill<<<vb, 256, 0, s>>>(V, t->ocnt.ptr, t->bpos.ptr, t->items.ptr);
   int per_sm = 0;
   MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_small, kTcWarps * 32, 0));
-  const int sblocks = device_sm_count(g->device) * std::max(per_sm, 1);
+  const int sblocks = device_sm_count(device) * std::max(per_sm, 1);
   k_tc_small<<<sblocks, kTcWarps * 32, 0, s>>>(t->orow.ptr, t->ocol.ptr, t->items.ptr,
                                               t->bpos.ptr + V, t->small + 1, t->dcount);
   // big vertices: one block each, global-memory set
@@ -541,7 +632,7 @@ static mk_status tc_static(mk_tc *t, cudaStream_t s) {
     const uint32_t mx = hs[2];
     uint32_t cap = 64;
     while (cap < 2ull * mx) cap <<= 1;
-    int bb = std::min<uint32_t>(nbig, (uint32_t)device_sm_count(g->device) * 2);
+    int bb = std::min<uint32_t>(nbig, (uint32_t)device_sm_count(device) * 2);
     MK_CHECK(t->big_scratch.reserve((size_t)bb * cap, &acc));
     k_tc_big<<<bb, 512, 0, s>>>(t->orow.ptr, t->ocol.ptr, t->big_list.ptr, t->small,
                                 t->big_scratch.ptr, cap, t->dcount);
@@ -650,6 +741,115 @@ mk_status mk_tc_count(mk_tc *t, uint64_t *h_count) {
   unsigned long long c = 0;
   MK_CUDA(cudaMemcpy(&c, t->dcount, 8, cudaMemcpyDeviceToHost));
   *h_count = c;
+  return MK_OK;
+}
+
+mk_status mk_tc_range_create(mk_graph *g, mk_tc_range **out) {
+  if (!g || !out) return fail(MK_ERR_INVALID, "mk_tc_range_create: null argument");
+  if (g->reverse) return fail(MK_ERR_INVALID, "mk_tc_range_create: needs an out-edge graph");
+  *out = nullptr;
+  DeviceGuard dg(g->device);
+  mk_tc_range *t = new mk_tc_range();
+  t->core.g = g;
+  cudaError_t e = cudaMalloc(&t->core.dcount, 16);
+  if (e == cudaSuccess) e = cudaMalloc(&t->core.small, 16);
+  if (e == cudaSuccess) e = cudaMemset(t->core.dcount, 0, 16);
+  if (e != cudaSuccess) {
+    mk_tc_range_destroy(t);
+    return cuda_fail(e, "mk_tc_range_create");
+  }
+  *out = t;
+  return MK_OK;
+}
+
+mk_status mk_tc_range_run(mk_tc_range *t, uint32_t v_begin, uint32_t v_end, void *stream,
+                          float *ms_out) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_tc_range_run: null handle");
+  mk_graph *g = t->core.g;
+  if (v_begin >= v_end || v_end > g->V) return fail(MK_ERR_INVALID, "mk_tc_range_run: bad vertex range");
+  DeviceGuard dg(g->device);
+  cudaStream_t s = as_stream(stream);
+  MK_CHECK(t->core.timer.start(s, ms_out != nullptr));
+  const uint32_t lo = v_begin, n = v_end - v_begin;
+  uint64_t E = 0;
+  MK_CHECK(mk_graph_count_edges_range(g, v_begin, v_end, stream, &E));
+  const size_t e1 = std::max<uint64_t>(E, 1);
+  size_t acc = 0;
+  MK_CHECK(t->rp.reserve((size_t)n + 1, &acc));
+  MK_CHECK(t->col.reserve(e1, &acc));
+  MK_CHECK(t->rowid.reserve(e1, &acc));
+  MK_CHECK(t->rflag.reserve(e1, &acc));
+  MK_CHECK(t->indeg.reserve(n, &acc));
+  MK_CHECK(t->recip.reserve(n, &acc));
+  MK_CHECK(t->dsym.reserve(n, &acc));
+  mk_tc *c = &t->core;
+  MK_CHECK(c->ocnt.reserve(n, &acc));
+  MK_CHECK(c->bpos.reserve((size_t)n + 1, &acc));
+  MK_CHECK(c->orow.reserve((size_t)n + 1, &acc));
+  MK_CHECK(c->ocol.reserve(e1, &acc));
+  MK_CHECK(mk_graph_export_csr_range(g, v_begin, v_end, reinterpret_cast<uint64_t *>(t->rp.ptr),
+                                     t->col.ptr, nullptr, stream));
+  MK_CUDA(cudaMemsetAsync(t->indeg.ptr, 0, (size_t)n * 4, s));
+  MK_CUDA(cudaMemsetAsync(t->recip.ptr, 0, (size_t)n * 4, s));
+  MK_CUDA(cudaMemsetAsync(c->ocnt.ptr, 0, (size_t)n * 4, s));
+  const int sms = device_sm_count(g->device);
+  const int rb = (int)std::min<uint64_t>((uint64_t)n / 8 + 1, (uint64_t)sms * 8);
+  k_trc_rows<<<rb, 256, 0, s>>>(t->rp.ptr, n, t->rowid.ptr);
+  const int eb = (int)std::min<uint64_t>(E / 256 + 1, (uint64_t)sms * 16);
+  if (g->weighted)
+    k_trc_probe<true><<<eb, 256, 0, s>>>(g->view(), lo, n, t->rowid.ptr, t->col.ptr, E,
+                                         t->rflag.ptr, t->indeg.ptr, t->recip.ptr);
+  else
+    k_trc_probe<false><<<eb, 256, 0, s>>>(g->view(), lo, n, t->rowid.ptr, t->col.ptr, E,
+                                          t->rflag.ptr, t->indeg.ptr, t->recip.ptr);
+  const int vb = (int)std::min<uint64_t>((uint64_t)n / 256 + 1, (uint64_t)sms * 8);
+  k_trc_dsym<<<vb, 256, 0, s>>>(g->deg, lo, n, t->indeg.ptr, t->recip.ptr, t->dsym.ptr);
+  k_trc_orient<false><<<eb, 256, 0, s>>>(t->rowid.ptr, t->col.ptr, lo, E, t->rflag.ptr,
+                                         t->dsym.ptr, c->ocnt.ptr, nullptr, nullptr);
+  MK_CHECK(scan_u32_to_u64(c->ocnt.ptr, c->orow.ptr, n, c->tmp, s));
+  MK_CUDA(cudaMemsetAsync(c->ocnt.ptr, 0, (size_t)n * 4, s));
+  k_trc_orient<true><<<eb, 256, 0, s>>>(t->rowid.ptr, t->col.ptr, lo, E, t->rflag.ptr,
+                                        t->dsym.ptr, c->ocnt.ptr, c->orow.ptr, c->ocol.ptr);
+  MK_CUDA(cudaGetLastError());
+  MK_CHECK(tc_count_oriented(c, n, g->device, s));
+  return c->timer.stop(ms_out);
+}
+
+mk_status mk_tc_range_count(mk_tc_range *t, uint64_t *h_count) {
+  if (!t) return fail(MK_ERR_INVALID, "mk_tc_range_count: null handle");
+  return mk_tc_count(&t->core, h_count);
+}
+
+mk_status mk_tc_range_count_async(mk_tc_range *t, uint64_t *h_count, void *stream) {
+  if (!t || !h_count) return fail(MK_ERR_INVALID, "mk_tc_range_count_async: null argument");
+  DeviceGuard dg(t->core.g->device);
+  MK_CUDA(cudaMemcpyAsync(h_count, t->core.dcount, 8, cudaMemcpyDeviceToHost, as_stream(stream)));
+  return MK_OK;
+}
+
+mk_status mk_tc_range_destroy(mk_tc_range *t) {
+  if (!t) return MK_OK;
+  DeviceGuard dg(t->core.g->device);
+  t->rp.release();
+  t->col.release();
+  t->rowid.release();
+  t->indeg.release();
+  t->recip.release();
+  t->dsym.release();
+  t->rflag.release();
+  // the core's buffers are released by its own destructor path
+  mk_tc *c = &t->core;
+  cudaFree(c->dcount);
+  cudaFree(c->small);
+  c->ocnt.release();
+  c->ocol.release();
+  c->big_list.release();
+  c->big_scratch.release();
+  c->orow.release();
+  c->tmp.release();
+  c->bpos.release();
+  c->items.release();
+  delete t;
   return MK_OK;
 }
 

@@ -781,6 +781,7 @@ struct mk_traversal {
   uint32_t n_small = 0, n_large = 0, small_max = 0;
   int small_grid = 0;
   bool members_prepared = false;
+  PinnedRing staging;  // stream-ordered source uploads
   Timer timer;
 };
 
@@ -964,6 +965,28 @@ mk_status mk_traversal_set_sources(mk_traversal *t, const uint32_t *h_sources, u
   // ordered after every earlier launch of this traversal on any stream
   MK_CUDA(cudaDeviceSynchronize());
   MK_CUDA(cudaMemcpy(t->sources, h_sources, (size_t)n * 4, cudaMemcpyHostToDevice));
+  t->nsources = n;
+  t->h_sources.assign(h_sources, h_sources + n);
+  t->has_static = false;
+  t->members_prepared = false;
+  return MK_OK;
+}
+
+mk_status mk_traversal_set_sources_async(mk_traversal *t, const uint32_t *h_sources, uint32_t n,
+                                         void *stream) {
+  if (!t || !h_sources) return fail(MK_ERR_INVALID, "mk_traversal_set_sources_async: null argument");
+  if (n == 0) return fail(MK_ERR_INVALID, "mk_traversal_set_sources_async: no source");
+  MK_CHECK(check_sources(t->g, h_sources, n, "mk_traversal_set_sources_async"));
+  DeviceGuard dg(t->g->device);
+  if (n > t->src_cap) {  // growing synchronises the device, as cudaFree does
+    MK_CUDA(cudaDeviceSynchronize());
+    uint32_t *p = nullptr;
+    MK_CUDA(cudaMalloc(&p, (size_t)n * 4));
+    cudaFree(t->sources);
+    t->sources = p;
+    t->src_cap = n;
+  }
+  MK_CHECK(t->staging.upload(t->sources, h_sources, (size_t)n * 4, as_stream(stream)));
   t->nsources = n;
   t->h_sources.assign(h_sources, h_sources + n);
   t->has_static = false;
@@ -1162,6 +1185,7 @@ mk_status mk_traversal_decremental_stats(mk_traversal *t, uint64_t *h_invalidate
 mk_status mk_traversal_destroy(mk_traversal *t) {
   if (!t) return MK_OK;
   DeviceGuard dg(t->g->device);
+  t->staging.release();
   cudaFree(t->dist);
   cudaFree(t->stamp);
   cudaFree(t->inval);

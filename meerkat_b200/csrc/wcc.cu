@@ -334,6 +334,7 @@ struct mk_wcc {
   uint64_t large_vt = 0, large_bt = 0;
   int small_grid = 0;
   bool prepared = false;
+  PinnedRing staging;  // stream-ordered range-table uploads
   Timer timer;
 };
 
@@ -422,9 +423,11 @@ mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stre
   return w->timer.stop(ms_out);
 }
 
-mk_status mk_wcc_prepare_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges, uint32_t nranges) {
-  if (!w || (nranges && !h_vertex_ranges))
-    return fail(MK_ERR_INVALID, "mk_wcc_prepare_ranges: null argument");
+// Builds and uploads the range table: blocking (device-wide wait, then a
+// plain copy) when async is false, else stream-ordered on `s` through pinned
+// staging.
+static mk_status wcc_prepare(mk_wcc *w, const uint32_t *h_vertex_ranges, uint32_t nranges,
+                             bool async, cudaStream_t s) {
   mk_graph *g = w->g;
   std::vector<uint32_t> small_ids, large_ids;
   for (uint32_t r = 0; r < nranges; ++r) {
@@ -459,11 +462,17 @@ mk_status mk_wcc_prepare_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges, uint
   vpre[nl] = (uint32_t)vt;
   bpre[nl] = (uint32_t)bt;
   DeviceGuard dg(g->device);
-  // queued work may still read the previous table
-  MK_CUDA(cudaDeviceSynchronize());
   w->prepared = false;
+  if (host.size() > w->ranges.cap) MK_CUDA(cudaDeviceSynchronize());  // growth frees the old table
   MK_CHECK(w->ranges.reserve(host.size(), &g->device_bytes));
-  MK_CUDA(cudaMemcpy(w->ranges.ptr, host.data(), host.size() * 4, cudaMemcpyHostToDevice));
+  if (async) {
+    // ordered after the earlier launches on s, which may still read the old table
+    MK_CHECK(w->staging.upload(w->ranges.ptr, host.data(), host.size() * 4, s));
+  } else {
+    // queued work may still read the previous table
+    MK_CUDA(cudaDeviceSynchronize());
+    MK_CUDA(cudaMemcpy(w->ranges.ptr, host.data(), host.size() * 4, cudaMemcpyHostToDevice));
+  }
   w->n_small = (uint32_t)ns;
   w->n_large = (uint32_t)nl;
   w->small_max = ns ? len(small_ids[0]) : 0;
@@ -480,6 +489,19 @@ mk_status mk_wcc_prepare_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges, uint
   }
   w->prepared = true;
   return MK_OK;
+}
+
+mk_status mk_wcc_prepare_ranges(mk_wcc *w, const uint32_t *h_vertex_ranges, uint32_t nranges) {
+  if (!w || (nranges && !h_vertex_ranges))
+    return fail(MK_ERR_INVALID, "mk_wcc_prepare_ranges: null argument");
+  return wcc_prepare(w, h_vertex_ranges, nranges, false, nullptr);
+}
+
+mk_status mk_wcc_prepare_ranges_async(mk_wcc *w, const uint32_t *h_vertex_ranges,
+                                      uint32_t nranges, void *stream) {
+  if (!w || (nranges && !h_vertex_ranges))
+    return fail(MK_ERR_INVALID, "mk_wcc_prepare_ranges_async: null argument");
+  return wcc_prepare(w, h_vertex_ranges, nranges, true, as_stream(stream));
 }
 
 mk_status mk_wcc_static_prepared(mk_wcc *w, void *stream, float *ms_out) {
@@ -590,6 +612,7 @@ mk_status mk_wcc_destroy(mk_wcc *w) {
   cudaFree(w->parent);
   cudaFree(w->aff_labels);
   cudaFree(w->aff_vertices);
+  w->staging.release();
   w->ranges.release();
   delete w;
   return MK_OK;

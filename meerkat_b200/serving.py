@@ -1,30 +1,39 @@
 """Serving loop: many resident dynamic graphs answering a stream of update
 and query requests, with continuous batching.
 
-All graphs live in one GraphSet (weighted, out-edges), so the requests of
-one scheduling round -- at most one per graph, the head of each graph's
-queue -- are served by coalesced launches:
+All graphs live in one GraphSet (weighted, out-edges).  A graph is a slot: it
+holds at most one request on the GPU at a time, so its requests run in
+arrival order, and a request that arrives while others are on the GPU is
+admitted as soon as its graph's slot and the memory it needs are free.  Each
+scheduling round takes the oldest pending request of every free graph:
 
   deletes of every graph in the round   one delete launch on the union graph
   inserts                               one insert launch
   BFS / SSSP queries                    one multi-source traversal each
                                         (one source per queried graph)
-  WCC queries                           one subset union-find pass
+  WCC queries                           one range union-find pass
 
-PageRank runs on the member's out-edges directly (push form,
-mk_pagerank_range_*).  Triangle counting needs the symmetric graph, so TC
-requests run on per-graph views built on first use from a CSR export of the
-member and kept current by replaying every later update of that graph on
-them.  Views are admitted under a device-memory budget and evicted
-least-recently-used.  These heavy requests run after the coalesced fast
-work of their round, one segment each, so a triangle count does not hold up
-the updates and traversals of other graphs in that round.
+These fast segments are issued on one CUDA stream without waiting for the
+device; a CUDA event after each segment marks its requests complete.
+PageRank (push form on the member's out-edges, mk_pagerank_range_*) and
+triangle counting (straight from the member's out-edges, mk_tc_range_*) are
+heavy: a worker thread runs them one at a time on a second stream, so they
+overlap the fast rounds instead of holding them up.
+
+Admission: an insert of m edges needs at most m new slabs, so it waits
+while the slabs in use (read back after every insert segment), plus the
+inserts still in flight, plus m would pass the slab pool's capacity, and is
+rejected when nothing in flight can change that (deletes never free slabs).
+Triangle counting's scratch grows to the largest member counted; a member
+whose scratch would take the resident set past the memory budget is
+rejected.
 
 Each graph's requests are served in arrival order, so every request sees
 exactly the updates of its graph that arrived before it, whether it shares
 its round with other graphs' requests ("coalesced") or runs alone ("alone":
-one request per round, the plain per-request launch sequence).  The tests
-check that every query answer is the same in both modes.
+one request at a time, synchronously: the plain per-request launch
+sequence).  The tests check that every query answer is the same in both
+modes and equals the oracle's.
 
 No counterpart in the reference, whose drivers run one graph and one
 algorithm per process (src/BFS.cu, src/PageRank.cu, src/TC.cu).
@@ -32,13 +41,15 @@ algorithm per process (src/BFS.cu, src/PageRank.cu, src/TC.cu).
 from __future__ import annotations
 
 import collections
+import queue
+import threading
 import time
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional
+from typing import Dict, List
 
 import numpy as np
 
-from . import BFS, SSSP, TC, WCC, DynamicGraph, GraphSet, PageRankRange, gen_rmat_members
+from . import BFS, SSSP, WCC, GraphSet, PageRankRange, TCRange, gen_rmat_members
 
 INSERT, DELETE, BFS_Q, SSSP_Q, PAGERANK_Q, TC_Q, WCC_Q = range(7)
 KIND_NAMES = ["insert", "delete", "bfs", "sssp", "pagerank", "tc", "wcc"]
@@ -55,8 +66,9 @@ class Request:
     lo: int = 0             # payload slice [lo, hi) of the update pool
     hi: int = 0
     done: float = -1.0      # completion time (seconds after the start)
-    service: float = 0.0    # seconds of the round that served it
+    service: float = 0.0    # seconds from issue to completion
     result: object = None   # query answer when results are recorded
+    status: str = "ok"      # "ok", or why admission refused it
 
 
 @dataclass
@@ -170,151 +182,120 @@ def make_requests(wl: Workload, edges, n: int, rate: float, seed: int, device: i
 
 
 HEAVY_KINDS = (PAGERANK_Q, TC_Q)
+FAST_SEGMENTS = ((INSERT, DELETE), (BFS_Q, WCC_Q), (SSSP_Q,))
 
-
-class _View:
-    """The symmetric copy of one member, for triangle counting (the union
-    graph holds out-edges only)."""
-
-    def __init__(self, gs: GraphSet, g: int, device: int):
-        import torch
-        lo, hi = int(gs.offsets[g]), int(gs.offsets[g + 1])
-        n = hi - lo
-        self.n = n
-        rp, col, _ = gs.graph.export_csr_range_device(lo, hi)
-        rows = torch.repeat_interleave(torch.arange(n, device=col.device, dtype=torch.int32),
-                                       (rp[1:] - rp[:-1]))
-        cols = col - lo
-        e = int(cols.numel())
-        indeg = torch.bincount(cols.long(), minlength=n).to(torch.int32).cpu().numpy().view(np.uint32)
-        outdeg = (rp[1:] - rp[:-1]).to(torch.int32).cpu().numpy().view(np.uint32)
-        self.graph = DynamicGraph(n, degree_hints=indeg + outdeg, device=device,
-                                  pool_slabs=max(4096, (n + e // 10) // 4))
-        self.graph.InsertEdges(torch.cat([rows, cols]), torch.cat([cols, rows]))
-        del rp, col, rows, cols
-        if self.graph.sync() != 0:
-            raise RuntimeError("device error while building a view")
-        self.tc = TC(self.graph, n)
-        # the graph, plus TC's oriented copy of the symmetric edges
-        self.bytes = self.graph.info()["device_bytes"] + 8 * n + 4 * e
-
-    def apply(self, kind: int, u, w_, reverse_found):
-        """Replays one update of the member (local ids) on the view."""
-        import torch
-        if kind == INSERT:
-            self.graph.InsertEdges(torch.cat([u, w_]), torch.cat([w_, u]))
-        else:
-            # the undirected edge goes only when neither direction is left
-            keep = reverse_found == 0
-            uu, ww = u[keep], w_[keep]
-            self.graph.DeleteEdges(torch.cat([uu, ww]), torch.cat([ww, uu]))
-
-    def close(self):
-        self.tc.close()
-        self.graph.close()
+# triangle-count scratch per member (mk_tc_range): CSR export, row ids,
+# reverse flags and the oriented CSR per edge; per-vertex counts and offsets
+TC_BYTES_PER_EDGE = 17
+TC_BYTES_PER_VERTEX = 64
 
 
 class GraphServer:
     """Serves requests on a resident GraphSet within a device-memory budget."""
 
-    def __init__(self, gs: GraphSet, budget_bytes: int, device: int = 0, record: bool = False):
+    def __init__(self, gs: GraphSet, budget_bytes: int, device: int = 0, record: bool = False,
+                 max_update: int = 1_000_000):
+        import torch
         self.gs = gs
         self.G = gs.graph
         self.device = device
+        self.dev = torch.device(f"cuda:{device}")
         self.budget = int(budget_bytes)
         self.record = record
         self.off = gs.offsets.astype(np.int64)
-        first = [int(self.off[0])]
-        self.bfs = BFS(self.G, first)
-        self.sssp = SSSP(self.G, first)
-        self.wcc = WCC(self.G)
+        ng = len(self.off) - 1
         sizes = np.diff(self.off)
+        first = [int(x) for x in self.off[:-1]]
+        ranges = [(int(self.off[g]), int(self.off[g + 1])) for g in range(ng)]
+        self.fast = torch.cuda.Stream(self.dev)
+        self.heavy = torch.cuda.Stream(self.dev)
+        self.bfs = BFS(self.G, first[:1])
+        self.sssp = SSSP(self.G, first[:1])
+        self.wcc = WCC(self.G)
         self.prr = PageRankRange(self.G, int(sizes.max()))
-        self.views: "collections.OrderedDict[int, _View]" = collections.OrderedDict()
-        V = gs.num_vertices
+        self.tcr = TCRange(self.G)
+        # size every per-round table for all members once, so rounds never
+        # grow a device buffer (growth synchronises the device)
+        self.bfs.set_sources(first)
+        self.sssp.set_sources(first)
+        self.wcc.PrepareRanges(ranges)
+        self.G.reserve_batch(ng * int(max_update))
         info = self.G.info()
+        V = gs.num_vertices
         # graph + two traversals (dist, stamp, bitmap, two frontiers, list) + WCC
         # + range PageRank (two FP64 vectors and an FP32 copy of the largest member)
         trav = 8 * V + 4 * V + V // 8 + 2 * 8 * (info["num_buckets"] + 64) + 4 * V
         self.resident = info["device_bytes"] + 2 * trav + 4 * V + V // 4 + 20 * int(sizes.max())
         if self.resident > self.budget:
             raise MemoryError(f"resident set {self.resident} B exceeds the budget {self.budget} B")
-        self.view_builds = 0
-        self.view_evictions = 0
+        self.tc_bytes = 0  # triangle-count scratch held so far
+        self.pool_cap = int(info["pool_capacity"])
+        self.slabs_used = int(info["slabs_used"])
+        self.h_used = torch.zeros(1, dtype=torch.int32).pin_memory()
+        self.h_tc = torch.zeros(1, dtype=torch.int64).pin_memory()
+        # size the heavy requests' scratch on the member with the most edges
+        # (a later growth would synchronise the device mid-run)
+        edges = [int(self.G.count_edges(lo, hi)) for lo, hi in ranges]
+        big = int(np.argmax(edges))
+        warm = Request(rid=-1, graph=big, kind=TC_Q, arrival=0.0)
+        self.run_heavy(warm, self.heavy)
+        if warm.status != "ok":
+            raise MemoryError("triangle-count scratch of the largest member exceeds the budget")
+        self.prr.Run(*ranges[big], 0.85, 1e-6, 200, stream=self.heavy, timed=False)
+        torch.cuda.synchronize(self.dev)
 
-    def reset_views(self) -> None:
-        """Drops every cached view (a run that must start cold)."""
-        for v in self.views.values():
-            v.close()
-        self.views.clear()
+    def close(self):
+        for o in (self.bfs, self.sssp, self.wcc, self.prr, self.tcr):
+            o.close()
 
-    def view_bytes(self) -> int:
-        return sum(v.bytes for v in self.views.values())
+    # ---- admission ----
+    def _tc_need(self, g: int, stream) -> int:
+        # (the edge count uses the graph's own accumulator: heavy requests
+        # alone call it, one at a time)
+        n = int(self.off[g + 1] - self.off[g])
+        e = int(self.G.count_edges(int(self.off[g]), int(self.off[g + 1]), stream=stream))
+        return TC_BYTES_PER_EDGE * e + TC_BYTES_PER_VERTEX * n
 
-    def _view(self, g: int) -> _View:
-        v = self.views.get(g)
-        if v is not None:
-            self.views.move_to_end(g)
-            return v
-        lo, hi = int(self.off[g]), int(self.off[g + 1])
-        n, e = hi - lo, int(self.G.count_edges(lo, hi))
-        est = 128 * (n + 2 * e // 15) + 8 * n + 4 * e
-        while self.views and self.resident + self.view_bytes() + est > self.budget:
-            _, old = self.views.popitem(last=False)
-            old.close()
-            self.view_evictions += 1
-        if self.resident + est > self.budget:
-            raise MemoryError(f"graph {g}: its symmetric view does not fit the budget")
-        v = _View(self.gs, g, self.device)
-        self.views[g] = v
-        self.view_builds += 1
-        # the estimate was short: evict older views until the real size fits
-        while len(self.views) > 1 and self.resident + self.view_bytes() > self.budget:
-            _, old = self.views.popitem(last=False)
-            old.close()
-            self.view_evictions += 1
-        return v
+    def _admit(self, r: Request, insert_inflight: int):
+        """'go', 'wait' or 'reject' for the head request r (triangle counts
+        are admitted against the budget by run_heavy)."""
+        if r.kind == INSERT:
+            m = r.hi - r.lo
+            if self.slabs_used + insert_inflight + m + 1024 <= self.pool_cap:
+                return "go"
+            return "wait" if insert_inflight else "reject"
+        return "go"
 
-    # ---- a coalesced round of fast requests: at most one per graph ----
-    def serve_fast(self, reqs: List[Request], wl: Workload) -> None:
+    # ---- the work of one fast segment (same-kind requests of distinct graphs) ----
+    def issue_fast(self, reqs: List[Request], wl: Workload, stream) -> None:
         import torch
-        assert len({r.graph for r in reqs}) == len(reqs), "one request per graph per round"
-        assert all(r.kind not in HEAVY_KINDS for r in reqs)
+        P_s, P_d, P_w = wl.pool_src, wl.pool_dst, wl.pool_w
         dels = [r for r in reqs if r.kind == DELETE]
         inss = [r for r in reqs if r.kind == INSERT]
-        P_s, P_d, P_w = wl.pool_src, wl.pool_dst, wl.pool_w
-        if dels:
-            ds = torch.cat([P_s[r.lo:r.hi] for r in dels])
-            dd = torch.cat([P_d[r.lo:r.hi] for r in dels])
-            self.G.DeleteEdges(ds, dd)
-        if inss:
-            is_ = torch.cat([P_s[r.lo:r.hi] for r in inss])
-            id_ = torch.cat([P_d[r.lo:r.hi] for r in inss])
-            iw = torch.cat([P_w[r.lo:r.hi] for r in inss])
-            self.G.InsertEdges(is_, id_, vals=iw)
-        # keep cached views current (per graph: the same batch, local ids)
-        for r in dels + inss:
-            v = self.views.get(r.graph)
-            if v is None:
-                continue
-            base = int(self.off[r.graph])
-            u, w_ = P_s[r.lo:r.hi] - base, P_d[r.lo:r.hi] - base
-            found = None
-            if r.kind == DELETE:
-                found = torch.zeros(u.numel(), dtype=torch.uint8, device=u.device)
-                self.G.SearchEdges(P_d[r.lo:r.hi], P_s[r.lo:r.hi], found)
-            v.apply(r.kind, u, w_, found)
+        with torch.cuda.stream(stream):
+            if dels:
+                ds = torch.cat([P_s[r.lo:r.hi] for r in dels])
+                dd = torch.cat([P_d[r.lo:r.hi] for r in dels])
+                self.G.DeleteEdges(ds, dd, stream=stream)
+            if inss:
+                is_ = torch.cat([P_s[r.lo:r.hi] for r in inss])
+                id_ = torch.cat([P_d[r.lo:r.hi] for r in inss])
+                iw = torch.cat([P_w[r.lo:r.hi] for r in inss])
+                self.G.InsertEdges(is_, id_, vals=iw, stream=stream)
+                self.G.slabs_used_async(self.h_used.data_ptr(), stream=stream)
         bfs = [r for r in reqs if r.kind == BFS_Q]
         sssp = [r for r in reqs if r.kind == SSSP_Q]
         wccs = [r for r in reqs if r.kind == WCC_Q]
         for trav, rs in ((self.bfs, bfs), (self.sssp, sssp)):
             if rs:
-                trav.set_sources([int(self.off[r.graph]) + r.source for r in rs])
-                trav.Static(timed=False)
+                trav.set_sources([int(self.off[r.graph]) + r.source for r in rs], stream=stream)
+                trav.Static(stream=stream, timed=False)
         if wccs:
-            self.wcc.StaticRanges([(int(self.off[r.graph]), int(self.off[r.graph + 1]))
-                                   for r in wccs], timed=False)
+            self.wcc.PrepareRanges([(int(self.off[r.graph]), int(self.off[r.graph + 1]))
+                                    for r in wccs], stream=stream)
+            self.wcc.StaticPrepared(stream=stream, timed=False)
         if self.record:
+            stream.synchronize()
             self._record(bfs, self.bfs)
             self._record(sssp, self.sssp)
             if wccs:
@@ -323,27 +304,23 @@ class GraphServer:
                     lo, hi = int(self.off[r.graph]), int(self.off[r.graph + 1])
                     r.result = (lab[lo:hi] - lo).astype(np.uint32)
 
-    # ---- one PageRank (on the member itself) or triangle-count (on its view) request ----
-    def serve_heavy(self, r: Request) -> None:
+    # ---- one PageRank or triangle-count request (blocking on `stream`) ----
+    def run_heavy(self, r: Request, stream) -> None:
+        lo, hi = int(self.off[r.graph]), int(self.off[r.graph + 1])
         if r.kind == PAGERANK_Q:
-            # PageRank on the member's out-edges: no view to build
-            self.prr.Run(int(self.off[r.graph]), int(self.off[r.graph + 1]), 0.85, 1e-6, 200,
-                         timed=False)
+            self.prr.Run(lo, hi, 0.85, 1e-6, 200, stream=stream, timed=False)
             if self.record:
                 r.result = self.prr.Values()
         else:
-            v = self._view(r.graph)
-            v.tc.Static(timed=False)
-            r.result = v.tc.GetCount()
-
-    def serve_round(self, reqs: List[Request], wl: Workload) -> None:
-        """Fast requests as one coalesced round, then the heavy ones in order."""
-        fast = [r for r in reqs if r.kind not in HEAVY_KINDS]
-        if fast:
-            self.serve_fast(fast, wl)
-        for r in reqs:
-            if r.kind in HEAVY_KINDS:
-                self.serve_heavy(r)
+            need = self._tc_need(r.graph, stream)
+            if need > self.tc_bytes and self.resident + need > self.budget:
+                r.status = "rejected"
+                return
+            self.tcr.Run(lo, hi, stream=stream, timed=False)
+            self.tc_bytes = max(self.tc_bytes, need)
+            self.tcr.count_async(self.h_tc.data_ptr(), stream=stream)
+            stream.synchronize()
+            r.result = int(self.h_tc[0])
 
     def _record(self, rs, trav):
         if not rs:
@@ -361,90 +338,176 @@ class GraphServer:
     def run(self, reqs: List[Request], wl: Workload, mode: str = "coalesced",
             max_round: int = 0) -> dict:
         """Serves `reqs` (sorted by arrival) against the wall clock: a request
-        is admitted once its arrival time has passed.  "coalesced": each round
-        takes the head request of every graph with a pending one, runs the fast
-        heads (at most max_round if > 0) as coalesced segments by kind (updates,
-        then BFS and WCC, then SSSP) and then the
-        heavy heads (PageRank / TC) one segment each.  "alone": each
-        round runs the single oldest request.  A request completes when the
-        GPU has finished its segment.  Returns latency and throughput."""
-        import torch
+        is admitted once its arrival time has passed.  "coalesced": continuous
+        batching as described in the module docstring (at most max_round fast
+        requests per round if > 0).  "alone": one request at a time, issued
+        and waited for (the plain per-request sequence).  A request completes
+        when the device has finished its work (CUDA event time).  Returns
+        latency and throughput."""
         assert mode in ("coalesced", "alone")
-        queues: Dict[int, collections.deque] = collections.defaultdict(collections.deque)
-        fifo = collections.deque()
-        i, served, rounds, n = 0, 0, 0, len(reqs)
-        builds0, evictions0 = self.view_builds, self.view_evictions
-        t0 = time.perf_counter() - (reqs[0].arrival if reqs else 0.0)
-        while served < n:
-            now = time.perf_counter() - t0
-            while i < n and reqs[i].arrival <= now:
-                queues[reqs[i].graph].append(reqs[i])
-                if mode == "alone":
-                    fifo.append(reqs[i])
-                i += 1
-            if served == i:  # idle until the next arrival
-                wait = reqs[i].arrival - now
-                if wait > 0.0005:
-                    time.sleep(wait - 0.0003)
-                continue
-            segments = []  # (kind of segment, requests)
-            if mode == "alone":
-                r = fifo.popleft()
-                queues[r.graph].popleft()
-                segments.append(("heavy" if r.kind in HEAVY_KINDS else "fast", [r]))
-            else:
-                heads = sorted((q[0] for q in queues.values() if q), key=lambda r: r.arrival)
-                fast = [r for r in heads if r.kind not in HEAVY_KINDS]
-                heavy = [r for r in heads if r.kind in HEAVY_KINDS]
-                if max_round > 0:
-                    fast = fast[:max_round]
-                # cheap kinds first, each kind group its own segment, so an
-                # update does not wait for the round's traversals
-                for kinds in ((INSERT, DELETE), (BFS_Q, WCC_Q), (SSSP_Q,)):
-                    seg = [r for r in fast if r.kind in kinds]
-                    if seg:
-                        segments.append(("fast", seg))
-                for r in heavy:  # each heavy request its own segment, oldest first
-                    segments.append(("heavy", [r]))
-                for _, rs in segments:
-                    for r in rs:
-                        queues[r.graph].popleft()
-            for kind, rs in segments:
-                start = time.perf_counter() - t0
-                if kind == "fast":
-                    self.serve_fast(rs, wl)
-                else:
-                    self.serve_heavy(rs[0])
-                torch.cuda.synchronize(self.device)
-                done = time.perf_counter() - t0
-                for r in rs:
-                    r.done = done
-                    r.service = done - start
-                served += len(rs)
-                rounds += 1
+        if mode == "alone":
+            return self._run_alone(reqs, wl)
+        return self._run_coalesced(reqs, wl, max_round)
+
+    def _summary(self, reqs, mode, rounds, rejected) -> dict:
         self.check()
-        lat = np.array([r.done - r.arrival for r in reqs]) * 1000.0
-        span = max(r.done for r in reqs) - min(r.arrival for r in reqs) if reqs else 0.0
+        done = [r for r in reqs if r.status == "ok"]
+        lat = np.array([r.done - r.arrival for r in done]) * 1000.0
+        span = (max(r.done for r in reqs) - min(r.arrival for r in reqs)) if reqs else 0.0
         by_kind = {}
         for k in range(len(KIND_NAMES)):
-            sel = [r.done - r.arrival for r in reqs if r.kind == k]
-            svc = [r.service for r in reqs if r.kind == k]
+            sel = [r.done - r.arrival for r in done if r.kind == k]
+            svc = [r.service for r in done if r.kind == k]
             if sel:
                 by_kind[KIND_NAMES[k]] = {"n": len(sel),
                                           "p50_ms": float(np.percentile(sel, 50) * 1000.0),
                                           "p99_ms": float(np.percentile(sel, 99) * 1000.0),
                                           "service_p50_ms": float(np.percentile(svc, 50) * 1000.0)}
-        return {"mode": mode, "requests": n, "rounds": rounds,
+        n = len(done)
+        return {"mode": mode, "requests": len(reqs), "rounds": rounds, "rejected": rejected,
                 "p50_ms": float(np.percentile(lat, 50)) if n else 0.0,
                 "p99_ms": float(np.percentile(lat, 99)) if n else 0.0,
                 "mean_ms": float(lat.mean()) if n else 0.0,
                 "throughput_rps": n / span if span > 0 else 0.0,
-                "by_kind": by_kind, "view_builds": self.view_builds - builds0,
-                "view_evictions": self.view_evictions - evictions0}
+                "by_kind": by_kind}
 
-    def close(self):
-        for v in self.views.values():
-            v.close()
-        self.views.clear()
-        for o in (self.bfs, self.sssp, self.wcc, self.prr):
-            o.close()
+    def _run_alone(self, reqs, wl) -> dict:
+        s = self.fast
+        t0 = time.perf_counter() - (reqs[0].arrival if reqs else 0.0)
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if r.arrival > now:
+                time.sleep(r.arrival - now)
+            start = time.perf_counter() - t0
+            if r.kind in HEAVY_KINDS:
+                self.run_heavy(r, s)
+            else:
+                self.issue_fast([r], wl, s)
+            s.synchronize()
+            r.done = time.perf_counter() - t0
+            r.service = r.done - start
+        return self._summary(reqs, "alone", len(reqs), sum(r.status != "ok" for r in reqs))
+
+    def _run_coalesced(self, reqs, wl, max_round) -> dict:
+        import torch
+        n = len(reqs)
+        queues: Dict[int, collections.deque] = collections.defaultdict(collections.deque)
+        # a graph's fast requests may queue up behind each other on the fast
+        # stream (stream order keeps them in arrival order); a heavy request
+        # waits until its graph has nothing in flight, and nothing of its
+        # graph is issued while it runs
+        fast_pending: Dict[int, int] = collections.defaultdict(int)
+        heavy_busy = set()
+        inflight = []             # (event, requests, issue time, inserted edges)
+        insert_inflight = 0
+        heavy_running = 0
+        heavy_q: "queue.Queue" = queue.Queue()
+        heavy_done: "queue.Queue" = queue.Queue()
+        base = torch.cuda.Event(enable_timing=True)
+        rounds = rejected = 0
+        t0 = time.perf_counter() - (reqs[0].arrival if reqs else 0.0)
+        base.record(self.fast)
+        base.synchronize()
+        t_base = time.perf_counter() - t0
+
+        def worker():
+            torch.cuda.set_device(self.dev)
+            while True:
+                r = heavy_q.get()
+                if r is None:
+                    return
+                start = time.perf_counter() - t0
+                self.run_heavy(r, self.heavy)
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(self.heavy)
+                ev.synchronize()
+                heavy_done.put((r, start, t_base + base.elapsed_time(ev) / 1000.0))
+
+        th = threading.Thread(target=worker, daemon=True)
+        th.start()
+        i = finished = 0
+        try:
+            while finished < n:
+                progressed = False
+                # completions
+                still = []
+                for ev, rs, start, ins in inflight:
+                    if ev.query():
+                        done = t_base + base.elapsed_time(ev) / 1000.0
+                        for r in rs:
+                            r.done, r.service = done, done - start
+                            fast_pending[r.graph] -= 1
+                        finished += len(rs)
+                        if ins:
+                            insert_inflight -= ins
+                            self.slabs_used = max(self.slabs_used, int(self.h_used[0]) & 0xFFFFFFFF)
+                        progressed = True
+                    else:
+                        still.append((ev, rs, start, ins))
+                inflight = still
+                while not heavy_done.empty():
+                    r, start, done = heavy_done.get()
+                    r.done, r.service = done, done - start
+                    heavy_busy.discard(r.graph)
+                    heavy_running -= 1
+                    finished += 1
+                    rejected += r.status != "ok"
+                    progressed = True
+                # arrivals
+                now = time.perf_counter() - t0
+                while i < n and reqs[i].arrival <= now:
+                    queues[reqs[i].graph].append(reqs[i])
+                    i += 1
+                # one round: the oldest pending request of every free graph
+                heads = sorted((q[0] for g, q in queues.items() if q and g not in heavy_busy),
+                               key=lambda r: r.arrival)
+                fast = []
+                for r in heads:
+                    heavy = r.kind in HEAVY_KINDS
+                    if heavy and fast_pending[r.graph]:
+                        continue  # its graph's fast work must finish first
+                    if not heavy and max_round > 0 and len(fast) >= max_round:
+                        continue
+                    verdict = self._admit(r, insert_inflight)
+                    if verdict == "wait":
+                        continue
+                    queues[r.graph].popleft()
+                    if verdict == "reject":
+                        r.status = "rejected"
+                        r.done = r.service = time.perf_counter() - t0
+                        finished += 1
+                        rejected += 1
+                        progressed = True
+                        continue
+                    if heavy:
+                        heavy_busy.add(r.graph)
+                        heavy_running += 1
+                        heavy_q.put(r)
+                    else:
+                        fast_pending[r.graph] += 1
+                        if r.kind == INSERT:
+                            insert_inflight += r.hi - r.lo
+                        fast.append(r)
+                for kinds in FAST_SEGMENTS:
+                    seg = [r for r in fast if r.kind in kinds]
+                    if not seg:
+                        continue
+                    start = time.perf_counter() - t0
+                    self.issue_fast(seg, wl, self.fast)
+                    ev = torch.cuda.Event(enable_timing=True)
+                    ev.record(self.fast)
+                    ins = sum(r.hi - r.lo for r in seg if r.kind == INSERT)
+                    inflight.append((ev, seg, start, ins))
+                    rounds += 1
+                    progressed = True
+                if not progressed:
+                    # nothing to do until an arrival or a completion
+                    wait = (reqs[i].arrival - (time.perf_counter() - t0)) if i < n else 1.0
+                    if inflight or heavy_running:
+                        wait = min(wait, 0.0001)
+                    time.sleep(min(max(wait, 0.00002), 0.002))
+        finally:
+            heavy_q.put(None)
+            th.join()
+        torch.cuda.synchronize(self.dev)
+        return self._summary(reqs, "coalesced", rounds, rejected)

@@ -99,16 +99,57 @@ def test_alone_and_coalesced_answers_match_each_other_and_the_oracle():
 
 
 @pytest.mark.gpu
-def test_views_are_evicted_under_a_small_budget():
+def test_inserts_beyond_the_slab_pool_are_refused_not_failed():
+    """Admission by slab-pool headroom: with the pool's capacity lowered on
+    the host, large inserts are refused at admission (status "rejected")
+    instead of running out of slabs on the device; everything else is
+    served and the graph stays consistent."""
     seed = 5
     gs, edges, wl = make_server(seed)
     reqs = S.make_requests(wl, edges, 40, rate=1e7, seed=7,
-                           mix=(0.1, 0.1, 0, 0, 0.4, 0.4, 0), upd_lo=10, upd_hi=500)
-    srv = S.GraphServer(gs, budget_bytes=1 << 40, record=True)
-    srv.budget = srv.resident + (1 << 20)  # room for about one view
-    r = srv.run(reqs, wl, mode="coalesced")
-    assert r["view_builds"] >= 2 and r["view_evictions"] >= 1
-    assert srv.resident + srv.view_bytes() <= srv.budget
+                           mix=(0.5, 0.1, 0.2, 0, 0, 0.2, 0), upd_lo=100, upd_hi=3000)
+    srv = S.GraphServer(gs, budget_bytes=1 << 40)
+    srv.pool_cap = srv.slabs_used + 1024 + 500  # room for one small insert at most
+    out = srv.run(reqs, wl, mode="coalesced")
+    rej = [r for r in reqs if r.status != "ok"]
+    assert rej and all(r.kind == S.INSERT and r.hi - r.lo > 500 for r in rej)
+    assert out["rejected"] == len(rej)
+    assert all(r.done >= 0 for r in reqs)
+    assert gs.graph.sync() == 0
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_triangle_counts_beyond_the_budget_are_refused():
+    seed = 6
+    gs, edges, wl = make_server(seed)
+    reqs = S.make_requests(wl, edges, 20, rate=1e7, seed=9, mix=(0, 0, 0, 0, 0, 1, 0))
+    srv = S.GraphServer(gs, budget_bytes=1 << 40)
+    srv.budget = srv.resident  # no room for any scratch beyond what is held
+    srv.tc_bytes = 0
+    out = srv.run(reqs, wl, mode="coalesced")
+    assert out["rejected"] == len(reqs)
+    assert all(r.status == "rejected" for r in reqs)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_saturated_coalesced_run_overlaps_heavy_and_fast_work():
+    """All requests at once: the coalesced server answers every request and
+    finishes no later than the one-at-a-time sequence of the same log."""
+    seed = 8
+    gsA, edgesA, wlA = make_server(seed)
+    reqs = S.make_requests(wlA, edgesA, 80, rate=1e9, seed=seed + 1, upd_lo=10, upd_hi=3000)
+    srv = S.GraphServer(gsA, budget_bytes=1 << 40)
+    srv.run([S.Request(r.rid, r.graph, r.kind, r.arrival, r.source, r.lo, r.hi) for r in reqs[:8]],
+            wlA, mode="coalesced")  # warm-up
+    a = srv.run([S.Request(r.rid, r.graph, r.kind, r.arrival, r.source, r.lo, r.hi) for r in reqs],
+                wlA, mode="coalesced")
+    b = srv.run([S.Request(r.rid, r.graph, r.kind, r.arrival, r.source, r.lo, r.hi) for r in reqs],
+                wlA, mode="alone")
+    assert a["rejected"] == b["rejected"] == 0
+    assert a["rounds"] < b["rounds"] == len(reqs)
+    assert a["throughput_rps"] > 0.9 * b["throughput_rps"]
     srv.close()
 
 
