@@ -483,6 +483,10 @@ def line_summary(line):
             ("sssp_dec", "sssp_dec_ms_p50", "sssp_dec_ms_p50")]
     gpu_ms = {k: r3(q.get(a)) for k, a, _ in keys}
     cpu_ms = {k: r3(cq.get(b)) for k, _, b in keys}
+    # decremental calls with the reverse graph attached (BFS: level-ordered
+    # repair; SSSP: re-seed from in-edges)
+    gpu_ms["bfs_dec_rev"] = r3(q.get("bfs_dec_rev_ms_p50"))
+    gpu_ms["sssp_dec_rev"] = r3(q.get("sssp_dec_rev_ms_p50"))
     for k in ("wcc", "pagerank", "tc"):
         gpu_ms[k + "_static"] = r3(q.get(k, {}).get("static_ms"))
         cpu_ms[k + "_static"] = r3(cq.get(k + "_static_ms"))

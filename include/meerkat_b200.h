@@ -471,6 +471,8 @@ mk_status mk_graphset_destroy(mk_graphset *s);
 /* The union graph, owned by the set: use it with every mk_graph_*, BFS,
  * SSSP, PageRank, TC and WCC entry point; never destroy it directly. */
 mk_status mk_graphset_union(mk_graphset *s, mk_graph **g);
+/* Number of member graphs. */
+mk_status mk_graphset_num_graphs(mk_graphset *s, uint32_t *h_num_graphs);
 /* Copies the num_graphs + 1 vertex offsets to host memory. */
 mk_status mk_graphset_offsets(mk_graphset *s, uint32_t *h_offsets);
 /* Device copy of the same offsets, owned by the set. */
@@ -506,6 +508,39 @@ mk_status mk_gen_set_batches(const uint32_t *d_vertex_offsets, uint32_t num_grap
                              uint32_t w_lo, uint32_t w_hi, uint32_t *d_del_src,
                              uint32_t *d_del_dst, uint32_t *d_ins_src,
                              uint32_t *d_ins_dst, uint32_t *d_ins_w, void *stream);
+
+/* ------------------------------------------------------------------------
+ * The batched many-graph step (no counterpart in the reference, whose
+ * drivers hold one graph and one algorithm object per process,
+ * src/BFS.cu:11-131).  A runner holds one query per member of a graph set:
+ * MK_QUERY_BFS (levels from the member's source; h_bfs_source_local[m] is a
+ * local vertex id, read only for BFS members), MK_QUERY_WCC (the member's
+ * components) or MK_QUERY_NONE.  create uploads the query tables (blocking).
+ * step applies one update batch covering any members (deletes, then inserts;
+ * global vertex ids, device arrays; d_ins_w may be NULL) and then answers
+ * every member's query: four launches, all asynchronous on `stream` and
+ * allocation-free once mk_graph_reserve_batch has sized the batch scratch,
+ * so a step can be captured into a CUDA graph.  A member's answers equal
+ * those of a DynamicGraph holding the member alone (an edge leaving its
+ * member sets MK_DEVERR_INVALID_ID on the union graph).
+ * ---------------------------------------------------------------------- */
+#define MK_QUERY_BFS 0u
+#define MK_QUERY_WCC 1u
+#define MK_QUERY_NONE 2u
+typedef struct mk_set_runner mk_set_runner;
+mk_status mk_set_runner_create(mk_graphset *s, const uint8_t *h_query,
+                               const uint32_t *h_bfs_source_local, mk_set_runner **out);
+mk_status mk_set_runner_step(mk_set_runner *r, const uint32_t *d_del_src,
+                             const uint32_t *d_del_dst, uint32_t n_del,
+                             const uint32_t *d_ins_src, const uint32_t *d_ins_dst,
+                             const uint32_t *d_ins_w, uint32_t n_ins, void *stream);
+/* Device pointers to the answers of the last step (either may be NULL): the
+ * packed dist << 32 | parent words of the BFS members' vertices (union ids;
+ * NULL when no member asks BFS) and the WCC labels (union ids, the minimum
+ * id of each component; NULL when no member asks WCC). */
+mk_status mk_set_runner_results(mk_set_runner *r, const uint64_t **d_bfs_packed,
+                                const uint32_t **d_wcc_labels);
+mk_status mk_set_runner_destroy(mk_set_runner *r);
 
 /* ------------------------------------------------------------------------
  * The reference drivers' text formats (host only; no GPU needed):

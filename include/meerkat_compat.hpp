@@ -301,6 +301,80 @@ class WCC {
   mk_wcc *w_ = nullptr;
 };
 
+// Many small dynamic graphs stored and updated as one (mk_graphset_*), and
+// the batched step over them (mk_set_runner_*): no counterpart in the
+// reference, whose drivers hold one graph per process.  Member m owns the
+// union vertex ids [Offsets()[m], Offsets()[m + 1]).
+class GraphSet {
+ public:
+  GraphSet(const std::vector<uint32_t> &num_vertices, bool weighted, int device = 0,
+           double load_factor = 0.7, const std::vector<const uint32_t *> *hints = nullptr,
+           uint64_t pool_slabs = 0) {
+    check(mk_graphset_create((uint32_t)num_vertices.size(), num_vertices.data(),
+                             hints ? hints->data() : nullptr, load_factor, weighted ? 1u : 0u,
+                             device, pool_slabs, &s_),
+          "GraphSet");
+  }
+  GraphSet(const GraphSet &) = delete;
+  ~GraphSet() { mk_graphset_destroy(s_); }
+  mk_graphset *handle() const { return s_; }
+  mk_graph *Union() const {
+    mk_graph *g = nullptr;
+    check(mk_graphset_union(s_, &g), "Union");
+    return g;
+  }
+  std::vector<uint32_t> Offsets() const {
+    uint32_t n = 0;
+    check(mk_graphset_num_graphs(s_, &n), "Offsets");
+    std::vector<uint32_t> off(n + 1);
+    check(mk_graphset_offsets(s_, off.data()), "Offsets");
+    return off;
+  }
+  // Device batches with union vertex ids, stream-ordered.
+  void InsertEdges(const uint32_t *S, const uint32_t *D, uint32_t n, const uint32_t *W = nullptr,
+                   void *stream = nullptr) {
+    check(mk_graph_insert_edges(Union(), S, D, W, n, stream), "InsertEdges");
+  }
+  void DeleteEdges(const uint32_t *S, const uint32_t *D, uint32_t n, void *stream = nullptr) {
+    check(mk_graph_delete_edges(Union(), S, D, n, stream), "DeleteEdges");
+  }
+
+ private:
+  mk_graphset *s_ = nullptr;
+};
+
+class GraphSetRunner {
+ public:
+  // query[m]: MK_QUERY_BFS / MK_QUERY_WCC / MK_QUERY_NONE; bfs_source[m]:
+  // local source of a BFS member.
+  GraphSetRunner(GraphSet &set, const std::vector<uint8_t> &query,
+                 const std::vector<uint32_t> &bfs_source) {
+    check(mk_set_runner_create(set.handle(), query.data(),
+                               bfs_source.empty() ? nullptr : bfs_source.data(), &r_),
+          "GraphSetRunner");
+  }
+  GraphSetRunner(const GraphSetRunner &) = delete;
+  ~GraphSetRunner() { mk_set_runner_destroy(r_); }
+  // One step: the deletes, the inserts, every member's query (asynchronous).
+  void Step(const uint32_t *dS, const uint32_t *dD, uint32_t nDel, const uint32_t *iS,
+            const uint32_t *iD, const uint32_t *iW, uint32_t nIns, void *stream = nullptr) {
+    check(mk_set_runner_step(r_, dS, dD, nDel, iS, iD, iW, nIns, stream), "Step");
+  }
+  const uint64_t *BfsPacked() const {
+    const uint64_t *p = nullptr;
+    check(mk_set_runner_results(r_, &p, nullptr), "BfsPacked");
+    return p;
+  }
+  const uint32_t *WccLabels() const {
+    const uint32_t *p = nullptr;
+    check(mk_set_runner_results(r_, nullptr, &p), "WccLabels");
+    return p;
+  }
+
+ private:
+  mk_set_runner *r_ = nullptr;
+};
+
 // The reference drivers' input files (src/BFS.cu:27-36, :76-91): a graph
 // file "V E" + E pairs, and update batches "<prefix>.batch.<i>".
 struct EdgeList {

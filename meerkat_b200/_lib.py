@@ -127,6 +127,7 @@ SIGNATURES = [
                                 C.c_int32, C.c_uint64, C.POINTER(vp)]),
     ("mk_graphset_destroy", _S, [vp]),
     ("mk_graphset_union", _S, [vp, C.POINTER(vp)]),
+    ("mk_graphset_num_graphs", _S, [vp, u32p]),
     ("mk_graphset_offsets", _S, [vp, u32p]),
     ("mk_graphset_select_bits", _S, [vp, vp, vp, vp]),
     ("mk_graphset_offsets_device", _S, [vp, C.POINTER(vp)]),
@@ -134,6 +135,10 @@ SIGNATURES = [
                              C.c_uint32, C.c_uint32, vp, vp, vp, vp]),
     ("mk_gen_set_batches", _S, [vp, C.c_uint32, vp, vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32,
                                 vp, vp, vp, vp, vp, vp]),
+    ("mk_set_runner_create", _S, [vp, vp, vp, C.POINTER(vp)]),
+    ("mk_set_runner_step", _S, [vp, vp, vp, C.c_uint32, vp, vp, vp, C.c_uint32, vp]),
+    ("mk_set_runner_results", _S, [vp, C.POINTER(vp), C.POINTER(vp)]),
+    ("mk_set_runner_destroy", _S, [vp]),
     ("mk_read_edge_list", _S, [C.c_char_p, u32p, u64p, vp, vp]),
     ("mk_read_batch_file", _S, [C.c_char_p, u64p, vp, vp]),
     ("mk_write_edge_list", _S, [C.c_char_p, C.c_uint32, C.c_uint64, vp, vp]),

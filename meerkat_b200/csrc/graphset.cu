@@ -252,6 +252,12 @@ mk_status mk_graphset_union(mk_graphset *s, mk_graph **g) {
   return MK_OK;
 }
 
+mk_status mk_graphset_num_graphs(mk_graphset *s, uint32_t *h_num_graphs) {
+  if (!s || !h_num_graphs) return fail(MK_ERR_INVALID, "mk_graphset_num_graphs: null argument");
+  *h_num_graphs = s->ngraphs;
+  return MK_OK;
+}
+
 mk_status mk_graphset_offsets(mk_graphset *s, uint32_t *h_offsets) {
   if (!s || !h_offsets) return fail(MK_ERR_INVALID, "mk_graphset_offsets: null argument");
   std::copy(s->h_off.begin(), s->h_off.end(), h_offsets);

@@ -1,0 +1,118 @@
+// The batched many-graph step behind the C ABI: a graph set, one query kind
+// per member (BFS from a source, or components), and a step that applies
+// every member's update batch and answers every member's query with four
+// stream-ordered launches.
+//
+// No counterpart in the reference, whose drivers hold one graph and one
+// algorithm object per process (src/BFS.cu:11-131); this is the path a C++
+// caller of the drop-in uses for thousands of small graphs.  The launches
+// are those of the Python batched runner: one delete and one insert kernel
+// over all members' batches, one shared-memory member BFS over the BFS
+// members, one member WCC over the WCC members.  Everything the step issues
+// is asynchronous and allocation-free once the batch scratch is reserved,
+// so a step can be captured into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "mk_internal.h"
+
+using namespace mk;
+
+struct mk_set_runner {
+  mk_graphset *set = nullptr;
+  mk_graph *g = nullptr;
+  mk_traversal *bfs = nullptr;
+  mk_wcc *wcc = nullptr;
+  uint32_t num_graphs = 0, n_bfs = 0, n_wcc = 0;
+};
+
+extern "C" {
+
+mk_status mk_set_runner_create(mk_graphset *s, const uint8_t *h_query,
+                               const uint32_t *h_bfs_source_local, mk_set_runner **out) {
+  if (!s || !h_query || !out) return fail(MK_ERR_INVALID, "mk_set_runner_create: null argument");
+  *out = nullptr;
+  mk_graph *g = nullptr;
+  MK_CHECK(mk_graphset_union(s, &g));
+  uint32_t ng = 0;
+  MK_CHECK(mk_graphset_num_graphs(s, &ng));
+  std::vector<uint32_t> off((size_t)ng + 1);
+  MK_CHECK(mk_graphset_offsets(s, off.data()));
+  const uint32_t G = (uint32_t)off.size() - 1;
+  std::vector<uint32_t> sources, bfs_ranges, wcc_ranges;
+  for (uint32_t m = 0; m < G; ++m) {
+    if (h_query[m] == MK_QUERY_BFS) {
+      if (!h_bfs_source_local) return fail(MK_ERR_INVALID, "mk_set_runner_create: BFS members need sources");
+      const uint64_t src = (uint64_t)off[m] + h_bfs_source_local[m];
+      if (src >= off[m + 1]) return fail(MK_ERR_INVALID, "mk_set_runner_create: source outside its member");
+      sources.push_back((uint32_t)src);
+      bfs_ranges.push_back(off[m]);
+      bfs_ranges.push_back(off[m + 1]);
+    } else if (h_query[m] == MK_QUERY_WCC) {
+      wcc_ranges.push_back(off[m]);
+      wcc_ranges.push_back(off[m + 1]);
+    } else if (h_query[m] != MK_QUERY_NONE) {
+      return fail(MK_ERR_INVALID, "mk_set_runner_create: unknown query kind");
+    }
+  }
+  mk_set_runner *r = new mk_set_runner();
+  r->set = s;
+  r->g = g;
+  r->num_graphs = G;
+  r->n_bfs = (uint32_t)sources.size();
+  r->n_wcc = (uint32_t)wcc_ranges.size() / 2;
+  mk_status st = MK_OK;
+  if (r->n_bfs) {
+    st = mk_bfs_create_multi(g, sources.data(), r->n_bfs, &r->bfs);
+    if (st == MK_OK) st = mk_bfs_prepare_members(r->bfs, bfs_ranges.data(), r->n_bfs);
+  }
+  if (st == MK_OK && r->n_wcc) {
+    st = mk_wcc_create(g, &r->wcc);
+    if (st == MK_OK) st = mk_wcc_prepare_ranges(r->wcc, wcc_ranges.data(), r->n_wcc);
+  }
+  if (st != MK_OK) {
+    mk_set_runner_destroy(r);
+    return st;
+  }
+  *out = r;
+  return MK_OK;
+}
+
+mk_status mk_set_runner_step(mk_set_runner *r, const uint32_t *d_del_src,
+                             const uint32_t *d_del_dst, uint32_t n_del,
+                             const uint32_t *d_ins_src, const uint32_t *d_ins_dst,
+                             const uint32_t *d_ins_w, uint32_t n_ins, void *stream) {
+  if (!r) return fail(MK_ERR_INVALID, "mk_set_runner_step: null handle");
+  if ((n_del && (!d_del_src || !d_del_dst)) || (n_ins && (!d_ins_src || !d_ins_dst)))
+    return fail(MK_ERR_INVALID, "mk_set_runner_step: null batch");
+  MK_CHECK(mk_graph_delete_edges(r->g, d_del_src, d_del_dst, n_del, stream));
+  MK_CHECK(mk_graph_insert_edges(r->g, d_ins_src, d_ins_dst, d_ins_w, n_ins, stream));
+  if (r->bfs) MK_CHECK(mk_bfs_static_members(r->bfs, stream, nullptr));
+  if (r->wcc) MK_CHECK(mk_wcc_static_prepared(r->wcc, stream, nullptr));
+  return MK_OK;
+}
+
+mk_status mk_set_runner_results(mk_set_runner *r, const uint64_t **d_bfs_packed,
+                                const uint32_t **d_wcc_labels) {
+  if (!r) return fail(MK_ERR_INVALID, "mk_set_runner_results: null handle");
+  if (d_bfs_packed) {
+    *d_bfs_packed = nullptr;
+    if (r->bfs) MK_CHECK(mk_traversal_packed(r->bfs, d_bfs_packed));
+  }
+  if (d_wcc_labels) {
+    *d_wcc_labels = nullptr;
+    if (r->wcc) MK_CHECK(mk_wcc_labels_device(r->wcc, d_wcc_labels));
+  }
+  return MK_OK;
+}
+
+mk_status mk_set_runner_destroy(mk_set_runner *r) {
+  if (!r) return MK_OK;
+  if (r->bfs) mk_traversal_destroy(r->bfs);
+  if (r->wcc) mk_wcc_destroy(r->wcc);
+  delete r;
+  return MK_OK;
+}
+
+}  // extern "C"

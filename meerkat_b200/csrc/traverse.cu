@@ -56,8 +56,13 @@ enum Ctl : int {
   kRestart = 14,  // decremental: 1 when the call recomputed from the sources
   kRound = 15,    // stamp base, persists across calls
   kFarMin0 = 16,  // near-far SSSP: smallest distance on far list 0 / 1 (set in-kernel)
-  kCtlWords = 20
+  kTrimN = 20,    // BFS repair: seeds (heads of deleted tree edges)
+  kTrimLo = 21,   // BFS repair: lowest / highest seed level
+  kTrimHi = 22,
+  kTrimC0 = 23,   // BFS repair: candidate list sizes kTrimC0 + (round % 3)
+  kCtlWords = 28
 };
+constexpr uint32_t kTrimMaxRounds = 256;  // BFS repair levels before a recompute
 
 struct TravArgs {
   GraphView g;
@@ -83,6 +88,11 @@ struct TravArgs {
   uint32_t *far0, *far1;    // far lists (vertex ids), one is appended at a time
   uint32_t *fbits;          // bit per vertex: on a far list
   unsigned long long limit_ns;
+  // BFS decremental repair with the reverse graph (trim != 0): seeds
+  // (level << 32 | vertex) and two candidate lists
+  uint32_t trim;
+  unsigned long long *tseeds;
+  uint32_t *tc0, *tc1;
 };
 
 constexpr int kTravBlock = 256;
@@ -444,6 +454,104 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       }
     }
   } else {  // kDecremental
+    uint64_t walked = 0;
+    bool restart = false;
+    if (!kUseW && a.trim) {
+      // BFS repair, level by level in the old levels.  A candidate at level
+      // L (a head of a deleted tree edge, or a tree child of a vertex that
+      // lost its level) keeps level L when some in-neighbour still at level
+      // L - 1 is not affected: that neighbour becomes its parent.  Otherwise
+      // its level rises: it is marked affected (invalidated) and its tree
+      // children become candidates of level L + 1.  Every vertex of level
+      // L - 1 is decided before level L is examined (a barrier per level), so
+      // the affected set is exact: only vertices whose level really rises
+      // are invalidated and re-seeded, not whole subtrees.
+      for (uint32_t e = tid; e < a.bn; e += nthreads) {
+        const uint32_t s = a.bsrc[e], d = a.bdst[e];
+        if (s == d || s >= a.g.V || d >= a.g.V) continue;
+        const unsigned long long pd = ld_dist(a.dist + d);
+        if (pd == kInfInf || is_source(pd, d) || pack_lo(pd) != s) continue;
+        if (atomicExch(a.stamp + d, round) == round) continue;  // already a candidate
+        const uint32_t lvl = pack_hi(pd);
+        a.tseeds[atomicAdd(ctl + kTrimN, 1u)] = ((unsigned long long)lvl << 32) | d;
+        atomicMin(ctl + kTrimLo, lvl);
+        atomicMax(ctl + kTrimHi, lvl);
+      }
+      if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+      const uint32_t nseeds = ld_acquire_u32(ctl + kTrimN);
+      const uint32_t lo = ld_acquire_u32(ctl + kTrimLo), hi_l = ld_acquire_u32(ctl + kTrimHi);
+      uint32_t ncur = 0;
+      for (uint32_t r = 0; nseeds && (lo + r <= hi_l || ncur); ++r) {
+        const uint32_t lev = lo + r;
+        if (r >= kTrimMaxRounds || (a.recompute_inv && ld_acquire_u32(ctl + kInvCount) >= a.recompute_inv)) {
+          restart = true;
+          break;
+        }
+        const uint32_t *cur = (r & 1) ? a.tc1 : a.tc0;
+        uint32_t *nxt = (r & 1) ? a.tc0 : a.tc1;
+        uint32_t *nsz = ctl + kTrimC0 + ((r + 1) % 3);
+        if (tid == 0) ctl[kTrimC0 + ((r + 2) % 3)] = 0;
+        for (uint32_t i = group; i < ncur + nseeds; i += ngroups) {
+          uint32_t v;
+          if (i < ncur) {
+            v = __ldcg(cur + i);
+          } else {
+            const unsigned long long sd = __ldcg(a.tseeds + (i - ncur));
+            if ((uint32_t)(sd >> 32) != lev) continue;
+            v = (uint32_t)sd;
+          }
+          // an in-neighbour at level L - 1 that is not affected?
+          uint32_t found = kEmptyKey;
+          const GraphView &rg = a.rg;
+          for (uint32_t b = rg.boff[v]; b < rg.boff[v + 1] && found == kEmptyKey; ++b) {
+            uint32_t sl = b;
+            for (uint32_t hop = 0; sl != kNoSlab && hop < (1u << 24) && found == kEmptyKey; ++hop) {
+              const uint4 q = ld_slab_ro(rg.slabs + 8ull * sl + L.gl);
+              uint32_t k[4], w[4];
+              if (rg.weighted)
+                lane_keys<true>(q, L.gl, k, w);
+              else
+                lane_keys<false>(q, L.gl, k, w);
+              uint32_t mine = kEmptyKey;
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                const uint32_t u = k[j];
+                if (u >= kTombKey || u == v || mine != kEmptyKey || inval_test(a.inval, u)) continue;
+                const unsigned long long pu = ld_dist(a.dist + u);
+                if (pu != kInfInf && pack_hi(pu) + 1u == lev) mine = u;
+              }
+              found = __reduce_min_sync(L.gmask, mine);
+              sl = __shfl_sync(L.gmask, q.w, L.gbase + 7);
+            }
+          }
+          if (found != kEmptyKey) {
+            if (L.gl == 0) a.dist[v] = pack(lev, found);  // same level, new parent
+            continue;
+          }
+          // v's level rises: invalidate it, its tree children become candidates
+          if (L.gl == 0) {
+            inval_set(a.inval, v);
+            a.dist[v] = kInfInf;
+            a.inv_list[atomicAdd(ctl + kInvCount, 1u)] = v;
+          }
+          walk_vertex(a.g, L, v, [&](const uint4 &q) {
+            uint32_t k[4], w[4];
+            lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+            for (int j = 0; j < keys_per_lane<kW>(); ++j) {
+              const uint32_t x = k[j];
+              if (x >= kTombKey || x == v) continue;
+              const unsigned long long px = ld_dist(a.dist + x);
+              if (px == kInfInf || pack_lo(px) != v || pack_hi(px) != lev + 1u) continue;
+              if (atomicExch(a.stamp + x, round) != round) nxt[atomicAdd(nsz, 1u)] = x;
+            }
+          });
+        }
+        if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+        ncur = ld_acquire_u32(nsz);
+      }
+      walked = ld_acquire_u32(ctl + kInvCount);
+    } else {
     // D1: children of deleted tree edges.  Every invalidated vertex goes to
     // inv_list (for the final flag reset) and to the invalidation frontier.
     auto invalidate = [&](uint32_t v, unsigned long long *gfr, uint32_t *gsz) {
@@ -467,8 +575,6 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
     // block is already filling for the next level.
     // The running total of the level sizes (each read after a barrier, the
     // same in every thread) stops the walk early once a recompute is due.
-    uint64_t walked = 0;
-    bool restart = false;
     for (uint32_t dl = 0;; ++dl) {
       const uint32_t n = ld_acquire_u32(ctl + kDSz0 + (dl % 3));
       if (n == 0) break;
@@ -500,6 +606,8 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       }
       if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
     }
+    }  // whole-subtree invalidation
+    (void)walked;
     const uint32_t hi = ld_acquire_u32(ctl + kInvCount);
     if (restart) {
       // Most of the tree is gone: a recompute from the sources costs less
@@ -773,6 +881,9 @@ struct mk_traversal {
   unsigned long long *pushed = nullptr;
   uint32_t *far0 = nullptr, *far1 = nullptr, *fbits = nullptr;  // near-far SSSP
   mk_graph *rev = nullptr;  // in-edges of the same graph, for pull levels (BFS)
+  // BFS decremental repair (allocated when a reverse graph is attached)
+  unsigned long long *tseeds = nullptr;
+  uint32_t *tc0 = nullptr, *tc1 = nullptr;
   std::vector<uint32_t> h_sources;
   // prepared member table (BFS): counter word, uint4 (lo, hi, b0, b1) per
   // small range (largest first), their sources, then the sources whose
@@ -870,6 +981,8 @@ static mk_status trav_issue(mk_traversal *t, uint32_t mode, const uint32_t *bs, 
   if (delta) MK_CUDA(cudaMemsetAsync(t->fbits, 0, ((size_t)g->V + 31) / 32 * 4, s));
   // clear everything but the persistent round counter
   MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
+  MK_CUDA(cudaMemsetAsync(t->ctl + kTrimN, 0, (kCtlWords - kTrimN) * 4, s));
+  MK_CUDA(cudaMemsetAsync(t->ctl + kTrimLo, 0xFF, 4, s));
   MK_CUDA(cudaMemsetAsync(t->pushed, 0, 8, s));
   TravArgs a;
   a.g = g->view();
@@ -901,6 +1014,10 @@ static mk_status trav_issue(mk_traversal *t, uint32_t mode, const uint32_t *bs, 
   a.fbits = t->fbits;
   a.mode = mode;
   a.limit_ns = g->wait_limit_ns();
+  a.trim = (mode == kDecremental && !t->sssp && t->rev && t->tseeds) ? 1u : 0u;
+  a.tseeds = t->tseeds;
+  a.tc0 = t->tc0;
+  a.tc1 = t->tc1;
   const void *fn;
   if (g->weighted)
     fn = t->sssp ? (const void *)k_traverse<true, true> : (const void *)k_traverse<true, false>;
@@ -1002,6 +1119,23 @@ mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev) {
     if (!g_rev->reverse || g_rev->V != t->g->V || g_rev->device != t->g->device)
       return fail(MK_ERR_INVALID,
                   "mk_traversal_set_reverse: needs a reverse graph of the same size on the same device");
+  }
+  DeviceGuard dg(t->g->device);
+  if (g_rev && !t->sssp && !t->tseeds) {
+    // BFS repair lists: a vertex is a seed or a candidate at most once per call
+    const size_t V = t->g->V;
+    MK_CUDA(cudaDeviceSynchronize());
+    cudaError_t e = cudaMalloc(&t->tseeds, (V + 16) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&t->tc0, (V + 16) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&t->tc1, (V + 16) * 4);
+    if (e != cudaSuccess) {
+      cudaFree(t->tseeds);
+      cudaFree(t->tc0);
+      cudaFree(t->tc1);
+      t->tseeds = nullptr;
+      t->tc0 = t->tc1 = nullptr;
+      return cuda_fail(e, "mk_traversal_set_reverse: repair lists");
+    }
   }
   t->rev = g_rev;
   return MK_OK;
@@ -1195,6 +1329,9 @@ mk_status mk_traversal_destroy(mk_traversal *t) {
   cudaFree(t->ctl);
   cudaFree(t->pushed);
   cudaFree(t->sources);
+  cudaFree(t->tseeds);
+  cudaFree(t->tc0);
+  cudaFree(t->tc1);
   cudaFree(t->far0);
   cudaFree(t->far1);
   cudaFree(t->fbits);

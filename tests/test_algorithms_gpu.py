@@ -395,8 +395,12 @@ def test_decremental_reseed_from_reverse_graph():
             dist = sssp.Distances()
             tree = np.flatnonzero((dist != mk.MK_INF) & (par != np.arange(V)))
             pick = rng.choice(tree, size=min(len(tree), 200), replace=False)
-            ds = np.concatenate([ds, par[pick]]).astype(np.uint32)
-            dd = np.concatenate([dd, pick]).astype(np.uint32)
+            # and BFS tree edges: the BFS repair re-parents or invalidates their heads
+            bpar = (bfs.packed() & np.uint64(0xFFFFFFFF)).astype(np.int64)
+            btree = np.flatnonzero((bfs.Distances() != mk.MK_INF) & (bpar != np.arange(V)))
+            bpick = rng.choice(btree, size=min(len(btree), 200), replace=False)
+            ds = np.concatenate([ds, par[pick], bpar[bpick]]).astype(np.uint32)
+            dd = np.concatenate([dd, pick, bpick]).astype(np.uint32)
             for g in (G, Gr):
                 g.DeleteEdges(to_dev(ds), to_dev(dd))
             O.delete(ds, dd)
@@ -404,6 +408,7 @@ def test_decremental_reseed_from_reverse_graph():
             sssp.Decremental(to_dev(ds), to_dev(dd))
             np.testing.assert_array_equal(bfs.Distances(), O.bfs(src))
             np.testing.assert_array_equal(sssp.Distances(), O.sssp(src))
+            assert O.check_parents(src, bfs.packed(), weighted=False) == 0
             assert O.check_parents(src, sssp.packed(), weighted=True) == 0
             is_, id_ = es.sample_absent(len(s) // 20, seed=60 + r)
             iw = rng.integers(1, 1001, len(is_)).astype(np.uint32)
@@ -417,3 +422,44 @@ def test_decremental_reseed_from_reverse_graph():
         with pytest.raises(mk.MeerkatError):
             Gu, _ = make_pair(V, s, d, reverse=True)  # unweighted reverse
             mk.SSSP(G, src, V).set_reverse(Gu)
+
+
+def test_bfs_repair_invalidates_only_vertices_whose_level_rises():
+    """With the reverse graph, decremental BFS invalidates only the vertices
+    whose level really rises (the others take a parent one level up), so it
+    invalidates no more than the whole-subtree walk without the reverse
+    graph, and exactly the oracle's count of vertices whose level changed or
+    that became unreachable; both give the oracle's levels."""
+    V = 1 << 13
+    s, d, w = mk.gen_rmat(13, 120000, seed=61, w_lo=1, w_hi=9)
+    G, O = make_pair(V, s, d, w, weighted=True)
+    Gr, _ = make_pair(V, s, d, w, weighted=True, reverse=True)
+    G.set_tuning(recompute_permille=0)
+    src = int(np.argmax(np.bincount(s, minlength=V)))
+    plain, rep = mk.BFS(G, src, V), mk.BFS(G, src, V)
+    rep.set_reverse(Gr)
+    plain.Static()
+    rep.Static()
+    rng = np.random.default_rng(62)
+    for r in range(3):
+        before = O.bfs(src)
+        par = (rep.packed() & np.uint64(0xFFFFFFFF)).astype(np.int64)
+        tree = np.flatnonzero((before != mk.MK_INF) & (par != np.arange(V)))
+        pick = rng.choice(tree, size=min(len(tree), 400), replace=False)
+        ds, dd = par[pick].astype(np.uint32), pick.astype(np.uint32)
+        for g in (G, Gr):
+            g.DeleteEdges(to_dev(ds), to_dev(dd))
+        O.delete(ds, dd)
+        plain.Decremental(to_dev(ds), to_dev(dd))
+        rep.Decremental(to_dev(ds), to_dev(dd))
+        after = O.bfs(src)
+        np.testing.assert_array_equal(rep.Distances(), after)
+        np.testing.assert_array_equal(plain.Distances(), after)
+        assert O.check_parents(src, rep.packed(), weighted=False) == 0
+        inv_rep, rec_rep = rep.decremental_stats()
+        inv_plain, _ = plain.decremental_stats()
+        assert not rec_rep
+        assert inv_rep == int((after != before).sum())
+        assert inv_rep <= inv_plain
+    for o in (plain, rep, G, Gr):
+        o.close()

@@ -14,6 +14,7 @@ from oracle import OracleGraph
 ROOT = Path(__file__).resolve().parent.parent
 SRC = ROOT / "tests" / "cpp" / "drop_in_driver.cpp"
 FILE_DRIVER = ROOT / "tests" / "cpp" / "bfs_file_driver.cpp"
+SET_DRIVER = ROOT / "tests" / "cpp" / "set_runner_driver.cpp"
 
 
 def build_driver(tmp_path, src=SRC) -> Path:
@@ -31,6 +32,7 @@ def test_shim_compiles_and_links(tmp_path):
     exe = build_driver(tmp_path)
     assert exe.exists()
     assert build_driver(tmp_path, FILE_DRIVER).exists()
+    assert build_driver(tmp_path, SET_DRIVER).exists()
 
 
 @pytest.mark.gpu
@@ -80,3 +82,40 @@ def test_reference_style_driver_matches_oracle(tmp_path):
     np.testing.assert_array_equal(got[:, 0], O.bfs(0))
     np.testing.assert_array_equal(got[:, 1], O.sssp(0))
     np.testing.assert_array_equal(got[:, 2], O.wcc())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("capture", ["0", "1"])
+def test_cpp_batched_step_matches_oracle(tmp_path, capture):
+    """The batched many-graph step through the C++ shim (GraphSet +
+    GraphSetRunner over mk_set_runner_*), issued step by step and captured
+    into a CUDA graph: every member's BFS levels or WCC labels equal the
+    oracle's on that member alone after the same update steps."""
+    exe = build_driver(tmp_path, SET_DRIVER)
+    G, K = 6, 5
+    r = subprocess.run([str(exe), str(G), str(K), capture], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    assert len(lines) == G
+    for m, ln in enumerate(lines):
+        f = list(map(int, ln.split()))
+        assert f[0] == m
+        kind, src, got = f[1], f[2], np.array(f[3:], dtype=np.uint32)
+        n = 256 << (m % 4)
+        scale = n.bit_length() - 1
+        E = 6 * n
+        s, d, w = mk.gen_rmat(scale, E, seed=100 + m, w_lo=1, w_hi=64)
+        O = OracleGraph(n)
+        O.insert(s, d, w)
+        us, ud = s[:E // 10], d[:E // 10]
+        for k in range(K):
+            if k % 2 == 0:
+                O.delete(us, ud)
+            else:
+                O.insert(us, ud, np.full(len(us), 7, np.uint32))
+        assert len(got) == n
+        if kind == 0:
+            np.testing.assert_array_equal(got, O.bfs(src))
+        else:
+            np.testing.assert_array_equal(got, O.wcc())
