@@ -238,6 +238,40 @@ def cpu_baseline(graph, batches, max_batches=3, warmup=0):
             "seconds": total}
 
 
+def head_slab_share(G, timed_batches):
+    """Share of batch edges whose head slab (the bucket slab their probe
+    reads first) is also the head slab of another edge of the same
+    sub-batch, and distinct head slabs per edge: what sorting a sub-batch by
+    slab could save at most (one line read per distinct slab instead of one
+    per edge).  Computed on the host from the graph's bucket layout with the
+    kernels' bucket hash (mix32, multiply-shift)."""
+    boff = G.GetVertexBucketsOffsets().astype(np.uint64)
+    nb = G.GetBucketsPerVertex().astype(np.uint64)
+
+    def mix32(x):
+        x = x.astype(np.uint64)
+        x ^= x >> np.uint64(16)
+        x = (x * np.uint64(0x7FEB352D)) & np.uint64(0xFFFFFFFF)
+        x ^= x >> np.uint64(15)
+        x = (x * np.uint64(0x846CA68B)) & np.uint64(0xFFFFFFFF)
+        x ^= x >> np.uint64(16)
+        return x
+
+    out = {}
+    for name, cols in (("delete", (0, 1)), ("insert", (2, 3))):
+        shared = distinct = total = 0
+        for b in timed_batches:
+            u, v = b[cols[0]].astype(np.int64), b[cols[1]]
+            head = boff[u] + ((mix32(v) * nb[u]) >> np.uint64(32))
+            _, cnt = np.unique(head, return_counts=True)
+            shared += int(cnt[cnt > 1].sum())
+            distinct += len(cnt)
+            total += len(head)
+        out[name + "_edges_sharing_a_head_slab"] = shared / total
+        out[name + "_distinct_head_slabs_per_edge"] = distinct / total
+    return out
+
+
 def oracle_large(graph, hist, timed_at, A, gpu, algo):
     """Rank 0, after the GPU work of the updates workload.  The oracle (C,
     OpenMP, every host core) replays every batch the GPU graph received, in
@@ -883,10 +917,21 @@ def serving_compare(num_graphs, scales, rates, N, budget_gb, rank, world, local,
     for mode in ("coalesced", "alone"):
         t1 = time.time()
         out = srv.run(copy(sat_reqs), wl, mode=mode)
+        if mode == "alone":
+            sat_alone_kinds = out["by_kind"]
         sat[mode] = slim(out)
         sat[mode]["by_kind_service_p50_ms"] = {k: v["service_p50_ms"] for k, v in out["by_kind"].items()}
         log(f"[serving] saturation {mode}: {out['throughput_rps']:.1f} rps, p50 {out['p50_ms']:.1f} ms,"
             f" {out['rounds']} rounds, {time.time() - t1:.1f}s")
+    # what bounds the coalesced mode: heavy requests (PageRank, TC) are not
+    # coalesced, so their one-at-a-time GPU time per request (the alone
+    # run's service times) caps any schedule's throughput
+    heavy_ms = sum(v["service_total_ms"] for k, v in sat_alone_kinds.items()
+                   if k in ("pagerank", "tc")) / N
+    fast_ms = sum(v["service_total_ms"] for k, v in sat_alone_kinds.items()
+                  if k not in ("pagerank", "tc")) / N
+    sat["heavy_bound"] = {"heavy_ms_per_request": heavy_ms, "fast_ms_per_request": fast_ms,
+                          "max_rps_if_fast_work_were_free": 1000.0 / heavy_ms if heavy_ms else None}
     if not rates:
         rates = [round(f * sat["alone"]["throughput_rps"], 1) for f in rate_fractions]
     table = []
@@ -1455,6 +1500,7 @@ def main():
     upd_ms = ms / K  # device time of one delete + insert pair (graph replay)
     achieved = upd_bytes / (upd_ms / 1000.0) / 1e9
     traffic = profile_traffic()
+    share = head_slab_share(G, batches[W:W + min(K, 4)])
     # the same random-line pattern without decision logic, on a buffer the
     # size of the slab pool: what the memory system gives this access pattern
     ceiling = probe_random_rmw(int(info["pool_capacity"]) * 128, V, 2 * HALF, device=local)
@@ -1514,6 +1560,7 @@ def main():
                          "unit": "GB/s", "frac": achieved / peak,
                          "algorithmic_bytes_per_step": upd_bytes,
                          "traffic": traffic,
+                         "head_slab_sharing": share,
                          "pattern_ceiling": {
                              "what": "benchmark probe: random 128-B line read + CAS + random "
                                      "4-B read and add per operation, no decision logic, "

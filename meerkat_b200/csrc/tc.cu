@@ -114,7 +114,8 @@ constexpr int kTcWarps = 4;           // warps per block in the small kernel (32
 constexpr int kTcSetCap = 2048;       // per-warp shared hash capacity (entries)
 constexpr uint32_t kTcSmallMax = 1024;  // N+(u) handled by one warp
 
-// Open-addressing sets of capacity 2^k (k >= 6), at most half full, with
+// Open-addressing sets of capacity 2^k (k >= 6), at most half full (a
+// quarter where the warp's share of shared memory allows), with
 // Fibonacci hashing: the slot is the top k bits of key * 2654435769 (one
 // multiply and one shift per probe; the sets are probed far more often than
 // built).  shift = 32 - k.  Probes are bounded by the capacity.
@@ -218,8 +219,10 @@ __global__ void __launch_bounds__(kTcWarps * 32)
     const uint32_t du = (uint32_t)(r1 - r0);
     if (u != have_u) {
       __syncwarp();
+      // load at most 1/4 (1/2 for the largest sets): most probes miss, and a
+      // miss walks the probe run to an EMPTY slot
       cap = 64;
-      while (cap < 2 * du) cap <<= 1;
+      while (cap < 4 * du && cap < (uint32_t)kTcSetCap) cap <<= 1;
       for (uint32_t i = lane; i < cap; i += 32) set[i] = kEmptyKey;
       __syncwarp();
       for (uint32_t i = lane; i < du; i += 32) set_insert(set, cap - 1, __clz(cap) + 1, ocol[r0 + i]);

@@ -362,7 +362,8 @@ class GraphServer:
                 by_kind[KIND_NAMES[k]] = {"n": len(sel),
                                           "p50_ms": float(np.percentile(sel, 50) * 1000.0),
                                           "p99_ms": float(np.percentile(sel, 99) * 1000.0),
-                                          "service_p50_ms": float(np.percentile(svc, 50) * 1000.0)}
+                                          "service_p50_ms": float(np.percentile(svc, 50) * 1000.0),
+                                          "service_total_ms": float(np.sum(svc) * 1000.0)}
         n = len(done)
         return {"mode": mode, "requests": len(reqs), "rounds": rounds, "rejected": rejected,
                 "p50_ms": float(np.percentile(lat, 50)) if n else 0.0,
