@@ -169,7 +169,7 @@ def probe_random_rmw(line_bytes: int, small_words: int, num_ops: int, repeats: i
     sink = torch.zeros(1, dtype=torch.int64, device=dev)
     torch.cuda.synchronize(dev)
     out = {}
-    for mode in (0, 1, 2):
+    for mode in (0, 1, 2, 3, 4):
         best = None
         for r in range(repeats):
             ms = C.c_float(0.0)
@@ -181,7 +181,8 @@ def probe_random_rmw(line_bytes: int, small_words: int, num_ops: int, repeats: i
         out[mode] = num_ops / (best / 1000.0)
     del lines, a, b, sink
     torch.cuda.empty_cache()
-    return {"read_lines_per_s": out[0], "read_cas_per_s": out[1], "update_pattern_per_s": out[2]}
+    return {"read_lines_per_s": out[0], "read_cas_per_s": out[1], "update_pattern_per_s": out[2],
+            "read_32B_sectors_per_s": out[3], "read_64B_halves_per_s": out[4]}
 
 
 def make_workload(n_batches: int, source: str = "product"):
@@ -1130,8 +1131,11 @@ def grid_stress(side, nbatch, batch, rank, world, local):
            "decremental_p50_ms": {k: p50(v) for k, v in dec.items()},
            "incremental_p50_ms": {k: p50(v) for k, v in inc.items()},
            "decremental_repair": {k: {"invalidated": [int(x) for x, _ in v],
-                                      "recomputed": [bool(r) for _, r in v]}
+                                      "recomputed": [bool(r) for _, r in v],
+                                      "ms": [round(x, 3) for x in dec[k + "_ms"]]}
                                   for k, v in repair.items()},
+           "recompute_rule": "a decremental call recomputes from the source once its "
+                             "invalidation walk passes recompute_permille of the vertices",
            "components_after": comps, "matches_static_recompute": same}
     if par is not None:
         out["parity"] = par

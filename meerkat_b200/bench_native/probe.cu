@@ -14,6 +14,8 @@
 //   mode 1  mode 0 + one CAS per line (the slab read-modify-write)
 //   mode 2  mode 1 + a random 4-byte read and a random 4-byte add on two
 //           per-vertex arrays of `small_words` words each
+//   mode 3  random 32-byte sector reads (one sector of a random line)
+//   mode 4  random 64-byte half-line reads
 //
 // Warp-cooperative: a warp reads the lines of its 32 operations as 32
 // coalesced loads, lane j then issues operation j's CAS / add.  Lines and
@@ -40,6 +42,25 @@ __global__ void __launch_bounds__(256) k_probe_rmw(uint32_t *__restrict__ lines,
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = (gridDim.x * (uint64_t)blockDim.x) >> 5;
   unsigned long long acc = 0;
+  if (mode >= 3) {
+    // partial-line reads: lane-group g of (2 or 4) lanes reads 32 or 64
+    // bytes of operation g's random line (16 bytes per lane)
+    const uint32_t per = mode == 3 ? 2u : 4u;  // lanes per operation
+    const uint32_t ops_per_warp = 32u / per;
+    for (uint64_t base = warp * ops_per_warp; base < nops; base += nwarps * ops_per_warp) {
+      const uint64_t op = base + lane / per;
+      if (op < nops) {
+        const unsigned long long h = probe_mix(seed ^ op);
+        const uint64_t line = h % nlines;
+        const uint32_t sec = (uint32_t)(h >> 40) & (mode == 3 ? 3u : 1u);  // which 32/64 B of the line
+        const uint4 *p = reinterpret_cast<const uint4 *>(lines + line * 32) + sec * per + (lane % per);
+        const uint4 q = __ldcg(p);
+        acc += q.x ^ q.y ^ q.z ^ q.w;
+      }
+    }
+    if (acc == 0x5EEDull) atomicAdd(sink, acc);
+    return;
+  }
   for (uint64_t base = warp * 32; base < nops; base += nwarps * 32) {
     const uint64_t op = base + lane;
     const unsigned long long h = probe_mix(seed ^ op);
@@ -79,7 +100,7 @@ extern "C" int mkb_probe_random_rmw(void *d_lines, uint64_t line_count, void *d_
                                     void *d_small_b, uint32_t small_words, uint64_t num_ops,
                                     uint32_t mode, uint64_t seed, void *d_sink, void *stream,
                                     float *ms_out) {
-  if (!d_lines || !line_count || !d_sink || !ms_out || mode > 2 ||
+  if (!d_lines || !line_count || !d_sink || !ms_out || mode > 4 ||
       (mode == 2 && (!d_small_a || !d_small_b || !small_words)))
     return 1;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
