@@ -48,12 +48,12 @@ enum Ctl : int {
   kBar1 = 1,      // barrier generation
   kErr = 2,       // sticky error bits
   kThr = 3,       // near-far SSSP: distance threshold of the near frontier
-  kSz0 = 4,       // frontier sizes kSz0 + (level % 3)
+  kSz0 = 4,       // frontier sizes kSz0 + (level % 3): words 4, 5, 6
+  kRestart = 7,   // decremental: 1 when the call recomputed from the sources
   kInvCount = 8,  // invalidated vertices so far (append cursor of inv_list)
   kLevels = 9,    // relaxation levels run by the last call
   kDSz0 = 10,     // invalidation frontier sizes kDSz0 + (level % 3)
-  kFarN0 = 13,    // near-far SSSP: far list sizes kFarN0 + (list 0 / 1)
-  kRestart = 14,  // decremental: 1 when the call recomputed from the sources
+  kFarN0 = 13,    // near-far SSSP: far list sizes kFarN0 + (list 0 / 1): words 13, 14
   kRound = 15,    // stamp base, persists across calls
   kFarMin0 = 16,  // near-far SSSP: smallest distance on far list 0 / 1 (set in-kernel)
   kTrimN = 20,    // BFS repair: seeds (heads of deleted tree edges)
@@ -404,6 +404,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   const uint32_t nthreads = gridDim.x * blockDim.x;
   const uint32_t group = tid >> 3;
   const uint32_t ngroups = nthreads >> 3;
+  const unsigned long long t_start = global_ns();
   uint32_t *ctl = a.ctl;
   uint32_t *err = ctl + kErr;
   unsigned long long *fr[2] = {a.fr0, a.fr1};
@@ -663,8 +664,17 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
   // is empty instead drains the far list: the threshold moves to the far
   // list's smallest distance plus delta, vertices below it join the next
   // level and the rest move to the other far list.
+  // The level loop ends when the frontier (and the far lists) run dry; as a
+  // guard against a logic error that would keep it going with every barrier
+  // met, a launch that has run longer than 64 wait limits (at least 60 s)
+  // reports a timeout and stops.
+  const unsigned long long guard_ns = max(64ull * a.limit_ns, 60000000000ull);
   uint32_t lv = 0;
   for (;; ++lv) {
+    if (global_ns() - t_start > guard_ns) {
+      if (tid == 0) atomicOr(err, kErrTimeout);
+      break;
+    }
     const uint32_t n = ld_acquire_u32(ctl + kSz0 + (lv % 3));
     uint32_t nfar = 0;
     if (n == 0) {
