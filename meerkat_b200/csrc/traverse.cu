@@ -59,9 +59,13 @@ enum Ctl : int {
   kTrimN = 20,    // BFS repair: seeds (heads of deleted tree edges)
   kTrimLo = 21,   // BFS repair: lowest / highest seed level
   kTrimHi = 22,
-  kTrimC0 = 23,   // BFS repair: candidate list sizes kTrimC0 + (round % 3)
-  kCtlWords = 28
+  kTCand0 = 23,   // BFS repair: candidate list sizes, words 23, 24 (round parity)
+  kTItem0 = 25,   // BFS repair: support-search item counts, words 25, 26
+  kTChild = 27,   // BFS repair: child-scan items of the level
+  kTReseed = 28,  // decremental with a reverse graph: re-seed items
+  kCtlWords = 32
 };
+constexpr uint32_t kRepairChunk = 8;  // buckets per repair / re-seed work item
 constexpr uint32_t kTrimMaxRounds = 256;  // BFS repair levels before a recompute
 
 struct TravArgs {
@@ -88,11 +92,14 @@ struct TravArgs {
   uint32_t *far0, *far1;    // far lists (vertex ids), one is appended at a time
   uint32_t *fbits;          // bit per vertex: on a far list
   unsigned long long limit_ns;
-  // BFS decremental repair with the reverse graph (trim != 0): seeds
-  // (level << 32 | vertex) and two candidate lists
+  // decremental with the reverse graph: BFS repair (trim != 0) -- seeds
+  // (level << 32 | vertex), candidate lists and support-search items per
+  // round parity, child-scan items, each candidate's best support (tpar,
+  // kEmptyKey when none) -- and the chunked re-seed items (BFS and SSSP)
   uint32_t trim;
   unsigned long long *tseeds;
-  uint32_t *tc0, *tc1;
+  uint32_t *tcand0, *tcand1, *tpar;
+  unsigned long long *titems0, *titems1, *tchild, *treseed;
 };
 
 constexpr int kTravBlock = 256;
@@ -124,6 +131,26 @@ __device__ __forceinline__ void push_vertex(const TravArgs &a, const BlockQueue 
     uint32_t base = atomicAdd(gsz, k);
     for (uint32_t j = 0; j < k; ++j) gfr[base + j] = item(v, j);
   }
+}
+
+// Work items (chunk << 32 | v) over v's buckets in `gv`, kRepairChunk
+// buckets each (one item for a vertex with no bucket beyond the first).
+__device__ __forceinline__ void push_items(const GraphView &gv, uint32_t v, unsigned long long *list,
+                                           uint32_t *cnt) {
+  const uint32_t nb = gv.boff[v + 1] - gv.boff[v];
+  const uint32_t k = max(1u, (nb + kRepairChunk - 1) / kRepairChunk);
+  const uint32_t base = atomicAdd(cnt, k);
+  for (uint32_t j = 0; j < k; ++j) list[base + j] = item(v, j);
+}
+
+// The vertex and bucket range [b0, b1) of a work item of push_items.
+__device__ __forceinline__ void item_buckets(const GraphView &gv, unsigned long long it, uint32_t &v,
+                                             uint32_t &b0, uint32_t &b1) {
+  v = (uint32_t)it;
+  const uint32_t c = (uint32_t)(it >> 32);
+  const uint32_t s = gv.boff[v], e = gv.boff[v + 1];
+  b0 = min(s + c * kRepairChunk, e);
+  b1 = min(b0 + kRepairChunk, e);
 }
 
 // Frontier buffers, sizes and dist words are rewritten by other SMs inside
@@ -356,14 +383,18 @@ __device__ __forceinline__ void pull_level(const TravArgs &a, const Lanes &L, co
 // its weights when SSSP), instead of a sweep over every bucket of the graph.
 template <bool kRW, bool kUseW>
 __device__ __forceinline__ void pull_reseed(const TravArgs &a, const Lanes &L, const BlockQueue &Q,
-                                            uint32_t group, uint32_t ngroups, uint32_t ninv,
+                                            uint32_t group, uint32_t ngroups, uint32_t nitems,
                                             uint32_t stamp_next, unsigned long long *gfr,
                                             uint32_t *gsz) {
+  // one work item per chunk of an invalidated vertex's in-edge buckets
+  // (a hub's in-edges spread over many groups); each item offers the best
+  // of its chunk with an atomic minimum
   const GraphView &rg = a.rg;
-  for (uint32_t i = group; i < ninv; i += ngroups) {
-    const uint32_t v = __ldcg(a.inv_list + i);
+  for (uint32_t i = group; i < nitems; i += ngroups) {
+    uint32_t v, b0, b1;
+    item_buckets(rg, __ldcg(a.treseed + i), v, b0, b1);
     unsigned long long best = kInfInf;  // pack(candidate distance, parent)
-    for (uint32_t b = rg.boff[v]; b < rg.boff[v + 1]; ++b) {
+    for (uint32_t b = b0; b < b1; ++b) {
       uint32_t s = b;
       for (uint32_t hop = 0; s != kNoSlab && hop < (1u << 24); ++hop) {
         const uint4 q = ld_slab_ro(rg.slabs + 8ull * s + L.gl);
@@ -481,30 +512,59 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
       const uint32_t nseeds = ld_acquire_u32(ctl + kTrimN);
       const uint32_t lo = ld_acquire_u32(ctl + kTrimLo), hi_l = ld_acquire_u32(ctl + kTrimHi);
-      uint32_t ncur = 0;
-      for (uint32_t r = 0; nseeds && (lo + r <= hi_l || ncur); ++r) {
-        const uint32_t lev = lo + r;
+      // the seeds of one level become candidates, with their support-search
+      // work items (chunks of their in-edge buckets)
+      auto seed_level = [&](uint32_t lev, uint32_t *cand, uint32_t *ncand,
+                            unsigned long long *items, uint32_t *nitems) {
+        for (uint32_t i = tid; i < nseeds; i += nthreads) {
+          const unsigned long long sd = __ldcg(a.tseeds + i);
+          if ((uint32_t)(sd >> 32) != lev) continue;
+          const uint32_t v = (uint32_t)sd;
+          cand[atomicAdd(ncand, 1u)] = v;
+          push_items(a.rg, v, items, nitems);
+        }
+      };
+      if (nseeds) {
+        seed_level(lo, a.tcand0, ctl + kTCand0, a.titems0, ctl + kTItem0);
+        if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+      }
+      // Each level in three steps, a barrier after each:
+      //   A  every support-search item scans its chunk of a candidate's
+      //      in-edges for a neighbour one level up that is not affected
+      //      (the smallest such id wins, by atomicMin on tpar);
+      //   B  a candidate with a support keeps its level under that parent;
+      //      one without is affected: invalidated, queued for the re-seed,
+      //      and its out-edges queued (in chunks) for the child scan;
+      //   C  the child-scan items find the tree children of the affected
+      //      vertices (the next level's candidates) and the next level's
+      //      seeds join them.
+      // Hubs are split into many items, so no vertex serialises a level.
+      for (uint32_t r = 0; nseeds; ++r) {
+        const uint32_t lev = lo + r, cb = r & 1u, nb = cb ^ 1u;
+        const uint32_t ncand = ld_acquire_u32(ctl + kTCand0 + cb);
+        const uint32_t nit = ld_acquire_u32(ctl + kTItem0 + cb);
+        if (ncand == 0 && lev >= hi_l) break;
         if (r >= kTrimMaxRounds || (a.recompute_inv && ld_acquire_u32(ctl + kInvCount) >= a.recompute_inv)) {
           restart = true;
           break;
         }
-        const uint32_t *cur = (r & 1) ? a.tc1 : a.tc0;
-        uint32_t *nxt = (r & 1) ? a.tc0 : a.tc1;
-        uint32_t *nsz = ctl + kTrimC0 + ((r + 1) % 3);
-        if (tid == 0) ctl[kTrimC0 + ((r + 2) % 3)] = 0;
-        for (uint32_t i = group; i < ncur + nseeds; i += ngroups) {
-          uint32_t v;
-          if (i < ncur) {
-            v = __ldcg(cur + i);
-          } else {
-            const unsigned long long sd = __ldcg(a.tseeds + (i - ncur));
-            if ((uint32_t)(sd >> 32) != lev) continue;
-            v = (uint32_t)sd;
-          }
-          // an in-neighbour at level L - 1 that is not affected?
+        const uint32_t *cand = cb ? a.tcand1 : a.tcand0;
+        const unsigned long long *items = cb ? a.titems1 : a.titems0;
+        uint32_t *cand_n = nb ? a.tcand1 : a.tcand0;
+        unsigned long long *items_n = nb ? a.titems1 : a.titems0;
+        if (tid == 0) {
+          ctl[kTCand0 + nb] = 0;
+          ctl[kTItem0 + nb] = 0;
+          ctl[kTChild] = 0;
+        }
+        // A
+        const GraphView &rg = a.rg;
+        for (uint32_t i = group; i < nit; i += ngroups) {
+          uint32_t v, b0, b1;
+          item_buckets(rg, __ldcg(items + i), v, b0, b1);
+          if (__ldcg(a.tpar + v) != kEmptyKey) continue;  // another chunk found one
           uint32_t found = kEmptyKey;
-          const GraphView &rg = a.rg;
-          for (uint32_t b = rg.boff[v]; b < rg.boff[v + 1] && found == kEmptyKey; ++b) {
+          for (uint32_t b = b0; b < b1 && found == kEmptyKey; ++b) {
             uint32_t sl = b;
             for (uint32_t hop = 0; sl != kNoSlab && hop < (1u << 24) && found == kEmptyKey; ++hop) {
               const uint4 q = ld_slab_ro(rg.slabs + 8ull * sl + L.gl);
@@ -517,7 +577,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
 #pragma unroll
               for (int j = 0; j < 4; ++j) {
                 const uint32_t u = k[j];
-                if (u >= kTombKey || u == v || mine != kEmptyKey || inval_test(a.inval, u)) continue;
+                if (u >= kTombKey || u == v || u >= mine || inval_test(a.inval, u)) continue;
                 const unsigned long long pu = ld_dist(a.dist + u);
                 if (pu != kInfInf && pack_hi(pu) + 1u == lev) mine = u;
               }
@@ -525,17 +585,31 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
               sl = __shfl_sync(L.gmask, q.w, L.gbase + 7);
             }
           }
-          if (found != kEmptyKey) {
-            if (L.gl == 0) a.dist[v] = pack(lev, found);  // same level, new parent
-            continue;
-          }
-          // v's level rises: invalidate it, its tree children become candidates
-          if (L.gl == 0) {
+          if (found != kEmptyKey && L.gl == 0) atomicMin(a.tpar + v, found);
+        }
+        if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+        // B
+        for (uint32_t i = tid; i < ncand; i += nthreads) {
+          const uint32_t v = __ldcg(cand + i);
+          const uint32_t w = __ldcg(a.tpar + v);
+          if (w != kEmptyKey) {
+            a.tpar[v] = kEmptyKey;
+            a.dist[v] = pack(lev, w);  // same level, new parent
+          } else {
             inval_set(a.inval, v);
             a.dist[v] = kInfInf;
             a.inv_list[atomicAdd(ctl + kInvCount, 1u)] = v;
+            push_items(a.g, v, a.tchild, ctl + kTChild);
+            push_items(rg, v, a.treseed, ctl + kTReseed);
           }
-          walk_vertex(a.g, L, v, [&](const uint4 &q) {
+        }
+        if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+        // C
+        const uint32_t nch = ld_acquire_u32(ctl + kTChild);
+        for (uint32_t i = group; i < nch; i += ngroups) {
+          uint32_t v, b0, b1;
+          item_buckets(a.g, __ldcg(a.tchild + i), v, b0, b1);
+          walk_buckets(a.g, L, b0, b1, [&](const uint4 &q) {
             uint32_t k[4], w[4];
             lane_keys<kW>(q, L.gl, k, w);
 #pragma unroll
@@ -544,12 +618,14 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
               if (x >= kTombKey || x == v) continue;
               const unsigned long long px = ld_dist(a.dist + x);
               if (px == kInfInf || pack_lo(px) != v || pack_hi(px) != lev + 1u) continue;
-              if (atomicExch(a.stamp + x, round) != round) nxt[atomicAdd(nsz, 1u)] = x;
+              if (atomicExch(a.stamp + x, round) == round) continue;
+              cand_n[atomicAdd(ctl + kTCand0 + nb, 1u)] = x;
+              push_items(rg, x, items_n, ctl + kTItem0 + nb);
             }
           });
         }
+        if (lev + 1u <= hi_l) seed_level(lev + 1u, cand_n, ctl + kTCand0 + nb, items_n, ctl + kTItem0 + nb);
         if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
-        ncur = ld_acquire_u32(nsz);
       }
       walked = ld_acquire_u32(ctl + kInvCount);
     } else {
@@ -558,6 +634,7 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
     auto invalidate = [&](uint32_t v, unsigned long long *gfr, uint32_t *gsz) {
       a.dist[v] = kInfInf;
       a.inv_list[atomicAdd(ctl + kInvCount, 1u)] = v;
+      if (a.rg.V && a.treseed) push_items(a.rg, v, a.treseed, ctl + kTReseed);
       const uint32_t nb = a.g.boff[v + 1] - a.g.boff[v];
       const uint32_t k = max(1u, (nb + a.chunk - 1) / a.chunk);
       const uint32_t base = atomicAdd(gsz, k);
@@ -633,12 +710,13 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
         atomicAdd(a.pushed, 1ull);
       }
       nearfar = kUseW && a.delta != 0 && a.far0 != nullptr;
-    } else if (hi > 0 && a.rg.V) {
+    } else if (hi > 0 && a.rg.V && a.treseed) {
       // D3 with the reverse graph: pull from each invalidated vertex's in-edges
+      const uint32_t nri = ld_acquire_u32(ctl + kTReseed);
       if (a.rg.weighted)
-        pull_reseed<true, kUseW>(a, L, Q, group, ngroups, hi, round + 1, a.fr0, ctl + kSz0);
+        pull_reseed<true, kUseW>(a, L, Q, group, ngroups, nri, round + 1, a.fr0, ctl + kSz0);
       else
-        pull_reseed<false, kUseW>(a, L, Q, group, ngroups, hi, round + 1, a.fr0, ctl + kSz0);
+        pull_reseed<false, kUseW>(a, L, Q, group, ngroups, nri, round + 1, a.fr0, ctl + kSz0);
     } else if (hi > 0) {
       // D3: re-seed invalidated vertices from valid in-neighbours: one sweep
       // over all buckets (balanced by construction)
@@ -891,9 +969,12 @@ struct mk_traversal {
   unsigned long long *pushed = nullptr;
   uint32_t *far0 = nullptr, *far1 = nullptr, *fbits = nullptr;  // near-far SSSP
   mk_graph *rev = nullptr;  // in-edges of the same graph, for pull levels (BFS)
-  // BFS decremental repair (allocated when a reverse graph is attached)
-  unsigned long long *tseeds = nullptr;
-  uint32_t *tc0 = nullptr, *tc1 = nullptr;
+  // decremental with a reverse graph (allocated when one is attached): the
+  // BFS repair's lists and the re-seed items (TravArgs has the layout)
+  unsigned long long *tseeds = nullptr, *titems0 = nullptr, *titems1 = nullptr;
+  unsigned long long *tchild = nullptr, *treseed = nullptr;
+  uint32_t *tcand0 = nullptr, *tcand1 = nullptr, *tpar = nullptr;
+  size_t rcap = 0;  // re-seed / support item capacity
   std::vector<uint32_t> h_sources;
   // prepared member table (BFS): counter word, uint4 (lo, hi, b0, b1) per
   // small range (largest first), their sources, then the sources whose
@@ -905,6 +986,23 @@ struct mk_traversal {
   PinnedRing staging;  // stream-ordered source uploads
   Timer timer;
 };
+
+// A launch that gave up on a wait leaves its error word set, its stamps
+// and invalidation bits behind and the round counter not advanced, so the
+// next call's stamps could collide with them.  Run before the next launch
+// clears the control words: when the error word holds a timeout, clear the
+// stamps and the bits and restart the round count.
+__global__ void k_trav_recover(uint32_t *ctl, uint32_t *stamp, uint32_t *inval, uint32_t *tpar,
+                               uint32_t V) {
+  if (!(ld_relaxed_u32(ctl + kErr) & kErrTimeout)) return;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, n = gridDim.x * blockDim.x;
+  for (uint32_t v = tid; v < V; v += n) {
+    stamp[v] = 0u;
+    if (tpar) tpar[v] = kEmptyKey;
+  }
+  for (uint32_t w = tid; w < (V + 31) / 32; w += n) inval[w] = 0u;
+  if (tid == 0) ctl[kRound] = 1u;
+}
 
 __global__ void k_set_sources(unsigned long long *dist, const uint32_t *sources, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -983,12 +1081,29 @@ static mk_status trav_create(mk_graph *g, const uint32_t *h_sources, uint32_t ns
 }
 
 // Issues one traversal launch (sources: t's own, or the given device list).
+static void free_repair(mk_traversal *t) {
+  for (unsigned long long **p : {&t->tseeds, &t->titems0, &t->titems1, &t->tchild, &t->treseed}) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  for (uint32_t **p : {&t->tcand0, &t->tcand1, &t->tpar}) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  t->rcap = 0;
+}
+
+static int recover_grid(const mk_graph *g) {
+  return (int)std::min<uint64_t>((uint64_t)g->V / 256 + 1, (uint64_t)device_sm_count(g->device) * 4);
+}
+
 static mk_status trav_issue(mk_traversal *t, uint32_t mode, const uint32_t *bs, const uint32_t *bd,
                             uint32_t n, cudaStream_t s, const uint32_t *srcs, uint32_t nsrc) {
   mk_graph *g = t->g;
   if (mode == kStatic) MK_CUDA(cudaMemsetAsync(t->dist, 0xFF, (size_t)g->V * 8, s));
   const uint32_t delta = (t->sssp && mode != kIncremental && t->far0) ? g->tuning.sssp_delta : 0u;
   if (delta) MK_CUDA(cudaMemsetAsync(t->fbits, 0, ((size_t)g->V + 31) / 32 * 4, s));
+  k_trav_recover<<<recover_grid(g), 256, 0, s>>>(t->ctl, t->stamp, t->inval, t->tpar, g->V);
   // clear everything but the persistent round counter
   MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
   MK_CUDA(cudaMemsetAsync(t->ctl + kTrimN, 0, (kCtlWords - kTrimN) * 4, s));
@@ -1026,8 +1141,13 @@ static mk_status trav_issue(mk_traversal *t, uint32_t mode, const uint32_t *bs, 
   a.limit_ns = g->wait_limit_ns();
   a.trim = (mode == kDecremental && !t->sssp && t->rev && t->tseeds) ? 1u : 0u;
   a.tseeds = t->tseeds;
-  a.tc0 = t->tc0;
-  a.tc1 = t->tc1;
+  a.tcand0 = t->tcand0;
+  a.tcand1 = t->tcand1;
+  a.tpar = t->tpar;
+  a.titems0 = t->titems0;
+  a.titems1 = t->titems1;
+  a.tchild = t->tchild;
+  a.treseed = t->rev ? t->treseed : nullptr;
   const void *fn;
   if (g->weighted)
     fn = t->sssp ? (const void *)k_traverse<true, true> : (const void *)k_traverse<true, false>;
@@ -1131,20 +1251,35 @@ mk_status mk_traversal_set_reverse(mk_traversal *t, mk_graph *g_rev) {
                   "mk_traversal_set_reverse: needs a reverse graph of the same size on the same device");
   }
   DeviceGuard dg(t->g->device);
-  if (g_rev && !t->sssp && !t->tseeds) {
-    // BFS repair lists: a vertex is a seed or a candidate at most once per call
+  if (g_rev) {
+    // Sized once per handle for the largest reverse graph attached.  A vertex
+    // is a seed, a candidate, affected or re-seeded at most once per call, and
+    // pushes at most (its buckets / kRepairChunk + 1) items to a list.
     const size_t V = t->g->V;
-    MK_CUDA(cudaDeviceSynchronize());
-    cudaError_t e = cudaMalloc(&t->tseeds, (V + 16) * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&t->tc0, (V + 16) * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&t->tc1, (V + 16) * 4);
-    if (e != cudaSuccess) {
-      cudaFree(t->tseeds);
-      cudaFree(t->tc0);
-      cudaFree(t->tc1);
-      t->tseeds = nullptr;
-      t->tc0 = t->tc1 = nullptr;
-      return cuda_fail(e, "mk_traversal_set_reverse: repair lists");
+    const size_t rin = (size_t)g_rev->num_buckets / kRepairChunk + V + 64;
+    const size_t fout = (size_t)t->g->num_buckets / kRepairChunk + V + 64;
+    if (t->treseed && rin > t->rcap) {
+      MK_CUDA(cudaDeviceSynchronize());
+      free_repair(t);
+    }
+    if (!t->treseed) {
+      MK_CUDA(cudaDeviceSynchronize());
+      cudaError_t e = cudaMalloc(&t->treseed, rin * 8);
+      if (e == cudaSuccess && !t->sssp) {
+        e = cudaMalloc(&t->tseeds, (V + 16) * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&t->tcand0, (V + 16) * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&t->tcand1, (V + 16) * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&t->tpar, V * 4 + 4);
+        if (e == cudaSuccess) e = cudaMalloc(&t->titems0, rin * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&t->titems1, rin * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&t->tchild, fout * 8);
+        if (e == cudaSuccess) e = cudaMemset(t->tpar, 0xFF, V * 4 + 4);
+      }
+      if (e != cudaSuccess) {
+        free_repair(t);
+        return cuda_fail(e, "mk_traversal_set_reverse: repair lists");
+      }
+      t->rcap = rin;
     }
   }
   t->rev = g_rev;
@@ -1236,6 +1371,7 @@ mk_status mk_bfs_static_members(mk_traversal *t, void *stream, float *ms_out) {
     MK_CHECK(trav_issue(t, kStatic, nullptr, nullptr, 0, s, lsrc, nl));
   } else {
     MK_CUDA(cudaMemsetAsync(t->dist, 0xFF, (size_t)g->V * 8, s));
+    k_trav_recover<<<recover_grid(g), 256, 0, s>>>(t->ctl, t->stamp, t->inval, t->tpar, g->V);
     MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
   }
   if (ns) {
@@ -1339,9 +1475,7 @@ mk_status mk_traversal_destroy(mk_traversal *t) {
   cudaFree(t->ctl);
   cudaFree(t->pushed);
   cudaFree(t->sources);
-  cudaFree(t->tseeds);
-  cudaFree(t->tc0);
-  cudaFree(t->tc1);
+  free_repair(t);
   cudaFree(t->far0);
   cudaFree(t->far1);
   cudaFree(t->fbits);
