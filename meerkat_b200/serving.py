@@ -207,8 +207,10 @@ class GraphServer:
         sizes = np.diff(self.off)
         first = [int(x) for x in self.off[:-1]]
         ranges = [(int(self.off[g]), int(self.off[g + 1])) for g in range(ng)]
-        self.fast = torch.cuda.Stream(self.dev)
-        self.heavy = torch.cuda.Stream(self.dev)
+        # the fast stream has the higher priority: its blocks are scheduled
+        # ahead of a running PageRank or triangle count's
+        self.fast = torch.cuda.Stream(self.dev, priority=-1)
+        self.heavy = torch.cuda.Stream(self.dev, priority=0)
         self.bfs = BFS(self.G, first[:1])
         self.sssp = SSSP(self.G, first[:1])
         self.wcc = WCC(self.G)
