@@ -63,6 +63,7 @@ enum Ctl : int {
   kTItem0 = 25,   // BFS repair: support-search item counts, words 25, 26
   kTChild = 27,   // BFS repair: child-scan items of the level
   kTReseed = 28,  // decremental with a reverse graph: re-seed items
+  kEarly = 29,    // decremental: deleted tree edges counted before an immediate recompute
   kCtlWords = 32
 };
 constexpr uint32_t kRepairChunk = 8;  // buckets per repair / re-seed work item
@@ -640,20 +641,40 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
       const uint32_t base = atomicAdd(gsz, k);
       for (uint32_t j = 0; j < k; ++j) gfr[base + j] = item(v, j);
     };
-    for (uint32_t e = tid; e < a.bn; e += nthreads) {
-      uint32_t s = a.bsrc[e], d = a.bdst[e];
-      if (s == d || s >= a.g.V || d >= a.g.V) continue;
-      unsigned long long pd = ld_dist(a.dist + d);
-      if (pd != kInfInf && !is_source(pd, d) && pack_lo(pd) == s && inval_set(a.inval, d))
-        invalidate(d, a.fr0, ctl + kDSz0);
+    auto tree_edge = [&](uint32_t e, uint32_t &d) {
+      const uint32_t s = a.bsrc[e];
+      d = a.bdst[e];
+      if (s == d || s >= a.g.V || d >= a.g.V) return false;
+      const unsigned long long pd = ld_dist(a.dist + d);
+      return pd != kInfInf && !is_source(pd, d) && pack_lo(pd) == s;
+    };
+    if (a.recompute_inv) {
+      // count the deleted tree edges first: when they alone reach the
+      // recompute threshold, recompute without invalidating anything
+      uint32_t c = 0;
+      for (uint32_t e = tid; e < a.bn; e += nthreads) {
+        uint32_t d;
+        c += tree_edge(e, d) ? 1u : 0u;
+      }
+      c = __reduce_add_sync(0xFFFFFFFFu, c);
+      if ((threadIdx.x & 31u) == 0 && c) atomicAdd(ctl + kEarly, c);
+      if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+      if (ld_acquire_u32(ctl + kEarly) >= a.recompute_inv) restart = true;
     }
-    if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+    if (!restart) {
+      if (tid == 0) ctl[kEarly] = 0u;
+      for (uint32_t e = tid; e < a.bn; e += nthreads) {
+        uint32_t d;
+        if (tree_edge(e, d) && inval_set(a.inval, d)) invalidate(d, a.fr0, ctl + kDSz0);
+      }
+      if (!grid_barrier(ctl + kBar0, err, a.limit_ns)) return;
+    }
     // D2: invalidate whole subtrees along tree edges, level by level.  Sizes
     // rotate over three counters so no block reads a counter that another
     // block is already filling for the next level.
     // The running total of the level sizes (each read after a barrier, the
     // same in every thread) stops the walk early once a recompute is due.
-    for (uint32_t dl = 0;; ++dl) {
+    for (uint32_t dl = 0; !restart; ++dl) {
       const uint32_t n = ld_acquire_u32(ctl + kDSz0 + (dl % 3));
       if (n == 0) break;
       walked += n;
@@ -1456,7 +1477,7 @@ mk_status mk_traversal_decremental_stats(mk_traversal *t, uint64_t *h_invalidate
   MK_CUDA(cudaDeviceSynchronize());
   uint32_t ctl[kCtlWords];
   MK_CUDA(cudaMemcpy(ctl, t->ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
-  if (h_invalidated) *h_invalidated = ctl[kInvCount];
+  if (h_invalidated) *h_invalidated = ctl[kInvCount] + ctl[kEarly];
   if (h_recomputed) *h_recomputed = ctl[kRestart];
   if (ctl[kErr] & kErrTimeout) return fail(MK_ERR_TIMEOUT, "traversal: grid barrier timed out");
   return MK_OK;
