@@ -17,8 +17,8 @@ These fast segments are issued on one CUDA stream without waiting for the
 device; a CUDA event after each segment marks its requests complete.
 PageRank (push form on the member's out-edges, mk_pagerank_range_*) and
 triangle counting (straight from the member's out-edges, mk_tc_range_*) are
-heavy: two worker threads (one per kind) run them on their own streams, so
-they overlap the fast rounds and each other instead of holding them up.
+heavy: a worker thread runs them one at a time on a second stream, so they
+overlap the fast rounds instead of holding them up.
 
 Admission: an insert of m edges needs at most m new slabs, so it waits
 while the slabs in use (read back after every insert segment), plus the
@@ -210,8 +210,7 @@ class GraphServer:
         # the fast stream has the higher priority: its blocks are scheduled
         # ahead of a running PageRank or triangle count's
         self.fast = torch.cuda.Stream(self.dev, priority=-1)
-        self.heavy = torch.cuda.Stream(self.dev, priority=0)     # triangle counts
-        self.heavy_pr = torch.cuda.Stream(self.dev, priority=0)  # PageRank
+        self.heavy = torch.cuda.Stream(self.dev, priority=0)
         self.bfs = BFS(self.G, first[:1])
         self.sssp = SSSP(self.G, first[:1])
         self.wcc = WCC(self.G)
@@ -244,7 +243,7 @@ class GraphServer:
         self.run_heavy(warm, self.heavy)
         if warm.status != "ok":
             raise MemoryError("triangle-count scratch of the largest member exceeds the budget")
-        self.prr.Run(*ranges[big], 0.85, 1e-6, 200, stream=self.heavy_pr, timed=False)
+        self.prr.Run(*ranges[big], 0.85, 1e-6, 200, stream=self.heavy, timed=False)
         torch.cuda.synchronize(self.dev)
 
     def close(self):
@@ -405,12 +404,7 @@ class GraphServer:
         inflight = []             # (event, requests, issue time, inserted edges)
         insert_inflight = 0
         heavy_running = 0
-        # one worker per heavy kind: a PageRank solve waits on the host between
-        # its iterations, so a triangle count fills those gaps (the two use
-        # separate handles; triangle counts share the graph's export scratch
-        # and run one at a time)
-        heavy_qs = {PAGERANK_Q: queue.Queue(), TC_Q: queue.Queue()}
-        heavy_streams = {PAGERANK_Q: self.heavy_pr, TC_Q: self.heavy}
+        heavy_q: "queue.Queue" = queue.Queue()
         heavy_done: "queue.Queue" = queue.Queue()
         base = torch.cuda.Event(enable_timing=True)
         rounds = rejected = 0
@@ -419,23 +413,21 @@ class GraphServer:
         base.synchronize()
         t_base = time.perf_counter() - t0
 
-        def worker(kind):
+        def worker():
             torch.cuda.set_device(self.dev)
-            q, st = heavy_qs[kind], heavy_streams[kind]
             while True:
-                r = q.get()
+                r = heavy_q.get()
                 if r is None:
                     return
                 start = time.perf_counter() - t0
-                self.run_heavy(r, st)
+                self.run_heavy(r, self.heavy)
                 ev = torch.cuda.Event(enable_timing=True)
-                ev.record(st)
+                ev.record(self.heavy)
                 ev.synchronize()
                 heavy_done.put((r, start, t_base + base.elapsed_time(ev) / 1000.0))
 
-        threads = [threading.Thread(target=worker, args=(k,), daemon=True) for k in heavy_qs]
-        for th in threads:
-            th.start()
+        th = threading.Thread(target=worker, daemon=True)
+        th.start()
         i = finished = 0
         try:
             while finished < n:
@@ -493,7 +485,7 @@ class GraphServer:
                     if heavy:
                         heavy_busy.add(r.graph)
                         heavy_running += 1
-                        heavy_qs[r.kind].put(r)
+                        heavy_q.put(r)
                     else:
                         fast_pending[r.graph] += 1
                         if r.kind == INSERT:
@@ -518,9 +510,7 @@ class GraphServer:
                         wait = min(wait, 0.0001)
                     time.sleep(min(max(wait, 0.00002), 0.002))
         finally:
-            for q in heavy_qs.values():
-                q.put(None)
-            for th in threads:
-                th.join()
+            heavy_q.put(None)
+            th.join()
         torch.cuda.synchronize(self.dev)
         return self._summary(reqs, "coalesced", rounds, rejected)
