@@ -391,7 +391,9 @@ __global__ void k_pairs_fill(const uint32_t *__restrict__ src, const uint32_t *_
   bcol[brow[b] + atomicAdd(bfill + b, 1u)] = a;
 }
 
-// Lane-level membership test of (u, v) in the slab graph.
+// Lane-level membership test of (u, v) in the slab graph.  The eight 16-byte
+// loads of a slab are all issued before any is examined, so a probe costs one
+// memory round trip per slab of the chain, not one per load.
 template <bool kW>
 __device__ __forceinline__ bool lane_find(const GraphView &g, uint32_t u, uint32_t v) {
   const uint32_t b0 = g.boff[u];
@@ -399,18 +401,19 @@ __device__ __forceinline__ bool lane_find(const GraphView &g, uint32_t u, uint32
   uint32_t s = b0 + bucket_of(v, nb);
   for (uint32_t it = 0; it < (1u << 24) && s != kNoSlab; ++it) {
     const uint4 *p = g.slabs + 8ull * s;
-    uint4 last;
+    uint4 q[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) q[j] = __ldg(p + j);
+    bool hit = false;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      uint4 q = __ldg(p + j);
-      if (!kW) {
-        if (q.x == v || q.y == v || q.z == v || (j != 7 && q.w == v)) return true;
-      } else {
-        if (q.x == v || (j != 7 && q.z == v)) return true;
-      }
-      last = q;
+      if (!kW)
+        hit |= q[j].x == v || q[j].y == v || q[j].z == v || (j != 7 && q[j].w == v);
+      else
+        hit |= q[j].x == v || (j != 7 && q[j].z == v);
     }
-    s = last.w;
+    if (hit) return true;
+    s = q[7].w;
   }
   return false;
 }
