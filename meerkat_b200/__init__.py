@@ -19,7 +19,7 @@ import numpy as np
 from ._lib import (DEVERR_INVALID_ID, DEVERR_OOM, DEVERR_OVERFLOW, DEVERR_TIMEOUT, MK_INF,
                    GraphDesc, GraphInfo, MeerkatError, Tuning, check, lib)
 
-__all__ = ["DynamicGraph", "GraphSet", "BFS", "SSSP", "PageRank", "PageRankRange", "TC", "TCRange",
+__all__ = ["DynamicGraph", "GraphSet", "SetRunner", "BFS", "SSSP", "PageRank", "PageRankRange", "TC", "TCRange",
            "WCC",
            "EdgeSet",
            "gen_rmat", "gen_grid", "gen_rmat_members", "read_edge_list", "read_batch",
@@ -293,7 +293,21 @@ class _Traversal(_Timed):
                                        len(self.sources), C.byref(h)), name)
         self._h = h
 
+    @classmethod
+    def _borrow(cls, handle, G: DynamicGraph, sources, owner):
+        """View of a traversal handle owned by another object (a SetRunner)."""
+        t = cls.__new__(cls)
+        t.G = G
+        t.sources = np.ascontiguousarray(np.asarray(sources, dtype=np.uint32))
+        t.source = t.sources
+        t._h = handle
+        t._owner = owner
+        return t
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             lib().mk_traversal_destroy(self._h)
             self._h = None
@@ -571,7 +585,19 @@ class WCC(_Timed):
         check(lib().mk_wcc_create(G.handle, C.byref(h)), "mk_wcc_create")
         self._h = h
 
+    @classmethod
+    def _borrow(cls, handle, G: DynamicGraph, owner):
+        """View of a WCC handle owned by another object (a SetRunner)."""
+        w = cls.__new__(cls)
+        w.G = G
+        w._h = handle
+        w._owner = owner
+        return w
+
     def close(self):
+        if getattr(self, "_owner", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             lib().mk_wcc_destroy(self._h)
             self._h = None
@@ -744,6 +770,68 @@ class GraphSet:
                                        dd.data_ptr(), is_.data_ptr(), id_.data_ptr(), _ptr(iw),
                                        _stream(stream)), "mk_gen_set_batches")
         return ds[:nd], dd[:nd], is_[:ni], id_[:ni], (iw[:ni] if iw is not None else None)
+
+
+class SetRunner:
+    """One query per member of a GraphSet (QUERY_BFS from a local source,
+    QUERY_WCC, or QUERY_NONE) and a step that applies one update batch to
+    every member and answers every query (mk_set_runner_*).  The step is four
+    launches, or ONE with fused=True (members of at most 65,535 vertices;
+    batches grouped by member in member order, as GraphSet.gen_batches
+    writes them).  `bfs` / `wcc` are views of the runner's own handles for
+    reading the answers."""
+
+    def __init__(self, gs: "GraphSet", query, sources_local=None, fused: bool = False):
+        q = np.ascontiguousarray(np.asarray(query, dtype=np.uint8))
+        if len(q) != gs.num_graphs:
+            raise ValueError("one query kind per member")
+        src = (np.zeros(gs.num_graphs, dtype=np.uint32) if sources_local is None
+               else np.ascontiguousarray(np.asarray(sources_local, dtype=np.uint32)))
+        if len(src) != gs.num_graphs:
+            raise ValueError("one (local) source entry per member")
+        self.gs = gs
+        h = C.c_void_p()
+        check(lib().mk_set_runner_create(gs._h, q.ctypes.data, src.ctypes.data, C.byref(h)),
+              "mk_set_runner_create")
+        self._h = h
+        bh, wh = C.c_void_p(), C.c_void_p()
+        check(lib().mk_set_runner_handles(h, C.byref(bh), C.byref(wh)), "mk_set_runner_handles")
+        bfs_m = np.flatnonzero(q == 0)
+        glob = gs.offsets[bfs_m].astype(np.uint64) + src[bfs_m]
+        self.bfs = BFS._borrow(bh, gs.graph, glob, self) if bh.value else None
+        self.wcc = WCC._borrow(wh, gs.graph, self) if wh.value else None
+        self.fused = False
+        if fused:
+            self.set_fused(True)
+
+    def set_fused(self, on: bool) -> None:
+        check(lib().mk_set_runner_set_fused(self._h, int(bool(on))), "mk_set_runner_set_fused")
+        self.fused = bool(on)
+
+    def launches_per_step(self) -> int:
+        n = C.c_uint32(0)
+        check(lib().mk_set_runner_launches(self._h, C.byref(n)), "mk_set_runner_launches")
+        return int(n.value)
+
+    def step(self, del_src, del_dst, ins_src, ins_dst, ins_w=None, stream=None) -> None:
+        check(lib().mk_set_runner_step(self._h, _ptr(del_src), _ptr(del_dst), _count(del_src, None),
+                                       _ptr(ins_src), _ptr(ins_dst), _ptr(ins_w),
+                                       _count(ins_src, None), _stream(stream)),
+              "mk_set_runner_step")
+
+    def close(self):
+        for v in (getattr(self, "bfs", None), getattr(self, "wcc", None)):
+            if v is not None:
+                v.close()
+        if getattr(self, "_h", None):
+            lib().mk_set_runner_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def gen_rmat_members(vertex_offsets, edges_per_graph, a=0.57, b=0.19, c=0.19, seed=0, w_lo=1,

@@ -37,6 +37,7 @@
 
 #include "mk_internal.h"
 #include "mk_slab.cuh"
+#include "mk_members.cuh"
 
 namespace mk {
 
@@ -847,48 +848,12 @@ __global__ void __launch_bounds__(kTravBlock) k_traverse(TravArgs a) {
 
 
 // ---- static BFS of ranges held in shared memory ----
-// One CTA per range (a member of a graph set that holds one source): the
-// member's BFS state lives in shared memory -- a 16-bit parent per vertex
-// (0xFFFF: not reached) and a visited bitmap -- and its levels are separated
-// by block barriers instead of grid barriers.  A level's frontier is a list
-// of work items (vertex, chunk of buckets) in the range's slice of a device
-// array, so a hub's buckets spread over many 8-lane groups.  A newly reached
-// vertex keeps the smallest-id frontier vertex with an edge to it as its
-// parent (a 16-bit CAS minimum).  Distances equal the device-wide kernel's;
-// parents form a valid BFS tree, as there, where (as in the reference,
-// BFSImpl.cuh:311-314) the first of several equal-distance parents stays.
-// After each level the newly reached vertices get their packed word in
-// device memory, their visited bit and their work items.
-constexpr uint32_t kMemLocalMax = 65535;  // 0xFFFF marks "not reached"
-constexpr int kMemThreads = 1024;
-constexpr uint32_t kMemChunk = 4;  // buckets per work item (head slabs loaded together)
-
-// Buckets per work item of a vertex with nb buckets: the chunk index must fit
-// 16 bits.
-__device__ __forceinline__ uint32_t mem_chunk(uint32_t nb) {
-  return nb > 65536u * kMemChunk ? (nb + 65535u) / 65536u : kMemChunk;
-}
-
-// Lowers *p to v if v is smaller; true if this call replaced 0xFFFF.  Every
-// failed CAS means another thread lowered *p, so the loop ends within 65,536
-// rounds.
-__device__ __forceinline__ bool cas_min16_first(uint16_t *p, uint32_t v) {
-  volatile unsigned short *vp = p;
-  unsigned short cur = *vp;
-  for (uint32_t it = 0; it <= 65536u; ++it) {
-    if (v >= cur) return false;
-    const unsigned short prev =
-        atomicCAS(reinterpret_cast<unsigned short *>(p), cur, (unsigned short)v);
-    if (prev == cur) return cur == 0xFFFFu;
-    cur = prev;
-  }
-  return false;
-}
-
-// rng[r] = (first vertex, end vertex, first bucket, end bucket) of a range of
-// at most kMemLocalMax vertices, src[r] its source (global id).  items holds
-// one word per bucket of the graph, found one per vertex; range r uses their
-// slices [b0, b1) and [lo, hi).  dist must already hold INFINF.
+// One CTA per range (a member of a graph set that holds one source), the
+// member's state in shared memory (bfs_member).  CTAs take ranges from a
+// counter, largest first.  rng[r] = (first vertex, end vertex, first bucket,
+// end bucket) of a range of at most kMemLocalMax vertices, src[r] its source
+// (global id).  items holds one word per bucket of the graph, found one per
+// vertex.  dist must already hold INFINF.
 template <bool kW>
 __global__ void __launch_bounds__(kMemThreads, 1)
     k_bfs_members(GraphView g, const uint4 *__restrict__ rng, const uint32_t *__restrict__ src,
@@ -897,75 +862,12 @@ __global__ void __launch_bounds__(kMemThreads, 1)
   extern __shared__ uint32_t smem[];
   __shared__ uint32_t s_range, s_nfound, s_nitems;
   const Lanes L = lanes();
-  const uint32_t group = threadIdx.x >> 3, ngroups = blockDim.x >> 3;
   for (;;) {
     if (threadIdx.x == 0) s_range = atomicAdd(counter, 1u);
     __syncthreads();
     const uint32_t r = s_range;
     if (r >= nr) break;
-    const uint4 R = rng[r];
-    const uint32_t lo = R.x, n = R.y - R.x, s0 = src[r] - lo;
-    const uint32_t nw = (n + 31) >> 5;
-    uint32_t *vis = smem;
-    uint16_t *par = reinterpret_cast<uint16_t *>(smem + nw);
-    uint32_t *q = items + R.z;  // capacity R.w - R.z: a vertex's items never exceed its buckets
-    uint32_t *fl = found + lo;  // capacity n: a vertex is reached once
-    for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x) vis[i] = 0u;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) par[i] = 0xFFFFu;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      par[s0] = (uint16_t)s0;
-      fl[0] = s0;
-      s_nfound = 1;
-      s_nitems = 0;
-    }
-    __syncthreads();
-    uint32_t fbeg = 0, ibeg = 0;
-    for (uint32_t level = 0; level <= n; ++level) {
-      // vertices reached at `level`: packed word, visited bit, work items
-      const uint32_t fend = s_nfound;
-      for (uint32_t i = fbeg + threadIdx.x; i < fend; i += blockDim.x) {
-        const uint32_t v = fl[i], gv = lo + v;
-        dist[gv] = pack(level, lo + par[v]);
-        atomicOr(vis + (v >> 5), 1u << (v & 31));
-        if (g.deg[gv] == 0) continue;
-        const uint32_t nb = g.boff[gv + 1] - g.boff[gv];
-        const uint32_t cs = mem_chunk(nb), nc = (nb + cs - 1) / cs;
-        const uint32_t pos = atomicAdd(&s_nitems, nc);
-        for (uint32_t c = 0; c < nc; ++c) q[pos + c] = v | (c << 16);
-      }
-      __syncthreads();
-      const uint32_t iend = s_nitems;
-      if (iend == ibeg) break;
-      // expand the items of `level`
-      for (uint32_t it = ibeg + group; it < iend; it += ngroups) {
-        const uint32_t item = q[it];
-        const uint32_t u = item & 0xFFFFu, gu = lo + u;
-        const uint32_t ub0 = g.boff[gu], nb = g.boff[gu + 1] - ub0, cs = mem_chunk(nb);
-        const uint32_t bb = ub0 + (item >> 16) * cs, be = min(bb + cs, ub0 + nb);
-        auto relax = [&](const uint4 x) {
-          uint32_t k[4], w[4];
-          lane_keys<kW>(x, L.gl, k, w);
-#pragma unroll
-          for (int t = 0; t < keys_per_lane<kW>(); ++t) {
-            if (k[t] >= kTombKey) continue;
-            const uint32_t v = k[t] - lo;
-            if (v >= n) {
-              atomicOr(err, kErrInvalidId);
-              continue;
-            }
-            if ((vis[v >> 5] >> (v & 31)) & 1u) continue;
-            if (cas_min16_first(par + v, u)) fl[atomicAdd(&s_nfound, 1u)] = v;
-          }
-        };
-        for (uint32_t b = bb; b < be; b += kMemChunk)
-          walk4_levels(g, L, b, min(kMemChunk, be - b), [&](uint32_t, const uint4 x) { relax(x); });
-      }
-      fbeg = fend;
-      ibeg = iend;
-      __syncthreads();
-    }
-    __syncthreads();  // shared memory and s_range are reused by the next range
+    bfs_member<kW, false>(g, L, rng[r], src[r], dist, items, found, err, smem, s_nfound, s_nitems);
   }
 }
 
@@ -1198,6 +1100,16 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   return MK_OK;
 }
 
+namespace mk {
+mk_status trav_member_bufs(mk_traversal *t, TravMemberBufs *out) {
+  if (!t || !out) return fail(MK_ERR_INVALID, "trav_member_bufs: null argument");
+  out->dist = t->dist;
+  out->items = reinterpret_cast<uint32_t *>(t->fr0);
+  out->found = t->inv_list;
+  return MK_OK;
+}
+}  // namespace mk
+
 extern "C" {
 
 mk_status mk_bfs_create(mk_graph *g, uint32_t source, mk_traversal **out) {
@@ -1363,9 +1275,9 @@ mk_status mk_bfs_prepare_members(mk_traversal *t, const uint32_t *h_vertex_range
   t->small_max = ns ? len(small_ids[0]) : 0;
   t->small_grid = 0;
   if (ns) {
-    const size_t smem = (((size_t)t->small_max + 31) / 32) * 4 + (((size_t)t->small_max * 2 + 15) & ~(size_t)15);
+    const size_t smem = bfs_member_smem(t->small_max);
     auto kern = g->weighted ? k_bfs_members<true> : k_bfs_members<false>;
-    const int most = (int)((kMemLocalMax + 31) / 32 * 4 + ((kMemLocalMax * 2 + 15) & ~15u));
+    const int most = (int)bfs_member_smem(kMemLocalMax);
     MK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
     int per_sm = 0;
     MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMemThreads, smem));
@@ -1396,7 +1308,7 @@ mk_status mk_bfs_static_members(mk_traversal *t, void *stream, float *ms_out) {
     MK_CUDA(cudaMemsetAsync(t->ctl, 0, kRound * 4, s));
   }
   if (ns) {
-    const size_t smem = (((size_t)t->small_max + 31) / 32) * 4 + (((size_t)t->small_max * 2 + 15) & ~(size_t)15);
+    const size_t smem = bfs_member_smem(t->small_max);
     MK_CUDA(cudaMemsetAsync(counter, 0, 4, s));
     uint32_t *items = reinterpret_cast<uint32_t *>(t->fr0);
     if (g->weighted)

@@ -24,10 +24,9 @@
 
 #include "mk_internal.h"
 #include "mk_slab.cuh"
+#include "mk_members.cuh"
 
 namespace mk {
-
-constexpr uint32_t kUfLimit = 1u << 26;
 
 // find with path halving; parent words are read through L2 because other
 // SMs hook and halve concurrently.
@@ -225,95 +224,23 @@ __global__ void k_uf_compress_ranges(uint32_t *p, const uint32_t *vpre, const ui
 }
 
 // ---- ranges held in shared memory ----
-// A range of at most kLocalMax vertices (a member of a graph set) is solved
-// by one CTA: its parent array lives in shared memory as 16-bit local ids, so
-// every find, halving store and hooking CAS stays on chip, and device memory
-// sees one pass over the range's slabs and one write of its labels.  CTAs
-// take ranges from a counter, largest first.  The union rule is the one of
-// the global kernels (larger root under smaller), so labels are again the
-// minimum vertex id of each component.
-constexpr uint32_t kLocalMax = 1u << 16;
-constexpr int kMemberThreads = 1024;
-constexpr uint32_t kMemberHeads = 4;  // head slabs a group loads together
-
-__device__ __forceinline__ uint32_t ls_find(uint16_t *p, uint32_t x) {
-  volatile uint16_t *vp = p;
-  for (uint32_t it = 0; it < kUfLimit; ++it) {
-    const uint32_t px = vp[x];
-    if (px == x) return x;
-    const uint32_t gx = vp[px];
-    if (px != gx) vp[x] = (uint16_t)gx;  // x is not a root: only halving writes it
-    x = gx;
-  }
-  return x;
-}
-
-__device__ __forceinline__ uint32_t ls_root(const uint16_t *p, uint32_t x) {
-  const volatile uint16_t *vp = p;
-  for (uint32_t it = 0; it < kUfLimit; ++it) {
-    const uint32_t px = vp[x];
-    if (px == x) return x;
-    x = px;
-  }
-  return x;
-}
-
-__device__ __forceinline__ void ls_union(uint16_t *p, uint32_t a, uint32_t b, uint32_t *err) {
-  for (uint32_t it = 0; it < kUfLimit; ++it) {
-    const uint32_t ra = ls_find(p, a), rb = ls_find(p, b);
-    if (ra == rb) return;
-    const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
-    if (atomicCAS(reinterpret_cast<unsigned short *>(p + hi), (unsigned short)hi,
-                  (unsigned short)lo) == (unsigned short)hi)
-      return;
-  }
-  atomicOr(err, kErrTimeout);
-}
-
-// rng[r] = (first vertex, end vertex, first bucket, end bucket), at most
-// kLocalMax vertices each.  A key outside its range (a range that is not
-// closed under edges) is skipped and reported as MK_DEVERR_INVALID_ID.
+// A range of at most kUfLocalMax vertices (a member of a graph set) is solved
+// by one CTA with its union-find in shared memory (uf_member).  CTAs take
+// ranges from a counter, largest first.  rng[r] = (first vertex, end vertex,
+// first bucket, end bucket).
 template <bool kW>
-__global__ void __launch_bounds__(kMemberThreads, 1)
+__global__ void __launch_bounds__(kMemThreads, 1)
     k_uf_members(GraphView g, const uint4 *__restrict__ rng, uint32_t nr, uint32_t *counter,
                  uint32_t *__restrict__ labels, uint32_t *err) {
   extern __shared__ uint16_t sp[];
   __shared__ uint32_t s_range;
   const Lanes L = lanes();
-  const uint32_t group = threadIdx.x >> 3, ngroups = blockDim.x >> 3;
   for (;;) {
     if (threadIdx.x == 0) s_range = atomicAdd(counter, 1u);
     __syncthreads();
     const uint32_t r = s_range;
     if (r >= nr) break;
-    const uint4 R = rng[r];
-    const uint32_t lo = R.x, n = R.y - R.x;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sp[i] = (uint16_t)i;
-    __syncthreads();
-    for (uint32_t b = R.z + group * kMemberHeads; b < R.w; b += ngroups * kMemberHeads) {
-      const uint32_t m = min(kMemberHeads, R.w - b);
-      uint32_t own[kMemberHeads];
-#pragma unroll
-      for (uint32_t j = 0; j < kMemberHeads; ++j) own[j] = j < m ? __ldg(g.bowner + b + j) - lo : 0u;
-      walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 x) {
-        const uint32_t u = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
-        uint32_t k[4], w[4];
-        lane_keys<kW>(x, L.gl, k, w);
-#pragma unroll
-        for (int t = 0; t < keys_per_lane<kW>(); ++t) {
-          if (k[t] >= kTombKey) continue;
-          const uint32_t v = k[t] - lo;
-          if (v >= n || u >= n) {
-            atomicOr(err, kErrInvalidId);
-            continue;
-          }
-          if (v != u) ls_union(sp, u, v, err);
-        }
-      });
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) labels[lo + i] = lo + ls_root(sp, i);
-    __syncthreads();  // sp and s_range are reused by the next range
+    uf_member<kW, false>(g, L, rng[r], labels, err, sp);
   }
 }
 
@@ -376,6 +303,10 @@ static bool batch_matches(const mk_graph *g, const uint32_t *d_src, const uint32
   return n == g->last_n && d_src == g->last_src && d_dst == g->last_dst && g->last_op == op;
 }
 
+namespace mk {
+uint32_t *wcc_label_buf(mk_wcc *w) { return w ? w->parent : nullptr; }
+}  // namespace mk
+
 extern "C" {
 
 mk_status mk_wcc_create(mk_graph *g, mk_wcc **out) {
@@ -433,7 +364,7 @@ static mk_status wcc_prepare(mk_wcc *w, const uint32_t *h_vertex_ranges, uint32_
   for (uint32_t r = 0; r < nranges; ++r) {
     const uint32_t b = h_vertex_ranges[2 * r], e = h_vertex_ranges[2 * r + 1];
     if (b >= e || e > g->V) return fail(MK_ERR_INVALID, "mk_wcc_prepare_ranges: bad vertex range");
-    (e - b <= kLocalMax ? small_ids : large_ids).push_back(r);
+    (e - b <= kUfLocalMax ? small_ids : large_ids).push_back(r);
   }
   auto len = [&](uint32_t r) { return h_vertex_ranges[2 * r + 1] - h_vertex_ranges[2 * r]; };
   std::stable_sort(small_ids.begin(), small_ids.end(),
@@ -480,11 +411,11 @@ static mk_status wcc_prepare(mk_wcc *w, const uint32_t *h_vertex_ranges, uint32_
   w->large_bt = bt;
   w->small_grid = 0;
   if (ns) {
-    const size_t smem = ((size_t)w->small_max * 2 + 15) & ~(size_t)15;
+    const size_t smem = uf_member_smem(w->small_max);
     auto kern = g->weighted ? k_uf_members<true> : k_uf_members<false>;
-    MK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kLocalMax * 2)));
+    MK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)uf_member_smem(kUfLocalMax)));
     int per_sm = 0;
-    MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMemberThreads, smem));
+    MK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMemThreads, smem));
     w->small_grid = (int)std::min<uint64_t>(ns, (uint64_t)device_sm_count(g->device) * std::max(per_sm, 1));
   }
   w->prepared = true;
@@ -515,13 +446,13 @@ mk_status mk_wcc_static_prepared(mk_wcc *w, void *stream, float *ms_out) {
   uint32_t *counter = w->ranges.ptr;
   const uint32_t ns = w->n_small, nl = w->n_large;
   if (ns) {
-    const size_t smem = ((size_t)w->small_max * 2 + 15) & ~(size_t)15;
+    const size_t smem = uf_member_smem(w->small_max);
     const uint4 *rng = reinterpret_cast<const uint4 *>(w->ranges.ptr + 4);
     MK_CUDA(cudaMemsetAsync(counter, 0, 4, s));
     if (g->weighted)
-      k_uf_members<true><<<w->small_grid, kMemberThreads, smem, s>>>(v, rng, ns, counter, w->parent, w->err);
+      k_uf_members<true><<<w->small_grid, kMemThreads, smem, s>>>(v, rng, ns, counter, w->parent, w->err);
     else
-      k_uf_members<false><<<w->small_grid, kMemberThreads, smem, s>>>(v, rng, ns, counter, w->parent, w->err);
+      k_uf_members<false><<<w->small_grid, kMemThreads, smem, s>>>(v, rng, ns, counter, w->parent, w->err);
   }
   if (nl) {
     const uint32_t *dv = w->ranges.ptr + 4 + 4 * (size_t)ns, *dvb = dv + nl + 1;

@@ -8,7 +8,7 @@ from meerkat_b200 import batched as B
 from oracle import OracleGraph
 
 
-def build(spec, dev):
+def build(spec, dev, weighted=True):
     import torch
     voff = B._offsets(spec.num_vertices)
     eoff = B._offsets(spec.num_edges)
@@ -17,8 +17,8 @@ def build(spec, dev):
     hints = torch.bincount(src.long(), minlength=V).to(torch.int32).cpu().numpy().view(np.uint32)
     gs = mk.GraphSet(spec.num_vertices, degree_hints=[hints[voff[m]:voff[m + 1]]
                                                       for m in range(spec.num_graphs)],
-                     weighted=True)
-    gs.graph.InsertEdges(src, dst, vals=w)
+                     weighted=weighted)
+    gs.graph.InsertEdges(src, dst, vals=w if weighted else None)
     assert gs.graph.sync() == 0
     s_h = src.cpu().numpy().view(np.uint32).astype(np.int64)
     d_h = dst.cpu().numpy().view(np.uint32).astype(np.int64)
@@ -69,34 +69,115 @@ def test_batched_runner_matches_plain_and_oracle(capture):
             del g
         else:
             br.step(batch)
-        # the same batch per member with local ids, for the plain graphs and the oracle
-        h = [x.cpu().numpy().view(np.uint32).astype(np.int64) for x in batch]
-        do, io = B._offsets(spec.deletes), B._offsets(spec.inserts)
-        slices = []
-        for m in range(Gn):
-            base = int(voff[m])
-            a = slice(do[m], do[m + 1])
-            b = slice(io[m], io[m + 1])
-            loc = [(h[0][a] - base), (h[1][a] - base), (h[2][b] - base), (h[3][b] - base)]
-            loc = [x.astype(np.uint32) for x in loc] + [h[4][b].astype(np.uint32)]
-            oracles[m].delete(loc[0], loc[1])
-            oracles[m].insert(loc[2], loc[3], loc[4])
-            slices.append(tuple(torch.from_numpy(x.view(np.int32)).cuda() for x in loc))
+        check_step(spec, batch, voff, oracles, gs, br, src_of, pr, plain)
+
+
+def check_step(spec, batch, voff, oracles, gs, br, src_of, pr=None, plain=()):
+    """Applies one set batch to the oracles (and, when given, the plain
+    per-graph runner with local ids), then compares every member's answer,
+    and the set's degrees, with the oracle's."""
+    import torch
+    Gn = spec.num_graphs
+    h = [x.cpu().numpy().view(np.uint32).astype(np.int64) for x in batch[:4]]
+    h.append(batch[4].cpu().numpy().view(np.uint32).astype(np.int64) if batch[4] is not None
+             else np.ones(len(h[2]), dtype=np.int64))
+    do, io = B._offsets(spec.deletes), B._offsets(spec.inserts)
+    slices = []
+    for m in range(Gn):
+        base = int(voff[m])
+        a = slice(do[m], do[m + 1])
+        b = slice(io[m], io[m + 1])
+        loc = [(h[0][a] - base), (h[1][a] - base), (h[2][b] - base), (h[3][b] - base)]
+        loc = [x.astype(np.uint32) for x in loc] + [h[4][b].astype(np.uint32)]
+        oracles[m].delete(loc[0], loc[1])
+        oracles[m].insert(loc[2], loc[3], loc[4])
+        slices.append(tuple(torch.from_numpy(x.view(np.int32)).cuda() for x in loc))
+    if pr is not None:
         pr.step(slices)
-        torch.cuda.synchronize()
-        assert gs.graph.sync() == 0 and all(g.sync() == 0 for g in plain)
-        d_union = br.bfs.Distances()
-        l_union = br.wcc.Labels().astype(np.int64)
-        for m in range(Gn):
-            lo, hi = int(voff[m]), int(voff[m + 1])
-            if spec.query[m] == B.QUERY_BFS:
-                want = oracles[m].bfs(src_of[m])
-                np.testing.assert_array_equal(d_union[lo:hi], want)
+    torch.cuda.synchronize()
+    assert gs.graph.sync() == 0 and all(g.sync() == 0 for g in plain)
+    d_union = br.bfs.Distances()
+    l_union = br.wcc.Labels().astype(np.int64)
+    deg = gs.graph.degrees()
+    for m in range(Gn):
+        lo, hi = int(voff[m]), int(voff[m + 1])
+        np.testing.assert_array_equal(deg[lo:hi], oracles[m].degrees())
+        if spec.query[m] == B.QUERY_BFS:
+            want = oracles[m].bfs(src_of[m])
+            np.testing.assert_array_equal(d_union[lo:hi], want)
+            if pr is not None:
                 np.testing.assert_array_equal(pr.algos[m].Distances(), want)
-            else:
-                want = oracles[m].wcc()
-                np.testing.assert_array_equal(l_union[lo:hi] - lo, want)
+        else:
+            want = oracles[m].wcc()
+            np.testing.assert_array_equal(l_union[lo:hi] - lo, want)
+            if pr is not None:
                 np.testing.assert_array_equal(pr.algos[m].Labels(), want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("capture,weighted", [(False, True), (True, True), (False, False)])
+def test_fused_step_matches_oracle(capture, weighted):
+    """The one-launch step (each member's deletes, inserts and query by one
+    CTA): every member's answer and degrees equal the oracle's after each
+    step, issued directly or captured into a CUDA graph, and the applied
+    insert count is published as after the four-launch step."""
+    import torch
+    spec = B.make_spec(48, seed=12, v_lo=32, v_hi=700, deg_lo=2, deg_hi=12, upd_lo=0.05,
+                       upd_hi=0.3)
+    gs, _, oracles, voff = build(spec, "cuda:0", weighted=weighted)
+    bfs_members = np.flatnonzero(spec.query == B.QUERY_BFS)
+    srcs = B.pick_sources(gs.graph.degrees(), voff, bfs_members, seed=4)
+    br = B.BatchedRunner(gs, spec.query, srcs, fused=True)
+    assert br.fusable and br.launches_per_step() == 1
+    gs.graph.reserve_batch(int(spec.inserts.sum()))
+    src_of = dict(zip(bfs_members.tolist(), srcs.tolist()))
+    for step in range(3):
+        batch = gs.gen_batches(spec.deletes, spec.inserts, seed=200 + step, weights=weighted)
+        edges_before = sum(O.num_edges() for O in oracles)
+        if capture:
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                br.step(batch, stream=s)
+            with torch.cuda.stream(s):
+                g.replay()
+            torch.cuda.synchronize()
+            del g
+        else:
+            br.step(batch)
+        torch.cuda.synchronize()
+        deleted = int(spec.deletes.sum())
+        check_step(spec, batch, voff, oracles, gs, br, src_of)
+        edges_after = sum(O.num_edges() for O in oracles)
+        # inserts applied = growth + deletes applied; deletes of live edges
+        # are all applied unless a member's batch names one edge twice
+        assert gs.graph.last_applied() <= int(spec.inserts.sum())
+        assert gs.graph.last_applied() >= edges_after - edges_before
+    br.close()
+    gs.close()
+
+
+@pytest.mark.gpu
+def test_fused_step_reports_a_batch_not_grouped_by_member():
+    """An insert batch in shuffled order: the fused step skips the edges
+    outside their member's slice and reports MK_DEVERR_INVALID_ID; every
+    access stays inside the batch and the member's ranges."""
+    import torch
+    spec = B.make_spec(16, seed=13, v_lo=64, v_hi=300, deg_lo=2, deg_hi=8, upd_lo=0.1,
+                       upd_hi=0.2)
+    gs, _, _, voff = build(spec, "cuda:0")
+    bfs_members = np.flatnonzero(spec.query == B.QUERY_BFS)
+    srcs = B.pick_sources(gs.graph.degrees(), voff, bfs_members, seed=5)
+    br = B.BatchedRunner(gs, spec.query, srcs, fused=True)
+    ds, dd, is_, id_, iw = gs.gen_batches(spec.deletes, spec.inserts, seed=300)
+    perm = torch.randperm(is_.numel(), generator=torch.Generator().manual_seed(1)).cuda()
+    br.step((ds, dd, is_[perm].contiguous(), id_[perm].contiguous(), iw[perm].contiguous()))
+    torch.cuda.synchronize()
+    with pytest.raises(mk.MeerkatError, match="not grouped by member"):
+        gs.graph.sync()
+    br.close()
+    gs.close()
 
 
 def test_spec_is_seeded_and_in_range():
