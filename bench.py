@@ -423,21 +423,31 @@ def more_queries(mk, G, V, dev, seed):
     rows = torch.repeat_interleave(torch.arange(V, device=dev, dtype=torch.int32), rp[1:] - rp[:-1])
     pick = torch.randint(0, E, (100_000,), generator=g, device=dev)
     bs, bd = rows[pick].contiguous(), col[pick].contiguous()
-    # WCC on the graph itself
+    # a reverse copy of the same edges (in-edges): decremental WCC rescans
+    # split-off pieces through it; PageRank and pull BFS read it below
+    indeg = torch.bincount(col.long(), minlength=V).to(torch.int32).cpu().numpy().view(np.uint32)
+    Gr = mk.DynamicGraph(V, degree_hints=indeg, reverse=True, device=dev.index or 0)
+    Gr.InsertEdges(rows, col)
+    # WCC on the graph itself; the decremental call repairs along the
+    # spanning forest with the reverse copy attached (both graphs get the
+    # batch first, as a caller keeping them in step would)
     wcc = mk.WCC(G)
+    wcc.set_reverse(Gr)
     t = wcc.Static()
     out["wcc"] = {"static_ms": t, "static_gbs": (8 * E + 8 * V) / (t / 1e3) / 1e9}
     G.DeleteEdges(bs, bd)
+    Gr.DeleteEdges(bs, bd)
     out["wcc"]["dec_ms"] = wcc.Decremental(bs, bd)
+    dead, rescanned, path = wcc.decremental_stats()
+    out["wcc"]["dec_repair"] = {"forest_edges_lost": dead, "vertices_rescanned": rescanned,
+                                "path": ["unchanged", "piece rescan", "component rebuild",
+                                         "static"][path]}
     G.InsertEdges(bs, bd)  # weight 0 on the re-inserted copies
+    Gr.InsertEdges(bs, bd)
     out["wcc"]["inc_ms"] = wcc.Incremental(bs, bd)
     finals["wcc"] = wcc.Labels()
     finals["batch"] = (bs.cpu().numpy().view(np.uint32).copy(), bd.cpu().numpy().view(np.uint32).copy())
     wcc.close()
-    # PageRank on a reverse copy
-    indeg = torch.bincount(col.long(), minlength=V).to(torch.int32).cpu().numpy().view(np.uint32)
-    Gr = mk.DynamicGraph(V, degree_hints=indeg, reverse=True, device=dev.index or 0)
-    Gr.InsertEdges(rows, col)
     # direction-optimizing static BFS: the reverse copy lets large levels pull
     from meerkat_b200.autotune import tune_bfs_pull
     src_bfs = int(torch.argmax(rp[1:] - rp[:-1]))
@@ -1077,7 +1087,7 @@ def grid_stress(side, nbatch, batch, rank, world, local):
     rng = np.random.default_rng(SEED + 22 + rank)
     rec = {k: [] for k in ("update_ms", "bfs_ms", "sssp_ms", "wcc_ms")}
     dec, inc = {k: [] for k in rec}, {k: [] for k in rec}
-    repair = {"bfs": [], "sssp": []}
+    repair = {"bfs": [], "sssp": [], "wcc": []}
     history = []  # host copies of every batch, for the oracle replay
     INFINF = np.uint64(2**64 - 1)
     for b in range(nbatch):
@@ -1101,6 +1111,7 @@ def grid_stress(side, nbatch, batch, rank, world, local):
         dec["wcc_ms"].append(wcc.Decremental(tds, tdd))
         repair["bfs"].append(bfs.decremental_stats())
         repair["sssp"].append(sssp.decremental_stats())
+        repair["wcc"].append(wcc.decremental_stats())
         history.append(("del", ds, dd, None))
     for b in range(nbatch):
         u = rng.integers(0, V, batch)
@@ -1160,10 +1171,14 @@ def grid_stress(side, nbatch, batch, rank, world, local):
            "batches": nbatch, "batch": batch, "source": src, "static": static,
            "decremental_p50_ms": {k: p50(v) for k, v in dec.items()},
            "incremental_p50_ms": {k: p50(v) for k, v in inc.items()},
-           "decremental_repair": {k: {"invalidated": [int(x) for x, _ in v],
-                                      "recomputed": [bool(r) for _, r in v],
-                                      "ms": [round(x, 3) for x in dec[k + "_ms"]]}
-                                  for k, v in repair.items()},
+           "decremental_repair": {
+               **{k: {"invalidated": [int(x) for x, _ in repair[k]],
+                      "recomputed": [bool(r) for _, r in repair[k]],
+                      "ms": [round(x, 3) for x in dec[k + "_ms"]]} for k in ("bfs", "sssp")},
+               "wcc": {"forest_edges_lost": [int(x) for x, _, _ in repair["wcc"]],
+                       "path": [["unchanged", "piece rescan", "component rebuild", "static"][p]
+                                for _, _, p in repair["wcc"]],
+                       "ms": [round(x, 3) for x in dec["wcc_ms"]]}},
            "recompute_rule": "a decremental call recomputes from the source once its "
                              "invalidation walk passes recompute_permille of the vertices",
            "components_after": comps, "matches_static_recompute": same}
@@ -1472,7 +1487,7 @@ def main():
         rec = {k: [] for k in ("bfs_dec_ms", "sssp_dec_ms", "bfs_inc_ms", "sssp_inc_ms",
                                "bfs_dec_rev_ms", "sssp_dec_rev_ms")}
         gbs = {k: [] for k in rec}
-        repair = {"bfs": [], "sssp": []}  # (invalidated, recomputed) per decremental call
+        repair = {"bfs": [], "sssp": [], "wcc": []}  # (invalidated, recomputed) per decremental call
 
         def timed_dynamic(key, trav, s_bytes, call):
             # algorithmic bytes: sum over vertices whose distance changed of

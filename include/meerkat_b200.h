@@ -446,6 +446,31 @@ mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src,
 mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src,
                              const uint32_t *d_dst, uint32_t n, void *stream,
                              float *ms_out);
+/* Attaches the reverse graph of the same edges (in-edges; the caller keeps
+ * it in step with g, as for mk_traversal_set_reverse), or detaches it with
+ * NULL.  Decremental calls use it to rescan the pieces a deletion split off.
+ *
+ * Every static, incremental and decremental call keeps a spanning forest:
+ * the edge of each union that hooked a root.  mk_wcc_decremental then
+ *   - changes nothing when the batch removed no forest edge (a deleted
+ *     forest edge whose reverse edge still exists stays in the forest);
+ *   - otherwise splits the affected components along the forest, keeps one
+ *     piece of each as its main piece, and rescans only the out- and (with
+ *     a reverse graph) in-edges of the other pieces' vertices;
+ *   - rebuilds the affected components from their out-edges when no reverse
+ *     graph is attached or the split-off pieces hold more than half of the
+ *     graph's edge ends.
+ * After mk_wcc_static_ranges / _prepared (which keep no forest) the next
+ * decremental call is a full static pass.  The labels are the same on every
+ * path.  The decremental call synchronises its stream (it picks the path on
+ * the host). */
+mk_status mk_wcc_set_reverse(mk_wcc *w, mk_graph *g_rev);
+/* The last decremental call: forest edges it removed, vertices rescanned
+ * outside their component's main piece, and its path: 0 no forest edge lost,
+ * 1 rescan of the split-off pieces, 2 rebuild of the affected components,
+ * 3 full static pass. */
+mk_status mk_wcc_decremental_stats(mk_wcc *w, uint64_t *h_dead_forest_edges,
+                                   uint64_t *h_rescanned_vertices, uint32_t *h_path);
 /* N labels: the minimum vertex id of each vertex's component (host). */
 mk_status mk_wcc_labels(mk_wcc *w, uint32_t *h_out);
 mk_status mk_wcc_labels_device(mk_wcc *w, const uint32_t **d_labels);

@@ -12,6 +12,7 @@ libmeerkat_b200.so.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from typing import Optional
 
 import numpy as np
@@ -656,6 +657,24 @@ class WCC(_Timed):
         check(lib().mk_wcc_labels(self._h, out.ctypes.data), "mk_wcc_labels")
         return out
 
+    def set_reverse(self, G_rev: Optional[DynamicGraph]) -> None:
+        """Attaches the reverse graph of the same edges (kept in step by the
+        caller); decremental calls rescan split-off pieces through it."""
+        self._rev = G_rev
+        check(lib().mk_wcc_set_reverse(self._h, G_rev.handle if G_rev is not None else None),
+              "mk_wcc_set_reverse")
+
+    def decremental_stats(self):
+        """(forest edges removed, vertices rescanned, path) of the last
+        Decremental call; path 0 no forest edge lost, 1 rescan of the
+        split-off pieces, 2 rebuild of the affected components, 3 full static."""
+        dead = C.c_uint64(0)
+        res = C.c_uint64(0)
+        path = C.c_uint32(0)
+        check(lib().mk_wcc_decremental_stats(self._h, C.byref(dead), C.byref(res), C.byref(path)),
+              "mk_wcc_decremental_stats")
+        return int(dead.value), int(res.value), int(path.value)
+
 
 class GraphSet:
     """Many small dynamic graphs stored, updated and queried as one union
@@ -798,8 +817,11 @@ class SetRunner:
         check(lib().mk_set_runner_handles(h, C.byref(bh), C.byref(wh)), "mk_set_runner_handles")
         bfs_m = np.flatnonzero(q == 0)
         glob = gs.offsets[bfs_m].astype(np.uint64) + src[bfs_m]
-        self.bfs = BFS._borrow(bh, gs.graph, glob, self) if bh.value else None
-        self.wcc = WCC._borrow(wh, gs.graph, self) if wh.value else None
+        # the views refer back weakly: no reference cycle, so the runner is
+        # released (and its handles destroyed) while the set it holds lives
+        me = weakref.ref(self)
+        self.bfs = BFS._borrow(bh, gs.graph, glob, me) if bh.value else None
+        self.wcc = WCC._borrow(wh, gs.graph, me) if wh.value else None
         self.fused = False
         if fused:
             self.set_fused(True)

@@ -120,6 +120,8 @@ SIGNATURES = [
     ("mk_wcc_static_prepared", _S, [vp, vp, f32p]),
     ("mk_wcc_incremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
     ("mk_wcc_decremental", _S, [vp, vp, vp, C.c_uint32, vp, f32p]),
+    ("mk_wcc_set_reverse", _S, [vp, vp]),
+    ("mk_wcc_decremental_stats", _S, [vp, u64p, u64p, u32p]),
     ("mk_wcc_labels", _S, [vp, vp]),
     ("mk_wcc_labels_device", _S, [vp, C.POINTER(vp)]),
     ("mk_wcc_destroy", _S, [vp]),

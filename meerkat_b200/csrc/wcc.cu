@@ -10,11 +10,32 @@
 //                not share a parent yet; then every vertex is compressed to
 //                its root;
 //   incremental  union of the edges the last insert applied, then compress;
-//   decremental  union-find cannot split, so every component that lost an
-//                edge is reset and rebuilt from its vertices' out-edges (an
-//                edge into an affected vertex comes from the same old
-//                component, so those out-edges are all its edges).
+//   decremental  see below.
 // Labels are the minimum vertex id of each weakly connected component.
+//
+// Spanning forest.  Every union whose CAS hooks a root records the graph edge
+// that caused it in the hooked root's slot (fe[root] = a << 32 | b, "a's slab
+// table holds b").  Each hook joins two different trees, so the recorded
+// edges form a spanning forest F of the graph: exactly the edges whose loss
+// can split a component.  The decremental call uses F:
+//   1. a forest edge whose directed edge the batch deleted stays in F,
+//      turned around, when the reverse edge b -> a still exists; otherwise it
+//      is dead and its component is affected.  No dead edge: nothing changed.
+//   2. the affected components' parents are reset and their surviving forest
+//      edges are unioned again: each component falls apart into the pieces
+//      of F minus the dead edges (min-id roots);
+//   3. one piece of each affected component is its main piece (the largest
+//      of a sample for the most sampled component, else the piece holding
+//      the old label); every edge that can join two pieces touches a vertex
+//      outside the main piece, so only those vertices' out-edges and
+//      (through the attached reverse graph) in-edges are scanned and unioned,
+//      then the affected vertices are compressed (min-id roots: the labels
+//      come out the same whichever piece is main).
+// Without a reverse graph, or when the vertices outside the main pieces hold
+// more than half of the graph's edge ends, the affected components are reset
+// and rebuilt from their vertices' out-edges instead (an edge into an affected
+// vertex comes from the same old component, so those out-edges are all its
+// edges).  Every rebuild records its hooks, so F stays a spanning forest.
 //
 // Every retry loop is bounded; on expiry the kernel sets MK_DEVERR_TIMEOUT.
 #include <cuda_runtime.h>
@@ -25,6 +46,7 @@
 #include "mk_internal.h"
 #include "mk_slab.cuh"
 #include "mk_members.cuh"
+#include "mk_update.cuh"
 
 namespace mk {
 
@@ -53,30 +75,55 @@ __device__ __forceinline__ uint32_t uf_root(const uint32_t *p, uint32_t x) {
   return x;
 }
 
-__device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b, uint32_t *err) {
+constexpr unsigned long long kNoForest = ~0ull;  // empty forest slot
+
+__device__ __forceinline__ unsigned long long fedge(uint32_t a, uint32_t b) {
+  return ((unsigned long long)a << 32) | b;
+}
+
+// Union of the sets of a and b for the graph edge a -> b (a's slab table
+// holds b).  With fe, the hook that joins two sets records that edge in the
+// hooked root's forest slot (empty: a root has never been hooked since its
+// reset).
+__device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b, uint32_t *err,
+                                         unsigned long long *fe = nullptr) {
   for (uint32_t it = 0; it < kUfLimit; ++it) {
     uint32_t ra = uf_find(p, a), rb = uf_find(p, b);
     if (ra == rb) return;
     uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
-    if (atomicCAS(p + hi, hi, lo) == hi) return;
+    if (atomicCAS(p + hi, hi, lo) == hi) {
+      if (fe) fe[hi] = fedge(a, b);
+      return;
+    }
   }
   atomicOr(err, kErrTimeout);
 }
 
-__global__ void k_uf_init(uint32_t *p, uint32_t V, const uint32_t *sel_bits = nullptr) {
+// Resets the selected vertices (all if sel_bits is null) to their own set
+// and, with fe, empties their forest slots.
+__global__ void k_uf_init(uint32_t *p, uint32_t V, const uint32_t *sel_bits = nullptr,
+                          unsigned long long *fe = nullptr) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
     if (sel_bits && !((sel_bits[i >> 5] >> (i & 31)) & 1u)) continue;
     p[i] = i;
+    if (fe) fe[i] = kNoForest;
   }
 }
 
+// Unions of the edges the last insert applied (rev: the graph stores each
+// batch edge turned around, so the recorded slab edge is dst -> src).
 __global__ void k_uf_batch(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
                            const uint8_t *__restrict__ applied, uint32_t n, uint32_t V,
-                           uint32_t *p, uint32_t *err) {
+                           uint32_t rev, uint32_t *p, uint32_t *err, unsigned long long *fe) {
   uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n || !applied[e]) return;
   uint32_t a = src[e], b = dst[e];
-  if (a != b && a < V && b < V) uf_union(p, a, b, err);
+  if (rev) {
+    const uint32_t t = a;
+    a = b;
+    b = t;
+  }
+  if (a != b && a < V && b < V) uf_union(p, a, b, err, fe);
 }
 
 __global__ void k_uf_compress(uint32_t *p, uint32_t V, const uint32_t *sel_bits) {
@@ -86,23 +133,15 @@ __global__ void k_uf_compress(uint32_t *p, uint32_t V, const uint32_t *sel_bits)
   }
 }
 
-// Marks the label (root) of every endpoint of an applied deletion.
-__global__ void k_uf_mark(const uint32_t *__restrict__ src, const uint8_t *__restrict__ applied,
-                          uint32_t n, uint32_t V, const uint32_t *p, uint32_t *aff_labels) {
-  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n || !applied[e]) return;
-  uint32_t a = src[e];
-  if (a >= V) return;
-  uint32_t r = p[a];
-  atomicOr(aff_labels + (r >> 5), 1u << (r & 31));
-}
-
-// Resets the vertices of affected components and records them.
-__global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, uint32_t *aff_vertices) {
+// Resets the vertices of affected components (their forest slots too) and
+// records them.
+__global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, uint32_t *aff_vertices,
+                           unsigned long long *fe) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
     uint32_t r = p[i];
     if ((aff_labels[r >> 5] >> (r & 31)) & 1u) {
       p[i] = i;
+      fe[i] = kNoForest;
       atomicOr(aff_vertices + (i >> 5), 1u << (i & 31));
     }
   }
@@ -117,14 +156,15 @@ __global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, 
 // between vertices already connected keeps the result exact, and it works for
 // every component at once (the members of a graph set included).
 template <bool kW>
-__global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
+__global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err,
+                            unsigned long long *fe) {
   for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.V; u += gridDim.x * blockDim.x) {
     if (g.deg[u] == 0) continue;
     if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
     const uint32_t *w = reinterpret_cast<const uint32_t *>(g.slabs + 8ull * g.boff[u]);
     const uint32_t k0 = w[0], k1 = kW ? w[2] : w[1];
-    if (k0 < kTombKey && k0 != u) uf_union(p, u, k0, err);
-    if (k1 < kTombKey && k1 != u) uf_union(p, u, k1, err);
+    if (k0 < kTombKey && k0 != u) uf_union(p, u, k0, err, fe);
+    if (k1 < kTombKey && k1 != u) uf_union(p, u, k1, err, fe);
   }
 }
 
@@ -132,7 +172,8 @@ __global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, 
 // a parent yet.
 template <bool kW>
 __device__ __forceinline__ void link_bucket_skip(const GraphView &g, const Lanes &L, uint32_t *p,
-                                                 uint32_t b, uint32_t u, uint32_t *err) {
+                                                 uint32_t b, uint32_t u, uint32_t *err,
+                                                 unsigned long long *fe) {
   const uint32_t pu = __ldcg(p + u);
   walk_bucket(g, L, b, [&](const uint4 &q) {
     uint32_t k[4], w[4];
@@ -142,13 +183,14 @@ __device__ __forceinline__ void link_bucket_skip(const GraphView &g, const Lanes
       const uint32_t v = k[j];
       if (v >= kTombKey || v == u) continue;
       if (__ldcg(p + v) == pu) continue;
-      uf_union(p, u, v, err);
+      uf_union(p, u, v, err, fe);
     }
   });
 }
 
 template <bool kW>
-__global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err) {
+__global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err,
+                                unsigned long long *fe) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
@@ -156,7 +198,274 @@ __global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bi
     const uint32_t u = g.bowner[b];
     if (g.deg[u] == 0) continue;
     if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
-    link_bucket_skip<kW>(g, L, p, b, u, err);
+    link_bucket_skip<kW>(g, L, p, b, u, err, fe);
+  }
+}
+
+// ---- decremental repair over the spanning forest ----
+// ctl words (u64) of one decremental call.
+enum : int {
+  kFDead = 0,       // forest edges the batch removed for good
+  kFNmCount = 1,    // vertices outside their component's main piece (list length)
+  kFNmEnds = 2,     // their out- plus in-degrees
+  kFEdges = 3,      // live edges of the graph
+  kFMainLabel = 4,  // old label + 1 of the component whose main piece was sampled (0: none)
+  kFMainPiece = 5,  // that main piece's root + 1
+  kFCtlWords = 6
+};
+
+// Set of the batch's deleted edges (slab orientation a << 32 | b): open
+// addressing over a power-of-two table (mask + 1 slots, at least twice the
+// batch), linear probing, EMPTY = ~0.
+__device__ __forceinline__ uint32_t dh_slot(unsigned long long key, uint32_t mask) {
+  key ^= key >> 33;
+  key *= 0xff51afd7ed558ccdull;
+  key ^= key >> 33;
+  return (uint32_t)key & mask;
+}
+
+__global__ void k_dh_insert(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                            const uint8_t *__restrict__ applied, uint32_t n, uint32_t rev,
+                            unsigned long long *tab, uint32_t mask) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n || !applied[e]) return;
+  uint32_t a = src[e], b = dst[e];
+  if (rev) {
+    const uint32_t t = a;
+    a = b;
+    b = t;
+  }
+  const unsigned long long key = fedge(a, b);
+  uint32_t s = dh_slot(key, mask);
+  for (uint32_t it = 0; it <= mask; ++it) {
+    const unsigned long long old = atomicCAS(tab + s, kNoForest, key);
+    if (old == kNoForest || old == key) return;
+    s = (s + 1) & mask;
+  }
+}
+
+__device__ __forceinline__ bool dh_has(const unsigned long long *tab, uint32_t mask,
+                                       unsigned long long key) {
+  uint32_t s = dh_slot(key, mask);
+  for (uint32_t it = 0; it <= mask; ++it) {
+    const unsigned long long k = __ldg(tab + s);
+    if (k == key) return true;
+    if (k == kNoForest) return false;
+    s = (s + 1) & mask;
+  }
+  return false;
+}
+
+// True when u's slab table holds key (one thread, whole slabs).
+template <bool kW>
+__device__ __forceinline__ bool lane_has_key(const GraphView &g, uint32_t u, uint32_t key) {
+  const uint32_t b0 = __ldg(g.boff + u), nb = __ldg(g.boff + u + 1) - b0;
+  if (nb == 0) return false;
+  uint32_t s = b0 + bucket_of(key, nb);
+  for (uint32_t it = 0; it < kProbeLimit; ++it) {
+    uint4 q[8];
+    lane_load_slab(g, s, q);
+    const LaneProbe pr = lane_probe<kW>(q, key);
+    if (pr.found_word < 32) return true;
+    if (pr.next == kNoSlab) return false;
+    s = pr.next;
+  }
+  return false;
+}
+
+// Step 1: forest edges the batch deleted.  A deleted a -> b whose reverse
+// b -> a still exists stays in the forest turned around; otherwise the slot
+// empties and the component (its label, the compressed parent of a) is
+// affected.
+template <bool kW>
+__global__ void k_fe_dead(GraphView g, unsigned long long *fe, const unsigned long long *tab,
+                          uint32_t mask, const uint32_t *p, uint32_t *aff_labels,
+                          unsigned long long *ctl) {
+  for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < g.V; x += gridDim.x * blockDim.x) {
+    const unsigned long long e = fe[x];
+    if (e == kNoForest || !dh_has(tab, mask, e)) continue;
+    const uint32_t a = (uint32_t)(e >> 32), b = (uint32_t)e;
+    if (lane_has_key<kW>(g, b, a)) {
+      fe[x] = fedge(b, a);
+      continue;
+    }
+    fe[x] = kNoForest;
+    const uint32_t r = p[a];
+    atomicOr(aff_labels + (r >> 5), 1u << (r & 31));
+    atomicAdd(ctl + kFDead, 1ull);
+  }
+}
+
+// Step 2a: every vertex of an affected component keeps its old label, is
+// reset to its own set and hands its forest edge over to fe2; aff_vertices
+// gets the affected-vertex bitmap (whole words, one ballot each).
+__global__ void k_fe_collect(uint32_t *p, unsigned long long *fe, unsigned long long *fe2, uint32_t V,
+                             const uint32_t *aff_labels, uint32_t *oldlab, uint32_t *aff_vertices) {
+  const uint32_t words = (V + 31) / 32, lane = threadIdx.x & 31u;
+  const uint32_t stride = gridDim.x * blockDim.x;  // a multiple of 32
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < words * 32u;
+       base += stride) {
+    const uint32_t x = base + lane;
+    bool aff = false;
+    if (x < V) {
+      const uint32_t r = p[x];
+      aff = (aff_labels[r >> 5] >> (r & 31)) & 1u;
+      if (aff) {
+        oldlab[x] = r;
+        p[x] = x;
+        fe2[x] = fe[x];
+        fe[x] = kNoForest;
+      }
+    }
+    const uint32_t word = __ballot_sync(0xFFFFFFFFu, aff);
+    if (lane == 0) aff_vertices[base >> 5] = word;
+  }
+}
+
+// Step 2b: the surviving forest edges of the affected vertices, unioned again
+// (every one joins two sets: they form a forest), recorded at their new hooks.
+__global__ void k_fe_union(uint32_t *p, unsigned long long *fe, const unsigned long long *fe2,
+                           uint32_t V, const uint32_t *aff_vertices, uint32_t *err) {
+  for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < V; x += gridDim.x * blockDim.x) {
+    if (!((aff_vertices[x >> 5] >> (x & 31)) & 1u)) continue;
+    const unsigned long long e = fe2[x];
+    if (e == kNoForest) continue;
+    uf_union(p, (uint32_t)(e >> 32), (uint32_t)e, err, fe);
+  }
+}
+
+// Step 3a: the main piece of the most sampled component.  Any one piece per
+// component may be its main piece (every edge between two pieces touches a
+// vertex outside it, and min-id unions give the same labels); the largest
+// leaves the least to rescan.  One CTA draws kMainSamples vertices, counts
+// the affected ones by piece root in shared memory and keeps the most
+// frequent piece (at least 32 samples) as the main piece of its component.
+// Every other component keeps the piece of its old label.
+constexpr int kMainThreads = 1024;
+constexpr uint32_t kMainSamples = 2048, kMainSlots = 4096;  // slots: twice the samples
+
+__global__ void __launch_bounds__(kMainThreads)
+    k_fe_main_sample(const uint32_t *p, const uint32_t *oldlab, const uint32_t *aff_vertices,
+                     uint32_t V, unsigned long long seed, unsigned long long *ctl) {
+  __shared__ uint32_t keys[kMainSlots], cnts[kMainSlots];
+  __shared__ unsigned long long best;
+  for (uint32_t i = threadIdx.x; i < kMainSlots; i += blockDim.x) {
+    keys[i] = 0xFFFFFFFFu;
+    cnts[i] = 0u;
+  }
+  if (threadIdx.x == 0) best = 0;
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < kMainSamples; j += blockDim.x) {
+    unsigned long long h = seed + 0x9E3779B97F4A7C15ull * (j + 1);
+    h ^= h >> 33;
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 33;
+    const uint32_t x = (uint32_t)(h % V);
+    if (!((aff_vertices[x >> 5] >> (x & 31)) & 1u)) continue;
+    const uint32_t k = __ldcg(p + x);
+    uint32_t sl = (k * 2654435761u) & (kMainSlots - 1);
+    for (uint32_t it = 0; it < kMainSlots; ++it) {
+      const uint32_t old = atomicCAS(keys + sl, 0xFFFFFFFFu, k);
+      if (old == 0xFFFFFFFFu || old == k) {
+        atomicAdd(cnts + sl, 1u);
+        break;
+      }
+      sl = (sl + 1) & (kMainSlots - 1);
+    }
+  }
+  __syncthreads();
+  unsigned long long mine = 0;
+  for (uint32_t i = threadIdx.x; i < kMainSlots; i += blockDim.x) {
+    const unsigned long long c = ((unsigned long long)cnts[i] << 32) | keys[i];
+    if (cnts[i] && c > mine) mine = c;
+  }
+  atomicMax(&best, mine);
+  __syncthreads();
+  if (threadIdx.x == 0 && (best >> 32) >= 32) {
+    const uint32_t piece = (uint32_t)best;
+    ctl[kFMainLabel] = (unsigned long long)oldlab[piece] + 1;
+    ctl[kFMainPiece] = (unsigned long long)piece + 1;
+  }
+}
+
+// Step 3b (after compressing the affected vertices): the affected vertices
+// outside their component's main piece, listed, counted with their out- plus
+// in-degrees; and the graph's live edge count.
+__global__ void k_fe_nonmain(const uint32_t *p, const uint32_t *oldlab, uint32_t V,
+                             const uint32_t *aff_vertices, const uint32_t *deg,
+                             const uint32_t *rdeg, uint32_t *nm_list, unsigned long long *ctl) {
+  const uint32_t words = (V + 31) / 32, lane = threadIdx.x & 31u;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const unsigned long long ml = ctl[kFMainLabel], mp = ctl[kFMainPiece];
+  unsigned long long ends = 0, edges = 0;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < words * 32u;
+       base += stride) {
+    const uint32_t x = base + lane;
+    bool nm = false;
+    if (x < V) {
+      const uint32_t d = deg[x];
+      edges += d;
+      if ((aff_vertices[x >> 5] >> (x & 31)) & 1u) {
+        const uint32_t r = oldlab[x];
+        const uint32_t main_piece = (ml && r == ml - 1) ? (uint32_t)(mp - 1) : __ldcg(p + r);
+        nm = __ldcg(p + x) != main_piece;
+        if (nm) ends += d + rdeg[x];
+      }
+    }
+    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, nm);
+    if (bal) {
+      uint32_t pos = 0;
+      if (lane == 0) pos = (uint32_t)atomicAdd(ctl + kFNmCount, (unsigned long long)__popc(bal));
+      pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
+      if (nm) nm_list[pos + __popc(bal & ((1u << lane) - 1u))] = x;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ends += __shfl_xor_sync(0xFFFFFFFFu, ends, o);
+    edges += __shfl_xor_sync(0xFFFFFFFFu, edges, o);
+  }
+  if (lane == 0) {
+    if (ends) atomicAdd(ctl + kFNmEnds, ends);
+    if (edges) atomicAdd(ctl + kFEdges, edges);
+  }
+}
+
+// Step 3c: out-edges (g) and in-edges (gr, the reverse graph) of the listed
+// vertices, one 8-lane group per vertex; an edge between two sets is a union
+// recorded in the forest.
+template <bool kW, bool kRW>
+__global__ void k_fe_scan(GraphView g, GraphView gr, uint32_t *p, unsigned long long *fe,
+                          const uint32_t *nm_list, const unsigned long long *ctl, uint32_t *err) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  const uint32_t n = (uint32_t)ctl[kFNmCount];
+  for (uint32_t i = group; i < n; i += ngroups) {
+    const uint32_t x = nm_list[i];
+    const uint32_t px = __ldcg(p + x);
+    walk_buckets(g, L, g.boff[x], g.boff[x + 1], [&](const uint4 &q) {
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+#pragma unroll
+      for (int j = 0; j < keys_per_lane<kW>(); ++j) {
+        const uint32_t y = k[j];
+        if (y >= kTombKey || y == x || y >= g.V) continue;
+        if (__ldcg(p + y) == px) continue;
+        uf_union(p, x, y, err, fe);
+      }
+    });
+    walk_buckets(gr, L, gr.boff[x], gr.boff[x + 1], [&](const uint4 &q) {
+      uint32_t k[4], w[4];
+      lane_keys<kRW>(q, L.gl, k, w);
+#pragma unroll
+      for (int j = 0; j < keys_per_lane<kRW>(); ++j) {
+        const uint32_t y = k[j];
+        if (y >= kTombKey || y == x || y >= g.V) continue;
+        if (__ldcg(p + y) == px) continue;
+        uf_union(p, y, x, err, fe);  // the slab edge y -> x of g
+      }
+    });
   }
 }
 
@@ -210,7 +519,7 @@ __global__ void k_uf_edges_ranges(GraphView g, uint32_t *p, const uint32_t *bpre
     const uint32_t b = range_at(bpre, nr, i, bbase);
     const uint32_t u = g.bowner[b];
     if (g.deg[u] == 0) continue;
-    link_bucket_skip<kW>(g, L, p, b, u, err);
+    link_bucket_skip<kW>(g, L, p, b, u, err, nullptr);
   }
 }
 
@@ -254,6 +563,20 @@ struct mk_wcc {
   uint32_t *aff_labels = nullptr;
   uint32_t *aff_vertices = nullptr;
   uint32_t *err = nullptr;  // the graph's sticky device error word
+  // spanning forest: fe[v] = the edge (a << 32 | b) whose union hooked root v
+  unsigned long long *fe = nullptr;
+  bool forest_valid = false;  // fe spans every component (after a full static)
+  mk_graph *rev = nullptr;    // reverse graph of the same edges (in-edges), optional
+  // decremental scratch: batch edge set, old labels, handed-over forest
+  // edges, vertices outside the main pieces, ctl words
+  DevBuf<unsigned long long> dtab;
+  DevBuf<unsigned long long> fe2;
+  DevBuf<uint32_t> oldlab, nm_list;
+  unsigned long long *fctl = nullptr;
+  // last decremental call: forest edges lost, vertices rescanned, path taken
+  uint64_t last_dead = 0, last_rescanned = 0;
+  uint32_t last_path = 0;
+  uint64_t calls = 0;  // decremental calls (seeds the main-piece sample)
   // prepared range table: counter word, then uint4 (lo, hi, b0, b1) per small
   // range (largest first), then vpre, vbase, bpre, bbase of the large ranges
   DevBuf<uint32_t> ranges;
@@ -277,16 +600,16 @@ static mk_status wcc_link(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
   const int fg = flat_grid(g->V, g->device);
   const GraphView v = g->view();
   if (g->weighted)
-    k_uf_sample<true><<<fg, 256, 0, s>>>(v, w->parent, sel, w->err);
+    k_uf_sample<true><<<fg, 256, 0, s>>>(v, w->parent, sel, w->err, w->fe);
   else
-    k_uf_sample<false><<<fg, 256, 0, s>>>(v, w->parent, sel, w->err);
+    k_uf_sample<false><<<fg, 256, 0, s>>>(v, w->parent, sel, w->err, w->fe);
   k_uf_compress<<<fg, 256, 0, s>>>(w->parent, g->V, sel);
   const int blocks = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1,
                                              (uint64_t)device_sm_count(g->device) * 8);
   if (g->weighted)
-    k_uf_edges_skip<true><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->err);
+    k_uf_edges_skip<true><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->err, w->fe);
   else
-    k_uf_edges_skip<false><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->err);
+    k_uf_edges_skip<false><<<blocks, 256, 0, s>>>(v, w->parent, sel, w->err, w->fe);
   k_uf_compress<<<fg, 256, 0, s>>>(w->parent, g->V, sel);
   MK_CUDA(cudaGetLastError());
   return MK_OK;
@@ -294,8 +617,89 @@ static mk_status wcc_link(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
 
 static mk_status wcc_static(mk_wcc *w, cudaStream_t s) {
   mk_graph *g = w->g;
-  k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V);
-  return wcc_link(w, nullptr, s);
+  k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, nullptr, w->fe);
+  MK_CHECK(wcc_link(w, nullptr, s));
+  w->forest_valid = true;
+  return MK_OK;
+}
+
+// Decremental repair over the spanning forest (the file header has the
+// steps).  Synchronises twice: after finding the lost forest edges and after
+// counting the vertices outside the main pieces, to choose the path.
+static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const uint32_t *d_dst,
+                                        uint32_t n, cudaStream_t s) {
+  mk_graph *g = w->g;
+  const uint32_t V = g->V;
+  const size_t words = ((size_t)V + 31) / 32;
+  const int fg = flat_grid(V, g->device);
+  const GraphView v = g->view();
+  uint32_t cap = 1024;
+  while (cap < 2ull * n) cap <<= 1;
+  MK_CHECK(w->dtab.reserve(cap, &g->device_bytes));
+  MK_CUDA(cudaMemsetAsync(w->dtab.ptr, 0xFF, (size_t)cap * 8, s));
+  MK_CUDA(cudaMemsetAsync(w->fctl, 0, kFCtlWords * 8, s));
+  MK_CUDA(cudaMemsetAsync(w->aff_labels, 0, words * 4, s));
+  k_dh_insert<<<(n + 255) / 256, 256, 0, s>>>(d_src, d_dst, g->applied.ptr, n, g->reverse,
+                                              w->dtab.ptr, cap - 1);
+  if (g->weighted)
+    k_fe_dead<true><<<fg, 256, 0, s>>>(v, w->fe, w->dtab.ptr, cap - 1, w->parent, w->aff_labels, w->fctl);
+  else
+    k_fe_dead<false><<<fg, 256, 0, s>>>(v, w->fe, w->dtab.ptr, cap - 1, w->parent, w->aff_labels, w->fctl);
+  MK_CUDA(cudaGetLastError());
+  unsigned long long h[kFCtlWords] = {};
+  MK_CUDA(cudaMemcpyAsync(h, w->fctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  w->last_dead = h[kFDead];
+  w->last_rescanned = 0;
+  if (h[kFDead] == 0) {
+    w->last_path = 0;  // the forest still spans every component: labels stand
+    return MK_OK;
+  }
+  if (!w->rev) {
+    // reset the affected components (forest slots too) and relink them
+    MK_CUDA(cudaMemsetAsync(w->aff_vertices, 0, words * 4, s));
+    k_uf_reset<<<fg, 256, 0, s>>>(w->parent, V, w->aff_labels, w->aff_vertices, w->fe);
+    w->last_path = 2;
+    return wcc_link(w, w->aff_vertices, s);
+  }
+  MK_CHECK(w->fe2.reserve(V, &g->device_bytes));
+  MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));
+  MK_CHECK(w->nm_list.reserve(V, &g->device_bytes));
+  k_fe_collect<<<fg, 256, 0, s>>>(w->parent, w->fe, w->fe2.ptr, V, w->aff_labels, w->oldlab.ptr,
+                                  w->aff_vertices);
+  k_fe_union<<<fg, 256, 0, s>>>(w->parent, w->fe, w->fe2.ptr, V, w->aff_vertices, w->err);
+  k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices);
+  k_fe_main_sample<<<1, kMainThreads, 0, s>>>(w->parent, w->oldlab.ptr, w->aff_vertices, V,
+                                              0x5EED0000ull + (++w->calls), w->fctl);
+  k_fe_nonmain<<<fg, 256, 0, s>>>(w->parent, w->oldlab.ptr, V, w->aff_vertices, g->deg,
+                                  w->rev->deg, w->nm_list.ptr, w->fctl);
+  MK_CUDA(cudaGetLastError());
+  MK_CUDA(cudaMemcpyAsync(h, w->fctl, sizeof(h), cudaMemcpyDeviceToHost, s));
+  MK_CUDA(cudaStreamSynchronize(s));
+  if (2 * h[kFNmEnds] > h[kFEdges]) {
+    // the split-off pieces hold most of the graph: relink from scratch
+    k_uf_init<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices, w->fe);
+    w->last_path = 2;
+    return wcc_link(w, w->aff_vertices, s);
+  }
+  w->last_path = 1;
+  w->last_rescanned = h[kFNmCount];
+  if (h[kFNmCount]) {
+    const int blocks = (int)std::min<uint64_t>(h[kFNmCount] * 8 / 256 + 1,
+                                               (uint64_t)device_sm_count(g->device) * 8);
+    const GraphView rv = w->rev->view();
+    if (g->weighted && w->rev->weighted)
+      k_fe_scan<true, true><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
+    else if (g->weighted)
+      k_fe_scan<true, false><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
+    else if (w->rev->weighted)
+      k_fe_scan<false, true><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
+    else
+      k_fe_scan<false, false><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
+    k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices);
+  }
+  MK_CUDA(cudaGetLastError());
+  return MK_OK;
 }
 
 static bool batch_matches(const mk_graph *g, const uint32_t *d_src, const uint32_t *d_dst,
@@ -318,12 +722,14 @@ mk_status mk_wcc_create(mk_graph *g, mk_wcc **out) {
   cudaError_t e = cudaMalloc(&w->parent, V * 4);
   if (e == cudaSuccess) e = cudaMalloc(&w->aff_labels, words * 4);
   if (e == cudaSuccess) e = cudaMalloc(&w->aff_vertices, words * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&w->fe, V * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&w->fctl, kFCtlWords * 8);
   w->err = g->err_word();
   if (e != cudaSuccess) {
     mk_wcc_destroy(w);
     return cuda_fail(e, "mk_wcc_create");
   }
-  k_uf_init<<<flat_grid(V, g->device), 256>>>(w->parent, (uint32_t)V);
+  k_uf_init<<<flat_grid(V, g->device), 256>>>(w->parent, (uint32_t)V, nullptr, w->fe);
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     mk_wcc_destroy(w);
@@ -349,7 +755,7 @@ mk_status mk_wcc_static_subset(mk_wcc *w, const uint32_t *d_sel_bits, void *stre
   DeviceGuard dg(g->device);
   cudaStream_t s = as_stream(stream);
   MK_CHECK(w->timer.start(s, ms_out != nullptr));
-  k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, d_sel_bits);
+  k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, d_sel_bits, w->fe);
   MK_CHECK(wcc_link(w, d_sel_bits, s));
   return w->timer.stop(ms_out);
 }
@@ -442,6 +848,7 @@ mk_status mk_wcc_static_prepared(mk_wcc *w, void *stream, float *ms_out) {
   DeviceGuard dg(g->device);
   cudaStream_t s = as_stream(stream);
   MK_CHECK(w->timer.start(s, ms_out != nullptr));
+  w->forest_valid = false;  // the range passes record no forest
   const GraphView v = g->view();
   uint32_t *counter = w->ranges.ptr;
   const uint32_t ns = w->n_small, nl = w->n_large;
@@ -493,7 +900,8 @@ mk_status mk_wcc_incremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d
   if (!batch_matches(g, d_src, d_dst, n, 1)) {
     MK_CHECK(wcc_static(w, s));
   } else if (n) {
-    k_uf_batch<<<(n + 255) / 256, 256, 0, s>>>(d_src, d_dst, g->applied.ptr, n, g->V, w->parent, w->err);
+    k_uf_batch<<<(n + 255) / 256, 256, 0, s>>>(d_src, d_dst, g->applied.ptr, n, g->V, g->reverse,
+                                                w->parent, w->err, w->fe);
     k_uf_compress<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, nullptr);
     MK_CUDA(cudaGetLastError());
   }
@@ -507,17 +915,33 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d
   DeviceGuard dg(g->device);
   cudaStream_t s = as_stream(stream);
   MK_CHECK(w->timer.start(s, ms_out != nullptr));
-  if (!batch_matches(g, d_src, d_dst, n, 2)) {
+  w->last_dead = w->last_rescanned = 0;
+  w->last_path = 0;
+  if (!batch_matches(g, d_src, d_dst, n, 2) || !w->forest_valid) {
     MK_CHECK(wcc_static(w, s));
+    w->last_path = 3;
   } else if (n) {
-    const size_t words = ((size_t)g->V + 31) / 32;
-    MK_CUDA(cudaMemsetAsync(w->aff_labels, 0, words * 4, s));
-    MK_CUDA(cudaMemsetAsync(w->aff_vertices, 0, words * 4, s));
-    k_uf_mark<<<(n + 255) / 256, 256, 0, s>>>(d_src, g->applied.ptr, n, g->V, w->parent, w->aff_labels);
-    k_uf_reset<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, w->aff_labels, w->aff_vertices);
-    MK_CHECK(wcc_link(w, w->aff_vertices, s));
+    MK_CHECK(wcc_decremental_forest(w, d_src, d_dst, n, s));
   }
   return w->timer.stop(ms_out);
+}
+
+mk_status mk_wcc_set_reverse(mk_wcc *w, mk_graph *g_rev) {
+  if (!w) return fail(MK_ERR_INVALID, "mk_wcc_set_reverse: null handle");
+  if (g_rev && (g_rev->V != w->g->V || g_rev->device != w->g->device || g_rev->reverse == w->g->reverse))
+    return fail(MK_ERR_INVALID,
+                "mk_wcc_set_reverse: need the reverse graph of the same vertices on the same device");
+  w->rev = g_rev;
+  return MK_OK;
+}
+
+mk_status mk_wcc_decremental_stats(mk_wcc *w, uint64_t *h_dead_forest_edges,
+                                   uint64_t *h_rescanned_vertices, uint32_t *h_path) {
+  if (!w) return fail(MK_ERR_INVALID, "mk_wcc_decremental_stats: null handle");
+  if (h_dead_forest_edges) *h_dead_forest_edges = w->last_dead;
+  if (h_rescanned_vertices) *h_rescanned_vertices = w->last_rescanned;
+  if (h_path) *h_path = w->last_path;
+  return MK_OK;
 }
 
 mk_status mk_wcc_labels(mk_wcc *w, uint32_t *h_out) {
@@ -543,6 +967,12 @@ mk_status mk_wcc_destroy(mk_wcc *w) {
   cudaFree(w->parent);
   cudaFree(w->aff_labels);
   cudaFree(w->aff_vertices);
+  cudaFree(w->fe);
+  cudaFree(w->fctl);
+  w->dtab.release();
+  w->fe2.release();
+  w->oldlab.release();
+  w->nm_list.release();
   w->staging.release();
   w->ranges.release();
   delete w;

@@ -265,6 +265,114 @@ def test_wcc_static_and_dynamic():
         np.testing.assert_array_equal(wcc.Labels(), O.wcc())
 
 
+@pytest.mark.parametrize("with_rev,weighted", [(True, False), (True, True), (False, False)])
+def test_wcc_decremental_over_the_spanning_forest(with_rev, weighted):
+    """Decremental WCC repairs along its spanning forest: with a reverse
+    graph it rescans only the pieces a lost forest edge split off (path 1),
+    without one it rebuilds the affected components (path 2); a batch that
+    removes no forest edge changes nothing (path 0).  Labels equal the
+    oracle's after every batch, and no call after the first static pass
+    falls back to a full static pass."""
+    V = 1 << 12
+    s, d, w = mk.gen_rmat(12, 9000, seed=83, w_lo=1, w_hi=50)  # sparse: many components
+    G = mk.DynamicGraph(V, degree_hints=degree_hints(s, V), weighted=weighted)
+    G.InsertEdges(to_dev(s), to_dev(d), vals=to_dev(w) if weighted else None)
+    O = OracleGraph(V)
+    O.insert(s, d, w if weighted else None)
+    Gr = None
+    if with_rev:
+        Gr = mk.DynamicGraph(V, degree_hints=degree_hints(d, V), reverse=True)
+        Gr.InsertEdges(to_dev(s), to_dev(d))
+    wcc = mk.WCC(G)
+    if Gr is not None:
+        wcc.set_reverse(Gr)
+    wcc.Static()
+    np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+    es = mk.EdgeSet(V, s, d)
+    paths = []
+    for r in range(6):
+        ds, dd = es.sample_present(400 if r % 2 else 2500, seed=120 + r)
+        tds, tdd = to_dev(ds), to_dev(dd)
+        G.DeleteEdges(tds, tdd)
+        if Gr is not None:
+            Gr.DeleteEdges(tds, tdd)
+        O.delete(ds, dd)
+        wcc.Decremental(tds, tdd)
+        np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+        dead, rescanned, path = wcc.decremental_stats()
+        assert (dead == 0) == (path == 0)
+        paths.append(path)
+        is_, id_ = es.sample_absent(700, seed=130 + r)
+        tis, tid = to_dev(is_), to_dev(id_)
+        G.InsertEdges(tis, tid)
+        if Gr is not None:
+            Gr.InsertEdges(tis, tid)
+        O.insert(is_, id_)
+        wcc.Incremental(tis, tid)
+        np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+    assert 3 not in paths
+    if with_rev:
+        assert 1 in paths
+    else:
+        assert 2 in paths and 1 not in paths
+
+
+def test_wcc_forest_edge_with_a_surviving_reverse_edge_changes_nothing():
+    """On a symmetric graph a batch that deletes one direction of each pair
+    removes no connection: the forest keeps the reverse edges and the call
+    takes path 0."""
+    V = 1 << 11
+    s0, d0, _ = mk.gen_rmat(11, 5000, seed=85)
+    s, d = symmetrise(s0, d0)
+    G, O = make_pair(V, s, d)
+    wcc = mk.WCC(G)
+    wcc.Static()
+    want = O.wcc()
+    keep = s < d
+    for r in range(2):
+        pick = np.random.default_rng(140 + r).choice(np.flatnonzero(keep), 1500, replace=False)
+        ds, dd = (s[pick], d[pick]) if r == 0 else (d[pick], s[pick])
+        tds, tdd = to_dev(ds), to_dev(dd)
+        G.DeleteEdges(tds, tdd)
+        O.delete(ds, dd)
+        wcc.Decremental(tds, tdd)
+        assert wcc.decremental_stats()[2] == 0
+        np.testing.assert_array_equal(wcc.Labels(), want)
+        np.testing.assert_array_equal(O.wcc(), want)
+        tis, tid = to_dev(ds), to_dev(dd)
+        G.InsertEdges(tis, tid)
+        O.insert(ds, dd)
+        wcc.Incremental(tis, tid)
+        np.testing.assert_array_equal(wcc.Labels(), want)
+
+
+def test_wcc_decremental_splits_paths_along_the_forest():
+    """Directed paths (deep forest): deleting path edges splits components
+    into pieces that must get their own min-id labels; with the reverse graph
+    attached the pieces are rescanned or the components rebuilt."""
+    V = 1 << 14
+    rng = np.random.default_rng(19)
+    perm = rng.permutation(V).astype(np.uint32)
+    paths = perm.reshape(64, -1)
+    s = paths[:, :-1].ravel()
+    d = paths[:, 1:].ravel()
+    G, O = make_pair(V, s, d)
+    Gr, _ = make_pair(V, s, d, reverse=True)
+    wcc = mk.WCC(G)
+    wcc.set_reverse(Gr)
+    wcc.Static()
+    for r in range(3):
+        pick = rng.choice(len(s), 40, replace=False)
+        ds, dd = s[pick], d[pick]
+        tds, tdd = to_dev(ds), to_dev(dd)
+        G.DeleteEdges(tds, tdd)
+        Gr.DeleteEdges(tds, tdd)
+        O.delete(ds, dd)
+        wcc.Decremental(tds, tdd)
+        assert wcc.decremental_stats()[2] in (1, 2)
+        np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+
+
 def test_algorithms_with_a_foreign_batch_fall_back_to_recompute():
     """Dynamic calls whose batch is not the graph's last update recompute."""
     V = 1 << 10
