@@ -1487,7 +1487,7 @@ def main():
         rec = {k: [] for k in ("bfs_dec_ms", "sssp_dec_ms", "bfs_inc_ms", "sssp_inc_ms",
                                "bfs_dec_rev_ms", "sssp_dec_rev_ms")}
         gbs = {k: [] for k in rec}
-        repair = {"bfs": [], "sssp": [], "wcc": []}  # (invalidated, recomputed) per decremental call
+        repair = {"bfs": [], "sssp": []}  # (invalidated, recomputed) per decremental call
 
         def timed_dynamic(key, trav, s_bytes, call):
             # algorithmic bytes: sum over vertices whose distance changed of
