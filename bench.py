@@ -722,13 +722,6 @@ def batched_compare(num_graphs, K, W, rank, world, local):
                           rounds=2)
     for i in range(1 + nt, Wb):
         br.step(both[i % 2])
-    if br.fusable:
-        # two fused steps (a batch and its inverse) warm the one-launch form
-        br.set_fused(True)
-        for i in range(Wb, Wb + 2):
-            br.step(both[i % 2])
-        br.set_fused(False)
-        Wb += 2
     br.query()
     chunk = tune_frontier_chunk(gs.graph, br.bfs) if br.bfs is not None else None
     for i in range(Wb):
@@ -755,33 +748,16 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         return g, cs
 
     clocks = Clocks(local)
-    # batched arm: K steps captured into one CUDA graph, replayed once; first
-    # the fused form (one launch per step) when every member fits one CTA,
-    # then the four-launch sequence over the next K steps (K is even, so both
-    # end on the same state of the cycle and give the same answers)
-    forms = (["fused"] if br.fusable else []) + ["sequence"]
-    form_ms, form_launches, answers = {}, {}, {}
-    i0 = Wb
-    for form in forms:
-        br.set_fused(form == "fused")
-        bg, bs = capture(lambda cs, a=i0: [br.step(both[i % 2], stream=cs) for i in range(a, a + K)])
-        barrier(world)
-        with torch.cuda.stream(bs):
-            form_ms[form] = timed(bg.replay) / K
-        assert gs.graph.sync() == 0
-        del bg
-        form_launches[form] = br.launches_per_step()
-        answers[form] = (br.bfs.Distances() if br.bfs is not None else None,
-                         br.wcc.Labels().astype(np.int64) if br.wcc is not None else None)
-        i0 += K
-    br.set_fused(False)
-    best = min(forms, key=lambda f: form_ms[f])
-    batched_ms = form_ms[best]
-    fused_equal = None
-    if "fused" in answers:
-        fa, sa = answers["fused"], answers["sequence"]
-        fused_equal = all(x is None or np.array_equal(x, y) for x, y in zip(fa, sa))
-        assert fused_equal, "fused and four-launch steps disagree"
+    # batched arm: K steps captured into one CUDA graph, replayed once
+    bg, bs = capture(lambda cs: [br.step(both[i % 2], stream=cs) for i in range(Wb, Wb + K)])
+    barrier(world)
+    with torch.cuda.stream(bs):
+        batched_ms = timed(bg.replay) / K
+    assert gs.graph.sync() == 0
+    del bg
+    d_union = br.bfs.Distances() if br.bfs is not None else None
+    l_union = br.wcc.Labels().astype(np.int64) if br.wcc is not None else None
+    i0 = Wb + K
     # plain arm, issued from the host: K steps
     barrier(world)
     plain_ms = timed(lambda: [pr.step(both_local[i % 2]) for i in range(Wb, Wb + K)]) / K
@@ -806,7 +782,6 @@ def batched_compare(num_graphs, K, W, rank, world, local):
 
     # every member's answer is the same in both arms
     mism = {"bfs": 0, "wcc": 0}
-    d_union, l_union = answers["sequence"]
     for m in range(Gn):
         lo, hi = int(voff[m]), int(voff[m + 1])
         a = pr.algos[m]
@@ -817,7 +792,7 @@ def batched_compare(num_graphs, K, W, rank, world, local):
     assert mism == {"bfs": 0, "wcc": 0}, mism
     # the oracle replays the sampled members' batches (a batch and its inverse
     # alternate, starting with the batch; every update the set received)
-    n_updates = i0 + 2  # warm-up and tuner steps, K timed steps per form, 2 phase-split steps
+    n_updates = i0 + 2  # warm-up and tuner steps, K timed steps, 2 phase-split steps
     host_local = {m: [tuple(x.cpu().numpy().view(np.uint32) for x in both_local[k][m])
                       for k in (0, 1)] for m in sample.tolist()}
     par = batched_oracle_check(sample, base_edges, host_local, n_updates, spec, srcs, voff,
@@ -843,9 +818,7 @@ def batched_compare(num_graphs, K, W, rank, world, local):
         "speedup_vs_plain": plain_ms / batched_ms,
         "speedup_vs_plain_cuda_graph": plain_graph_ms / batched_ms,
         "batched_ms_per_step": batched_ms, "plain_ms_per_step": plain_ms,
-        "batched_form": best,
-        "forms_ms_per_step": form_ms, "forms_launches_per_step": form_launches,
-        "fused_equals_sequence": fused_equal,
+
         "batched_phases_ms": phases,
         "plain_cuda_graph_ms_per_step": plain_graph_ms, "plain_capture_s": cap_s,
         "steps": K, "warmup": Wb,
@@ -857,7 +830,7 @@ def batched_compare(num_graphs, K, W, rank, world, local):
                 "alternate",
         "vertices": V, "edges": E, "updates_per_step": upd,
         "batched_updates_per_s": upd / (batched_ms / 1000.0),
-        "gpu_launches_per_step": form_launches[best],
+        "gpu_launches_per_step": br.launches_per_step(),
         "plain_launches_per_step": pr.launches_per_step(),
         "queries": {"bfs_members": int(len(br.bfs_members)), "wcc_members": int(len(br.wcc_members))},
         "tuning": {"updates": tuning["best"], "frontier_chunk": chunk["best"] if chunk else None},

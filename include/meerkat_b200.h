@@ -559,21 +559,9 @@ mk_status mk_set_runner_step(mk_set_runner *r, const uint32_t *d_del_src,
                              const uint32_t *d_del_dst, uint32_t n_del,
                              const uint32_t *d_ins_src, const uint32_t *d_ins_dst,
                              const uint32_t *d_ins_w, uint32_t n_ins, void *stream);
-/* Fused step (opt-in): with on != 0 every later step is ONE kernel launch.
- * A CTA takes a member (largest first), finds the member's slices of the
- * delete and insert arrays, applies its deletes, then its inserts, then
- * answers its query with the member's state in shared memory; the answers
- * and the graph are those of the four-launch step.  The batch arrays must
- * then be grouped by member in ascending member order (the layout
- * mk_gen_set_batches writes); an edge outside its member's slice is skipped
- * and sets MK_DEVERR_INVALID_ID.  After a step the graph's last update is
- * the insert batch (mk_graph_applied_count counts its applied inserts), as
- * after the four-launch step.  MK_ERR_INVALID when a member has more than
- * 65,535 vertices (the runner keeps the four-launch step). */
-mk_status mk_set_runner_set_fused(mk_set_runner *r, uint32_t on);
-/* Kernel launches one step issues: 1 fused; otherwise 2 plus one per query
- * kind present (members beyond one CTA's shared memory add the device-wide
- * kernels). */
+/* Kernel launches one step issues: 2 plus one per query kind present
+ * (members beyond one CTA's shared memory add the device-wide kernels, not
+ * counted here). */
 mk_status mk_set_runner_launches(mk_set_runner *r, uint32_t *h_launches);
 /* The runner's BFS and WCC handles (owned by the runner; NULL when no member
  * asks that query), for mk_traversal_distances / mk_wcc_labels. */

@@ -355,9 +355,6 @@ class GraphSetRunner {
   }
   GraphSetRunner(const GraphSetRunner &) = delete;
   ~GraphSetRunner() { mk_set_runner_destroy(r_); }
-  // One launch per step from now on (members of at most 65,535 vertices;
-  // batches grouped by member in member order); false: four launches.
-  void SetFused(bool on) { check(mk_set_runner_set_fused(r_, on ? 1u : 0u), "SetFused"); }
   uint32_t LaunchesPerStep() const {
     uint32_t n = 0;
     check(mk_set_runner_launches(r_, &n), "LaunchesPerStep");

@@ -794,13 +794,11 @@ class GraphSet:
 class SetRunner:
     """One query per member of a GraphSet (QUERY_BFS from a local source,
     QUERY_WCC, or QUERY_NONE) and a step that applies one update batch to
-    every member and answers every query (mk_set_runner_*).  The step is four
-    launches, or ONE with fused=True (members of at most 65,535 vertices;
-    batches grouped by member in member order, as GraphSet.gen_batches
-    writes them).  `bfs` / `wcc` are views of the runner's own handles for
-    reading the answers."""
+    every member and answers every query (mk_set_runner_*): four
+    asynchronous launches, capturable into a CUDA graph.  `bfs` / `wcc` are
+    views of the runner's own handles for reading the answers."""
 
-    def __init__(self, gs: "GraphSet", query, sources_local=None, fused: bool = False):
+    def __init__(self, gs: "GraphSet", query, sources_local=None):
         q = np.ascontiguousarray(np.asarray(query, dtype=np.uint8))
         if len(q) != gs.num_graphs:
             raise ValueError("one query kind per member")
@@ -822,13 +820,6 @@ class SetRunner:
         me = weakref.ref(self)
         self.bfs = BFS._borrow(bh, gs.graph, glob, me) if bh.value else None
         self.wcc = WCC._borrow(wh, gs.graph, me) if wh.value else None
-        self.fused = False
-        if fused:
-            self.set_fused(True)
-
-    def set_fused(self, on: bool) -> None:
-        check(lib().mk_set_runner_set_fused(self._h, int(bool(on))), "mk_set_runner_set_fused")
-        self.fused = bool(on)
 
     def launches_per_step(self) -> int:
         n = C.c_uint32(0)

@@ -140,7 +140,6 @@ SIGNATURES = [
     ("mk_set_runner_create", _S, [vp, vp, vp, C.POINTER(vp)]),
     ("mk_set_runner_step", _S, [vp, vp, vp, C.c_uint32, vp, vp, vp, C.c_uint32, vp]),
     ("mk_set_runner_results", _S, [vp, C.POINTER(vp), C.POINTER(vp)]),
-    ("mk_set_runner_set_fused", _S, [vp, C.c_uint32]),
     ("mk_set_runner_launches", _S, [vp, u32p]),
     ("mk_set_runner_handles", _S, [vp, C.POINTER(vp), C.POINTER(vp)]),
     ("mk_set_runner_destroy", _S, [vp]),

@@ -17,14 +17,10 @@ members in one GraphSet and issues, per step,
   one WCC launch over the WCC-queried members (a member of at most 65,536
   vertices is solved by one CTA with its union-find in shared memory),
 
-each member's results being those of the member alone.  When every member
-has at most 65,535 vertices the step can instead be ONE persistent launch
-(set_fused): a CTA takes a member, largest first, applies its deletes, then
-its inserts, then answers its query in shared memory, so the phases of
-different members overlap and no launch boundary or grid barrier separates
-them.  Either form can be captured into a CUDA graph and replayed; the
-autotuner picks the update kernel and the BFS frontier chunk of the
-four-launch form on the live set.  There is no counterpart in the reference.
+each member's results being those of the member alone.  The step can be
+captured into a CUDA graph and replayed; the autotuner picks the update
+kernel and the BFS frontier chunk on the live set.  There is no counterpart
+in the reference.
 """
 from __future__ import annotations
 
@@ -100,11 +96,10 @@ def pick_sources(degrees: np.ndarray, offsets: np.ndarray, members: Sequence[int
 
 
 class BatchedRunner:
-    """All members in one GraphSet; one coalesced launch sequence per step,
-    or one fused launch (set_fused) when every member fits one CTA."""
+    """All members in one GraphSet; one coalesced launch sequence per step
+    (the C set runner's, mk_set_runner_step)."""
 
-    def __init__(self, gs: GraphSet, query: np.ndarray, sources_local: np.ndarray,
-                 fused: bool = False):
+    def __init__(self, gs: GraphSet, query: np.ndarray, sources_local: np.ndarray):
         self.gs = gs
         self.G = gs.graph
         off = gs.offsets.astype(np.int64)
@@ -114,8 +109,8 @@ class BatchedRunner:
         self.sources_global = glob
         src_m = np.zeros(gs.num_graphs, dtype=np.uint32)
         src_m[self.bfs_members] = sources_local
-        # the C runner holds the member tables of both forms; bfs / wcc are
-        # views of its handles
+        # the C runner holds the member tables; bfs / wcc are views of its
+        # handles
         self.runner = SetRunner(gs, query, src_m)
         self.bfs = self.runner.bfs
         self.wcc = self.runner.wcc
@@ -123,16 +118,6 @@ class BatchedRunner:
         self._bfs_large = int((bsz > BFS_LOCAL_MAX).sum())
         sizes = off[self.wcc_members + 1] - off[self.wcc_members]
         self._wcc_large = int((sizes > WCC_LOCAL_MAX).sum())
-        self.fusable = int((off[1:] - off[:-1]).max()) <= BFS_LOCAL_MAX
-        self.fused = False
-        if fused:
-            self.set_fused(True)
-
-    def set_fused(self, on: bool) -> None:
-        """One launch per step (each member's deletes, inserts and query by
-        one CTA) instead of the four-launch sequence."""
-        self.runner.set_fused(on)
-        self.fused = bool(on)
 
     def update(self, ds, dd, is_, id_, iw, stream=None):
         self.G.DeleteEdges(ds, dd, stream=stream)
@@ -145,15 +130,9 @@ class BatchedRunner:
             self.wcc.StaticPrepared(stream=stream, timed=False)
 
     def step(self, batch, stream=None):
-        if self.fused:
-            self.runner.step(*batch, stream=stream)
-            return
-        self.update(*batch, stream=stream)
-        self.query(stream=stream)
+        self.runner.step(*batch, stream=stream)
 
     def launches_per_step(self) -> int:
-        if self.fused:
-            return 1
         # kernels: delete, insert; BFS: 1 shared-memory kernel (plus 2
         # memsets) and the cooperative device-wide kernel when some member is
         # larger than shared memory holds; WCC: 1 shared-memory kernel (plus 1

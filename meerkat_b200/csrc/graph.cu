@@ -1238,9 +1238,8 @@ mk_status mk_graph_sync(mk_graph *g, void *stream, uint32_t *h_deverr) {
   if (err & kErrOom) return fail(MK_ERR_OOM, "slab pool exhausted");
   if (err & kErrInvalidId)
     return fail(MK_ERR_INVALID,
-                "vertex id out of range: a batch id >= num_vertices, an edge leaving the "
-                "vertex range of a range call, or a fused graph-set step given a batch that "
-                "is not grouped by member");
+                "vertex id out of range: a batch id >= num_vertices, or an edge leaving the "
+                "vertex range of a range call");
   return MK_OK;
 }
 

@@ -84,13 +84,6 @@ __device__ __forceinline__ uint32_t bucket_of(uint32_t key, uint32_t nb) {
 // Read-only slab load for traversals (graph is not mutated during them).
 __device__ __forceinline__ uint4 ld_slab_ro(const uint4 *p) { return __ldg(p); }
 
-// Slab load for a kernel that also writes slabs (the fused graph-set step
-// updates a member, then walks it): through L2, never the non-coherent path.
-template <bool kCg>
-__device__ __forceinline__ uint4 ld_slab(const uint4 *p) {
-  return kCg ? __ldcg(p) : __ldg(p);
-}
-
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

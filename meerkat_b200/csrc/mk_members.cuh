@@ -1,7 +1,5 @@
 // Per-member solvers of a graph set, run by one whole CTA with the member's
-// state in shared memory.  The member kernels (one query kind per launch)
-// and the fused graph-set step (updates and queries of a member in one CTA)
-// both call them.
+// state in shared memory (one query kind per member kernel launch).
 //
 // bfs_member: static BFS of one vertex range from its source.  The member's
 // BFS state lives in shared memory -- a 16-bit parent per vertex (0xFFFF:
@@ -23,12 +21,6 @@
 // of the device-wide kernels (larger root under smaller, as the reference's
 // UnionAsync, include/Util/UnionFind.cuh:194-215), so labels are the minimum
 // vertex id of each component.
-//
-// kFused selects the loads of a kernel that updated the member's slabs and
-// degrees itself earlier in the same launch: slabs and degrees are read
-// through L2 (never the non-coherent path), and the BFS writes the
-// unreached vertices' words itself instead of relying on a reset before the
-// launch.
 #pragma once
 
 #include "mk_common.cuh"
@@ -73,19 +65,14 @@ __device__ __forceinline__ bool cas_min16_first(uint16_t *p, uint32_t v) {
   return false;
 }
 
-template <bool kFused>
-__device__ __forceinline__ uint32_t ld_deg(const GraphView &g, uint32_t v) {
-  return kFused ? __ldcg(g.deg + v) : g.deg[v];
-}
-
 // R = (first vertex, end vertex, first bucket, end bucket) of a range of at
 // most kMemLocalMax vertices, src its source (global id).  The range uses the
 // slices [R.z, R.w) of items (one word per bucket: a vertex's items never
 // exceed its buckets) and [R.x, R.y) of found (a vertex is reached once).
-// Without kFused, dist must already hold kInfInf for the range.  smem holds
+// dist must already hold kInfInf for the range.  smem holds
 // bfs_member_smem(n) bytes; s_nfound / s_nitems are CTA-shared words.  Ends
 // with the CTA synchronised.
-template <bool kW, bool kFused>
+template <bool kW>
 __device__ __forceinline__ void bfs_member(const GraphView &g, const Lanes &L, const uint4 R,
                                            uint32_t src, unsigned long long *__restrict__ dist,
                                            uint32_t *__restrict__ items,
@@ -117,7 +104,7 @@ __device__ __forceinline__ void bfs_member(const GraphView &g, const Lanes &L, c
       const uint32_t v = fl[i], gv = lo + v;
       dist[gv] = pack(level, lo + par[v]);
       atomicOr(vis + (v >> 5), 1u << (v & 31));
-      if (ld_deg<kFused>(g, gv) == 0) continue;
+      if (g.deg[gv] == 0) continue;
       const uint32_t nb = g.boff[gv + 1] - g.boff[gv];
       const uint32_t cs = mem_chunk(nb), nc = (nb + cs - 1) / cs;
       const uint32_t pos = atomicAdd(&s_nitems, nc);
@@ -148,16 +135,11 @@ __device__ __forceinline__ void bfs_member(const GraphView &g, const Lanes &L, c
         }
       };
       for (uint32_t b = bb; b < be; b += kMemChunk)
-        walk4_levels<kFused>(g, L, b, min(kMemChunk, be - b),
-                             [&](uint32_t, const uint4 x) { relax(x); });
+        walk4_levels(g, L, b, min(kMemChunk, be - b), [&](uint32_t, const uint4 x) { relax(x); });
     }
     fbeg = fend;
     ibeg = iend;
     __syncthreads();
-  }
-  if (kFused) {
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
-      if (!((vis[i >> 5] >> (i & 31)) & 1u)) dist[lo + i] = kInfInf;
   }
   __syncthreads();
 }
@@ -201,7 +183,7 @@ __device__ __forceinline__ void ls_union(uint16_t *p, uint32_t a, uint32_t b, ui
 // component.  A key outside the range (a range that is not closed under
 // edges) is skipped and reported as MK_DEVERR_INVALID_ID.  sp holds
 // uf_member_smem(n) bytes.  Ends with the CTA synchronised.
-template <bool kW, bool kFused>
+template <bool kW>
 __device__ __forceinline__ void uf_member(const GraphView &g, const Lanes &L, const uint4 R,
                                           uint32_t *__restrict__ labels, uint32_t *err,
                                           uint16_t *sp) {
@@ -214,7 +196,7 @@ __device__ __forceinline__ void uf_member(const GraphView &g, const Lanes &L, co
     uint32_t own[kMemberHeads];
 #pragma unroll
     for (uint32_t j = 0; j < kMemberHeads; ++j) own[j] = j < m ? __ldg(g.bowner + b + j) - lo : 0u;
-    walk4_levels<kFused>(g, L, b, m, [&](uint32_t j, const uint4 x) {
+    walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 x) {
       const uint32_t u = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
       uint32_t k[4], w[4];
       lane_keys<kW>(x, L.gl, k, w);

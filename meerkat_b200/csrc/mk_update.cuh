@@ -1,5 +1,5 @@
-// Thread-per-edge slab updates, shared by the device-wide update kernels and
-// the fused graph-set step.  A lane loads its edge's whole head slab with 8
+// Thread-per-edge slab probes and updates, shared by the update kernels and
+// the connected-components edge probe.  A lane loads its edge's whole head slab with 8
 // independent 16-byte loads (through L2: other SMs write the same slabs),
 // decides alone (no cross-lane synchronisation) and commits with one CAS;
 // a chain that continues, a lost race or a full slab is walked by the same

@@ -206,7 +206,7 @@ __global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bi
 // ctl words (u64) of one decremental call.
 enum : int {
   kFDead = 0,       // forest edges the batch removed for good
-  kFNmCount = 1,    // vertices outside their component's main piece (list length)
+  kFNmCount = 1,    // vertices outside their component's main piece
   kFNmEnds = 2,     // their out- plus in-degrees
   kFEdges = 3,      // live edges of the graph
   kFMainLabel = 4,  // old label + 1 of the component whose main piece was sampled (0: none)
@@ -388,16 +388,17 @@ __global__ void __launch_bounds__(kMainThreads)
   }
 }
 
-// Step 3b (after compressing the affected vertices): the affected vertices
-// outside their component's main piece, listed, counted with their out- plus
-// in-degrees; and the graph's live edge count.
+// Step 3b (after compressing the affected vertices): the bitmap of the
+// affected vertices outside their component's main piece (whole words, one
+// ballot each), their count and out- plus in-degrees, and the graph's live
+// edge count.
 __global__ void k_fe_nonmain(const uint32_t *p, const uint32_t *oldlab, uint32_t V,
                              const uint32_t *aff_vertices, const uint32_t *deg,
-                             const uint32_t *rdeg, uint32_t *nm_list, unsigned long long *ctl) {
+                             const uint32_t *rdeg, uint32_t *nm_bits, unsigned long long *ctl) {
   const uint32_t words = (V + 31) / 32, lane = threadIdx.x & 31u;
   const uint32_t stride = gridDim.x * blockDim.x;
   const unsigned long long ml = ctl[kFMainLabel], mp = ctl[kFMainPiece];
-  unsigned long long ends = 0, edges = 0;
+  unsigned long long ends = 0, edges = 0, count = 0;
   for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < words * 32u;
        base += stride) {
     const uint32_t x = base + lane;
@@ -409,61 +410,52 @@ __global__ void k_fe_nonmain(const uint32_t *p, const uint32_t *oldlab, uint32_t
         const uint32_t r = oldlab[x];
         const uint32_t main_piece = (ml && r == ml - 1) ? (uint32_t)(mp - 1) : __ldcg(p + r);
         nm = __ldcg(p + x) != main_piece;
-        if (nm) ends += d + rdeg[x];
+        if (nm) {
+          ends += d + rdeg[x];
+          ++count;
+        }
       }
     }
-    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, nm);
-    if (bal) {
-      uint32_t pos = 0;
-      if (lane == 0) pos = (uint32_t)atomicAdd(ctl + kFNmCount, (unsigned long long)__popc(bal));
-      pos = __shfl_sync(0xFFFFFFFFu, pos, 0);
-      if (nm) nm_list[pos + __popc(bal & ((1u << lane) - 1u))] = x;
-    }
+    const uint32_t word = __ballot_sync(0xFFFFFFFFu, nm);
+    if (lane == 0) nm_bits[base >> 5] = word;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     ends += __shfl_xor_sync(0xFFFFFFFFu, ends, o);
     edges += __shfl_xor_sync(0xFFFFFFFFu, edges, o);
+    count += __shfl_xor_sync(0xFFFFFFFFu, count, o);
   }
   if (lane == 0) {
+    if (count) atomicAdd(ctl + kFNmCount, count);
     if (ends) atomicAdd(ctl + kFNmEnds, ends);
     if (edges) atomicAdd(ctl + kFEdges, edges);
   }
 }
 
-// Step 3c: out-edges (g) and in-edges (gr, the reverse graph) of the listed
-// vertices, one 8-lane group per vertex; an edge between two sets is a union
-// recorded in the forest.
-template <bool kW, bool kRW>
-__global__ void k_fe_scan(GraphView g, GraphView gr, uint32_t *p, unsigned long long *fe,
-                          const uint32_t *nm_list, const unsigned long long *ctl, uint32_t *err) {
+// Step 3c, in-edges: every bucket of the reverse graph gr whose owner x is
+// outside its main piece (bit set), one 8-lane group per bucket; a key y is
+// the slab edge y -> x of the graph, unioned and recorded when y and x are
+// in different sets.  (The out-edges go through k_uf_edges_skip with the
+// same bitmap.)
+template <bool kRW>
+__global__ void k_fe_scan_in(GraphView gr, uint32_t *p, const uint32_t *nm_bits, uint32_t *err,
+                             unsigned long long *fe) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  const uint32_t n = (uint32_t)ctl[kFNmCount];
-  for (uint32_t i = group; i < n; i += ngroups) {
-    const uint32_t x = nm_list[i];
+  for (uint32_t b = group; b < gr.nbuckets; b += ngroups) {
+    const uint32_t x = gr.bowner[b];
+    if (!((nm_bits[x >> 5] >> (x & 31)) & 1u) || gr.deg[x] == 0) continue;
     const uint32_t px = __ldcg(p + x);
-    walk_buckets(g, L, g.boff[x], g.boff[x + 1], [&](const uint4 &q) {
-      uint32_t k[4], w[4];
-      lane_keys<kW>(q, L.gl, k, w);
-#pragma unroll
-      for (int j = 0; j < keys_per_lane<kW>(); ++j) {
-        const uint32_t y = k[j];
-        if (y >= kTombKey || y == x || y >= g.V) continue;
-        if (__ldcg(p + y) == px) continue;
-        uf_union(p, x, y, err, fe);
-      }
-    });
-    walk_buckets(gr, L, gr.boff[x], gr.boff[x + 1], [&](const uint4 &q) {
+    walk_bucket(gr, L, b, [&](const uint4 &q) {
       uint32_t k[4], w[4];
       lane_keys<kRW>(q, L.gl, k, w);
 #pragma unroll
       for (int j = 0; j < keys_per_lane<kRW>(); ++j) {
         const uint32_t y = k[j];
-        if (y >= kTombKey || y == x || y >= g.V) continue;
+        if (y >= kTombKey || y == x || y >= gr.V) continue;
         if (__ldcg(p + y) == px) continue;
-        uf_union(p, y, x, err, fe);  // the slab edge y -> x of g
+        uf_union(p, y, x, err, fe);
       }
     });
   }
@@ -549,7 +541,7 @@ __global__ void __launch_bounds__(kMemThreads, 1)
     __syncthreads();
     const uint32_t r = s_range;
     if (r >= nr) break;
-    uf_member<kW, false>(g, L, rng[r], labels, err, sp);
+    uf_member<kW>(g, L, rng[r], labels, err, sp);
   }
 }
 
@@ -571,7 +563,7 @@ struct mk_wcc {
   // edges, vertices outside the main pieces, ctl words
   DevBuf<unsigned long long> dtab;
   DevBuf<unsigned long long> fe2;
-  DevBuf<uint32_t> oldlab, nm_list;
+  DevBuf<uint32_t> oldlab, nm_bits;
   unsigned long long *fctl = nullptr;
   // last decremental call: forest edges lost, vertices rescanned, path taken
   uint64_t last_dead = 0, last_rescanned = 0;
@@ -664,7 +656,7 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   }
   MK_CHECK(w->fe2.reserve(V, &g->device_bytes));
   MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));
-  MK_CHECK(w->nm_list.reserve(V, &g->device_bytes));
+  MK_CHECK(w->nm_bits.reserve(words, &g->device_bytes));
   k_fe_collect<<<fg, 256, 0, s>>>(w->parent, w->fe, w->fe2.ptr, V, w->aff_labels, w->oldlab.ptr,
                                   w->aff_vertices);
   k_fe_union<<<fg, 256, 0, s>>>(w->parent, w->fe, w->fe2.ptr, V, w->aff_vertices, w->err);
@@ -672,7 +664,7 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   k_fe_main_sample<<<1, kMainThreads, 0, s>>>(w->parent, w->oldlab.ptr, w->aff_vertices, V,
                                               0x5EED0000ull + (++w->calls), w->fctl);
   k_fe_nonmain<<<fg, 256, 0, s>>>(w->parent, w->oldlab.ptr, V, w->aff_vertices, g->deg,
-                                  w->rev->deg, w->nm_list.ptr, w->fctl);
+                                  w->rev->deg, w->nm_bits.ptr, w->fctl);
   MK_CUDA(cudaGetLastError());
   MK_CUDA(cudaMemcpyAsync(h, w->fctl, sizeof(h), cudaMemcpyDeviceToHost, s));
   MK_CUDA(cudaStreamSynchronize(s));
@@ -685,17 +677,20 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   w->last_path = 1;
   w->last_rescanned = h[kFNmCount];
   if (h[kFNmCount]) {
-    const int blocks = (int)std::min<uint64_t>(h[kFNmCount] * 8 / 256 + 1,
-                                               (uint64_t)device_sm_count(g->device) * 8);
+    // bucket-parallel: a hub outside its main piece spreads over many groups
     const GraphView rv = w->rev->view();
-    if (g->weighted && w->rev->weighted)
-      k_fe_scan<true, true><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
-    else if (g->weighted)
-      k_fe_scan<true, false><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
-    else if (w->rev->weighted)
-      k_fe_scan<false, true><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
+    const int ob = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1,
+                                           (uint64_t)device_sm_count(g->device) * 8);
+    const int ib = (int)std::min<uint64_t>(w->rev->num_buckets * 8 / 256 + 1,
+                                           (uint64_t)device_sm_count(g->device) * 8);
+    if (g->weighted)
+      k_uf_edges_skip<true><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->err, w->fe);
     else
-      k_fe_scan<false, false><<<blocks, 256, 0, s>>>(v, rv, w->parent, w->fe, w->nm_list.ptr, w->fctl, w->err);
+      k_uf_edges_skip<false><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->err, w->fe);
+    if (w->rev->weighted)
+      k_fe_scan_in<true><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->err, w->fe);
+    else
+      k_fe_scan_in<false><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->err, w->fe);
     k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices);
   }
   MK_CUDA(cudaGetLastError());
@@ -706,10 +701,6 @@ static bool batch_matches(const mk_graph *g, const uint32_t *d_src, const uint32
                           uint32_t n, int op) {
   return n == g->last_n && d_src == g->last_src && d_dst == g->last_dst && g->last_op == op;
 }
-
-namespace mk {
-uint32_t *wcc_label_buf(mk_wcc *w) { return w ? w->parent : nullptr; }
-}  // namespace mk
 
 extern "C" {
 
@@ -972,7 +963,7 @@ mk_status mk_wcc_destroy(mk_wcc *w) {
   w->dtab.release();
   w->fe2.release();
   w->oldlab.release();
-  w->nm_list.release();
+  w->nm_bits.release();
   w->staging.release();
   w->ranges.release();
   delete w;

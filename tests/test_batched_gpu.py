@@ -115,25 +115,25 @@ def check_step(spec, batch, voff, oracles, gs, br, src_of, pr=None, plain=()):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("capture,weighted", [(False, True), (True, True), (False, False)])
-def test_fused_step_matches_oracle(capture, weighted):
-    """The one-launch step (each member's deletes, inserts and query by one
-    CTA): every member's answer and degrees equal the oracle's after each
-    step, issued directly or captured into a CUDA graph, and the applied
-    insert count is published as after the four-launch step."""
+@pytest.mark.parametrize("capture,weighted", [(False, False), (True, True), (True, False)])
+def test_runner_step_matches_oracle(capture, weighted):
+    """The whole batched step through the C set runner (mk_set_runner_step:
+    both update kernels and both member queries), issued directly or
+    captured into a CUDA graph and replayed: every member's answer and the
+    set's degrees equal the oracle's after each step, on weighted and
+    unweighted sets."""
     import torch
     spec = B.make_spec(48, seed=12, v_lo=32, v_hi=700, deg_lo=2, deg_hi=12, upd_lo=0.05,
                        upd_hi=0.3)
     gs, _, oracles, voff = build(spec, "cuda:0", weighted=weighted)
     bfs_members = np.flatnonzero(spec.query == B.QUERY_BFS)
     srcs = B.pick_sources(gs.graph.degrees(), voff, bfs_members, seed=4)
-    br = B.BatchedRunner(gs, spec.query, srcs, fused=True)
-    assert br.fusable and br.launches_per_step() == 1
-    gs.graph.reserve_batch(int(spec.inserts.sum()))
+    br = B.BatchedRunner(gs, spec.query, srcs)
+    assert br.launches_per_step() == br.runner.launches_per_step() == 4
+    gs.graph.reserve_batch(int(max(spec.inserts.sum(), spec.deletes.sum())))
     src_of = dict(zip(bfs_members.tolist(), srcs.tolist()))
     for step in range(3):
         batch = gs.gen_batches(spec.deletes, spec.inserts, seed=200 + step, weights=weighted)
-        edges_before = sum(O.num_edges() for O in oracles)
         if capture:
             s = torch.cuda.Stream()
             s.wait_stream(torch.cuda.current_stream())
@@ -146,36 +146,7 @@ def test_fused_step_matches_oracle(capture, weighted):
             del g
         else:
             br.step(batch)
-        torch.cuda.synchronize()
-        deleted = int(spec.deletes.sum())
         check_step(spec, batch, voff, oracles, gs, br, src_of)
-        edges_after = sum(O.num_edges() for O in oracles)
-        # inserts applied = growth + deletes applied; deletes of live edges
-        # are all applied unless a member's batch names one edge twice
-        assert gs.graph.last_applied() <= int(spec.inserts.sum())
-        assert gs.graph.last_applied() >= edges_after - edges_before
-    br.close()
-    gs.close()
-
-
-@pytest.mark.gpu
-def test_fused_step_reports_a_batch_not_grouped_by_member():
-    """An insert batch in shuffled order: the fused step skips the edges
-    outside their member's slice and reports MK_DEVERR_INVALID_ID; every
-    access stays inside the batch and the member's ranges."""
-    import torch
-    spec = B.make_spec(16, seed=13, v_lo=64, v_hi=300, deg_lo=2, deg_hi=8, upd_lo=0.1,
-                       upd_hi=0.2)
-    gs, _, _, voff = build(spec, "cuda:0")
-    bfs_members = np.flatnonzero(spec.query == B.QUERY_BFS)
-    srcs = B.pick_sources(gs.graph.degrees(), voff, bfs_members, seed=5)
-    br = B.BatchedRunner(gs, spec.query, srcs, fused=True)
-    ds, dd, is_, id_, iw = gs.gen_batches(spec.deletes, spec.inserts, seed=300)
-    perm = torch.randperm(is_.numel(), generator=torch.Generator().manual_seed(1)).cuda()
-    br.step((ds, dd, is_[perm].contiguous(), id_[perm].contiguous(), iw[perm].contiguous()))
-    torch.cuda.synchronize()
-    with pytest.raises(mk.MeerkatError, match="not grouped by member"):
-        gs.graph.sync()
     br.close()
     gs.close()
 
