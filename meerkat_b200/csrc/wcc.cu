@@ -919,10 +919,23 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d
 
 mk_status mk_wcc_set_reverse(mk_wcc *w, mk_graph *g_rev) {
   if (!w) return fail(MK_ERR_INVALID, "mk_wcc_set_reverse: null handle");
-  if (g_rev && (g_rev->V != w->g->V || g_rev->device != w->g->device || g_rev->reverse == w->g->reverse))
+  mk_graph *g = w->g;
+  if (g_rev && (g_rev->V != g->V || g_rev->device != g->device || g_rev->reverse == g->reverse))
     return fail(MK_ERR_INVALID,
                 "mk_wcc_set_reverse: need the reverse graph of the same vertices on the same device");
   w->rev = g_rev;
+  if (g_rev) {
+    // the piece-rescan scratch, and a batch set sized for the graph's batch
+    // scratch, allocated here rather than inside a timed decremental call
+    DeviceGuard dg(g->device);
+    const size_t V = g->V, words = (V + 31) / 32;
+    MK_CHECK(w->fe2.reserve(V, &g->device_bytes));
+    MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));
+    MK_CHECK(w->nm_bits.reserve(words, &g->device_bytes));
+    uint64_t cap = 1024;
+    while (cap < 2ull * std::min<uint64_t>(g->applied.cap, g->V)) cap <<= 1;
+    MK_CHECK(w->dtab.reserve(cap, &g->device_bytes));
+  }
   return MK_OK;
 }
 
