@@ -463,7 +463,9 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src,
  *     a reverse graph) in-edges of the other pieces' vertices;
  *   - rebuilds the affected components from their out-edges when no reverse
  *     graph is attached or the split-off pieces hold more than half of the
- *     graph's edge ends.
+ *     graph's edge ends (the whole graph by the static passes when the
+ *     affected components hold most of its vertices); after such a call a
+ *     batch that cuts at least half as many forest edges skips the split.
  * After mk_wcc_static_ranges / _prepared (which keep no forest) the next
  * decremental call is a full static pass.  The labels are the same on every
  * path.  The decremental call synchronises its stream (it picks the path on
@@ -472,7 +474,8 @@ mk_status mk_wcc_set_reverse(mk_wcc *w, mk_graph *g_rev);
 /* The last decremental call: forest edges it removed, vertices rescanned
  * outside their component's main piece, and its path: 0 no forest edge lost,
  * 1 rescan of the split-off pieces, 2 rebuild of the affected components,
- * 3 full static pass. */
+ * 3 full static pass (the affected components hold most of the vertices, or
+ * no forest was kept). */
 mk_status mk_wcc_decremental_stats(mk_wcc *w, uint64_t *h_dead_forest_edges,
                                    uint64_t *h_rescanned_vertices, uint32_t *h_path);
 /* N labels: the minimum vertex id of each vertex's component (host). */

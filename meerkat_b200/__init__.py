@@ -667,7 +667,8 @@ class WCC(_Timed):
     def decremental_stats(self):
         """(forest edges removed, vertices rescanned, path) of the last
         Decremental call; path 0 no forest edge lost, 1 rescan of the
-        split-off pieces, 2 rebuild of the affected components, 3 full static."""
+        split-off pieces, 2 rebuild of the affected components, 3 full static
+        pass (the affected components hold most vertices, or no forest)."""
         dead = C.c_uint64(0)
         res = C.c_uint64(0)
         path = C.c_uint32(0)

@@ -211,7 +211,8 @@ enum : int {
   kFEdges = 3,      // live edges of the graph
   kFMainLabel = 4,  // old label + 1 of the component whose main piece was sampled (0: none)
   kFMainPiece = 5,  // that main piece's root + 1
-  kFCtlWords = 6
+  kFAffected = 6,   // vertices of the affected components
+  kFCtlWords = 7
 };
 
 // Set of the batch's deleted edges (slab orientation a << 32 | b): open
@@ -294,6 +295,20 @@ __global__ void k_fe_dead(GraphView g, unsigned long long *fe, const unsigned lo
     atomicOr(aff_labels + (r >> 5), 1u << (r & 31));
     atomicAdd(ctl + kFDead, 1ull);
   }
+}
+
+// Step 1b: vertices of the affected components (labels still compressed),
+// one atomic per warp.
+__global__ void k_fe_count_aff(const uint32_t *p, uint32_t V, const uint32_t *aff_labels,
+                               unsigned long long *ctl) {
+  unsigned long long n = 0;
+  for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < V; x += gridDim.x * blockDim.x) {
+    const uint32_t r = p[x];
+    n += (aff_labels[r >> 5] >> (r & 31)) & 1u;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+  if ((threadIdx.x & 31u) == 0 && n) atomicAdd(ctl + kFAffected, n);
 }
 
 // Step 2a: every vertex of an affected component keeps its old label, is
@@ -569,6 +584,7 @@ struct mk_wcc {
   uint64_t last_dead = 0, last_rescanned = 0;
   uint32_t last_path = 0;
   uint64_t calls = 0;  // decremental calls (seeds the main-piece sample)
+  uint64_t fell_back_dead = 0;  // forest edges lost by the last call whose pieces were too large
   // prepared range table: counter word, then uint4 (lo, hi, b0, b1) per small
   // range (largest first), then vpre, vbase, bpre, bbase of the large ranges
   DevBuf<uint32_t> ranges;
@@ -637,6 +653,7 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
     k_fe_dead<true><<<fg, 256, 0, s>>>(v, w->fe, w->dtab.ptr, cap - 1, w->parent, w->aff_labels, w->fctl);
   else
     k_fe_dead<false><<<fg, 256, 0, s>>>(v, w->fe, w->dtab.ptr, cap - 1, w->parent, w->aff_labels, w->fctl);
+  k_fe_count_aff<<<fg, 256, 0, s>>>(w->parent, V, w->aff_labels, w->fctl);
   MK_CUDA(cudaGetLastError());
   unsigned long long h[kFCtlWords] = {};
   MK_CUDA(cudaMemcpyAsync(h, w->fctl, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -647,13 +664,23 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
     w->last_path = 0;  // the forest still spans every component: labels stand
     return MK_OK;
   }
-  if (!w->rev) {
-    // reset the affected components (forest slots too) and relink them
+  const bool most = 2 * h[kFAffected] > V;
+  // without a rescan: the affected components rebuilt from their out-edges,
+  // or the whole graph when they hold most of it (the same passes without the
+  // per-vertex selection)
+  auto rebuild = [&]() -> mk_status {
+    if (most) {
+      w->last_path = 3;
+      return wcc_static(w, s);
+    }
     MK_CUDA(cudaMemsetAsync(w->aff_vertices, 0, words * 4, s));
     k_uf_reset<<<fg, 256, 0, s>>>(w->parent, V, w->aff_labels, w->aff_vertices, w->fe);
     w->last_path = 2;
     return wcc_link(w, w->aff_vertices, s);
-  }
+  };
+  // the last call's pieces were too large to rescan and this batch cuts at
+  // least half as many forest edges: skip the split
+  if (!w->rev || (w->fell_back_dead && 2 * h[kFDead] >= w->fell_back_dead)) return rebuild();
   MK_CHECK(w->fe2.reserve(V, &g->device_bytes));
   MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));
   MK_CHECK(w->nm_bits.reserve(words, &g->device_bytes));
@@ -669,11 +696,17 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   MK_CUDA(cudaMemcpyAsync(h, w->fctl, sizeof(h), cudaMemcpyDeviceToHost, s));
   MK_CUDA(cudaStreamSynchronize(s));
   if (2 * h[kFNmEnds] > h[kFEdges]) {
-    // the split-off pieces hold most of the graph: relink from scratch
-    k_uf_init<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices, w->fe);
+    // the split-off pieces hold most of the graph's edge ends
+    w->fell_back_dead = h[kFDead];
+    if (!most) k_uf_init<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices, w->fe);
+    if (most) {
+      w->last_path = 3;
+      return wcc_static(w, s);
+    }
     w->last_path = 2;
     return wcc_link(w, w->aff_vertices, s);
   }
+  w->fell_back_dead = 0;
   w->last_path = 1;
   w->last_rescanned = h[kFNmCount];
   if (h[kFNmCount]) {
