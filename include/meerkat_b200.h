@@ -464,8 +464,10 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src,
  *   - rebuilds the affected components from their out-edges when no reverse
  *     graph is attached or the split-off pieces hold more than half of the
  *     graph's edge ends (the whole graph by the static passes when the
- *     affected components hold most of its vertices); after such a call a
- *     batch that cuts at least half as many forest edges skips the split.
+ *     affected components hold most of its vertices).  After a split whose
+ *     pieces were too large, the next calls run the static passes directly
+ *     (1, then 2, 4, up to 8 calls after each further such split; a rescan
+ *     that succeeds resets this).
  * After mk_wcc_static_ranges / _prepared (which keep no forest) the next
  * decremental call is a full static pass.  The labels are the same on every
  * path.  The decremental call synchronises its stream (it picks the path on

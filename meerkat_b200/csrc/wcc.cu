@@ -584,7 +584,10 @@ struct mk_wcc {
   uint64_t last_dead = 0, last_rescanned = 0;
   uint32_t last_path = 0;
   uint64_t calls = 0;  // decremental calls (seeds the main-piece sample)
-  uint64_t fell_back_dead = 0;  // forest edges lost by the last call whose pieces were too large
+  // after a split whose pieces were too large to rescan, the next calls go
+  // straight to the static passes: skip_left of them, doubling (to 8) with
+  // every further such split, reset by a rescan that succeeds
+  uint32_t skip_left = 0, skip_next = 0;
   // prepared range table: counter word, then uint4 (lo, hi, b0, b1) per small
   // range (largest first), then vpre, vbase, bpre, bbase of the large ranges
   DevBuf<uint32_t> ranges;
@@ -678,9 +681,7 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
     w->last_path = 2;
     return wcc_link(w, w->aff_vertices, s);
   };
-  // the last call's pieces were too large to rescan and this batch cuts at
-  // least half as many forest edges: skip the split
-  if (!w->rev || (w->fell_back_dead && 2 * h[kFDead] >= w->fell_back_dead)) return rebuild();
+  if (!w->rev) return rebuild();
   MK_CHECK(w->fe2.reserve(V, &g->device_bytes));
   MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));
   MK_CHECK(w->nm_bits.reserve(words, &g->device_bytes));
@@ -697,7 +698,8 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   MK_CUDA(cudaStreamSynchronize(s));
   if (2 * h[kFNmEnds] > h[kFEdges]) {
     // the split-off pieces hold most of the graph's edge ends
-    w->fell_back_dead = h[kFDead];
+    w->skip_next = std::min<uint32_t>(w->skip_next ? 2 * w->skip_next : 1, 8);
+    w->skip_left = w->skip_next;
     if (!most) k_uf_init<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices, w->fe);
     if (most) {
       w->last_path = 3;
@@ -706,7 +708,7 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
     w->last_path = 2;
     return wcc_link(w, w->aff_vertices, s);
   }
-  w->fell_back_dead = 0;
+  w->skip_next = 0;
   w->last_path = 1;
   w->last_rescanned = h[kFNmCount];
   if (h[kFNmCount]) {
@@ -941,7 +943,8 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d
   MK_CHECK(w->timer.start(s, ms_out != nullptr));
   w->last_dead = w->last_rescanned = 0;
   w->last_path = 0;
-  if (!batch_matches(g, d_src, d_dst, n, 2) || !w->forest_valid) {
+  if (!batch_matches(g, d_src, d_dst, n, 2) || !w->forest_valid || (n && w->rev && w->skip_left)) {
+    if (w->skip_left) --w->skip_left;
     MK_CHECK(wcc_static(w, s));
     w->last_path = 3;
   } else if (n) {
