@@ -155,16 +155,38 @@ __global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, 
 // edges cost two reads instead of two finds and a CAS.  Skipping only edges
 // between vertices already connected keeps the result exact, and it works for
 // every component at once (the members of a graph set included).
+// Sampled linking: each selected vertex (all if sel_bits is null) unions
+// with the first two keys of its first head slab.  A thread takes 4 vertices
+// a stride apart per round, so their degree, offset and slab reads are in
+// flight together before the unions.
 template <bool kW>
 __global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err,
                             unsigned long long *fe) {
-  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.V; u += gridDim.x * blockDim.x) {
-    if (g.deg[u] == 0) continue;
-    if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
-    const uint32_t *w = reinterpret_cast<const uint32_t *>(g.slabs + 8ull * g.boff[u]);
-    const uint32_t k0 = w[0], k1 = kW ? w[2] : w[1];
-    if (k0 < kTombKey && k0 != u) uf_union(p, u, k0, err, fe);
-    if (k1 < kTombKey && k1 != u) uf_union(p, u, k1, err, fe);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint64_t u0 = blockIdx.x * blockDim.x + threadIdx.x; u0 < g.V; u0 += 4ull * stride) {
+    uint32_t uu[4], k0[4], k1[4];
+    bool ok[4];
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      const uint64_t u = u0 + (uint64_t)j * stride;
+      uu[j] = (uint32_t)u;
+      ok[j] = u < g.V && g.deg[u] != 0 &&
+              (!sel_bits || ((sel_bits[uu[j] >> 5] >> (uu[j] & 31)) & 1u));
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      k0[j] = k1[j] = kEmptyKey;
+      if (ok[j]) {
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(g.slabs + 8ull * g.boff[uu[j]]);
+        k0[j] = w[0];
+        k1[j] = kW ? w[2] : w[1];
+      }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      if (k0[j] < kTombKey && k0[j] != uu[j]) uf_union(p, uu[j], k0[j], err, fe);
+      if (k1[j] < kTombKey && k1[j] != uu[j]) uf_union(p, uu[j], k1[j], err, fe);
+    }
   }
 }
 
@@ -188,17 +210,45 @@ __device__ __forceinline__ void link_bucket_skip(const GraphView &g, const Lanes
   });
 }
 
+// Every selected bucket (owner's bit set, all if sel_bits is null): unions of
+// the out-edges whose endpoints do not share a parent yet.  A group takes 4
+// consecutive buckets at a time: their owners' parents and head slabs are
+// loaded together, chains are followed level by level, and a lane loads the
+// parents of all its keys before comparing, so one group keeps several
+// reads in flight instead of one dependent read per key.
 template <bool kW>
 __global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err,
                                 unsigned long long *fe) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t b = group; b < g.nbuckets; b += ngroups) {
-    const uint32_t u = g.bowner[b];
-    if (g.deg[u] == 0) continue;
-    if (sel_bits && !((sel_bits[u >> 5] >> (u & 31)) & 1u)) continue;
-    link_bucket_skip<kW>(g, L, p, b, u, err, fe);
+  for (uint64_t b0 = (uint64_t)group * 4; b0 < g.nbuckets; b0 += (uint64_t)ngroups * 4) {
+    const uint32_t b = (uint32_t)b0, m = min(4u, g.nbuckets - b);
+    uint32_t own[4], pu[4], live = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      own[j] = j < m ? __ldg(g.bowner + b + j) : 0u;
+      const bool ok = j < m && g.deg[own[j]] != 0 &&
+                      (!sel_bits || ((sel_bits[own[j] >> 5] >> (own[j] & 31)) & 1u));
+      live |= (ok ? 1u : 0u) << j;
+    }
+    if (!live) continue;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) pu[j] = ((live >> j) & 1u) ? __ldcg(p + own[j]) : 0u;
+    walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 q) {
+      if (!((live >> j) & 1u)) return;
+      const uint32_t u = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
+      const uint32_t pj = pu[0] * (j == 0) + pu[1] * (j == 1) + pu[2] * (j == 2) + pu[3] * (j == 3);
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+      uint32_t pv[4];
+#pragma unroll
+      for (int t = 0; t < keys_per_lane<kW>(); ++t)
+        pv[t] = (k[t] < kTombKey && k[t] != u) ? __ldcg(p + k[t]) : pj;
+#pragma unroll
+      for (int t = 0; t < keys_per_lane<kW>(); ++t)
+        if (pv[t] != pj) uf_union(p, u, k[t], err, fe);
+    });
   }
 }
 
@@ -447,30 +497,70 @@ __global__ void k_fe_nonmain(const uint32_t *p, const uint32_t *oldlab, uint32_t
   }
 }
 
-// Step 3c, in-edges: every bucket of the reverse graph gr whose owner x is
-// outside its main piece (bit set), one 8-lane group per bucket; a key y is
-// the slab edge y -> x of the graph, unioned and recorded when y and x are
-// in different sets.  (The out-edges go through k_uf_edges_skip with the
-// same bitmap.)
-template <bool kRW>
-__global__ void k_fe_scan_in(GraphView gr, uint32_t *p, const uint32_t *nm_bits, uint32_t *err,
-                             unsigned long long *fe) {
+// True once x's set holds its component's main piece: its root is the
+// main piece's (the sampled piece for the sampled component, else the piece
+// of the old label).  The rescan skips such a vertex's remaining buckets:
+// any piece still joined through x finds the edge from its own side.
+__device__ __forceinline__ bool fe_joined(uint32_t *p, const uint32_t *oldlab, uint32_t x,
+                                          unsigned long long ml, unsigned long long mp) {
+  const uint32_t r = __ldg(oldlab + x);
+  const uint32_t m = (ml && r == ml - 1) ? (uint32_t)(mp - 1) : r;
+  return uf_find(p, x) == uf_find(p, m);
+}
+
+// Step 3c: every bucket of the graph (kIn: of the reverse graph, whose key y
+// is the graph edge y -> x) whose owner x is outside its main piece (bit
+// set) and not yet joined to it; an edge between two sets is a union
+// recorded in the forest.  Groups take 4 buckets at a time as in
+// k_uf_edges_skip.
+template <bool kW, bool kIn>
+__global__ void k_fe_scan(GraphView g, uint32_t *p, const uint32_t *nm_bits,
+                          const uint32_t *oldlab, const unsigned long long *ctl, uint32_t *err,
+                          unsigned long long *fe) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (uint32_t b = group; b < gr.nbuckets; b += ngroups) {
-    const uint32_t x = gr.bowner[b];
-    if (!((nm_bits[x >> 5] >> (x & 31)) & 1u) || gr.deg[x] == 0) continue;
-    const uint32_t px = __ldcg(p + x);
-    walk_bucket(gr, L, b, [&](const uint4 &q) {
-      uint32_t k[4], w[4];
-      lane_keys<kRW>(q, L.gl, k, w);
+  const unsigned long long ml = ctl[kFMainLabel], mp = ctl[kFMainPiece];
+  for (uint64_t b0 = (uint64_t)group * 4; b0 < g.nbuckets; b0 += (uint64_t)ngroups * 4) {
+    const uint32_t b = (uint32_t)b0, m = min(4u, g.nbuckets - b);
+    uint32_t own[4], px[4], live = 0;
 #pragma unroll
-      for (int j = 0; j < keys_per_lane<kRW>(); ++j) {
-        const uint32_t y = k[j];
-        if (y >= kTombKey || y == x || y >= gr.V) continue;
-        if (__ldcg(p + y) == px) continue;
-        uf_union(p, y, x, err, fe);
+    for (uint32_t j = 0; j < 4; ++j) {
+      own[j] = j < m ? __ldg(g.bowner + b + j) : 0u;
+      const bool ok = j < m && ((nm_bits[own[j] >> 5] >> (own[j] & 31)) & 1u) && g.deg[own[j]] != 0;
+      live |= (ok ? 1u : 0u) << j;
+    }
+    if (!live) continue;
+    // decided on one lane and broadcast: the walk below shuffles within the
+    // group, so every lane must take the same buckets (lanes reading the
+    // parents at different moments could disagree)
+    uint32_t drop = 0;
+    if (L.gl == 0) {
+#pragma unroll
+      for (uint32_t j = 0; j < 4; ++j)
+        if (((live >> j) & 1u) && fe_joined(p, oldlab, own[j], ml, mp)) drop |= 1u << j;
+    }
+    live &= ~__shfl_sync(L.gmask, drop, L.gbase);
+    if (!live) continue;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) px[j] = ((live >> j) & 1u) ? __ldcg(p + own[j]) : 0u;
+    walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 q) {
+      if (!((live >> j) & 1u)) return;
+      const uint32_t x = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
+      const uint32_t pj = px[0] * (j == 0) + px[1] * (j == 1) + px[2] * (j == 2) + px[3] * (j == 3);
+      uint32_t k[4], w[4];
+      lane_keys<kW>(q, L.gl, k, w);
+      uint32_t py[4];
+#pragma unroll
+      for (int t = 0; t < keys_per_lane<kW>(); ++t)
+        py[t] = (k[t] < kTombKey && k[t] != x && k[t] < g.V) ? __ldcg(p + k[t]) : pj;
+#pragma unroll
+      for (int t = 0; t < keys_per_lane<kW>(); ++t) {
+        if (py[t] == pj) continue;
+        if (kIn)
+          uf_union(p, k[t], x, err, fe);  // the slab edge k -> x of the graph
+        else
+          uf_union(p, x, k[t], err, fe);
       }
     });
   }
@@ -719,13 +809,17 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
     const int ib = (int)std::min<uint64_t>(w->rev->num_buckets * 8 / 256 + 1,
                                            (uint64_t)device_sm_count(g->device) * 8);
     if (g->weighted)
-      k_uf_edges_skip<true><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->err, w->fe);
+      k_fe_scan<true, false><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
+                                                 w->err, w->fe);
     else
-      k_uf_edges_skip<false><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->err, w->fe);
+      k_fe_scan<false, false><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
+                                                  w->err, w->fe);
     if (w->rev->weighted)
-      k_fe_scan_in<true><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->err, w->fe);
+      k_fe_scan<true, true><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
+                                                w->err, w->fe);
     else
-      k_fe_scan_in<false><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->err, w->fe);
+      k_fe_scan<false, true><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
+                                                 w->err, w->fe);
     k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices);
   }
   MK_CUDA(cudaGetLastError());

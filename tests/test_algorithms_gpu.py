@@ -300,7 +300,7 @@ def test_wcc_decremental_over_the_spanning_forest(with_rev, weighted):
         wcc.Decremental(tds, tdd)
         np.testing.assert_array_equal(wcc.Labels(), O.wcc())
         dead, rescanned, path = wcc.decremental_stats()
-        assert (dead == 0) == (path == 0)
+        assert (path == 0) <= (dead == 0) and (path in (1, 2)) <= (dead > 0)
         paths.append(path)
         is_, id_ = es.sample_absent(700, seed=130 + r)
         tis, tid = to_dev(is_), to_dev(id_)
