@@ -20,7 +20,10 @@
 //   * vertices of in-degree <= kPrFlat: a warp takes 32 consecutive ones and
 //     walks the concatenation of their rows 32 edges per step (coalesced
 //     column loads, several steps in flight), a segmented warp scan giving
-//     each vertex its share of every step;
+//     each vertex its share of every step; each warp owns a contiguous run
+//     of these 32-vertex groups holding an equal share of the flat edges
+//     (a prefix sum per solve, one binary search per warp), so no warp
+//     waits at the iteration's barrier for a neighbour with heavier rows;
 //   * hubs (in-degree > kPrFlat) are split into work items of kPrChunk
 //     in-edges, one warp per item, and combine their item partials in a
 //     second, fixed-order pass.
@@ -77,6 +80,8 @@ struct PrArgs {
   const uint32_t *item_v;          // vertex of each item (items of a vertex are contiguous)
   const unsigned long long *moff;  // V+1: moff[V] = vertices with several items
   const uint32_t *multi;           // those vertices, in increasing id order
+  const unsigned long long *gpre;  // ngroups+1: prefix sums of the flat work of the 32-vertex groups
+  uint32_t ngroups;
   float *ipart;      // per-item Kahan partials (s, c) = 2 * items
   float *pr0, *pr1;
   float *c0, *c1;
@@ -205,6 +210,27 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
   auto part = [&](uint32_t parity, uint32_t kind) { return a.part + ((parity * 2 + kind) * 2) * nb; };
   uint32_t cur = a.cur;
   const unsigned long long nitems = a.ioff[V], nmulti = a.moff[V];
+  // this warp's run of 32-vertex groups: [glo, ghi), an equal share of the
+  // flat work (lane 0 searches, the warp shares the result)
+  uint32_t glo = 0, ghi = 0;
+  if (lane == 0) {
+    const unsigned long long total = a.gpre[a.ngroups];
+    auto first_at = [&](unsigned long long t) {  // first group g with gpre[g + 1] > t
+      uint32_t lo = 0, hi = a.ngroups;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.gpre[mid + 1] > t)
+          hi = mid;
+        else
+          lo = mid + 1;
+      }
+      return lo;
+    };
+    glo = first_at(total * wid / nwarps);
+    ghi = wid + 1 == nwarps ? a.ngroups : first_at(total * (wid + 1) / nwarps);
+  }
+  glo = __shfl_sync(0xFFFFFFFFu, glo, 0);
+  ghi = __shfl_sync(0xFFFFFFFFu, ghi, 0);
   const float d = a.damping;
   const float invV = 1.0f / (float)V;
 
@@ -243,8 +269,8 @@ __global__ void __launch_bounds__(kPrBlock) k_pagerank(PrArgs a) {
     // concatenation of their in-edge rows (hubs excluded) 32 edges per step,
     // kPrSteps steps with their loads in flight together; a segmented scan
     // hands every vertex the sum of its part of each step
-    for (uint32_t vb = wid * 32u; vb < V; vb += nwarps * 32u) {
-      const uint32_t u = vb + lane;
+    for (uint32_t grp = glo; grp < ghi; ++grp) {
+      const uint32_t u = grp * 32u + lane;
       unsigned long long j0 = 0;
       uint32_t dl = 0;
       bool mine = false;
@@ -390,6 +416,22 @@ __global__ void k_pr_item_counts(const unsigned long long *__restrict__ rp, uint
   }
 }
 
+// flat work of each 32-vertex group: in-edges of its vertices of in-degree
+// <= kPrFlat, plus 2 per vertex for the per-vertex finish
+__global__ void k_pr_group_counts(const unsigned long long *__restrict__ rp, uint32_t V,
+                                  uint32_t *__restrict__ gcnt) {
+  const uint32_t G = (V + 31) / 32;
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    uint32_t c = 0;
+    const uint32_t u1 = min(V, g * 32u + 32u);
+    for (uint32_t u = g * 32u; u < u1; ++u) {
+      const unsigned long long d = rp[u + 1] - rp[u];
+      c += (d <= kPrFlat ? (uint32_t)d : 0u) + 2u;
+    }
+    gcnt[g] = c;
+  }
+}
+
 __global__ void k_pr_item_fill(const uint32_t *__restrict__ cnt, const unsigned long long *__restrict__ ioff,
                                const unsigned long long *__restrict__ moff, uint32_t V,
                                uint32_t *__restrict__ item_v, uint32_t *__restrict__ multi) {
@@ -419,8 +461,8 @@ struct mk_pagerank {
   float *part = nullptr;
   float *delta = nullptr;
   // per-solve CSR of the reverse graph and its work items
-  DevBuf<unsigned long long> rp, ioff, moff, scan_tmp;
-  DevBuf<uint32_t> col, cnt, mflag, item_v, multi;
+  DevBuf<unsigned long long> rp, ioff, moff, gpre, scan_tmp;
+  DevBuf<uint32_t> col, cnt, mflag, item_v, multi, gcnt;
   DevBuf<float> ipart;
   uint32_t *ctl = nullptr;
   uint32_t cur = 0;  // host mirror of the buffer with the latest ranks
@@ -462,6 +504,12 @@ static mk_status pr_prepare(mk_pagerank *p, cudaStream_t s) {
   MK_CHECK(scan_u32_to_u64(p->cnt.ptr, p->ioff.ptr, V, p->scan_tmp, s));
   MK_CHECK(scan_u32_to_u64(p->mflag.ptr, p->moff.ptr, V, p->scan_tmp, s));
   k_pr_item_fill<<<fb, 256, 0, s>>>(p->cnt.ptr, p->ioff.ptr, p->moff.ptr, V, p->item_v.ptr, p->multi.ptr);
+  const uint32_t G = (V + 31) / 32;
+  MK_CHECK(p->gcnt.reserve(G));
+  MK_CHECK(p->gpre.reserve((size_t)G + 1));
+  k_pr_group_counts<<<(int)std::min<uint64_t>(G / 256 + 1, (uint64_t)device_sm_count(g->device) * 8), 256, 0, s>>>(
+      p->rp.ptr, V, p->gcnt.ptr);
+  MK_CHECK(scan_u32_to_u64(p->gcnt.ptr, p->gpre.ptr, G, p->scan_tmp, s));
   MK_CUDA(cudaGetLastError());
   return MK_OK;
 }
@@ -492,6 +540,8 @@ static mk_status pr_solve(mk_pagerank *p, cudaStream_t s) {
   a.item_v = p->item_v.ptr;
   a.moff = p->moff.ptr;
   a.multi = p->multi.ptr;
+  a.gpre = p->gpre.ptr;
+  a.ngroups = (g->V + 31) / 32;
   a.ipart = p->ipart.ptr;
   a.pr0 = p->pr0;
   a.pr1 = p->pr1;
@@ -695,6 +745,8 @@ mk_status mk_pagerank_destroy(mk_pagerank *p) {
   p->mflag.release();
   p->item_v.release();
   p->multi.release();
+  p->gcnt.release();
+  p->gpre.release();
   p->ipart.release();
   delete p;
   return MK_OK;
