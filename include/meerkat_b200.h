@@ -568,9 +568,20 @@ mk_status mk_set_runner_step(mk_set_runner *r, const uint32_t *d_del_src,
                              const uint32_t *d_del_dst, uint32_t n_del,
                              const uint32_t *d_ins_src, const uint32_t *d_ins_dst,
                              const uint32_t *d_ins_w, uint32_t n_ins, void *stream);
-/* Kernel launches one step issues: 2 plus one per query kind present
- * (members beyond one CTA's shared memory add the device-wide kernels, not
- * counted here). */
+/* One-launch step (opt-in): with on != 0 every later step is ONE
+ * cooperative kernel (one 1,024-thread CTA per SM) in three phases
+ * separated by bounded grid barriers: every delete of the batch, every
+ * insert, then the members' queries, a CTA taking members from a counter
+ * (largest first) and solving each in shared memory.  The answers and the
+ * graph are those of the four-launch step, the batch arrays need no order,
+ * and after a step the graph's last update is the insert batch, as there.
+ * A wait that runs out sets MK_DEVERR_TIMEOUT (mk_graph_sync).
+ * MK_ERR_INVALID when a member has more than 65,535 vertices (the runner
+ * keeps the four-launch step). */
+mk_status mk_set_runner_set_single(mk_set_runner *r, uint32_t on);
+/* Kernel launches one step issues: 1 in the one-launch form, else 2 plus
+ * one per query kind present (members beyond one CTA's shared memory add the
+ * device-wide kernels, not counted here). */
 mk_status mk_set_runner_launches(mk_set_runner *r, uint32_t *h_launches);
 /* The runner's BFS and WCC handles (owned by the runner; NULL when no member
  * asks that query), for mk_traversal_distances / mk_wcc_labels. */

@@ -360,6 +360,9 @@ class GraphSetRunner {
     check(mk_set_runner_launches(r_, &n), "LaunchesPerStep");
     return n;
   }
+  // One cooperative launch per step from now on (members of at most 65,535
+  // vertices); false: four launches.
+  void SetSingle(bool on) { check(mk_set_runner_set_single(r_, on ? 1u : 0u), "SetSingle"); }
   // One step: the deletes, the inserts, every member's query (asynchronous).
   void Step(const uint32_t *dS, const uint32_t *dD, uint32_t nDel, const uint32_t *iS,
             const uint32_t *iD, const uint32_t *iW, uint32_t nIns, void *stream = nullptr) {

@@ -796,8 +796,9 @@ class SetRunner:
     """One query per member of a GraphSet (QUERY_BFS from a local source,
     QUERY_WCC, or QUERY_NONE) and a step that applies one update batch to
     every member and answers every query (mk_set_runner_*): four
-    asynchronous launches, capturable into a CUDA graph.  `bfs` / `wcc` are
-    views of the runner's own handles for reading the answers."""
+    asynchronous launches, or one (set_single) when every member has at most
+    65,535 vertices; either is capturable into a CUDA graph.  `bfs` / `wcc`
+    are views of the runner's own handles for reading the answers."""
 
     def __init__(self, gs: "GraphSet", query, sources_local=None):
         q = np.ascontiguousarray(np.asarray(query, dtype=np.uint8))
@@ -821,6 +822,13 @@ class SetRunner:
         me = weakref.ref(self)
         self.bfs = BFS._borrow(bh, gs.graph, glob, me) if bh.value else None
         self.wcc = WCC._borrow(wh, gs.graph, me) if wh.value else None
+        self.single = False
+
+    def set_single(self, on: bool) -> None:
+        """One cooperative launch per step (deletes, inserts, then the member
+        queries, separated by grid barriers) instead of four launches."""
+        check(lib().mk_set_runner_set_single(self._h, int(bool(on))), "mk_set_runner_set_single")
+        self.single = bool(on)
 
     def launches_per_step(self) -> int:
         n = C.c_uint32(0)

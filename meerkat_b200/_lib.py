@@ -141,6 +141,7 @@ SIGNATURES = [
     ("mk_set_runner_step", _S, [vp, vp, vp, C.c_uint32, vp, vp, vp, C.c_uint32, vp]),
     ("mk_set_runner_results", _S, [vp, C.POINTER(vp), C.POINTER(vp)]),
     ("mk_set_runner_launches", _S, [vp, u32p]),
+    ("mk_set_runner_set_single", _S, [vp, C.c_uint32]),
     ("mk_set_runner_handles", _S, [vp, C.POINTER(vp), C.POINTER(vp)]),
     ("mk_set_runner_destroy", _S, [vp]),
     ("mk_read_edge_list", _S, [C.c_char_p, u32p, u64p, vp, vp]),

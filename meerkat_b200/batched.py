@@ -17,10 +17,12 @@ members in one GraphSet and issues, per step,
   one WCC launch over the WCC-queried members (a member of at most 65,536
   vertices is solved by one CTA with its union-find in shared memory),
 
-each member's results being those of the member alone.  The step can be
-captured into a CUDA graph and replayed; the autotuner picks the update
-kernel and the BFS frontier chunk on the live set.  There is no counterpart
-in the reference.
+each member's results being those of the member alone.  When every member
+fits one CTA the step can also be ONE cooperative launch (set_single):
+every delete, every insert, then the member queries, separated by grid
+barriers.  Either form can be captured into a CUDA graph and replayed; the
+autotuner picks the update kernel and the BFS frontier chunk of the
+four-launch form on the live set.  There is no counterpart in the reference.
 """
 from __future__ import annotations
 
@@ -118,6 +120,13 @@ class BatchedRunner:
         self._bfs_large = int((bsz > BFS_LOCAL_MAX).sum())
         sizes = off[self.wcc_members + 1] - off[self.wcc_members]
         self._wcc_large = int((sizes > WCC_LOCAL_MAX).sum())
+        # every member fits one CTA: the step can also be one launch
+        self.single_ok = int((off[1:] - off[:-1]).max()) <= BFS_LOCAL_MAX
+
+    def set_single(self, on: bool) -> None:
+        """One cooperative launch per step instead of four (set_single of the
+        C runner)."""
+        self.runner.set_single(on)
 
     def update(self, ds, dd, is_, id_, iw, stream=None):
         self.G.DeleteEdges(ds, dd, stream=stream)
@@ -133,6 +142,8 @@ class BatchedRunner:
         self.runner.step(*batch, stream=stream)
 
     def launches_per_step(self) -> int:
+        if self.runner.single:
+            return 1
         # kernels: delete, insert; BFS: 1 shared-memory kernel (plus 2
         # memsets) and the cooperative device-wide kernel when some member is
         # larger than shared memory holds; WCC: 1 shared-memory kernel (plus 1

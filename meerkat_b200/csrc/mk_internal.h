@@ -120,6 +120,19 @@ mk_status export_csr_grow(mk_graph *g, DevBuf<unsigned long long> &row_ptr, DevB
 // Number of co-resident blocks for a persistent cooperative launch.
 int persistent_blocks(const void *kernel, int block, size_t smem, int device);
 
+// Device buffers of a BFS handle that the member solver writes: the packed
+// dist << 32 | parent words (one per vertex), the work-item array (one word
+// per bucket) and the reached-vertex list (one word per vertex).  For the
+// one-launch graph-set step, which runs the member solver itself.
+struct TravMemberBufs {
+  unsigned long long *dist;
+  uint32_t *items;
+  uint32_t *found;
+};
+mk_status trav_member_bufs(mk_traversal *t, TravMemberBufs *out);
+// Label array (one word per vertex) of a WCC handle.
+uint32_t *wcc_label_buf(mk_wcc *w);
+
 }  // namespace mk
 
 struct mk_graph {

@@ -1,5 +1,6 @@
 // Per-member solvers of a graph set, run by one whole CTA with the member's
-// state in shared memory (one query kind per member kernel launch).
+// state in shared memory.  The member kernels (one query kind per launch)
+// and the one-launch graph-set step (its last phase) both call them.
 //
 // bfs_member: static BFS of one vertex range from its source.  The member's
 // BFS state lives in shared memory -- a 16-bit parent per vertex (0xFFFF:
@@ -21,6 +22,11 @@
 // of the device-wide kernels (larger root under smaller, as the reference's
 // UnionAsync, include/Util/UnionFind.cuh:194-215), so labels are the minimum
 // vertex id of each component.
+//
+// kFused: the kernel updated the graph itself earlier in the same launch
+// (behind a grid barrier): slabs are read with plain loads, never the
+// non-coherent path (ld_slab), and the BFS writes the unreached vertices'
+// words itself instead of relying on a reset before the launch.
 #pragma once
 
 #include "mk_common.cuh"
@@ -69,10 +75,10 @@ __device__ __forceinline__ bool cas_min16_first(uint16_t *p, uint32_t v) {
 // most kMemLocalMax vertices, src its source (global id).  The range uses the
 // slices [R.z, R.w) of items (one word per bucket: a vertex's items never
 // exceed its buckets) and [R.x, R.y) of found (a vertex is reached once).
-// dist must already hold kInfInf for the range.  smem holds
+// Without kFused, dist must already hold kInfInf for the range.  smem holds
 // bfs_member_smem(n) bytes; s_nfound / s_nitems are CTA-shared words.  Ends
 // with the CTA synchronised.
-template <bool kW>
+template <bool kW, bool kFused>
 __device__ __forceinline__ void bfs_member(const GraphView &g, const Lanes &L, const uint4 R,
                                            uint32_t src, unsigned long long *__restrict__ dist,
                                            uint32_t *__restrict__ items,
@@ -135,11 +141,16 @@ __device__ __forceinline__ void bfs_member(const GraphView &g, const Lanes &L, c
         }
       };
       for (uint32_t b = bb; b < be; b += kMemChunk)
-        walk4_levels(g, L, b, min(kMemChunk, be - b), [&](uint32_t, const uint4 x) { relax(x); });
+        walk4_levels<kFused>(g, L, b, min(kMemChunk, be - b),
+                             [&](uint32_t, const uint4 x) { relax(x); });
     }
     fbeg = fend;
     ibeg = iend;
     __syncthreads();
+  }
+  if (kFused) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+      if (!((vis[i >> 5] >> (i & 31)) & 1u)) dist[lo + i] = kInfInf;
   }
   __syncthreads();
 }
@@ -183,7 +194,7 @@ __device__ __forceinline__ void ls_union(uint16_t *p, uint32_t a, uint32_t b, ui
 // component.  A key outside the range (a range that is not closed under
 // edges) is skipped and reported as MK_DEVERR_INVALID_ID.  sp holds
 // uf_member_smem(n) bytes.  Ends with the CTA synchronised.
-template <bool kW>
+template <bool kW, bool kFused>
 __device__ __forceinline__ void uf_member(const GraphView &g, const Lanes &L, const uint4 R,
                                           uint32_t *__restrict__ labels, uint32_t *err,
                                           uint16_t *sp) {
@@ -196,7 +207,7 @@ __device__ __forceinline__ void uf_member(const GraphView &g, const Lanes &L, co
     uint32_t own[kMemberHeads];
 #pragma unroll
     for (uint32_t j = 0; j < kMemberHeads; ++j) own[j] = j < m ? __ldg(g.bowner + b + j) - lo : 0u;
-    walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 x) {
+    walk4_levels<kFused>(g, L, b, m, [&](uint32_t j, const uint4 x) {
       const uint32_t u = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
       uint32_t k[4], w[4];
       lane_keys<kW>(x, L.gl, k, w);

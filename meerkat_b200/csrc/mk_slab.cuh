@@ -157,15 +157,16 @@ __device__ __forceinline__ void walk_buckets(const GraphView &g, const Lanes &L,
 // Visits buckets [b, b + m), m <= 4: the head slabs are loaded together,
 // then the overflow chains level by level, the next slabs of every chain
 // still running loaded together.  f(j, q) gets the bucket's index j in
-// [0, m) and the lane's quarter of one slab.
-template <class F>
+// [0, m) and the lane's quarter of one slab.  kCg: the kernel wrote slabs
+// earlier in the same launch (ld_slab).
+template <bool kCg = false, class F>
 __device__ __forceinline__ void walk4_levels(const GraphView &g, const Lanes &L, uint32_t b,
                                              uint32_t m, F &&f) {
   uint4 q[4];
   uint32_t nx[4];
 #pragma unroll
   for (uint32_t j = 0; j < 4; ++j)
-    if (j < m) q[j] = ld_slab_ro(g.slabs + 8ull * (b + j) + L.gl);
+    if (j < m) q[j] = ld_slab<kCg>(g.slabs + 8ull * (b + j) + L.gl);
 #pragma unroll
   for (uint32_t j = 0; j < 4; ++j) {
     nx[j] = kNoSlab;
@@ -177,7 +178,7 @@ __device__ __forceinline__ void walk4_levels(const GraphView &g, const Lanes &L,
   while ((nx[0] & nx[1] & nx[2] & nx[3]) != kNoSlab) {  // some chain still running
 #pragma unroll
     for (uint32_t j = 0; j < 4; ++j)
-      if (nx[j] != kNoSlab) q[j] = ld_slab_ro(g.slabs + 8ull * nx[j] + L.gl);
+      if (nx[j] != kNoSlab) q[j] = ld_slab<kCg>(g.slabs + 8ull * nx[j] + L.gl);
 #pragma unroll
     for (uint32_t j = 0; j < 4; ++j)
       if (nx[j] != kNoSlab) {

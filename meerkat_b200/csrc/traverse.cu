@@ -867,7 +867,7 @@ __global__ void __launch_bounds__(kMemThreads, 1)
     __syncthreads();
     const uint32_t r = s_range;
     if (r >= nr) break;
-    bfs_member<kW>(g, L, rng[r], src[r], dist, items, found, err, smem, s_nfound, s_nitems);
+    bfs_member<kW, false>(g, L, rng[r], src[r], dist, items, found, err, smem, s_nfound, s_nitems);
   }
 }
 
@@ -1099,6 +1099,16 @@ static mk_status trav_launch(mk_traversal *t, uint32_t mode, const uint32_t *bs,
   if (mode == kStatic) t->has_static = true;
   return MK_OK;
 }
+
+namespace mk {
+mk_status trav_member_bufs(mk_traversal *t, TravMemberBufs *out) {
+  if (!t || !out) return fail(MK_ERR_INVALID, "trav_member_bufs: null argument");
+  out->dist = t->dist;
+  out->items = reinterpret_cast<uint32_t *>(t->fr0);
+  out->found = t->inv_list;
+  return MK_OK;
+}
+}  // namespace mk
 
 extern "C" {
 

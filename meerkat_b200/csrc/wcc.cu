@@ -646,7 +646,7 @@ __global__ void __launch_bounds__(kMemThreads, 1)
     __syncthreads();
     const uint32_t r = s_range;
     if (r >= nr) break;
-    uf_member<kW>(g, L, rng[r], labels, err, sp);
+    uf_member<kW, false>(g, L, rng[r], labels, err, sp);
   }
 }
 
@@ -830,6 +830,10 @@ static bool batch_matches(const mk_graph *g, const uint32_t *d_src, const uint32
                           uint32_t n, int op) {
   return n == g->last_n && d_src == g->last_src && d_dst == g->last_dst && g->last_op == op;
 }
+
+namespace mk {
+uint32_t *wcc_label_buf(mk_wcc *w) { return w ? w->parent : nullptr; }
+}  // namespace mk
 
 extern "C" {
 

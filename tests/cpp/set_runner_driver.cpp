@@ -5,10 +5,11 @@
 // Prints, per member, its query kind and its answer (BFS levels or local WCC
 // labels) for the test to compare with the oracle.
 //
-//   set_runner_driver <members> <steps> <capture 0|1>
+//   set_runner_driver <members> <steps> <capture 0|1> [single 0|1]
 //
-// The driver exits 5 if the runner reports other than four launches per
-// step (two update kernels, the member BFS, the member WCC).
+// With single = 1 every step is the one-launch form.  The driver exits 5 if
+// the runner reports other than four launches per step (two update kernels,
+// the member BFS, the member WCC), or one in the one-launch form.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -28,6 +29,7 @@ int main(int argc, char **argv) {
   const uint32_t G = argc > 1 ? (uint32_t)atoi(argv[1]) : 6;
   const uint32_t K = argc > 2 ? (uint32_t)atoi(argv[2]) : 3;
   const bool capture = argc > 3 && atoi(argv[3]) != 0;
+  const bool single = argc > 4 && atoi(argv[4]) != 0;
   std::vector<uint32_t> nv(G);
   for (uint32_t m = 0; m < G; ++m) nv[m] = 256u << (m % 4);  // 256 .. 2048 vertices
   meerkat::GraphSet set(nv, /*weighted=*/true);
@@ -60,7 +62,8 @@ int main(int argc, char **argv) {
   uint32_t *uS = to_device(dsrc), *uD = to_device(ddst), *uW = to_device(dw);
   meerkat::check(mk_graph_reserve_batch(set.Union(), (uint32_t)dsrc.size()), "reserve");
   meerkat::GraphSetRunner run(set, query, bsrc);
-  if (run.LaunchesPerStep() != 4) return 5;
+  if (single) run.SetSingle(true);
+  if (run.LaunchesPerStep() != (single ? 1u : 4u)) return 5;
   cudaStream_t st;
   cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   // step k deletes the updated edges (k even) or inserts them back with

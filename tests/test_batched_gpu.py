@@ -115,13 +115,16 @@ def check_step(spec, batch, voff, oracles, gs, br, src_of, pr=None, plain=()):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("capture,weighted", [(False, False), (True, True), (True, False)])
-def test_runner_step_matches_oracle(capture, weighted):
+@pytest.mark.parametrize("capture,weighted,single", [
+    (False, False, False), (True, True, False), (True, False, False),
+    (False, True, True), (True, True, True), (False, False, True)])
+def test_runner_step_matches_oracle(capture, weighted, single):
     """The whole batched step through the C set runner (mk_set_runner_step:
-    both update kernels and both member queries), issued directly or
-    captured into a CUDA graph and replayed: every member's answer and the
-    set's degrees equal the oracle's after each step, on weighted and
-    unweighted sets."""
+    both update kernels and both member queries, or the one cooperative
+    launch), issued directly or captured into a CUDA graph and replayed:
+    every member's answer and the set's degrees equal the oracle's after
+    each step, on weighted and unweighted sets, and the applied-insert count
+    is published as after the four launches."""
     import torch
     spec = B.make_spec(48, seed=12, v_lo=32, v_hi=700, deg_lo=2, deg_hi=12, upd_lo=0.05,
                        upd_hi=0.3)
@@ -129,7 +132,10 @@ def test_runner_step_matches_oracle(capture, weighted):
     bfs_members = np.flatnonzero(spec.query == B.QUERY_BFS)
     srcs = B.pick_sources(gs.graph.degrees(), voff, bfs_members, seed=4)
     br = B.BatchedRunner(gs, spec.query, srcs)
-    assert br.launches_per_step() == br.runner.launches_per_step() == 4
+    if single:
+        assert br.single_ok
+        br.set_single(True)
+    assert br.launches_per_step() == br.runner.launches_per_step() == (1 if single else 4)
     gs.graph.reserve_batch(int(max(spec.inserts.sum(), spec.deletes.sum())))
     src_of = dict(zip(bfs_members.tolist(), srcs.tolist()))
     for step in range(3):
@@ -146,7 +152,11 @@ def test_runner_step_matches_oracle(capture, weighted):
             del g
         else:
             br.step(batch)
+        edges_before = sum(O.num_edges() for O in oracles)
         check_step(spec, batch, voff, oracles, gs, br, src_of)
+        # inserts applied = the edge count's growth + the deletes applied
+        grown = sum(O.num_edges() for O in oracles) - edges_before
+        assert grown <= gs.graph.last_applied() <= int(spec.inserts.sum())
     br.close()
     gs.close()
 

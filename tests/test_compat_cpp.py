@@ -86,15 +86,17 @@ def test_reference_style_driver_matches_oracle(tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("capture", ["0", "1"])
-def test_cpp_batched_step_matches_oracle(tmp_path, capture):
+@pytest.mark.parametrize("single", ["0", "1"])
+def test_cpp_batched_step_matches_oracle(tmp_path, capture, single):
     """The batched many-graph step through the C++ shim (GraphSet +
-    GraphSetRunner over mk_set_runner_*), issued step by step and captured
-    into a CUDA graph: every member's BFS levels or WCC labels equal the
-    oracle's on that member alone after the same update steps."""
+    GraphSetRunner over mk_set_runner_*), four launches or one cooperative
+    launch per step, issued step by step and captured into a CUDA graph:
+    every member's BFS levels or WCC labels equal the oracle's on that
+    member alone after the same update steps."""
     exe = build_driver(tmp_path, SET_DRIVER)
     G, K = 6, 5
-    r = subprocess.run([str(exe), str(G), str(K), capture], capture_output=True, text=True,
-                       timeout=300)
+    r = subprocess.run([str(exe), str(G), str(K), capture, single], capture_output=True,
+                       text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     lines = r.stdout.strip().splitlines()
     assert len(lines) == G
