@@ -734,7 +734,7 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   const size_t words = ((size_t)V + 31) / 32;
   const int fg = flat_grid(V, g->device);
   const GraphView v = g->view();
-  uint32_t cap = 1024;
+  uint32_t cap = 1024;  // n < 2^30 (checked by the caller): cap <= 2^31
   while (cap < 2ull * n) cap <<= 1;
   MK_CHECK(w->dtab.reserve(cap, &g->device_bytes));
   MK_CUDA(cudaMemsetAsync(w->dtab.ptr, 0xFF, (size_t)cap * 8, s));
@@ -1044,6 +1044,9 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d
   if (!batch_matches(g, d_src, d_dst, n, 2) || !w->forest_valid || (n && w->rev && w->skip_left)) {
     if (w->skip_left) --w->skip_left;
     MK_CHECK(wcc_static(w, s));
+    w->last_path = 3;
+  } else if (n >= (1u << 30)) {
+    MK_CHECK(wcc_static(w, s));  // beyond the batch set's size
     w->last_path = 3;
   } else if (n) {
     MK_CHECK(wcc_decremental_forest(w, d_src, d_dst, n, s));
