@@ -188,4 +188,36 @@ __device__ __forceinline__ void walk4_levels(const GraphView &g, const Lanes &L,
   }
 }
 
+// walk4_levels over 4 arbitrary buckets bk[j] (those with bit j of live
+// set), chains followed level by level.  Every lane of the group must pass
+// the same bk and live.
+template <class F>
+__device__ __forceinline__ void walk4_set(const GraphView &g, const Lanes &L, const uint32_t (&bk)[4],
+                                          uint32_t live, F &&f) {
+  uint4 q[4];
+  uint32_t nx[4];
+#pragma unroll
+  for (uint32_t j = 0; j < 4; ++j)
+    if ((live >> j) & 1u) q[j] = ld_slab<false>(g.slabs + 8ull * bk[j] + L.gl);
+#pragma unroll
+  for (uint32_t j = 0; j < 4; ++j) {
+    nx[j] = kNoSlab;
+    if ((live >> j) & 1u) {
+      f(j, q[j]);
+      nx[j] = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
+    }
+  }
+  while ((nx[0] & nx[1] & nx[2] & nx[3]) != kNoSlab) {
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j)
+      if (nx[j] != kNoSlab) q[j] = ld_slab<false>(g.slabs + 8ull * nx[j] + L.gl);
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j)
+      if (nx[j] != kNoSlab) {
+        f(j, q[j]);
+        nx[j] = __shfl_sync(L.gmask, q[j].w, L.gbase + 7);
+      }
+  }
+}
+
 }  // namespace mk

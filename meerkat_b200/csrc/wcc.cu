@@ -211,14 +211,16 @@ __device__ __forceinline__ void link_bucket_skip(const GraphView &g, const Lanes
 }
 
 // Every selected bucket (owner's bit set, all if sel_bits is null): unions of
-// the out-edges whose endpoints do not share a parent yet.  A group takes 4
+// the out-edges whose endpoints do not share a parent yet (nothing when
+// skip_if is given and holds a non-zero word).  A group takes 4
 // consecutive buckets at a time: their owners' parents and head slabs are
 // loaded together, chains are followed level by level, and a lane loads the
 // parents of all its keys before comparing, so one group keeps several
 // reads in flight instead of one dependent read per key.
 template <bool kW>
 __global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bits, uint32_t *err,
-                                unsigned long long *fe) {
+                                unsigned long long *fe, const unsigned long long *skip_if = nullptr) {
+  if (skip_if && *skip_if) return;
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
@@ -262,7 +264,9 @@ enum : int {
   kFMainLabel = 4,  // old label + 1 of the component whose main piece was sampled (0: none)
   kFMainPiece = 5,  // that main piece's root + 1
   kFAffected = 6,   // vertices of the affected components
-  kFCtlWords = 7
+  kFGiant = 7,      // static passes: the most sampled set's root + 1 (0: none)
+  kFOutside = 8,    // static passes: vertices listed outside the giant set
+  kFCtlWords = 9
 };
 
 // Set of the batch's deleted edges (slab orientation a << 32 | b): open
@@ -566,6 +570,140 @@ __global__ void k_fe_scan(GraphView g, uint32_t *p, const uint32_t *nm_bits,
   }
 }
 
+// ---- static passes with a reverse graph: skip the largest set ----
+// After sampled linking (and a compress) most vertices of a large component
+// already point at its root.  One CTA draws kMainSamples vertices with
+// out-edges and keeps the most frequent root (at least 32 samples) as the
+// giant set.  Every edge with both ends in it needs no union; every other
+// edge has an end outside it, whose out-edges (graph) or in-edges (reverse
+// graph) are then scanned, so the giant set's own edges are never read.  The
+// outside vertices are compacted into a list first: a pass over every bucket
+// that only skips most of them costs about as much as one that walks them
+// when the buckets are short (on a grid, one slab per vertex).
+__global__ void __launch_bounds__(kMainThreads)
+    k_uf_giant_sample(const uint32_t *p, const uint32_t *deg, uint32_t V, unsigned long long seed,
+                      unsigned long long *ctl) {
+  __shared__ uint32_t keys[kMainSlots], cnts[kMainSlots];
+  __shared__ unsigned long long best;
+  for (uint32_t i = threadIdx.x; i < kMainSlots; i += blockDim.x) {
+    keys[i] = 0xFFFFFFFFu;
+    cnts[i] = 0u;
+  }
+  if (threadIdx.x == 0) best = 0;
+  __syncthreads();
+  __shared__ uint32_t drawn;
+  if (threadIdx.x == 0) drawn = 0;
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < kMainSamples; j += blockDim.x) {
+    unsigned long long h = seed + 0x9E3779B97F4A7C15ull * (j + 1);
+    h ^= h >> 33;
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 33;
+    const uint32_t x = (uint32_t)(h % V);
+    if (deg[x] == 0) continue;
+    atomicAdd(&drawn, 1u);
+    const uint32_t k = __ldcg(p + x);
+    uint32_t sl = (k * 2654435761u) & (kMainSlots - 1);
+    for (uint32_t it = 0; it < kMainSlots; ++it) {
+      const uint32_t old = atomicCAS(keys + sl, 0xFFFFFFFFu, k);
+      if (old == 0xFFFFFFFFu || old == k) {
+        atomicAdd(cnts + sl, 1u);
+        break;
+      }
+      sl = (sl + 1) & (kMainSlots - 1);
+    }
+  }
+  __syncthreads();
+  unsigned long long mine = 0;
+  for (uint32_t i = threadIdx.x; i < kMainSlots; i += blockDim.x) {
+    const unsigned long long c = ((unsigned long long)cnts[i] << 32) | keys[i];
+    if (cnts[i] && c > mine) mine = c;
+  }
+  atomicMax(&best, mine);
+  __syncthreads();
+  // a set holding under three quarters of the samples would leave most
+  // edges to scan from both ends: then no giant set (every out-edge once, as
+  // without a reverse graph)
+  if (threadIdx.x == 0)
+    ctl[kFGiant] = ((best >> 32) >= 32 && 4 * (best >> 32) >= 3ull * drawn)
+                       ? (unsigned long long)(uint32_t)best + 1 : 0ull;
+}
+
+// The vertices outside the giant set that have an out- or in-edge, compacted
+// into list (one atomic per warp; any order).  Nothing without a giant set.
+__global__ void k_uf_outside_list(const uint32_t *p, uint32_t V, const uint32_t *deg,
+                                  const uint32_t *rdeg, unsigned long long *ctl, uint32_t *list) {
+  const unsigned long long giant = ctl[kFGiant];
+  if (giant == 0) return;
+  const uint32_t lane = threadIdx.x & 31u, stride = gridDim.x * blockDim.x;
+  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < V; base += stride) {
+    const uint32_t x = base + lane;
+    const bool out = x < V && (deg[x] | rdeg[x]) != 0 && __ldcg(p + x) != (uint32_t)(giant - 1);
+    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, out);
+    if (!bal) continue;
+    uint32_t at = 0;
+    if (lane == 0) at = (uint32_t)atomicAdd(ctl + kFOutside, (unsigned long long)__popc(bal));
+    at = __shfl_sync(0xFFFFFFFFu, at, 0);
+    if (out) list[at + __popc(bal & ((1u << lane) - 1u))] = x;
+  }
+}
+
+// The out-edges (kIn: the in-edges, through the reverse graph, whose key y is
+// the graph edge y -> x) of the listed vertices: unions of the edges whose
+// endpoints do not share a parent yet.  A group takes 4 list entries at a
+// time and walks one bucket of each per round, so vertices of several
+// buckets take several rounds.
+template <bool kW, bool kIn>
+__global__ void k_uf_scan_list(GraphView g, uint32_t *p, const uint32_t *list,
+                               const unsigned long long *ctl, uint32_t *err,
+                               unsigned long long *fe) {
+  const Lanes L = lanes();
+  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
+  const uint64_t n = ctl[kFOutside];
+  for (uint64_t i0 = (uint64_t)group * 4; i0 < n; i0 += (uint64_t)ngroups * 4) {
+    const uint32_t m = n - i0 < 4 ? (uint32_t)(n - i0) : 4u;
+    uint32_t own[4], bk[4], be[4], px[4];
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      own[j] = j < m ? __ldcg(list + i0 + j) : 0u;
+      bk[j] = be[j] = 0;
+      if (j < m && g.deg[own[j]] != 0) {
+        bk[j] = g.boff[own[j]];
+        be[j] = g.boff[own[j] + 1];
+      }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) px[j] = bk[j] < be[j] ? __ldcg(p + own[j]) : 0u;
+    for (;;) {
+      uint32_t live = 0;
+#pragma unroll
+      for (uint32_t j = 0; j < 4; ++j) live |= (bk[j] < be[j] ? 1u : 0u) << j;
+      if (!live) break;
+      walk4_set(g, L, bk, live, [&](uint32_t j, const uint4 q) {
+        const uint32_t x = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
+        const uint32_t pj = px[0] * (j == 0) + px[1] * (j == 1) + px[2] * (j == 2) + px[3] * (j == 3);
+        uint32_t k[4], w[4];
+        lane_keys<kW>(q, L.gl, k, w);
+        uint32_t py[4];
+#pragma unroll
+        for (int t = 0; t < keys_per_lane<kW>(); ++t)
+          py[t] = (k[t] < kTombKey && k[t] != x && k[t] < g.V) ? __ldcg(p + k[t]) : pj;
+#pragma unroll
+        for (int t = 0; t < keys_per_lane<kW>(); ++t) {
+          if (py[t] == pj) continue;
+          if (kIn)
+            uf_union(p, k[t], x, err, fe);  // the slab edge k -> x of the graph
+          else
+            uf_union(p, x, k[t], err, fe);
+        }
+      });
+#pragma unroll
+      for (uint32_t j = 0; j < 4; ++j) bk[j] += bk[j] < be[j] ? 1u : 0u;
+    }
+  }
+}
+
 // ---- vertex-range variants: only the listed ranges are touched ----
 // Ranges are given as prefix sums: range r covers the global indices
 // [pre[r], pre[r+1]) of a concatenation, starting at base[r].
@@ -716,11 +854,47 @@ static mk_status wcc_link(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
   return MK_OK;
 }
 
+// Static passes.  With a reverse graph attached: sampled linking, then only
+// the listed vertices outside the largest sampled set have their out- and
+// in-edges scanned (k_uf_giant_sample; when that set holds under 3/4 of the
+// samples, every out-edge once instead: the device decides, the host
+// launches both forms and one returns at once); without one, every edge
+// through k_uf_edges_skip.
 static mk_status wcc_static(mk_wcc *w, cudaStream_t s) {
   mk_graph *g = w->g;
-  k_uf_init<<<flat_grid(g->V, g->device), 256, 0, s>>>(w->parent, g->V, nullptr, w->fe);
-  MK_CHECK(wcc_link(w, nullptr, s));
+  const uint32_t V = g->V;
+  const int fg = flat_grid(V, g->device);
+  k_uf_init<<<fg, 256, 0, s>>>(w->parent, V, nullptr, w->fe);
   w->forest_valid = true;
+  if (!w->rev) return wcc_link(w, nullptr, s);
+  const GraphView v = g->view(), rv = w->rev->view();
+  MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));  // the outside list
+  uint32_t *list = w->oldlab.ptr;
+  if (g->weighted)
+    k_uf_sample<true><<<fg, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe);
+  else
+    k_uf_sample<false><<<fg, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe);
+  k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, nullptr);
+  MK_CUDA(cudaMemsetAsync(w->fctl, 0, kFCtlWords * 8, s));
+  k_uf_giant_sample<<<1, kMainThreads, 0, s>>>(w->parent, g->deg, V, 0x61A0000ull + (++w->calls),
+                                               w->fctl);
+  k_uf_outside_list<<<fg, 256, 0, s>>>(w->parent, V, g->deg, w->rev->deg, w->fctl, list);
+  const int sm8 = device_sm_count(g->device) * 8;
+  const int ob = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1, (uint64_t)sm8);
+  const unsigned long long *giant = w->fctl + kFGiant;
+  if (g->weighted) {
+    k_uf_edges_skip<true><<<ob, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe, giant);
+    k_uf_scan_list<true, false><<<fg, 256, 0, s>>>(v, w->parent, list, w->fctl, w->err, w->fe);
+  } else {
+    k_uf_edges_skip<false><<<ob, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe, giant);
+    k_uf_scan_list<false, false><<<fg, 256, 0, s>>>(v, w->parent, list, w->fctl, w->err, w->fe);
+  }
+  if (w->rev->weighted)
+    k_uf_scan_list<true, true><<<fg, 256, 0, s>>>(rv, w->parent, list, w->fctl, w->err, w->fe);
+  else
+    k_uf_scan_list<false, true><<<fg, 256, 0, s>>>(rv, w->parent, list, w->fctl, w->err, w->fe);
+  k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, nullptr);
+  MK_CUDA(cudaGetLastError());
   return MK_OK;
 }
 
