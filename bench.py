@@ -433,7 +433,7 @@ def more_queries(mk, G, V, dev, seed):
     # batch first, as a caller keeping them in step would)
     wcc = mk.WCC(G)
     wcc.set_reverse(Gr)
-    t = wcc.Static()
+    t = min(wcc.Static() for _ in range(2))
     out["wcc"] = {"static_ms": t, "static_gbs": (8 * E + 8 * V) / (t / 1e3) / 1e9}
     G.DeleteEdges(bs, bd)
     Gr.DeleteEdges(bs, bd)

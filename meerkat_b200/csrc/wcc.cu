@@ -265,9 +265,36 @@ enum : int {
   kFMainPiece = 5,  // that main piece's root + 1
   kFAffected = 6,   // vertices of the affected components
   kFGiant = 7,      // static passes: the most sampled set's root + 1 (0: none)
-  kFOutside = 8,    // static passes: vertices listed outside the giant set
-  kFCtlWords = 9
+  kFItemsOut = 8,   // scan items listed for the graph (out-edges)
+  kFItemsIn = 9,    // scan items listed for the reverse graph (in-edges)
+  kFCtlWords = 10
 };
+
+// A scan item is the first of up to kItemBuckets consecutive buckets of one
+// vertex (its owner is bowner[item]), so a hub's buckets spread over many
+// groups.  A vertex with nb buckets takes ceil(nb / kItemBuckets) items: a
+// list never holds more than V + nbuckets / kItemBuckets of them.
+constexpr uint32_t kItemBuckets = 16;
+
+// Appends the items of buckets [b0, b1) of every lane with sel set (one
+// atomic per warp; any order).  All 32 lanes of the warp call it together.
+__device__ __forceinline__ void append_items(bool sel, uint32_t b0, uint32_t b1, uint32_t *items,
+                                             unsigned long long *count) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t n = (sel && b1 > b0) ? (b1 - b0 + kItemBuckets - 1) / kItemBuckets : 0u;
+  uint32_t incl = n;
+#pragma unroll
+  for (uint32_t o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  if (total == 0) return;
+  uint32_t at = 0;
+  if (lane == 0) at = (uint32_t)atomicAdd(count, (unsigned long long)total);
+  at = __shfl_sync(0xFFFFFFFFu, at, 0) + incl - n;
+  for (uint32_t i = 0; i < n; ++i) items[at + i] = b0 + i * kItemBuckets;
+}
 
 // Set of the batch's deleted edges (slab orientation a << 32 | b): open
 // addressing over a power-of-two table (mask + 1 slots, at least twice the
@@ -457,13 +484,13 @@ __global__ void __launch_bounds__(kMainThreads)
   }
 }
 
-// Step 3b (after compressing the affected vertices): the bitmap of the
-// affected vertices outside their component's main piece (whole words, one
-// ballot each), their count and out- plus in-degrees, and the graph's live
-// edge count.
+// Step 3b (after compressing the affected vertices): the affected vertices
+// outside their component's main piece, as scan items of their out-buckets
+// (graph) and in-buckets (reverse graph); their count and out- plus
+// in-degrees, and the graph's live edge count.
 __global__ void k_fe_nonmain(const uint32_t *p, const uint32_t *oldlab, uint32_t V,
-                             const uint32_t *aff_vertices, const uint32_t *deg,
-                             const uint32_t *rdeg, uint32_t *nm_bits, unsigned long long *ctl) {
+                             const uint32_t *aff_vertices, GraphView g, GraphView rg,
+                             uint32_t *items_out, uint32_t *items_in, unsigned long long *ctl) {
   const uint32_t words = (V + 31) / 32, lane = threadIdx.x & 31u;
   const uint32_t stride = gridDim.x * blockDim.x;
   const unsigned long long ml = ctl[kFMainLabel], mp = ctl[kFMainPiece];
@@ -472,21 +499,25 @@ __global__ void k_fe_nonmain(const uint32_t *p, const uint32_t *oldlab, uint32_t
        base += stride) {
     const uint32_t x = base + lane;
     bool nm = false;
+    uint32_t d = 0, rd = 0;
     if (x < V) {
-      const uint32_t d = deg[x];
+      d = g.deg[x];
       edges += d;
       if ((aff_vertices[x >> 5] >> (x & 31)) & 1u) {
         const uint32_t r = oldlab[x];
         const uint32_t main_piece = (ml && r == ml - 1) ? (uint32_t)(mp - 1) : __ldcg(p + r);
         nm = __ldcg(p + x) != main_piece;
         if (nm) {
-          ends += d + rdeg[x];
+          rd = rg.deg[x];
+          ends += d + rd;
           ++count;
         }
       }
     }
-    const uint32_t word = __ballot_sync(0xFFFFFFFFu, nm);
-    if (lane == 0) nm_bits[base >> 5] = word;
+    append_items(nm && d != 0, nm ? g.boff[x] : 0u, nm ? g.boff[x + 1] : 0u, items_out,
+                 ctl + kFItemsOut);
+    append_items(nm && rd != 0, nm ? rg.boff[x] : 0u, nm ? rg.boff[x + 1] : 0u, items_in,
+                 ctl + kFItemsIn);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -510,64 +541,6 @@ __device__ __forceinline__ bool fe_joined(uint32_t *p, const uint32_t *oldlab, u
   const uint32_t r = __ldg(oldlab + x);
   const uint32_t m = (ml && r == ml - 1) ? (uint32_t)(mp - 1) : r;
   return uf_find(p, x) == uf_find(p, m);
-}
-
-// Step 3c: every bucket of the graph (kIn: of the reverse graph, whose key y
-// is the graph edge y -> x) whose owner x is outside its main piece (bit
-// set) and not yet joined to it; an edge between two sets is a union
-// recorded in the forest.  Groups take 4 buckets at a time as in
-// k_uf_edges_skip.
-template <bool kW, bool kIn>
-__global__ void k_fe_scan(GraphView g, uint32_t *p, const uint32_t *nm_bits,
-                          const uint32_t *oldlab, const unsigned long long *ctl, uint32_t *err,
-                          unsigned long long *fe) {
-  const Lanes L = lanes();
-  const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
-  const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  const unsigned long long ml = ctl[kFMainLabel], mp = ctl[kFMainPiece];
-  for (uint64_t b0 = (uint64_t)group * 4; b0 < g.nbuckets; b0 += (uint64_t)ngroups * 4) {
-    const uint32_t b = (uint32_t)b0, m = min(4u, g.nbuckets - b);
-    uint32_t own[4], px[4], live = 0;
-#pragma unroll
-    for (uint32_t j = 0; j < 4; ++j) {
-      own[j] = j < m ? __ldg(g.bowner + b + j) : 0u;
-      const bool ok = j < m && ((nm_bits[own[j] >> 5] >> (own[j] & 31)) & 1u) && g.deg[own[j]] != 0;
-      live |= (ok ? 1u : 0u) << j;
-    }
-    if (!live) continue;
-    // decided on one lane and broadcast: the walk below shuffles within the
-    // group, so every lane must take the same buckets (lanes reading the
-    // parents at different moments could disagree)
-    uint32_t drop = 0;
-    if (L.gl == 0) {
-#pragma unroll
-      for (uint32_t j = 0; j < 4; ++j)
-        if (((live >> j) & 1u) && fe_joined(p, oldlab, own[j], ml, mp)) drop |= 1u << j;
-    }
-    live &= ~__shfl_sync(L.gmask, drop, L.gbase);
-    if (!live) continue;
-#pragma unroll
-    for (uint32_t j = 0; j < 4; ++j) px[j] = ((live >> j) & 1u) ? __ldcg(p + own[j]) : 0u;
-    walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 q) {
-      if (!((live >> j) & 1u)) return;
-      const uint32_t x = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
-      const uint32_t pj = px[0] * (j == 0) + px[1] * (j == 1) + px[2] * (j == 2) + px[3] * (j == 3);
-      uint32_t k[4], w[4];
-      lane_keys<kW>(q, L.gl, k, w);
-      uint32_t py[4];
-#pragma unroll
-      for (int t = 0; t < keys_per_lane<kW>(); ++t)
-        py[t] = (k[t] < kTombKey && k[t] != x && k[t] < g.V) ? __ldcg(p + k[t]) : pj;
-#pragma unroll
-      for (int t = 0; t < keys_per_lane<kW>(); ++t) {
-        if (py[t] == pj) continue;
-        if (kIn)
-          uf_union(p, k[t], x, err, fe);  // the slab edge k -> x of the graph
-        else
-          uf_union(p, x, k[t], err, fe);
-      }
-    });
-  }
 }
 
 // ---- static passes with a reverse graph: skip the largest set ----
@@ -629,57 +602,80 @@ __global__ void __launch_bounds__(kMainThreads)
                        ? (unsigned long long)(uint32_t)best + 1 : 0ull;
 }
 
-// The vertices outside the giant set that have an out- or in-edge, compacted
-// into list (one atomic per warp; any order).  Nothing without a giant set.
-__global__ void k_uf_outside_list(const uint32_t *p, uint32_t V, const uint32_t *deg,
-                                  const uint32_t *rdeg, unsigned long long *ctl, uint32_t *list) {
+// The vertices outside the giant set, as scan items of their out-buckets
+// (graph) and in-buckets (reverse graph).  Nothing without a giant set.
+__global__ void k_uf_outside_items(const uint32_t *p, uint32_t V, GraphView g, GraphView rg,
+                                   unsigned long long *ctl, uint32_t *items_out,
+                                   uint32_t *items_in) {
   const unsigned long long giant = ctl[kFGiant];
   if (giant == 0) return;
-  const uint32_t lane = threadIdx.x & 31u, stride = gridDim.x * blockDim.x;
+  const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < V; base += stride) {
-    const uint32_t x = base + lane;
-    const bool out = x < V && (deg[x] | rdeg[x]) != 0 && __ldcg(p + x) != (uint32_t)(giant - 1);
-    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, out);
-    if (!bal) continue;
-    uint32_t at = 0;
-    if (lane == 0) at = (uint32_t)atomicAdd(ctl + kFOutside, (unsigned long long)__popc(bal));
-    at = __shfl_sync(0xFFFFFFFFu, at, 0);
-    if (out) list[at + __popc(bal & ((1u << lane) - 1u))] = x;
+    const uint32_t x = base + (threadIdx.x & 31u);
+    uint32_t d = 0, rd = 0;
+    bool out = false;
+    if (x < V) {
+      d = g.deg[x];
+      rd = rg.deg[x];
+      out = (d | rd) != 0 && __ldcg(p + x) != (uint32_t)(giant - 1);
+    }
+    append_items(out && d != 0, out ? g.boff[x] : 0u, out ? g.boff[x + 1] : 0u, items_out,
+                 ctl + kFItemsOut);
+    append_items(out && rd != 0, out ? rg.boff[x] : 0u, out ? rg.boff[x + 1] : 0u, items_in,
+                 ctl + kFItemsIn);
   }
 }
 
-// The out-edges (kIn: the in-edges, through the reverse graph, whose key y is
-// the graph edge y -> x) of the listed vertices: unions of the edges whose
-// endpoints do not share a parent yet.  A group takes 4 list entries at a
-// time and walks one bucket of each per round, so vertices of several
-// buckets take several rounds.
-template <bool kW, bool kIn>
-__global__ void k_uf_scan_list(GraphView g, uint32_t *p, const uint32_t *list,
-                               const unsigned long long *ctl, uint32_t *err,
-                               unsigned long long *fe) {
+// The edges of the listed items (ctl[which] of them) of the graph (kIn: of
+// the reverse graph, whose key y is the graph edge y -> x): unions of the
+// edges whose endpoints do not share a parent yet.  A group takes 4 items at
+// a time and walks one bucket of each per round.  With kStop (the
+// decremental rescan) an item stops once its owner is joined to its main
+// piece: any piece still joined through it finds the edge from its own side.
+template <bool kW, bool kIn, bool kStop>
+__global__ void k_uf_scan_items(GraphView g, uint32_t *p, const uint32_t *items, int which,
+                                const uint32_t *oldlab, const unsigned long long *ctl,
+                                uint32_t *err, unsigned long long *fe) {
   const Lanes L = lanes();
   const uint32_t group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const uint32_t ngroups = (gridDim.x * blockDim.x) >> 3;
-  const uint64_t n = ctl[kFOutside];
+  const uint64_t n = ctl[which];
+  const unsigned long long ml = kStop ? ctl[kFMainLabel] : 0, mp = kStop ? ctl[kFMainPiece] : 0;
   for (uint64_t i0 = (uint64_t)group * 4; i0 < n; i0 += (uint64_t)ngroups * 4) {
     const uint32_t m = n - i0 < 4 ? (uint32_t)(n - i0) : 4u;
     uint32_t own[4], bk[4], be[4], px[4];
 #pragma unroll
     for (uint32_t j = 0; j < 4; ++j) {
-      own[j] = j < m ? __ldcg(list + i0 + j) : 0u;
-      bk[j] = be[j] = 0;
-      if (j < m && g.deg[own[j]] != 0) {
-        bk[j] = g.boff[own[j]];
-        be[j] = g.boff[own[j] + 1];
-      }
+      bk[j] = j < m ? __ldcg(items + i0 + j) : 0u;
+      own[j] = j < m ? __ldg(g.bowner + bk[j]) : 0u;
+      be[j] = j < m ? min(bk[j] + kItemBuckets, __ldg(g.boff + own[j] + 1)) : 0u;
     }
-#pragma unroll
-    for (uint32_t j = 0; j < 4; ++j) px[j] = bk[j] < be[j] ? __ldcg(p + own[j]) : 0u;
+    bool first = true;
     for (;;) {
       uint32_t live = 0;
 #pragma unroll
       for (uint32_t j = 0; j < 4; ++j) live |= (bk[j] < be[j] ? 1u : 0u) << j;
+      if (kStop) {
+        // decided on one lane and broadcast: the walk below shuffles within
+        // the group, so every lane must take the same buckets
+        uint32_t drop = 0;
+        if (L.gl == 0) {
+#pragma unroll
+          for (uint32_t j = 0; j < 4; ++j)
+            if (((live >> j) & 1u) && fe_joined(p, oldlab, own[j], ml, mp)) drop |= 1u << j;
+        }
+        drop = __shfl_sync(L.gmask, drop, L.gbase);
+        live &= ~drop;
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j)
+          if ((drop >> j) & 1u) be[j] = bk[j];
+      }
       if (!live) break;
+      if (first) {
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) px[j] = ((live >> j) & 1u) ? __ldcg(p + own[j]) : 0u;
+        first = false;
+      }
       walk4_set(g, L, bk, live, [&](uint32_t j, const uint4 q) {
         const uint32_t x = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
         const uint32_t pj = px[0] * (j == 0) + px[1] * (j == 1) + px[2] * (j == 2) + px[3] * (j == 3);
@@ -702,6 +698,26 @@ __global__ void k_uf_scan_list(GraphView g, uint32_t *p, const uint32_t *list,
       for (uint32_t j = 0; j < 4; ++j) bk[j] += bk[j] < be[j] ? 1u : 0u;
     }
   }
+}
+
+// Both item scans over the graph and its reverse graph.
+template <bool kStop>
+static void launch_item_scans(const GraphView &v, bool vw, const GraphView &rv, bool rw, int blocks,
+                              uint32_t *p, const uint32_t *items_out, const uint32_t *items_in,
+                              const uint32_t *oldlab, const unsigned long long *ctl, uint32_t *err,
+                              unsigned long long *fe, cudaStream_t s) {
+  if (vw)
+    k_uf_scan_items<true, false, kStop><<<blocks, 256, 0, s>>>(v, p, items_out, kFItemsOut, oldlab,
+                                                               ctl, err, fe);
+  else
+    k_uf_scan_items<false, false, kStop><<<blocks, 256, 0, s>>>(v, p, items_out, kFItemsOut, oldlab,
+                                                                ctl, err, fe);
+  if (rw)
+    k_uf_scan_items<true, true, kStop><<<blocks, 256, 0, s>>>(rv, p, items_in, kFItemsIn, oldlab,
+                                                              ctl, err, fe);
+  else
+    k_uf_scan_items<false, true, kStop><<<blocks, 256, 0, s>>>(rv, p, items_in, kFItemsIn, oldlab,
+                                                               ctl, err, fe);
 }
 
 // ---- vertex-range variants: only the listed ranges are touched ----
@@ -803,10 +819,12 @@ struct mk_wcc {
   bool forest_valid = false;  // fe spans every component (after a full static)
   mk_graph *rev = nullptr;    // reverse graph of the same edges (in-edges), optional
   // decremental scratch: batch edge set, old labels, handed-over forest
-  // edges, vertices outside the main pieces, ctl words
+  // edges, ctl words
   DevBuf<unsigned long long> dtab;
   DevBuf<unsigned long long> fe2;
-  DevBuf<uint32_t> oldlab, nm_bits;
+  DevBuf<uint32_t> oldlab;
+  // scan items (first buckets) of the graph and of the reverse graph
+  DevBuf<uint32_t> items_out, items_in;
   unsigned long long *fctl = nullptr;
   // last decremental call: forest edges lost, vertices rescanned, path taken
   uint64_t last_dead = 0, last_rescanned = 0;
@@ -829,6 +847,14 @@ struct mk_wcc {
 
 static int flat_grid(uint64_t n, int device) {
   return (int)std::min<uint64_t>(n / 256 + 1, (uint64_t)device_sm_count(device) * 8);
+}
+
+// Room for every scan item of the graph and of the reverse graph.
+static mk_status reserve_items(mk_wcc *w) {
+  mk_graph *g = w->g;
+  MK_CHECK(w->items_out.reserve(g->V + g->num_buckets / kItemBuckets + 1, &g->device_bytes));
+  MK_CHECK(w->items_in.reserve(g->V + w->rev->num_buckets / kItemBuckets + 1, &g->device_bytes));
+  return MK_OK;
 }
 
 // Unions of the out-edges of the selected vertices (all if sel is null), whose
@@ -855,11 +881,11 @@ static mk_status wcc_link(mk_wcc *w, const uint32_t *sel, cudaStream_t s) {
 }
 
 // Static passes.  With a reverse graph attached: sampled linking, then only
-// the listed vertices outside the largest sampled set have their out- and
-// in-edges scanned (k_uf_giant_sample; when that set holds under 3/4 of the
-// samples, every out-edge once instead: the device decides, the host
-// launches both forms and one returns at once); without one, every edge
-// through k_uf_edges_skip.
+// the vertices outside the largest sampled set have their out- and in-edges
+// scanned, as lists of bucket items (k_uf_giant_sample; when that set holds
+// under 3/4 of the samples, every out-edge once instead: the device decides,
+// the host launches both forms and one returns at once); without one, every
+// edge through k_uf_edges_skip.
 static mk_status wcc_static(mk_wcc *w, cudaStream_t s) {
   mk_graph *g = w->g;
   const uint32_t V = g->V;
@@ -868,8 +894,7 @@ static mk_status wcc_static(mk_wcc *w, cudaStream_t s) {
   w->forest_valid = true;
   if (!w->rev) return wcc_link(w, nullptr, s);
   const GraphView v = g->view(), rv = w->rev->view();
-  MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));  // the outside list
-  uint32_t *list = w->oldlab.ptr;
+  MK_CHECK(reserve_items(w));
   if (g->weighted)
     k_uf_sample<true><<<fg, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe);
   else
@@ -878,21 +903,16 @@ static mk_status wcc_static(mk_wcc *w, cudaStream_t s) {
   MK_CUDA(cudaMemsetAsync(w->fctl, 0, kFCtlWords * 8, s));
   k_uf_giant_sample<<<1, kMainThreads, 0, s>>>(w->parent, g->deg, V, 0x61A0000ull + (++w->calls),
                                                w->fctl);
-  k_uf_outside_list<<<fg, 256, 0, s>>>(w->parent, V, g->deg, w->rev->deg, w->fctl, list);
-  const int sm8 = device_sm_count(g->device) * 8;
-  const int ob = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1, (uint64_t)sm8);
-  const unsigned long long *giant = w->fctl + kFGiant;
-  if (g->weighted) {
-    k_uf_edges_skip<true><<<ob, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe, giant);
-    k_uf_scan_list<true, false><<<fg, 256, 0, s>>>(v, w->parent, list, w->fctl, w->err, w->fe);
-  } else {
-    k_uf_edges_skip<false><<<ob, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe, giant);
-    k_uf_scan_list<false, false><<<fg, 256, 0, s>>>(v, w->parent, list, w->fctl, w->err, w->fe);
-  }
-  if (w->rev->weighted)
-    k_uf_scan_list<true, true><<<fg, 256, 0, s>>>(rv, w->parent, list, w->fctl, w->err, w->fe);
+  k_uf_outside_items<<<fg, 256, 0, s>>>(w->parent, V, v, rv, w->fctl, w->items_out.ptr,
+                                        w->items_in.ptr);
+  const int ob = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1,
+                                         (uint64_t)device_sm_count(g->device) * 8);
+  if (g->weighted)
+    k_uf_edges_skip<true><<<ob, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe, w->fctl + kFGiant);
   else
-    k_uf_scan_list<false, true><<<fg, 256, 0, s>>>(rv, w->parent, list, w->fctl, w->err, w->fe);
+    k_uf_edges_skip<false><<<ob, 256, 0, s>>>(v, w->parent, nullptr, w->err, w->fe, w->fctl + kFGiant);
+  launch_item_scans<false>(v, g->weighted, rv, w->rev->weighted, fg, w->parent, w->items_out.ptr,
+                           w->items_in.ptr, nullptr, w->fctl, w->err, w->fe, s);
   k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, nullptr);
   MK_CUDA(cudaGetLastError());
   return MK_OK;
@@ -948,15 +968,16 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   if (!w->rev) return rebuild();
   MK_CHECK(w->fe2.reserve(V, &g->device_bytes));
   MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));
-  MK_CHECK(w->nm_bits.reserve(words, &g->device_bytes));
+  MK_CHECK(reserve_items(w));
   k_fe_collect<<<fg, 256, 0, s>>>(w->parent, w->fe, w->fe2.ptr, V, w->aff_labels, w->oldlab.ptr,
                                   w->aff_vertices);
   k_fe_union<<<fg, 256, 0, s>>>(w->parent, w->fe, w->fe2.ptr, V, w->aff_vertices, w->err);
   k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices);
   k_fe_main_sample<<<1, kMainThreads, 0, s>>>(w->parent, w->oldlab.ptr, w->aff_vertices, V,
                                               0x5EED0000ull + (++w->calls), w->fctl);
-  k_fe_nonmain<<<fg, 256, 0, s>>>(w->parent, w->oldlab.ptr, V, w->aff_vertices, g->deg,
-                                  w->rev->deg, w->nm_bits.ptr, w->fctl);
+  const GraphView rv = w->rev->view();
+  k_fe_nonmain<<<fg, 256, 0, s>>>(w->parent, w->oldlab.ptr, V, w->aff_vertices, v, rv,
+                                  w->items_out.ptr, w->items_in.ptr, w->fctl);
   MK_CUDA(cudaGetLastError());
   MK_CUDA(cudaMemcpyAsync(h, w->fctl, sizeof(h), cudaMemcpyDeviceToHost, s));
   MK_CUDA(cudaStreamSynchronize(s));
@@ -976,24 +997,9 @@ static mk_status wcc_decremental_forest(mk_wcc *w, const uint32_t *d_src, const 
   w->last_path = 1;
   w->last_rescanned = h[kFNmCount];
   if (h[kFNmCount]) {
-    // bucket-parallel: a hub outside its main piece spreads over many groups
-    const GraphView rv = w->rev->view();
-    const int ob = (int)std::min<uint64_t>(g->num_buckets * 8 / 256 + 1,
-                                           (uint64_t)device_sm_count(g->device) * 8);
-    const int ib = (int)std::min<uint64_t>(w->rev->num_buckets * 8 / 256 + 1,
-                                           (uint64_t)device_sm_count(g->device) * 8);
-    if (g->weighted)
-      k_fe_scan<true, false><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
-                                                 w->err, w->fe);
-    else
-      k_fe_scan<false, false><<<ob, 256, 0, s>>>(v, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
-                                                  w->err, w->fe);
-    if (w->rev->weighted)
-      k_fe_scan<true, true><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
-                                                w->err, w->fe);
-    else
-      k_fe_scan<false, true><<<ib, 256, 0, s>>>(rv, w->parent, w->nm_bits.ptr, w->oldlab.ptr, w->fctl,
-                                                 w->err, w->fe);
+    // item lists: a hub outside its main piece spreads over many groups
+    launch_item_scans<true>(v, g->weighted, rv, w->rev->weighted, fg, w->parent, w->items_out.ptr,
+                            w->items_in.ptr, w->oldlab.ptr, w->fctl, w->err, w->fe, s);
     k_uf_compress<<<fg, 256, 0, s>>>(w->parent, V, w->aff_vertices);
   }
   MK_CUDA(cudaGetLastError());
@@ -1228,6 +1234,27 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src, const uint32_t *d
   return w->timer.stop(ms_out);
 }
 
+// Loads the kernels of the static passes and of the decremental repair: with
+// lazy module loading the first launch of each would otherwise pay for it
+// inside the first (timed) call.
+static mk_status preload_kernels() {
+  cudaFuncAttributes a;
+  const void *fns[] = {
+      (const void *)k_uf_init, (const void *)k_uf_compress, (const void *)k_uf_reset,
+      (const void *)k_uf_sample<false>, (const void *)k_uf_sample<true>,
+      (const void *)k_uf_edges_skip<false>, (const void *)k_uf_edges_skip<true>,
+      (const void *)k_uf_giant_sample, (const void *)k_uf_outside_items,
+      (const void *)k_uf_scan_items<false, false, false>, (const void *)k_uf_scan_items<true, false, false>,
+      (const void *)k_uf_scan_items<false, true, false>, (const void *)k_uf_scan_items<true, true, false>,
+      (const void *)k_uf_scan_items<false, false, true>, (const void *)k_uf_scan_items<true, false, true>,
+      (const void *)k_uf_scan_items<false, true, true>, (const void *)k_uf_scan_items<true, true, true>,
+      (const void *)k_dh_insert, (const void *)k_fe_dead<false>, (const void *)k_fe_dead<true>,
+      (const void *)k_fe_count_aff, (const void *)k_fe_collect, (const void *)k_fe_union,
+      (const void *)k_fe_main_sample, (const void *)k_fe_nonmain};
+  for (const void *f : fns) MK_CUDA(cudaFuncGetAttributes(&a, f));
+  return MK_OK;
+}
+
 mk_status mk_wcc_set_reverse(mk_wcc *w, mk_graph *g_rev) {
   if (!w) return fail(MK_ERR_INVALID, "mk_wcc_set_reverse: null handle");
   mk_graph *g = w->g;
@@ -1239,10 +1266,11 @@ mk_status mk_wcc_set_reverse(mk_wcc *w, mk_graph *g_rev) {
     // the piece-rescan scratch, and a batch set sized for the graph's batch
     // scratch, allocated here rather than inside a timed decremental call
     DeviceGuard dg(g->device);
-    const size_t V = g->V, words = (V + 31) / 32;
+    const size_t V = g->V;
     MK_CHECK(w->fe2.reserve(V, &g->device_bytes));
     MK_CHECK(w->oldlab.reserve(V, &g->device_bytes));
-    MK_CHECK(w->nm_bits.reserve(words, &g->device_bytes));
+    MK_CHECK(reserve_items(w));
+    MK_CHECK(preload_kernels());
     uint64_t cap = 1024;
     while (cap < 2ull * std::min<uint64_t>(g->applied.cap, g->V)) cap <<= 1;
     MK_CHECK(w->dtab.reserve(cap, &g->device_bytes));
@@ -1287,7 +1315,8 @@ mk_status mk_wcc_destroy(mk_wcc *w) {
   w->dtab.release();
   w->fe2.release();
   w->oldlab.release();
-  w->nm_bits.release();
+  w->items_out.release();
+  w->items_in.release();
   w->staging.release();
   w->ranges.release();
   delete w;

@@ -316,6 +316,69 @@ def test_wcc_decremental_over_the_spanning_forest(with_rev, weighted):
         assert 1 not in paths and (2 in paths or 3 in paths)
 
 
+def _core_and_leaves(rng):
+    """A core of 1,000 vertices (ring plus 8 random core edges each), 1,500
+    leaves joined by leaf -> core edges, 1,500 leaves reached only by core ->
+    leaf edges (out-degree 0: linked by no sample, only by their in-edges),
+    50 separate pairs and 252 isolated vertices (4,352 in all); no
+    duplicate edges."""
+    core = np.arange(1000, dtype=np.uint32)
+    s = [core, np.repeat(core, 8)]
+    d = [np.roll(core, -1), rng.integers(0, 1000, 8000).astype(np.uint32)]
+    out_leaves = np.arange(1000, 2500, dtype=np.uint32)
+    in_leaves = np.arange(2500, 4000, dtype=np.uint32)
+    s += [out_leaves, rng.integers(0, 1000, 1500).astype(np.uint32)]
+    d += [rng.integers(0, 1000, 1500).astype(np.uint32), in_leaves]
+    s.append(np.arange(4000, 4100, 2, dtype=np.uint32))
+    d.append(np.arange(4001, 4100, 2, dtype=np.uint32))
+    s, d = np.concatenate(s), np.concatenate(d)
+    keep = s != d
+    s, d = s[keep], d[keep]
+    _, first = np.unique(s.astype(np.uint64) << np.uint64(32) | d, return_index=True)
+    first.sort()
+    return 4352, s[first], d[first]
+
+
+def _rings(rng):
+    """512 separate rings of 8 vertices: no sampled set holds more than a
+    few samples."""
+    V = 4096
+    x = np.arange(V, dtype=np.uint32)
+    return V, x, (x & ~np.uint32(7)) | ((x + 1) & np.uint32(7))
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("shape", ["core_and_leaves", "rings"])
+def test_wcc_static_with_reverse_graph(shape, weighted):
+    """Static WCC with a reverse graph attached: when one sampled set holds
+    most samples (core_and_leaves) only the vertices outside it have their
+    out- and in-edges scanned, and leaves reached only by in-edges must be
+    joined through the reverse graph; with no such set (rings) every
+    out-edge is scanned once.  Labels equal the oracle's, repeated calls
+    included, and after a deletion batch that falls back to them."""
+    rng = np.random.default_rng(71)
+    V, s, d = _core_and_leaves(rng) if shape == "core_and_leaves" else _rings(rng)
+    w = (np.arange(len(s)) % 40 + 1).astype(np.uint32)
+    G, O = make_pair(V, s, d, w=w if weighted else None, weighted=weighted)
+    Gr = mk.DynamicGraph(V, degree_hints=degree_hints(d, V), reverse=True)
+    Gr.InsertEdges(to_dev(s), to_dev(d))
+    wcc = mk.WCC(G)
+    wcc.set_reverse(Gr)
+    for _ in range(3):
+        wcc.Static()
+        np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+    # the core's ring and random edges go: most of the graph is affected
+    ds, dd = s[:9000], d[:9000]
+    tds, tdd = to_dev(ds), to_dev(dd)
+    G.DeleteEdges(tds, tdd)
+    Gr.DeleteEdges(tds, tdd)
+    O.delete(ds, dd)
+    wcc.Decremental(tds, tdd)
+    np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+    wcc.Static()
+    np.testing.assert_array_equal(wcc.Labels(), O.wcc())
+
+
 @pytest.mark.parametrize("weighted", [False, True])
 def test_wcc_decremental_rescans_only_split_off_pieces(weighted):
     """A hub with 2,047 leaves (leaf -> hub) and 1,500 leaf -> leaf edges:
