@@ -156,7 +156,10 @@ __global__ void k_uf_reset(uint32_t *p, uint32_t V, const uint32_t *aff_labels, 
 // between vertices already connected keeps the result exact, and it works for
 // every component at once (the members of a graph set included).
 // Sampled linking: each selected vertex (all if sel_bits is null) unions
-// with the first two keys of its first head slab.  A thread takes 4 vertices
+// with the first two live keys among the key slots of the first 32-byte
+// sector of its first head slab (4 keys weighted, 8 unweighted; deleted
+// edges leave tombstones there, so the first two slots alone link fewer
+// vertices on a graph that has seen deletions).  A thread takes 4 vertices
 // a stride apart per round, so their degree, offset and slab reads are in
 // flight together before the unions.
 template <bool kW>
@@ -173,19 +176,36 @@ __global__ void k_uf_sample(GraphView g, uint32_t *p, const uint32_t *sel_bits, 
       ok[j] = u < g.V && g.deg[u] != 0 &&
               (!sel_bits || ((sel_bits[uu[j] >> 5] >> (uu[j] & 31)) & 1u));
     }
+    uint4 qa[4], qb[4];
 #pragma unroll
     for (uint32_t j = 0; j < 4; ++j) {
-      k0[j] = k1[j] = kEmptyKey;
       if (ok[j]) {
-        const uint32_t *w = reinterpret_cast<const uint32_t *>(g.slabs + 8ull * g.boff[uu[j]]);
-        k0[j] = w[0];
-        k1[j] = kW ? w[2] : w[1];
+        const uint4 *q = g.slabs + 8ull * g.boff[uu[j]];
+        qa[j] = q[0];
+        qb[j] = q[1];
       }
     }
 #pragma unroll
     for (uint32_t j = 0; j < 4; ++j) {
-      if (k0[j] < kTombKey && k0[j] != uu[j]) uf_union(p, uu[j], k0[j], err, fe);
-      if (k1[j] < kTombKey && k1[j] != uu[j]) uf_union(p, uu[j], k1[j], err, fe);
+      k0[j] = k1[j] = kEmptyKey;
+      if (!ok[j]) continue;
+      constexpr int kN = kW ? 4 : 8;
+      const uint32_t keys[8] = {qa[j].x, kW ? qa[j].z : qa[j].y, kW ? qb[j].x : qa[j].z,
+                                kW ? qb[j].z : qa[j].w, qb[j].x, qb[j].y, qb[j].z, qb[j].w};
+#pragma unroll
+      for (int t = 0; t < kN; ++t) {
+        const uint32_t k = keys[t];
+        if (k >= kTombKey || k == uu[j]) continue;
+        if (k0[j] == kEmptyKey)
+          k0[j] = k;
+        else if (k1[j] == kEmptyKey)
+          k1[j] = k;
+      }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+      if (k0[j] < kTombKey) uf_union(p, uu[j], k0[j], err, fe);
+      if (k1[j] < kTombKey) uf_union(p, uu[j], k1[j], err, fe);
     }
   }
 }
