@@ -294,7 +294,7 @@ enum : int {
 // vertex (its owner is bowner[item]), so a hub's buckets spread over many
 // groups.  A vertex with nb buckets takes ceil(nb / kItemBuckets) items: a
 // list never holds more than V + nbuckets / kItemBuckets of them.
-constexpr uint32_t kItemBuckets = 16;
+constexpr uint32_t kItemBuckets = 4;
 
 // Appends the items of buckets [b0, b1) of every lane with sel set (one
 // atomic per warp; any order).  All 32 lanes of the warp call it together.
