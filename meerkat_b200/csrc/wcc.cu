@@ -296,12 +296,22 @@ enum : int {
 // list never holds more than V + nbuckets / kItemBuckets of them.
 constexpr uint32_t kItemBuckets = 4;
 
-// Appends the items of buckets [b0, b1) of every lane with sel set (one
-// atomic per warp; any order).  All 32 lanes of the warp call it together.
-__device__ __forceinline__ void append_items(bool sel, uint32_t b0, uint32_t b1, uint32_t *items,
+// Vertices per lane of the list-building passes: a warp takes 256 at a time
+// and appends their items with one atomic (one per warp and 32 vertices
+// queued tens of thousands of atomics on the same word).
+constexpr int kPerLane = 8;
+
+// Appends the items of buckets [b0[i], b1[i]) of every lane (empty ranges
+// add none), one atomic per warp; any order.  All 32 lanes of the warp call
+// it together.
+__device__ __forceinline__ void append_items(const uint32_t (&b0)[kPerLane],
+                                             const uint32_t (&b1)[kPerLane], uint32_t *items,
                                              unsigned long long *count) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t n = (sel && b1 > b0) ? (b1 - b0 + kItemBuckets - 1) / kItemBuckets : 0u;
+  uint32_t n = 0;
+#pragma unroll
+  for (int i = 0; i < kPerLane; ++i)
+    n += b1[i] > b0[i] ? (b1[i] - b0[i] + kItemBuckets - 1) / kItemBuckets : 0u;
   uint32_t incl = n;
 #pragma unroll
   for (uint32_t o = 1; o < 32; o <<= 1) {
@@ -313,7 +323,26 @@ __device__ __forceinline__ void append_items(bool sel, uint32_t b0, uint32_t b1,
   uint32_t at = 0;
   if (lane == 0) at = (uint32_t)atomicAdd(count, (unsigned long long)total);
   at = __shfl_sync(0xFFFFFFFFu, at, 0) + incl - n;
-  for (uint32_t i = 0; i < n; ++i) items[at + i] = b0 + i * kItemBuckets;
+#pragma unroll
+  for (int i = 0; i < kPerLane; ++i)
+    for (uint32_t b = b0[i]; b < b1[i]; b += kItemBuckets) items[at++] = b;
+}
+
+// Adds v summed over the block to *dst with one atomic.  Every thread of the
+// block calls it (blockDim.x a multiple of 32).
+__device__ __forceinline__ void block_add(unsigned long long v, unsigned long long *dst) {
+  __shared__ unsigned long long part[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  if ((threadIdx.x & 31u) == 0) part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    unsigned long long t = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+    if (threadIdx.x == 0 && t) atomicAdd(dst, t);
+  }
+  __syncthreads();  // part is reused by the next call
 }
 
 // Set of the batch's deleted edges (slab orientation a << 32 | b): open
@@ -399,7 +428,7 @@ __global__ void k_fe_dead(GraphView g, unsigned long long *fe, const unsigned lo
 }
 
 // Step 1b: vertices of the affected components (labels still compressed),
-// one atomic per warp.
+// one atomic per block.
 __global__ void k_fe_count_aff(const uint32_t *p, uint32_t V, const uint32_t *aff_labels,
                                unsigned long long *ctl) {
   unsigned long long n = 0;
@@ -407,9 +436,7 @@ __global__ void k_fe_count_aff(const uint32_t *p, uint32_t V, const uint32_t *af
     const uint32_t r = p[x];
     n += (aff_labels[r >> 5] >> (r & 31)) & 1u;
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
-  if ((threadIdx.x & 31u) == 0 && n) atomicAdd(ctl + kFAffected, n);
+  block_add(n, ctl + kFAffected);
 }
 
 // Step 2a: every vertex of an affected component keeps its old label, is
@@ -507,49 +534,47 @@ __global__ void __launch_bounds__(kMainThreads)
 // Step 3b (after compressing the affected vertices): the affected vertices
 // outside their component's main piece, as scan items of their out-buckets
 // (graph) and in-buckets (reverse graph); their count and out- plus
-// in-degrees, and the graph's live edge count.
+// in-degrees, and the graph's live edge count (one atomic per block).
 __global__ void k_fe_nonmain(const uint32_t *p, const uint32_t *oldlab, uint32_t V,
                              const uint32_t *aff_vertices, GraphView g, GraphView rg,
                              uint32_t *items_out, uint32_t *items_in, unsigned long long *ctl) {
-  const uint32_t words = (V + 31) / 32, lane = threadIdx.x & 31u;
-  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const unsigned long long ml = ctl[kFMainLabel], mp = ctl[kFMainPiece];
   unsigned long long ends = 0, edges = 0, count = 0;
-  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < words * 32u;
-       base += stride) {
-    const uint32_t x = base + lane;
-    bool nm = false;
-    uint32_t d = 0, rd = 0;
-    if (x < V) {
-      d = g.deg[x];
+  for (uint64_t base = warp * 32 * kPerLane; base < V; base += nwarps * 32 * kPerLane) {
+    uint32_t ob[kPerLane], oe[kPerLane], ib[kPerLane], ie[kPerLane];
+#pragma unroll
+    for (int i = 0; i < kPerLane; ++i) {
+      ob[i] = oe[i] = ib[i] = ie[i] = 0;
+      const uint64_t xx = base + (uint64_t)i * 32 + lane;
+      if (xx >= V) continue;
+      const uint32_t x = (uint32_t)xx;
+      const uint32_t d = g.deg[x];
       edges += d;
-      if ((aff_vertices[x >> 5] >> (x & 31)) & 1u) {
-        const uint32_t r = oldlab[x];
-        const uint32_t main_piece = (ml && r == ml - 1) ? (uint32_t)(mp - 1) : __ldcg(p + r);
-        nm = __ldcg(p + x) != main_piece;
-        if (nm) {
-          rd = rg.deg[x];
-          ends += d + rd;
-          ++count;
-        }
+      if (!((aff_vertices[x >> 5] >> (x & 31)) & 1u)) continue;
+      const uint32_t r = oldlab[x];
+      const uint32_t main_piece = (ml && r == ml - 1) ? (uint32_t)(mp - 1) : __ldcg(p + r);
+      if (__ldcg(p + x) == main_piece) continue;
+      const uint32_t rd = rg.deg[x];
+      ends += d + rd;
+      ++count;
+      if (d) {
+        ob[i] = g.boff[x];
+        oe[i] = g.boff[x + 1];
+      }
+      if (rd) {
+        ib[i] = rg.boff[x];
+        ie[i] = rg.boff[x + 1];
       }
     }
-    append_items(nm && d != 0, nm ? g.boff[x] : 0u, nm ? g.boff[x + 1] : 0u, items_out,
-                 ctl + kFItemsOut);
-    append_items(nm && rd != 0, nm ? rg.boff[x] : 0u, nm ? rg.boff[x + 1] : 0u, items_in,
-                 ctl + kFItemsIn);
+    append_items(ob, oe, items_out, ctl + kFItemsOut);
+    append_items(ib, ie, items_in, ctl + kFItemsIn);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    ends += __shfl_xor_sync(0xFFFFFFFFu, ends, o);
-    edges += __shfl_xor_sync(0xFFFFFFFFu, edges, o);
-    count += __shfl_xor_sync(0xFFFFFFFFu, count, o);
-  }
-  if (lane == 0) {
-    if (count) atomicAdd(ctl + kFNmCount, count);
-    if (ends) atomicAdd(ctl + kFNmEnds, ends);
-    if (edges) atomicAdd(ctl + kFEdges, edges);
-  }
+  block_add(count, ctl + kFNmCount);
+  block_add(ends, ctl + kFNmEnds);
+  block_add(edges, ctl + kFEdges);
 }
 
 // True once x's set holds its component's main piece: its root is the
@@ -629,20 +654,30 @@ __global__ void k_uf_outside_items(const uint32_t *p, uint32_t V, GraphView g, G
                                    uint32_t *items_in) {
   const unsigned long long giant = ctl[kFGiant];
   if (giant == 0) return;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; base < V; base += stride) {
-    const uint32_t x = base + (threadIdx.x & 31u);
-    uint32_t d = 0, rd = 0;
-    bool out = false;
-    if (x < V) {
-      d = g.deg[x];
-      rd = rg.deg[x];
-      out = (d | rd) != 0 && __ldcg(p + x) != (uint32_t)(giant - 1);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint64_t base = warp * 32 * kPerLane; base < V; base += nwarps * 32 * kPerLane) {
+    uint32_t ob[kPerLane], oe[kPerLane], ib[kPerLane], ie[kPerLane];
+#pragma unroll
+    for (int i = 0; i < kPerLane; ++i) {
+      ob[i] = oe[i] = ib[i] = ie[i] = 0;
+      const uint64_t xx = base + (uint64_t)i * 32 + lane;
+      if (xx >= V) continue;
+      const uint32_t x = (uint32_t)xx;
+      const uint32_t d = g.deg[x], rd = rg.deg[x];
+      if ((d | rd) == 0 || __ldcg(p + x) == (uint32_t)(giant - 1)) continue;
+      if (d) {
+        ob[i] = g.boff[x];
+        oe[i] = g.boff[x + 1];
+      }
+      if (rd) {
+        ib[i] = rg.boff[x];
+        ie[i] = rg.boff[x + 1];
+      }
     }
-    append_items(out && d != 0, out ? g.boff[x] : 0u, out ? g.boff[x + 1] : 0u, items_out,
-                 ctl + kFItemsOut);
-    append_items(out && rd != 0, out ? rg.boff[x] : 0u, out ? rg.boff[x + 1] : 0u, items_in,
-                 ctl + kFItemsIn);
+    append_items(ob, oe, items_out, ctl + kFItemsOut);
+    append_items(ib, ie, items_in, ctl + kFItemsIn);
   }
 }
 
