@@ -448,11 +448,16 @@ mk_status mk_wcc_decremental(mk_wcc *w, const uint32_t *d_src,
                              float *ms_out);
 /* Attaches the reverse graph of the same edges (in-edges; the caller keeps
  * it in step with g, as for mk_traversal_set_reverse), or detaches it with
- * NULL.  Decremental calls use it to rescan the pieces a deletion split off.
- * Attaching allocates the rescan scratch (about 17 bytes per vertex) and a
- * set for batches of up to min(the graph's batch scratch, V) edges (size the
- * batch scratch first with mk_graph_reserve_batch); a larger batch grows the
- * set on its first decremental call.
+ * NULL.  Decremental calls use it to rescan the pieces a deletion split off;
+ * static calls (mk_wcc_static) use it to scan only the vertices outside the
+ * largest set that sampled linking formed, when that set holds at least 3/4
+ * of 2,048 sampled vertices: their out-edges and, through it, their
+ * in-edges, so the edges inside that set are never read.  Attaching
+ * allocates the scratch (about 20 bytes per vertex plus 1 per bucket of
+ * either graph), loads the kernels of both paths, and sizes a set for
+ * batches of up to min(the graph's batch scratch, V) edges (size the batch
+ * scratch first with mk_graph_reserve_batch); a larger batch grows the set
+ * on its first decremental call.
  *
  * Every static, incremental and decremental call keeps a spanning forest:
  * the edge of each union that hooked a root.  mk_wcc_decremental then
