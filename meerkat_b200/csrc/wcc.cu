@@ -99,6 +99,25 @@ __device__ __forceinline__ void uf_union(uint32_t *p, uint32_t a, uint32_t b, ui
   atomicOr(err, kErrTimeout);
 }
 
+// uf_union that returns a vertex of the joined set which was its root during
+// the call (kEmptyKey when the retry limit ran out).  An edge pass keeps it
+// as the owner's parent for the owner's next keys: a key whose parent equals
+// it is in the same set, so the hook just made is not tried again key by key.
+__device__ __forceinline__ uint32_t uf_union_root(uint32_t *p, uint32_t a, uint32_t b,
+                                                  uint32_t *err, unsigned long long *fe) {
+  for (uint32_t it = 0; it < kUfLimit; ++it) {
+    const uint32_t ra = uf_find(p, a), rb = uf_find(p, b);
+    if (ra == rb) return ra;
+    const uint32_t hi = ra > rb ? ra : rb, lo = ra > rb ? rb : ra;
+    if (atomicCAS(p + hi, hi, lo) == hi) {
+      if (fe) fe[hi] = fedge(a, b);
+      return lo;
+    }
+  }
+  atomicOr(err, kErrTimeout);
+  return kEmptyKey;
+}
+
 // Resets the selected vertices (all if sel_bits is null) to their own set
 // and, with fe, empties their forest slots.
 __global__ void k_uf_init(uint32_t *p, uint32_t V, const uint32_t *sel_bits = nullptr,
@@ -260,16 +279,22 @@ __global__ void k_uf_edges_skip(GraphView g, uint32_t *p, const uint32_t *sel_bi
     walk4_levels(g, L, b, m, [&](uint32_t j, const uint4 q) {
       if (!((live >> j) & 1u)) return;
       const uint32_t u = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
-      const uint32_t pj = pu[0] * (j == 0) + pu[1] * (j == 1) + pu[2] * (j == 2) + pu[3] * (j == 3);
+      uint32_t pj = pu[0] * (j == 0) + pu[1] * (j == 1) + pu[2] * (j == 2) + pu[3] * (j == 3);
       uint32_t k[4], w[4];
       lane_keys<kW>(q, L.gl, k, w);
       uint32_t pv[4];
+      bool ok[4];
+#pragma unroll
+      for (int t = 0; t < keys_per_lane<kW>(); ++t) {
+        ok[t] = k[t] < kTombKey && k[t] != u;
+        pv[t] = ok[t] ? __ldcg(p + k[t]) : 0u;
+      }
 #pragma unroll
       for (int t = 0; t < keys_per_lane<kW>(); ++t)
-        pv[t] = (k[t] < kTombKey && k[t] != u) ? __ldcg(p + k[t]) : pj;
+        if (ok[t] && pv[t] != pj) pj = uf_union_root(p, u, k[t], err, fe);
 #pragma unroll
-      for (int t = 0; t < keys_per_lane<kW>(); ++t)
-        if (pv[t] != pj) uf_union(p, u, k[t], err, fe);
+      for (uint32_t i = 0; i < 4; ++i)
+        if (i == j) pu[i] = pj;
     });
   }
 }
@@ -733,21 +758,25 @@ __global__ void k_uf_scan_items(GraphView g, uint32_t *p, const uint32_t *items,
       }
       walk4_set(g, L, bk, live, [&](uint32_t j, const uint4 q) {
         const uint32_t x = own[0] * (j == 0) + own[1] * (j == 1) + own[2] * (j == 2) + own[3] * (j == 3);
-        const uint32_t pj = px[0] * (j == 0) + px[1] * (j == 1) + px[2] * (j == 2) + px[3] * (j == 3);
+        uint32_t pj = px[0] * (j == 0) + px[1] * (j == 1) + px[2] * (j == 2) + px[3] * (j == 3);
         uint32_t k[4], w[4];
         lane_keys<kW>(q, L.gl, k, w);
         uint32_t py[4];
-#pragma unroll
-        for (int t = 0; t < keys_per_lane<kW>(); ++t)
-          py[t] = (k[t] < kTombKey && k[t] != x && k[t] < g.V) ? __ldcg(p + k[t]) : pj;
+        bool ok[4];
 #pragma unroll
         for (int t = 0; t < keys_per_lane<kW>(); ++t) {
-          if (py[t] == pj) continue;
-          if (kIn)
-            uf_union(p, k[t], x, err, fe);  // the slab edge k -> x of the graph
-          else
-            uf_union(p, x, k[t], err, fe);
+          ok[t] = k[t] < kTombKey && k[t] != x && k[t] < g.V;
+          py[t] = ok[t] ? __ldcg(p + k[t]) : 0u;
         }
+#pragma unroll
+        for (int t = 0; t < keys_per_lane<kW>(); ++t) {
+          if (!ok[t] || py[t] == pj) continue;
+          // kIn: the slab edge k -> x of the graph
+          pj = kIn ? uf_union_root(p, k[t], x, err, fe) : uf_union_root(p, x, k[t], err, fe);
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < 4; ++i)
+          if (i == j) px[i] = pj;
       });
 #pragma unroll
       for (uint32_t j = 0; j < 4; ++j) bk[j] += bk[j] < be[j] ? 1u : 0u;
