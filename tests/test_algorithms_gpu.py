@@ -347,17 +347,36 @@ def _rings(rng):
     return V, x, (x & ~np.uint32(7)) | ((x + 1) & np.uint32(7))
 
 
+def _hubs_outside(rng):
+    """A core of 6,000 vertices (ring plus 4 random core edges each) holds
+    most samples; outside it a source hub with 700 out-edges to its own
+    leaves and a sink hub with 700 in-edges from its own leaves: both hubs
+    span many buckets, so their edges are listed as several scan items."""
+    core = np.arange(6000, dtype=np.uint32)
+    s = [core, np.repeat(core, 4), np.full(700, 6000, np.uint32), np.arange(6801, 7501, dtype=np.uint32)]
+    d = [np.roll(core, -1), rng.integers(0, 6000, 24000).astype(np.uint32),
+         np.arange(6001, 6701, dtype=np.uint32), np.full(700, 6800, np.uint32)]
+    s, d = np.concatenate(s), np.concatenate(d)
+    keep = s != d
+    s, d = s[keep], d[keep]
+    _, first = np.unique(s.astype(np.uint64) << np.uint64(32) | d, return_index=True)
+    first.sort()
+    return 8192, s[first], d[first]
+
+
 @pytest.mark.parametrize("weighted", [False, True])
-@pytest.mark.parametrize("shape", ["core_and_leaves", "rings"])
+@pytest.mark.parametrize("shape", ["core_and_leaves", "rings", "hubs_outside"])
 def test_wcc_static_with_reverse_graph(shape, weighted):
     """Static WCC with a reverse graph attached: when one sampled set holds
     most samples (core_and_leaves) only the vertices outside it have their
     out- and in-edges scanned, and leaves reached only by in-edges must be
     joined through the reverse graph; with no such set (rings) every
-    out-edge is scanned once.  Labels equal the oracle's, repeated calls
+    out-edge is scanned once; hubs outside the set (hubs_outside) are split
+    into several scan items.  Labels equal the oracle's, repeated calls
     included, and after a deletion batch that falls back to them."""
     rng = np.random.default_rng(71)
-    V, s, d = _core_and_leaves(rng) if shape == "core_and_leaves" else _rings(rng)
+    V, s, d = {"core_and_leaves": _core_and_leaves, "rings": _rings,
+               "hubs_outside": _hubs_outside}[shape](rng)
     w = (np.arange(len(s)) % 40 + 1).astype(np.uint32)
     G, O = make_pair(V, s, d, w=w if weighted else None, weighted=weighted)
     Gr = mk.DynamicGraph(V, degree_hints=degree_hints(d, V), reverse=True)
