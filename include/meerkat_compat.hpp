@@ -166,6 +166,14 @@ class Traversal {
     check(mk_traversal_distances(t_, out.data()), "Distances");
     return out;
   }
+  // Extension (no counterpart in the reference): attaches the reverse graph
+  // of the same edges (a DynGraph with a Rev*EdgePolicy, weighted for SSSP),
+  // which the caller updates with every batch; decremental calls then repair
+  // from in-edges (mk_traversal_set_reverse).
+  template <class RevGraph>
+  void SetReverse(RevGraph &Gr) {
+    check(mk_traversal_set_reverse(t_, Gr.handle()), "SetReverse");
+  }
 
  private:
   uint32_t N_;
@@ -294,6 +302,14 @@ class WCC {
     std::vector<uint32_t> out(N_);
     check(mk_wcc_labels(w_, out.data()), "Labels");
     return out;
+  }
+  // Extension: attaches the reverse graph of the same edges, which the
+  // caller updates with every batch; static calls then scan only the edges
+  // of the vertices outside the largest sampled set, decremental calls only
+  // the pieces a deletion split off (mk_wcc_set_reverse).
+  template <class RevGraph>
+  void SetReverse(RevGraph &Gr) {
+    check(mk_wcc_set_reverse(w_, Gr.handle()), "SetReverse");
   }
 
  private:

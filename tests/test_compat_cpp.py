@@ -65,9 +65,13 @@ def test_reference_file_workflow_matches_oracle(tmp_path, op):
 
 
 @pytest.mark.gpu
-def test_reference_style_driver_matches_oracle(tmp_path):
+@pytest.mark.parametrize("rev", ["", "rev"])
+def test_reference_style_driver_matches_oracle(tmp_path, rev):
+    """The reference's driver sequence on the shim; with rev the algorithms
+    also get reverse graphs (SetReverse) kept in step with every batch."""
     exe = build_driver(tmp_path)
-    r = subprocess.run([str(exe), "12"], capture_output=True, text=True, timeout=300)
+    r = subprocess.run([str(exe), "12"] + ([rev] if rev else []), capture_output=True, text=True,
+                       timeout=300)
     assert r.returncode == 0, r.stderr
     lines = r.stdout.strip().splitlines()
     got = np.array([list(map(int, ln.split())) for ln in lines[1:]], dtype=np.uint64)
