@@ -659,7 +659,9 @@ class WCC(_Timed):
 
     def set_reverse(self, G_rev: Optional[DynamicGraph]) -> None:
         """Attaches the reverse graph of the same edges (kept in step by the
-        caller); decremental calls rescan split-off pieces through it."""
+        caller).  Static calls then scan only the out- and in-edges of the
+        vertices outside the largest sampled set; decremental calls rescan
+        split-off pieces through it.  None detaches it."""
         self._rev = G_rev
         check(lib().mk_wcc_set_reverse(self._h, G_rev.handle if G_rev is not None else None),
               "mk_wcc_set_reverse")
