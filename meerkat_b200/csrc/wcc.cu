@@ -628,14 +628,15 @@ __global__ void __launch_bounds__(kMainThreads)
                       unsigned long long *ctl) {
   __shared__ uint32_t keys[kMainSlots], cnts[kMainSlots];
   __shared__ unsigned long long best;
+  __shared__ uint32_t drawn;  // samples with out-edges
   for (uint32_t i = threadIdx.x; i < kMainSlots; i += blockDim.x) {
     keys[i] = 0xFFFFFFFFu;
     cnts[i] = 0u;
   }
-  if (threadIdx.x == 0) best = 0;
-  __syncthreads();
-  __shared__ uint32_t drawn;
-  if (threadIdx.x == 0) drawn = 0;
+  if (threadIdx.x == 0) {
+    best = 0;
+    drawn = 0;
+  }
   __syncthreads();
   for (uint32_t j = threadIdx.x; j < kMainSamples; j += blockDim.x) {
     unsigned long long h = seed + 0x9E3779B97F4A7C15ull * (j + 1);
